@@ -1,0 +1,150 @@
+/*
+ * nodals_b200 -- C ABI of the B200 steady P1+BF3/P0 SIMPLE solver.
+ *
+ * The reference (JD63021/NodalS, gpu/serial_cuda) exposes no library API:
+ * its drop-in surface is the process boundary of nodals_gpu_h8_{fp32,fp64}
+ * (argv flags gpu/serial_cuda/h8_main_base.cu:1787-1911, NODALS_GPU_* stdout
+ * markers, exit codes 0/35/90 at :2202-2203, --vtu-out files).  This header
+ * is the layer underneath the drop-in executable of this package; each entry
+ * point names the reference step it replaces.
+ *
+ * Conventions
+ *  - every call returns an int status: NDS_OK (0) or a negative NDS_E_* code;
+ *    nds_last_error() gives the message of the calling thread's last failure;
+ *  - nothing throws across this boundary and nothing aborts the process;
+ *  - the caller owns all host arrays passed in or out; the library owns all
+ *    device memory;
+ *  - one solver handle per thread; a handle is not internally synchronised;
+ *  - the GPU solver entry points fail loudly (NDS_E_CUDA) when no CUDA
+ *    device or kernel image is available: there is no CPU fallback.
+ */
+#ifndef NODALS_B200_H
+#define NODALS_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NDS_OK 0
+#define NDS_E_INVALID (-1)      /* bad argument / option (reference: "H8 usage error") */
+#define NDS_E_SETUP (-2)        /* mesh or setup failure (reference: std::runtime_error during setup) */
+#define NDS_E_CUDA (-3)         /* CUDA runtime failure or no device */
+#define NDS_E_BREAKDOWN (-4)    /* Krylov breakdown / non-finite value (reference throws, h8_main_base.cu:570-572) */
+#define NDS_E_NOT_CONVERGED (-5)/* pressure solve missed its target within p_max (h8_main_base.cu:2101) */
+#define NDS_E_STATE (-6)        /* call out of order */
+
+typedef struct nds_mesh nds_mesh;
+typedef struct nds_problem nds_problem;
+typedef struct nds_solver nds_solver;
+
+enum nds_precision { NDS_FP64 = 0, NDS_FP32 = 1, NDS_AMG_FP32 = 2 };
+enum nds_run_mode { NDS_RUN_FIXED10 = 0, NDS_RUN_CONVERGE = 1 };
+enum nds_momentum_work { NDS_MOM_FGS1 = 0, NDS_MOM_ALTGS1 = 1, NDS_MOM_SGS1 = 2 };
+enum nds_pressure_solver { NDS_P_PCG = 0, NDS_P_RICHARDSON = 1, NDS_P_CHEB = 2 };
+enum nds_amg_hierarchy { NDS_AMG_SA = 0, NDS_AMG_CF = 1 };
+enum nds_amg_smoother { NDS_SM_CHEB2 = 0, NDS_SM_JACOBI = 1, NDS_SM_L1JACOBI = 2, NDS_SM_MCGS = 3 };
+enum nds_spectrum_policy { NDS_SPEC_AUTO = 0, NDS_SPEC_ALWAYS = 1, NDS_SPEC_OFF = 2 };
+enum nds_mcgs_order { NDS_MCGS_SYMMETRIC = 0, NDS_MCGS_FORWARD = 1, NDS_MCGS_BACKWARD = 2 };
+enum nds_cf_interp { NDS_CF_DIRECT = 0, NDS_CF_EXTI = 1 };
+
+/* All H8 CLI controls (h8_main_base.cu:1749-1850); nds_options_default()
+ * fills the binary's own defaults. */
+typedef struct nds_options {
+  double re, bulk, simple_tol, alpha_u, alpha_p, rau_scale;
+  int max_outer, run_mode, momentum_work;
+  double mom_omega, mom_rtol, mom_atol, mom_drop;
+  int mom_max;
+  int pressure_solver;
+  double p_rtol, p_atol;
+  int p_max;
+  double snapshot_tol;
+  int fine_csr_refresh_every;
+  double p_richardson_omega;
+  int p_cheb_degree, p_power_its;
+  double p_cheb_low_fraction, p_power_safety;
+  int amg_hierarchy, amg_smoother, amg_terminal, amg_spectrum_policy;
+  int amg_power_its, amg_cheb_degree;
+  double amg_lambda_safety, amg_lambda_low_fraction, amg_jacobi_omega;
+  int amg_jacobi_fine_sweeps, amg_jacobi_coarse_sweeps;
+  double amg_mcgs_omega;
+  int amg_mcgs_fine_sweeps, amg_mcgs_coarse_sweeps, amg_mcgs_order;
+  double cf_theta;
+  int cf_pmax, cf_interp, cf_aggressive_first;
+  char wall[64], inlet[64], outlet[64];
+  int precision;   /* enum nds_precision */
+  int threads;     /* host threads for setup; 0 = all */
+  int device;      /* CUDA device ordinal */
+  int verbose;     /* 1: print the reference's NODALS_GPU_* markers to stdout */
+} nds_options;
+
+/* One SIMPLE outer iteration (h8_main_base.cu:2046-2119). */
+typedef struct nds_iter_report {
+  int it;
+  double rel_cont;          /* ||B u + fixedDiv|| / same at it = 1 */
+  double cont_norm;
+  int p_its;
+  double p_rel;
+  int audited;              /* pre-sweep momentum audit performed this iteration */
+  double audit_rel[3];
+  int all_momentum_met;
+  int converged;
+  double ms_assembly, ms_momentum, ms_continuity, ms_pressure, ms_update;
+} nds_iter_report;
+
+typedef struct nds_solve_report {
+  int outer_its;
+  int converged;
+  int pressure_all;         /* every pressure solve met its target */
+  int finite_all;
+  double final_rel_cont;
+  double final_audit_rel[3];
+  double avg_pressure_its;
+  double loop_ms;           /* device-timed loop */
+  double assembly_ms, momentum_ms, continuity_ms, pressure_ms, update_ms;
+} nds_solve_report;
+
+/* Host array view of a named setup array (read-only, owned by the problem). */
+typedef struct nds_array {
+  const void* data;
+  int64_t count;
+  int dtype;                /* 0 f64, 1 i32, 2 i64, 3 u8, 4 u32 */
+} nds_array;
+
+const char* nds_last_error(void);
+const char* nds_version(void);
+void nds_options_default(nds_options* o);
+
+/* ---- meshes: replace load_foam_tet_mesh (foam_mesh_g2.hpp:55) ---------- */
+int nds_mesh_read_polymesh(const char* polymesh_dir, nds_mesh** out);
+int nds_mesh_read_msh2(const char* path, nds_mesh** out);
+int nds_mesh_from_arrays(int n_points, const double* xyz, int n_cells, const int32_t* tets, int n_bfaces,
+                         const int32_t* btri, const int32_t* bpatch, int n_patches, const char* const* patch_names,
+                         nds_mesh** out);
+int nds_mesh_counts(const nds_mesh* m, int* n_points, int* n_cells, int* n_faces, int* n_internal);
+void nds_mesh_destroy(nds_mesh* m);
+
+/* ---- host setup: replaces build_g4_setup (g4_host.hpp:289),
+ *      build_h2_fine_csr_host (h2b_fine_csr.cuh:445) and
+ *      build_sa_hierarchy / build_cf_hierarchy (g5_sa_host.hpp:1545,
+ *      g8_cf_hierarchy_host.hpp:1584) ------------------------------------- */
+int nds_problem_create(const nds_mesh* m, const nds_options* o, nds_problem** out);
+int nds_problem_array(const nds_problem* p, const char* name, nds_array* out);
+int nds_problem_counts(const nds_problem* p, int* nc, int* nv, int* ncolors, int* levels);
+void nds_problem_destroy(nds_problem* p);
+
+/* ---- device solver: replaces upload_all (h8_main_base.cu:761-788), the
+ *      setup policies (:1984-2025) and the SIMPLE loop (:2046-2119) ------- */
+int nds_solver_create(const nds_problem* p, nds_solver** out);
+int nds_solver_reset(nds_solver* s);                         /* u = p = 0, it = 0 */
+int nds_simple_step(nds_solver* s, nds_iter_report* rep);
+int nds_solve(nds_solver* s, nds_solve_report* rep);         /* the run_mode loop */
+int nds_get_fields(nds_solver* s, double* u0, double* u1, double* u2, double* p);
+int nds_set_fields(nds_solver* s, const double* u0, const double* u1, const double* u2, const double* p);
+void nds_solver_destroy(nds_solver* s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NODALS_B200_H */

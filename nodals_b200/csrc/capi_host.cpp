@@ -1,0 +1,348 @@
+// Host half of the C ABI: meshes, options and the host setup ("problem").
+// No CUDA call is made here, so these entry points work on CPU-only hosts.
+#include <cstring>
+#include <map>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/nodals_b200.h"
+#include "capi_internal.hpp"
+#include "host/amg.hpp"
+#include "host/mesh.hpp"
+#include "host/setup.hpp"
+
+namespace {
+thread_local std::string g_err;
+}
+
+namespace nds {
+void set_error(const std::string& e) { g_err = e; }
+}  // namespace nds
+
+using nds::set_error;
+
+extern "C" {
+
+const char* nds_last_error(void) { return g_err.c_str(); }
+const char* nds_version(void) { return "nodals_b200 0.1 (sm_100a)"; }
+
+void nds_options_default(nds_options* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  // the H8 binary's own defaults (h8_main_base.cu:1749-1785)
+  o->re = 20;
+  o->bulk = 1;
+  o->simple_tol = 1e-6;
+  o->alpha_u = 0.5;
+  o->alpha_p = 0.5;
+  o->rau_scale = 1.0;
+  o->max_outer = 2500;
+  o->run_mode = NDS_RUN_FIXED10;
+  o->momentum_work = NDS_MOM_FGS1;
+  o->mom_omega = 1.0;
+  o->mom_rtol = 1e-6;
+  o->mom_atol = 1e-12;
+  o->mom_drop = 0.1;
+  o->mom_max = 20000;
+  o->pressure_solver = NDS_P_PCG;
+  o->p_rtol = 0.5;
+  o->p_atol = 1e-12;
+  o->p_max = 20;
+  o->snapshot_tol = 5e-6;
+  o->fine_csr_refresh_every = 1;
+  o->p_richardson_omega = 1.0;
+  o->p_cheb_degree = 3;
+  o->p_power_its = 6;
+  o->p_cheb_low_fraction = 0.05;
+  o->p_power_safety = 1.15;
+  o->amg_hierarchy = NDS_AMG_SA;
+  o->amg_smoother = NDS_SM_CHEB2;
+  o->amg_terminal = 1000;
+  o->amg_spectrum_policy = NDS_SPEC_AUTO;
+  o->amg_power_its = 16;
+  o->amg_cheb_degree = 2;
+  o->amg_lambda_safety = 1.5;
+  o->amg_lambda_low_fraction = 0.05;
+  o->amg_jacobi_omega = 0.7;
+  o->amg_jacobi_fine_sweeps = 1;
+  o->amg_jacobi_coarse_sweeps = 1;
+  o->amg_mcgs_omega = 1.0;
+  o->amg_mcgs_fine_sweeps = 1;
+  o->amg_mcgs_coarse_sweeps = 1;
+  o->amg_mcgs_order = NDS_MCGS_SYMMETRIC;
+  o->cf_theta = 0.25;
+  o->cf_pmax = 4;
+  o->cf_interp = NDS_CF_DIRECT;
+  o->cf_aggressive_first = 0;
+  std::strcpy(o->wall, "patch_0_0");
+  std::strcpy(o->inlet, "patch_2_0");
+  std::strcpy(o->outlet, "patch_1_0");
+  o->precision = NDS_FP64;
+  o->threads = 0;
+  o->device = 0;
+  o->verbose = 0;
+}
+
+int nds_mesh_read_polymesh(const char* dir, nds_mesh** out) {
+  if (!dir || !out) { set_error("null argument"); return NDS_E_INVALID; }
+  try {
+    *out = reinterpret_cast<nds_mesh*>(new nds::Mesh(nds::read_polymesh(dir)));
+    return NDS_OK;
+  } catch (const std::exception& e) {
+    set_error(e.what());
+    return NDS_E_SETUP;
+  }
+}
+
+int nds_mesh_read_msh2(const char* path, nds_mesh** out) {
+  if (!path || !out) { set_error("null argument"); return NDS_E_INVALID; }
+  try {
+    *out = reinterpret_cast<nds_mesh*>(new nds::Mesh(nds::read_msh2(path)));
+    return NDS_OK;
+  } catch (const std::exception& e) {
+    set_error(e.what());
+    return NDS_E_SETUP;
+  }
+}
+
+int nds_mesh_from_arrays(int n_points, const double* xyz, int n_cells, const int32_t* tets, int n_bfaces,
+                         const int32_t* btri, const int32_t* bpatch, int n_patches, const char* const* patch_names,
+                         nds_mesh** out) {
+  if (!xyz || !tets || !btri || !bpatch || !patch_names || !out || n_patches <= 0) {
+    set_error("null or empty mesh arrays");
+    return NDS_E_INVALID;
+  }
+  try {
+    std::vector<std::string> names;
+    for (int i = 0; i < n_patches; ++i) names.emplace_back(patch_names[i] ? patch_names[i] : "");
+    *out = reinterpret_cast<nds_mesh*>(
+        new nds::Mesh(nds::mesh_from_arrays(n_points, xyz, n_cells, tets, n_bfaces, btri, bpatch, names)));
+    return NDS_OK;
+  } catch (const std::exception& e) {
+    set_error(e.what());
+    return NDS_E_SETUP;
+  }
+}
+
+int nds_mesh_counts(const nds_mesh* mm, int* np, int* nc, int* nf, int* ni) {
+  if (!mm) { set_error("null mesh"); return NDS_E_INVALID; }
+  const auto* m = reinterpret_cast<const nds::Mesh*>(mm);
+  if (np) *np = m->n_points();
+  if (nc) *nc = m->n_cells();
+  if (nf) *nf = m->n_faces();
+  if (ni) *ni = m->n_internal();
+  return NDS_OK;
+}
+
+void nds_mesh_destroy(nds_mesh* m) { delete reinterpret_cast<nds::Mesh*>(m); }
+
+int nds_problem_create(const nds_mesh* mm, const nds_options* o, nds_problem** out) {
+  if (!mm || !o || !out) { set_error("null argument"); return NDS_E_INVALID; }
+  try {
+    std::string why;
+    if (!nds::validate_options(*o, why)) {
+      set_error(why);
+      return NDS_E_INVALID;
+    }
+    auto P = std::make_unique<nds::Problem>();
+    P->opt = *o;
+    P->mesh = *reinterpret_cast<const nds::Mesh*>(mm);
+    nds::SetupOptions so;
+    so.re = o->re;
+    so.bulk = o->bulk;
+    so.alpha_u = o->alpha_u;
+    so.rau_scale = o->rau_scale;
+    so.wall = o->wall;
+    so.inlet = o->inlet;
+    so.outlet = o->outlet;
+    so.threads = o->threads;
+    P->setup = nds::build_setup(P->mesh, so);
+    P->power_its = nds::effective_amg_power_its(*o);
+    nds::AmgOptions ao;
+    ao.hierarchy = o->amg_hierarchy == NDS_AMG_SA ? "sa" : "cf";
+    ao.terminal = o->amg_terminal;
+    ao.power_its = P->power_its;
+    ao.lambda_safety = o->amg_lambda_safety;
+    ao.cf_theta = o->cf_theta;
+    ao.cf_pmax = o->cf_pmax;
+    ao.cf_interp = o->cf_interp == NDS_CF_EXTI ? "exti" : "direct";
+    ao.cf_aggressive_first = o->cf_aggressive_first != 0;
+    P->hier = nds::build_hierarchy(P->mesh, P->setup, P->setup.init_rau, ao);
+    P->index_arrays();
+    *out = reinterpret_cast<nds_problem*>(P.release());
+    return NDS_OK;
+  } catch (const std::exception& e) {
+    set_error(e.what());
+    return NDS_E_SETUP;
+  }
+}
+
+int nds_problem_array(const nds_problem* pp, const char* name, nds_array* out) {
+  if (!pp || !name || !out) { set_error("null argument"); return NDS_E_INVALID; }
+  const auto* P = reinterpret_cast<const nds::Problem*>(pp);
+  auto it = P->arrays.find(name);
+  if (it == P->arrays.end()) {
+    set_error(std::string("unknown problem array ") + name);
+    return NDS_E_INVALID;
+  }
+  *out = it->second;
+  return NDS_OK;
+}
+
+int nds_problem_counts(const nds_problem* pp, int* nc, int* nv, int* ncolors, int* levels) {
+  if (!pp) { set_error("null problem"); return NDS_E_INVALID; }
+  const auto* P = reinterpret_cast<const nds::Problem*>(pp);
+  if (nc) *nc = P->setup.nc;
+  if (nv) *nv = P->setup.nv;
+  if (ncolors) *ncolors = P->setup.ncolors;
+  if (levels) *levels = (int)P->hier.A.size();
+  return NDS_OK;
+}
+
+void nds_problem_destroy(nds_problem* p) { delete reinterpret_cast<nds::Problem*>(p); }
+
+}  // extern "C"
+
+namespace nds {
+
+int effective_amg_power_its(const nds_options& o) {
+  if (o.amg_spectrum_policy == NDS_SPEC_ALWAYS) return o.amg_power_its;
+  if (o.amg_spectrum_policy == NDS_SPEC_AUTO && o.amg_smoother == NDS_SM_CHEB2) return o.amg_power_its;
+  return 0;
+}
+
+bool validate_options(const nds_options& o, std::string& why) {
+  auto bad = [&](const char* m) { why = m; return false; };
+  // ranges of h8_main_base.cu:1851-1911 (laminar subset)
+  if (!(o.simple_tol > 0.0) || o.max_outer < 1) return bad("H8 invalid SIMPLE controls");
+  if (!(o.alpha_u > 0.0 && o.alpha_u <= 1.0) || !(o.alpha_p > 0.0 && o.alpha_p <= 1.0)) return bad("H8 alpha-u/alpha-p must be in (0,1]");
+  if (!(o.rau_scale > 0.0)) return bad("H8 rau-scale must be finite and > 0");
+  if (o.mom_rtol < 0.0 || o.mom_atol < 0.0 || o.mom_drop < 0.0 || o.mom_max < 1 || !(o.mom_omega > 0.0)) return bad("H8 invalid momentum controls");
+  if (o.p_rtol < 0.0 || o.p_atol < 0.0 || o.p_max < 1) return bad("H8 invalid pressure controls");
+  if (o.amg_hierarchy != NDS_AMG_SA && o.amg_hierarchy != NDS_AMG_CF) return bad("H8 amg-hierarchy must be sa or cf");
+  if (!(o.cf_theta > 0.0 && o.cf_theta <= 1.0)) return bad("H8 cf-theta must be in (0,1]");
+  if (o.cf_pmax < 1 || o.cf_pmax > 16) return bad("H8 cf-pmax must be in [1,16]");
+  if (o.cf_interp != NDS_CF_DIRECT && o.cf_interp != NDS_CF_EXTI) return bad("H8 cf-interp must be direct or exti");
+  if (o.cf_aggressive_first != 0 && o.cf_aggressive_first != 1) return bad("H8 cf-aggressive-first must be 0 or 1");
+  if (o.amg_terminal < 16) return bad("H8 amg-terminal must be >=16");
+  if (o.amg_spectrum_policy < 0 || o.amg_spectrum_policy > 2) return bad("H8 amg-spectrum-policy must be auto, always or off");
+  if (o.amg_power_its < 1 || o.amg_power_its > 64) return bad("H8 amg-power-its must be in [1,64]");
+  if (o.amg_cheb_degree < 1 || o.amg_cheb_degree > 16) return bad("H8 amg-cheb-degree must be in [1,16]");
+  if (!(o.amg_lambda_safety > 1.0 && o.amg_lambda_safety <= 3.0)) return bad("H8 amg-lambda-safety must be in (1,3]");
+  if (!(o.amg_lambda_low_fraction > 0.0 && o.amg_lambda_low_fraction < 1.0)) return bad("H8 amg-lambda-low-fraction must be in (0,1)");
+  if (o.pressure_solver < 0 || o.pressure_solver > 2) return bad("G12 pressure-solver must be pcg, richardson or cheb");
+  if (!(o.p_richardson_omega > 0.0 && o.p_richardson_omega < 2.0)) return bad("G12 Richardson omega must be in (0,2)");
+  if (o.p_cheb_degree < 1 || o.p_cheb_degree > 16) return bad("G12 Cheb degree must be in [1,16]");
+  if (o.p_power_its < 1 || o.p_power_its > 64) return bad("G12 pressure power its must be in [1,64]");
+  if (!(o.p_cheb_low_fraction > 0.0 && o.p_cheb_low_fraction < 1.0)) return bad("G12 Cheb low fraction must be in (0,1)");
+  if (!(o.p_power_safety > 1.0 && o.p_power_safety <= 2.0)) return bad("G12 pressure power safety must be in (1,2]");
+  if (o.amg_smoother < 0 || o.amg_smoother > 3) return bad("H8 amg-smoother must be cheb2, jacobi, l1jacobi or mcgs");
+  if (!(o.amg_jacobi_omega > 0.0 && o.amg_jacobi_omega <= 2.0)) return bad("H8 amg-jacobi-omega must be in (0,2]");
+  if (o.amg_jacobi_fine_sweeps < 1 || o.amg_jacobi_fine_sweeps > 16 || o.amg_jacobi_coarse_sweeps < 1 || o.amg_jacobi_coarse_sweeps > 16)
+    return bad("H8 Jacobi sweeps must be in [1,16]");
+  if (!(o.amg_mcgs_omega > 0.0 && o.amg_mcgs_omega < 2.0)) return bad("H8 amg-mcgs-omega must be in (0,2)");
+  if (o.amg_mcgs_fine_sweeps < 1 || o.amg_mcgs_fine_sweeps > 16 || o.amg_mcgs_coarse_sweeps < 1 || o.amg_mcgs_coarse_sweeps > 16)
+    return bad("H8 MCGS sweeps must be in [1,16]");
+  if (o.amg_mcgs_order < 0 || o.amg_mcgs_order > 2) return bad("H8 amg-mcgs-order must be symmetric, forward or backward");
+  if (o.pressure_solver == NDS_P_PCG && o.amg_smoother == NDS_SM_MCGS && o.amg_mcgs_order != NDS_MCGS_SYMMETRIC)
+    return bad("H8 PCG requires symmetric MCGS");
+  if (!(o.snapshot_tol > 0.0)) return bad("H8 snapshot tolerance must be positive");
+  if (o.fine_csr_refresh_every != 1) return bad("H8 requires fine CSR refreshEvery=1");
+  if (o.momentum_work < 0 || o.momentum_work > 2) return bad("H8 momentum-work must be fgs1, altgs1 or sgs1");
+  if (o.run_mode != NDS_RUN_FIXED10 && o.run_mode != NDS_RUN_CONVERGE) return bad("H8 run-mode must be fixed10 or converge");
+  if (o.run_mode == NDS_RUN_FIXED10 && o.max_outer != 10) return bad("H8 fixed10 requires maxOuter=10");
+  if (o.amg_smoother == NDS_SM_CHEB2 && effective_amg_power_its(o) <= 0) return bad("H8 Chebyshev AMG smoother requires spectrum estimation");
+  if (o.precision < 0 || o.precision > 2) return bad("precision must be fp64, fp32 or amg_fp32");
+  return true;
+}
+
+namespace {
+template <class T>
+nds_array view(const std::vector<T>& v, int dt) {
+  nds_array a;
+  a.data = v.data();
+  a.count = (int64_t)v.size();
+  a.dtype = dt;
+  return a;
+}
+}  // namespace
+
+void Problem::index_arrays() {
+  auto& A = arrays;
+  auto& S = setup;
+  auto& H = hier;
+  auto scal = [&](const std::string& n, double x) {
+    scalars[n] = {x};
+    A[n] = view(scalars[n], 0);
+  };
+  mesh_tets.clear();
+  mesh_opp.clear();
+  for (auto& t : mesh.tets) for (int k = 0; k < 4; ++k) mesh_tets.push_back(t[(size_t)k]);
+  for (auto& t : mesh.opp) for (int k = 0; k < 4; ++k) mesh_opp.push_back(t[(size_t)k]);
+  A["mesh.tets"] = view(mesh_tets, 1);
+  A["mesh.opp_face"] = view(mesh_opp, 1);
+  A["mesh.face_patch"] = view(mesh.face_patch, 1);
+  A["mesh.xyz"] = view(mesh.xyz, 0);
+  scal("pipe.nu", S.pipe.nu);
+  scal("pipe.R", S.pipe.R);
+  scal("pipe.L", S.pipe.L);
+  scal("pipe.profileScale", S.pipe.profile_scale);
+  scal("pipe.hpDrop", S.pipe.hp_drop);
+  scal("pipe.hpGradient", S.pipe.hp_gradient);
+  scal("pipe.zOut", S.pipe.z_out);
+  scal("pipe.cx", S.pipe.cx);
+  scal("pipe.cy", S.pipe.cy);
+  scal("pipe.bulk", S.pipe.bulk);
+  A["g2free"] = view(S.g2free, 1);
+  A["fixedSlot"] = view(S.fixed_slot, 1);
+  A["fixedValue"] = view(S.fixed_value, 0);
+  A["mom.row"] = view(S.mom.row, 2);
+  A["mom.col"] = view(S.mom.col, 1);
+  A["mom.val"] = view(S.mom.val, 0);
+  A["mom.diagPos"] = view(S.mom_diag_pos, 1);
+  A["color"] = view(S.color, 1);
+  A["color.offset"] = view(S.color_off, 1);
+  A["color.rows"] = view(S.color_rows, 1);
+  A["cell.ref"] = view(S.ref, 1);
+  A["cell.rowSlot"] = view(S.row_slot, 3);
+  A["cell.det"] = view(S.det, 0);
+  A["cell.invJ"] = view(S.invJ, 0);
+  A["cell.bcoeff"] = view(S.bco, 0);
+  for (int d = 0; d < 3; ++d) A["staticRhs" + std::to_string(d)] = view(S.static_rhs[(size_t)d], 0);
+  A["fixedDiv"] = view(S.fixed_div, 0);
+  A["volume"] = view(S.volume, 0);
+  A["initRau"] = view(S.init_rau, 0);
+  A["initDelta"] = view(S.init_delta, 0);
+  A["fine.row"] = view(S.fine.row, 1);
+  A["fine.col"] = view(S.fine.col, 1);
+  A["fine.diagPos"] = view(S.fine.diag_pos, 1);
+  A["fine.incOff"] = view(S.fine.inc_off, 1);
+  A["fine.packed"] = view(S.fine.packed, 4);
+  A["fine.contribOff"] = view(S.fine.contrib_off, 1);
+  A["fine.slot"] = view(S.fine.slot, 3);
+  scal("amg.levels", (double)H.A.size());
+  scal("amg.fineLambda", H.fine_lambda);
+  scal("amg.powerIts", (double)power_its);
+  A["amg.fineDiag"] = view(H.fine_diag, 0);
+  A["amg.levelLambda"] = view(H.level_lambda, 0);
+  A["amg.terminal_inv"] = view(H.terminal_inv, 0);
+  for (size_t l = 0; l < H.agg.size(); ++l) A["amg.agg" + std::to_string(l)] = view(H.agg[l], 1);
+  for (size_t l = 0; l < H.P.size(); ++l) {
+    const std::string p = "amg.P" + std::to_string(l) + ".";
+    scal(p + "nCoarse", (double)H.P[l].nc);
+    A[p + "row"] = view(H.P[l].row, 2);
+    A[p + "col"] = view(H.P[l].col, 1);
+    A[p + "val"] = view(H.P[l].val, 0);
+  }
+  for (size_t l = 0; l < H.A.size(); ++l) {
+    const std::string p = "amg.A" + std::to_string(l) + ".";
+    A[p + "row"] = view(H.A[l].row, 2);
+    A[p + "col"] = view(H.A[l].col, 1);
+    A[p + "val"] = view(H.A[l].val, 0);
+    A[p + "diag"] = view(H.A[l].diag, 0);
+  }
+}
+
+}  // namespace nds

@@ -1,0 +1,735 @@
+#include "amg.hpp"
+
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstdint>
+#include <stdexcept>
+#include <unordered_map>
+#include <utility>
+
+namespace nds {
+
+namespace {
+
+using Entry = std::pair<int, double>;
+
+// rows of (col -> value) accumulated in a fixed order, then packed sorted;
+// exact zeros are dropped like the reference packer (g5_sa_host.hpp:504-521)
+CsrHost pack_rows(std::vector<std::unordered_map<int, double>>& rows) {
+  CsrHost A;
+  A.n = (int)rows.size();
+  A.row.assign((size_t)A.n + 1, 0);
+  A.diag.assign((size_t)A.n, 0.0);
+  std::vector<Entry> tmp;
+  for (int i = 0; i < A.n; ++i) {
+    tmp.clear();
+    for (const auto& kv : rows[(size_t)i])
+      if (kv.second != 0.0) tmp.push_back(kv);
+    std::sort(tmp.begin(), tmp.end(), [](const Entry& a, const Entry& b) { return a.first < b.first; });
+    for (const auto& e : tmp) {
+      A.col.push_back(e.first);
+      A.val.push_back(e.second);
+      if (e.first == i) A.diag[(size_t)i] = e.second;
+    }
+    A.row[(size_t)i + 1] = (int64_t)A.col.size();
+    std::unordered_map<int, double>().swap(rows[(size_t)i]);
+  }
+  for (int i = 0; i < A.n; ++i)
+    if (!(A.diag[(size_t)i] > 0.0) || !std::isfinite(A.diag[(size_t)i]))
+      throw std::runtime_error("coarse AMG matrix has a non-positive diagonal");
+  return A;
+}
+
+// SA transfer row: merge duplicates, keep own + largest |w|, normalise to sum 1
+void normalize_prune(std::vector<Entry>& row, int own, int max_nnz) {
+  if (row.empty()) row.push_back({own, 1.0});
+  std::sort(row.begin(), row.end(), [](const Entry& a, const Entry& b) { return a.first < b.first; });
+  size_t w = 0;
+  for (size_t k = 0; k < row.size();) {
+    const int c = row[k].first;
+    double v = 0.0;
+    size_t j = k;
+    for (; j < row.size() && row[j].first == c; ++j) v += row[j].second;
+    row[w++] = {c, v};
+    k = j;
+  }
+  row.resize(w);
+  if (max_nnz > 0 && (int)row.size() > max_nnz) {
+    std::vector<Entry> keep;
+    keep.reserve((size_t)max_nnz);
+    auto it = std::find_if(row.begin(), row.end(), [&](const Entry& e) { return e.first == own; });
+    keep.push_back(it != row.end() ? *it : Entry{own, 0.0});
+    std::vector<Entry> others;
+    for (const auto& e : row)
+      if (e.first != own) others.push_back(e);
+    std::sort(others.begin(), others.end(), [](const Entry& a, const Entry& b) {
+      const double aa = std::abs(a.second), bb = std::abs(b.second);
+      return aa > bb || (aa == bb && a.first < b.first);
+    });
+    for (const auto& e : others)
+      if ((int)keep.size() < max_nnz) keep.push_back(e);
+    std::sort(keep.begin(), keep.end(), [](const Entry& a, const Entry& b) { return a.first < b.first; });
+    row.swap(keep);
+  }
+  double sum = 0.0;
+  for (const auto& e : row) sum += e.second;
+  if (!std::isfinite(sum) || std::abs(sum) < 1e-14) {
+    row.clear();
+    row.push_back({own, 1.0});
+    return;
+  }
+  for (auto& e : row) e.second /= sum;
+}
+
+void csr_apply(const CsrHost& A, const std::vector<double>& x, std::vector<double>& y) {
+  y.assign((size_t)A.n, 0.0);
+  for (int i = 0; i < A.n; ++i) {
+    double s = 0.0;
+    for (int64_t k = A.row[(size_t)i]; k < A.row[(size_t)i + 1]; ++k) s += A.val[(size_t)k] * x[(size_t)A.col[(size_t)k]];
+    y[(size_t)i] = s;
+  }
+}
+
+// deterministic power-iteration start vector
+inline double power_seed(int i) {
+  const double g = (double)(i + 1);
+  return std::sin(.731 * g) + .27 * std::cos(1.117 * g);
+}
+
+// lambda_max(D^-1/2 A D^-1/2) by power iteration, with a generic apply
+template <class Apply>
+double power_generic(int n, const std::vector<double>& diag, int its, double safety, Apply apply) {
+  std::vector<double> v((size_t)n), u((size_t)n), au, w((size_t)n);
+  long double ss = 0;
+  for (int i = 0; i < n; ++i) {
+    v[(size_t)i] = power_seed(i);
+    ss += (long double)v[(size_t)i] * v[(size_t)i];
+  }
+  const double vn = std::sqrt((double)ss);
+  for (auto& q : v) q /= vn;
+  double ray = 0.0;
+  for (int it = 0; it < its; ++it) {
+    for (int i = 0; i < n; ++i) u[(size_t)i] = v[(size_t)i] / std::sqrt(diag[(size_t)i]);
+    apply(u, au);
+    long double num = 0, den = 0, nw = 0;
+    for (int i = 0; i < n; ++i) {
+      w[(size_t)i] = au[(size_t)i] / std::sqrt(diag[(size_t)i]);
+      num += (long double)v[(size_t)i] * w[(size_t)i];
+      den += (long double)v[(size_t)i] * v[(size_t)i];
+      nw += (long double)w[(size_t)i] * w[(size_t)i];
+    }
+    ray = (double)(num / std::max(den, (long double)1e-300));
+    const double nrm = std::sqrt((double)nw);
+    if (!(nrm > 0.0) || !std::isfinite(nrm) || !(ray > 0.0) || !std::isfinite(ray))
+      throw std::runtime_error("AMG power iteration failed");
+    for (int i = 0; i < n; ++i) v[(size_t)i] = w[(size_t)i] / nrm;
+  }
+  return safety * ray;
+}
+
+// matrix-free fine Schur action y = B diag(rau) B^T x in cell order
+struct FineApply {
+  const Setup& S;
+  const std::vector<double>& rau;
+  std::vector<double> v0, v1, v2;
+  FineApply(const Setup& s, const std::vector<double>& r) : S(s), rau(r), v0((size_t)s.nv), v1((size_t)s.nv), v2((size_t)s.nv) {}
+  void operator()(const std::vector<double>& x, std::vector<double>& y) {
+    std::fill(v0.begin(), v0.end(), 0.0);
+    std::fill(v1.begin(), v1.end(), 0.0);
+    std::fill(v2.begin(), v2.end(), 0.0);
+    for (int c = 0; c < S.nc; ++c) {
+      const double p = x[(size_t)c];
+      for (int a = 0; a < 8; ++a) {
+        const int g = S.ref[8 * (size_t)c + a];
+        if (g < 0) continue;
+        const double* b = &S.bco[24 * (size_t)c + 3 * a];
+        v0[(size_t)g] += b[0] * p;
+        v1[(size_t)g] += b[1] * p;
+        v2[(size_t)g] += b[2] * p;
+      }
+    }
+    for (int g = 0; g < S.nv; ++g) {
+      const double r = rau[(size_t)g];
+      v0[(size_t)g] *= r;
+      v1[(size_t)g] *= r;
+      v2[(size_t)g] *= r;
+    }
+    y.assign((size_t)S.nc, 0.0);
+    for (int c = 0; c < S.nc; ++c) {
+      double s = 0.0;
+      for (int a = 0; a < 8; ++a) {
+        const int g = S.ref[8 * (size_t)c + a];
+        if (g < 0) continue;
+        const double* b = &S.bco[24 * (size_t)c + 3 * a];
+        s += b[0] * v0[(size_t)g] + b[1] * v1[(size_t)g] + b[2] * v2[(size_t)g];
+      }
+      y[(size_t)c] = s;
+    }
+  }
+};
+
+// Galerkin P^T A P accumulated per coarse entry in ascending fine-row order
+CsrHost galerkin(const CsrHost& A, const Transfer& P) {
+  if (P.nf != A.n) throw std::runtime_error("Galerkin transfer size mismatch");
+  std::vector<std::unordered_map<int, double>> rows((size_t)P.nc);
+  std::vector<Entry> q;
+  for (int i = 0; i < A.n; ++i) {
+    q.clear();
+    for (int64_t k = A.row[(size_t)i]; k < A.row[(size_t)i + 1]; ++k) {
+      const int j = A.col[(size_t)k];
+      const double a = A.val[(size_t)k];
+      for (int64_t kp = P.row[(size_t)j]; kp < P.row[(size_t)j + 1]; ++kp) q.push_back({P.col[(size_t)kp], a * P.val[(size_t)kp]});
+    }
+    std::sort(q.begin(), q.end(), [](const Entry& a, const Entry& b) { return a.first < b.first; });
+    size_t w = 0;
+    for (size_t k = 0; k < q.size();) {
+      const int c = q[k].first;
+      double v = 0.0;
+      size_t j = k;
+      for (; j < q.size() && q[j].first == c; ++j) v += q[j].second;
+      q[w++] = {c, v};
+      k = j;
+    }
+    q.resize(w);
+    for (int64_t kp = P.row[(size_t)i]; kp < P.row[(size_t)i + 1]; ++kp) {
+      const int I = P.col[(size_t)kp];
+      const double pi = P.val[(size_t)kp];
+      for (const auto& e : q) {
+        const double v = pi * e.second;
+        if (v != 0.0) rows[(size_t)I][e.first] += v;
+      }
+    }
+  }
+  return pack_rows(rows);
+}
+
+// ----------------------------------------------------------------------------
+// SA pieces
+// ----------------------------------------------------------------------------
+std::vector<std::vector<int32_t>> face_graph(const Mesh& m) {
+  std::vector<std::vector<int32_t>> g((size_t)m.n_cells());
+  for (int f = 0; f < m.n_internal(); ++f) {
+    const int a = m.owner[(size_t)f], b = m.neighbour[(size_t)f];
+    g[(size_t)a].push_back(b);
+    g[(size_t)b].push_back(a);
+  }
+  for (auto& v : g) {
+    std::sort(v.begin(), v.end());
+    v.erase(std::unique(v.begin(), v.end()), v.end());
+  }
+  return g;
+}
+
+std::vector<std::vector<int32_t>> csr_graph(const CsrHost& A) {
+  std::vector<std::vector<int32_t>> g((size_t)A.n);
+  for (int i = 0; i < A.n; ++i)
+    for (int64_t k = A.row[(size_t)i]; k < A.row[(size_t)i + 1]; ++k) {
+      const int j = A.col[(size_t)k];
+      if (j != i) g[(size_t)i].push_back(j);
+    }
+  return g;
+}
+
+// fine -> first aggregate level, smoothed with damping / lambda
+Transfer sa_fine_transfer(const Setup& S, const std::vector<double>& rau, const std::vector<int32_t>& id, int nagg,
+                          const std::vector<double>& diag, double lambda, double damping, int max_nnz) {
+  const double omega = damping / lambda;
+  const FineTopo& F = S.fine;
+  Transfer P;
+  P.nf = S.nc;
+  P.nc = nagg;
+  P.row.assign((size_t)P.nf + 1, 0);
+  std::vector<Entry> row;
+  for (int i = 0; i < P.nf; ++i) {
+    row.clear();
+    const int own = id[(size_t)i];
+    row.push_back({own, 1.0});
+    const double invd = 1.0 / diag[(size_t)i];
+    for (int a = 0; a < 8; ++a) {
+      const int g = S.ref[8 * (size_t)i + a];
+      if (g < 0) continue;
+      const double* bi = &S.bco[24 * (size_t)i + 3 * a];
+      for (int k = F.inc_off[(size_t)g]; k < F.inc_off[(size_t)g + 1]; ++k) {
+        const uint32_t pk = F.packed[(size_t)k];
+        const int j = (int)(pk >> 3);
+        const double* bj = &S.bco[24 * (size_t)j + 3 * (pk & 7u)];
+        double dot = 0.0;
+        for (int d = 0; d < 3; ++d) dot += bi[d] * bj[d];
+        row.push_back({id[(size_t)j], -omega * invd * rau[(size_t)g] * dot});
+      }
+    }
+    normalize_prune(row, own, max_nnz);
+    for (const auto& e : row) {
+      P.col.push_back(e.first);
+      P.val.push_back(e.second);
+    }
+    P.row[(size_t)i + 1] = (int64_t)P.col.size();
+  }
+  return P;
+}
+
+// A1 = P^T B diag(rau) B^T P, per velocity dof in ascending order
+CsrHost sa_first_coarse(const Setup& S, const std::vector<double>& rau, const Transfer& P) {
+  const FineTopo& F = S.fine;
+  std::vector<std::unordered_map<int, double>> rows((size_t)P.nc);
+  struct QE {
+    int coarse;
+    double b[3];
+  };
+  std::vector<QE> q;
+  for (int g = 0; g < S.nv; ++g) {
+    q.clear();
+    for (int k = F.inc_off[(size_t)g]; k < F.inc_off[(size_t)g + 1]; ++k) {
+      const uint32_t pk = F.packed[(size_t)k];
+      const int c = (int)(pk >> 3);
+      const double* bb = &S.bco[24 * (size_t)c + 3 * (pk & 7u)];
+      for (int64_t kp = P.row[(size_t)c]; kp < P.row[(size_t)c + 1]; ++kp) {
+        const double pv = P.val[(size_t)kp];
+        QE e;
+        e.coarse = P.col[(size_t)kp];
+        for (int d = 0; d < 3; ++d) e.b[d] = pv * bb[d];
+        q.push_back(e);
+      }
+    }
+    std::sort(q.begin(), q.end(), [](const QE& a, const QE& b) { return a.coarse < b.coarse; });
+    size_t w = 0;
+    for (size_t k = 0; k < q.size();) {
+      const int c = q[k].coarse;
+      double s[3] = {0, 0, 0};
+      size_t j = k;
+      for (; j < q.size() && q[j].coarse == c; ++j)
+        for (int d = 0; d < 3; ++d) s[d] += q[j].b[d];
+      q[w].coarse = c;
+      for (int d = 0; d < 3; ++d) q[w].b[d] = s[d];
+      ++w;
+      k = j;
+    }
+    q.resize(w);
+    const double r = rau[(size_t)g];
+    for (size_t a = 0; a < q.size(); ++a)
+      for (size_t b = a; b < q.size(); ++b) {
+        const double v = r * (q[a].b[0] * q[b].b[0] + q[a].b[1] * q[b].b[1] + q[a].b[2] * q[b].b[2]);
+        if (v == 0.0) continue;
+        rows[(size_t)q[a].coarse][q[b].coarse] += v;
+        if (a != b) rows[(size_t)q[b].coarse][q[a].coarse] += v;
+      }
+  }
+  return pack_rows(rows);
+}
+
+Transfer sa_explicit_transfer(const CsrHost& A, const std::vector<int32_t>& id, int nagg, double lambda, double damping,
+                              int max_nnz) {
+  const double omega = damping / lambda;
+  Transfer P;
+  P.nf = A.n;
+  P.nc = nagg;
+  P.row.assign((size_t)A.n + 1, 0);
+  std::vector<Entry> row;
+  for (int i = 0; i < A.n; ++i) {
+    row.clear();
+    const int own = id[(size_t)i];
+    row.push_back({own, 1.0});
+    const double invd = 1.0 / A.diag[(size_t)i];
+    for (int64_t k = A.row[(size_t)i]; k < A.row[(size_t)i + 1]; ++k)
+      row.push_back({id[(size_t)A.col[(size_t)k]], -omega * invd * A.val[(size_t)k]});
+    normalize_prune(row, own, max_nnz);
+    for (const auto& e : row) {
+      P.col.push_back(e.first);
+      P.val.push_back(e.second);
+    }
+    P.row[(size_t)i + 1] = (int64_t)P.col.size();
+  }
+  return P;
+}
+
+// ----------------------------------------------------------------------------
+// CF pieces
+// ----------------------------------------------------------------------------
+inline uint64_t mix64(uint64_t x) {  // splitmix64 output function (Steele, Lea, Flood 2014)
+  x += 0x9e3779b97f4a7c15ull;
+  x = (x ^ (x >> 30)) * 0xbf58476d1ce4e5b9ull;
+  x = (x ^ (x >> 27)) * 0x94d049bb133111ebull;
+  return x ^ (x >> 31);
+}
+
+struct Split {
+  int n = 0, nC = 0;
+  std::vector<uint8_t> state;  // 1 = C, 2 = F
+  std::vector<int32_t> cid;
+  std::vector<std::vector<int32_t>> strong, graph;
+};
+
+double csr_entry(const CsrHost& A, int i, int j) {
+  auto b = A.col.begin() + A.row[(size_t)i], e = A.col.begin() + A.row[(size_t)i + 1];
+  auto it = std::lower_bound(b, e, j);
+  return (it == e || *it != j) ? 0.0 : A.val[(size_t)(it - A.col.begin())];
+}
+
+Split pmis_split(const CsrHost& A, double theta) {
+  Split R;
+  R.n = A.n;
+  std::vector<double> maxneg((size_t)A.n, 0.0);
+  for (int i = 0; i < A.n; ++i)
+    for (int64_t k = A.row[(size_t)i]; k < A.row[(size_t)i + 1]; ++k) {
+      const int j = A.col[(size_t)k];
+      const double a = A.val[(size_t)k];
+      if (j != i && a < 0.0) maxneg[(size_t)i] = std::max(maxneg[(size_t)i], -a);
+    }
+  R.strong.resize((size_t)A.n);
+  R.graph.resize((size_t)A.n);
+  for (int i = 0; i < A.n; ++i) {
+    const double thr = theta * maxneg[(size_t)i];
+    auto& s = R.strong[(size_t)i];
+    if (thr > 0.0)
+      for (int64_t k = A.row[(size_t)i]; k < A.row[(size_t)i + 1]; ++k) {
+        const int j = A.col[(size_t)k];
+        const double a = A.val[(size_t)k];
+        if (j != i && a < 0.0 && -a >= thr) s.push_back(j);
+      }
+    std::sort(s.begin(), s.end());
+    s.erase(std::unique(s.begin(), s.end()), s.end());
+    for (int j : s) {
+      R.graph[(size_t)i].push_back(j);
+      R.graph[(size_t)j].push_back(i);
+    }
+  }
+  for (auto& g : R.graph) {
+    std::sort(g.begin(), g.end());
+    g.erase(std::unique(g.begin(), g.end()), g.end());
+  }
+  std::vector<uint64_t> h((size_t)A.n);
+  for (int i = 0; i < A.n; ++i) h[(size_t)i] = mix64((uint64_t)i + 0x63021ull);
+  auto higher = [&](int a, int b) {
+    const size_t da = R.graph[(size_t)a].size(), db = R.graph[(size_t)b].size();
+    if (da != db) return da > db;
+    if (h[(size_t)a] != h[(size_t)b]) return h[(size_t)a] > h[(size_t)b];
+    return a > b;
+  };
+  R.state.assign((size_t)A.n, 0);
+  int undecided = A.n, rounds = 0;
+  std::vector<int32_t> win;
+  while (undecided > 0) {
+    win.clear();
+    for (int i = 0; i < A.n; ++i) {
+      if (R.state[(size_t)i]) continue;
+      bool w = true;
+      for (int j : R.graph[(size_t)i])
+        if (R.state[(size_t)j] == 0 && higher(j, i)) { w = false; break; }
+      if (w) win.push_back(i);
+    }
+    if (win.empty()) throw std::runtime_error("PMIS made no progress");
+    for (int i : win)
+      if (R.state[(size_t)i] == 0) { R.state[(size_t)i] = 1; --undecided; }
+    for (int i : win)
+      for (int j : R.graph[(size_t)i])
+        if (R.state[(size_t)j] == 0) { R.state[(size_t)j] = 2; --undecided; }
+    if (++rounds > A.n) throw std::runtime_error("PMIS excessive rounds");
+  }
+  R.cid.assign((size_t)A.n, -1);
+  for (int i = 0; i < A.n; ++i)
+    if (R.state[(size_t)i] == 1) R.cid[(size_t)i] = R.nC++;
+  return R;
+}
+
+Transfer cf_transfer(const CsrHost& A, const Split& S, int pmax, const std::string& interp) {
+  if (interp != "direct" && interp != "exti") throw std::runtime_error("CF interpolation must be direct or exti");
+  const bool ext = interp == "exti";
+  Transfer P;
+  P.nf = A.n;
+  P.nc = S.nC;
+  P.row.assign((size_t)A.n + 1, 0);
+  std::vector<Entry> cand;
+  // accumulator keyed by coarse id, remembering first-insertion order
+  std::unordered_map<int, double> acc;
+  for (int i = 0; i < A.n; ++i) {
+    cand.clear();
+    if (S.state[(size_t)i] == 1) {
+      cand.push_back({S.cid[(size_t)i], 1.0});
+    } else {
+      acc.clear();
+      for (int j : S.strong[(size_t)i]) {
+        if (S.state[(size_t)j] != 1) continue;
+        const double a = csr_entry(A, i, j);
+        const double w = a < 0.0 ? -a : std::abs(a);
+        if (w > 0.0) acc[S.cid[(size_t)j]] += w;
+      }
+      if (ext) {
+        for (int k : S.strong[(size_t)i]) {
+          if (S.state[(size_t)k] != 2) continue;
+          const double aik = csr_entry(A, i, k);
+          const double path = aik < 0.0 ? -aik : 0.0;
+          if (!(path > 0.0)) continue;
+          double denom = 0.0;
+          for (int j : S.strong[(size_t)k]) {
+            if (S.state[(size_t)j] != 1) continue;
+            const double akj = csr_entry(A, k, j);
+            if (akj < 0.0) denom += -akj;
+          }
+          if (!(denom > 0.0)) continue;
+          for (int j : S.strong[(size_t)k]) {
+            if (S.state[(size_t)j] != 1) continue;
+            const double akj = csr_entry(A, k, j);
+            if (akj < 0.0) acc[S.cid[(size_t)j]] += path * ((-akj) / denom);
+          }
+        }
+      }
+      if (acc.empty()) {
+        for (int j : S.graph[(size_t)i]) {
+          if (S.state[(size_t)j] != 1) continue;
+          const double w = std::abs(csr_entry(A, i, j));
+          if (w > 0.0) acc[S.cid[(size_t)j]] += w;
+        }
+      }
+      if (acc.empty()) throw std::runtime_error("CF interpolation row has no C target");
+      for (const auto& kv : acc)
+        if (kv.second > 0.0) cand.push_back(kv);
+      if (cand.empty()) throw std::runtime_error("CF interpolation empty candidates");
+      std::sort(cand.begin(), cand.end(), [](const Entry& a, const Entry& b) {
+        if (a.second != b.second) return a.second > b.second;
+        return a.first < b.first;
+      });
+      if (pmax > 0 && (int)cand.size() > pmax) cand.resize((size_t)pmax);
+      double sum = 0.0;
+      for (const auto& e : cand) sum += e.second;
+      if (!(sum > 0.0) || !std::isfinite(sum)) throw std::runtime_error("CF interpolation invalid weight sum");
+      for (auto& e : cand) e.second /= sum;
+      std::sort(cand.begin(), cand.end(), [](const Entry& a, const Entry& b) { return a.first < b.first; });
+    }
+    for (const auto& e : cand) {
+      P.col.push_back(e.first);
+      P.val.push_back(e.second);
+    }
+    P.row[(size_t)i + 1] = (int64_t)P.col.size();
+  }
+  return P;
+}
+
+// exact product P01 * P12 (no pruning)
+Transfer compose(const Transfer& A, const Transfer& B) {
+  if (A.nc != B.nf) throw std::runtime_error("transfer composition size mismatch");
+  Transfer P;
+  P.nf = A.nf;
+  P.nc = B.nc;
+  P.row.assign((size_t)A.nf + 1, 0);
+  std::vector<Entry> q;
+  for (int i = 0; i < A.nf; ++i) {
+    q.clear();
+    for (int64_t k = A.row[(size_t)i]; k < A.row[(size_t)i + 1]; ++k) {
+      const int j = A.col[(size_t)k];
+      const double a = A.val[(size_t)k];
+      for (int64_t kb = B.row[(size_t)j]; kb < B.row[(size_t)j + 1]; ++kb) q.push_back({B.col[(size_t)kb], a * B.val[(size_t)kb]});
+    }
+    std::stable_sort(q.begin(), q.end(), [](const Entry& a, const Entry& b) { return a.first < b.first; });
+    for (size_t k = 0; k < q.size();) {
+      const int c = q[k].first;
+      double v = 0.0;
+      size_t j = k;
+      for (; j < q.size() && q[j].first == c; ++j) v += q[j].second;
+      if (v != 0.0) {
+        P.col.push_back(c);
+        P.val.push_back(v);
+      }
+      k = j;
+    }
+    P.row[(size_t)i + 1] = (int64_t)P.col.size();
+  }
+  return P;
+}
+
+}  // namespace
+
+std::vector<int32_t> aggregate_graph(const std::vector<std::vector<int32_t>>& g, int target, int minsz, int softmax,
+                                     int* nagg_out) {
+  const int n = (int)g.size();
+  std::vector<int> id((size_t)n, -1);
+  std::vector<std::vector<int>> m;
+  std::vector<int> q;
+  for (int seed = 0; seed < n; ++seed) {
+    if (id[(size_t)seed] >= 0) continue;
+    const int a = (int)m.size();
+    q.clear();
+    q.push_back(seed);
+    id[(size_t)seed] = a;
+    for (size_t h = 0; h < q.size() && (int)q.size() < target; ++h) {
+      const int i = q[h];
+      for (int j : g[(size_t)i])
+        if (id[(size_t)j] < 0 && (int)q.size() < target) {
+          id[(size_t)j] = a;
+          q.push_back(j);
+        }
+    }
+    m.push_back(q);
+  }
+  for (int a = 0; a < (int)m.size(); ++a) {
+    if (m[(size_t)a].empty() || (int)m[(size_t)a].size() >= minsz) continue;
+    int best = -1, bestsize = INT_MAX;
+    bool bestfit = false;
+    for (int i : m[(size_t)a])
+      for (int j : g[(size_t)i]) {
+        const int b = id[(size_t)j];
+        if (b < 0 || b == a || m[(size_t)b].empty()) continue;
+        const int combined = (int)m[(size_t)a].size() + (int)m[(size_t)b].size();
+        const bool fit = combined <= softmax;
+        if (best < 0 || (fit && !bestfit) || (fit == bestfit && (int)m[(size_t)b].size() < bestsize)) {
+          best = b;
+          bestsize = (int)m[(size_t)b].size();
+          bestfit = fit;
+        }
+      }
+    if (best >= 0) {
+      for (int i : m[(size_t)a]) {
+        id[(size_t)i] = best;
+        m[(size_t)best].push_back(i);
+      }
+      m[(size_t)a].clear();
+    }
+  }
+  std::vector<int> compact(m.size(), -1);
+  int na = 0;
+  for (size_t a = 0; a < m.size(); ++a)
+    if (!m[a].empty()) compact[a] = na++;
+  std::vector<int32_t> out((size_t)n);
+  for (int i = 0; i < n; ++i) {
+    out[(size_t)i] = compact[(size_t)id[(size_t)i]];
+    if (out[(size_t)i] < 0) throw std::runtime_error("aggregation lost a row");
+  }
+  if (nagg_out) *nagg_out = na;
+  return out;
+}
+
+double power_csr(const CsrHost& A, int its, double safety) {
+  return power_generic(A.n, A.diag, its, safety, [&](const std::vector<double>& x, std::vector<double>& y) { csr_apply(A, x, y); });
+}
+
+std::vector<double> dense_inverse_cholesky(const CsrHost& A) {
+  const int n = A.n;
+  std::vector<double> M((size_t)n * n, 0.0), L((size_t)n * n, 0.0);
+  for (int i = 0; i < n; ++i)
+    for (int64_t k = A.row[(size_t)i]; k < A.row[(size_t)i + 1]; ++k) M[(size_t)i * n + A.col[(size_t)k]] = A.val[(size_t)k];
+  double md = 0;
+  for (int i = 0; i < n; ++i) md = std::max(md, std::abs(M[(size_t)i * n + i]));
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j <= i; ++j) {
+      double s = M[(size_t)i * n + j];
+      for (int k = 0; k < j; ++k) s -= L[(size_t)i * n + k] * L[(size_t)j * n + k];
+      if (i == j) {
+        if (!(s > std::max(1e-30, md * 1e-20)) || !std::isfinite(s))
+          throw std::runtime_error("terminal Cholesky pivot failure at row " + std::to_string(i));
+        L[(size_t)i * n + j] = std::sqrt(s);
+      } else {
+        L[(size_t)i * n + j] = s / L[(size_t)j * n + j];
+      }
+    }
+  std::vector<double> inv((size_t)n * n, 0.0);
+#pragma omp parallel
+  {
+    std::vector<double> y((size_t)n), x((size_t)n);
+#pragma omp for schedule(dynamic, 8)
+    for (int col = 0; col < n; ++col) {
+      for (int i = 0; i < n; ++i) {
+        double s = (i == col) ? 1.0 : 0.0;
+        for (int k = 0; k < i; ++k) s -= L[(size_t)i * n + k] * y[(size_t)k];
+        y[(size_t)i] = s / L[(size_t)i * n + i];
+      }
+      for (int i = n - 1; i >= 0; --i) {
+        double s = y[(size_t)i];
+        for (int k = i + 1; k < n; ++k) s -= L[(size_t)k * n + i] * x[(size_t)k];
+        x[(size_t)i] = s / L[(size_t)i * n + i];
+      }
+      for (int i = 0; i < n; ++i) inv[(size_t)i * n + col] = x[(size_t)i];
+    }
+  }
+  for (int i = 0; i < n; ++i)
+    for (int j = i + 1; j < n; ++j) {
+      const double v = 0.5 * (inv[(size_t)i * n + j] + inv[(size_t)j * n + i]);
+      inv[(size_t)i * n + j] = inv[(size_t)j * n + i] = v;
+    }
+  return inv;
+}
+
+Hierarchy build_hierarchy(const Mesh& m, const Setup& S, const std::vector<double>& rau, const AmgOptions& o) {
+  Hierarchy H;
+  if (o.hierarchy == "sa") {
+    int na = 0;
+    auto id0 = aggregate_graph(face_graph(m), o.agg_target, o.agg_min, o.agg_softmax, &na);
+    H.agg.push_back(id0);
+    // fine diagonal of B diag(rau) B^T
+    H.fine_diag.assign((size_t)S.nc, 0.0);
+    for (int c = 0; c < S.nc; ++c) {
+      double s = 0;
+      for (int a = 0; a < 8; ++a) {
+        const int g = S.ref[8 * (size_t)c + a];
+        if (g < 0) continue;
+        for (int k = 0; k < 3; ++k) {
+          const double b = S.bco[24 * (size_t)c + 3 * a + k];
+          s += rau[(size_t)g] * b * b;
+        }
+      }
+      H.fine_diag[(size_t)c] = s;
+    }
+    FineApply fa(S, rau);
+    H.fine_lambda = power_generic(S.nc, H.fine_diag, o.power_its, o.lambda_safety,
+                                  [&](const std::vector<double>& x, std::vector<double>& y) { fa(x, y); });
+    H.P.push_back(sa_fine_transfer(S, rau, id0, na, H.fine_diag, H.fine_lambda, o.sa_damping, o.interp_max_nnz));
+    H.A.push_back(sa_first_coarse(S, rau, H.P[0]));
+    while (H.A.back().n > o.terminal) {
+      const CsrHost& A = H.A.back();
+      const double lam = power_csr(A, o.power_its, o.lambda_safety);
+      if (H.level_lambda.size() < H.A.size()) H.level_lambda.resize(H.A.size(), 0.0);
+      H.level_lambda[H.A.size() - 1] = lam;
+      int nb = 0;
+      auto id = aggregate_graph(csr_graph(A), o.agg_target, o.agg_min, o.agg_softmax, &nb);
+      H.agg.push_back(id);
+      H.P.push_back(sa_explicit_transfer(A, id, nb, lam, o.sa_damping, o.interp_max_nnz));
+      CsrHost C = galerkin(A, H.P.back());
+      H.A.push_back(std::move(C));
+    }
+    if (H.level_lambda.size() < H.A.size()) H.level_lambda.resize(H.A.size(), 0.0);
+  } else if (o.hierarchy == "cf") {
+    CsrHost A = host_fine_csr(S, rau);
+    H.fine_diag = A.diag;
+    H.fine_lambda = o.power_its > 0 ? power_csr(A, o.power_its, o.lambda_safety) : 1.0;
+    int logical = 0;
+    if (o.cf_aggressive_first && A.n > o.terminal) {
+      Split s0 = pmis_split(A, o.cf_theta);
+      Transfer P01 = cf_transfer(A, s0, o.cf_pmax, o.cf_interp);
+      CsrHost A1 = galerkin(A, P01);
+      if (A1.n <= o.terminal) {
+        H.P.push_back(std::move(P01));
+        H.A.push_back(std::move(A1));
+      } else {
+        Split s1 = pmis_split(A1, o.cf_theta);
+        Transfer P12 = cf_transfer(A1, s1, o.cf_pmax, o.cf_interp);
+        CsrHost A2 = galerkin(A1, P12);
+        H.P.push_back(compose(P01, P12));
+        H.A.push_back(std::move(A2));
+      }
+      if (H.A.back().n > o.terminal) {
+        H.level_lambda.resize(H.A.size(), 0.0);
+        H.level_lambda[0] = o.power_its > 0 ? power_csr(H.A.back(), o.power_its, o.lambda_safety) : 1.0;
+      }
+      A = H.A.back();
+      logical = 1;
+    }
+    while (H.A.empty() || H.A.back().n > o.terminal) {
+      Split s = pmis_split(A, o.cf_theta);
+      H.P.push_back(cf_transfer(A, s, o.cf_pmax, o.cf_interp));
+      H.A.push_back(galerkin(A, H.P.back()));
+      if (H.A.back().n <= o.terminal) break;
+      const size_t idx = H.A.size() - 1;
+      if (H.level_lambda.size() < H.A.size()) H.level_lambda.resize(H.A.size(), 0.0);
+      H.level_lambda[idx] = o.power_its > 0 ? power_csr(H.A.back(), o.power_its, o.lambda_safety) : 1.0;
+      A = H.A.back();
+      if (++logical > 20) throw std::runtime_error("CF hierarchy excessive levels");
+    }
+    if (H.level_lambda.size() < H.A.size()) H.level_lambda.resize(H.A.size(), 1.0);
+  } else {
+    throw std::runtime_error("amg hierarchy must be sa or cf");
+  }
+  H.terminal_n = H.A.back().n;
+  H.terminal_inv = dense_inverse_cholesky(H.A.back());
+  return H;
+}
+
+}  // namespace nds

@@ -1,0 +1,239 @@
+"""ctypes binding of the C ABI in include/nodals_b200.h.
+
+The library is built in-tree (``python -m nodals_b200.build``) and loaded
+from ``nodals_b200/_lib``.  There is no fallback: if the library is missing
+the import fails with the build command to run.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+_LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libnodals_b200.so"
+_lib = None
+
+NDS_OK = 0
+ERRORS = {-1: "NDS_E_INVALID", -2: "NDS_E_SETUP", -3: "NDS_E_CUDA", -4: "NDS_E_BREAKDOWN",
+          -5: "NDS_E_NOT_CONVERGED", -6: "NDS_E_STATE"}
+
+PRECISION = {"fp64": 0, "fp32": 1, "amg_fp32": 2}
+RUN_MODE = {"fixed10": 0, "converge": 1}
+MOMENTUM_WORK = {"fgs1": 0, "altgs1": 1, "sgs1": 2}
+PRESSURE_SOLVER = {"pcg": 0, "richardson": 1, "cheb": 2}
+AMG_HIERARCHY = {"sa": 0, "cf": 1}
+AMG_SMOOTHER = {"cheb2": 0, "jacobi": 1, "l1jacobi": 2, "mcgs": 3}
+SPECTRUM = {"auto": 0, "always": 1, "off": 2}
+MCGS_ORDER = {"symmetric": 0, "forward": 1, "backward": 2}
+CF_INTERP = {"direct": 0, "exti": 1}
+_ENUMS = {"precision": PRECISION, "run_mode": RUN_MODE, "momentum_work": MOMENTUM_WORK,
+          "pressure_solver": PRESSURE_SOLVER, "amg_hierarchy": AMG_HIERARCHY, "amg_smoother": AMG_SMOOTHER,
+          "amg_spectrum_policy": SPECTRUM, "amg_mcgs_order": MCGS_ORDER, "cf_interp": CF_INTERP}
+
+
+class NdsError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Options(C.Structure):
+    _fields_ = [
+        ("re", C.c_double), ("bulk", C.c_double), ("simple_tol", C.c_double), ("alpha_u", C.c_double),
+        ("alpha_p", C.c_double), ("rau_scale", C.c_double),
+        ("max_outer", C.c_int), ("run_mode", C.c_int), ("momentum_work", C.c_int),
+        ("mom_omega", C.c_double), ("mom_rtol", C.c_double), ("mom_atol", C.c_double), ("mom_drop", C.c_double),
+        ("mom_max", C.c_int),
+        ("pressure_solver", C.c_int),
+        ("p_rtol", C.c_double), ("p_atol", C.c_double),
+        ("p_max", C.c_int),
+        ("snapshot_tol", C.c_double),
+        ("fine_csr_refresh_every", C.c_int),
+        ("p_richardson_omega", C.c_double),
+        ("p_cheb_degree", C.c_int), ("p_power_its", C.c_int),
+        ("p_cheb_low_fraction", C.c_double), ("p_power_safety", C.c_double),
+        ("amg_hierarchy", C.c_int), ("amg_smoother", C.c_int), ("amg_terminal", C.c_int),
+        ("amg_spectrum_policy", C.c_int),
+        ("amg_power_its", C.c_int), ("amg_cheb_degree", C.c_int),
+        ("amg_lambda_safety", C.c_double), ("amg_lambda_low_fraction", C.c_double), ("amg_jacobi_omega", C.c_double),
+        ("amg_jacobi_fine_sweeps", C.c_int), ("amg_jacobi_coarse_sweeps", C.c_int),
+        ("amg_mcgs_omega", C.c_double),
+        ("amg_mcgs_fine_sweeps", C.c_int), ("amg_mcgs_coarse_sweeps", C.c_int), ("amg_mcgs_order", C.c_int),
+        ("cf_theta", C.c_double),
+        ("cf_pmax", C.c_int), ("cf_interp", C.c_int), ("cf_aggressive_first", C.c_int),
+        ("wall", C.c_char * 64), ("inlet", C.c_char * 64), ("outlet", C.c_char * 64),
+        ("precision", C.c_int), ("threads", C.c_int), ("device", C.c_int), ("verbose", C.c_int),
+    ]
+
+    @classmethod
+    def make(cls, **kw) -> "Options":
+        o = cls()
+        lib().nds_options_default(C.byref(o))
+        for k, v in kw.items():
+            if k in _ENUMS and isinstance(v, str):
+                v = _ENUMS[k][v]
+            if k in ("wall", "inlet", "outlet"):
+                v = v.encode()
+            if not hasattr(o, k):
+                raise KeyError(f"unknown option {k}")
+            setattr(o, k, v)
+        return o
+
+
+class IterReport(C.Structure):
+    _fields_ = [("it", C.c_int), ("rel_cont", C.c_double), ("cont_norm", C.c_double), ("p_its", C.c_int),
+                ("p_rel", C.c_double), ("audited", C.c_int), ("audit_rel", C.c_double * 3),
+                ("all_momentum_met", C.c_int), ("converged", C.c_int),
+                ("ms_assembly", C.c_double), ("ms_momentum", C.c_double), ("ms_continuity", C.c_double),
+                ("ms_pressure", C.c_double), ("ms_update", C.c_double)]
+
+
+class SolveReport(C.Structure):
+    _fields_ = [("outer_its", C.c_int), ("converged", C.c_int), ("pressure_all", C.c_int), ("finite_all", C.c_int),
+                ("final_rel_cont", C.c_double), ("final_audit_rel", C.c_double * 3),
+                ("avg_pressure_its", C.c_double), ("loop_ms", C.c_double), ("assembly_ms", C.c_double),
+                ("momentum_ms", C.c_double), ("continuity_ms", C.c_double), ("pressure_ms", C.c_double),
+                ("update_ms", C.c_double)]
+
+
+class _Array(C.Structure):
+    _fields_ = [("data", C.c_void_p), ("count", C.c_int64), ("dtype", C.c_int)]
+
+
+_DT = {0: np.float64, 1: np.int32, 2: np.int64, 3: np.uint8, 4: np.uint32}
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not _LIB_PATH.exists():
+            raise ImportError(f"{_LIB_PATH} is missing; build it with `python -m nodals_b200.build`")
+        L = C.CDLL(str(_LIB_PATH))
+        vp = C.c_void_p
+        L.nds_last_error.restype = C.c_char_p
+        L.nds_version.restype = C.c_char_p
+        L.nds_options_default.argtypes = [C.POINTER(Options)]
+        L.nds_mesh_read_polymesh.argtypes = [C.c_char_p, C.POINTER(vp)]
+        L.nds_mesh_read_msh2.argtypes = [C.c_char_p, C.POINTER(vp)]
+        L.nds_mesh_from_arrays.argtypes = [C.c_int, vp, C.c_int, vp, C.c_int, vp, vp, C.c_int, C.POINTER(C.c_char_p),
+                                           C.POINTER(vp)]
+        L.nds_mesh_counts.argtypes = [vp] + [C.POINTER(C.c_int)] * 4
+        L.nds_mesh_destroy.argtypes = [vp]
+        L.nds_problem_create.argtypes = [vp, C.POINTER(Options), C.POINTER(vp)]
+        L.nds_problem_array.argtypes = [vp, C.c_char_p, C.POINTER(_Array)]
+        L.nds_problem_counts.argtypes = [vp] + [C.POINTER(C.c_int)] * 4
+        L.nds_problem_destroy.argtypes = [vp]
+        if hasattr(L, "nds_solver_create"):
+            L.nds_solver_create.argtypes = [vp, C.POINTER(vp)]
+            L.nds_solver_reset.argtypes = [vp]
+            L.nds_simple_step.argtypes = [vp, C.POINTER(IterReport)]
+            L.nds_solve.argtypes = [vp, C.POINTER(SolveReport)]
+            L.nds_get_fields.argtypes = [vp] * 5
+            L.nds_set_fields.argtypes = [vp] * 5
+            L.nds_solver_destroy.argtypes = [vp]
+        _lib = L
+    return _lib
+
+
+def _check(rc: int):
+    if rc != NDS_OK:
+        raise NdsError(rc, lib().nds_last_error().decode(errors="replace"))
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+class Mesh:
+    def __init__(self, handle):
+        self._h = handle
+
+    @classmethod
+    def read_polymesh(cls, path) -> "Mesh":
+        h = C.c_void_p()
+        _check(lib().nds_mesh_read_polymesh(str(path).encode(), C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def read_msh2(cls, path) -> "Mesh":
+        h = C.c_void_p()
+        _check(lib().nds_mesh_read_msh2(str(path).encode(), C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_tetmesh(cls, m) -> "Mesh":
+        """From a nodals_b200.meshgen.TetMesh (points, tets, tagged boundary triangles)."""
+        from .meshgen import PATCHES
+        xyz = np.ascontiguousarray(m.points, dtype=np.float64)
+        tets = np.ascontiguousarray(m.tets, dtype=np.int32)
+        btri = np.ascontiguousarray(m.bfaces, dtype=np.int32)
+        bpat = np.ascontiguousarray(m.btag, dtype=np.int32)
+        names = (C.c_char_p * len(PATCHES))(*[p.encode() for p in PATCHES])
+        h = C.c_void_p()
+        _check(lib().nds_mesh_from_arrays(len(xyz), _p(xyz), len(tets), _p(tets), len(btri), _p(btri), _p(bpat),
+                                          len(PATCHES), names, C.byref(h)))
+        return cls(h)
+
+    def counts(self):
+        v = [C.c_int() for _ in range(4)]
+        _check(lib().nds_mesh_counts(self._h, *[C.byref(x) for x in v]))
+        return dict(zip(("points", "cells", "faces", "internal"), (x.value for x in v)))
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.nds_mesh_destroy(self._h)
+            self._h = None
+
+
+class Problem:
+    """Host setup: numbering, momentum CSR, colouring, cell plans, AMG hierarchy."""
+
+    def __init__(self, mesh: Mesh, options: Options | None = None, **kw):
+        self.mesh = mesh
+        self.options = options if options is not None else Options.make(**kw)
+        h = C.c_void_p()
+        _check(lib().nds_problem_create(mesh._h, C.byref(self.options), C.byref(h)))
+        self._h = h
+
+    def array(self, name: str) -> np.ndarray:
+        a = _Array()
+        _check(lib().nds_problem_array(self._h, name.encode(), C.byref(a)))
+        dt = np.dtype(_DT[a.dtype])
+        if a.count == 0:
+            return np.zeros(0, dtype=dt)
+        buf = (C.c_char * (a.count * dt.itemsize)).from_address(a.data)
+        return np.frombuffer(buf, dtype=dt).copy()
+
+    def scalar(self, name: str) -> float:
+        return float(self.array(name)[0])
+
+    def counts(self):
+        v = [C.c_int() for _ in range(4)]
+        _check(lib().nds_problem_counts(self._h, *[C.byref(x) for x in v]))
+        return dict(zip(("nc", "nv", "ncolors", "levels"), (x.value for x in v)))
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.nds_problem_destroy(self._h)
+            self._h = None
+
+
+def read_dump(path) -> dict:
+    """Reader of the flat record files written by oracle/ref_setup_dump."""
+    dt = {"f64": np.float64, "i32": np.int32, "i64": np.int64, "u8": np.uint8, "u32": np.uint32}
+    out = {}
+    with open(path, "rb") as f:
+        if f.read(8) != b"NDSDUMP1":
+            raise ValueError("not an NDSDUMP1 file")
+        while True:
+            nm = f.read(48)
+            if len(nm) < 48:
+                break
+            name = nm.split(b"\0", 1)[0].decode()
+            d = f.read(8).split(b"\0", 1)[0].decode()
+            n = int(np.frombuffer(f.read(8), dtype=np.int64)[0])
+            t = np.dtype(dt[d])
+            out[name] = np.frombuffer(f.read(n * t.itemsize), dtype=t).copy()
+    return out
