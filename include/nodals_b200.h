@@ -134,6 +134,21 @@ int nds_problem_array(const nds_problem* p, const char* name, nds_array* out);
 int nds_problem_counts(const nds_problem* p, int* nc, int* nv, int* ncolors, int* levels);
 void nds_problem_destroy(nds_problem* p);
 
+/* ---- output surface: replaces h12_write_vtu (h12_vtu_output.hpp:26-94),
+ *      h8_compute_hp_errors (h8_hp_diagnostics.inc:18-100) and
+ *      pressure_drop_fit_g4 (g4_host.hpp:424).  Fields are the solver's
+ *      free-DOF vectors (nv velocity values per component, nc pressures). */
+typedef struct nds_hp_errors {
+  double h_eff, u_l2, u_rel_l2, p_shifted_l2, p_shifted_rel_l2, pressure_shift;
+  double dp_fit, dp_exact, dp_rel_err;
+} nds_hp_errors;
+int nds_write_vtu(const nds_problem* p, const char* path, const double* u0, const double* u1, const double* u2,
+                  const double* pr, int converged, int outer_its);
+int nds_compute_hp_errors(const nds_problem* p, const double* u0, const double* u1, const double* u2, const double* pr,
+                          nds_hp_errors* out);
+int nds_cell_average_velocity(const nds_problem* p, const double* u0, const double* u1, const double* u2,
+                              double* out_xyz /* 3 * nc */);
+
 /* ---- device solver: replaces upload_all (h8_main_base.cu:761-788), the
  *      setup policies (:1984-2025) and the SIMPLE loop (:2046-2119) ------- */
 int nds_solver_create(const nds_problem* p, nds_solver** out);

@@ -23,7 +23,7 @@ CSRC = PKG / "csrc"
 BUILD = PKG / "_build"
 LIB = PKG / "_lib"
 NVCC = os.environ.get("NVCC", "nvcc")
-CXX = os.environ.get("CXX", "g++")
+CXX = os.environ.get("NDS_CXX", "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CXXFLAGS = ["-O3", "-std=c++17", "-fPIC", "-fopenmp", "-Wall", "-Wextra", "-Wno-unused-parameter", "-ffp-contract=off"]
 NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC,-fopenmp",

@@ -1,5 +1,6 @@
 // Host half of the C ABI: meshes, options and the host setup ("problem").
 // No CUDA call is made here, so these entry points work on CPU-only hosts.
+#include <algorithm>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -10,6 +11,8 @@
 #include "../../include/nodals_b200.h"
 #include "capi_internal.hpp"
 #include "host/amg.hpp"
+#include "host/diagnostics.hpp"
+#include "host/fem.hpp"
 #include "host/mesh.hpp"
 #include "host/setup.hpp"
 
@@ -203,6 +206,46 @@ int nds_problem_counts(const nds_problem* pp, int* nc, int* nv, int* ncolors, in
 
 void nds_problem_destroy(nds_problem* p) { delete reinterpret_cast<nds::Problem*>(p); }
 
+int nds_write_vtu(const nds_problem* pp, const char* path, const double* u0, const double* u1, const double* u2,
+                  const double* pr, int converged, int outer_its) {
+  if (!pp || !path || !u0 || !u1 || !u2 || !pr) { set_error("null argument"); return NDS_E_INVALID; }
+  const auto* P = reinterpret_cast<const nds::Problem*>(pp);
+  try {
+    nds::write_vtu(path, P->mesh, P->setup, u0, u1, u2, pr, converged != 0, outer_its);
+    return NDS_OK;
+  } catch (const std::exception& e) {
+    set_error(e.what());
+    return NDS_E_SETUP;
+  }
+}
+
+int nds_compute_hp_errors(const nds_problem* pp, const double* u0, const double* u1, const double* u2, const double* pr,
+                          nds_hp_errors* out) {
+  if (!pp || !u0 || !u1 || !u2 || !pr || !out) { set_error("null argument"); return NDS_E_INVALID; }
+  const auto* P = reinterpret_cast<const nds::Problem*>(pp);
+  const nds::HpErrors E = nds::hp_errors(P->mesh, P->setup, u0, u1, u2, pr);
+  out->h_eff = E.h_eff;
+  out->u_l2 = E.u_l2;
+  out->u_rel_l2 = E.u_rel_l2;
+  out->p_shifted_l2 = E.p_shifted_l2;
+  out->p_shifted_rel_l2 = E.p_shifted_rel_l2;
+  out->pressure_shift = E.pressure_shift;
+  out->dp_fit = E.dp_fit;
+  out->dp_exact = E.dp_exact;
+  out->dp_rel_err = E.dp_rel_err;
+  return NDS_OK;
+}
+
+int nds_cell_average_velocity(const nds_problem* pp, const double* u0, const double* u1, const double* u2,
+                              double* out_xyz) {
+  if (!pp || !u0 || !u1 || !u2 || !out_xyz) { set_error("null argument"); return NDS_E_INVALID; }
+  const auto* P = reinterpret_cast<const nds::Problem*>(pp);
+  std::vector<double> v;
+  nds::cell_average_velocity(P->setup, u0, u1, u2, v);
+  std::copy(v.begin(), v.end(), out_xyz);
+  return NDS_OK;
+}
+
 }  // extern "C"
 
 namespace nds {
@@ -285,6 +328,15 @@ void Problem::index_arrays() {
   A["mesh.opp_face"] = view(mesh_opp, 1);
   A["mesh.face_patch"] = view(mesh.face_patch, 1);
   A["mesh.xyz"] = view(mesh.xyz, 0);
+  {
+    const RefTensors& RT = ref_tensors();
+    auto& t = scalars["centT"];
+    t.assign(&RT.T[0][0][0][0], &RT.T[0][0][0][0] + 8 * 8 * 8 * 3);
+    A["centT"] = view(t, 0);
+    auto& dd = scalars["diffT"];
+    dd.assign(&RT.D[0][0][0][0], &RT.D[0][0][0][0] + 8 * 8 * 3 * 3);
+    A["diffT"] = view(dd, 0);
+  }
   scal("pipe.nu", S.pipe.nu);
   scal("pipe.R", S.pipe.R);
   scal("pipe.L", S.pipe.L);

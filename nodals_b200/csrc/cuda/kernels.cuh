@@ -1,0 +1,578 @@
+// sm_100a kernels of the SIMPLE hot path.  All kernels are deterministic:
+// every output element is owned by one thread, group or warp, and every
+// reduction goes through fixed-order block partials (no floating atomics).
+//
+// T is the storage/arithmetic type of states, operators and AMG data
+// (double for the FP64 path, float for FP32); reductions and Krylov scalars
+// are double in both, as in the reference (gpu/serial_cuda/precision.hpp:7-36).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "common.cuh"
+
+namespace nds {
+namespace k {
+
+// ---------------------------------------------------------------------------
+// block partial reductions -> out[NV] (single block, fixed order)
+// ---------------------------------------------------------------------------
+template <int NV>
+__global__ void reduce_partials(const double* __restrict__ part, int nblocks, double* __restrict__ out) {
+  double v[NV];
+#pragma unroll
+  for (int k = 0; k < NV; ++k) v[k] = 0.0;
+  for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
+#pragma unroll
+    for (int k = 0; k < NV; ++k) v[k] += part[(size_t)b * NV + k];
+  block_sum<NV>(v);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int k = 0; k < NV; ++k) out[k] = v[k];
+}
+
+template <int NV>
+__device__ __forceinline__ void write_partials(double (&v)[NV], double* part) {
+  block_sum<NV>(v);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int k = 0; k < NV; ++k) part[(size_t)blockIdx.x * NV + k] = v[k];
+}
+
+// ---------------------------------------------------------------------------
+// Momentum: fused row-owned assembly (a9 + a10 + a11 + a12)
+//
+//   A[i,:]  = K[i,:] + sum_{(c,a) incident to i} C_c[a,:]           (convection, lagged u)
+//   conv_i  = - sum C_c[a,b] u_fixed(b)                              (Dirichlet columns)
+//   delta_i = (1/alpha_u - 1) sum_k |A[i,k]|, A[i,i] += delta_i     (row-L1 relaxation)
+//   diag_i  = A[i,i], rau_i = rau_scale / A[i,i]
+//   b_d[i]  = s_d[i] + conv_d[i] + (B^T p)_d[i] + delta_i u_d[i]
+// with C_c[a,b] = det_c sum_m sum_j ur[m][j] T[a][m][b][j],
+//      ur[m][j] = sum_d u_d(m) invJ_c[j][d].
+// Reference: h7_momentum_assembly.cuh:16-85, h4_kernels.cuh:10-56,
+// g5e_fp32_kernels.cuh:78-85 and :97-105, h8_precomputed_b.cuh:93-114.
+// One group of 8 lanes owns a row; incident cells are visited in ascending
+// cell order, so every A entry is summed in a fixed order (K first).
+// ---------------------------------------------------------------------------
+template <class T>
+struct MomArgs {
+  int nrows;
+  const int32_t* __restrict__ row;      // momentum CSR (int32 offsets)
+  const int32_t* __restrict__ dpos;     // diagonal position (absolute)
+  const T* __restrict__ K;              // persistent diffusion values
+  const int32_t* __restrict__ inc_off;  // row -> incident (cell,a)
+  const uint32_t* __restrict__ inc;     // (cell << 3) | a
+  const int32_t* __restrict__ ref;      // 8 per cell
+  const uint8_t* __restrict__ slot;     // 64 per cell
+  const T* __restrict__ det;
+  const T* __restrict__ invJ;           // 9 per cell
+  const T* __restrict__ bco;            // 24 per cell
+  const T* __restrict__ fixed;          // 3 per fixed slot
+  const T* __restrict__ u0;
+  const T* __restrict__ u1;
+  const T* __restrict__ u2;
+  const T* __restrict__ p;
+  const T* __restrict__ s0;
+  const T* __restrict__ s1;
+  const T* __restrict__ s2;
+  const T* __restrict__ centT;          // 8*8*8*3 reference convection tensor
+  T alpha_u, rau_scale;
+  int row_cap;                          // shared row buffer length per group
+  T* __restrict__ A;
+  T* __restrict__ delta;
+  T* __restrict__ diag;
+  T* __restrict__ rau;
+  T* __restrict__ b0;
+  T* __restrict__ b1;
+  T* __restrict__ b2;
+};
+
+template <class T>
+__global__ void __launch_bounds__(kBlock) mom_assemble(MomArgs<T> g) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* sT = reinterpret_cast<T*>(smem_raw);                  // 1536
+  T* sRow = sT + 1536;                                     // groups * row_cap
+  const int tid = threadIdx.x;
+  for (int k = tid; k < 1536; k += blockDim.x) sT[k] = g.centT[k];
+  __syncthreads();
+  const int lane8 = tid & 7;
+  const int grp = tid >> 3;
+  const int groups = blockDim.x >> 3;
+  T* buf = sRow + (size_t)grp * g.row_cap;
+  const unsigned gmask = group8_mask();
+  for (int i = blockIdx.x * groups + grp; i < g.nrows; i += gridDim.x * groups) {
+    const int rb = g.row[i], re = g.row[i + 1], len = re - rb;
+    for (int k = lane8; k < len; k += 8) buf[k] = g.K[rb + k];
+    __syncwarp(gmask);
+    T conv0 = 0, conv1 = 0, conv2 = 0, bt0 = 0, bt1 = 0, bt2 = 0;
+    for (int z = g.inc_off[i]; z < g.inc_off[i + 1]; ++z) {
+      const uint32_t pk = g.inc[z];
+      const int c = (int)(pk >> 3), a = (int)(pk & 7u);
+      // lane m: value of basis function m of cell c
+      const int gm = g.ref[8 * (size_t)c + lane8];
+      T q0, q1, q2;
+      if (gm >= 0) {
+        q0 = g.u0[gm];
+        q1 = g.u1[gm];
+        q2 = g.u2[gm];
+      } else {
+        const T* f = g.fixed + 3 * (size_t)(-gm - 1);
+        q0 = f[0];
+        q1 = f[1];
+        q2 = f[2];
+      }
+      const T* I = g.invJ + 9 * (size_t)c;
+      const T r0 = q0 * I[0] + q1 * I[1] + q2 * I[2];
+      const T r1 = q0 * I[3] + q1 * I[4] + q2 * I[5];
+      const T r2 = q0 * I[6] + q1 * I[7] + q2 * I[8];
+      // lane b: C[a][b]
+      T cv = 0;
+#pragma unroll
+      for (int m = 0; m < 8; ++m) {
+        const T w0 = __shfl_sync(gmask, r0, m, 8);
+        const T w1 = __shfl_sync(gmask, r1, m, 8);
+        const T w2 = __shfl_sync(gmask, r2, m, 8);
+        const T* t = sT + ((a * 8 + m) * 8 + lane8) * 3;
+        cv += w0 * t[0] + w1 * t[1] + w2 * t[2];
+      }
+      cv *= g.det[c];
+      if (gm >= 0) {
+        buf[g.slot[64 * (size_t)c + 8 * a + lane8]] += cv;
+      } else {
+        conv0 -= cv * q0;
+        conv1 -= cv * q1;
+        conv2 -= cv * q2;
+      }
+      if (lane8 == 0) {
+        const T pv = g.p[c];
+        const T* B = g.bco + 24 * (size_t)c + 3 * a;
+        bt0 += B[0] * pv;
+        bt1 += B[1] * pv;
+        bt2 += B[2] * pv;
+      }
+      __syncwarp(gmask);
+    }
+    conv0 = group_sum<8>(conv0, gmask);
+    conv1 = group_sum<8>(conv1, gmask);
+    conv2 = group_sum<8>(conv2, gmask);
+    T l1 = 0;
+    for (int k = lane8; k < len; k += 8) l1 += fabs(buf[k]);
+    l1 = group_sum<8>(l1, gmask);
+    const int dl = g.dpos[i] - rb;
+    const T de = (T(1) / g.alpha_u - T(1)) * l1;
+    __syncwarp(gmask);
+    if (lane8 == 0) buf[dl] += de;
+    __syncwarp(gmask);
+    for (int k = lane8; k < len; k += 8) g.A[rb + k] = buf[k];
+    if (lane8 == 0) {
+      const T d = buf[dl];
+      g.delta[i] = de;
+      g.diag[i] = d;
+      g.rau[i] = (T(1) / d) * g.rau_scale;
+      g.b0[i] = g.s0[i] + conv0 + bt0 + de * g.u0[i];
+      g.b1[i] = g.s1[i] + conv1 + bt1 + de * g.u1[i];
+      g.b2[i] = g.s2[i] + conv2 + bt2 + de * g.u2[i];
+    }
+    __syncwarp(gmask);
+  }
+}
+
+// One multicolour Gauss-Seidel colour pass on the shared momentum matrix,
+// three right-hand sides (g5e_fp32_kernels.cuh:106-116).  8 lanes per row.
+template <class T>
+__global__ void __launch_bounds__(kBlock) mom_gs_color(int count, const int32_t* __restrict__ rows,
+                                                       const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                                       const T* __restrict__ av, const T* __restrict__ diag,
+                                                       const T* __restrict__ b0, const T* __restrict__ b1,
+                                                       const T* __restrict__ b2, T* __restrict__ x0, T* __restrict__ x1,
+                                                       T* __restrict__ x2, T omega) {
+  const int lane8 = threadIdx.x & 7;
+  const int q = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
+  if (q >= count) return;
+  const unsigned gmask = group8_mask();
+  const int i = rows[q];
+  T s0 = 0, s1 = 0, s2 = 0;
+  for (int k = rp[i] + lane8; k < rp[i + 1]; k += 8) {
+    const int j = ci[k];
+    if (j == i) continue;
+    const T a = av[k];
+    s0 += a * x0[j];
+    s1 += a * x1[j];
+    s2 += a * x2[j];
+  }
+  s0 = group_sum<8>(s0, gmask);
+  s1 = group_sum<8>(s1, gmask);
+  s2 = group_sum<8>(s2, gmask);
+  if (lane8 == 0) {
+    const T iv = T(1) / diag[i];
+    x0[i] = (T(1) - omega) * x0[i] + omega * ((b0[i] - s0) * iv);
+    x1[i] = (T(1) - omega) * x1[i] + omega * ((b1[i] - s1) * iv);
+    x2[i] = (T(1) - omega) * x2[i] + omega * ((b2[i] - s2) * iv);
+  }
+}
+
+// ||b_d||^2 and ||b_d - A u_d||^2 (g5e_fp32_kernels.cuh:117-126); 6 partials per block.
+template <class T>
+__global__ void __launch_bounds__(kBlock) mom_audit(int n, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                                    const T* __restrict__ av, const T* __restrict__ b0,
+                                                    const T* __restrict__ b1, const T* __restrict__ b2,
+                                                    const T* __restrict__ x0, const T* __restrict__ x1,
+                                                    const T* __restrict__ x2, double* __restrict__ part) {
+  const int lane8 = threadIdx.x & 7;
+  const unsigned gmask = group8_mask();
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  const int groups_total = (gridDim.x * blockDim.x) >> 3;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 3; i < n; i += groups_total) {
+    T a0 = 0, a1 = 0, a2 = 0;
+    for (int k = rp[i] + lane8; k < rp[i + 1]; k += 8) {
+      const int j = ci[k];
+      const T a = av[k];
+      a0 += a * x0[j];
+      a1 += a * x1[j];
+      a2 += a * x2[j];
+    }
+    a0 = group_sum<8>(a0, gmask);
+    a1 = group_sum<8>(a1, gmask);
+    a2 = group_sum<8>(a2, gmask);
+    if (lane8 == 0) {
+      const double db0 = (double)b0[i], db1 = (double)b1[i], db2 = (double)b2[i];
+      const double r0 = (double)(b0[i] - a0), r1 = (double)(b1[i] - a1), r2 = (double)(b2[i] - a2);
+      acc[0] += db0 * db0;
+      acc[1] += db1 * db1;
+      acc[2] += db2 * db2;
+      acc[3] += r0 * r0;
+      acc[4] += r1 * r1;
+      acc[5] += r2 * r2;
+    }
+  }
+  write_partials<6>(acc, part);
+}
+
+// ---------------------------------------------------------------------------
+// Continuity r_c = fixedDiv_c + sum_a B[c][a] . u(ref a)  (h8_precomputed_b.cuh:140-163),
+// stored negated as the pressure right-hand side, with sum r^2 partials.
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void __launch_bounds__(kBlock) continuity(int nc, const int32_t* __restrict__ ref, const T* __restrict__ bco,
+                                                     const T* __restrict__ fixed_div, const T* __restrict__ u0,
+                                                     const T* __restrict__ u1, const T* __restrict__ u2,
+                                                     T* __restrict__ rhs, double* __restrict__ part) {
+  double acc[1] = {0.0};
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
+    T s = fixed_div[c];
+    const int32_t* rf = ref + 8 * (size_t)c;
+    const T* B = bco + 24 * (size_t)c;
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+      const int g = rf[a];
+      if (g < 0) continue;
+      s += B[3 * a] * u0[g] + B[3 * a + 1] * u1[g] + B[3 * a + 2] * u2[g];
+    }
+    const T sr = s;
+    acc[0] += (double)sr * (double)sr;
+    rhs[c] = -s;
+  }
+  write_partials<1>(acc, part);
+}
+
+// ---------------------------------------------------------------------------
+// Fine Schur CSR numeric refresh A_p = B diag(rau) B^T (a16).
+// Warp per pressure row.  Contributions were sorted by destination slot at
+// setup (stable, from the reference's (basis, incidence) order of
+// h2b_fine_csr.cuh:480-520), so each value is a sequential sum in the
+// reference's serial order; no atomics.
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void __launch_bounds__(kBlock) fine_refresh(int nc, const int32_t* __restrict__ row,
+                                                       const int32_t* __restrict__ coff, const uint8_t* __restrict__ cnt,
+                                                       const uint32_t* __restrict__ cpk, const uint8_t* __restrict__ ca,
+                                                       const int32_t* __restrict__ ref, const T* __restrict__ bco,
+                                                       const T* __restrict__ rau, const int32_t* __restrict__ dpos,
+                                                       T* __restrict__ val, T* __restrict__ diag, T* __restrict__ l1) {
+  __shared__ T sB[kWarps][24];
+  __shared__ T sR[kWarps][8];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (c >= nc) return;
+  if (lane < 24) sB[w][lane] = bco[24 * (size_t)c + lane];
+  if (lane < 8) {
+    const int g = ref[8 * (size_t)c + lane];
+    sR[w][lane] = g >= 0 ? rau[g] : T(0);
+  }
+  __syncwarp();
+  const int rb = row[c], re = row[c + 1];
+  int base = coff[c];
+  T asum = 0;
+  for (int k0 = rb; k0 < re; k0 += 32) {
+    const int k = k0 + lane;
+    const int n = k < re ? (int)cnt[k] : 0;
+    // exclusive scan of counts within the chunk
+    int incl = n;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    const int q0 = base + incl - n;
+    T v = 0;
+    for (int q = q0; q < q0 + n; ++q) {
+      const uint32_t pk = cpk[q];
+      const int a = ca[q];
+      const T* bb = bco + 24 * (size_t)(pk >> 3) + 3 * (pk & 7u);
+      const T dot = sB[w][3 * a] * bb[0] + sB[w][3 * a + 1] * bb[1] + sB[w][3 * a + 2] * bb[2];
+      v += sR[w][a] * dot;
+    }
+    if (k < re) {
+      val[k] = v;
+      asum += fabs(v);
+    }
+    base += __shfl_sync(0xffffffffu, incl, 31);
+  }
+  if (l1) {
+    asum = warp_sum(asum);
+    if (lane == 0) l1[c] = asum;
+  }
+  __syncwarp();
+  if (lane == 0) diag[c] = val[dpos[c]];
+}
+
+// ---------------------------------------------------------------------------
+// CSR SpMV family, warp per row (h2b_fine_csr.cuh:579-596, h6_coarse_spmv.cuh:10-32)
+// ---------------------------------------------------------------------------
+template <class T>
+__device__ __forceinline__ T warp_row_dot(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                          const T* __restrict__ v, const T* __restrict__ x, int i, int lane) {
+  T s = 0;
+  const int rb = rp[i], re = rp[i + 1];
+  for (int k = rb + lane; k < re; k += 32) s += v[k] * x[ci[k]];
+  return warp_sum(s);
+}
+
+// y = A x
+template <class T>
+__global__ void __launch_bounds__(kBlock) spmv(int n, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                               const T* __restrict__ v, const T* __restrict__ x, T* __restrict__ y) {
+  const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (i >= n) return;
+  const T s = warp_row_dot(rp, ci, v, x, i, lane);
+  if (lane == 0) y[i] = s;
+}
+
+// r = b - A x  (optionally also r2 = r)
+template <class T>
+__global__ void __launch_bounds__(kBlock) spmv_resid(int n, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                                     const T* __restrict__ v, const T* __restrict__ x,
+                                                     const T* __restrict__ b, T* __restrict__ r, T* __restrict__ r2) {
+  const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (i >= n) return;
+  const T s = warp_row_dot(rp, ci, v, x, i, lane);
+  if (lane == 0) {
+    const T q = b[i] - s;
+    r[i] = q;
+    if (r2) r2[i] = q;
+  }
+}
+
+// Jacobi-type smoothing step: x_out = x_in + w (b - A x_in) / den
+template <class T>
+__global__ void __launch_bounds__(kBlock) spmv_smooth(int n, const int32_t* __restrict__ rp,
+                                                      const int32_t* __restrict__ ci, const T* __restrict__ v,
+                                                      const T* __restrict__ xin, const T* __restrict__ b,
+                                                      const T* __restrict__ den, T w, T* __restrict__ xout) {
+  const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (i >= n) return;
+  const T s = warp_row_dot(rp, ci, v, xin, i, lane);
+  if (lane == 0) {
+    const T r = b[i] - s;
+    xout[i] = xin[i] + w * r / den[i];
+  }
+}
+
+// q = A p with sum p_i q_i partials
+template <class T>
+__global__ void __launch_bounds__(kBlock) spmv_dot(int n, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                                   const T* __restrict__ v, const T* __restrict__ x, T* __restrict__ y,
+                                                   double* __restrict__ part) {
+  double acc[1] = {0.0};
+  const int lane = threadIdx.x & 31;
+  const int warps_total = (gridDim.x * blockDim.x) >> 5;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += warps_total) {
+    const T s = warp_row_dot(rp, ci, v, x, i, lane);
+    if (lane == 0) {
+      y[i] = s;
+      acc[0] += (double)x[i] * (double)s;
+    }
+  }
+  write_partials<1>(acc, part);
+}
+
+// ---------------------------------------------------------------------------
+// vector kernels (g5e_fp32_kernels.cuh:132-150, vector_kernels.cuh)
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void jacobi_zero(int n, T w, const T* __restrict__ b, const T* __restrict__ d, T* __restrict__ x) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) x[i] = w * b[i] / d[i];
+}
+template <class T>
+__global__ void axpy(int n, T a, const T* __restrict__ x, T* __restrict__ y) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) y[i] += a * x[i];
+}
+template <class T>
+__global__ void copy(int n, const T* __restrict__ a, T* __restrict__ b) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) b[i] = a[i];
+}
+template <class T>
+__global__ void scale(int n, T s, T* __restrict__ x) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) x[i] *= s;
+}
+// x *= 1 / *nrm (norm from a device scalar holding its square)
+template <class T>
+__global__ void scale_inv_sqrt(int n, const double* __restrict__ sq, T* __restrict__ x) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) x[i] *= T(1.0 / sqrt(*sq));
+}
+template <class T>
+__global__ void div_sqrt(int n, const T* __restrict__ x, const T* __restrict__ d, T* __restrict__ y) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) y[i] = x[i] / sqrt(d[i]);
+}
+template <class T>
+__global__ void power_init(int n, T* __restrict__ v) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    const T g = T(i + 1);
+    v[i] = sin(T(0.731) * g) + T(0.27) * cos(T(1.117) * g);
+  }
+}
+
+// partial sums of x.y
+template <class T>
+__global__ void __launch_bounds__(kBlock) dot(int n, const T* __restrict__ x, const T* __restrict__ y,
+                                              double* __restrict__ part) {
+  double acc[1] = {0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    acc[0] += (double)x[i] * (double)y[i];
+  write_partials<1>(acc, part);
+}
+// partial sums of x.y and y.y
+template <class T>
+__global__ void __launch_bounds__(kBlock) dot2(int n, const T* __restrict__ x, const T* __restrict__ y,
+                                               double* __restrict__ part) {
+  double acc[2] = {0.0, 0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double yy = (double)y[i];
+    acc[0] += (double)x[i] * yy;
+    acc[1] += yy * yy;
+  }
+  write_partials<2>(acc, part);
+}
+
+// x += a p; r -= a q; partial r.r.  a = alpha_dev ? *alpha_dev : alpha
+template <class T>
+__global__ void __launch_bounds__(kBlock) xr_update(int n, double alpha, const double* __restrict__ alpha_dev,
+                                                    const T* __restrict__ p, const T* __restrict__ q,
+                                                    T* __restrict__ x, T* __restrict__ r, double* __restrict__ part) {
+  const T a = T(alpha_dev ? *alpha_dev : alpha);
+  double acc[1] = {0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    x[i] += a * p[i];
+    const T rr = r[i] - a * q[i];
+    r[i] = rr;
+    acc[0] += (double)rr * (double)rr;
+  }
+  write_partials<1>(acc, part);
+}
+
+// p = z + beta p, beta = *beta_dev
+template <class T>
+__global__ void p_update(int n, const double* __restrict__ beta_dev, const T* __restrict__ z, T* __restrict__ p) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) p[i] = z[i] + T(*beta_dev) * p[i];
+}
+
+// PCG scalar steps on device.  flags bit 1: pAp <= 0 or non-finite; bit 2: rho <= 0 or non-finite.
+// sc layout: [0] rho  [1] pq  [2] alpha  [3] rn2  [4] rhon  [5] beta
+__global__ void pcg_alpha(double* __restrict__ sc, int* __restrict__ flags) {
+  const double pq = sc[1];
+  if (!(pq > 0.0) || !isfinite(pq)) {
+    *flags |= 1;
+    sc[2] = 0.0;
+    return;
+  }
+  sc[2] = sc[0] / pq;
+}
+__global__ void pcg_beta(double* __restrict__ sc, int* __restrict__ flags) {
+  const double rhon = sc[4];
+  if (!(rhon > 0.0) || !isfinite(rhon)) {
+    *flags |= 2;
+    sc[5] = 0.0;
+    return;
+  }
+  sc[5] = rhon / sc[0];
+  sc[0] = rhon;
+}
+
+// ---------------------------------------------------------------------------
+// transfers and terminal solve (g5e_fp32_kernels.cuh:140-150)
+// ---------------------------------------------------------------------------
+// c = P^T f as a gather over R = P^T (one thread per coarse row)
+template <class T>
+__global__ void restrict_gather(int nc, const int32_t* __restrict__ rr, const int32_t* __restrict__ rc,
+                                const T* __restrict__ rv, const T* __restrict__ f, T* __restrict__ c) {
+  const int I = blockIdx.x * blockDim.x + threadIdx.x;
+  if (I >= nc) return;
+  T s = 0;
+  for (int k = rr[I]; k < rr[I + 1]; ++k) s += rv[k] * f[rc[k]];
+  c[I] = s;
+}
+// f += P c (one thread per fine row)
+template <class T>
+__global__ void prolong_add(int nf, const int32_t* __restrict__ pr, const int32_t* __restrict__ pc,
+                            const T* __restrict__ pv, const T* __restrict__ c, T* __restrict__ f) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nf) return;
+  T s = 0;
+  for (int k = pr[i]; k < pr[i + 1]; ++k) s += pv[k] * c[pc[k]];
+  f[i] += s;
+}
+// x = Ainv b, dense row-major, warp per row
+template <class T>
+__global__ void __launch_bounds__(kBlock) dense_mv(int n, const T* __restrict__ A, const T* __restrict__ b,
+                                                   T* __restrict__ x) {
+  const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (i >= n) return;
+  const T* a = A + (size_t)i * n;
+  T s = 0;
+  for (int j = lane; j < n; j += 32) s += a[j] * b[j];
+  s = warp_sum(s);
+  if (lane == 0) x[i] = s;
+}
+
+// multicolour GS colour pass on an AMG level (h8_main_base.cu:205-223)
+template <class T>
+__global__ void amg_gs_color(int count, const int32_t* __restrict__ rows, const int32_t* __restrict__ rp,
+                             const int32_t* __restrict__ ci, const T* __restrict__ v, const T* __restrict__ diag,
+                             const T* __restrict__ b, T* __restrict__ x, T omega) {
+  const int q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (q >= count) return;
+  const int i = rows[q];
+  T off = 0;
+  for (int k = rp[i] + lane; k < rp[i + 1]; k += 32) {
+    const int j = ci[k];
+    if (j != i) off += v[k] * x[j];
+  }
+  off = warp_sum(off);
+  if (lane == 0) {
+    const T old = x[i];
+    const T gs = (b[i] - off) / diag[i];
+    x[i] = old + omega * (gs - old);
+  }
+}
+
+}  // namespace k
+}  // namespace nds

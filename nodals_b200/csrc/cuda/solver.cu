@@ -1,0 +1,995 @@
+// Device SIMPLE solver: upload of the host setup, the pressure AMG V-cycle,
+// the outer pressure solvers, one SIMPLE iteration, and the C ABI entry
+// points nds_solver_*.  Numerics follow gpu/serial_cuda/h8_main_base.cu:
+//   G4AMG::apply / explicit_vcycle        :544-564
+//   smoothers cheb2 / jacobi / l1jacobi / mcgs  :425-542
+//   pressure_pcg / richardson / cheb_poly  :569-611, :670-726
+//   pressure_precond_power                 :613-668
+//   g5_gpu_spectrum_refresh                :873-906
+//   SIMPLE iteration                       :2046-2119
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <array>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../capi_internal.hpp"
+#include "../host/fem.hpp"
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace nds {
+
+template <class T>
+struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DBuf() = default;
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  DBuf(DBuf&& o) noexcept : p(o.p), n(o.n) {
+    o.p = nullptr;
+    o.n = 0;
+  }
+  DBuf& operator=(DBuf&& o) noexcept {
+    if (this != &o) {
+      release();
+      p = o.p;
+      n = o.n;
+      o.p = nullptr;
+      o.n = 0;
+    }
+    return *this;
+  }
+  ~DBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  void alloc(size_t m) {
+    release();
+    n = m;
+    if (m) NDS_CUDA(cudaMalloc((void**)&p, m * sizeof(T)));
+  }
+  template <class U>
+  void upload(const std::vector<U>& h) {
+    std::vector<T> t(h.begin(), h.end());
+    alloc(t.size());
+    if (n) NDS_CUDA(cudaMemcpy(p, t.data(), n * sizeof(T), cudaMemcpyHostToDevice));
+  }
+  void zero(cudaStream_t s) {
+    if (n) NDS_CUDA(cudaMemsetAsync(p, 0, n * sizeof(T), s));
+  }
+  size_t bytes() const { return n * sizeof(T); }
+};
+
+struct ISolver {
+  virtual ~ISolver() = default;
+  virtual void reset() = 0;
+  virtual void step(nds_iter_report* rep) = 0;
+  virtual void solve(nds_solve_report* rep) = 0;
+  virtual void get_fields(double* u0, double* u1, double* u2, double* p) = 0;
+  virtual void set_fields(const double* u0, const double* u1, const double* u2, const double* p) = 0;
+};
+
+struct SolveFailure : std::runtime_error {
+  int code;
+  SolveFailure(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+namespace {
+
+std::vector<int32_t> to_i32(const std::vector<int64_t>& v, const char* what) {
+  std::vector<int32_t> o(v.size());
+  for (size_t i = 0; i < v.size(); ++i) {
+    if (v[i] > INT32_MAX) throw std::runtime_error(std::string(what) + " exceeds int32 offsets");
+    o[i] = (int32_t)v[i];
+  }
+  return o;
+}
+
+// greedy colouring of a CSR graph in row order (h8_main_base.cu:125-180)
+void greedy_color(int n, const std::vector<int32_t>& row, const std::vector<int32_t>& col, std::vector<int32_t>& rows_out,
+                  std::vector<int>& off_out) {
+  std::vector<int32_t> color((size_t)n, -1);
+  std::vector<int> mark(64, -1);
+  int nc = 0;
+  for (int i = 0; i < n; ++i) {
+    for (int k = row[(size_t)i]; k < row[(size_t)i + 1]; ++k) {
+      const int j = col[(size_t)k];
+      if (j == i) continue;
+      const int cj = color[(size_t)j];
+      if (cj >= 0) {
+        if ((size_t)cj >= mark.size()) mark.resize((size_t)cj + 2, -1);
+        mark[(size_t)cj] = i;
+      }
+    }
+    int c = 0;
+    while ((size_t)c < mark.size() && mark[(size_t)c] == i) ++c;
+    if ((size_t)c >= mark.size()) mark.resize((size_t)c + 2, -1);
+    color[(size_t)i] = c;
+    nc = std::max(nc, c + 1);
+  }
+  off_out.assign((size_t)nc + 1, 0);
+  for (int i = 0; i < n; ++i) ++off_out[(size_t)color[(size_t)i] + 1];
+  for (int c = 0; c < nc; ++c) off_out[(size_t)c + 1] += off_out[(size_t)c];
+  rows_out.resize((size_t)n);
+  std::vector<int> next(off_out.begin(), off_out.end() - 1);
+  for (int i = 0; i < n; ++i) rows_out[(size_t)next[(size_t)color[(size_t)i]]++] = i;
+}
+
+double cheb_root(double hi, double lo, int k, int degree) {
+  const double centre = .5 * (hi + lo), radius = .5 * (hi - lo), pi = 3.141592653589793238462643383279502884;
+  return centre - radius * std::cos(pi * (2.0 * (double)k + 1.0) / (2.0 * (double)degree));
+}
+
+}  // namespace
+
+template <class T>
+class Solver final : public ISolver {
+ public:
+  struct Level {  // explicit AMG level
+    int n = 0;
+    DBuf<int32_t> row, col, crows;
+    std::vector<int> coff;
+    DBuf<T> val, diag, l1, b, x, r, tmp, corr, pong;
+  };
+  struct Xfer {  // P (fine rows) and R = P^T (coarse rows)
+    int nf = 0, nc = 0;
+    DBuf<int32_t> prow, pcol, rrow, rcol;
+    DBuf<T> pval, rval;
+  };
+
+  Solver(const Problem& P) : P_(P), o_(P.opt) {
+    NDS_CUDA(cudaSetDevice(o_.device));
+    NDS_CUDA(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
+    for (auto& e : ev_) NDS_CUDA(cudaEventCreate(&e));
+    upload();
+  }
+  ~Solver() override {
+    for (auto& e : ev_)
+      if (e) cudaEventDestroy(e);
+    if (hsc_) cudaFreeHost(hsc_);
+    if (st_) cudaStreamDestroy(st_);
+  }
+
+  // ------------------------------------------------------------------ setup
+  void upload() {
+    const Setup& S = P_.setup;
+    const Hierarchy& H = P_.hier;
+    nc_ = S.nc;
+    nv_ = S.nv;
+    mrow_.upload(to_i32(S.mom.row, "momentum CSR"));
+    mcol_.upload(S.mom.col);
+    mdpos_.upload(S.mom_diag_pos);
+    K_.upload(S.mom.val);
+    A_.alloc(S.mom.col.size());
+    diag_.alloc((size_t)nv_);
+    delta_.alloc((size_t)nv_);
+    rau_.upload(S.init_rau);
+    rau_pc_.upload(S.init_rau);
+    inc_off_.upload(S.fine.inc_off);
+    inc_.upload(S.fine.packed);
+    ref_.upload(S.ref);
+    slot_.upload(S.row_slot);
+    det_.upload(S.det);
+    invJ_.upload(S.invJ);
+    bco_.upload(S.bco);
+    fixed_.upload(S.fixed_value);
+    fixed_div_.upload(S.fixed_div);
+    for (int d = 0; d < 3; ++d) {
+      s_[d].upload(S.static_rhs[(size_t)d]);
+      u_[d].alloc((size_t)nv_);
+      b_[d].alloc((size_t)nv_);
+      v_[d].alloc((size_t)nv_);
+    }
+    p_.alloc((size_t)nc_);
+    color_rows_.upload(S.color_rows);
+    color_off_ = S.color_off;
+    {
+      const RefTensors& RT = ref_tensors();
+      std::vector<double> t(1536);
+      std::memcpy(t.data(), &RT.T[0][0][0][0], sizeof(double) * 1536);
+      centT_.upload(t);
+    }
+    row_cap_ = 8;
+    for (int i = 0; i < nv_; ++i) row_cap_ = std::max<int>(row_cap_, (int)(S.mom.row[(size_t)i + 1] - S.mom.row[(size_t)i]));
+    row_cap_ = (row_cap_ + 7) / 8 * 8;
+    mom_smem_ = (1536 + (size_t)(kBlock / 8) * row_cap_) * sizeof(T);
+    if (mom_smem_ > 200 * 1024) throw std::runtime_error("momentum row too long for the shared-memory assembly buffer");
+    NDS_CUDA(cudaFuncSetAttribute(k::mom_assemble<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mom_smem_));
+
+    // fine Schur CSR with contributions regrouped by destination slot
+    const FineTopo& F = S.fine;
+    frow_.upload(F.row);
+    fcol_.upload(F.col);
+    fdpos_.upload(F.diag_pos);
+    fcoff_.upload(F.contrib_off);
+    {
+      std::vector<uint8_t> cnt(F.col.size(), 0), ca(F.slot.size());
+      std::vector<uint32_t> cpk(F.slot.size());
+      std::vector<int32_t> cur;
+      for (int c = 0; c < nc_; ++c) {
+        const int rb = F.row[(size_t)c], len = F.row[(size_t)c + 1] - rb;
+        const int q0 = F.contrib_off[(size_t)c];
+        // counts per slot, then stable placement (the order of (a, incidence))
+        for (int q = q0; q < F.contrib_off[(size_t)c + 1]; ++q) {
+          if (cnt[(size_t)rb + F.slot[(size_t)q]] == 255) throw std::runtime_error("more than 255 contributions to one fine entry");
+          ++cnt[(size_t)rb + F.slot[(size_t)q]];
+        }
+        cur.assign((size_t)len + 1, 0);
+        for (int s = 0; s < len; ++s) cur[(size_t)s + 1] = cur[(size_t)s] + cnt[(size_t)rb + s];
+        int q = q0;
+        for (int a = 0; a < 8; ++a) {
+          const int g = S.ref[8 * (size_t)c + a];
+          if (g < 0) continue;
+          for (int k = F.inc_off[(size_t)g]; k < F.inc_off[(size_t)g + 1]; ++k, ++q) {
+            const int pos = q0 + cur[(size_t)F.slot[(size_t)q]]++;
+            cpk[(size_t)pos] = F.packed[(size_t)k];
+            ca[(size_t)pos] = (uint8_t)a;
+          }
+        }
+      }
+      fcnt_.upload(cnt);
+      fca_.upload(ca);
+      fcpk_.upload(cpk);
+    }
+    fval_.alloc(F.col.size());
+    fdiag_.upload(H.fine_diag);
+    const bool l1 = o_.amg_smoother == NDS_SM_L1JACOBI;
+    if (l1) fl1_.alloc((size_t)nc_);
+    if (o_.amg_smoother == NDS_SM_MCGS) {
+      std::vector<int32_t> rows;
+      greedy_color(nc_, F.row, F.col, rows, fine_coff_);
+      fine_crows_.upload(rows);
+    }
+    for (auto* b : {&x_, &r_, &z_, &pp_, &q_, &rhs_, &fr_, &ftmp_, &fcorr_, &frhs_, &fpong_}) b->alloc((size_t)nc_);
+
+    // AMG levels and transfers
+    L_.resize(H.A.size());
+    for (size_t l = 0; l < H.A.size(); ++l) {
+      const CsrHost& A = H.A[l];
+      Level& Lv = L_[l];
+      Lv.n = A.n;
+      Lv.row.upload(to_i32(A.row, "AMG level CSR"));
+      Lv.col.upload(A.col);
+      Lv.val.upload(A.val);
+      Lv.diag.upload(A.diag);
+      std::vector<double> l1h((size_t)A.n);
+      for (int i = 0; i < A.n; ++i) {
+        double ss = 0.0;
+        for (int64_t k = A.row[(size_t)i]; k < A.row[(size_t)i + 1]; ++k) ss += std::abs(A.val[(size_t)k]);
+        l1h[(size_t)i] = ss;
+      }
+      Lv.l1.upload(l1h);
+      for (auto* b : {&Lv.b, &Lv.x, &Lv.r, &Lv.tmp, &Lv.corr, &Lv.pong}) b->alloc((size_t)A.n);
+      if (o_.amg_smoother == NDS_SM_MCGS && l + 1 < H.A.size()) {
+        std::vector<int32_t> rows;
+        std::vector<int32_t> r32 = to_i32(A.row, "AMG level CSR");
+        greedy_color(A.n, r32, A.col, rows, Lv.coff);
+        Lv.crows.upload(rows);
+      }
+    }
+    X_.resize(H.P.size());
+    for (size_t l = 0; l < H.P.size(); ++l) {
+      const Transfer& Ph = H.P[l];
+      Xfer& X = X_[l];
+      X.nf = Ph.nf;
+      X.nc = Ph.nc;
+      X.prow.upload(to_i32(Ph.row, "transfer"));
+      X.pcol.upload(Ph.col);
+      X.pval.upload(Ph.val);
+      // R = P^T, entries of each coarse row in ascending fine row
+      std::vector<int32_t> rr((size_t)Ph.nc + 1, 0), rc(Ph.col.size());
+      std::vector<double> rv(Ph.col.size());
+      for (int32_t c : Ph.col) ++rr[(size_t)c + 1];
+      for (int c = 0; c < Ph.nc; ++c) rr[(size_t)c + 1] += rr[(size_t)c];
+      std::vector<int32_t> pos(rr.begin(), rr.end() - 1);
+      for (int i = 0; i < Ph.nf; ++i)
+        for (int64_t k = Ph.row[(size_t)i]; k < Ph.row[(size_t)i + 1]; ++k) {
+          const int c = Ph.col[(size_t)k];
+          rc[(size_t)pos[(size_t)c]] = i;
+          rv[(size_t)pos[(size_t)c]++] = Ph.val[(size_t)k];
+        }
+      X.rrow.upload(rr);
+      X.rcol.upload(rc);
+      X.rval.upload(rv);
+    }
+    tinv_.upload(H.terminal_inv);
+    fine_lambda_ = H.fine_lambda;
+    level_lambda_ = H.level_lambda;
+    level_lambda_.resize(L_.size(), 0.0);
+
+    part_.alloc((size_t)kMaxPartBlocks * 8);
+    sc_.alloc(kScalars);
+    flags_.alloc(1);
+    NDS_CUDA(cudaMallocHost((void**)&hsc_, sizeof(double) * kScalars));
+    NDS_CUDA(cudaMemsetAsync(flags_.p, 0, sizeof(int), st_));
+
+    // setup-time state: fine CSR refreshed with the initial rAU
+    refresh_fine(rau_.p);
+    if (P_.power_its > 0) {
+      fine_lambda_ = power_fine(P_.power_its, o_.amg_lambda_safety);
+      for (size_t l = 0; l + 1 < L_.size(); ++l) level_lambda_[l] = power_level(L_[l], P_.power_its, o_.amg_lambda_safety);
+    } else {
+      fine_lambda_ = 1.0;
+      for (auto& v : level_lambda_) v = 1.0;
+    }
+    if (o_.pressure_solver == NDS_P_CHEB) p_cheb_lambda_ = precond_power(o_.p_power_its, o_.p_power_safety);
+    NDS_CUDA(cudaStreamSynchronize(st_));
+    reset();
+  }
+
+  // ------------------------------------------------------------------ helpers
+  static constexpr int kMaxPartBlocks = 1184;  // 8 x 148 SMs
+  static constexpr int kScalars = 32;
+  enum { S_RHO = 0, S_PQ = 1, S_ALPHA = 2, S_RN2 = 3, S_RHON = 4, S_BETA = 5, S_TMP = 8, S_TMP2 = 9, S_CONT2 = 10,
+         S_AUDIT = 16 };
+
+  int red_grid(long long n, int per = kBlock) const { return std::min(grid_for(n, per), kMaxPartBlocks); }
+  template <int NV>
+  void reduce_to(int nblocks, int slot) {
+    k::reduce_partials<NV><<<1, kBlock, 0, st_>>>(part_.p, nblocks, sc_.p + slot);
+    NDS_LAUNCH();
+  }
+  void fetch(int first, int count) {
+    NDS_CUDA(cudaMemcpyAsync(hsc_ + first, sc_.p + first, sizeof(double) * count, cudaMemcpyDeviceToHost, st_));
+    NDS_CUDA(cudaStreamSynchronize(st_));
+  }
+  double dot_fetch(const T* x, const T* y, int n, int slot) {
+    const int g = red_grid(n);
+    k::dot<T><<<g, kBlock, 0, st_>>>(n, x, y, part_.p);
+    NDS_LAUNCH();
+    reduce_to<1>(g, slot);
+    fetch(slot, 1);
+    return hsc_[slot];
+  }
+  void dot_dev(const T* x, const T* y, int n, int slot) {
+    const int g = red_grid(n);
+    k::dot<T><<<g, kBlock, 0, st_>>>(n, x, y, part_.p);
+    NDS_LAUNCH();
+    reduce_to<1>(g, slot);
+  }
+
+  void spmv(int n, const int32_t* rp, const int32_t* ci, const T* v, const T* x, T* y) {
+    k::spmv<T><<<grid_for((long long)n * 32), kBlock, 0, st_>>>(n, rp, ci, v, x, y);
+    NDS_LAUNCH();
+  }
+  void resid(int n, const int32_t* rp, const int32_t* ci, const T* v, const T* x, const T* b, T* r, T* r2 = nullptr) {
+    k::spmv_resid<T><<<grid_for((long long)n * 32), kBlock, 0, st_>>>(n, rp, ci, v, x, b, r, r2);
+    NDS_LAUNCH();
+  }
+  void smooth_step(int n, const int32_t* rp, const int32_t* ci, const T* v, const T* xin, const T* b, const T* den,
+                   double w, T* xout) {
+    k::spmv_smooth<T><<<grid_for((long long)n * 32), kBlock, 0, st_>>>(n, rp, ci, v, xin, b, den, T(w), xout);
+    NDS_LAUNCH();
+  }
+  void vcopy(int n, const T* a, T* b) {
+    k::copy<T><<<grid_for(n), kBlock, 0, st_>>>(n, a, b);
+    NDS_LAUNCH();
+  }
+  void vaxpy(int n, double a, const T* x, T* y) {
+    k::axpy<T><<<grid_for(n), kBlock, 0, st_>>>(n, T(a), x, y);
+    NDS_LAUNCH();
+  }
+
+  // fine Schur operator
+  void refresh_fine(const T* rau) {
+    k::fine_refresh<T><<<grid_for((long long)nc_ * 32), kBlock, 0, st_>>>(
+        nc_, frow_.p, fcoff_.p, fcnt_.p, fcpk_.p, fca_.p, ref_.p, bco_.p, rau, fdpos_.p, fval_.p, fdiag_.p, fl1_.p);
+    NDS_LAUNCH();
+  }
+  void fine_apply(const T* x, T* y) { spmv(nc_, frow_.p, fcol_.p, fval_.p, x, y); }
+
+  // ------------------------------------------------------------- smoothers
+  // x = S(b) from a zero initial guess.  Jacobi-type steps write to a second
+  // buffer (xin is read by every row), then the result is copied back.
+  void poly_smooth(int n, const int32_t* rp, const int32_t* ci, const T* v, const T* diag, const T* b, T* x, T* pong,
+                   double lambda, bool cheb, const T* den_jac, int sweeps) {
+    if (cheb) {
+      const double lo = o_.amg_lambda_low_fraction * lambda;
+      if (!(lambda > lo && lo > 0)) throw SolveFailure(NDS_E_BREAKDOWN, "Chebyshev smoother interval invalid");
+      const int deg = o_.amg_cheb_degree;
+      k::jacobi_zero<T><<<grid_for(n), kBlock, 0, st_>>>(n, T(1.0 / cheb_root(lambda, lo, 0, deg)), b, diag, x);
+      NDS_LAUNCH();
+      T* cur = x;
+      T* nxt = pong;
+      for (int kk = 1; kk < deg; ++kk) {
+        smooth_step(n, rp, ci, v, cur, b, diag, 1.0 / cheb_root(lambda, lo, kk, deg), nxt);
+        std::swap(cur, nxt);
+      }
+      if (cur != x) vcopy(n, cur, x);
+    } else {
+      k::jacobi_zero<T><<<grid_for(n), kBlock, 0, st_>>>(n, T(o_.amg_jacobi_omega), b, den_jac, x);
+      NDS_LAUNCH();
+      T* cur = x;
+      T* nxt = pong;
+      for (int s = 1; s < sweeps; ++s) {
+        smooth_step(n, rp, ci, v, cur, b, den_jac, o_.amg_jacobi_omega, nxt);
+        std::swap(cur, nxt);
+      }
+      if (cur != x) vcopy(n, cur, x);
+    }
+  }
+  void mcgs(int n, const int32_t* rp, const int32_t* ci, const T* v, const T* diag, const T* b, T* x,
+            const DBuf<int32_t>& crows, const std::vector<int>& coff, int sweeps) {
+    NDS_CUDA(cudaMemsetAsync(x, 0, sizeof(T) * (size_t)n, st_));
+    const int ncol = (int)coff.size() - 1;
+    auto pass = [&](bool reverse) {
+      for (int qq = 0; qq < ncol; ++qq) {
+        const int c = reverse ? ncol - 1 - qq : qq;
+        const int cnt = coff[(size_t)c + 1] - coff[(size_t)c];
+        if (cnt <= 0) continue;
+        k::amg_gs_color<T><<<grid_for((long long)cnt * 32), kBlock, 0, st_>>>(cnt, crows.p + coff[(size_t)c], rp, ci, v, diag,
+                                                                             b, x, T(o_.amg_mcgs_omega));
+        NDS_LAUNCH();
+      }
+    };
+    for (int s = 0; s < sweeps; ++s) {
+      if (o_.amg_mcgs_order == NDS_MCGS_FORWARD) pass(false);
+      else if (o_.amg_mcgs_order == NDS_MCGS_BACKWARD) pass(true);
+      else { pass(false); pass(true); }
+    }
+  }
+  void smooth_fine(const T* b, T* x) {
+    const int sm = o_.amg_smoother;
+    if (sm == NDS_SM_MCGS) {
+      mcgs(nc_, frow_.p, fcol_.p, fval_.p, fdiag_.p, b, x, fine_crows_, fine_coff_, o_.amg_mcgs_fine_sweeps);
+      return;
+    }
+    const T* den = sm == NDS_SM_L1JACOBI ? fl1_.p : fdiag_.p;
+    poly_smooth(nc_, frow_.p, fcol_.p, fval_.p, fdiag_.p, b, x, fpong_.p, fine_lambda_, sm == NDS_SM_CHEB2, den,
+                o_.amg_jacobi_fine_sweeps);
+  }
+  void smooth_level(Level& A, const T* b, T* x, double lambda) {
+    const int sm = o_.amg_smoother;
+    if (sm == NDS_SM_MCGS) {
+      mcgs(A.n, A.row.p, A.col.p, A.val.p, A.diag.p, b, x, A.crows, A.coff, o_.amg_mcgs_coarse_sweeps);
+      return;
+    }
+    const T* den = sm == NDS_SM_L1JACOBI ? A.l1.p : A.diag.p;
+    poly_smooth(A.n, A.row.p, A.col.p, A.val.p, A.diag.p, b, x, A.pong.p, lambda, sm == NDS_SM_CHEB2, den,
+                o_.amg_jacobi_coarse_sweeps);
+  }
+  void restrict_to(const Xfer& X, const T* f, T* c) {
+    k::restrict_gather<T><<<grid_for(X.nc), kBlock, 0, st_>>>(X.nc, X.rrow.p, X.rcol.p, X.rval.p, f, c);
+    NDS_LAUNCH();
+  }
+  void prolong(const Xfer& X, const T* c, T* f) {
+    k::prolong_add<T><<<grid_for(X.nf), kBlock, 0, st_>>>(X.nf, X.prow.p, X.pcol.p, X.pval.p, c, f);
+    NDS_LAUNCH();
+  }
+
+  // -------------------------------------------------------------- V-cycle
+  void vcycle(int l, const T* b, T* x) {
+    Level& A = L_[(size_t)l];
+    if (l == (int)L_.size() - 1) {
+      k::dense_mv<T><<<grid_for((long long)A.n * 32), kBlock, 0, st_>>>(A.n, tinv_.p, b, x);
+      NDS_LAUNCH();
+      return;
+    }
+    smooth_level(A, b, x, level_lambda_[(size_t)l]);
+    resid(A.n, A.row.p, A.col.p, A.val.p, x, b, A.r.p);
+    Level& C = L_[(size_t)l + 1];
+    restrict_to(X_[(size_t)l + 1], A.r.p, C.b.p);
+    vcycle(l + 1, C.b.p, C.x.p);
+    prolong(X_[(size_t)l + 1], C.x.p, x);
+    // r = b - A x, then the post-smoother solves A corr = r (b is no longer needed)
+    resid(A.n, A.row.p, A.col.p, A.val.p, x, b, A.r.p, A.b.p);
+    smooth_level(A, A.b.p, A.corr.p, level_lambda_[(size_t)l]);
+    vaxpy(A.n, 1.0, A.corr.p, x);
+  }
+  void amg_apply(const T* b, T* z) {
+    smooth_fine(b, z);
+    resid(nc_, frow_.p, fcol_.p, fval_.p, z, b, fr_.p);
+    Level& C = L_[0];
+    restrict_to(X_[0], fr_.p, C.b.p);
+    vcycle(0, C.b.p, C.x.p);
+    prolong(X_[0], C.x.p, z);
+    resid(nc_, frow_.p, fcol_.p, fval_.p, z, b, fr_.p, frhs_.p);
+    smooth_fine(frhs_.p, fcorr_.p);
+    vaxpy(nc_, 1.0, fcorr_.p, z);
+  }
+
+  // ------------------------------------------------------ spectrum estimates
+  double power_fine(int its, double safety) {
+    T* v = fcorr_.p;
+    T* u = frhs_.p;
+    T* au = ftmp_.p;
+    T* w = fr_.p;
+    k::power_init<T><<<grid_for(nc_), kBlock, 0, st_>>>(nc_, v);
+    NDS_LAUNCH();
+    const double vn = std::sqrt(dot_fetch(v, v, nc_, S_TMP));
+    k::scale<T><<<grid_for(nc_), kBlock, 0, st_>>>(nc_, T(1.0 / vn), v);
+    NDS_LAUNCH();
+    double ray = 0.0;
+    for (int it = 0; it < its; ++it) {
+      k::div_sqrt<T><<<grid_for(nc_), kBlock, 0, st_>>>(nc_, v, fdiag_.p, u);
+      fine_apply(u, au);
+      k::div_sqrt<T><<<grid_for(nc_), kBlock, 0, st_>>>(nc_, au, fdiag_.p, w);
+      NDS_LAUNCH();
+      const double num = dot_fetch(v, w, nc_, S_TMP), den = dot_fetch(v, v, nc_, S_TMP2);
+      ray = num / std::max(den, 1e-300);
+      const double wn = std::sqrt(dot_fetch(w, w, nc_, S_TMP));
+      if (!(ray > 0.0) || !(wn > 0.0) || !std::isfinite(ray) || !std::isfinite(wn))
+        throw SolveFailure(NDS_E_BREAKDOWN, "fine GPU power iteration failed");
+      vcopy(nc_, w, v);
+      k::scale<T><<<grid_for(nc_), kBlock, 0, st_>>>(nc_, T(1.0 / wn), v);
+      NDS_LAUNCH();
+    }
+    return safety * ray;
+  }
+  double power_level(Level& A, int its, double safety) {
+    const int n = A.n;
+    k::power_init<T><<<grid_for(n), kBlock, 0, st_>>>(n, A.corr.p);
+    NDS_LAUNCH();
+    const double vn = std::sqrt(dot_fetch(A.corr.p, A.corr.p, n, S_TMP));
+    k::scale<T><<<grid_for(n), kBlock, 0, st_>>>(n, T(1.0 / vn), A.corr.p);
+    NDS_LAUNCH();
+    double ray = 0.0;
+    for (int it = 0; it < its; ++it) {
+      k::div_sqrt<T><<<grid_for(n), kBlock, 0, st_>>>(n, A.corr.p, A.diag.p, A.b.p);
+      spmv(n, A.row.p, A.col.p, A.val.p, A.b.p, A.tmp.p);
+      k::div_sqrt<T><<<grid_for(n), kBlock, 0, st_>>>(n, A.tmp.p, A.diag.p, A.r.p);
+      NDS_LAUNCH();
+      const double num = dot_fetch(A.corr.p, A.r.p, n, S_TMP), den = dot_fetch(A.corr.p, A.corr.p, n, S_TMP2);
+      ray = num / std::max(den, 1e-300);
+      const double wn = std::sqrt(dot_fetch(A.r.p, A.r.p, n, S_TMP));
+      if (!(ray > 0.0) || !(wn > 0.0) || !std::isfinite(ray) || !std::isfinite(wn))
+        throw SolveFailure(NDS_E_BREAKDOWN, "coarse GPU power iteration failed");
+      vcopy(n, A.r.p, A.corr.p);
+      k::scale<T><<<grid_for(n), kBlock, 0, st_>>>(n, T(1.0 / wn), A.corr.p);
+      NDS_LAUNCH();
+    }
+    return safety * ray;
+  }
+  // lambda_max(M^-1 A) for the outer Chebyshev solver
+  double precond_power(int its, double safety) {
+    k::power_init<T><<<grid_for(nc_), kBlock, 0, st_>>>(nc_, pp_.p);
+    NDS_LAUNCH();
+    const double vn = std::sqrt(dot_fetch(pp_.p, pp_.p, nc_, S_TMP));
+    k::scale<T><<<grid_for(nc_), kBlock, 0, st_>>>(nc_, T(1.0 / vn), pp_.p);
+    NDS_LAUNCH();
+    double est = 0.0;
+    for (int kk = 0; kk < its; ++kk) {
+      fine_apply(pp_.p, q_.p);
+      amg_apply(q_.p, z_.p);
+      const double zn = std::sqrt(dot_fetch(z_.p, z_.p, nc_, S_TMP));
+      const double ray = dot_fetch(pp_.p, z_.p, nc_, S_TMP2);
+      if (!(zn > 0.0) || !std::isfinite(zn) || !std::isfinite(ray)) throw SolveFailure(NDS_E_BREAKDOWN, "preconditioned power failed");
+      est = std::max(est, std::max(std::abs(ray), zn));
+      vcopy(nc_, z_.p, pp_.p);
+      k::scale<T><<<grid_for(nc_), kBlock, 0, st_>>>(nc_, T(1.0 / zn), pp_.p);
+      NDS_LAUNCH();
+    }
+    const double hi = safety * est;
+    if (!(hi > 0.0) || !std::isfinite(hi)) throw SolveFailure(NDS_E_BREAKDOWN, "preconditioned lambda invalid");
+    return hi;
+  }
+
+  // ------------------------------------------------------ pressure solvers
+  struct PRes {
+    int its = 0;
+    double rel = 1;
+    bool ok = false;
+  };
+  void check_flags() {
+    int f = 0;
+    NDS_CUDA(cudaMemcpyAsync(&f, flags_.p, sizeof(int), cudaMemcpyDeviceToHost, st_));
+    NDS_CUDA(cudaStreamSynchronize(st_));
+    if (f & 1) throw SolveFailure(NDS_E_BREAKDOWN, "pressure PCG pAp nonpositive");
+    if (f & 2) throw SolveFailure(NDS_E_BREAKDOWN, "pressure PCG rho nonpositive");
+  }
+  // ||r0|| and the zero solution
+  double p_start(const T* rhs) {
+    x_.zero(st_);
+    vcopy(nc_, rhs, r_.p);
+    const double r0 = std::sqrt(dot_fetch(r_.p, r_.p, nc_, S_TMP));
+    if (!std::isfinite(r0)) throw SolveFailure(NDS_E_BREAKDOWN, "pressure initial norm nonfinite");
+    return r0;
+  }
+  PRes pcg(const T* rhs) {
+    const double r0 = p_start(rhs);
+    if (r0 <= o_.p_atol) return {0, 0.0, true};
+    amg_apply(r_.p, z_.p);
+    vcopy(nc_, z_.p, pp_.p);
+    dot_dev(r_.p, z_.p, nc_, S_RHO);
+    fetch(S_RHO, 1);
+    if (!(hsc_[S_RHO] > 0) || !std::isfinite(hsc_[S_RHO])) throw SolveFailure(NDS_E_BREAKDOWN, "pressure PCG initial rho nonpositive");
+    NDS_CUDA(cudaMemsetAsync(flags_.p, 0, sizeof(int), st_));
+    const double target = std::max(o_.p_atol, o_.p_rtol * r0);
+    PRes R;
+    for (int kk = 0; kk < o_.p_max; ++kk) {
+      // q = A p, pq = p.q ; alpha = rho/pq ; x += a p, r -= a q, rn2
+      int g = red_grid((long long)nc_ * 32);
+      k::spmv_dot<T><<<g, kBlock, 0, st_>>>(nc_, frow_.p, fcol_.p, fval_.p, pp_.p, q_.p, part_.p);
+      NDS_LAUNCH();
+      reduce_to<1>(g, S_PQ);
+      k::pcg_alpha<<<1, 1, 0, st_>>>(sc_.p, flags_.p);
+      NDS_LAUNCH();
+      g = red_grid(nc_);
+      k::xr_update<T><<<g, kBlock, 0, st_>>>(nc_, 0.0, sc_.p + S_ALPHA, pp_.p, q_.p, x_.p, r_.p, part_.p);
+      NDS_LAUNCH();
+      reduce_to<1>(g, S_RN2);
+      check_flags();
+      fetch(S_RN2, 1);
+      const double rn = std::sqrt(hsc_[S_RN2]);
+      R.its = kk + 1;
+      R.rel = rn / std::max(r0, 1e-300);
+      if (!std::isfinite(R.rel)) throw SolveFailure(NDS_E_BREAKDOWN, "pressure PCG residual nonfinite");
+      if (rn <= target) {
+        R.ok = true;
+        break;
+      }
+      amg_apply(r_.p, z_.p);
+      dot_dev(r_.p, z_.p, nc_, S_RHON);
+      k::pcg_beta<<<1, 1, 0, st_>>>(sc_.p, flags_.p);
+      NDS_LAUNCH();
+      k::p_update<T><<<grid_for(nc_), kBlock, 0, st_>>>(nc_, sc_.p + S_BETA, z_.p, pp_.p);
+      NDS_LAUNCH();
+    }
+    check_flags();
+    return R;
+  }
+  // Richardson (omega fixed) and outer Chebyshev (omega = 1/root_k)
+  PRes stationary(const T* rhs, bool cheb) {
+    const double r0 = p_start(rhs);
+    if (r0 <= o_.p_atol) return {0, 0.0, true};
+    const double target = std::max(o_.p_atol, o_.p_rtol * r0);
+    double centre = 0, radius = 0;
+    if (cheb) {
+      const double lo = o_.p_cheb_low_fraction * p_cheb_lambda_;
+      centre = .5 * (p_cheb_lambda_ + lo);
+      radius = .5 * (p_cheb_lambda_ - lo);
+    }
+    const double pi = 3.141592653589793238462643383279502884;
+    PRes R;
+    for (int kk = 0; kk < o_.p_max; ++kk) {
+      double omega = o_.p_richardson_omega;
+      if (cheb) {
+        const int ri = kk % o_.p_cheb_degree;
+        omega = 1.0 / (centre - radius * std::cos(pi * (2.0 * (double)ri + 1.0) / (2.0 * (double)o_.p_cheb_degree)));
+      }
+      amg_apply(r_.p, z_.p);
+      fine_apply(z_.p, q_.p);
+      const int g = red_grid(nc_);
+      k::xr_update<T><<<g, kBlock, 0, st_>>>(nc_, omega, nullptr, z_.p, q_.p, x_.p, r_.p, part_.p);
+      NDS_LAUNCH();
+      reduce_to<1>(g, S_RN2);
+      fetch(S_RN2, 1);
+      const double rn = std::sqrt(hsc_[S_RN2]);
+      R.its = kk + 1;
+      R.rel = rn / std::max(r0, 1e-300);
+      if (!std::isfinite(R.rel)) throw SolveFailure(NDS_E_BREAKDOWN, "pressure stationary residual nonfinite");
+      if (rn <= target) {
+        R.ok = true;
+        break;
+      }
+    }
+    return R;
+  }
+
+  // ------------------------------------------------------ SIMPLE iteration
+  void assemble() {
+    k::MomArgs<T> a;
+    a.nrows = nv_;
+    a.row = mrow_.p;
+    a.dpos = mdpos_.p;
+    a.K = K_.p;
+    a.inc_off = inc_off_.p;
+    a.inc = inc_.p;
+    a.ref = ref_.p;
+    a.slot = slot_.p;
+    a.det = det_.p;
+    a.invJ = invJ_.p;
+    a.bco = bco_.p;
+    a.fixed = fixed_.p;
+    a.u0 = u_[0].p;
+    a.u1 = u_[1].p;
+    a.u2 = u_[2].p;
+    a.p = p_.p;
+    a.s0 = s_[0].p;
+    a.s1 = s_[1].p;
+    a.s2 = s_[2].p;
+    a.centT = centT_.p;
+    a.alpha_u = T(o_.alpha_u);
+    a.rau_scale = T(o_.rau_scale);
+    a.row_cap = row_cap_;
+    a.A = A_.p;
+    a.delta = delta_.p;
+    a.diag = diag_.p;
+    a.rau = rau_.p;
+    a.b0 = b_[0].p;
+    a.b1 = b_[1].p;
+    a.b2 = b_[2].p;
+    k::mom_assemble<T><<<grid_for(nv_, kBlock / 8), kBlock, mom_smem_, st_>>>(a);
+    NDS_LAUNCH();
+  }
+  void gs_pass(bool reverse) {
+    const int ncol = (int)color_off_.size() - 1;
+    for (int qq = 0; qq < ncol; ++qq) {
+      const int c = reverse ? ncol - 1 - qq : qq;
+      const int s = color_off_[(size_t)c], n = color_off_[(size_t)c + 1] - s;
+      if (!n) continue;
+      k::mom_gs_color<T><<<grid_for((long long)n * 8), kBlock, 0, st_>>>(n, color_rows_.p + s, mrow_.p, mcol_.p, A_.p,
+                                                                       diag_.p, b_[0].p, b_[1].p, b_[2].p, u_[0].p,
+                                                                       u_[1].p, u_[2].p, T(o_.mom_omega));
+      NDS_LAUNCH();
+    }
+  }
+  std::array<double, 3> audit() {
+    const int g = red_grid((long long)nv_ * 8);
+    k::mom_audit<T><<<g, kBlock, 0, st_>>>(nv_, mrow_.p, mcol_.p, A_.p, b_[0].p, b_[1].p, b_[2].p, u_[0].p, u_[1].p,
+                                           u_[2].p, part_.p);
+    NDS_LAUNCH();
+    reduce_to<6>(g, S_AUDIT);
+    fetch(S_AUDIT, 6);
+    std::array<double, 3> q{};
+    for (int d = 0; d < 3; ++d) {
+      double bn = std::sqrt(std::max(0.0, hsc_[S_AUDIT + d]));
+      if (bn == 0.0) bn = 1.0;
+      q[(size_t)d] = std::sqrt(std::max(0.0, hsc_[S_AUDIT + 3 + d])) / bn;
+    }
+    return q;
+  }
+  double rau_snapshot_rel() {
+    // ||rau - rau_setup|| / ||rau_setup||, in double on the host copies
+    std::vector<T> a((size_t)nv_), b((size_t)nv_);
+    NDS_CUDA(cudaMemcpyAsync(a.data(), rau_.p, sizeof(T) * nv_, cudaMemcpyDeviceToHost, st_));
+    NDS_CUDA(cudaMemcpyAsync(b.data(), rau_pc_.p, sizeof(T) * nv_, cudaMemcpyDeviceToHost, st_));
+    NDS_CUDA(cudaStreamSynchronize(st_));
+    long double d = 0, r = 0;
+    for (int i = 0; i < nv_; ++i) {
+      const long double q = (long double)a[(size_t)i] - (long double)b[(size_t)i];
+      d += q * q;
+      r += (long double)b[(size_t)i] * b[(size_t)i];
+    }
+    return std::sqrt((double)d) / std::max(std::sqrt((double)r), 1e-300);
+  }
+
+  void reset() override {
+    for (int d = 0; d < 3; ++d) u_[d].zero(st_);
+    p_.zero(st_);
+    it_ = 0;
+    cont0_ = -1.0;
+    cont_rel_ = 1.0;
+    NDS_CUDA(cudaStreamSynchronize(st_));
+  }
+
+  void step(nds_iter_report* rep) override {
+    const int it = ++it_;
+    nds_iter_report R{};
+    R.it = it;
+    NDS_CUDA(cudaEventRecord(ev_[0], st_));
+    assemble();
+    NDS_CUDA(cudaEventRecord(ev_[1], st_));
+    if (it == 1) {
+      const double rr = rau_snapshot_rel();
+      if (!(rr < o_.snapshot_tol))
+        throw SolveFailure(NDS_E_SETUP, "setup rAU snapshot mismatch (rel " + std::to_string(rr) + ")");
+    }
+    const bool converge = o_.run_mode == NDS_RUN_CONVERGE;
+    if (converge && it > 1 && cont_rel_ <= o_.simple_tol) {
+      auto q = audit();
+      R.audited = 1;
+      for (int d = 0; d < 3; ++d) R.audit_rel[d] = q[(size_t)d];
+    }
+    if (o_.momentum_work == NDS_MOM_FGS1) gs_pass(false);
+    else if (o_.momentum_work == NDS_MOM_ALTGS1) gs_pass((it & 1) == 0);
+    else { gs_pass(false); gs_pass(true); }
+    NDS_CUDA(cudaEventRecord(ev_[2], st_));
+    {
+      const int g = red_grid(nc_);
+      k::continuity<T><<<g, kBlock, 0, st_>>>(nc_, ref_.p, bco_.p, fixed_div_.p, u_[0].p, u_[1].p, u_[2].p, rhs_.p,
+                                             part_.p);
+      NDS_LAUNCH();
+      reduce_to<1>(g, S_CONT2);
+      fetch(S_CONT2, 1);
+    }
+    const double cn = std::sqrt(hsc_[S_CONT2]);
+    if (it == 1) cont0_ = cn;
+    cont_rel_ = cn / std::max(cont0_, 1e-300);
+    R.cont_norm = cn;
+    R.rel_cont = cont_rel_;
+    NDS_CUDA(cudaEventRecord(ev_[3], st_));
+    refresh_fine(rau_.p);
+    PRes pr;
+    if (o_.pressure_solver == NDS_P_PCG) pr = pcg(rhs_.p);
+    else pr = stationary(rhs_.p, o_.pressure_solver == NDS_P_CHEB);
+    R.p_its = pr.its;
+    R.p_rel = pr.rel;
+    NDS_CUDA(cudaEventRecord(ev_[4], st_));
+    if (!pr.ok) {
+      last_ = R;
+      throw SolveFailure(NDS_E_NOT_CONVERGED, "pressure solve failed its requested target");
+    }
+    vaxpy(nc_, o_.alpha_p, x_.p, p_.p);
+    NDS_CUDA(cudaEventRecord(ev_[5], st_));
+    NDS_CUDA(cudaEventSynchronize(ev_[5]));
+    float ms[5];
+    for (int q = 0; q < 5; ++q) NDS_CUDA(cudaEventElapsedTime(&ms[q], ev_[q], ev_[q + 1]));
+    R.ms_assembly = ms[0];
+    R.ms_momentum = ms[1];
+    R.ms_continuity = ms[2];
+    R.ms_pressure = ms[3];
+    R.ms_update = ms[4];
+    const bool finite = std::isfinite(R.rel_cont) && std::isfinite(R.p_rel) &&
+                        (!R.audited || (std::isfinite(R.audit_rel[0]) && std::isfinite(R.audit_rel[1]) &&
+                                        std::isfinite(R.audit_rel[2])));
+    finite_all_ = finite_all_ && finite;
+    if (R.audited)
+      R.all_momentum_met = R.audit_rel[0] <= o_.simple_tol && R.audit_rel[1] <= o_.simple_tol &&
+                           R.audit_rel[2] <= o_.simple_tol;
+    R.converged = converge && finite_all_ && R.rel_cont <= o_.simple_tol && R.audited && R.all_momentum_met;
+    last_ = R;
+    if (rep) *rep = R;
+  }
+
+  void solve(nds_solve_report* rep) override {
+    nds_solve_report S{};
+    S.pressure_all = 1;
+    finite_all_ = true;
+    long long sumP = 0;
+    for (int it = 1; it <= o_.max_outer; ++it) {
+      nds_iter_report R{};
+      step(&R);
+      sumP += R.p_its;
+      S.outer_its = R.it;
+      S.final_rel_cont = R.rel_cont;
+      if (R.audited)
+        for (int d = 0; d < 3; ++d) S.final_audit_rel[d] = R.audit_rel[d];
+      S.assembly_ms += R.ms_assembly;
+      S.momentum_ms += R.ms_momentum;
+      S.continuity_ms += R.ms_continuity;
+      S.pressure_ms += R.ms_pressure;
+      S.update_ms += R.ms_update;
+      if (o_.verbose)
+        std::printf(
+            "NODALS_GPU_H8_SIMPLE it=%d relCont=%.12e pCG=%d pTrueRel=%.3e residualAudit=%s auditInitRel=[%.3e,%.3e,%.3e] "
+            "allMomentumMet=%d converged=%d\n",
+            R.it, R.rel_cont, R.p_its, R.p_rel, R.audited ? "DONE" : "SKIPPED", R.audit_rel[0], R.audit_rel[1],
+            R.audit_rel[2], R.all_momentum_met, R.converged);
+      if (R.converged) {
+        S.converged = 1;
+        break;
+      }
+    }
+    S.finite_all = finite_all_;
+    S.avg_pressure_its = S.outer_its ? (double)sumP / S.outer_its : 0.0;
+    S.loop_ms = S.assembly_ms + S.momentum_ms + S.continuity_ms + S.pressure_ms + S.update_ms;
+    if (rep) *rep = S;
+  }
+
+  void get_fields(double* u0, double* u1, double* u2, double* p) override {
+    std::vector<T> h;
+    auto get = [&](const DBuf<T>& b, double* out) {
+      if (!out) return;
+      h.resize(b.n);
+      NDS_CUDA(cudaMemcpyAsync(h.data(), b.p, b.bytes(), cudaMemcpyDeviceToHost, st_));
+      NDS_CUDA(cudaStreamSynchronize(st_));
+      for (size_t i = 0; i < b.n; ++i) out[i] = (double)h[i];
+    };
+    get(u_[0], u0);
+    get(u_[1], u1);
+    get(u_[2], u2);
+    get(p_, p);
+  }
+  void set_fields(const double* u0, const double* u1, const double* u2, const double* p) override {
+    auto put = [&](DBuf<T>& b, const double* in) {
+      if (!in) return;
+      std::vector<T> h(in, in + b.n);
+      NDS_CUDA(cudaMemcpyAsync(b.p, h.data(), b.bytes(), cudaMemcpyHostToDevice, st_));
+      NDS_CUDA(cudaStreamSynchronize(st_));
+    };
+    put(u_[0], u0);
+    put(u_[1], u1);
+    put(u_[2], u2);
+    put(p_, p);
+  }
+
+  nds_iter_report last_{};
+
+ private:
+  const Problem& P_;
+  nds_options o_;
+  cudaStream_t st_ = nullptr;
+  cudaEvent_t ev_[6] = {};
+  int nc_ = 0, nv_ = 0, row_cap_ = 0, it_ = 0;
+  size_t mom_smem_ = 0;
+  double cont0_ = -1, cont_rel_ = 1, fine_lambda_ = 1, p_cheb_lambda_ = 1;
+  bool finite_all_ = true;
+  std::vector<double> level_lambda_;
+  // momentum
+  DBuf<int32_t> mrow_, mcol_, mdpos_, inc_off_, ref_, color_rows_;
+  DBuf<uint32_t> inc_;
+  DBuf<uint8_t> slot_;
+  DBuf<T> K_, A_, diag_, delta_, rau_, rau_pc_, det_, invJ_, bco_, fixed_, fixed_div_, centT_, p_;
+  DBuf<T> u_[3], b_[3], s_[3], v_[3];
+  std::vector<int> color_off_;
+  // pressure
+  DBuf<int32_t> frow_, fcol_, fdpos_, fcoff_, fine_crows_;
+  std::vector<int> fine_coff_;
+  DBuf<uint8_t> fcnt_, fca_;
+  DBuf<uint32_t> fcpk_;
+  DBuf<T> fval_, fdiag_, fl1_, x_, r_, z_, pp_, q_, rhs_, fr_, ftmp_, fcorr_, frhs_, fpong_, tinv_;
+  std::vector<Level> L_;
+  std::vector<Xfer> X_;
+  DBuf<double> part_, sc_;
+  DBuf<int> flags_;
+  double* hsc_ = nullptr;
+};
+
+}  // namespace nds
+
+// ============================================================== C ABI
+struct nds_solver {
+  std::unique_ptr<nds::ISolver> impl;
+};
+
+namespace {
+int fail(int code, const std::string& m) {
+  nds::set_error(m);
+  return code;
+}
+template <class F>
+int guarded(F&& f) {
+  try {
+    f();
+    return NDS_OK;
+  } catch (const nds::SolveFailure& e) {
+    return fail(e.code, e.what());
+  } catch (const nds::CudaError& e) {
+    return fail(NDS_E_CUDA, e.what());
+  } catch (const std::exception& e) {
+    return fail(NDS_E_SETUP, e.what());
+  }
+}
+}  // namespace
+
+extern "C" {
+
+int nds_solver_create(const nds_problem* pp, nds_solver** out) {
+  if (!pp || !out) return fail(NDS_E_INVALID, "null argument");
+  const auto* P = reinterpret_cast<const nds::Problem*>(pp);
+  return guarded([&] {
+    int ndev = 0;
+    const cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev <= P->opt.device)
+      throw nds::CudaError(std::string("no CUDA device available: ") + cudaGetErrorString(e));
+    auto s = std::make_unique<nds_solver>();
+    if (P->opt.precision == NDS_FP64) s->impl = std::make_unique<nds::Solver<double>>(*P);
+    else if (P->opt.precision == NDS_FP32) s->impl = std::make_unique<nds::Solver<float>>(*P);
+    else throw nds::SolveFailure(NDS_E_INVALID, "precision amg_fp32 is not supported (mixed State/AMG types)");
+    *out = s.release();
+  });
+}
+int nds_solver_reset(nds_solver* s) {
+  if (!s) return fail(NDS_E_INVALID, "null solver");
+  return guarded([&] { s->impl->reset(); });
+}
+int nds_simple_step(nds_solver* s, nds_iter_report* r) {
+  if (!s) return fail(NDS_E_INVALID, "null solver");
+  return guarded([&] { s->impl->step(r); });
+}
+int nds_solve(nds_solver* s, nds_solve_report* r) {
+  if (!s) return fail(NDS_E_INVALID, "null solver");
+  return guarded([&] { s->impl->solve(r); });
+}
+int nds_get_fields(nds_solver* s, double* u0, double* u1, double* u2, double* p) {
+  if (!s) return fail(NDS_E_INVALID, "null solver");
+  return guarded([&] { s->impl->get_fields(u0, u1, u2, p); });
+}
+int nds_set_fields(nds_solver* s, const double* u0, const double* u1, const double* u2, const double* p) {
+  if (!s) return fail(NDS_E_INVALID, "null solver");
+  return guarded([&] { s->impl->set_fields(u0, u1, u2, p); });
+}
+void nds_solver_destroy(nds_solver* s) { delete s; }
+
+}  // extern "C"

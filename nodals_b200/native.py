@@ -98,6 +98,11 @@ class SolveReport(C.Structure):
                 ("update_ms", C.c_double)]
 
 
+class HpErrors(C.Structure):
+    _fields_ = [(n, C.c_double) for n in ("h_eff", "u_l2", "u_rel_l2", "p_shifted_l2", "p_shifted_rel_l2",
+                                          "pressure_shift", "dp_fit", "dp_exact", "dp_rel_err")]
+
+
 class _Array(C.Structure):
     _fields_ = [("data", C.c_void_p), ("count", C.c_int64), ("dtype", C.c_int)]
 
@@ -125,6 +130,9 @@ def lib():
         L.nds_problem_array.argtypes = [vp, C.c_char_p, C.POINTER(_Array)]
         L.nds_problem_counts.argtypes = [vp] + [C.POINTER(C.c_int)] * 4
         L.nds_problem_destroy.argtypes = [vp]
+        L.nds_write_vtu.argtypes = [vp, C.c_char_p, vp, vp, vp, vp, C.c_int, C.c_int]
+        L.nds_compute_hp_errors.argtypes = [vp, vp, vp, vp, vp, C.POINTER(HpErrors)]
+        L.nds_cell_average_velocity.argtypes = [vp, vp, vp, vp, vp]
         if hasattr(L, "nds_solver_create"):
             L.nds_solver_create.argtypes = [vp, C.POINTER(vp)]
             L.nds_solver_reset.argtypes = [vp]
@@ -218,6 +226,72 @@ class Problem:
         if getattr(self, "_h", None) and _lib is not None:
             _lib.nds_problem_destroy(self._h)
             self._h = None
+
+
+class Solver:
+    """Device solver over a Problem (the problem must outlive the solver)."""
+
+    def __init__(self, problem: Problem):
+        self.problem = problem
+        h = C.c_void_p()
+        _check(lib().nds_solver_create(problem._h, C.byref(h)))
+        self._h = h
+        c = problem.counts()
+        self.nc, self.nv = c["nc"], c["nv"]
+
+    def reset(self):
+        _check(lib().nds_solver_reset(self._h))
+
+    def step(self) -> IterReport:
+        r = IterReport()
+        _check(lib().nds_simple_step(self._h, C.byref(r)))
+        return r
+
+    def solve(self) -> SolveReport:
+        r = SolveReport()
+        _check(lib().nds_solve(self._h, C.byref(r)))
+        return r
+
+    def fields(self):
+        u = [np.zeros(self.nv) for _ in range(3)]
+        p = np.zeros(self.nc)
+        _check(lib().nds_get_fields(self._h, *[_p(x) for x in u], _p(p)))
+        return u[0], u[1], u[2], p
+
+    def set_fields(self, u0, u1, u2, p):
+        arrs = [np.ascontiguousarray(x, dtype=np.float64) for x in (u0, u1, u2, p)]
+        _check(lib().nds_set_fields(self._h, *[_p(x) for x in arrs]))
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.nds_solver_destroy(self._h)
+            self._h = None
+
+
+def _f64(x):
+    return np.ascontiguousarray(x, dtype=np.float64)
+
+
+def cell_average_velocity(problem: Problem, u0, u1, u2, out: np.ndarray | None = None) -> np.ndarray:
+    """U0 cell averages (1/4 vertex + 9/40 face bubbles), shape (nc, 3)."""
+    a = [_f64(x) for x in (u0, u1, u2)]
+    res = np.zeros((problem.counts()["nc"], 3))
+    _check(lib().nds_cell_average_velocity(problem._h, *[_p(x) for x in a], _p(res)))
+    if out is not None:
+        out[...] = res
+    return res
+
+
+def hp_errors(problem: Problem, u0, u1, u2, p) -> dict:
+    a = [_f64(x) for x in (u0, u1, u2, p)]
+    e = HpErrors()
+    _check(lib().nds_compute_hp_errors(problem._h, *[_p(x) for x in a], C.byref(e)))
+    return {k: getattr(e, k) for k, _ in HpErrors._fields_}
+
+
+def write_vtu(problem: Problem, path, u0, u1, u2, p, converged: bool = False, outer_its: int = 0):
+    a = [_f64(x) for x in (u0, u1, u2, p)]
+    _check(lib().nds_write_vtu(problem._h, str(path).encode(), *[_p(x) for x in a], int(converged), int(outer_its)))
 
 
 def read_dump(path) -> dict:

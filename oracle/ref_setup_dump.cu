@@ -185,6 +185,14 @@ int main(int argc, char** argv) {
       w.vec(p + "diag", H.csr[l].diag);
     }
     w.vec("amg.terminal_inv", H.terminal_inv);
+    {
+      const auto& CT = central_tensor_g4();
+      const auto& DT = diffusion_tensor_g3();
+      std::vector<double> ct(&CT.t[0][0][0][0], &CT.t[0][0][0][0] + 8 * 8 * 8 * 3);
+      std::vector<double> dt(&DT.t[0][0][0][0], &DT.t[0][0][0][0] + 8 * 8 * 3 * 3);
+      w.vec("centT", ct);
+      w.vec("diffT", dt);
+    }
     std::printf("NDS_REF_SETUP_DUMP cells=%zu freeVel=%d momNnz=%zu colors=%d fineNnz=%zu levels=%zu status=PASS\n",
                 M.tets.size(), S.topo.n, S.topo.val.size(), S.coloring.ncolors, FH.col.size(), H.csr.size());
     return 0;

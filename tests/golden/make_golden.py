@@ -1,0 +1,173 @@
+#!/usr/bin/env python3
+"""Generate the committed golden fixtures from the reference itself.
+
+Two sources, both built from the reference tree by ``make -C oracle ref``
+into the git-ignored ``oracle/_ref/``:
+
+* ``--setup``   (CPU): ``oracle/_ref/ref_setup_dump`` runs the reference's own
+  host setup builders on a seeded mesh and its arrays are stored as
+  ``setup_<mesh>_<hier>.npz``.
+* ``--runs``    (needs a GPU): the reference H8 binaries
+  ``oracle/_ref/nodals_gpu_h8_{fp64,fp32}`` are run on seeded meshes for the
+  cases in ``CASES``; the NODALS_GPU_H8_SIMPLE history and the VTU fields
+  (P0 pressure, cell-average velocity, 17 digits) are stored as
+  ``run_<case>.npz``.
+
+Meshes are regenerated from ``nodals_b200.meshgen`` (deterministic, seeded),
+so the fixtures only hold reference outputs, never mesh files.
+
+Usage:
+    python tests/golden/make_golden.py --setup  [--out tests/golden]
+    python tests/golden/make_golden.py --runs   [--out DIR]
+"""
+from __future__ import annotations
+
+import argparse
+import re
+import subprocess
+import sys
+import tempfile
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+
+from nodals_b200 import meshgen  # noqa: E402
+from nodals_b200.native import read_dump  # noqa: E402
+
+REF = ROOT / "oracle" / "_ref"
+
+# Setup fixtures: arrays kept (all integer structure + the main float arrays)
+SETUP_KEYS = ["mesh.tets", "mesh.opp_face", "g2free", "fixedValue", "mom.row", "mom.col", "mom.val", "color",
+              "color.offset", "color.rows", "cell.ref", "cell.rowSlot", "cell.det", "cell.bcoeff", "staticRhs0",
+              "staticRhs1", "staticRhs2", "fixedDiv", "initRau", "fine.row", "fine.col", "fine.diagPos", "fine.incOff",
+              "fine.packed", "fine.contribOff", "fine.slot", "amg.fineDiag", "amg.fineLambda", "amg.levelLambda",
+              "amg.terminal_inv", "centT", "diffT", "pipe.nu", "pipe.hpDrop", "pipe.profileScale"]
+SETUP_CASES = {
+    "tiny_sa": ("pipe_tiny", ["--amg-hierarchy", "sa", "--amg-terminal", "60", "--re", "20", "--alpha-u", "0.7"]),
+    "tiny_cf": ("pipe_tiny", ["--amg-hierarchy", "cf", "--cf-pmax", "8", "--cf-interp", "exti", "--amg-terminal", "60",
+                              "--power-its", "0", "--re", "20", "--alpha-u", "0.7"]),
+}
+
+# Reference runs.  Common flags of the ~40k-tet Re=20 configuration:
+# alpha_u 0.7, alpha_p 0.3, pressure rtol 1e-6.
+_CFG1 = ["--re", "20", "--alpha-u", "0.7", "--alpha-p", "0.3", "--p-rtol", "1e-6", "--p-max", "400"]
+_SA = ["--amg-hierarchy", "sa", "--amg-smoother", "cheb2", "--pressure-solver", "pcg"]
+_CF = ["--amg-hierarchy", "cf", "--cf-interp", "exti", "--cf-pmax", "8", "--amg-smoother", "jacobi",
+       "--pressure-solver", "richardson"]
+CASES = {
+    # mesh, precision, run mode flags, solver flags
+    "tiny_sa_fixed10": ("pipe_tiny", "fp64", ["--run-mode", "fixed10", "--max-outer", "10"], _CFG1 + _SA + ["--amg-terminal", "60"]),
+    "tiny_cf_fixed10": ("pipe_tiny", "fp64", ["--run-mode", "fixed10", "--max-outer", "10"], _CFG1 + _CF + ["--amg-terminal", "60"]),
+    "small_sa_fixed10": ("pipe_small", "fp64", ["--run-mode", "fixed10", "--max-outer", "10"], _CFG1 + _SA + ["--amg-terminal", "100"]),
+    "small_cf_fixed10": ("pipe_small", "fp64", ["--run-mode", "fixed10", "--max-outer", "10"], _CFG1 + _CF + ["--amg-terminal", "100"]),
+    "small_sa_default10": ("pipe_small", "fp64", ["--run-mode", "fixed10", "--max-outer", "10"], ["--amg-terminal", "100"]),
+    "small_l1cheb_fixed10": ("pipe_small", "fp64", ["--run-mode", "fixed10", "--max-outer", "10"],
+                             _CFG1 + ["--amg-hierarchy", "cf", "--cf-interp", "direct", "--amg-smoother", "l1jacobi",
+                                      "--pressure-solver", "cheb", "--amg-terminal", "100"]),
+    "small_sa_sgs_fixed10": ("pipe_small", "fp64", ["--run-mode", "fixed10", "--max-outer", "10"],
+                             _CFG1 + _SA + ["--amg-terminal", "100", "--momentum-work", "sgs1"]),
+    "small_sa_converge": ("pipe_small", "fp64", ["--run-mode", "converge", "--max-outer", "400", "--simple-tol", "1e-3"],
+                          _CFG1 + _SA + ["--amg-terminal", "100"]),
+    "small_sa_fixed10_fp32": ("pipe_small", "fp32", ["--run-mode", "fixed10", "--max-outer", "10"], _CFG1 + _SA + ["--amg-terminal", "100"]),
+    "m40k_cf_fixed10": ("pipe40k", "fp64", ["--run-mode", "fixed10", "--max-outer", "10"], _CFG1 + _CF),
+}
+
+_SIMPLE = re.compile(r"NODALS_GPU_H8_SIMPLE .*?it=(\d+) relCont=(\S+) .*?pCG=(\d+) pTrueRel=(\S+)")
+_AUDIT = re.compile(r"auditInitRel=\[(\S+?),(\S+?),(\S+?)\]")
+
+
+def parse_log(text: str):
+    its, rel, pcg, prel, audit = [], [], [], [], []
+    for line in text.splitlines():
+        m = _SIMPLE.search(line)
+        if m:
+            its.append(int(m.group(1)))
+            rel.append(float(m.group(2)))
+            pcg.append(int(m.group(3)))
+            prel.append(float(m.group(4)))
+            a = _AUDIT.search(line)
+            audit.append([float(a.group(k)) for k in (1, 2, 3)] if a else [np.nan] * 3)
+    return np.array(its), np.array(rel), np.array(pcg), np.array(prel), np.array(audit)
+
+
+def parse_vtu(path: Path):
+    text = path.read_text()
+
+    def block(name):
+        m = re.search(r'Name="%s"[^>]*>\s*(.*?)</DataArray>' % name, text, re.S)
+        return np.array(m.group(1).split(), dtype=np.float64)
+
+    return block("p_P0"), block("U0").reshape(-1, 3)
+
+
+def write_mesh(name: str, d: Path) -> Path:
+    return meshgen.write_polymesh(meshgen.named(name), d / name)
+
+
+def make_setup(out: Path):
+    exe = REF / "ref_setup_dump"
+    if not exe.exists():
+        raise SystemExit(f"{exe} missing: run `make -C oracle ref`")
+    with tempfile.TemporaryDirectory() as td:
+        td = Path(td)
+        for case, (mesh, flags) in SETUP_CASES.items():
+            pm = write_mesh(mesh, td)
+            dump = td / f"{case}.bin"
+            subprocess.run([str(exe), "--mesh", str(pm), "--out", str(dump), *flags], check=True,
+                           stdout=subprocess.DEVNULL)
+            R = read_dump(dump)
+            keep = {k: R[k] for k in SETUP_KEYS if k in R}
+            levels = int(R["amg.levels"][0])
+            for l in range(levels):
+                for k in ("row", "col", "val", "diag"):
+                    keep[f"amg.A{l}.{k}"] = R[f"amg.A{l}.{k}"]
+                for k in ("row", "col", "val", "nCoarse"):
+                    keep[f"amg.P{l}.{k}"] = R[f"amg.P{l}.{k}"]
+                if f"amg.agg{l}" in R:
+                    keep[f"amg.agg{l}"] = R[f"amg.agg{l}"]
+            keep["amg.levels"] = R["amg.levels"]
+            np.savez_compressed(out / f"setup_{case}.npz", **keep)
+            print("wrote", out / f"setup_{case}.npz")
+
+
+def make_runs(out: Path, only=None):
+    with tempfile.TemporaryDirectory() as td:
+        td = Path(td)
+        meshes = {}
+        for case, (mesh, prec, mode, flags) in CASES.items():
+            if only and case not in only:
+                continue
+            if mesh not in meshes:
+                meshes[mesh] = write_mesh(mesh, td)
+            exe = REF / f"nodals_gpu_h8_{prec}"
+            vtu = td / f"{case}.vtu"
+            cmd = [str(exe), "--mesh", str(meshes[mesh]), "--tag", case, "--vtu-out", str(vtu), *mode, *flags]
+            r = subprocess.run(cmd, capture_output=True, text=True, timeout=900)
+            (out / f"run_{case}.log").write_text(r.stdout + r.stderr)
+            if r.returncode not in (0, 35):
+                print("FAILED", case, r.returncode, r.stderr[-2000:])
+                continue
+            its, rel, pcg, prel, audit = parse_log(r.stdout)
+            p, u0 = parse_vtu(vtu)
+            np.savez_compressed(out / f"run_{case}.npz", it=its, rel_cont=rel, p_its=pcg, p_rel=prel, audit=audit,
+                                p=p, u_cell=u0, rc=np.array([r.returncode]),
+                                cmd=np.array(" ".join(cmd[3:])))
+            print("wrote", case, "rc", r.returncode, "its", len(its))
+
+
+if __name__ == "__main__":
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--setup", action="store_true")
+    ap.add_argument("--runs", action="store_true")
+    ap.add_argument("--only", nargs="*")
+    ap.add_argument("--out", default=str(Path(__file__).resolve().parent))
+    ns = ap.parse_args()
+    out = Path(ns.out)
+    out.mkdir(parents=True, exist_ok=True)
+    if ns.setup:
+        make_setup(out)
+    if ns.runs:
+        make_runs(out, ns.only)

@@ -1,0 +1,114 @@
+"""GPU parity of the CUDA SIMPLE path (through the C ABI) against the CPU oracle
+and against fixtures produced by the reference H8 binaries.
+
+Tolerances (FP64 path): per-iteration relCont relative difference <= 1e-9 and
+field relative L2 <= 1e-9 against the oracle run on the same setup; the
+pressure iteration counts must match exactly.  Against the reference fixtures
+(independent setup code, different summation order): relCont <= 1e-8 relative,
+P0 pressure and cell-average velocity relative L2 <= 1e-8.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, rel_l2
+
+CFG1 = dict(re=20.0, alpha_u=0.7, alpha_p=0.3, p_rtol=1e-6, p_max=400)
+SA = dict(amg_hierarchy="sa", amg_smoother="cheb2", pressure_solver="pcg")
+CF = dict(amg_hierarchy="cf", cf_interp="exti", cf_pmax=8, amg_smoother="jacobi", pressure_solver="richardson")
+
+ORACLE_CASES = {
+    "sa_pcg": dict(CFG1, **SA, amg_terminal=100),
+    "cf_richardson": dict(CFG1, **CF, amg_terminal=100),
+    "cf_l1_cheb": dict(CFG1, amg_hierarchy="cf", cf_interp="direct", amg_smoother="l1jacobi", pressure_solver="cheb",
+                       amg_terminal=100),
+    "sa_sgs": dict(CFG1, **SA, amg_terminal=100, momentum_work="sgs1"),
+    "defaults": dict(amg_terminal=100),
+}
+
+
+def _make(native, meshes, mesh, **kw):
+    m = native.Mesh.from_tetmesh(meshes(mesh))
+    kw.setdefault("max_outer", 10)
+    return native.Problem(m, **kw)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", sorted(ORACLE_CASES))
+def test_gpu_matches_oracle(native, oracle_mod, meshes, case):
+    P = _make(native, meshes, "pipe_small", **ORACLE_CASES[case])
+    S = native.Solver(P)
+    O = oracle_mod.Oracle(P)
+    for _ in range(10):
+        r = S.step()
+        o = O.step()
+        assert r.p_its == o.p_its, (r.it, r.p_its, o.p_its)
+        assert abs(r.rel_cont - o.rel_cont) <= 1e-9 * abs(o.rel_cont), (r.it, r.rel_cont, o.rel_cont)
+    for a, b in zip(S.fields(), O.fields()):
+        assert rel_l2(a, b) <= 1e-9
+
+
+@pytest.mark.gpu
+def test_gpu_fp32_close_to_fp64(native, meshes):
+    P64 = _make(native, meshes, "pipe_small", **ORACLE_CASES["sa_pcg"])
+    P32 = _make(native, meshes, "pipe_small", precision="fp32", **ORACLE_CASES["sa_pcg"])
+    S64, S32 = native.Solver(P64), native.Solver(P32)
+    for _ in range(10):
+        a, b = S64.step(), S32.step()
+        assert abs(a.rel_cont - b.rel_cont) <= 1e-3 * abs(a.rel_cont)
+    for x, y in zip(S64.fields(), S32.fields()):
+        assert rel_l2(y, x) <= 1e-4
+
+
+def _golden_cases():
+    return sorted(p.stem[4:] for p in GOLDEN.glob("run_*.npz"))
+
+
+def _options_from_cmd(cmd: str):
+    """Translate the reference command line stored with a fixture into options."""
+    toks = cmd.split()
+    kv = dict(zip(toks[0::2], toks[1::2]))
+    o = {}
+    num = {"--re": "re", "--alpha-u": "alpha_u", "--alpha-p": "alpha_p", "--p-rtol": "p_rtol", "--p-max": "p_max",
+           "--amg-terminal": "amg_terminal", "--max-outer": "max_outer", "--simple-tol": "simple_tol",
+           "--cf-pmax": "cf_pmax"}
+    enum = {"--amg-hierarchy": "amg_hierarchy", "--amg-smoother": "amg_smoother", "--pressure-solver": "pressure_solver",
+            "--cf-interp": "cf_interp", "--run-mode": "run_mode", "--momentum-work": "momentum_work"}
+    for k, v in kv.items():
+        if k in num:
+            o[num[k]] = int(v) if num[k] in ("p_max", "amg_terminal", "max_outer", "cf_pmax") else float(v)
+        elif k in enum:
+            o[enum[k]] = v
+    return o
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", _golden_cases())
+def test_gpu_matches_reference_fixture(native, meshes, case):
+    g = np.load(GOLDEN / f"run_{case}.npz")
+    mesh = {"tiny": "pipe_tiny", "small": "pipe_small", "m40k": "pipe40k"}[case.split("_")[0]]
+    opts = _options_from_cmd(str(g["cmd"]))
+    if case.endswith("fp32"):
+        opts["precision"] = "fp32"
+    P = _make(native, meshes, mesh, **opts)
+    S = native.Solver(P)
+    its = {int(i): k for k, i in enumerate(g["it"])}
+    fp32 = opts.get("precision") == "fp32"
+    tol = 2e-3 if fp32 else 1e-8
+    last = None
+    for it in range(1, int(g["it"].max()) + 1):
+        r = S.step()
+        if it in its:
+            k = its[it]
+            assert abs(r.rel_cont - g["rel_cont"][k]) <= tol * abs(g["rel_cont"][k]) + 1e-12, (it, r.rel_cont, g["rel_cont"][k])
+            if not fp32:
+                assert r.p_its == int(g["p_its"][k]), (it, r.p_its, int(g["p_its"][k]))
+        last = r
+    u0, u1, u2, p = S.fields()
+    uc = np.zeros((P.counts()["nc"], 3))
+    native.cell_average_velocity(P, u0, u1, u2, uc)
+    ftol = 1e-3 if fp32 else 1e-8
+    assert rel_l2(p, g["p"]) <= ftol
+    assert rel_l2(uc, g["u_cell"]) <= ftol
+    assert last is not None
