@@ -159,6 +159,18 @@ int nds_get_fields(nds_solver* s, double* u0, double* u1, double* u2, double* p)
 int nds_set_fields(nds_solver* s, const double* u0, const double* u1, const double* u2, const double* p);
 void nds_solver_destroy(nds_solver* s);
 
+/* ---- kernel timing by category with CUDA events on the solver's stream
+ *      (replaces the reference's H0Profiler, h8_main_base.cu:58-99) -------- */
+typedef struct nds_profile_entry {
+  char name[32];
+  long long calls;
+  double total_ms;
+} nds_profile_entry;
+int nds_profile_enable(nds_solver* s, int on);   /* resets the counters */
+int nds_profile_read(nds_solver* s, nds_profile_entry* out, int max_entries, int* n_out);
+/* number of kernels this library has launched in this process */
+unsigned long long nds_launch_count(void);
+
 #ifdef __cplusplus
 }
 #endif

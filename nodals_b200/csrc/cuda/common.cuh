@@ -18,7 +18,10 @@ inline void cuda_check(cudaError_t e, const char* what, const char* file, int li
                     cudaGetErrorString(e));
 }
 #define NDS_CUDA(call) ::nds::cuda_check((call), #call, __FILE__, __LINE__)
-#define NDS_LAUNCH() ::nds::cuda_check(cudaGetLastError(), "kernel launch", __FILE__, __LINE__)
+// every kernel launch of the library goes through NDS_LAUNCH, which also
+// counts launches (nds_launch_count)
+extern unsigned long long g_launches;
+#define NDS_LAUNCH() (++::nds::g_launches, ::nds::cuda_check(cudaGetLastError(), "kernel launch", __FILE__, __LINE__))
 
 constexpr int kBlock = 256;
 constexpr int kWarps = kBlock / 32;

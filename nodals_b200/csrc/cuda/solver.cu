@@ -17,6 +17,7 @@
 #include <cstring>
 #include <memory>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../capi_internal.hpp"
@@ -25,6 +26,8 @@
 #include "kernels.cuh"
 
 namespace nds {
+
+unsigned long long g_launches = 0;
 
 template <class T>
 struct DBuf {
@@ -70,6 +73,62 @@ struct DBuf {
   size_t bytes() const { return n * sizeof(T); }
 };
 
+// Optional per-category CUDA-event timing of kernel launches on the solver's
+// stream (the analogue of the reference's H0Profiler, h8_main_base.cu:58-99).
+enum ProfCat { P_FINE_SPMV = 0, P_COARSE_SPMV, P_REFRESH, P_ASSEMBLE, P_GS, P_CONTINUITY, P_TRANSFER, P_TERMINAL,
+               P_VECTOR, P_NCAT };
+static const char* const kProfNames[P_NCAT] = {"fine_spmv", "coarse_spmv", "fine_refresh", "mom_assemble", "mom_gs",
+                                               "continuity", "transfer", "terminal_dense", "vector_reduce"};
+struct Profiler {
+  bool on = false;
+  std::vector<cudaEvent_t> ev;
+  std::vector<int> cat;
+  int used = 0;
+  double total[P_NCAT] = {};
+  long long calls[P_NCAT] = {};
+  ~Profiler() {
+    for (auto e : ev) cudaEventDestroy(e);
+  }
+  int begin(cudaStream_t s, int c) {
+    if (!on) return -1;
+    if (2 * (size_t)used + 2 > ev.size()) {
+      const size_t n = ev.size();
+      ev.resize(n + 512);
+      cat.resize(ev.size() / 2);
+      for (size_t i = n; i < ev.size(); ++i) NDS_CUDA(cudaEventCreate(&ev[i]));
+    }
+    const int id = used++;
+    cat[(size_t)id] = c;
+    NDS_CUDA(cudaEventRecord(ev[2 * (size_t)id], s));
+    return id;
+  }
+  void end(cudaStream_t s, int id) {
+    if (id >= 0) NDS_CUDA(cudaEventRecord(ev[2 * (size_t)id + 1], s));
+  }
+  void collect() {
+    if (!used) return;
+    NDS_CUDA(cudaEventSynchronize(ev[2 * (size_t)used - 1]));
+    for (int i = 0; i < used; ++i) {
+      float ms = 0;
+      NDS_CUDA(cudaEventElapsedTime(&ms, ev[2 * (size_t)i], ev[2 * (size_t)i + 1]));
+      total[cat[(size_t)i]] += ms;
+      ++calls[cat[(size_t)i]];
+    }
+    used = 0;
+  }
+  void reset() {
+    used = 0;
+    for (int c = 0; c < P_NCAT; ++c) { total[c] = 0; calls[c] = 0; }
+  }
+};
+struct ProfScope {
+  Profiler& p;
+  cudaStream_t s;
+  int id;
+  ProfScope(Profiler& pp, cudaStream_t ss, int c) : p(pp), s(ss), id(pp.begin(ss, c)) {}
+  ~ProfScope() { p.end(s, id); }
+};
+
 struct ISolver {
   virtual ~ISolver() = default;
   virtual void reset() = 0;
@@ -77,6 +136,7 @@ struct ISolver {
   virtual void solve(nds_solve_report* rep) = 0;
   virtual void get_fields(double* u0, double* u1, double* u2, double* p) = 0;
   virtual void set_fields(const double* u0, const double* u1, const double* u2, const double* p) = 0;
+  Profiler prof;
 };
 
 struct SolveFailure : std::runtime_error {
@@ -358,16 +418,20 @@ class Solver final : public ISolver {
     reduce_to<1>(g, slot);
   }
 
+  int spcat(const int32_t* rp) const { return rp == frow_.p ? P_FINE_SPMV : P_COARSE_SPMV; }
   void spmv(int n, const int32_t* rp, const int32_t* ci, const T* v, const T* x, T* y) {
+    ProfScope ps(prof, st_, spcat(rp));
     k::spmv<T><<<grid_for((long long)n * 32), kBlock, 0, st_>>>(n, rp, ci, v, x, y);
     NDS_LAUNCH();
   }
   void resid(int n, const int32_t* rp, const int32_t* ci, const T* v, const T* x, const T* b, T* r, T* r2 = nullptr) {
+    ProfScope ps(prof, st_, spcat(rp));
     k::spmv_resid<T><<<grid_for((long long)n * 32), kBlock, 0, st_>>>(n, rp, ci, v, x, b, r, r2);
     NDS_LAUNCH();
   }
   void smooth_step(int n, const int32_t* rp, const int32_t* ci, const T* v, const T* xin, const T* b, const T* den,
                    double w, T* xout) {
+    ProfScope ps(prof, st_, spcat(rp));
     k::spmv_smooth<T><<<grid_for((long long)n * 32), kBlock, 0, st_>>>(n, rp, ci, v, xin, b, den, T(w), xout);
     NDS_LAUNCH();
   }
@@ -382,6 +446,7 @@ class Solver final : public ISolver {
 
   // fine Schur operator
   void refresh_fine(const T* rau) {
+    ProfScope ps(prof, st_, P_REFRESH);
     k::fine_refresh<T><<<grid_for((long long)nc_ * 32), kBlock, 0, st_>>>(
         nc_, frow_.p, fcoff_.p, fcnt_.p, fcpk_.p, fca_.p, ref_.p, bco_.p, rau, fdpos_.p, fval_.p, fdiag_.p, fl1_.p);
     NDS_LAUNCH();
@@ -459,10 +524,12 @@ class Solver final : public ISolver {
                 o_.amg_jacobi_coarse_sweeps);
   }
   void restrict_to(const Xfer& X, const T* f, T* c) {
+    ProfScope ps(prof, st_, P_TRANSFER);
     k::restrict_gather<T><<<grid_for(X.nc), kBlock, 0, st_>>>(X.nc, X.rrow.p, X.rcol.p, X.rval.p, f, c);
     NDS_LAUNCH();
   }
   void prolong(const Xfer& X, const T* c, T* f) {
+    ProfScope ps(prof, st_, P_TRANSFER);
     k::prolong_add<T><<<grid_for(X.nf), kBlock, 0, st_>>>(X.nf, X.prow.p, X.pcol.p, X.pval.p, c, f);
     NDS_LAUNCH();
   }
@@ -471,6 +538,7 @@ class Solver final : public ISolver {
   void vcycle(int l, const T* b, T* x) {
     Level& A = L_[(size_t)l];
     if (l == (int)L_.size() - 1) {
+      ProfScope ps(prof, st_, P_TERMINAL);
       k::dense_mv<T><<<grid_for((long long)A.n * 32), kBlock, 0, st_>>>(A.n, tinv_.p, b, x);
       NDS_LAUNCH();
       return;
@@ -609,6 +677,7 @@ class Solver final : public ISolver {
     for (int kk = 0; kk < o_.p_max; ++kk) {
       // q = A p, pq = p.q ; alpha = rho/pq ; x += a p, r -= a q, rn2
       int g = red_grid((long long)nc_ * 32);
+      ProfScope ps(prof, st_, P_FINE_SPMV);
       k::spmv_dot<T><<<g, kBlock, 0, st_>>>(nc_, frow_.p, fcol_.p, fval_.p, pp_.p, q_.p, part_.p);
       NDS_LAUNCH();
       reduce_to<1>(g, S_PQ);
@@ -709,6 +778,7 @@ class Solver final : public ISolver {
     a.b0 = b_[0].p;
     a.b1 = b_[1].p;
     a.b2 = b_[2].p;
+    ProfScope ps(prof, st_, P_ASSEMBLE);
     k::mom_assemble<T><<<grid_for(nv_, kBlock / 8), kBlock, mom_smem_, st_>>>(a);
     NDS_LAUNCH();
   }
@@ -718,6 +788,7 @@ class Solver final : public ISolver {
       const int c = reverse ? ncol - 1 - qq : qq;
       const int s = color_off_[(size_t)c], n = color_off_[(size_t)c + 1] - s;
       if (!n) continue;
+      ProfScope ps(prof, st_, P_GS);
       k::mom_gs_color<T><<<grid_for((long long)n * 8), kBlock, 0, st_>>>(n, color_rows_.p + s, mrow_.p, mcol_.p, A_.p,
                                                                        diag_.p, b_[0].p, b_[1].p, b_[2].p, u_[0].p,
                                                                        u_[1].p, u_[2].p, T(o_.mom_omega));
@@ -787,6 +858,7 @@ class Solver final : public ISolver {
     NDS_CUDA(cudaEventRecord(ev_[2], st_));
     {
       const int g = red_grid(nc_);
+      ProfScope ps(prof, st_, P_CONTINUITY);
       k::continuity<T><<<g, kBlock, 0, st_>>>(nc_, ref_.p, bco_.p, fixed_div_.p, u_[0].p, u_[1].p, u_[2].p, rhs_.p,
                                              part_.p);
       NDS_LAUNCH();
@@ -813,6 +885,7 @@ class Solver final : public ISolver {
     vaxpy(nc_, o_.alpha_p, x_.p, p_.p);
     NDS_CUDA(cudaEventRecord(ev_[5], st_));
     NDS_CUDA(cudaEventSynchronize(ev_[5]));
+    prof.collect();
     float ms[5];
     for (int q = 0; q < 5; ++q) NDS_CUDA(cudaEventElapsedTime(&ms[q], ev_[q], ev_[q + 1]));
     R.ms_assembly = ms[0];
@@ -871,6 +944,11 @@ class Solver final : public ISolver {
     std::vector<T> h;
     auto get = [&](const DBuf<T>& b, double* out) {
       if (!out) return;
+      if (std::is_same<T, double>::value) {  // straight DMA into the caller's buffer
+        NDS_CUDA(cudaMemcpyAsync(out, b.p, b.bytes(), cudaMemcpyDeviceToHost, st_));
+        NDS_CUDA(cudaStreamSynchronize(st_));
+        return;
+      }
       h.resize(b.n);
       NDS_CUDA(cudaMemcpyAsync(h.data(), b.p, b.bytes(), cudaMemcpyDeviceToHost, st_));
       NDS_CUDA(cudaStreamSynchronize(st_));
@@ -884,6 +962,11 @@ class Solver final : public ISolver {
   void set_fields(const double* u0, const double* u1, const double* u2, const double* p) override {
     auto put = [&](DBuf<T>& b, const double* in) {
       if (!in) return;
+      if (std::is_same<T, double>::value) {
+        NDS_CUDA(cudaMemcpyAsync(b.p, in, b.bytes(), cudaMemcpyHostToDevice, st_));
+        NDS_CUDA(cudaStreamSynchronize(st_));
+        return;
+      }
       std::vector<T> h(in, in + b.n);
       NDS_CUDA(cudaMemcpyAsync(b.p, h.data(), b.bytes(), cudaMemcpyHostToDevice, st_));
       NDS_CUDA(cudaStreamSynchronize(st_));
@@ -991,5 +1074,30 @@ int nds_set_fields(nds_solver* s, const double* u0, const double* u1, const doub
   return guarded([&] { s->impl->set_fields(u0, u1, u2, p); });
 }
 void nds_solver_destroy(nds_solver* s) { delete s; }
+
+unsigned long long nds_launch_count(void) { return nds::g_launches; }
+
+int nds_profile_enable(nds_solver* s, int on) {
+  if (!s) return fail(NDS_E_INVALID, "null solver");
+  return guarded([&] {
+    s->impl->prof.collect();
+    s->impl->prof.reset();
+    s->impl->prof.on = on != 0;
+  });
+}
+int nds_profile_read(nds_solver* s, nds_profile_entry* out, int max_entries, int* n_out) {
+  if (!s || !out || !n_out) return fail(NDS_E_INVALID, "null argument");
+  return guarded([&] {
+    auto& P = s->impl->prof;
+    P.collect();
+    int n = 0;
+    for (int c = 0; c < nds::P_NCAT && n < max_entries; ++c, ++n) {
+      std::snprintf(out[n].name, sizeof(out[n].name), "%s", nds::kProfNames[c]);
+      out[n].calls = P.calls[c];
+      out[n].total_ms = P.total[c];
+    }
+    *n_out = n;
+  });
+}
 
 }  // extern "C"

@@ -14,33 +14,6 @@ namespace {
 
 using Entry = std::pair<int, double>;
 
-// rows of (col -> value) accumulated in a fixed order, then packed sorted;
-// exact zeros are dropped like the reference packer (g5_sa_host.hpp:504-521)
-CsrHost pack_rows(std::vector<std::unordered_map<int, double>>& rows) {
-  CsrHost A;
-  A.n = (int)rows.size();
-  A.row.assign((size_t)A.n + 1, 0);
-  A.diag.assign((size_t)A.n, 0.0);
-  std::vector<Entry> tmp;
-  for (int i = 0; i < A.n; ++i) {
-    tmp.clear();
-    for (const auto& kv : rows[(size_t)i])
-      if (kv.second != 0.0) tmp.push_back(kv);
-    std::sort(tmp.begin(), tmp.end(), [](const Entry& a, const Entry& b) { return a.first < b.first; });
-    for (const auto& e : tmp) {
-      A.col.push_back(e.first);
-      A.val.push_back(e.second);
-      if (e.first == i) A.diag[(size_t)i] = e.second;
-    }
-    A.row[(size_t)i + 1] = (int64_t)A.col.size();
-    std::unordered_map<int, double>().swap(rows[(size_t)i]);
-  }
-  for (int i = 0; i < A.n; ++i)
-    if (!(A.diag[(size_t)i] > 0.0) || !std::isfinite(A.diag[(size_t)i]))
-      throw std::runtime_error("coarse AMG matrix has a non-positive diagonal");
-  return A;
-}
-
 // SA transfer row: merge duplicates, keep own + largest |w|, normalise to sum 1
 void normalize_prune(std::vector<Entry>& row, int own, int max_nnz) {
   if (row.empty()) row.push_back({own, 1.0});
@@ -84,6 +57,7 @@ void normalize_prune(std::vector<Entry>& row, int own, int max_nnz) {
 
 void csr_apply(const CsrHost& A, const std::vector<double>& x, std::vector<double>& y) {
   y.assign((size_t)A.n, 0.0);
+#pragma omp parallel for schedule(static)
   for (int i = 0; i < A.n; ++i) {
     double s = 0.0;
     for (int64_t k = A.row[(size_t)i]; k < A.row[(size_t)i + 1]; ++k) s += A.val[(size_t)k] * x[(size_t)A.col[(size_t)k]];
@@ -110,6 +84,7 @@ double power_generic(int n, const std::vector<double>& diag, int its, double saf
   for (auto& q : v) q /= vn;
   double ray = 0.0;
   for (int it = 0; it < its; ++it) {
+#pragma omp parallel for schedule(static)
     for (int i = 0; i < n; ++i) u[(size_t)i] = v[(size_t)i] / std::sqrt(diag[(size_t)i]);
     apply(u, au);
     long double num = 0, den = 0, nw = 0;
@@ -128,34 +103,35 @@ double power_generic(int n, const std::vector<double>& diag, int its, double saf
   return safety * ray;
 }
 
-// matrix-free fine Schur action y = B diag(rau) B^T x in cell order
+// matrix-free fine Schur action y = B diag(rau) B^T x; B^T x gathered per
+// velocity dof over its incident cells in ascending cell order (the order of
+// the reference's cell-major scatter)
 struct FineApply {
   const Setup& S;
   const std::vector<double>& rau;
   std::vector<double> v0, v1, v2;
   FineApply(const Setup& s, const std::vector<double>& r) : S(s), rau(r), v0((size_t)s.nv), v1((size_t)s.nv), v2((size_t)s.nv) {}
   void operator()(const std::vector<double>& x, std::vector<double>& y) {
-    std::fill(v0.begin(), v0.end(), 0.0);
-    std::fill(v1.begin(), v1.end(), 0.0);
-    std::fill(v2.begin(), v2.end(), 0.0);
-    for (int c = 0; c < S.nc; ++c) {
-      const double p = x[(size_t)c];
-      for (int a = 0; a < 8; ++a) {
-        const int g = S.ref[8 * (size_t)c + a];
-        if (g < 0) continue;
-        const double* b = &S.bco[24 * (size_t)c + 3 * a];
-        v0[(size_t)g] += b[0] * p;
-        v1[(size_t)g] += b[1] * p;
-        v2[(size_t)g] += b[2] * p;
-      }
-    }
+    const FineTopo& F = S.fine;
+#pragma omp parallel for schedule(static)
     for (int g = 0; g < S.nv; ++g) {
+      double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+      for (int k = F.inc_off[(size_t)g]; k < F.inc_off[(size_t)g + 1]; ++k) {
+        const uint32_t pk = F.packed[(size_t)k];
+        const int c = (int)(pk >> 3);
+        const double* b = &S.bco[24 * (size_t)c + 3 * (pk & 7u)];
+        const double p = x[(size_t)c];
+        s0 += b[0] * p;
+        s1 += b[1] * p;
+        s2 += b[2] * p;
+      }
       const double r = rau[(size_t)g];
-      v0[(size_t)g] *= r;
-      v1[(size_t)g] *= r;
-      v2[(size_t)g] *= r;
+      v0[(size_t)g] = s0 * r;
+      v1[(size_t)g] = s1 * r;
+      v2[(size_t)g] = s2 * r;
     }
     y.assign((size_t)S.nc, 0.0);
+#pragma omp parallel for schedule(static)
     for (int c = 0; c < S.nc; ++c) {
       double s = 0.0;
       for (int a = 0; a < 8; ++a) {
@@ -169,39 +145,122 @@ struct FineApply {
   }
 };
 
-// Galerkin P^T A P accumulated per coarse entry in ascending fine-row order
-CsrHost galerkin(const CsrHost& A, const Transfer& P) {
-  if (P.nf != A.n) throw std::runtime_error("Galerkin transfer size mismatch");
-  std::vector<std::unordered_map<int, double>> rows((size_t)P.nc);
-  std::vector<Entry> q;
-  for (int i = 0; i < A.n; ++i) {
-    q.clear();
-    for (int64_t k = A.row[(size_t)i]; k < A.row[(size_t)i + 1]; ++k) {
-      const int j = A.col[(size_t)k];
-      const double a = A.val[(size_t)k];
-      for (int64_t kp = P.row[(size_t)j]; kp < P.row[(size_t)j + 1]; ++kp) q.push_back({P.col[(size_t)kp], a * P.val[(size_t)kp]});
-    }
-    std::sort(q.begin(), q.end(), [](const Entry& a, const Entry& b) { return a.first < b.first; });
-    size_t w = 0;
-    for (size_t k = 0; k < q.size();) {
-      const int c = q[k].first;
-      double v = 0.0;
-      size_t j = k;
-      for (; j < q.size() && q[j].first == c; ++j) v += q[j].second;
-      q[w++] = {c, v};
-      k = j;
-    }
-    q.resize(w);
-    for (int64_t kp = P.row[(size_t)i]; kp < P.row[(size_t)i + 1]; ++kp) {
-      const int I = P.col[(size_t)kp];
-      const double pi = P.val[(size_t)kp];
-      for (const auto& e : q) {
-        const double v = pi * e.second;
-        if (v != 0.0) rows[(size_t)I][e.first] += v;
+// Row-owned accumulation of a sparse matrix: fill(I, add) calls add(J, v) for
+// every non-zero contribution to row I in the order that defines the sum;
+// entries whose final sum is exactly zero are dropped (as the reference
+// packer does, g5_sa_host.hpp:504-521).  Rows are independent -> parallel.
+template <class Fill>
+CsrHost accumulate_rows(int nrows, int ncols, Fill fill) {
+  std::vector<std::vector<int32_t>> cols((size_t)nrows);
+  std::vector<std::vector<double>> vals((size_t)nrows);
+#pragma omp parallel
+  {
+    std::vector<double> acc((size_t)ncols, 0.0);
+    std::vector<char> mark((size_t)ncols, 0);
+    std::vector<int32_t> touched;
+#pragma omp for schedule(dynamic, 32)
+    for (int I = 0; I < nrows; ++I) {
+      touched.clear();
+      fill(I, [&](int J, double v) {
+        if (!mark[(size_t)J]) {
+          mark[(size_t)J] = 1;
+          touched.push_back(J);
+        }
+        acc[(size_t)J] += v;
+      });
+      std::sort(touched.begin(), touched.end());
+      auto& c = cols[(size_t)I];
+      auto& w = vals[(size_t)I];
+      for (int32_t J : touched) {
+        if (acc[(size_t)J] != 0.0) {
+          c.push_back(J);
+          w.push_back(acc[(size_t)J]);
+        }
+        acc[(size_t)J] = 0.0;
+        mark[(size_t)J] = 0;
       }
     }
   }
-  return pack_rows(rows);
+  CsrHost A;
+  A.n = nrows;
+  A.row.assign((size_t)nrows + 1, 0);
+  for (int I = 0; I < nrows; ++I) A.row[(size_t)I + 1] = A.row[(size_t)I] + (int64_t)cols[(size_t)I].size();
+  A.col.resize((size_t)A.row.back());
+  A.val.resize((size_t)A.row.back());
+  A.diag.assign((size_t)nrows, 0.0);
+#pragma omp parallel for schedule(static)
+  for (int I = 0; I < nrows; ++I) {
+    std::copy(cols[(size_t)I].begin(), cols[(size_t)I].end(), A.col.begin() + A.row[(size_t)I]);
+    std::copy(vals[(size_t)I].begin(), vals[(size_t)I].end(), A.val.begin() + A.row[(size_t)I]);
+    for (size_t k = 0; k < cols[(size_t)I].size(); ++k)
+      if (cols[(size_t)I][k] == I) A.diag[(size_t)I] = vals[(size_t)I][k];
+  }
+  for (int i = 0; i < A.n; ++i)
+    if (!(A.diag[(size_t)i] > 0.0) || !std::isfinite(A.diag[(size_t)i]))
+      throw std::runtime_error("coarse AMG matrix has a non-positive diagonal");
+  return A;
+}
+
+// coarse row -> (fine row, weight) incidence of a transfer, ascending fine row
+struct RevTransfer {
+  std::vector<int64_t> off;
+  std::vector<int32_t> fine;
+  std::vector<double> w;
+};
+RevTransfer reverse(const Transfer& P) {
+  RevTransfer R;
+  R.off.assign((size_t)P.nc + 1, 0);
+  for (int32_t c : P.col) ++R.off[(size_t)c + 1];
+  for (int c = 0; c < P.nc; ++c) R.off[(size_t)c + 1] += R.off[(size_t)c];
+  R.fine.resize(P.col.size());
+  R.w.resize(P.col.size());
+  std::vector<int64_t> pos(R.off.begin(), R.off.end() - 1);
+  for (int i = 0; i < P.nf; ++i)
+    for (int64_t k = P.row[(size_t)i]; k < P.row[(size_t)i + 1]; ++k) {
+      const int c = P.col[(size_t)k];
+      R.fine[(size_t)pos[(size_t)c]] = i;
+      R.w[(size_t)pos[(size_t)c]++] = P.val[(size_t)k];
+    }
+  return R;
+}
+
+// Galerkin P^T A P (g5_sa_host.hpp:940-971): q_i = A_i P merged per coarse
+// column, then coarse entry (I,K) = sum over fine rows i (ascending) of
+// P_iI q_i(K) -- the reference's accumulation order.
+CsrHost galerkin(const CsrHost& A, const Transfer& P) {
+  if (P.nf != A.n) throw std::runtime_error("Galerkin transfer size mismatch");
+  std::vector<std::vector<Entry>> q((size_t)A.n);
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int i = 0; i < A.n; ++i) {
+    auto& qi = q[(size_t)i];
+    for (int64_t k = A.row[(size_t)i]; k < A.row[(size_t)i + 1]; ++k) {
+      const int j = A.col[(size_t)k];
+      const double a = A.val[(size_t)k];
+      for (int64_t kp = P.row[(size_t)j]; kp < P.row[(size_t)j + 1]; ++kp) qi.push_back({P.col[(size_t)kp], a * P.val[(size_t)kp]});
+    }
+    std::sort(qi.begin(), qi.end(), [](const Entry& x, const Entry& y) { return x.first < y.first; });
+    size_t w = 0;
+    for (size_t k = 0; k < qi.size();) {
+      const int c = qi[k].first;
+      double v = 0.0;
+      size_t j = k;
+      for (; j < qi.size() && qi[j].first == c; ++j) v += qi[j].second;
+      qi[w++] = {c, v};
+      k = j;
+    }
+    qi.resize(w);
+    qi.shrink_to_fit();
+  }
+  const RevTransfer R = reverse(P);
+  return accumulate_rows(P.nc, P.nc, [&](int I, auto&& add) {
+    for (int64_t z = R.off[(size_t)I]; z < R.off[(size_t)I + 1]; ++z) {
+      const double pi = R.w[(size_t)z];
+      for (const auto& e : q[(size_t)R.fine[(size_t)z]]) {
+        const double v = pi * e.second;
+        if (v != 0.0) add(e.first, v);
+      }
+    }
+  });
 }
 
 // ----------------------------------------------------------------------------
@@ -231,18 +290,34 @@ std::vector<std::vector<int32_t>> csr_graph(const CsrHost& A) {
   return g;
 }
 
-// fine -> first aggregate level, smoothed with damping / lambda
+Transfer pack_transfer(int nf, int nc, std::vector<std::vector<Entry>>& rows) {
+  Transfer P;
+  P.nf = nf;
+  P.nc = nc;
+  P.row.assign((size_t)nf + 1, 0);
+  for (int i = 0; i < nf; ++i) P.row[(size_t)i + 1] = P.row[(size_t)i] + (int64_t)rows[(size_t)i].size();
+  P.col.resize((size_t)P.row.back());
+  P.val.resize((size_t)P.row.back());
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < nf; ++i) {
+    int64_t k = P.row[(size_t)i];
+    for (const auto& e : rows[(size_t)i]) {
+      P.col[(size_t)k] = e.first;
+      P.val[(size_t)k++] = e.second;
+    }
+  }
+  return P;
+}
+
+// fine -> first aggregate level, smoothed with damping / lambda (g5_sa_host.hpp:173-203)
 Transfer sa_fine_transfer(const Setup& S, const std::vector<double>& rau, const std::vector<int32_t>& id, int nagg,
                           const std::vector<double>& diag, double lambda, double damping, int max_nnz) {
   const double omega = damping / lambda;
   const FineTopo& F = S.fine;
-  Transfer P;
-  P.nf = S.nc;
-  P.nc = nagg;
-  P.row.assign((size_t)P.nf + 1, 0);
-  std::vector<Entry> row;
-  for (int i = 0; i < P.nf; ++i) {
-    row.clear();
+  std::vector<std::vector<Entry>> rows((size_t)S.nc);
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int i = 0; i < S.nc; ++i) {
+    auto& row = rows[(size_t)i];
     const int own = id[(size_t)i];
     row.push_back({own, 1.0});
     const double invd = 1.0 / diag[(size_t)i];
@@ -260,26 +335,23 @@ Transfer sa_fine_transfer(const Setup& S, const std::vector<double>& rau, const 
       }
     }
     normalize_prune(row, own, max_nnz);
-    for (const auto& e : row) {
-      P.col.push_back(e.first);
-      P.val.push_back(e.second);
-    }
-    P.row[(size_t)i + 1] = (int64_t)P.col.size();
   }
-  return P;
+  return pack_transfer(S.nc, nagg, rows);
 }
 
-// A1 = P^T B diag(rau) B^T P, per velocity dof in ascending order
+// A1 = P^T B diag(rau) B^T P (g5_sa_host.hpp:525-546): per velocity dof g the
+// merged list q_g of (coarse, P-weighted B row); coarse entry (I,J) sums
+// rau_g q_g(I).q_g(J) over ascending g, the reference's order.
 CsrHost sa_first_coarse(const Setup& S, const std::vector<double>& rau, const Transfer& P) {
   const FineTopo& F = S.fine;
-  std::vector<std::unordered_map<int, double>> rows((size_t)P.nc);
   struct QE {
     int coarse;
     double b[3];
   };
-  std::vector<QE> q;
+  std::vector<std::vector<QE>> qs((size_t)S.nv);
+#pragma omp parallel for schedule(dynamic, 512)
   for (int g = 0; g < S.nv; ++g) {
-    q.clear();
+    auto& q = qs[(size_t)g];
     for (int k = F.inc_off[(size_t)g]; k < F.inc_off[(size_t)g + 1]; ++k) {
       const uint32_t pk = F.packed[(size_t)k];
       const int c = (int)(pk >> 3);
@@ -306,41 +378,53 @@ CsrHost sa_first_coarse(const Setup& S, const std::vector<double>& rau, const Tr
       k = j;
     }
     q.resize(w);
-    const double r = rau[(size_t)g];
-    for (size_t a = 0; a < q.size(); ++a)
-      for (size_t b = a; b < q.size(); ++b) {
-        const double v = r * (q[a].b[0] * q[b].b[0] + q[a].b[1] * q[b].b[1] + q[a].b[2] * q[b].b[2]);
-        if (v == 0.0) continue;
-        rows[(size_t)q[a].coarse][q[b].coarse] += v;
-        if (a != b) rows[(size_t)q[b].coarse][q[a].coarse] += v;
+    q.shrink_to_fit();
+  }
+  // coarse row -> (g, position in q_g), ascending g
+  std::vector<int64_t> off((size_t)P.nc + 1, 0);
+  for (int g = 0; g < S.nv; ++g)
+    for (const auto& e : qs[(size_t)g]) ++off[(size_t)e.coarse + 1];
+  for (int c = 0; c < P.nc; ++c) off[(size_t)c + 1] += off[(size_t)c];
+  std::vector<int32_t> rg((size_t)off.back());
+  std::vector<int32_t> ra((size_t)off.back());
+  {
+    std::vector<int64_t> pos(off.begin(), off.end() - 1);
+    for (int g = 0; g < S.nv; ++g)
+      for (size_t a = 0; a < qs[(size_t)g].size(); ++a) {
+        const int c = qs[(size_t)g][a].coarse;
+        rg[(size_t)pos[(size_t)c]] = g;
+        ra[(size_t)pos[(size_t)c]++] = (int32_t)a;
       }
   }
-  return pack_rows(rows);
+  return accumulate_rows(P.nc, P.nc, [&](int I, auto&& add) {
+    for (int64_t z = off[(size_t)I]; z < off[(size_t)I + 1]; ++z) {
+      const int g = rg[(size_t)z];
+      const auto& q = qs[(size_t)g];
+      const QE& qa = q[(size_t)ra[(size_t)z]];
+      const double r = rau[(size_t)g];
+      for (const auto& qb : q) {
+        const double v = r * (qa.b[0] * qb.b[0] + qa.b[1] * qb.b[1] + qa.b[2] * qb.b[2]);
+        if (v != 0.0) add(qb.coarse, v);
+      }
+    }
+  });
 }
 
 Transfer sa_explicit_transfer(const CsrHost& A, const std::vector<int32_t>& id, int nagg, double lambda, double damping,
                               int max_nnz) {
   const double omega = damping / lambda;
-  Transfer P;
-  P.nf = A.n;
-  P.nc = nagg;
-  P.row.assign((size_t)A.n + 1, 0);
-  std::vector<Entry> row;
+  std::vector<std::vector<Entry>> rows((size_t)A.n);
+#pragma omp parallel for schedule(dynamic, 256)
   for (int i = 0; i < A.n; ++i) {
-    row.clear();
+    auto& row = rows[(size_t)i];
     const int own = id[(size_t)i];
     row.push_back({own, 1.0});
     const double invd = 1.0 / A.diag[(size_t)i];
     for (int64_t k = A.row[(size_t)i]; k < A.row[(size_t)i + 1]; ++k)
       row.push_back({id[(size_t)A.col[(size_t)k]], -omega * invd * A.val[(size_t)k]});
     normalize_prune(row, own, max_nnz);
-    for (const auto& e : row) {
-      P.col.push_back(e.first);
-      P.val.push_back(e.second);
-    }
-    P.row[(size_t)i + 1] = (int64_t)P.col.size();
   }
-  return P;
+  return pack_transfer(A.n, nagg, rows);
 }
 
 // ----------------------------------------------------------------------------
@@ -369,17 +453,17 @@ double csr_entry(const CsrHost& A, int i, int j) {
 Split pmis_split(const CsrHost& A, double theta) {
   Split R;
   R.n = A.n;
-  std::vector<double> maxneg((size_t)A.n, 0.0);
-  for (int i = 0; i < A.n; ++i)
+  R.strong.resize((size_t)A.n);
+  R.graph.resize((size_t)A.n);
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int i = 0; i < A.n; ++i) {
+    double maxneg = 0.0;
     for (int64_t k = A.row[(size_t)i]; k < A.row[(size_t)i + 1]; ++k) {
       const int j = A.col[(size_t)k];
       const double a = A.val[(size_t)k];
-      if (j != i && a < 0.0) maxneg[(size_t)i] = std::max(maxneg[(size_t)i], -a);
+      if (j != i && a < 0.0) maxneg = std::max(maxneg, -a);
     }
-  R.strong.resize((size_t)A.n);
-  R.graph.resize((size_t)A.n);
-  for (int i = 0; i < A.n; ++i) {
-    const double thr = theta * maxneg[(size_t)i];
+    const double thr = theta * maxneg;
     auto& s = R.strong[(size_t)i];
     if (thr > 0.0)
       for (int64_t k = A.row[(size_t)i]; k < A.row[(size_t)i + 1]; ++k) {
@@ -389,12 +473,16 @@ Split pmis_split(const CsrHost& A, double theta) {
       }
     std::sort(s.begin(), s.end());
     s.erase(std::unique(s.begin(), s.end()), s.end());
-    for (int j : s) {
+  }
+  for (int i = 0; i < A.n; ++i) {
+    for (int j : R.strong[(size_t)i]) {
       R.graph[(size_t)i].push_back(j);
       R.graph[(size_t)j].push_back(i);
     }
   }
-  for (auto& g : R.graph) {
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int i = 0; i < A.n; ++i) {
+    auto& g = R.graph[(size_t)i];
     std::sort(g.begin(), g.end());
     g.erase(std::unique(g.begin(), g.end()), g.end());
   }
@@ -435,25 +523,27 @@ Split pmis_split(const CsrHost& A, double theta) {
 Transfer cf_transfer(const CsrHost& A, const Split& S, int pmax, const std::string& interp) {
   if (interp != "direct" && interp != "exti") throw std::runtime_error("CF interpolation must be direct or exti");
   const bool ext = interp == "exti";
-  Transfer P;
-  P.nf = A.n;
-  P.nc = S.nC;
-  P.row.assign((size_t)A.n + 1, 0);
-  std::vector<Entry> cand;
-  // accumulator keyed by coarse id, remembering first-insertion order
-  std::unordered_map<int, double> acc;
-  for (int i = 0; i < A.n; ++i) {
-    cand.clear();
-    if (S.state[(size_t)i] == 1) {
-      cand.push_back({S.cid[(size_t)i], 1.0});
-    } else {
+  std::vector<std::vector<Entry>> rows((size_t)A.n);
+  bool bad_target = false, bad_sum = false;
+#pragma omp parallel
+  {
+    std::unordered_map<int, double> acc;
+#pragma omp for schedule(dynamic, 256)
+    for (int i = 0; i < A.n; ++i) {
+      auto& cand = rows[(size_t)i];
+      if (S.state[(size_t)i] == 1) {
+        cand.push_back({S.cid[(size_t)i], 1.0});
+        continue;
+      }
       acc.clear();
+      // direct strong C neighbours, weight |a_ij|
       for (int j : S.strong[(size_t)i]) {
         if (S.state[(size_t)j] != 1) continue;
         const double a = csr_entry(A, i, j);
         const double w = a < 0.0 ? -a : std::abs(a);
         if (w > 0.0) acc[S.cid[(size_t)j]] += w;
       }
+      // extended+i: i -> strong F k -> strong C j, |a_ik| split by k's negative couplings
       if (ext) {
         for (int k : S.strong[(size_t)i]) {
           if (S.state[(size_t)k] != 2) continue;
@@ -474,6 +564,7 @@ Transfer cf_transfer(const CsrHost& A, const Split& S, int pmax, const std::stri
           }
         }
       }
+      // fallback: C neighbours in the symmetric strength graph
       if (acc.empty()) {
         for (int j : S.graph[(size_t)i]) {
           if (S.state[(size_t)j] != 1) continue;
@@ -481,28 +572,33 @@ Transfer cf_transfer(const CsrHost& A, const Split& S, int pmax, const std::stri
           if (w > 0.0) acc[S.cid[(size_t)j]] += w;
         }
       }
-      if (acc.empty()) throw std::runtime_error("CF interpolation row has no C target");
       for (const auto& kv : acc)
         if (kv.second > 0.0) cand.push_back(kv);
-      if (cand.empty()) throw std::runtime_error("CF interpolation empty candidates");
-      std::sort(cand.begin(), cand.end(), [](const Entry& a, const Entry& b) {
-        if (a.second != b.second) return a.second > b.second;
-        return a.first < b.first;
+      if (cand.empty()) {
+#pragma omp atomic write
+        bad_target = true;
+        continue;
+      }
+      // keep the pmax largest weights (ties: lower coarse id), normalise to sum 1
+      std::sort(cand.begin(), cand.end(), [](const Entry& x, const Entry& y) {
+        if (x.second != y.second) return x.second > y.second;
+        return x.first < y.first;
       });
       if (pmax > 0 && (int)cand.size() > pmax) cand.resize((size_t)pmax);
       double sum = 0.0;
       for (const auto& e : cand) sum += e.second;
-      if (!(sum > 0.0) || !std::isfinite(sum)) throw std::runtime_error("CF interpolation invalid weight sum");
+      if (!(sum > 0.0) || !std::isfinite(sum)) {
+#pragma omp atomic write
+        bad_sum = true;
+        continue;
+      }
       for (auto& e : cand) e.second /= sum;
-      std::sort(cand.begin(), cand.end(), [](const Entry& a, const Entry& b) { return a.first < b.first; });
+      std::sort(cand.begin(), cand.end(), [](const Entry& x, const Entry& y) { return x.first < y.first; });
     }
-    for (const auto& e : cand) {
-      P.col.push_back(e.first);
-      P.val.push_back(e.second);
-    }
-    P.row[(size_t)i + 1] = (int64_t)P.col.size();
   }
-  return P;
+  if (bad_target) throw std::runtime_error("CF interpolation row has no C target");
+  if (bad_sum) throw std::runtime_error("CF interpolation invalid weight sum");
+  return pack_transfer(A.n, S.nC, rows);
 }
 
 // exact product P01 * P12 (no pruning)
@@ -649,11 +745,13 @@ std::vector<double> dense_inverse_cholesky(const CsrHost& A) {
 }
 
 Hierarchy build_hierarchy(const Mesh& m, const Setup& S, const std::vector<double>& rau, const AmgOptions& o) {
+  StageTimer tm("amg");
   Hierarchy H;
   if (o.hierarchy == "sa") {
     int na = 0;
     auto id0 = aggregate_graph(face_graph(m), o.agg_target, o.agg_min, o.agg_softmax, &na);
     H.agg.push_back(id0);
+    tm.mark("aggregate0");
     // fine diagonal of B diag(rau) B^T
     H.fine_diag.assign((size_t)S.nc, 0.0);
     for (int c = 0; c < S.nc; ++c) {
@@ -671,8 +769,11 @@ Hierarchy build_hierarchy(const Mesh& m, const Setup& S, const std::vector<doubl
     FineApply fa(S, rau);
     H.fine_lambda = power_generic(S.nc, H.fine_diag, o.power_its, o.lambda_safety,
                                   [&](const std::vector<double>& x, std::vector<double>& y) { fa(x, y); });
+    tm.mark("fine_power");
     H.P.push_back(sa_fine_transfer(S, rau, id0, na, H.fine_diag, H.fine_lambda, o.sa_damping, o.interp_max_nnz));
+    tm.mark("P0");
     H.A.push_back(sa_first_coarse(S, rau, H.P[0]));
+    tm.mark("A1");
     while (H.A.back().n > o.terminal) {
       const CsrHost& A = H.A.back();
       const double lam = power_csr(A, o.power_its, o.lambda_safety);
@@ -684,11 +785,13 @@ Hierarchy build_hierarchy(const Mesh& m, const Setup& S, const std::vector<doubl
       H.P.push_back(sa_explicit_transfer(A, id, nb, lam, o.sa_damping, o.interp_max_nnz));
       CsrHost C = galerkin(A, H.P.back());
       H.A.push_back(std::move(C));
+      tm.mark("level");
     }
     if (H.level_lambda.size() < H.A.size()) H.level_lambda.resize(H.A.size(), 0.0);
   } else if (o.hierarchy == "cf") {
     CsrHost A = host_fine_csr(S, rau);
     H.fine_diag = A.diag;
+    tm.mark("fine_csr");
     H.fine_lambda = o.power_its > 0 ? power_csr(A, o.power_its, o.lambda_safety) : 1.0;
     int logical = 0;
     if (o.cf_aggressive_first && A.n > o.terminal) {
@@ -714,8 +817,11 @@ Hierarchy build_hierarchy(const Mesh& m, const Setup& S, const std::vector<doubl
     }
     while (H.A.empty() || H.A.back().n > o.terminal) {
       Split s = pmis_split(A, o.cf_theta);
+      tm.mark("pmis");
       H.P.push_back(cf_transfer(A, s, o.cf_pmax, o.cf_interp));
+      tm.mark("interpolation");
       H.A.push_back(galerkin(A, H.P.back()));
+      tm.mark("galerkin");
       if (H.A.back().n <= o.terminal) break;
       const size_t idx = H.A.size() - 1;
       if (H.level_lambda.size() < H.A.size()) H.level_lambda.resize(H.A.size(), 0.0);
@@ -729,6 +835,7 @@ Hierarchy build_hierarchy(const Mesh& m, const Setup& S, const std::vector<doubl
   }
   H.terminal_n = H.A.back().n;
   H.terminal_inv = dense_inverse_cholesky(H.A.back());
+  tm.mark("terminal_inverse");
   return H;
 }
 

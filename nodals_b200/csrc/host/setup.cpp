@@ -2,7 +2,10 @@
 
 #include <algorithm>
 #include <cmath>
+#include <chrono>
 #include <cstdio>
+#include <cstdlib>
+#include <cstring>
 #include <limits>
 #include <stdexcept>
 #include <string>
@@ -120,6 +123,22 @@ int hw_threads(int req) {
 #endif
 }
 
+}  // namespace
+
+StageTimer::StageTimer(const char* scope) : scope_(scope), t0_(std::chrono::steady_clock::now()), last_(t0_) {
+  const char* e = std::getenv("NDS_SETUP_TIMING");
+  on_ = e && *e && std::strcmp(e, "0") != 0;
+}
+void StageTimer::mark(const char* stage) {
+  const auto t = std::chrono::steady_clock::now();
+  if (on_)
+    std::fprintf(stderr, "NDS_SETUP_STAGE scope=%s stage=%s seconds=%.6f total=%.6f\n", scope_, stage,
+                 std::chrono::duration<double>(t - last_).count(), std::chrono::duration<double>(t - t0_).count());
+  last_ = t;
+}
+
+namespace {
+
 // Exceptions cannot leave an OpenMP region: record the first message and
 // rethrow after the region ends.
 struct OmpError {
@@ -147,6 +166,7 @@ double bcoeff(double det, const double* invJ, int a, int d) {
 }
 
 Setup build_setup(const Mesh& m, const SetupOptions& o) {
+  StageTimer tm("setup");
   Setup S;
   const int nth = hw_threads(o.threads);
   (void)nth;
@@ -205,6 +225,7 @@ Setup build_setup(const Mesh& m, const SetupOptions& o) {
     }
   }
 
+  tm.mark("numbering");
   // --- cell refs, geometry
   S.ref.assign(8 * (size_t)nc, 0);
   S.det.assign((size_t)nc, 0);
@@ -262,6 +283,7 @@ Setup build_setup(const Mesh& m, const SetupOptions& o) {
       }
   }
 
+  tm.mark("geometry+incidence");
   // --- momentum topology: sorted unique free neighbours of every row
   S.mom.n = nv;
   S.mom.row.assign((size_t)nv + 1, 0);
@@ -346,6 +368,7 @@ Setup build_setup(const Mesh& m, const SetupOptions& o) {
     S.mom.diag[(size_t)r] = d;
   }
 
+  tm.mark("momentum_csr");
   // --- greedy colouring in row order: lowest colour unused by lower neighbours
   S.color.assign((size_t)nv, -1);
   {
@@ -379,6 +402,7 @@ Setup build_setup(const Mesh& m, const SetupOptions& o) {
       }
   }
 
+  tm.mark("colouring");
   // --- static Dirichlet diffusion RHS (cell order)
   for (auto& r : S.static_rhs) r.assign((size_t)nv, 0.0);
   for (int c = 0; c < nc; ++c) {
@@ -425,17 +449,7 @@ Setup build_setup(const Mesh& m, const SetupOptions& o) {
     S.fixed_div[(size_t)c] = q;
   }
 
-  // --- initial rAU: assemble at U = 0 (Dirichlet values still convect) and relax
-  {
-    std::array<std::vector<double>, 3> U0, conv;
-    for (auto& u : U0) u.assign((size_t)nv, 0.0);
-    std::vector<double> a;
-    host_assemble_central(S, U0, a, conv);
-    S.init_rau = host_finalize_relax(S, a, o.alpha_u, &S.init_delta);
-    if (o.rau_scale != 1.0)
-      for (double& q : S.init_rau) q *= o.rau_scale;
-  }
-
+  tm.mark("rhs+bcoeff");
   // --- fine Schur topology (velocity incidence, sorted unique pressure columns)
   {
     FineTopo& F = S.fine;
@@ -514,35 +528,53 @@ Setup build_setup(const Mesh& m, const SetupOptions& o) {
     oerr.rethrow();
     F.row_max = rmax;
   }
+  tm.mark("fine_topology");
+  // --- initial rAU: assemble at U = 0 (Dirichlet values still convect) and relax
+  {
+    std::array<std::vector<double>, 3> U0, conv;
+    for (auto& u : U0) u.assign((size_t)nv, 0.0);
+    std::vector<double> a;
+    host_assemble_central(S, U0, a, conv);
+    S.init_rau = host_finalize_relax(S, a, o.alpha_u, &S.init_delta);
+    if (o.rau_scale != 1.0)
+      for (double& q : S.init_rau) q *= o.rau_scale;
+  }
+
+  tm.mark("initial_rau");
   return S;
 }
 
 void host_assemble_central(const Setup& S, const std::array<std::vector<double>, 3>& U, std::vector<double>& aval,
                            std::array<std::vector<double>, 3>& conv) {
+  // Row-owned gather over the incident cells of each row in ascending cell
+  // order: every entry is summed in the order of the reference's cell-major
+  // loop (g4_host.hpp:326-340), so the result is identical to it.
   aval = S.mom.val;
   for (auto& r : conv) r.assign((size_t)S.nv, 0.0);
   const RefTensors& T = ref_tensors();
-  for (int c = 0; c < S.nc; ++c) {
-    const int32_t* rf = &S.ref[8 * (size_t)c];
-    const double* I = &S.invJ[9 * (size_t)c];
-    double cf[3][8];
-    for (int m = 0; m < 8; ++m)
-      for (int d = 0; d < 3; ++d)
-        cf[d][m] = rf[m] >= 0 ? U[(size_t)d][(size_t)rf[m]] : S.fixed_value[3 * (size_t)(-rf[m] - 1) + d];
-    double ur[8][3] = {{0}};
-    for (int m = 0; m < 8; ++m)
-      for (int j = 0; j < 3; ++j)
-        for (int d = 0; d < 3; ++d) ur[m][j] += cf[d][m] * I[3 * j + d];
-    for (int a = 0; a < 8; ++a) {
-      if (rf[a] < 0) continue;
-      const int r = rf[a];
+  const FineTopo& F = S.fine;
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int r = 0; r < S.nv; ++r) {
+    const int64_t rb = S.mom.row[(size_t)r];
+    for (int z = F.inc_off[(size_t)r]; z < F.inc_off[(size_t)r + 1]; ++z) {
+      const int c = (int)(F.packed[(size_t)z] >> 3), a = (int)(F.packed[(size_t)z] & 7u);
+      const int32_t* rf = &S.ref[8 * (size_t)c];
+      const double* I = &S.invJ[9 * (size_t)c];
+      double cf[3][8];
+      for (int m = 0; m < 8; ++m)
+        for (int d = 0; d < 3; ++d)
+          cf[d][m] = rf[m] >= 0 ? U[(size_t)d][(size_t)rf[m]] : S.fixed_value[3 * (size_t)(-rf[m] - 1) + d];
+      double ur[8][3] = {{0}};
+      for (int m = 0; m < 8; ++m)
+        for (int j = 0; j < 3; ++j)
+          for (int d = 0; d < 3; ++d) ur[m][j] += cf[d][m] * I[3 * j + d];
       for (int b = 0; b < 8; ++b) {
         double v = 0;
         for (int m = 0; m < 8; ++m)
           for (int j = 0; j < 3; ++j) v += ur[m][j] * T.T[a][m][b][j];
         const double C = S.det[(size_t)c] * v;
         if (rf[b] >= 0) {
-          aval[(size_t)(S.mom.row[(size_t)r] + S.row_slot[64 * (size_t)c + 8 * a + b])] += C;
+          aval[(size_t)(rb + S.row_slot[64 * (size_t)c + 8 * a + b])] += C;
         } else {
           const double* fv = &S.fixed_value[3 * (size_t)(-rf[b] - 1)];
           for (int d = 0; d < 3; ++d) conv[(size_t)d][(size_t)r] -= C * fv[d];

@@ -13,6 +13,7 @@
 // Only the laminar configuration is modelled (no DG inlet, no weak wall).
 #pragma once
 #include <array>
+#include <chrono>
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -20,6 +21,18 @@
 #include "mesh.hpp"
 
 namespace nds {
+
+// stderr stage timings when NDS_SETUP_TIMING is set
+class StageTimer {
+ public:
+  explicit StageTimer(const char* scope);
+  void mark(const char* stage);
+
+ private:
+  const char* scope_;
+  std::chrono::steady_clock::time_point t0_, last_;
+  bool on_ = false;
+};
 
 struct PipeBC {
   int wall = -1, inlet = -1, outlet = -1;

@@ -103,6 +103,10 @@ class HpErrors(C.Structure):
                                           "pressure_shift", "dp_fit", "dp_exact", "dp_rel_err")]
 
 
+class ProfileEntry(C.Structure):
+    _fields_ = [("name", C.c_char * 32), ("calls", C.c_longlong), ("total_ms", C.c_double)]
+
+
 class _Array(C.Structure):
     _fields_ = [("data", C.c_void_p), ("count", C.c_int64), ("dtype", C.c_int)]
 
@@ -141,6 +145,9 @@ def lib():
             L.nds_get_fields.argtypes = [vp] * 5
             L.nds_set_fields.argtypes = [vp] * 5
             L.nds_solver_destroy.argtypes = [vp]
+            L.nds_profile_enable.argtypes = [vp, C.c_int]
+            L.nds_launch_count.restype = C.c_ulonglong
+            L.nds_profile_read.argtypes = [vp, C.POINTER(ProfileEntry), C.c_int, C.POINTER(C.c_int)]
         _lib = L
     return _lib
 
@@ -262,10 +269,23 @@ class Solver:
         arrs = [np.ascontiguousarray(x, dtype=np.float64) for x in (u0, u1, u2, p)]
         _check(lib().nds_set_fields(self._h, *[_p(x) for x in arrs]))
 
+    def profile(self, enable: bool = True):
+        _check(lib().nds_profile_enable(self._h, int(enable)))
+
+    def profile_read(self) -> dict:
+        buf = (ProfileEntry * 32)()
+        n = C.c_int()
+        _check(lib().nds_profile_read(self._h, buf, 32, C.byref(n)))
+        return {buf[i].name.decode(): (buf[i].calls, buf[i].total_ms) for i in range(n.value)}
+
     def __del__(self):
         if getattr(self, "_h", None) and _lib is not None:
             _lib.nds_solver_destroy(self._h)
             self._h = None
+
+
+def launch_count() -> int:
+    return int(lib().nds_launch_count())
 
 
 def _f64(x):
