@@ -373,6 +373,8 @@ CONFIGS = {
     "pipe40k": dict(nr=8, ntheta=24, nz=35, radius=0.5, length=10.0, jitter=0.05, seed=0),
     # ~1M-tet pipe, Re=100 (24 rings x 72 sectors x 100 slabs)
     "pipe1m": dict(nr=24, ntheta=72, nz=100, radius=0.5, length=10.0, jitter=0.05, seed=1),
+    # ~380k-tet pipe for kernel profiling (fine CSR ~300 MB > L2)
+    "pipe400k": dict(nr=16, ntheta=48, nz=70, radius=0.5, length=10.0, jitter=0.05, seed=2),
     # small parity meshes
     "pipe_tiny": dict(nr=2, ntheta=8, nz=6, radius=0.5, length=3.0, jitter=0.05, seed=7),
     "pipe_small": dict(nr=3, ntheta=16, nz=12, radius=0.5, length=5.0, jitter=0.05, seed=3),
