@@ -49,7 +49,7 @@ OPTIONS = dict(re=100.0, alpha_u=0.7, alpha_p=0.3, p_rtol=1e-6, p_max=400, run_m
                max_outer=100000, amg_hierarchy="sa", amg_smoother="cheb2", pressure_solver="pcg")
 # SIMPLE iterations of a complete solve of OPTIONS on WORKLOAD to relCont <= 1e-6
 # plus the momentum audit (profiles/steady_state_pipe1m.md).
-STEADY_STATE_ITERATIONS = {"fp64": 2450}
+STEADY_STATE_ITERATIONS = {"fp64": 4193}
 STEADY_STATE_SOURCE = "profiles/steady_state_pipe1m.md"
 
 
@@ -323,8 +323,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--ref-seconds", type=float, default=60.0)
     args = ap.parse_args()
-    global WORKLOAD
-    WORKLOAD = args.workload
+    globals()["WORKLOAD"] = args.workload
     if args.warmup < 3 and args.impl == "nodals":
         args.warmup = 3
     if args.impl == "reference":
