@@ -576,3 +576,187 @@ __global__ void amg_gs_color(int count, const int32_t* __restrict__ rows, const 
 
 }  // namespace k
 }  // namespace nds
+
+namespace nds {
+namespace k {
+
+// ---------------------------------------------------------------------------
+// Fine Schur operator in sliced ELL (SELL-32): rows grouped in slices of 32;
+// entry k of row i (slice s = i/32, lane l = i%32) lives at
+// base[s] + 32 k + l, k < width[s].  Padding entries carry value 0 and the
+// row's own column.  One thread owns a row: fully coalesced value / column
+// streams, a sequential per-row sum in column order (deterministic).
+// ---------------------------------------------------------------------------
+struct Sell {
+  int n;
+  const int32_t* __restrict__ base;
+  const int32_t* __restrict__ width;
+  const int32_t* __restrict__ col;   // absolute columns (used when dcol is null)
+  const int16_t* __restrict__ dcol;  // column - row, when every |column - row| < 2^15
+};
+
+template <bool D16>
+__device__ __forceinline__ int sell_col(const Sell& A, int o, int i) {
+  if (D16) return i + (int)A.dcol[o];
+  return A.col[o];
+}
+
+enum SellMode { SELL_Y = 0, SELL_RESID = 1, SELL_SMOOTH = 2, SELL_DOT = 3 };
+
+// Row dot product with 8 independent entries in flight per thread (column
+// and value streams first, then the x gathers) to cover HBM latency; two
+// accumulators, fixed order -> deterministic.
+template <class T, bool D16>
+__device__ __forceinline__ T sell_row(const Sell& A, const T* __restrict__ v, const T* __restrict__ x, int i) {
+  const int s = i >> 5;
+  const int b = A.base[s] + (i & 31);
+  const int w = A.width[s];
+  T s0 = 0, s1 = 0;
+  int k = 0;
+  for (; k + 8 <= w; k += 8) {
+    int j[8];
+    T a[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int o = b + 32 * (k + u);
+      j[u] = sell_col<D16>(A, o, i);
+      a[u] = v[o];
+    }
+    T xv[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) xv[u] = x[j[u]];
+#pragma unroll
+    for (int u = 0; u < 8; u += 2) {
+      s0 += a[u] * xv[u];
+      s1 += a[u + 1] * xv[u + 1];
+    }
+  }
+  for (; k < w; ++k) {
+    const int o = b + 32 * k;
+    s0 += v[o] * x[sell_col<D16>(A, o, i)];
+  }
+  return s0 + s1;
+}
+
+// MODE SELL_Y:      y = A x
+// MODE SELL_RESID:  y = b - A x (and y2 = y when y2 != null)
+// MODE SELL_SMOOTH: y = x + w (b - A x) / den
+// MODE SELL_DOT:    y = A x, partials of x.y (grid-stride; blockDim = kBlock)
+template <class T, int MODE, bool D16>
+__global__ void __launch_bounds__(kBlock) sell_spmv(Sell A, const T* __restrict__ v, const T* __restrict__ x,
+                                                    const T* __restrict__ b, const T* __restrict__ den, T w,
+                                                    T* __restrict__ y, T* __restrict__ y2, double* __restrict__ part) {
+  if (MODE == SELL_DOT) {
+    double acc[1] = {0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n; i += gridDim.x * blockDim.x) {
+      const T s = sell_row<T, D16>(A, v, x, i);
+      y[i] = s;
+      acc[0] += (double)x[i] * (double)s;
+    }
+    write_partials<1>(acc, part);
+    return;
+  }
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= A.n) return;
+  const T s = sell_row<T, D16>(A, v, x, i);
+  if (MODE == SELL_Y) {
+    y[i] = s;
+  } else if (MODE == SELL_RESID) {
+    const T q = b[i] - s;
+    y[i] = q;
+    if (y2) y2[i] = q;
+  } else {
+    y[i] = x[i] + w * (b[i] - s) / den[i];
+  }
+}
+
+// Fine Schur refresh into the SELL layout (same arithmetic as fine_refresh).
+template <class T>
+__global__ void __launch_bounds__(kBlock) sell_refresh(int nc, const int32_t* __restrict__ row,
+                                                       const int32_t* __restrict__ coff, const uint8_t* __restrict__ cnt,
+                                                       const uint32_t* __restrict__ cpk, const uint8_t* __restrict__ ca,
+                                                       const int32_t* __restrict__ ref, const T* __restrict__ bco,
+                                                       const T* __restrict__ rau, const int32_t* __restrict__ dslot,
+                                                       const int32_t* __restrict__ sbase, T* __restrict__ val,
+                                                       T* __restrict__ diag, T* __restrict__ l1) {
+  __shared__ T sB[kWarps][24];
+  __shared__ T sR[kWarps][8];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (c >= nc) return;
+  if (lane < 24) sB[w][lane] = bco[24 * (size_t)c + lane];
+  if (lane < 8) {
+    const int g = ref[8 * (size_t)c + lane];
+    sR[w][lane] = g >= 0 ? rau[g] : T(0);
+  }
+  __syncwarp();
+  const int rb = row[c], re = row[c + 1];
+  const int out = sbase[c >> 5] + (c & 31);
+  int base = coff[c];
+  T asum = 0;
+  for (int k0 = rb; k0 < re; k0 += 32) {
+    const int k = k0 + lane;
+    const int n = k < re ? (int)cnt[k] : 0;
+    int incl = n;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    const int q0 = base + incl - n;
+    T v = 0;
+    for (int q = q0; q < q0 + n; ++q) {
+      const uint32_t pk = cpk[q];
+      const int a = ca[q];
+      const T* bb = bco + 24 * (size_t)(pk >> 3) + 3 * (pk & 7u);
+      const T dot = sB[w][3 * a] * bb[0] + sB[w][3 * a + 1] * bb[1] + sB[w][3 * a + 2] * bb[2];
+      v += sR[w][a] * dot;
+    }
+    if (k < re) {
+      val[out + 32 * (k - rb)] = v;
+      asum += fabs(v);
+      if (k - rb == dslot[c]) diag[c] = v;
+    }
+    base += __shfl_sync(0xffffffffu, incl, 31);
+  }
+  if (l1) {
+    asum = warp_sum(asum);
+    if (lane == 0) l1[c] = asum;
+  }
+}
+
+// multicolour GS colour pass on the SELL fine operator (thread per row)
+template <class T, bool D16>
+__global__ void sell_gs_color(int count, const int32_t* __restrict__ rows, Sell A, const T* __restrict__ v,
+                              const T* __restrict__ diag, const T* __restrict__ b, T* __restrict__ x, T omega) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= count) return;
+  const int i = rows[q];
+  const int s = i >> 5;
+  const int base = A.base[s] + (i & 31);
+  T off = 0;
+  for (int k = 0; k < A.width[s]; ++k) {
+    const int o = base + 32 * k;
+    const int j = sell_col<D16>(A, o, i);
+    if (j != i) off += v[o] * x[j];
+  }
+  const T old = x[i];
+  const T gs = (b[i] - off) / diag[i];
+  x[i] = old + omega * (gs - old);
+}
+
+// c = P^T f, warp per coarse row over R = P^T (deterministic tree per row)
+template <class T>
+__global__ void __launch_bounds__(kBlock) restrict_warp(int nc, const int32_t* __restrict__ rr,
+                                                        const int32_t* __restrict__ rc, const T* __restrict__ rv,
+                                                        const T* __restrict__ f, T* __restrict__ c) {
+  const int I = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (I >= nc) return;
+  T s = 0;
+  for (int k = rr[I] + lane; k < rr[I + 1]; k += 32) s += rv[k] * f[rc[k]];
+  s = warp_sum(s);
+  if (lane == 0) c[I] = s;
+}
+
+}  // namespace k
+}  // namespace nds

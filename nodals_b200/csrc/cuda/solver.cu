@@ -14,6 +14,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -217,6 +218,7 @@ class Solver final : public ISolver {
     for (auto& e : ev_)
       if (e) cudaEventDestroy(e);
     if (hsc_) cudaFreeHost(hsc_);
+    if (hflags_) cudaFreeHost(hflags_);
     if (st_) cudaStreamDestroy(st_);
   }
 
@@ -268,9 +270,7 @@ class Solver final : public ISolver {
 
     // fine Schur CSR with contributions regrouped by destination slot
     const FineTopo& F = S.fine;
-    frow_.upload(F.row);
-    fcol_.upload(F.col);
-    fdpos_.upload(F.diag_pos);
+    frow_.upload(F.row);  // CSR offsets index the per-entry contribution counts
     fcoff_.upload(F.contrib_off);
     {
       std::vector<uint8_t> cnt(F.col.size(), 0), ca(F.slot.size());
@@ -301,7 +301,57 @@ class Solver final : public ISolver {
       fca_.upload(ca);
       fcpk_.upload(cpk);
     }
-    fval_.alloc(F.col.size());
+    {
+      // SELL-32 layout of the fine pattern
+      const int ns = (nc_ + 31) / 32;
+      std::vector<int32_t> width((size_t)ns, 0), base((size_t)ns + 1, 0), dslot((size_t)nc_);
+      for (int c = 0; c < nc_; ++c) {
+        const int len = F.row[(size_t)c + 1] - F.row[(size_t)c];
+        width[(size_t)(c >> 5)] = std::max(width[(size_t)(c >> 5)], len);
+        dslot[(size_t)c] = F.diag_pos[(size_t)c] - F.row[(size_t)c];
+      }
+      for (int q = 0; q < ns; ++q) {
+        const int64_t nb = (int64_t)base[(size_t)q] + 32LL * width[(size_t)q];
+        if (nb > INT32_MAX) throw std::runtime_error("SELL fine operator exceeds int32 offsets");
+        base[(size_t)q + 1] = (int32_t)nb;
+      }
+      std::vector<int32_t> scol((size_t)base[(size_t)ns]);
+      for (int c = 0; c < nc_; ++c) {
+        const int s0 = c >> 5, l = c & 31, rb = F.row[(size_t)c], len = F.row[(size_t)c + 1] - rb;
+        for (int q = 0; q < width[(size_t)s0]; ++q)
+          scol[(size_t)base[(size_t)s0] + 32 * (size_t)q + l] = q < len ? F.col[(size_t)rb + q] : c;
+      }
+      // lanes past the last row of the final slice point at row 0 (never read by a live thread)
+      for (int c = nc_; c < ns * 32; ++c) {
+        const int s0 = c >> 5, l = c & 31;
+        for (int q = 0; q < width[(size_t)s0]; ++q) scol[(size_t)base[(size_t)s0] + 32 * (size_t)q + l] = 0;
+      }
+      swidth_.upload(width);
+      sbase_.upload(base);
+      fdslot_.upload(dslot);
+      fval_.alloc(scol.size());
+      NDS_CUDA(cudaMemset(fval_.p, 0, fval_.bytes()));
+      // 16-bit column deltas when the ordering keeps every |column - row| < 2^15
+      bool fits = true;
+      std::vector<int16_t> dcol(scol.size());
+      for (int q = 0; q < ns && fits; ++q)
+        for (int kk = 0; kk < width[(size_t)q] && fits; ++kk)
+          for (int l = 0; l < 32; ++l) {
+            const int row = 32 * q + l;
+            const size_t o = (size_t)base[(size_t)q] + 32 * (size_t)kk + l;
+            const int d = row < nc_ ? scol[o] - row : 0;
+            if (d < -32767 || d > 32767) { fits = false; break; }
+            dcol[o] = (int16_t)d;
+          }
+      if (fits && !std::getenv("NDS_SELL_COL32")) {
+        sdcol_.upload(dcol);
+        sell_ = k::Sell{nc_, sbase_.p, swidth_.p, nullptr, sdcol_.p};
+      } else {
+        scol_.upload(scol);
+        sell_ = k::Sell{nc_, sbase_.p, swidth_.p, scol_.p, nullptr};
+      }
+      sell_nnz_ = (long long)scol.size();
+    }
     fdiag_.upload(H.fine_diag);
     const bool l1 = o_.amg_smoother == NDS_SM_L1JACOBI;
     if (l1) fl1_.alloc((size_t)nc_);
@@ -371,6 +421,7 @@ class Solver final : public ISolver {
     sc_.alloc(kScalars);
     flags_.alloc(1);
     NDS_CUDA(cudaMallocHost((void**)&hsc_, sizeof(double) * kScalars));
+    NDS_CUDA(cudaMallocHost((void**)&hflags_, sizeof(int)));
     NDS_CUDA(cudaMemsetAsync(flags_.p, 0, sizeof(int), st_));
 
     // setup-time state: fine CSR refreshed with the initial rAU
@@ -392,6 +443,51 @@ class Solver final : public ISolver {
   static constexpr int kScalars = 32;
   enum { S_RHO = 0, S_PQ = 1, S_ALPHA = 2, S_RN2 = 3, S_RHON = 4, S_BETA = 5, S_TMP = 8, S_TMP2 = 9, S_CONT2 = 10,
          S_AUDIT = 16 };
+
+  // CUDA graphs of fixed launch sequences (no host decisions inside)
+  struct Graph {
+    cudaGraphExec_t exec = nullptr;
+    unsigned long long kernels = 0;
+    ~Graph() {
+      if (exec) cudaGraphExecDestroy(exec);
+    }
+  };
+  template <class F>
+  void capture(Graph& g, F&& body) {
+    const bool was = prof.on;
+    prof.on = false;
+    const unsigned long long l0 = g_launches;
+    NDS_CUDA(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
+    try {
+      body();
+    } catch (...) {
+      cudaGraph_t junk = nullptr;
+      cudaStreamEndCapture(st_, &junk);
+      if (junk) cudaGraphDestroy(junk);
+      prof.on = was;
+      throw;
+    }
+    cudaGraph_t graph = nullptr;
+    NDS_CUDA(cudaStreamEndCapture(st_, &graph));
+    const cudaError_t e = cudaGraphInstantiate(&g.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    NDS_CUDA(e);
+    g.kernels = g_launches - l0;
+    g_launches = l0;
+    prof.on = was;
+  }
+  void replay(Graph& g) {
+    NDS_CUDA(cudaGraphLaunch(g.exec, st_));
+    g_launches += g.kernels;
+  }
+  bool use_graphs_ = std::getenv("NDS_NO_GRAPHS") == nullptr;
+  Graph g_amg_, g_pcg1_, g_pcg2_;
+  // z = M r on the solver's fixed PCG buffers, replayed from a graph
+  void amg_rz() {
+    if (!use_graphs_) return amg_apply(r_.p, z_.p);
+    if (!g_amg_.exec) capture(g_amg_, [&] { amg_apply(r_.p, z_.p); });
+    replay(g_amg_);
+  }
 
   int red_grid(long long n, int per = kBlock) const { return std::min(grid_for(n, per), kMaxPartBlocks); }
   template <int NV>
@@ -418,22 +514,48 @@ class Solver final : public ISolver {
     reduce_to<1>(g, slot);
   }
 
-  int spcat(const int32_t* rp) const { return rp == frow_.p ? P_FINE_SPMV : P_COARSE_SPMV; }
-  void spmv(int n, const int32_t* rp, const int32_t* ci, const T* v, const T* x, T* y) {
-    ProfScope ps(prof, st_, spcat(rp));
-    k::spmv<T><<<grid_for((long long)n * 32), kBlock, 0, st_>>>(n, rp, ci, v, x, y);
+  // operator view: the fine Schur matrix in SELL-32, AMG levels in CSR
+  struct OpView {
+    int n;
+    bool sell;
+    k::Sell s;
+    const int32_t* rp;
+    const int32_t* ci;
+    const T* v;
+  };
+  template <int MODE>
+  void sell_launch(const OpView& A, int grid, const T* x, const T* b, const T* den, double w, T* y, T* y2) {
+    if (A.s.dcol)
+      k::sell_spmv<T, MODE, true><<<grid, kBlock, 0, st_>>>(A.s, A.v, x, b, den, T(w), y, y2, part_.p);
+    else
+      k::sell_spmv<T, MODE, false><<<grid, kBlock, 0, st_>>>(A.s, A.v, x, b, den, T(w), y, y2, part_.p);
+  }
+  OpView fine_op() const { return {nc_, true, sell_, nullptr, nullptr, fval_.p}; }
+  OpView level_op(const Level& A) const { return {A.n, false, k::Sell{}, A.row.p, A.col.p, A.val.p}; }
+  void op_spmv(const OpView& A, const T* x, T* y) {
+    ProfScope ps(prof, st_, A.sell ? P_FINE_SPMV : P_COARSE_SPMV);
+    if (A.sell) sell_launch<k::SELL_Y>(A, grid_for(A.n), x, nullptr, nullptr, 0.0, y, nullptr);
+    else k::spmv<T><<<grid_for((long long)A.n * 32), kBlock, 0, st_>>>(A.n, A.rp, A.ci, A.v, x, y);
     NDS_LAUNCH();
+  }
+  void op_resid(const OpView& A, const T* x, const T* b, T* r, T* r2 = nullptr) {
+    ProfScope ps(prof, st_, A.sell ? P_FINE_SPMV : P_COARSE_SPMV);
+    if (A.sell) sell_launch<k::SELL_RESID>(A, grid_for(A.n), x, b, nullptr, 0.0, r, r2);
+    else k::spmv_resid<T><<<grid_for((long long)A.n * 32), kBlock, 0, st_>>>(A.n, A.rp, A.ci, A.v, x, b, r, r2);
+    NDS_LAUNCH();
+  }
+  void op_smooth(const OpView& A, const T* xin, const T* b, const T* den, double w, T* xout) {
+    ProfScope ps(prof, st_, A.sell ? P_FINE_SPMV : P_COARSE_SPMV);
+    if (A.sell) sell_launch<k::SELL_SMOOTH>(A, grid_for(A.n), xin, b, den, w, xout, nullptr);
+    else k::spmv_smooth<T><<<grid_for((long long)A.n * 32), kBlock, 0, st_>>>(A.n, A.rp, A.ci, A.v, xin, b, den, T(w), xout);
+    NDS_LAUNCH();
+  }
+  // CSR helpers kept for coarse-level code paths
+  void spmv(int n, const int32_t* rp, const int32_t* ci, const T* v, const T* x, T* y) {
+    op_spmv(OpView{n, false, k::Sell{}, rp, ci, v}, x, y);
   }
   void resid(int n, const int32_t* rp, const int32_t* ci, const T* v, const T* x, const T* b, T* r, T* r2 = nullptr) {
-    ProfScope ps(prof, st_, spcat(rp));
-    k::spmv_resid<T><<<grid_for((long long)n * 32), kBlock, 0, st_>>>(n, rp, ci, v, x, b, r, r2);
-    NDS_LAUNCH();
-  }
-  void smooth_step(int n, const int32_t* rp, const int32_t* ci, const T* v, const T* xin, const T* b, const T* den,
-                   double w, T* xout) {
-    ProfScope ps(prof, st_, spcat(rp));
-    k::spmv_smooth<T><<<grid_for((long long)n * 32), kBlock, 0, st_>>>(n, rp, ci, v, xin, b, den, T(w), xout);
-    NDS_LAUNCH();
+    op_resid(OpView{n, false, k::Sell{}, rp, ci, v}, x, b, r, r2);
   }
   void vcopy(int n, const T* a, T* b) {
     k::copy<T><<<grid_for(n), kBlock, 0, st_>>>(n, a, b);
@@ -447,44 +569,46 @@ class Solver final : public ISolver {
   // fine Schur operator
   void refresh_fine(const T* rau) {
     ProfScope ps(prof, st_, P_REFRESH);
-    k::fine_refresh<T><<<grid_for((long long)nc_ * 32), kBlock, 0, st_>>>(
-        nc_, frow_.p, fcoff_.p, fcnt_.p, fcpk_.p, fca_.p, ref_.p, bco_.p, rau, fdpos_.p, fval_.p, fdiag_.p, fl1_.p);
+    k::sell_refresh<T><<<grid_for((long long)nc_ * 32), kBlock, 0, st_>>>(
+        nc_, frow_.p, fcoff_.p, fcnt_.p, fcpk_.p, fca_.p, ref_.p, bco_.p, rau, fdslot_.p, sbase_.p, fval_.p, fdiag_.p, fl1_.p);
     NDS_LAUNCH();
   }
-  void fine_apply(const T* x, T* y) { spmv(nc_, frow_.p, fcol_.p, fval_.p, x, y); }
+  void fine_apply(const T* x, T* y) { op_spmv(fine_op(), x, y); }
 
   // ------------------------------------------------------------- smoothers
   // x = S(b) from a zero initial guess.  Jacobi-type steps write to a second
   // buffer (xin is read by every row), then the result is copied back.
-  void poly_smooth(int n, const int32_t* rp, const int32_t* ci, const T* v, const T* diag, const T* b, T* x, T* pong,
-                   double lambda, bool cheb, const T* den_jac, int sweeps) {
+  void poly_smooth(const OpView& A, const T* diag, const T* b, T* x, T* pong, double lambda, bool cheb,
+                   const T* den_jac, int sweeps) {
+    // x = S(b) from a zero guess: one diagonal step, then m Jacobi-type steps
+    // ping-ponging between two buffers; the first buffer is chosen by the
+    // parity of m so that the last step writes x (no copy-back).
+    const int n = A.n;
+    const int deg = o_.amg_cheb_degree;
+    const int m = cheb ? deg - 1 : sweeps - 1;
+    T* cur = (m % 2 == 0) ? x : pong;
+    T* nxt = (m % 2 == 0) ? pong : x;
     if (cheb) {
       const double lo = o_.amg_lambda_low_fraction * lambda;
       if (!(lambda > lo && lo > 0)) throw SolveFailure(NDS_E_BREAKDOWN, "Chebyshev smoother interval invalid");
-      const int deg = o_.amg_cheb_degree;
-      k::jacobi_zero<T><<<grid_for(n), kBlock, 0, st_>>>(n, T(1.0 / cheb_root(lambda, lo, 0, deg)), b, diag, x);
+      k::jacobi_zero<T><<<grid_for(n), kBlock, 0, st_>>>(n, T(1.0 / cheb_root(lambda, lo, 0, deg)), b, diag, cur);
       NDS_LAUNCH();
-      T* cur = x;
-      T* nxt = pong;
       for (int kk = 1; kk < deg; ++kk) {
-        smooth_step(n, rp, ci, v, cur, b, diag, 1.0 / cheb_root(lambda, lo, kk, deg), nxt);
+        op_smooth(A, cur, b, diag, 1.0 / cheb_root(lambda, lo, kk, deg), nxt);
         std::swap(cur, nxt);
       }
-      if (cur != x) vcopy(n, cur, x);
     } else {
-      k::jacobi_zero<T><<<grid_for(n), kBlock, 0, st_>>>(n, T(o_.amg_jacobi_omega), b, den_jac, x);
+      k::jacobi_zero<T><<<grid_for(n), kBlock, 0, st_>>>(n, T(o_.amg_jacobi_omega), b, den_jac, cur);
       NDS_LAUNCH();
-      T* cur = x;
-      T* nxt = pong;
-      for (int s = 1; s < sweeps; ++s) {
-        smooth_step(n, rp, ci, v, cur, b, den_jac, o_.amg_jacobi_omega, nxt);
+      for (int q = 1; q < sweeps; ++q) {
+        op_smooth(A, cur, b, den_jac, o_.amg_jacobi_omega, nxt);
         std::swap(cur, nxt);
       }
-      if (cur != x) vcopy(n, cur, x);
     }
   }
-  void mcgs(int n, const int32_t* rp, const int32_t* ci, const T* v, const T* diag, const T* b, T* x,
-            const DBuf<int32_t>& crows, const std::vector<int>& coff, int sweeps) {
+  void mcgs(const OpView& A, const T* diag, const T* b, T* x, const DBuf<int32_t>& crows, const std::vector<int>& coff,
+            int sweeps) {
+    const int n = A.n;
     NDS_CUDA(cudaMemsetAsync(x, 0, sizeof(T) * (size_t)n, st_));
     const int ncol = (int)coff.size() - 1;
     auto pass = [&](bool reverse) {
@@ -492,8 +616,15 @@ class Solver final : public ISolver {
         const int c = reverse ? ncol - 1 - qq : qq;
         const int cnt = coff[(size_t)c + 1] - coff[(size_t)c];
         if (cnt <= 0) continue;
-        k::amg_gs_color<T><<<grid_for((long long)cnt * 32), kBlock, 0, st_>>>(cnt, crows.p + coff[(size_t)c], rp, ci, v, diag,
-                                                                             b, x, T(o_.amg_mcgs_omega));
+        if (A.sell && A.s.dcol)
+          k::sell_gs_color<T, true><<<grid_for(cnt), kBlock, 0, st_>>>(cnt, crows.p + coff[(size_t)c], A.s, A.v, diag, b,
+                                                                    x, T(o_.amg_mcgs_omega));
+        else if (A.sell)
+          k::sell_gs_color<T, false><<<grid_for(cnt), kBlock, 0, st_>>>(cnt, crows.p + coff[(size_t)c], A.s, A.v, diag, b,
+                                                                     x, T(o_.amg_mcgs_omega));
+        else
+          k::amg_gs_color<T><<<grid_for((long long)cnt * 32), kBlock, 0, st_>>>(cnt, crows.p + coff[(size_t)c], A.rp, A.ci,
+                                                                               A.v, diag, b, x, T(o_.amg_mcgs_omega));
         NDS_LAUNCH();
       }
     };
@@ -506,26 +637,24 @@ class Solver final : public ISolver {
   void smooth_fine(const T* b, T* x) {
     const int sm = o_.amg_smoother;
     if (sm == NDS_SM_MCGS) {
-      mcgs(nc_, frow_.p, fcol_.p, fval_.p, fdiag_.p, b, x, fine_crows_, fine_coff_, o_.amg_mcgs_fine_sweeps);
+      mcgs(fine_op(), fdiag_.p, b, x, fine_crows_, fine_coff_, o_.amg_mcgs_fine_sweeps);
       return;
     }
     const T* den = sm == NDS_SM_L1JACOBI ? fl1_.p : fdiag_.p;
-    poly_smooth(nc_, frow_.p, fcol_.p, fval_.p, fdiag_.p, b, x, fpong_.p, fine_lambda_, sm == NDS_SM_CHEB2, den,
-                o_.amg_jacobi_fine_sweeps);
+    poly_smooth(fine_op(), fdiag_.p, b, x, fpong_.p, fine_lambda_, sm == NDS_SM_CHEB2, den, o_.amg_jacobi_fine_sweeps);
   }
   void smooth_level(Level& A, const T* b, T* x, double lambda) {
     const int sm = o_.amg_smoother;
     if (sm == NDS_SM_MCGS) {
-      mcgs(A.n, A.row.p, A.col.p, A.val.p, A.diag.p, b, x, A.crows, A.coff, o_.amg_mcgs_coarse_sweeps);
+      mcgs(level_op(A), A.diag.p, b, x, A.crows, A.coff, o_.amg_mcgs_coarse_sweeps);
       return;
     }
     const T* den = sm == NDS_SM_L1JACOBI ? A.l1.p : A.diag.p;
-    poly_smooth(A.n, A.row.p, A.col.p, A.val.p, A.diag.p, b, x, A.pong.p, lambda, sm == NDS_SM_CHEB2, den,
-                o_.amg_jacobi_coarse_sweeps);
+    poly_smooth(level_op(A), A.diag.p, b, x, A.pong.p, lambda, sm == NDS_SM_CHEB2, den, o_.amg_jacobi_coarse_sweeps);
   }
   void restrict_to(const Xfer& X, const T* f, T* c) {
     ProfScope ps(prof, st_, P_TRANSFER);
-    k::restrict_gather<T><<<grid_for(X.nc), kBlock, 0, st_>>>(X.nc, X.rrow.p, X.rcol.p, X.rval.p, f, c);
+    k::restrict_warp<T><<<grid_for((long long)X.nc * 32), kBlock, 0, st_>>>(X.nc, X.rrow.p, X.rcol.p, X.rval.p, f, c);
     NDS_LAUNCH();
   }
   void prolong(const Xfer& X, const T* c, T* f) {
@@ -556,12 +685,12 @@ class Solver final : public ISolver {
   }
   void amg_apply(const T* b, T* z) {
     smooth_fine(b, z);
-    resid(nc_, frow_.p, fcol_.p, fval_.p, z, b, fr_.p);
+    op_resid(fine_op(), z, b, fr_.p);
     Level& C = L_[0];
     restrict_to(X_[0], fr_.p, C.b.p);
     vcycle(0, C.b.p, C.x.p);
     prolong(X_[0], C.x.p, z);
-    resid(nc_, frow_.p, fcol_.p, fval_.p, z, b, fr_.p, frhs_.p);
+    op_resid(fine_op(), z, b, fr_.p, frhs_.p);
     smooth_fine(frhs_.p, fcorr_.p);
     vaxpy(nc_, 1.0, fcorr_.p, z);
   }
@@ -663,32 +792,54 @@ class Solver final : public ISolver {
     if (!std::isfinite(r0)) throw SolveFailure(NDS_E_BREAKDOWN, "pressure initial norm nonfinite");
     return r0;
   }
+  // one PCG iteration, first half: q = A p, pq = p.q, alpha = rho/pq,
+  // x += alpha p, r -= alpha q, rn2 = r.r; then rn2 and the flags to the host
+  void pcg_half1() {
+    const int g = red_grid(nc_);
+    {
+      ProfScope ps(prof, st_, P_FINE_SPMV);
+      sell_launch<k::SELL_DOT>(fine_op(), g, pp_.p, nullptr, nullptr, 0.0, q_.p, nullptr);
+      NDS_LAUNCH();
+    }
+    reduce_to<1>(g, S_PQ);
+    k::pcg_alpha<<<1, 1, 0, st_>>>(sc_.p, flags_.p);
+    NDS_LAUNCH();
+    k::xr_update<T><<<g, kBlock, 0, st_>>>(nc_, 0.0, sc_.p + S_ALPHA, pp_.p, q_.p, x_.p, r_.p, part_.p);
+    NDS_LAUNCH();
+    reduce_to<1>(g, S_RN2);
+    NDS_CUDA(cudaMemcpyAsync(hsc_ + S_RN2, sc_.p + S_RN2, sizeof(double), cudaMemcpyDeviceToHost, st_));
+    NDS_CUDA(cudaMemcpyAsync(hflags_, flags_.p, sizeof(int), cudaMemcpyDeviceToHost, st_));
+  }
+  // second half: z = M r, rho_new = r.z, beta = rho_new/rho, p = z + beta p
+  void pcg_half2() {
+    amg_apply(r_.p, z_.p);
+    dot_dev(r_.p, z_.p, nc_, S_RHON);
+    k::pcg_beta<<<1, 1, 0, st_>>>(sc_.p, flags_.p);
+    NDS_LAUNCH();
+    k::p_update<T><<<grid_for(nc_), kBlock, 0, st_>>>(nc_, sc_.p + S_BETA, z_.p, pp_.p);
+    NDS_LAUNCH();
+  }
   PRes pcg(const T* rhs) {
     const double r0 = p_start(rhs);
     if (r0 <= o_.p_atol) return {0, 0.0, true};
-    amg_apply(r_.p, z_.p);
+    amg_rz();
     vcopy(nc_, z_.p, pp_.p);
     dot_dev(r_.p, z_.p, nc_, S_RHO);
     fetch(S_RHO, 1);
     if (!(hsc_[S_RHO] > 0) || !std::isfinite(hsc_[S_RHO])) throw SolveFailure(NDS_E_BREAKDOWN, "pressure PCG initial rho nonpositive");
     NDS_CUDA(cudaMemsetAsync(flags_.p, 0, sizeof(int), st_));
     const double target = std::max(o_.p_atol, o_.p_rtol * r0);
+    if (use_graphs_ && !g_pcg1_.exec) {
+      capture(g_pcg1_, [&] { pcg_half1(); });
+      capture(g_pcg2_, [&] { pcg_half2(); });
+    }
     PRes R;
     for (int kk = 0; kk < o_.p_max; ++kk) {
-      // q = A p, pq = p.q ; alpha = rho/pq ; x += a p, r -= a q, rn2
-      int g = red_grid((long long)nc_ * 32);
-      ProfScope ps(prof, st_, P_FINE_SPMV);
-      k::spmv_dot<T><<<g, kBlock, 0, st_>>>(nc_, frow_.p, fcol_.p, fval_.p, pp_.p, q_.p, part_.p);
-      NDS_LAUNCH();
-      reduce_to<1>(g, S_PQ);
-      k::pcg_alpha<<<1, 1, 0, st_>>>(sc_.p, flags_.p);
-      NDS_LAUNCH();
-      g = red_grid(nc_);
-      k::xr_update<T><<<g, kBlock, 0, st_>>>(nc_, 0.0, sc_.p + S_ALPHA, pp_.p, q_.p, x_.p, r_.p, part_.p);
-      NDS_LAUNCH();
-      reduce_to<1>(g, S_RN2);
-      check_flags();
-      fetch(S_RN2, 1);
+      if (use_graphs_) replay(g_pcg1_);
+      else pcg_half1();
+      NDS_CUDA(cudaStreamSynchronize(st_));
+      if (*hflags_ & 1) throw SolveFailure(NDS_E_BREAKDOWN, "pressure PCG pAp nonpositive");
+      if (*hflags_ & 2) throw SolveFailure(NDS_E_BREAKDOWN, "pressure PCG rho nonpositive");
       const double rn = std::sqrt(hsc_[S_RN2]);
       R.its = kk + 1;
       R.rel = rn / std::max(r0, 1e-300);
@@ -697,12 +848,8 @@ class Solver final : public ISolver {
         R.ok = true;
         break;
       }
-      amg_apply(r_.p, z_.p);
-      dot_dev(r_.p, z_.p, nc_, S_RHON);
-      k::pcg_beta<<<1, 1, 0, st_>>>(sc_.p, flags_.p);
-      NDS_LAUNCH();
-      k::p_update<T><<<grid_for(nc_), kBlock, 0, st_>>>(nc_, sc_.p + S_BETA, z_.p, pp_.p);
-      NDS_LAUNCH();
+      if (use_graphs_) replay(g_pcg2_);
+      else pcg_half2();
     }
     check_flags();
     return R;
@@ -726,7 +873,7 @@ class Solver final : public ISolver {
         const int ri = kk % o_.p_cheb_degree;
         omega = 1.0 / (centre - radius * std::cos(pi * (2.0 * (double)ri + 1.0) / (2.0 * (double)o_.p_cheb_degree)));
       }
-      amg_apply(r_.p, z_.p);
+      amg_rz();
       fine_apply(z_.p, q_.p);
       const int g = red_grid(nc_);
       k::xr_update<T><<<g, kBlock, 0, st_>>>(nc_, omega, nullptr, z_.p, q_.p, x_.p, r_.p, part_.p);
@@ -997,7 +1144,10 @@ class Solver final : public ISolver {
   DBuf<T> u_[3], b_[3], s_[3], v_[3];
   std::vector<int> color_off_;
   // pressure
-  DBuf<int32_t> frow_, fcol_, fdpos_, fcoff_, fine_crows_;
+  DBuf<int32_t> frow_, fcol_, fdpos_, fcoff_, fine_crows_, sbase_, swidth_, scol_, fdslot_;
+  DBuf<int16_t> sdcol_;
+  k::Sell sell_{};
+  long long sell_nnz_ = 0;
   std::vector<int> fine_coff_;
   DBuf<uint8_t> fcnt_, fca_;
   DBuf<uint32_t> fcpk_;
@@ -1007,6 +1157,7 @@ class Solver final : public ISolver {
   DBuf<double> part_, sc_;
   DBuf<int> flags_;
   double* hsc_ = nullptr;
+  int* hflags_ = nullptr;
 };
 
 }  // namespace nds
