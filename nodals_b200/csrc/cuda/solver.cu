@@ -481,7 +481,7 @@ class Solver final : public ISolver {
     g_launches += g.kernels;
   }
   bool use_graphs_ = std::getenv("NDS_NO_GRAPHS") == nullptr;
-  Graph g_amg_, g_pcg1_, g_pcg2_;
+  Graph g_amg_, g_pcg2_;
   // z = M r on the solver's fixed PCG buffers, replayed from a graph
   void amg_rz() {
     if (!use_graphs_) return amg_apply(r_.p, z_.p);
@@ -829,14 +829,12 @@ class Solver final : public ISolver {
     if (!(hsc_[S_RHO] > 0) || !std::isfinite(hsc_[S_RHO])) throw SolveFailure(NDS_E_BREAKDOWN, "pressure PCG initial rho nonpositive");
     NDS_CUDA(cudaMemsetAsync(flags_.p, 0, sizeof(int), st_));
     const double target = std::max(o_.p_atol, o_.p_rtol * r0);
-    if (use_graphs_ && !g_pcg1_.exec) {
-      capture(g_pcg1_, [&] { pcg_half1(); });
-      capture(g_pcg2_, [&] { pcg_half2(); });
-    }
+    // the first half stays a direct launch sequence, so the fine SpMV of the
+    // Krylov step is timed live by the profiler; the AMG half is a graph
+    if (use_graphs_ && !g_pcg2_.exec) capture(g_pcg2_, [&] { pcg_half2(); });
     PRes R;
     for (int kk = 0; kk < o_.p_max; ++kk) {
-      if (use_graphs_) replay(g_pcg1_);
-      else pcg_half1();
+      pcg_half1();
       NDS_CUDA(cudaStreamSynchronize(st_));
       if (*hflags_ & 1) throw SolveFailure(NDS_E_BREAKDOWN, "pressure PCG pAp nonpositive");
       if (*hflags_ & 2) throw SolveFailure(NDS_E_BREAKDOWN, "pressure PCG rho nonpositive");
