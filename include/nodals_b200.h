@@ -39,6 +39,11 @@ typedef struct nds_mesh nds_mesh;
 typedef struct nds_problem nds_problem;
 typedef struct nds_solver nds_solver;
 
+/* NDS_FP64 / NDS_FP32: the reference's two builds (NODALS_GPU_PRECISION_MODE
+ * 0 / 1, gpu/serial_cuda/h8_main.cu).  NDS_AMG_FP32 has no reference build:
+ * state, momentum, continuity and the Krylov method (including its A*p) stay
+ * FP64 while the AMG V-cycle -- levels, transfers, smoothers and an FP32 copy
+ * of the fine Schur operator written by the same refresh -- runs in FP32. */
 enum nds_precision { NDS_FP64 = 0, NDS_FP32 = 1, NDS_AMG_FP32 = 2 };
 enum nds_run_mode { NDS_RUN_FIXED10 = 0, NDS_RUN_CONVERGE = 1 };
 enum nds_momentum_work { NDS_MOM_FGS1 = 0, NDS_MOM_ALTGS1 = 1, NDS_MOM_SGS1 = 2 };
@@ -91,6 +96,7 @@ typedef struct nds_iter_report {
   int all_momentum_met;
   int converged;
   double ms_assembly, ms_momentum, ms_continuity, ms_pressure, ms_update;
+  double ms_refresh;        /* fine Schur refresh, the first part of ms_pressure */
 } nds_iter_report;
 
 typedef struct nds_solve_report {

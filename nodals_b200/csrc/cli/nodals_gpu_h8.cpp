@@ -121,7 +121,8 @@ int run(int argc, char** argv) {
       const std::string p = sv();
       if (p == "fp64") o.precision = NDS_FP64;
       else if (p == "fp32") o.precision = NDS_FP32;
-      else throw Fail("--precision must be fp64 or fp32");
+      else if (p == "amg_fp32") o.precision = NDS_AMG_FP32;
+      else throw Fail("--precision must be fp64, fp32 or amg_fp32");
     } else if (a == "--device") o.device = iv();
     else throw Fail("H8 usage error");
   }
@@ -149,7 +150,7 @@ int run(int argc, char** argv) {
   o.amg_mcgs_order = pick(mcgsOrder, {"symmetric", "forward", "backward"}, "H8 amg-mcgs-order must be symmetric, forward or backward");
   if (coarsening != "pmis") throw Fail("H8 cf-coarsening currently supports pmis");
   if (strength != "classical-negative") throw Fail("H8 cf-strength currently supports classical-negative");
-  const char* prec = o.precision == NDS_FP32 ? "fp32" : "fp64";
+  const char* prec = o.precision == NDS_FP32 ? "fp32" : o.precision == NDS_AMG_FP32 ? "amg_fp32" : "fp64";
 
   const auto t0 = std::chrono::steady_clock::now();
   nds_mesh* M = nullptr;

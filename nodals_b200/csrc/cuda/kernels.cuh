@@ -41,7 +41,7 @@ __device__ __forceinline__ void write_partials(double (&v)[NV], double* part) {
 }
 
 // ---------------------------------------------------------------------------
-// Momentum: fused row-owned assembly (a9 + a10 + a11 + a12)
+// Momentum assembly (a9 + a10 + a11 + a12) in two passes
 //
 //   A[i,:]  = K[i,:] + sum_{(c,a) incident to i} C_c[a,:]           (convection, lagged u)
 //   conv_i  = - sum C_c[a,b] u_fixed(b)                              (Dirichlet columns)
@@ -52,9 +52,68 @@ __device__ __forceinline__ void write_partials(double (&v)[NV], double* part) {
 //      ur[m][j] = sum_d u_d(m) invJ_c[j][d].
 // Reference: h7_momentum_assembly.cuh:16-85, h4_kernels.cuh:10-56,
 // g5e_fp32_kernels.cuh:78-85 and :97-105, h8_precomputed_b.cuh:93-114.
-// One group of 8 lanes owns a row; incident cells are visited in ascending
-// cell order, so every A entry is summed in a fixed order (K first).
+//
+// Pass 1 (mom_cell_conv, cell-owned) evaluates each cell's 8x8 convection
+// block once.  Pass 2 (mom_assemble, row-owned) builds every velocity row in
+// shared memory from K and the blocks of its incident cells, visited in
+// ascending cell order, so every A entry is summed in a fixed order (K
+// first) with no atomics; relaxation, diag, rAU, B^T p and the RHS follow in
+// the same pass.
 // ---------------------------------------------------------------------------
+
+// 8 lanes per cell; lane b computes column b of the cell's block.
+template <class T>
+__global__ void __launch_bounds__(kBlock) mom_cell_conv(int nc, const int32_t* __restrict__ ref,
+                                                        const T* __restrict__ fixed, const T* __restrict__ u0,
+                                                        const T* __restrict__ u1, const T* __restrict__ u2,
+                                                        const T* __restrict__ invJ, const T* __restrict__ det,
+                                                        const T* __restrict__ centT, T* __restrict__ C) {
+  __shared__ T sT[1536];
+  for (int k = threadIdx.x; k < 1536; k += blockDim.x) sT[k] = centT[k];
+  __syncthreads();
+  const int lane8 = threadIdx.x & 7;
+  const int groups = blockDim.x >> 3;
+  const unsigned gmask = group8_mask();
+  for (int c = blockIdx.x * groups + (threadIdx.x >> 3); c < nc; c += gridDim.x * groups) {
+    // lane m: velocity of basis function m of cell c, mapped by J^-1
+    const int gm = ref[8 * (size_t)c + lane8];
+    T q0, q1, q2;
+    if (gm >= 0) {
+      q0 = u0[gm];
+      q1 = u1[gm];
+      q2 = u2[gm];
+    } else {
+      const T* f = fixed + 3 * (size_t)(-gm - 1);
+      q0 = f[0];
+      q1 = f[1];
+      q2 = f[2];
+    }
+    const T* I = invJ + 9 * (size_t)c;
+    const T r0 = q0 * I[0] + q1 * I[1] + q2 * I[2];
+    const T r1 = q0 * I[3] + q1 * I[4] + q2 * I[5];
+    const T r2 = q0 * I[6] + q1 * I[7] + q2 * I[8];
+    T w[8][3];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      w[m][0] = __shfl_sync(gmask, r0, m, 8);
+      w[m][1] = __shfl_sync(gmask, r1, m, 8);
+      w[m][2] = __shfl_sync(gmask, r2, m, 8);
+    }
+    const T dc = det[c];
+    T* out = C + 64 * (size_t)c + lane8;
+#pragma unroll 2
+    for (int a = 0; a < 8; ++a) {
+      T cv = 0;
+#pragma unroll
+      for (int m = 0; m < 8; ++m) {
+        const T* t = sT + ((a * 8 + m) * 8 + lane8) * 3;
+        cv += w[m][0] * t[0] + w[m][1] * t[1] + w[m][2] * t[2];
+      }
+      out[8 * a] = cv * dc;
+    }
+  }
+}
+
 template <class T>
 struct MomArgs {
   int nrows;
@@ -65,8 +124,7 @@ struct MomArgs {
   const uint32_t* __restrict__ inc;     // (cell << 3) | a
   const int32_t* __restrict__ ref;      // 8 per cell
   const uint8_t* __restrict__ slot;     // 64 per cell
-  const T* __restrict__ det;
-  const T* __restrict__ invJ;           // 9 per cell
+  const T* __restrict__ C;              // 64 per cell: convection blocks from mom_cell_conv
   const T* __restrict__ bco;            // 24 per cell
   const T* __restrict__ fixed;          // 3 per fixed slot
   const T* __restrict__ u0;
@@ -76,7 +134,6 @@ struct MomArgs {
   const T* __restrict__ s0;
   const T* __restrict__ s1;
   const T* __restrict__ s2;
-  const T* __restrict__ centT;          // 8*8*8*3 reference convection tensor
   T alpha_u, rau_scale;
   int row_cap;                          // shared row buffer length per group
   T* __restrict__ A;
@@ -88,14 +145,12 @@ struct MomArgs {
   T* __restrict__ b2;
 };
 
+// 8 lanes per velocity row; lane b adds column b of each incident block.
 template <class T>
 __global__ void __launch_bounds__(kBlock) mom_assemble(MomArgs<T> g) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* sT = reinterpret_cast<T*>(smem_raw);                  // 1536
-  T* sRow = sT + 1536;                                     // groups * row_cap
+  T* sRow = reinterpret_cast<T*>(smem_raw);  // groups * row_cap
   const int tid = threadIdx.x;
-  for (int k = tid; k < 1536; k += blockDim.x) sT[k] = g.centT[k];
-  __syncthreads();
   const int lane8 = tid & 7;
   const int grp = tid >> 3;
   const int groups = blockDim.x >> 3;
@@ -106,50 +161,47 @@ __global__ void __launch_bounds__(kBlock) mom_assemble(MomArgs<T> g) {
     for (int k = lane8; k < len; k += 8) buf[k] = g.K[rb + k];
     __syncwarp(gmask);
     T conv0 = 0, conv1 = 0, conv2 = 0, bt0 = 0, bt1 = 0, bt2 = 0;
-    for (int z = g.inc_off[i]; z < g.inc_off[i + 1]; ++z) {
-      const uint32_t pk = g.inc[z];
-      const int c = (int)(pk >> 3), a = (int)(pk & 7u);
-      // lane m: value of basis function m of cell c
-      const int gm = g.ref[8 * (size_t)c + lane8];
-      T q0, q1, q2;
-      if (gm >= 0) {
-        q0 = g.u0[gm];
-        q1 = g.u1[gm];
-        q2 = g.u2[gm];
+    const int z0 = g.inc_off[i], z1 = g.inc_off[i + 1];
+    for (int z = z0; z < z1; z += 2) {
+      // two incidences in flight; applied in order
+      const bool two = z + 1 < z1;
+      const uint32_t pa = g.inc[z], pb = two ? g.inc[z + 1] : pa;
+      const int ca = (int)(pa >> 3), aa = (int)(pa & 7u), cb = (int)(pb >> 3), ab = (int)(pb & 7u);
+      const int ga = g.ref[8 * (size_t)ca + lane8], gb = g.ref[8 * (size_t)cb + lane8];
+      const T va = g.C[64 * (size_t)ca + 8 * aa + lane8], vb = g.C[64 * (size_t)cb + 8 * ab + lane8];
+      const int sa = g.slot[64 * (size_t)ca + 8 * aa + lane8], sb = g.slot[64 * (size_t)cb + 8 * ab + lane8];
+      if (ga >= 0) {
+        buf[sa] += va;
       } else {
-        const T* f = g.fixed + 3 * (size_t)(-gm - 1);
-        q0 = f[0];
-        q1 = f[1];
-        q2 = f[2];
-      }
-      const T* I = g.invJ + 9 * (size_t)c;
-      const T r0 = q0 * I[0] + q1 * I[1] + q2 * I[2];
-      const T r1 = q0 * I[3] + q1 * I[4] + q2 * I[5];
-      const T r2 = q0 * I[6] + q1 * I[7] + q2 * I[8];
-      // lane b: C[a][b]
-      T cv = 0;
-#pragma unroll
-      for (int m = 0; m < 8; ++m) {
-        const T w0 = __shfl_sync(gmask, r0, m, 8);
-        const T w1 = __shfl_sync(gmask, r1, m, 8);
-        const T w2 = __shfl_sync(gmask, r2, m, 8);
-        const T* t = sT + ((a * 8 + m) * 8 + lane8) * 3;
-        cv += w0 * t[0] + w1 * t[1] + w2 * t[2];
-      }
-      cv *= g.det[c];
-      if (gm >= 0) {
-        buf[g.slot[64 * (size_t)c + 8 * a + lane8]] += cv;
-      } else {
-        conv0 -= cv * q0;
-        conv1 -= cv * q1;
-        conv2 -= cv * q2;
+        const T* f = g.fixed + 3 * (size_t)(-ga - 1);
+        conv0 -= va * f[0];
+        conv1 -= va * f[1];
+        conv2 -= va * f[2];
       }
       if (lane8 == 0) {
-        const T pv = g.p[c];
-        const T* B = g.bco + 24 * (size_t)c + 3 * a;
+        const T pv = g.p[ca];
+        const T* B = g.bco + 24 * (size_t)ca + 3 * aa;
         bt0 += B[0] * pv;
         bt1 += B[1] * pv;
         bt2 += B[2] * pv;
+      }
+      __syncwarp(gmask);
+      if (two) {
+        if (gb >= 0) {
+          buf[sb] += vb;
+        } else {
+          const T* f = g.fixed + 3 * (size_t)(-gb - 1);
+          conv0 -= vb * f[0];
+          conv1 -= vb * f[1];
+          conv2 -= vb * f[2];
+        }
+        if (lane8 == 0) {
+          const T pv = g.p[cb];
+          const T* B = g.bco + 24 * (size_t)cb + 3 * ab;
+          bt0 += B[0] * pv;
+          bt1 += B[1] * pv;
+          bt2 += B[2] * pv;
+        }
       }
       __syncwarp(gmask);
     }
@@ -277,67 +329,6 @@ __global__ void __launch_bounds__(kBlock) continuity(int nc, const int32_t* __re
 }
 
 // ---------------------------------------------------------------------------
-// Fine Schur CSR numeric refresh A_p = B diag(rau) B^T (a16).
-// Warp per pressure row.  Contributions were sorted by destination slot at
-// setup (stable, from the reference's (basis, incidence) order of
-// h2b_fine_csr.cuh:480-520), so each value is a sequential sum in the
-// reference's serial order; no atomics.
-// ---------------------------------------------------------------------------
-template <class T>
-__global__ void __launch_bounds__(kBlock) fine_refresh(int nc, const int32_t* __restrict__ row,
-                                                       const int32_t* __restrict__ coff, const uint8_t* __restrict__ cnt,
-                                                       const uint32_t* __restrict__ cpk, const uint8_t* __restrict__ ca,
-                                                       const int32_t* __restrict__ ref, const T* __restrict__ bco,
-                                                       const T* __restrict__ rau, const int32_t* __restrict__ dpos,
-                                                       T* __restrict__ val, T* __restrict__ diag, T* __restrict__ l1) {
-  __shared__ T sB[kWarps][24];
-  __shared__ T sR[kWarps][8];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (c >= nc) return;
-  if (lane < 24) sB[w][lane] = bco[24 * (size_t)c + lane];
-  if (lane < 8) {
-    const int g = ref[8 * (size_t)c + lane];
-    sR[w][lane] = g >= 0 ? rau[g] : T(0);
-  }
-  __syncwarp();
-  const int rb = row[c], re = row[c + 1];
-  int base = coff[c];
-  T asum = 0;
-  for (int k0 = rb; k0 < re; k0 += 32) {
-    const int k = k0 + lane;
-    const int n = k < re ? (int)cnt[k] : 0;
-    // exclusive scan of counts within the chunk
-    int incl = n;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int t = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= o) incl += t;
-    }
-    const int q0 = base + incl - n;
-    T v = 0;
-    for (int q = q0; q < q0 + n; ++q) {
-      const uint32_t pk = cpk[q];
-      const int a = ca[q];
-      const T* bb = bco + 24 * (size_t)(pk >> 3) + 3 * (pk & 7u);
-      const T dot = sB[w][3 * a] * bb[0] + sB[w][3 * a + 1] * bb[1] + sB[w][3 * a + 2] * bb[2];
-      v += sR[w][a] * dot;
-    }
-    if (k < re) {
-      val[k] = v;
-      asum += fabs(v);
-    }
-    base += __shfl_sync(0xffffffffu, incl, 31);
-  }
-  if (l1) {
-    asum = warp_sum(asum);
-    if (lane == 0) l1[c] = asum;
-  }
-  __syncwarp();
-  if (lane == 0) diag[c] = val[dpos[c]];
-}
-
-// ---------------------------------------------------------------------------
 // CSR SpMV family, warp per row (h2b_fine_csr.cuh:579-596, h6_coarse_spmv.cuh:10-32)
 // ---------------------------------------------------------------------------
 template <class T>
@@ -389,24 +380,6 @@ __global__ void __launch_bounds__(kBlock) spmv_smooth(int n, const int32_t* __re
   }
 }
 
-// q = A p with sum p_i q_i partials
-template <class T>
-__global__ void __launch_bounds__(kBlock) spmv_dot(int n, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
-                                                   const T* __restrict__ v, const T* __restrict__ x, T* __restrict__ y,
-                                                   double* __restrict__ part) {
-  double acc[1] = {0.0};
-  const int lane = threadIdx.x & 31;
-  const int warps_total = (gridDim.x * blockDim.x) >> 5;
-  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += warps_total) {
-    const T s = warp_row_dot(rp, ci, v, x, i, lane);
-    if (lane == 0) {
-      y[i] = s;
-      acc[0] += (double)x[i] * (double)s;
-    }
-  }
-  write_partials<1>(acc, part);
-}
-
 // ---------------------------------------------------------------------------
 // vector kernels (g5e_fp32_kernels.cuh:132-150, vector_kernels.cuh)
 // ---------------------------------------------------------------------------
@@ -429,12 +402,6 @@ template <class T>
 __global__ void scale(int n, T s, T* __restrict__ x) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) x[i] *= s;
-}
-// x *= 1 / *nrm (norm from a device scalar holding its square)
-template <class T>
-__global__ void scale_inv_sqrt(int n, const double* __restrict__ sq, T* __restrict__ x) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) x[i] *= T(1.0 / sqrt(*sq));
 }
 template <class T>
 __global__ void div_sqrt(int n, const T* __restrict__ x, const T* __restrict__ d, T* __restrict__ y) {
@@ -459,19 +426,6 @@ __global__ void __launch_bounds__(kBlock) dot(int n, const T* __restrict__ x, co
     acc[0] += (double)x[i] * (double)y[i];
   write_partials<1>(acc, part);
 }
-// partial sums of x.y and y.y
-template <class T>
-__global__ void __launch_bounds__(kBlock) dot2(int n, const T* __restrict__ x, const T* __restrict__ y,
-                                               double* __restrict__ part) {
-  double acc[2] = {0.0, 0.0};
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const double yy = (double)y[i];
-    acc[0] += (double)x[i] * yy;
-    acc[1] += yy * yy;
-  }
-  write_partials<2>(acc, part);
-}
-
 // x += a p; r -= a q; partial r.r.  a = alpha_dev ? *alpha_dev : alpha
 template <class T>
 __global__ void __launch_bounds__(kBlock) xr_update(int n, double alpha, const double* __restrict__ alpha_dev,
@@ -520,16 +474,6 @@ __global__ void pcg_beta(double* __restrict__ sc, int* __restrict__ flags) {
 // ---------------------------------------------------------------------------
 // transfers and terminal solve (g5e_fp32_kernels.cuh:140-150)
 // ---------------------------------------------------------------------------
-// c = P^T f as a gather over R = P^T (one thread per coarse row)
-template <class T>
-__global__ void restrict_gather(int nc, const int32_t* __restrict__ rr, const int32_t* __restrict__ rc,
-                                const T* __restrict__ rv, const T* __restrict__ f, T* __restrict__ c) {
-  const int I = blockIdx.x * blockDim.x + threadIdx.x;
-  if (I >= nc) return;
-  T s = 0;
-  for (int k = rr[I]; k < rr[I + 1]; ++k) s += rv[k] * f[rc[k]];
-  c[I] = s;
-}
 // f += P c (one thread per fine row)
 template <class T>
 __global__ void prolong_add(int nf, const int32_t* __restrict__ pr, const int32_t* __restrict__ pc,
@@ -670,15 +614,25 @@ __global__ void __launch_bounds__(kBlock) sell_spmv(Sell A, const T* __restrict_
   }
 }
 
-// Fine Schur refresh into the SELL layout (same arithmetic as fine_refresh).
-template <class T>
-__global__ void __launch_bounds__(kBlock) sell_refresh(int nc, const int32_t* __restrict__ row,
-                                                       const int32_t* __restrict__ coff, const uint8_t* __restrict__ cnt,
-                                                       const uint32_t* __restrict__ cpk, const uint8_t* __restrict__ ca,
-                                                       const int32_t* __restrict__ ref, const T* __restrict__ bco,
-                                                       const T* __restrict__ rau, const int32_t* __restrict__ dslot,
-                                                       const int32_t* __restrict__ sbase, T* __restrict__ val,
-                                                       T* __restrict__ diag, T* __restrict__ l1) {
+// Fine Schur numeric refresh A_p = B diag(rau) B^T (h8_precomputed_b.cuh:37-91),
+// warp per pressure row, written into the SELL layout.  The directed
+// contributions of a row were sorted by destination slot at setup (stable,
+// from the reference's (basis, incidence) order of h2b_fine_csr.cuh:480-520).
+// Lanes take one contribution each (32 independent gathers in flight), then
+// every slot is summed sequentially in that order by a shuffle chain: lane L
+// adds its product to the final running sum of lane L-1 when both belong to
+// the same slot, so each value is the reference's serial sum; no atomics.
+// Slots are written by the lane holding their last contribution.  Values go
+// to val (operator precision T) and, in the mixed mode, also to valA (AMG
+// precision TA); the diagonal and L1 row sums feed the AMG smoothers.
+template <class T, class TA>
+__global__ void __launch_bounds__(kBlock) sell_refresh(int nc, const int32_t* __restrict__ coff,
+                                                       const uint8_t* __restrict__ csl, const uint32_t* __restrict__ cpk,
+                                                       const uint8_t* __restrict__ ca, const int32_t* __restrict__ ref,
+                                                       const T* __restrict__ bco, const T* __restrict__ rau,
+                                                       const int32_t* __restrict__ dslot, const int32_t* __restrict__ sbase,
+                                                       T* __restrict__ val, TA* __restrict__ valA, TA* __restrict__ diag,
+                                                       TA* __restrict__ l1) {
   __shared__ T sB[kWarps][24];
   __shared__ T sR[kWarps][8];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -690,39 +644,64 @@ __global__ void __launch_bounds__(kBlock) sell_refresh(int nc, const int32_t* __
     sR[w][lane] = g >= 0 ? rau[g] : T(0);
   }
   __syncwarp();
-  const int rb = row[c], re = row[c + 1];
+  const int qb = coff[c], qe = coff[c + 1];
   const int out = sbase[c >> 5] + (c & 31);
-  int base = coff[c];
-  T asum = 0;
-  for (int k0 = rb; k0 < re; k0 += 32) {
-    const int k = k0 + lane;
-    const int n = k < re ? (int)cnt[k] : 0;
-    int incl = n;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int t = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= o) incl += t;
-    }
-    const int q0 = base + incl - n;
-    T v = 0;
-    for (int q = q0; q < q0 + n; ++q) {
+  const int ds = dslot[c];
+  T asum = 0, carry = 0;
+  int carry_slot = -1;
+  const unsigned below = (1u << lane) - 1u;
+  for (int q0 = qb; q0 < qe; q0 += 32) {
+    const int q = q0 + lane;
+    const bool live = q < qe;
+    int sl = -1;
+    T p = 0;
+    if (live) {
       const uint32_t pk = cpk[q];
       const int a = ca[q];
+      sl = csl[q];
       const T* bb = bco + 24 * (size_t)(pk >> 3) + 3 * (pk & 7u);
       const T dot = sB[w][3 * a] * bb[0] + sB[w][3 * a + 1] * bb[1] + sB[w][3 * a + 2] * bb[2];
-      v += sR[w][a] * dot;
+      p = sR[w][a] * dot;
     }
-    if (k < re) {
-      val[out + 32 * (k - rb)] = v;
-      asum += fabs(v);
-      if (k - rb == dslot[c]) diag[c] = v;
+    const int prev = __shfl_up_sync(0xffffffffu, sl, 1);
+    const int next = __shfl_down_sync(0xffffffffu, sl, 1);
+    // lane 31's run continues into the next chunk when the next contribution
+    // has the same slot
+    const bool cont = lane == 31 && live && q + 1 < qe && (int)csl[q + 1] == sl;
+    const bool head = !live || (lane == 0 ? sl != carry_slot : sl != prev);
+    const bool tail = live && (lane == 31 ? !cont : next != sl);
+    const unsigned heads = __ballot_sync(0xffffffffu, head) | 1u;
+    // position of this lane inside its slot's run within this chunk
+    const int pos = lane - (31 - __clz(heads & (below | (1u << lane))));
+    T acc = (lane == 0 && !head) ? carry + p : p;
+    int maxpos = pos;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) maxpos = max(maxpos, __shfl_xor_sync(0xffffffffu, maxpos, o));
+    for (int j = 1; j <= maxpos; ++j) {
+      const T up = __shfl_up_sync(0xffffffffu, acc, 1);
+      if (pos == j) acc = up + p;
     }
-    base += __shfl_sync(0xffffffffu, incl, 31);
+    if (tail) {
+      const size_t o = (size_t)out + 32 * (size_t)sl;
+      val[o] = acc;
+      if (valA) valA[o] = TA(acc);
+      if (sl == ds) diag[c] = TA(acc);
+      asum += fabs(acc);
+    }
+    // a slot run cut by the chunk end continues from lane 31's running sum
+    carry = __shfl_sync(0xffffffffu, acc, 31);
+    carry_slot = __shfl_sync(0xffffffffu, sl, 31);
   }
   if (l1) {
     asum = warp_sum(asum);
-    if (lane == 0) l1[c] = asum;
+    if (lane == 0) l1[c] = TA(asum);
   }
+}
+
+template <class Tin, class Tout>
+__global__ void cast_copy(int n, const Tin* __restrict__ a, Tout* __restrict__ b) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) b[i] = Tout(a[i]);
 }
 
 // multicolour GS colour pass on the SELL fine operator (thread per row)

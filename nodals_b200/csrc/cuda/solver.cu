@@ -193,19 +193,24 @@ double cheb_root(double hi, double lo, int k, int degree) {
 
 }  // namespace
 
-template <class T>
+// T: state, momentum and pressure-operator precision (and the outer Krylov
+// vectors); TA: precision of the AMG V-cycle (levels, transfers, smoothers,
+// fine-level copy of the operator).  T == TA for the FP64 and FP32 modes;
+// the mixed mode runs an FP32 V-cycle inside FP64 PCG.
+template <class T, class TA>
 class Solver final : public ISolver {
  public:
+  static constexpr bool kSame = std::is_same<T, TA>::value;
   struct Level {  // explicit AMG level
     int n = 0;
     DBuf<int32_t> row, col, crows;
     std::vector<int> coff;
-    DBuf<T> val, diag, l1, b, x, r, tmp, corr, pong;
+    DBuf<TA> val, diag, l1, b, x, r, tmp, corr, pong;
   };
   struct Xfer {  // P (fine rows) and R = P^T (coarse rows)
     int nf = 0, nc = 0;
     DBuf<int32_t> prow, pcol, rrow, rcol;
-    DBuf<T> pval, rval;
+    DBuf<TA> pval, rval;
   };
 
   Solver(const Problem& P) : P_(P), o_(P.opt) {
@@ -264,16 +269,16 @@ class Solver final : public ISolver {
     row_cap_ = 8;
     for (int i = 0; i < nv_; ++i) row_cap_ = std::max<int>(row_cap_, (int)(S.mom.row[(size_t)i + 1] - S.mom.row[(size_t)i]));
     row_cap_ = (row_cap_ + 7) / 8 * 8;
-    mom_smem_ = (1536 + (size_t)(kBlock / 8) * row_cap_) * sizeof(T);
+    mom_smem_ = (size_t)(kBlock / 8) * row_cap_ * sizeof(T);
     if (mom_smem_ > 200 * 1024) throw std::runtime_error("momentum row too long for the shared-memory assembly buffer");
     NDS_CUDA(cudaFuncSetAttribute(k::mom_assemble<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mom_smem_));
+    cconv_.alloc(64 * (size_t)nc_);
 
     // fine Schur CSR with contributions regrouped by destination slot
     const FineTopo& F = S.fine;
-    frow_.upload(F.row);  // CSR offsets index the per-entry contribution counts
     fcoff_.upload(F.contrib_off);
     {
-      std::vector<uint8_t> cnt(F.col.size(), 0), ca(F.slot.size());
+      std::vector<uint8_t> cnt(F.col.size(), 0), ca(F.slot.size()), csl(F.slot.size());
       std::vector<uint32_t> cpk(F.slot.size());
       std::vector<int32_t> cur;
       for (int c = 0; c < nc_; ++c) {
@@ -284,6 +289,7 @@ class Solver final : public ISolver {
           if (cnt[(size_t)rb + F.slot[(size_t)q]] == 255) throw std::runtime_error("more than 255 contributions to one fine entry");
           ++cnt[(size_t)rb + F.slot[(size_t)q]];
         }
+        if (cnt[(size_t)F.diag_pos[(size_t)c]] == 0) throw std::runtime_error("fine Schur row without a diagonal contribution");
         cur.assign((size_t)len + 1, 0);
         for (int s = 0; s < len; ++s) cur[(size_t)s + 1] = cur[(size_t)s] + cnt[(size_t)rb + s];
         int q = q0;
@@ -294,10 +300,11 @@ class Solver final : public ISolver {
             const int pos = q0 + cur[(size_t)F.slot[(size_t)q]]++;
             cpk[(size_t)pos] = F.packed[(size_t)k];
             ca[(size_t)pos] = (uint8_t)a;
+            csl[(size_t)pos] = F.slot[(size_t)q];
           }
         }
       }
-      fcnt_.upload(cnt);
+      fcsl_.upload(csl);
       fca_.upload(ca);
       fcpk_.upload(cpk);
     }
@@ -331,6 +338,10 @@ class Solver final : public ISolver {
       fdslot_.upload(dslot);
       fval_.alloc(scol.size());
       NDS_CUDA(cudaMemset(fval_.p, 0, fval_.bytes()));
+      if (!kSame) {
+        fvalA_.alloc(scol.size());
+        NDS_CUDA(cudaMemset(fvalA_.p, 0, fvalA_.bytes()));
+      }
       // 16-bit column deltas when the ordering keeps every |column - row| < 2^15
       bool fits = true;
       std::vector<int16_t> dcol(scol.size());
@@ -360,7 +371,12 @@ class Solver final : public ISolver {
       greedy_color(nc_, F.row, F.col, rows, fine_coff_);
       fine_crows_.upload(rows);
     }
-    for (auto* b : {&x_, &r_, &z_, &pp_, &q_, &rhs_, &fr_, &ftmp_, &fcorr_, &frhs_, &fpong_}) b->alloc((size_t)nc_);
+    for (auto* b : {&x_, &r_, &z_, &pp_, &q_, &rhs_}) b->alloc((size_t)nc_);
+    for (auto* b : {&fr_, &ftmp_, &fcorr_, &frhs_, &fpong_}) b->alloc((size_t)nc_);
+    if (!kSame) {
+      rA_.alloc((size_t)nc_);
+      zA_.alloc((size_t)nc_);
+    }
 
     // AMG levels and transfers
     L_.resize(H.A.size());
@@ -482,10 +498,23 @@ class Solver final : public ISolver {
   }
   bool use_graphs_ = std::getenv("NDS_NO_GRAPHS") == nullptr;
   Graph g_amg_, g_pcg2_;
+  // z = M b with b, z in the state precision (casts around the V-cycle in
+  // the mixed mode)
+  void amg_T(const T* b, T* z) {
+    if constexpr (kSame) {
+      amg_apply(b, z);
+    } else {
+      k::cast_copy<T, TA><<<grid_for(nc_), kBlock, 0, st_>>>(nc_, b, rA_.p);
+      NDS_LAUNCH();
+      amg_apply(rA_.p, zA_.p);
+      k::cast_copy<TA, T><<<grid_for(nc_), kBlock, 0, st_>>>(nc_, zA_.p, z);
+      NDS_LAUNCH();
+    }
+  }
   // z = M r on the solver's fixed PCG buffers, replayed from a graph
   void amg_rz() {
-    if (!use_graphs_) return amg_apply(r_.p, z_.p);
-    if (!g_amg_.exec) capture(g_amg_, [&] { amg_apply(r_.p, z_.p); });
+    if (!use_graphs_) return amg_T(r_.p, z_.p);
+    if (!g_amg_.exec) capture(g_amg_, [&] { amg_T(r_.p, z_.p); });
     replay(g_amg_);
   }
 
@@ -499,78 +528,85 @@ class Solver final : public ISolver {
     NDS_CUDA(cudaMemcpyAsync(hsc_ + first, sc_.p + first, sizeof(double) * count, cudaMemcpyDeviceToHost, st_));
     NDS_CUDA(cudaStreamSynchronize(st_));
   }
-  double dot_fetch(const T* x, const T* y, int n, int slot) {
+  template <class V>
+  double dot_fetch(const V* x, const V* y, int n, int slot) {
     const int g = red_grid(n);
-    k::dot<T><<<g, kBlock, 0, st_>>>(n, x, y, part_.p);
+    k::dot<V><<<g, kBlock, 0, st_>>>(n, x, y, part_.p);
     NDS_LAUNCH();
     reduce_to<1>(g, slot);
     fetch(slot, 1);
     return hsc_[slot];
   }
-  void dot_dev(const T* x, const T* y, int n, int slot) {
+  template <class V>
+  void dot_dev(const V* x, const V* y, int n, int slot) {
     const int g = red_grid(n);
-    k::dot<T><<<g, kBlock, 0, st_>>>(n, x, y, part_.p);
+    k::dot<V><<<g, kBlock, 0, st_>>>(n, x, y, part_.p);
     NDS_LAUNCH();
     reduce_to<1>(g, slot);
   }
 
   // operator view: the fine Schur matrix in SELL-32, AMG levels in CSR
+  template <class V>
   struct OpView {
     int n;
     bool sell;
     k::Sell s;
     const int32_t* rp;
     const int32_t* ci;
-    const T* v;
+    const V* v;
   };
-  template <int MODE>
-  void sell_launch(const OpView& A, int grid, const T* x, const T* b, const T* den, double w, T* y, T* y2) {
+  template <int MODE, class V>
+  void sell_launch(const OpView<V>& A, int grid, const V* x, const V* b, const V* den, double w, V* y, V* y2) {
     if (A.s.dcol)
-      k::sell_spmv<T, MODE, true><<<grid, kBlock, 0, st_>>>(A.s, A.v, x, b, den, T(w), y, y2, part_.p);
+      k::sell_spmv<V, MODE, true><<<grid, kBlock, 0, st_>>>(A.s, A.v, x, b, den, V(w), y, y2, part_.p);
     else
-      k::sell_spmv<T, MODE, false><<<grid, kBlock, 0, st_>>>(A.s, A.v, x, b, den, T(w), y, y2, part_.p);
+      k::sell_spmv<V, MODE, false><<<grid, kBlock, 0, st_>>>(A.s, A.v, x, b, den, V(w), y, y2, part_.p);
   }
-  OpView fine_op() const { return {nc_, true, sell_, nullptr, nullptr, fval_.p}; }
-  OpView level_op(const Level& A) const { return {A.n, false, k::Sell{}, A.row.p, A.col.p, A.val.p}; }
-  void op_spmv(const OpView& A, const T* x, T* y) {
+  // physical operator (precision T) and the AMG's fine operator (precision TA)
+  OpView<T> fine_op() const { return {nc_, true, sell_, nullptr, nullptr, fval_.p}; }
+  OpView<TA> fine_opA() const {
+    if constexpr (kSame) return {nc_, true, sell_, nullptr, nullptr, fval_.p};
+    else return {nc_, true, sell_, nullptr, nullptr, fvalA_.p};
+  }
+  OpView<TA> level_op(const Level& A) const { return {A.n, false, k::Sell{}, A.row.p, A.col.p, A.val.p}; }
+  template <class V>
+  void op_spmv(const OpView<V>& A, const V* x, V* y) {
     ProfScope ps(prof, st_, A.sell ? P_FINE_SPMV : P_COARSE_SPMV);
-    if (A.sell) sell_launch<k::SELL_Y>(A, grid_for(A.n), x, nullptr, nullptr, 0.0, y, nullptr);
-    else k::spmv<T><<<grid_for((long long)A.n * 32), kBlock, 0, st_>>>(A.n, A.rp, A.ci, A.v, x, y);
+    if (A.sell) sell_launch<k::SELL_Y, V>(A, grid_for(A.n), x, nullptr, nullptr, 0.0, y, nullptr);
+    else k::spmv<V><<<grid_for((long long)A.n * 32), kBlock, 0, st_>>>(A.n, A.rp, A.ci, A.v, x, y);
     NDS_LAUNCH();
   }
-  void op_resid(const OpView& A, const T* x, const T* b, T* r, T* r2 = nullptr) {
+  template <class V>
+  void op_resid(const OpView<V>& A, const V* x, const V* b, V* r, V* r2 = nullptr) {
     ProfScope ps(prof, st_, A.sell ? P_FINE_SPMV : P_COARSE_SPMV);
-    if (A.sell) sell_launch<k::SELL_RESID>(A, grid_for(A.n), x, b, nullptr, 0.0, r, r2);
-    else k::spmv_resid<T><<<grid_for((long long)A.n * 32), kBlock, 0, st_>>>(A.n, A.rp, A.ci, A.v, x, b, r, r2);
+    if (A.sell) sell_launch<k::SELL_RESID, V>(A, grid_for(A.n), x, b, nullptr, 0.0, r, r2);
+    else k::spmv_resid<V><<<grid_for((long long)A.n * 32), kBlock, 0, st_>>>(A.n, A.rp, A.ci, A.v, x, b, r, r2);
     NDS_LAUNCH();
   }
-  void op_smooth(const OpView& A, const T* xin, const T* b, const T* den, double w, T* xout) {
+  template <class V>
+  void op_smooth(const OpView<V>& A, const V* xin, const V* b, const V* den, double w, V* xout) {
     ProfScope ps(prof, st_, A.sell ? P_FINE_SPMV : P_COARSE_SPMV);
-    if (A.sell) sell_launch<k::SELL_SMOOTH>(A, grid_for(A.n), xin, b, den, w, xout, nullptr);
-    else k::spmv_smooth<T><<<grid_for((long long)A.n * 32), kBlock, 0, st_>>>(A.n, A.rp, A.ci, A.v, xin, b, den, T(w), xout);
+    if (A.sell) sell_launch<k::SELL_SMOOTH, V>(A, grid_for(A.n), xin, b, den, w, xout, nullptr);
+    else k::spmv_smooth<V><<<grid_for((long long)A.n * 32), kBlock, 0, st_>>>(A.n, A.rp, A.ci, A.v, xin, b, den, V(w), xout);
     NDS_LAUNCH();
   }
-  // CSR helpers kept for coarse-level code paths
-  void spmv(int n, const int32_t* rp, const int32_t* ci, const T* v, const T* x, T* y) {
-    op_spmv(OpView{n, false, k::Sell{}, rp, ci, v}, x, y);
-  }
-  void resid(int n, const int32_t* rp, const int32_t* ci, const T* v, const T* x, const T* b, T* r, T* r2 = nullptr) {
-    op_resid(OpView{n, false, k::Sell{}, rp, ci, v}, x, b, r, r2);
-  }
-  void vcopy(int n, const T* a, T* b) {
-    k::copy<T><<<grid_for(n), kBlock, 0, st_>>>(n, a, b);
+  template <class V>
+  void vcopy(int n, const V* a, V* b) {
+    k::copy<V><<<grid_for(n), kBlock, 0, st_>>>(n, a, b);
     NDS_LAUNCH();
   }
-  void vaxpy(int n, double a, const T* x, T* y) {
-    k::axpy<T><<<grid_for(n), kBlock, 0, st_>>>(n, T(a), x, y);
+  template <class V>
+  void vaxpy(int n, double a, const V* x, V* y) {
+    k::axpy<V><<<grid_for(n), kBlock, 0, st_>>>(n, V(a), x, y);
     NDS_LAUNCH();
   }
 
   // fine Schur operator
   void refresh_fine(const T* rau) {
     ProfScope ps(prof, st_, P_REFRESH);
-    k::sell_refresh<T><<<grid_for((long long)nc_ * 32), kBlock, 0, st_>>>(
-        nc_, frow_.p, fcoff_.p, fcnt_.p, fcpk_.p, fca_.p, ref_.p, bco_.p, rau, fdslot_.p, sbase_.p, fval_.p, fdiag_.p, fl1_.p);
+    k::sell_refresh<T, TA><<<grid_for((long long)nc_ * 32), kBlock, 0, st_>>>(
+        nc_, fcoff_.p, fcsl_.p, fcpk_.p, fca_.p, ref_.p, bco_.p, rau, fdslot_.p, sbase_.p, fval_.p,
+        kSame ? nullptr : fvalA_.p, fdiag_.p, fl1_.p);
     NDS_LAUNCH();
   }
   void fine_apply(const T* x, T* y) { op_spmv(fine_op(), x, y); }
@@ -578,27 +614,27 @@ class Solver final : public ISolver {
   // ------------------------------------------------------------- smoothers
   // x = S(b) from a zero initial guess.  Jacobi-type steps write to a second
   // buffer (xin is read by every row), then the result is copied back.
-  void poly_smooth(const OpView& A, const T* diag, const T* b, T* x, T* pong, double lambda, bool cheb,
-                   const T* den_jac, int sweeps) {
+  void poly_smooth(const OpView<TA>& A, const TA* diag, const TA* b, TA* x, TA* pong, double lambda, bool cheb,
+                   const TA* den_jac, int sweeps) {
     // x = S(b) from a zero guess: one diagonal step, then m Jacobi-type steps
     // ping-ponging between two buffers; the first buffer is chosen by the
     // parity of m so that the last step writes x (no copy-back).
     const int n = A.n;
     const int deg = o_.amg_cheb_degree;
     const int m = cheb ? deg - 1 : sweeps - 1;
-    T* cur = (m % 2 == 0) ? x : pong;
-    T* nxt = (m % 2 == 0) ? pong : x;
+    TA* cur = (m % 2 == 0) ? x : pong;
+    TA* nxt = (m % 2 == 0) ? pong : x;
     if (cheb) {
       const double lo = o_.amg_lambda_low_fraction * lambda;
       if (!(lambda > lo && lo > 0)) throw SolveFailure(NDS_E_BREAKDOWN, "Chebyshev smoother interval invalid");
-      k::jacobi_zero<T><<<grid_for(n), kBlock, 0, st_>>>(n, T(1.0 / cheb_root(lambda, lo, 0, deg)), b, diag, cur);
+      k::jacobi_zero<TA><<<grid_for(n), kBlock, 0, st_>>>(n, TA(1.0 / cheb_root(lambda, lo, 0, deg)), b, diag, cur);
       NDS_LAUNCH();
       for (int kk = 1; kk < deg; ++kk) {
         op_smooth(A, cur, b, diag, 1.0 / cheb_root(lambda, lo, kk, deg), nxt);
         std::swap(cur, nxt);
       }
     } else {
-      k::jacobi_zero<T><<<grid_for(n), kBlock, 0, st_>>>(n, T(o_.amg_jacobi_omega), b, den_jac, cur);
+      k::jacobi_zero<TA><<<grid_for(n), kBlock, 0, st_>>>(n, TA(o_.amg_jacobi_omega), b, den_jac, cur);
       NDS_LAUNCH();
       for (int q = 1; q < sweeps; ++q) {
         op_smooth(A, cur, b, den_jac, o_.amg_jacobi_omega, nxt);
@@ -606,10 +642,10 @@ class Solver final : public ISolver {
       }
     }
   }
-  void mcgs(const OpView& A, const T* diag, const T* b, T* x, const DBuf<int32_t>& crows, const std::vector<int>& coff,
-            int sweeps) {
+  void mcgs(const OpView<TA>& A, const TA* diag, const TA* b, TA* x, const DBuf<int32_t>& crows,
+            const std::vector<int>& coff, int sweeps) {
     const int n = A.n;
-    NDS_CUDA(cudaMemsetAsync(x, 0, sizeof(T) * (size_t)n, st_));
+    NDS_CUDA(cudaMemsetAsync(x, 0, sizeof(TA) * (size_t)n, st_));
     const int ncol = (int)coff.size() - 1;
     auto pass = [&](bool reverse) {
       for (int qq = 0; qq < ncol; ++qq) {
@@ -617,14 +653,14 @@ class Solver final : public ISolver {
         const int cnt = coff[(size_t)c + 1] - coff[(size_t)c];
         if (cnt <= 0) continue;
         if (A.sell && A.s.dcol)
-          k::sell_gs_color<T, true><<<grid_for(cnt), kBlock, 0, st_>>>(cnt, crows.p + coff[(size_t)c], A.s, A.v, diag, b,
-                                                                    x, T(o_.amg_mcgs_omega));
+          k::sell_gs_color<TA, true><<<grid_for(cnt), kBlock, 0, st_>>>(cnt, crows.p + coff[(size_t)c], A.s, A.v, diag, b,
+                                                                     x, TA(o_.amg_mcgs_omega));
         else if (A.sell)
-          k::sell_gs_color<T, false><<<grid_for(cnt), kBlock, 0, st_>>>(cnt, crows.p + coff[(size_t)c], A.s, A.v, diag, b,
-                                                                     x, T(o_.amg_mcgs_omega));
+          k::sell_gs_color<TA, false><<<grid_for(cnt), kBlock, 0, st_>>>(cnt, crows.p + coff[(size_t)c], A.s, A.v, diag,
+                                                                      b, x, TA(o_.amg_mcgs_omega));
         else
-          k::amg_gs_color<T><<<grid_for((long long)cnt * 32), kBlock, 0, st_>>>(cnt, crows.p + coff[(size_t)c], A.rp, A.ci,
-                                                                               A.v, diag, b, x, T(o_.amg_mcgs_omega));
+          k::amg_gs_color<TA><<<grid_for((long long)cnt * 32), kBlock, 0, st_>>>(cnt, crows.p + coff[(size_t)c], A.rp, A.ci,
+                                                                                A.v, diag, b, x, TA(o_.amg_mcgs_omega));
         NDS_LAUNCH();
       }
     };
@@ -634,115 +670,117 @@ class Solver final : public ISolver {
       else { pass(false); pass(true); }
     }
   }
-  void smooth_fine(const T* b, T* x) {
+  void smooth_fine(const TA* b, TA* x) {
     const int sm = o_.amg_smoother;
     if (sm == NDS_SM_MCGS) {
-      mcgs(fine_op(), fdiag_.p, b, x, fine_crows_, fine_coff_, o_.amg_mcgs_fine_sweeps);
+      mcgs(fine_opA(), fdiag_.p, b, x, fine_crows_, fine_coff_, o_.amg_mcgs_fine_sweeps);
       return;
     }
-    const T* den = sm == NDS_SM_L1JACOBI ? fl1_.p : fdiag_.p;
-    poly_smooth(fine_op(), fdiag_.p, b, x, fpong_.p, fine_lambda_, sm == NDS_SM_CHEB2, den, o_.amg_jacobi_fine_sweeps);
+    const TA* den = sm == NDS_SM_L1JACOBI ? fl1_.p : fdiag_.p;
+    poly_smooth(fine_opA(), fdiag_.p, b, x, fpong_.p, fine_lambda_, sm == NDS_SM_CHEB2, den, o_.amg_jacobi_fine_sweeps);
   }
-  void smooth_level(Level& A, const T* b, T* x, double lambda) {
+  void smooth_level(Level& A, const TA* b, TA* x, double lambda) {
     const int sm = o_.amg_smoother;
     if (sm == NDS_SM_MCGS) {
       mcgs(level_op(A), A.diag.p, b, x, A.crows, A.coff, o_.amg_mcgs_coarse_sweeps);
       return;
     }
-    const T* den = sm == NDS_SM_L1JACOBI ? A.l1.p : A.diag.p;
+    const TA* den = sm == NDS_SM_L1JACOBI ? A.l1.p : A.diag.p;
     poly_smooth(level_op(A), A.diag.p, b, x, A.pong.p, lambda, sm == NDS_SM_CHEB2, den, o_.amg_jacobi_coarse_sweeps);
   }
-  void restrict_to(const Xfer& X, const T* f, T* c) {
+  void restrict_to(const Xfer& X, const TA* f, TA* c) {
     ProfScope ps(prof, st_, P_TRANSFER);
-    k::restrict_warp<T><<<grid_for((long long)X.nc * 32), kBlock, 0, st_>>>(X.nc, X.rrow.p, X.rcol.p, X.rval.p, f, c);
+    k::restrict_warp<TA><<<grid_for((long long)X.nc * 32), kBlock, 0, st_>>>(X.nc, X.rrow.p, X.rcol.p, X.rval.p, f, c);
     NDS_LAUNCH();
   }
-  void prolong(const Xfer& X, const T* c, T* f) {
+  void prolong(const Xfer& X, const TA* c, TA* f) {
     ProfScope ps(prof, st_, P_TRANSFER);
-    k::prolong_add<T><<<grid_for(X.nf), kBlock, 0, st_>>>(X.nf, X.prow.p, X.pcol.p, X.pval.p, c, f);
+    k::prolong_add<TA><<<grid_for(X.nf), kBlock, 0, st_>>>(X.nf, X.prow.p, X.pcol.p, X.pval.p, c, f);
     NDS_LAUNCH();
   }
 
   // -------------------------------------------------------------- V-cycle
-  void vcycle(int l, const T* b, T* x) {
+  void vcycle(int l, const TA* b, TA* x) {
     Level& A = L_[(size_t)l];
     if (l == (int)L_.size() - 1) {
       ProfScope ps(prof, st_, P_TERMINAL);
-      k::dense_mv<T><<<grid_for((long long)A.n * 32), kBlock, 0, st_>>>(A.n, tinv_.p, b, x);
+      k::dense_mv<TA><<<grid_for((long long)A.n * 32), kBlock, 0, st_>>>(A.n, tinv_.p, b, x);
       NDS_LAUNCH();
       return;
     }
     smooth_level(A, b, x, level_lambda_[(size_t)l]);
-    resid(A.n, A.row.p, A.col.p, A.val.p, x, b, A.r.p);
+    op_resid(level_op(A), x, b, A.r.p);
     Level& C = L_[(size_t)l + 1];
     restrict_to(X_[(size_t)l + 1], A.r.p, C.b.p);
     vcycle(l + 1, C.b.p, C.x.p);
     prolong(X_[(size_t)l + 1], C.x.p, x);
     // r = b - A x, then the post-smoother solves A corr = r (b is no longer needed)
-    resid(A.n, A.row.p, A.col.p, A.val.p, x, b, A.r.p, A.b.p);
+    op_resid(level_op(A), x, b, A.r.p, A.b.p);
     smooth_level(A, A.b.p, A.corr.p, level_lambda_[(size_t)l]);
     vaxpy(A.n, 1.0, A.corr.p, x);
   }
-  void amg_apply(const T* b, T* z) {
+  void amg_apply(const TA* b, TA* z) {
     smooth_fine(b, z);
-    op_resid(fine_op(), z, b, fr_.p);
+    op_resid(fine_opA(), z, b, fr_.p);
     Level& C = L_[0];
     restrict_to(X_[0], fr_.p, C.b.p);
     vcycle(0, C.b.p, C.x.p);
     prolong(X_[0], C.x.p, z);
-    op_resid(fine_op(), z, b, fr_.p, frhs_.p);
+    op_resid(fine_opA(), z, b, fr_.p, frhs_.p);
     smooth_fine(frhs_.p, fcorr_.p);
     vaxpy(nc_, 1.0, fcorr_.p, z);
   }
 
   // ------------------------------------------------------ spectrum estimates
   double power_fine(int its, double safety) {
-    T* v = fcorr_.p;
-    T* u = frhs_.p;
-    T* au = ftmp_.p;
-    T* w = fr_.p;
-    k::power_init<T><<<grid_for(nc_), kBlock, 0, st_>>>(nc_, v);
+    TA* v = fcorr_.p;
+    TA* u = frhs_.p;
+    TA* au = ftmp_.p;
+    TA* w = fr_.p;
+    k::power_init<TA><<<grid_for(nc_), kBlock, 0, st_>>>(nc_, v);
     NDS_LAUNCH();
-    const double vn = std::sqrt(dot_fetch(v, v, nc_, S_TMP));
-    k::scale<T><<<grid_for(nc_), kBlock, 0, st_>>>(nc_, T(1.0 / vn), v);
+    const double vn = std::sqrt(dot_fetch((const TA*)v, (const TA*)v, nc_, S_TMP));
+    k::scale<TA><<<grid_for(nc_), kBlock, 0, st_>>>(nc_, TA(1.0 / vn), v);
     NDS_LAUNCH();
     double ray = 0.0;
     for (int it = 0; it < its; ++it) {
-      k::div_sqrt<T><<<grid_for(nc_), kBlock, 0, st_>>>(nc_, v, fdiag_.p, u);
-      fine_apply(u, au);
-      k::div_sqrt<T><<<grid_for(nc_), kBlock, 0, st_>>>(nc_, au, fdiag_.p, w);
+      k::div_sqrt<TA><<<grid_for(nc_), kBlock, 0, st_>>>(nc_, v, fdiag_.p, u);
+      op_spmv(fine_opA(), (const TA*)u, au);
+      k::div_sqrt<TA><<<grid_for(nc_), kBlock, 0, st_>>>(nc_, au, fdiag_.p, w);
       NDS_LAUNCH();
-      const double num = dot_fetch(v, w, nc_, S_TMP), den = dot_fetch(v, v, nc_, S_TMP2);
+      const double num = dot_fetch((const TA*)v, (const TA*)w, nc_, S_TMP),
+                   den = dot_fetch((const TA*)v, (const TA*)v, nc_, S_TMP2);
       ray = num / std::max(den, 1e-300);
-      const double wn = std::sqrt(dot_fetch(w, w, nc_, S_TMP));
+      const double wn = std::sqrt(dot_fetch((const TA*)w, (const TA*)w, nc_, S_TMP));
       if (!(ray > 0.0) || !(wn > 0.0) || !std::isfinite(ray) || !std::isfinite(wn))
         throw SolveFailure(NDS_E_BREAKDOWN, "fine GPU power iteration failed");
-      vcopy(nc_, w, v);
-      k::scale<T><<<grid_for(nc_), kBlock, 0, st_>>>(nc_, T(1.0 / wn), v);
+      vcopy(nc_, (const TA*)w, v);
+      k::scale<TA><<<grid_for(nc_), kBlock, 0, st_>>>(nc_, TA(1.0 / wn), v);
       NDS_LAUNCH();
     }
     return safety * ray;
   }
   double power_level(Level& A, int its, double safety) {
     const int n = A.n;
-    k::power_init<T><<<grid_for(n), kBlock, 0, st_>>>(n, A.corr.p);
+    k::power_init<TA><<<grid_for(n), kBlock, 0, st_>>>(n, A.corr.p);
     NDS_LAUNCH();
-    const double vn = std::sqrt(dot_fetch(A.corr.p, A.corr.p, n, S_TMP));
-    k::scale<T><<<grid_for(n), kBlock, 0, st_>>>(n, T(1.0 / vn), A.corr.p);
+    const double vn = std::sqrt(dot_fetch((const TA*)A.corr.p, (const TA*)A.corr.p, n, S_TMP));
+    k::scale<TA><<<grid_for(n), kBlock, 0, st_>>>(n, TA(1.0 / vn), A.corr.p);
     NDS_LAUNCH();
     double ray = 0.0;
     for (int it = 0; it < its; ++it) {
-      k::div_sqrt<T><<<grid_for(n), kBlock, 0, st_>>>(n, A.corr.p, A.diag.p, A.b.p);
-      spmv(n, A.row.p, A.col.p, A.val.p, A.b.p, A.tmp.p);
-      k::div_sqrt<T><<<grid_for(n), kBlock, 0, st_>>>(n, A.tmp.p, A.diag.p, A.r.p);
+      k::div_sqrt<TA><<<grid_for(n), kBlock, 0, st_>>>(n, A.corr.p, A.diag.p, A.b.p);
+      op_spmv(level_op(A), (const TA*)A.b.p, A.tmp.p);
+      k::div_sqrt<TA><<<grid_for(n), kBlock, 0, st_>>>(n, A.tmp.p, A.diag.p, A.r.p);
       NDS_LAUNCH();
-      const double num = dot_fetch(A.corr.p, A.r.p, n, S_TMP), den = dot_fetch(A.corr.p, A.corr.p, n, S_TMP2);
+      const double num = dot_fetch((const TA*)A.corr.p, (const TA*)A.r.p, n, S_TMP),
+                   den = dot_fetch((const TA*)A.corr.p, (const TA*)A.corr.p, n, S_TMP2);
       ray = num / std::max(den, 1e-300);
-      const double wn = std::sqrt(dot_fetch(A.r.p, A.r.p, n, S_TMP));
+      const double wn = std::sqrt(dot_fetch((const TA*)A.r.p, (const TA*)A.r.p, n, S_TMP));
       if (!(ray > 0.0) || !(wn > 0.0) || !std::isfinite(ray) || !std::isfinite(wn))
         throw SolveFailure(NDS_E_BREAKDOWN, "coarse GPU power iteration failed");
-      vcopy(n, A.r.p, A.corr.p);
-      k::scale<T><<<grid_for(n), kBlock, 0, st_>>>(n, T(1.0 / wn), A.corr.p);
+      vcopy(n, (const TA*)A.r.p, A.corr.p);
+      k::scale<TA><<<grid_for(n), kBlock, 0, st_>>>(n, TA(1.0 / wn), A.corr.p);
       NDS_LAUNCH();
     }
     return safety * ray;
@@ -757,7 +795,7 @@ class Solver final : public ISolver {
     double est = 0.0;
     for (int kk = 0; kk < its; ++kk) {
       fine_apply(pp_.p, q_.p);
-      amg_apply(q_.p, z_.p);
+      amg_T(q_.p, z_.p);
       const double zn = std::sqrt(dot_fetch(z_.p, z_.p, nc_, S_TMP));
       const double ray = dot_fetch(pp_.p, z_.p, nc_, S_TMP2);
       if (!(zn > 0.0) || !std::isfinite(zn) || !std::isfinite(ray)) throw SolveFailure(NDS_E_BREAKDOWN, "preconditioned power failed");
@@ -798,7 +836,7 @@ class Solver final : public ISolver {
     const int g = red_grid(nc_);
     {
       ProfScope ps(prof, st_, P_FINE_SPMV);
-      sell_launch<k::SELL_DOT>(fine_op(), g, pp_.p, nullptr, nullptr, 0.0, q_.p, nullptr);
+      sell_launch<k::SELL_DOT, T>(fine_op(), g, pp_.p, nullptr, nullptr, 0.0, q_.p, nullptr);
       NDS_LAUNCH();
     }
     reduce_to<1>(g, S_PQ);
@@ -812,7 +850,7 @@ class Solver final : public ISolver {
   }
   // second half: z = M r, rho_new = r.z, beta = rho_new/rho, p = z + beta p
   void pcg_half2() {
-    amg_apply(r_.p, z_.p);
+    amg_T(r_.p, z_.p);
     dot_dev(r_.p, z_.p, nc_, S_RHON);
     k::pcg_beta<<<1, 1, 0, st_>>>(sc_.p, flags_.p);
     NDS_LAUNCH();
@@ -901,8 +939,7 @@ class Solver final : public ISolver {
     a.inc = inc_.p;
     a.ref = ref_.p;
     a.slot = slot_.p;
-    a.det = det_.p;
-    a.invJ = invJ_.p;
+    a.C = cconv_.p;
     a.bco = bco_.p;
     a.fixed = fixed_.p;
     a.u0 = u_[0].p;
@@ -912,7 +949,6 @@ class Solver final : public ISolver {
     a.s0 = s_[0].p;
     a.s1 = s_[1].p;
     a.s2 = s_[2].p;
-    a.centT = centT_.p;
     a.alpha_u = T(o_.alpha_u);
     a.rau_scale = T(o_.rau_scale);
     a.row_cap = row_cap_;
@@ -924,6 +960,10 @@ class Solver final : public ISolver {
     a.b1 = b_[1].p;
     a.b2 = b_[2].p;
     ProfScope ps(prof, st_, P_ASSEMBLE);
+    // cell blocks: a grid of 8 blocks per SM amortises the shared tensor load
+    k::mom_cell_conv<T><<<std::min(grid_for(nc_, kBlock / 8), 8 * 148), kBlock, 0, st_>>>(
+        nc_, ref_.p, fixed_.p, u_[0].p, u_[1].p, u_[2].p, invJ_.p, det_.p, centT_.p, cconv_.p);
+    NDS_LAUNCH();
     k::mom_assemble<T><<<grid_for(nv_, kBlock / 8), kBlock, mom_smem_, st_>>>(a);
     NDS_LAUNCH();
   }
@@ -1017,6 +1057,7 @@ class Solver final : public ISolver {
     R.rel_cont = cont_rel_;
     NDS_CUDA(cudaEventRecord(ev_[3], st_));
     refresh_fine(rau_.p);
+    NDS_CUDA(cudaEventRecord(ev_[6], st_));
     PRes pr;
     if (o_.pressure_solver == NDS_P_PCG) pr = pcg(rhs_.p);
     else pr = stationary(rhs_.p, o_.pressure_solver == NDS_P_CHEB);
@@ -1038,6 +1079,9 @@ class Solver final : public ISolver {
     R.ms_continuity = ms[2];
     R.ms_pressure = ms[3];
     R.ms_update = ms[4];
+    float msr = 0.f;
+    NDS_CUDA(cudaEventElapsedTime(&msr, ev_[3], ev_[6]));
+    R.ms_refresh = msr;
     const bool finite = std::isfinite(R.rel_cont) && std::isfinite(R.p_rel) &&
                         (!R.audited || (std::isfinite(R.audit_rel[0]) && std::isfinite(R.audit_rel[1]) &&
                                         std::isfinite(R.audit_rel[2])));
@@ -1128,7 +1172,7 @@ class Solver final : public ISolver {
   const Problem& P_;
   nds_options o_;
   cudaStream_t st_ = nullptr;
-  cudaEvent_t ev_[6] = {};
+  cudaEvent_t ev_[7] = {};
   int nc_ = 0, nv_ = 0, row_cap_ = 0, it_ = 0;
   size_t mom_smem_ = 0;
   double cont0_ = -1, cont_rel_ = 1, fine_lambda_ = 1, p_cheb_lambda_ = 1;
@@ -1138,18 +1182,19 @@ class Solver final : public ISolver {
   DBuf<int32_t> mrow_, mcol_, mdpos_, inc_off_, ref_, color_rows_;
   DBuf<uint32_t> inc_;
   DBuf<uint8_t> slot_;
-  DBuf<T> K_, A_, diag_, delta_, rau_, rau_pc_, det_, invJ_, bco_, fixed_, fixed_div_, centT_, p_;
+  DBuf<T> K_, A_, diag_, delta_, rau_, rau_pc_, det_, invJ_, bco_, fixed_, fixed_div_, centT_, cconv_, p_;
   DBuf<T> u_[3], b_[3], s_[3], v_[3];
   std::vector<int> color_off_;
   // pressure
-  DBuf<int32_t> frow_, fcol_, fdpos_, fcoff_, fine_crows_, sbase_, swidth_, scol_, fdslot_;
+  DBuf<int32_t> fcoff_, fine_crows_, sbase_, swidth_, scol_, fdslot_;
   DBuf<int16_t> sdcol_;
   k::Sell sell_{};
   long long sell_nnz_ = 0;
   std::vector<int> fine_coff_;
-  DBuf<uint8_t> fcnt_, fca_;
+  DBuf<uint8_t> fcsl_, fca_;
   DBuf<uint32_t> fcpk_;
-  DBuf<T> fval_, fdiag_, fl1_, x_, r_, z_, pp_, q_, rhs_, fr_, ftmp_, fcorr_, frhs_, fpong_, tinv_;
+  DBuf<T> fval_, x_, r_, z_, pp_, q_, rhs_;
+  DBuf<TA> fvalA_, fdiag_, fl1_, fr_, ftmp_, fcorr_, frhs_, fpong_, tinv_, rA_, zA_;
   std::vector<Level> L_;
   std::vector<Xfer> X_;
   DBuf<double> part_, sc_;
@@ -1196,9 +1241,9 @@ int nds_solver_create(const nds_problem* pp, nds_solver** out) {
     if (e != cudaSuccess || ndev <= P->opt.device)
       throw nds::CudaError(std::string("no CUDA device available: ") + cudaGetErrorString(e));
     auto s = std::make_unique<nds_solver>();
-    if (P->opt.precision == NDS_FP64) s->impl = std::make_unique<nds::Solver<double>>(*P);
-    else if (P->opt.precision == NDS_FP32) s->impl = std::make_unique<nds::Solver<float>>(*P);
-    else throw nds::SolveFailure(NDS_E_INVALID, "precision amg_fp32 is not supported (mixed State/AMG types)");
+    if (P->opt.precision == NDS_FP64) s->impl = std::make_unique<nds::Solver<double, double>>(*P);
+    else if (P->opt.precision == NDS_FP32) s->impl = std::make_unique<nds::Solver<float, float>>(*P);
+    else s->impl = std::make_unique<nds::Solver<double, float>>(*P);
     *out = s.release();
   });
 }

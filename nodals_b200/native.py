@@ -87,7 +87,7 @@ class IterReport(C.Structure):
                 ("p_rel", C.c_double), ("audited", C.c_int), ("audit_rel", C.c_double * 3),
                 ("all_momentum_met", C.c_int), ("converged", C.c_int),
                 ("ms_assembly", C.c_double), ("ms_momentum", C.c_double), ("ms_continuity", C.c_double),
-                ("ms_pressure", C.c_double), ("ms_update", C.c_double)]
+                ("ms_pressure", C.c_double), ("ms_update", C.c_double), ("ms_refresh", C.c_double)]
 
 
 class SolveReport(C.Structure):

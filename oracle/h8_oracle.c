@@ -6,11 +6,13 @@
  * under OpenMP, sums that the reference accumulates in cell order are
  * gathered in ascending cell order.
  */
+#define _POSIX_C_SOURCE 199309L /* clock_gettime */
 #include "h8_oracle.h"
 
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
+#include <time.h>
 
 #ifdef _OPENMP
 #include <omp.h>
@@ -504,10 +506,17 @@ ora_state* ora_create(const ora_problem* P) {
 
 double ora_fine_lambda(const ora_state* S) { return S->fine_lambda; }
 
+static double now_ms(void) {
+  struct timespec t;
+  clock_gettime(CLOCK_MONOTONIC, &t);
+  return 1e3 * (double)t.tv_sec + 1e-6 * (double)t.tv_nsec;
+}
+
 /* one SIMPLE iteration (h8_main_base.cu:2046-2119) */
 int ora_step(ora_state* S, ora_report* R) {
   const ora_problem* P = S->P;
   memset(R, 0, sizeof(*R));
+  const double t0 = now_ms();
   const int it = ++S->it;
   R->it = it;
   assemble(S);
@@ -522,7 +531,9 @@ int ora_step(ora_state* S, ora_report* R) {
   R->rel_cont = S->cont_rel;
   R->cont_norm = cn;
   refresh(S);
+  const double tp = now_ms();
   const int st = pressure(S, &R->p_its, &R->p_rel);
+  R->ms_pressure = now_ms() - tp;
   if (st < 0) {
     R->status = st;
     return st;
@@ -536,6 +547,7 @@ int ora_step(ora_state* S, ora_report* R) {
   const int met = R->audited && R->audit_rel[0] <= P->simple_tol && R->audit_rel[1] <= P->simple_tol &&
                   R->audit_rel[2] <= P->simple_tol;
   R->converged = P->run_mode == 1 && isfinite(R->rel_cont) && R->rel_cont <= P->simple_tol && met;
+  R->ms_total = now_ms() - t0;
   return 0;
 }
 

@@ -96,6 +96,8 @@ typedef struct ora_report {
   double audit_rel[3];
   int converged;
   int status;               /* 0 ok, <0 breakdown */
+  double ms_total;          /* wall time of the step */
+  double ms_pressure;       /* wall time of the pressure solve */
 } ora_report;
 
 typedef struct ora_state ora_state;

@@ -49,7 +49,7 @@ class _Problem(C.Structure):
 class Report(C.Structure):
     _fields_ = [("it", C.c_int), ("rel_cont", C.c_double), ("cont_norm", C.c_double), ("p_its", C.c_int),
                 ("p_rel", C.c_double), ("p_ok", C.c_int), ("audited", C.c_int), ("audit_rel", C.c_double * 3),
-                ("converged", C.c_int), ("status", C.c_int)]
+                ("converged", C.c_int), ("status", C.c_int), ("ms_total", C.c_double), ("ms_pressure", C.c_double)]
 
 
 _lib = None

@@ -64,12 +64,11 @@ CASES = {
     "small_sa_fixed10": ("pipe_small", "fp64", ["--run-mode", "fixed10", "--max-outer", "10"], _CFG1 + _SA + ["--amg-terminal", "100"]),
     "small_cf_fixed10": ("pipe_small", "fp64", ["--run-mode", "fixed10", "--max-outer", "10"], _CFG1 + _CF + ["--amg-terminal", "100"]),
     "small_sa_default10": ("pipe_small", "fp64", ["--run-mode", "fixed10", "--max-outer", "10"], ["--amg-terminal", "100"]),
-    # l1jacobi with the Richardson outer solver; the reference's outer
-    # Chebyshev cannot start with l1jacobi (its setup refresh leaves the fine
-    # L1 sums unset and its preconditioned power iteration fails)
-    "small_l1_fixed10": ("pipe_small", "fp64", ["--run-mode", "fixed10", "--max-outer", "10"],
-                         _CFG1 + ["--amg-hierarchy", "cf", "--cf-interp", "direct", "--amg-smoother", "l1jacobi",
-                                  "--pressure-solver", "richardson", "--amg-terminal", "100"]),
+    # No l1jacobi fixture: the reference's outer Chebyshev cannot start with
+    # l1jacobi (its setup refresh leaves the fine L1 sums unset and its
+    # preconditioned power iteration fails), and with the Richardson outer
+    # solver its per-iteration profiler overflows (2048 records) at this
+    # tolerance.  The l1jacobi path is checked against the oracle instead.
     "small_cheb_fixed10": ("pipe_small", "fp64", ["--run-mode", "fixed10", "--max-outer", "10"],
                            _CFG1 + ["--amg-hierarchy", "cf", "--cf-interp", "exti", "--cf-pmax", "8",
                                     "--amg-smoother", "jacobi", "--pressure-solver", "cheb", "--amg-terminal", "100"]),
