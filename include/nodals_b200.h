@@ -177,6 +177,7 @@ int nds_profile_read(nds_solver* s, nds_profile_entry* out, int max_entries, int
 /* number of kernels this library has launched in this process */
 unsigned long long nds_launch_count(void);
 
+
 #ifdef __cplusplus
 }
 #endif

@@ -162,48 +162,55 @@ __global__ void __launch_bounds__(kBlock) mom_assemble(MomArgs<T> g) {
     __syncwarp(gmask);
     T conv0 = 0, conv1 = 0, conv2 = 0, bt0 = 0, bt1 = 0, bt2 = 0;
     const int z0 = g.inc_off[i], z1 = g.inc_off[i + 1];
-    for (int z = z0; z < z1; z += 2) {
-      // two incidences in flight; applied in order
-      const bool two = z + 1 < z1;
-      const uint32_t pa = g.inc[z], pb = two ? g.inc[z + 1] : pa;
-      const int ca = (int)(pa >> 3), aa = (int)(pa & 7u), cb = (int)(pb >> 3), ab = (int)(pb & 7u);
-      const int ga = g.ref[8 * (size_t)ca + lane8], gb = g.ref[8 * (size_t)cb + lane8];
-      const T va = g.C[64 * (size_t)ca + 8 * aa + lane8], vb = g.C[64 * (size_t)cb + 8 * ab + lane8];
-      const int sa = g.slot[64 * (size_t)ca + 8 * aa + lane8], sb = g.slot[64 * (size_t)cb + 8 * ab + lane8];
-      if (ga >= 0) {
-        buf[sa] += va;
-      } else {
-        const T* f = g.fixed + 3 * (size_t)(-ga - 1);
-        conv0 -= va * f[0];
-        conv1 -= va * f[1];
-        conv2 -= va * f[2];
-      }
-      if (lane8 == 0) {
-        const T pv = g.p[ca];
-        const T* B = g.bco + 24 * (size_t)ca + 3 * aa;
-        bt0 += B[0] * pv;
-        bt1 += B[1] * pv;
-        bt2 += B[2] * pv;
-      }
-      __syncwarp(gmask);
-      if (two) {
-        if (gb >= 0) {
-          buf[sb] += vb;
-        } else {
-          const T* f = g.fixed + 3 * (size_t)(-gb - 1);
-          conv0 -= vb * f[0];
-          conv1 -= vb * f[1];
-          conv2 -= vb * f[2];
+    for (int zb = z0; zb < z1; zb += 8) {
+      // up to 8 incidence words in one coalesced load, then the gathers of
+      // four incidences in flight before their (ordered) updates
+      const int zn = min(8, z1 - zb);
+      const uint32_t mine = lane8 < zn ? g.inc[zb + lane8] : 0u;
+      for (int k0 = 0; k0 < zn; k0 += 4) {
+        int gk[4], sk[4];
+        T vk[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const bool ok = k0 + u < zn;
+          const uint32_t pk = __shfl_sync(gmask, mine, (k0 + u) & 7, 8);
+          const int c = (int)(pk >> 3), a = (int)(pk & 7u);
+          const size_t e = 64 * (size_t)c + 8 * a + lane8;
+          gk[u] = ok ? g.ref[8 * (size_t)c + lane8] : 0;
+          vk[u] = ok ? g.C[e] : T(0);
+          sk[u] = ok ? (int)g.slot[e] : 0;
         }
-        if (lane8 == 0) {
-          const T pv = g.p[cb];
-          const T* B = g.bco + 24 * (size_t)cb + 3 * ab;
-          bt0 += B[0] * pv;
-          bt1 += B[1] * pv;
-          bt2 += B[2] * pv;
+        // lane u < 4: the B^T p terms of incidence k0 + u
+        T t0 = 0, t1 = 0, t2 = 0;
+        {
+          const uint32_t pk = __shfl_sync(gmask, mine, (k0 + (lane8 & 3)) & 7, 8);
+          if (lane8 < 4 && k0 + lane8 < zn) {
+            const int c = (int)(pk >> 3), a = (int)(pk & 7u);
+            const T* B = g.bco + 24 * (size_t)c + 3 * a;
+            const T pv = g.p[c];
+            t0 = B[0] * pv;
+            t1 = B[1] * pv;
+            t2 = B[2] * pv;
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          if (k0 + u < zn) {
+            if (gk[u] >= 0) {
+              buf[sk[u]] += vk[u];
+            } else {
+              const T* f = g.fixed + 3 * (size_t)(-gk[u] - 1);
+              conv0 -= vk[u] * f[0];
+              conv1 -= vk[u] * f[1];
+              conv2 -= vk[u] * f[2];
+            }
+            bt0 += __shfl_sync(gmask, t0, u, 8);
+            bt1 += __shfl_sync(gmask, t1, u, 8);
+            bt2 += __shfl_sync(gmask, t2, u, 8);
+            __syncwarp(gmask);
+          }
         }
       }
-      __syncwarp(gmask);
     }
     conv0 = group_sum<8>(conv0, gmask);
     conv1 = group_sum<8>(conv1, gmask);
@@ -471,6 +478,53 @@ __global__ void pcg_beta(double* __restrict__ sc, int* __restrict__ flags) {
   sc[0] = rhon;
 }
 
+// Device-resident PCG loop (one CUDA graph with a conditional while node).
+// ctl: [0] iterations done, [1] converged, [2] first iteration pending.
+// flags bit 8: initial rho <= 0 or non-finite; bit 4: residual non-finite.
+//
+// rho step of the loop body: on the first iteration rho = r.z (p = z follows),
+// afterwards beta = rho_new / rho as pcg_beta.
+__global__ void pcg_rho_dev(double* __restrict__ sc, int* __restrict__ flags, const int* __restrict__ ctl) {
+  const double rhon = sc[4];
+  if (ctl[2]) {
+    if (!(rhon > 0.0) || !isfinite(rhon)) *flags |= 8;
+    sc[0] = rhon;
+    sc[5] = 0.0;
+    return;
+  }
+  if (!(rhon > 0.0) || !isfinite(rhon)) {
+    *flags |= 2;
+    sc[5] = 0.0;
+    return;
+  }
+  sc[5] = rhon / sc[0];
+  sc[0] = rhon;
+}
+// p = z on the first iteration, else p = z + beta p
+template <class T>
+__global__ void p_update_dev(int n, const double* __restrict__ beta_dev, const int* __restrict__ ctl,
+                             const T* __restrict__ z, T* __restrict__ p) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  p[i] = ctl[2] ? z[i] : z[i] + T(*beta_dev) * p[i];
+}
+// End of the loop body: count the iteration and test ||r|| <= target the way
+// the host loop does (sqrt, then compare); stop on convergence, on any flag
+// or at max_its.  The loop always ends: every body pass runs this kernel and
+// the count reaches max_its.
+__global__ void pcg_check(const double* __restrict__ sc, int rn2_slot, int r0_slot, int target_slot,
+                          int* __restrict__ flags, int* __restrict__ ctl, int max_its,
+                          cudaGraphConditionalHandle loop) {
+  const int it = ++ctl[0];
+  ctl[2] = 0;
+  const double rn = sqrt(sc[rn2_slot]);
+  if (!isfinite(rn / fmax(sc[r0_slot], 1e-300))) *flags |= 4;
+  const int conv = rn <= sc[target_slot];
+  ctl[1] = conv;
+  const bool stop = conv || *flags != 0 || it >= max_its;
+  cudaGraphSetConditional(loop, stop ? 0u : 1u);
+}
+
 // ---------------------------------------------------------------------------
 // transfers and terminal solve (g5e_fp32_kernels.cuh:140-150)
 // ---------------------------------------------------------------------------
@@ -552,25 +606,27 @@ enum SellMode { SELL_Y = 0, SELL_RESID = 1, SELL_SMOOTH = 2, SELL_DOT = 3 };
 // accumulators, fixed order -> deterministic.
 template <class T, bool D16>
 __device__ __forceinline__ T sell_row(const Sell& A, const T* __restrict__ v, const T* __restrict__ x, int i) {
+  // entries in flight per thread: 8 for 8-byte values, 16 for 4-byte ones
+  constexpr int U = sizeof(T) == 4 ? 16 : 8;
   const int s = i >> 5;
   const int b = A.base[s] + (i & 31);
   const int w = A.width[s];
   T s0 = 0, s1 = 0;
   int k = 0;
-  for (; k + 8 <= w; k += 8) {
-    int j[8];
-    T a[8];
+  for (; k + U <= w; k += U) {
+    int j[U];
+    T a[U];
 #pragma unroll
-    for (int u = 0; u < 8; ++u) {
+    for (int u = 0; u < U; ++u) {
       const int o = b + 32 * (k + u);
       j[u] = sell_col<D16>(A, o, i);
       a[u] = v[o];
     }
-    T xv[8];
+    T xv[U];
 #pragma unroll
-    for (int u = 0; u < 8; ++u) xv[u] = x[j[u]];
+    for (int u = 0; u < U; ++u) xv[u] = x[j[u]];
 #pragma unroll
-    for (int u = 0; u < 8; u += 2) {
+    for (int u = 0; u < U; u += 2) {
       s0 += a[u] * xv[u];
       s1 += a[u + 1] * xv[u + 1];
     }
@@ -614,11 +670,30 @@ __global__ void __launch_bounds__(kBlock) sell_spmv(Sell A, const T* __restrict_
   }
 }
 
+// Static part of the fine Schur refresh: for every directed contribution q of
+// row c (basis a of c, incidence (c2, b) of the shared velocity dof), the
+// geometric factor G_q = B[c][a] . B[c2][b].  Evaluated once at setup.
+// cs[q] = slot << 3 | a; cpk[q] = c2 << 3 | b.
+template <class T>
+__global__ void refresh_geometry(int nc, const int32_t* __restrict__ coff, const uint32_t* __restrict__ cpk,
+                                 const uint16_t* __restrict__ cs, const T* __restrict__ bco, T* __restrict__ G) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+  const T* Bc = bco + 24 * (size_t)c;
+  for (int q = coff[c]; q < coff[c + 1]; ++q) {
+    const int a = cs[q] & 7;
+    const uint32_t pk = cpk[q];
+    const T* bb = bco + 24 * (size_t)(pk >> 3) + 3 * (pk & 7u);
+    G[q] = Bc[3 * a] * bb[0] + Bc[3 * a + 1] * bb[1] + Bc[3 * a + 2] * bb[2];
+  }
+}
+
 // Fine Schur numeric refresh A_p = B diag(rau) B^T (h8_precomputed_b.cuh:37-91),
-// warp per pressure row, written into the SELL layout.  The directed
+// warp per pressure row, written into the SELL layout.  Each value is
+// sum_q rau_{g(c,a_q)} G_q over the row's contributions to that entry.  The
 // contributions of a row were sorted by destination slot at setup (stable,
 // from the reference's (basis, incidence) order of h2b_fine_csr.cuh:480-520).
-// Lanes take one contribution each (32 independent gathers in flight), then
+// Lanes take one contribution each (a coalesced stream of G and cs), then
 // every slot is summed sequentially in that order by a shuffle chain: lane L
 // adds its product to the final running sum of lane L-1 when both belong to
 // the same slot, so each value is the reference's serial sum; no atomics.
@@ -627,18 +702,15 @@ __global__ void __launch_bounds__(kBlock) sell_spmv(Sell A, const T* __restrict_
 // precision TA); the diagonal and L1 row sums feed the AMG smoothers.
 template <class T, class TA>
 __global__ void __launch_bounds__(kBlock) sell_refresh(int nc, const int32_t* __restrict__ coff,
-                                                       const uint8_t* __restrict__ csl, const uint32_t* __restrict__ cpk,
-                                                       const uint8_t* __restrict__ ca, const int32_t* __restrict__ ref,
-                                                       const T* __restrict__ bco, const T* __restrict__ rau,
+                                                       const uint16_t* __restrict__ cs, const T* __restrict__ G,
+                                                       const int32_t* __restrict__ ref, const T* __restrict__ rau,
                                                        const int32_t* __restrict__ dslot, const int32_t* __restrict__ sbase,
                                                        T* __restrict__ val, TA* __restrict__ valA, TA* __restrict__ diag,
                                                        TA* __restrict__ l1) {
-  __shared__ T sB[kWarps][24];
   __shared__ T sR[kWarps][8];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (c >= nc) return;
-  if (lane < 24) sB[w][lane] = bco[24 * (size_t)c + lane];
   if (lane < 8) {
     const int g = ref[8 * (size_t)c + lane];
     sR[w][lane] = g >= 0 ? rau[g] : T(0);
@@ -656,18 +728,15 @@ __global__ void __launch_bounds__(kBlock) sell_refresh(int nc, const int32_t* __
     int sl = -1;
     T p = 0;
     if (live) {
-      const uint32_t pk = cpk[q];
-      const int a = ca[q];
-      sl = csl[q];
-      const T* bb = bco + 24 * (size_t)(pk >> 3) + 3 * (pk & 7u);
-      const T dot = sB[w][3 * a] * bb[0] + sB[w][3 * a + 1] * bb[1] + sB[w][3 * a + 2] * bb[2];
-      p = sR[w][a] * dot;
+      const unsigned v = cs[q];
+      sl = (int)(v >> 3);
+      p = sR[w][v & 7u] * G[q];
     }
     const int prev = __shfl_up_sync(0xffffffffu, sl, 1);
     const int next = __shfl_down_sync(0xffffffffu, sl, 1);
     // lane 31's run continues into the next chunk when the next contribution
     // has the same slot
-    const bool cont = lane == 31 && live && q + 1 < qe && (int)csl[q + 1] == sl;
+    const bool cont = lane == 31 && live && q + 1 < qe && (int)(cs[q + 1] >> 3) == sl;
     const bool head = !live || (lane == 0 ? sl != carry_slot : sl != prev);
     const bool tail = live && (lane == 31 ? !cont : next != sl);
     const unsigned heads = __ballot_sync(0xffffffffu, head) | 1u;

@@ -304,9 +304,17 @@ class Solver final : public ISolver {
           }
         }
       }
-      fcsl_.upload(csl);
-      fca_.upload(ca);
-      fcpk_.upload(cpk);
+      // (slot << 3 | basis) per contribution, and its static geometric factor
+      // B[c][a] . B[c2][b], evaluated once on the device
+      std::vector<uint16_t> cs(ca.size());
+      for (size_t q = 0; q < cs.size(); ++q) cs[q] = (uint16_t)(((unsigned)csl[q] << 3) | ca[q]);
+      fcs_.upload(cs);
+      DBuf<uint32_t> cpk_d;
+      cpk_d.upload(cpk);
+      fgeo_.alloc(cpk.size());
+      k::refresh_geometry<T><<<grid_for(nc_), kBlock, 0, st_>>>(nc_, fcoff_.p, cpk_d.p, fcs_.p, bco_.p, fgeo_.p);
+      NDS_LAUNCH();
+      NDS_CUDA(cudaStreamSynchronize(st_));
     }
     {
       // SELL-32 layout of the fine pattern
@@ -436,8 +444,9 @@ class Solver final : public ISolver {
     part_.alloc((size_t)kMaxPartBlocks * 8);
     sc_.alloc(kScalars);
     flags_.alloc(1);
+    ctl_.alloc(4);
     NDS_CUDA(cudaMallocHost((void**)&hsc_, sizeof(double) * kScalars));
-    NDS_CUDA(cudaMallocHost((void**)&hflags_, sizeof(int)));
+    NDS_CUDA(cudaMallocHost((void**)&hflags_, sizeof(int) * 8));
     NDS_CUDA(cudaMemsetAsync(flags_.p, 0, sizeof(int), st_));
 
     // setup-time state: fine CSR refreshed with the initial rAU
@@ -457,7 +466,8 @@ class Solver final : public ISolver {
   // ------------------------------------------------------------------ helpers
   static constexpr int kMaxPartBlocks = 1184;  // 8 x 148 SMs
   static constexpr int kScalars = 32;
-  enum { S_RHO = 0, S_PQ = 1, S_ALPHA = 2, S_RN2 = 3, S_RHON = 4, S_BETA = 5, S_TMP = 8, S_TMP2 = 9, S_CONT2 = 10,
+  enum { S_RHO = 0, S_PQ = 1, S_ALPHA = 2, S_RN2 = 3, S_RHON = 4, S_BETA = 5, S_R0 = 6, S_TARGET = 7, S_TMP = 8,
+         S_TMP2 = 9, S_CONT2 = 10,
          S_AUDIT = 16 };
 
   // CUDA graphs of fixed launch sequences (no host decisions inside)
@@ -498,6 +508,58 @@ class Solver final : public ISolver {
   }
   bool use_graphs_ = std::getenv("NDS_NO_GRAPHS") == nullptr;
   Graph g_amg_, g_pcg2_;
+  // the whole PCG iteration loop as one graph: a conditional while node whose
+  // body is one iteration and ends with pcg_check, which sets the condition
+  struct LoopGraph {
+    cudaGraphExec_t exec = nullptr;
+    unsigned long long body_kernels = 0;
+    bool failed = false;
+    ~LoopGraph() {
+      if (exec) cudaGraphExecDestroy(exec);
+    }
+  };
+  LoopGraph g_loop_;
+  bool build_pcg_loop() {
+    const bool was = prof.on;
+    prof.on = false;
+    cudaGraph_t graph = nullptr;
+    bool ok = cudaGraphCreate(&graph, 0) == cudaSuccess;
+    cudaGraphConditionalHandle h{};
+    cudaGraphNodeParams cp{};
+    cudaGraphNode_t node{};
+    if (ok) ok = cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault) == cudaSuccess;
+    if (ok) {
+      cp.type = cudaGraphNodeTypeConditional;
+      cp.conditional.handle = h;
+      cp.conditional.type = cudaGraphCondTypeWhile;
+      cp.conditional.size = 1;
+      ok = cudaGraphAddNode(&node, graph, nullptr, 0, &cp) == cudaSuccess;
+    }
+    const unsigned long long l0 = g_launches;
+    if (ok) ok = cudaStreamBeginCaptureToGraph(st_, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                               cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+    if (ok) {
+      bool body_ok = true;
+      try {
+        pcg_loop_body(h);
+      } catch (...) {
+        body_ok = false;
+      }
+      ok = cudaStreamEndCapture(st_, nullptr) == cudaSuccess && body_ok;
+    }
+    g_loop_.body_kernels = g_launches - l0;
+    g_launches = l0;
+    if (ok) ok = cudaGraphInstantiate(&g_loop_.exec, graph, 0) == cudaSuccess;
+    if (graph) cudaGraphDestroy(graph);
+    if (!ok) {
+      if (g_loop_.exec) cudaGraphExecDestroy(g_loop_.exec);
+      g_loop_.exec = nullptr;
+      g_loop_.failed = true;
+      cudaGetLastError();  // the fallback path runs instead
+    }
+    prof.on = was;
+    return ok;
+  }
   // z = M b with b, z in the state precision (casts around the V-cycle in
   // the mixed mode)
   void amg_T(const T* b, T* z) {
@@ -605,7 +667,7 @@ class Solver final : public ISolver {
   void refresh_fine(const T* rau) {
     ProfScope ps(prof, st_, P_REFRESH);
     k::sell_refresh<T, TA><<<grid_for((long long)nc_ * 32), kBlock, 0, st_>>>(
-        nc_, fcoff_.p, fcsl_.p, fcpk_.p, fca_.p, ref_.p, bco_.p, rau, fdslot_.p, sbase_.p, fval_.p,
+        nc_, fcoff_.p, fcs_.p, fgeo_.p, ref_.p, rau, fdslot_.p, sbase_.p, fval_.p,
         kSame ? nullptr : fvalA_.p, fdiag_.p, fl1_.p);
     NDS_LAUNCH();
   }
@@ -857,9 +919,67 @@ class Solver final : public ISolver {
     k::p_update<T><<<grid_for(nc_), kBlock, 0, st_>>>(nc_, sc_.p + S_BETA, z_.p, pp_.p);
     NDS_LAUNCH();
   }
+  // one pass of the device loop: z = M r; rho (first pass: p = z); q = A p;
+  // alpha; x, r update; ||r||^2; check
+  void pcg_loop_body(cudaGraphConditionalHandle h) {
+    amg_T(r_.p, z_.p);
+    dot_dev(r_.p, z_.p, nc_, S_RHON);
+    k::pcg_rho_dev<<<1, 1, 0, st_>>>(sc_.p, flags_.p, ctl_.p);
+    NDS_LAUNCH();
+    k::p_update_dev<T><<<grid_for(nc_), kBlock, 0, st_>>>(nc_, sc_.p + S_BETA, ctl_.p, z_.p, pp_.p);
+    NDS_LAUNCH();
+    const int g = red_grid(nc_);
+    sell_launch<k::SELL_DOT, T>(fine_op(), g, pp_.p, nullptr, nullptr, 0.0, q_.p, nullptr);
+    NDS_LAUNCH();
+    reduce_to<1>(g, S_PQ);
+    k::pcg_alpha<<<1, 1, 0, st_>>>(sc_.p, flags_.p);
+    NDS_LAUNCH();
+    k::xr_update<T><<<g, kBlock, 0, st_>>>(nc_, 0.0, sc_.p + S_ALPHA, pp_.p, q_.p, x_.p, r_.p, part_.p);
+    NDS_LAUNCH();
+    reduce_to<1>(g, S_RN2);
+    k::pcg_check<<<1, 1, 0, st_>>>(sc_.p, S_RN2, S_R0, S_TARGET, flags_.p, ctl_.p, o_.p_max, h);
+    NDS_LAUNCH();
+  }
+  // PCG with the iteration loop on the device: two host synchronisations per
+  // solve (initial norm, final state) instead of one per iteration.  Same
+  // arithmetic and stopping rule as pcg_host.
+  PRes pcg_device(double r0) {
+    const double target = std::max(o_.p_atol, o_.p_rtol * r0);
+    hsc_[S_R0] = r0;
+    hsc_[S_TARGET] = target;
+    NDS_CUDA(cudaMemcpyAsync(sc_.p + S_R0, hsc_ + S_R0, 2 * sizeof(double), cudaMemcpyHostToDevice, st_));
+    const int init[4] = {0, 0, 1, 0};
+    std::memcpy(hflags_ + 4, init, sizeof(init));
+    NDS_CUDA(cudaMemcpyAsync(ctl_.p, hflags_ + 4, 4 * sizeof(int), cudaMemcpyHostToDevice, st_));
+    NDS_CUDA(cudaMemsetAsync(flags_.p, 0, sizeof(int), st_));
+    NDS_CUDA(cudaGraphLaunch(g_loop_.exec, st_));
+    NDS_CUDA(cudaMemcpyAsync(hflags_ + 4, ctl_.p, 4 * sizeof(int), cudaMemcpyDeviceToHost, st_));
+    NDS_CUDA(cudaMemcpyAsync(hflags_, flags_.p, sizeof(int), cudaMemcpyDeviceToHost, st_));
+    NDS_CUDA(cudaMemcpyAsync(hsc_ + S_RN2, sc_.p + S_RN2, sizeof(double), cudaMemcpyDeviceToHost, st_));
+    NDS_CUDA(cudaStreamSynchronize(st_));
+    const int its = hflags_[4], f = hflags_[0];
+    g_launches += (unsigned long long)its * g_loop_.body_kernels;
+    if (f & 8) throw SolveFailure(NDS_E_BREAKDOWN, "pressure PCG initial rho nonpositive");
+    if (f & 1) throw SolveFailure(NDS_E_BREAKDOWN, "pressure PCG pAp nonpositive");
+    if (f & 2) throw SolveFailure(NDS_E_BREAKDOWN, "pressure PCG rho nonpositive");
+    PRes R;
+    R.its = its;
+    R.rel = std::sqrt(hsc_[S_RN2]) / std::max(r0, 1e-300);
+    if ((f & 4) || !std::isfinite(R.rel)) throw SolveFailure(NDS_E_BREAKDOWN, "pressure PCG residual nonfinite");
+    R.ok = hflags_[5] != 0;
+    return R;
+  }
   PRes pcg(const T* rhs) {
     const double r0 = p_start(rhs);
     if (r0 <= o_.p_atol) return {0, 0.0, true};
+    // device loop unless the category profiler needs per-kernel events (or
+    // graphs are off / the conditional graph could not be built)
+    if (use_graphs_ && !prof.on && !g_loop_.failed && o_.p_max >= 1) {
+      if (g_loop_.exec || build_pcg_loop()) return pcg_device(r0);
+    }
+    return pcg_host(r0);
+  }
+  PRes pcg_host(double r0) {
     amg_rz();
     vcopy(nc_, z_.p, pp_.p);
     dot_dev(r_.p, z_.p, nc_, S_RHO);
@@ -1182,7 +1302,7 @@ class Solver final : public ISolver {
   DBuf<int32_t> mrow_, mcol_, mdpos_, inc_off_, ref_, color_rows_;
   DBuf<uint32_t> inc_;
   DBuf<uint8_t> slot_;
-  DBuf<T> K_, A_, diag_, delta_, rau_, rau_pc_, det_, invJ_, bco_, fixed_, fixed_div_, centT_, cconv_, p_;
+  DBuf<T> K_, A_, diag_, delta_, rau_, rau_pc_, det_, invJ_, bco_, fixed_, fixed_div_, centT_, cconv_, fgeo_, p_;
   DBuf<T> u_[3], b_[3], s_[3], v_[3];
   std::vector<int> color_off_;
   // pressure
@@ -1191,8 +1311,9 @@ class Solver final : public ISolver {
   k::Sell sell_{};
   long long sell_nnz_ = 0;
   std::vector<int> fine_coff_;
-  DBuf<uint8_t> fcsl_, fca_;
-  DBuf<uint32_t> fcpk_;
+  DBuf<uint16_t> fcs_;
+  DBuf<int> ctl_;
+
   DBuf<T> fval_, x_, r_, z_, pp_, q_, rhs_;
   DBuf<TA> fvalA_, fdiag_, fl1_, fr_, ftmp_, fcorr_, frhs_, fpong_, tinv_, rA_, zA_;
   std::vector<Level> L_;
@@ -1200,7 +1321,7 @@ class Solver final : public ISolver {
   DBuf<double> part_, sc_;
   DBuf<int> flags_;
   double* hsc_ = nullptr;
-  int* hflags_ = nullptr;
+  int* hflags_ = nullptr;  // [0] flags, [4..7] device-loop control words
 };
 
 }  // namespace nds
@@ -1270,6 +1391,7 @@ int nds_set_fields(nds_solver* s, const double* u0, const double* u1, const doub
 void nds_solver_destroy(nds_solver* s) { delete s; }
 
 unsigned long long nds_launch_count(void) { return nds::g_launches; }
+
 
 int nds_profile_enable(nds_solver* s, int on) {
   if (!s) return fail(NDS_E_INVALID, "null solver");

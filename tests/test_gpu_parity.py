@@ -79,6 +79,23 @@ def test_gpu_amg_fp32_close_to_fp64(native, meshes, case):
         assert rel_l2(y, x) <= 1e-6
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "amg_fp32"])
+def test_device_loop_matches_host_loop(native, meshes, precision):
+    """The PCG loop run on the device (conditional CUDA graph) and the
+    launch-by-launch loop (taken while the category profiler is on) launch
+    the same kernels in the same order: results must be bitwise equal."""
+    P = _make(native, meshes, "pipe_small", precision=precision, **ORACLE_CASES["sa_pcg"])
+    A, B = native.Solver(P), native.Solver(P)
+    B.profile(True)
+    for _ in range(6):
+        a, b = A.step(), B.step()
+        assert a.p_its == b.p_its, (a.it, a.p_its, b.p_its)
+        assert a.rel_cont == b.rel_cont and a.p_rel == b.p_rel
+    for x, y in zip(A.fields(), B.fields()):
+        assert np.array_equal(x, y)
+
+
 def _golden_cases():
     return sorted(p.stem[4:] for p in GOLDEN.glob("run_*.npz"))
 
