@@ -177,6 +177,24 @@ int nds_profile_read(nds_solver* s, nds_profile_entry* out, int max_entries, int
 /* number of kernels this library has launched in this process */
 unsigned long long nds_launch_count(void);
 
+/* ---- allocation-free continuity residual (no counterpart in the
+ *      reference, which computes this only inside its SIMPLE loop,
+ *      h8_precomputed_b.cuh:140-163).
+ * For callers that must not allocate device memory.  u0..u2 (nv doubles
+ * each), r (nc doubles) and norm (1 double) are caller-owned DEVICE
+ * pointers on the solver's device; stream is a cudaStream_t (NULL: the
+ * legacy default stream).  Enqueues r = -(B u + fixedDiv) and
+ * *norm = ||B u + fixedDiv||_2, the quantity nds_simple_step reports as
+ * cont_norm, and returns without synchronising.  Needs a solver whose state
+ * is FP64 (precision fp64 or amg_fp32).  Makes no cudaMalloc/cudaFree or
+ * other allocating call: the partial sums live in a 16 KiB device array of
+ * the library (at most 1184 blocks).  The first call on a device resolves
+ * that array's address (cudaGetSymbolAddress), so make it before any stream
+ * capture.  Calls that overlap in time on one device race on the array, and
+ * so do calls overlapping an nds_simple_step of the same solver.  Failures
+ * return a status only: nds_last_error() is not updated. */
+int nds_continuity_noalloc(nds_solver* s, const double* u0, const double* u1, const double* u2, double* r,
+                           double* norm, void* stream);
 
 #ifdef __cplusplus
 }

@@ -17,6 +17,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <type_traits>
 #include <vector>
@@ -137,6 +138,10 @@ struct ISolver {
   virtual void solve(nds_solve_report* rep) = 0;
   virtual void get_fields(double* u0, double* u1, double* u2, double* p) = 0;
   virtual void set_fields(const double* u0, const double* u1, const double* u2, const double* p) = 0;
+  // device cell-plan arrays read by nds_continuity_noalloc; false unless the
+  // state type is double
+  virtual bool cell_arrays(const int32_t** ref, const double** bco, const double** fixed_div, int* nc,
+                           int* device) const = 0;
   Profiler prof;
 };
 
@@ -1249,6 +1254,19 @@ class Solver final : public ISolver {
     if (rep) *rep = S;
   }
 
+  bool cell_arrays(const int32_t** ref, const double** bco, const double** fixed_div, int* nc,
+                   int* device) const override {
+    if constexpr (std::is_same<T, double>::value) {
+      *ref = ref_.p;
+      *bco = bco_.p;
+      *fixed_div = fixed_div_.p;
+      *nc = nc_;
+      *device = o_.device;
+      return true;
+    } else {
+      return false;
+    }
+  }
   void get_fields(double* u0, double* u1, double* u2, double* p) override {
     std::vector<T> h;
     auto get = [&](const DBuf<T>& b, double* out) {
@@ -1392,6 +1410,73 @@ void nds_solver_destroy(nds_solver* s) { delete s; }
 
 unsigned long long nds_launch_count(void) { return nds::g_launches; }
 
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free continuity residual.
+//
+// Callers that may not allocate device memory -- code running between the
+// steps of its own captured or real-time loop, or under an allocator that
+// forbids cudaMalloc after start-up -- get the continuity residual of the
+// solver's mesh for velocity vectors they own.  The partial sums of the
+// continuity kernel go to a file-scope device array instead of a cudaMalloc'd
+// buffer: at most kNoAllocBlocks blocks (the same 8 x 148 cap as the solver's
+// own reductions), 16 KiB per device.  Every block overwrites its own slot
+// and the reduction reads only the slots written by the same call, so
+// nothing has to start at zero.  The array is shared by all calls on a
+// device: calls that overlap in time (two host threads, or two streams
+// without ordering between them) race on it.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr int kNoAllocBlocks = 1184;
+constexpr int kNoAllocScratch = 2048;  // doubles; >= kNoAllocBlocks
+constexpr int kNoAllocMaxDevices = 64;
+static_assert(kNoAllocScratch >= kNoAllocBlocks, "scratch too small for the block cap");
+std::mutex g_noalloc_mu;
+double* g_noalloc_addr[kNoAllocMaxDevices] = {};
+
+__global__ void sqrt_in_place(double* x) { *x = sqrt(*x); }
+}  // namespace
+
+static __device__ __align__(256) double g_noalloc_part[kNoAllocScratch];
+
+extern "C" {
+
+int nds_continuity_noalloc(nds_solver* s, const double* u0, const double* u1, const double* u2, double* r,
+                           double* norm, void* stream) {
+  if (!s || !u0 || !u1 || !u2 || !r || !norm) return NDS_E_INVALID;
+  const int32_t* ref = nullptr;
+  const double *bco = nullptr, *fdiv = nullptr;
+  int nc = 0, dev = 0;
+  if (!s->impl->cell_arrays(&ref, &bco, &fdiv, &nc, &dev)) return NDS_E_INVALID;
+  if (nc < 1 || dev < 0 || dev >= kNoAllocMaxDevices) return NDS_E_INVALID;
+  const int grid = std::min(nds::grid_for(nc), kNoAllocBlocks);
+  if (grid > kNoAllocScratch) return NDS_E_INVALID;
+  int prev = -1;
+  if (cudaGetDevice(&prev) != cudaSuccess) return NDS_E_CUDA;
+  if (prev != dev && cudaSetDevice(dev) != cudaSuccess) return NDS_E_CUDA;
+  int st = NDS_OK;
+  double* part = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+      void* a = nullptr;
+      if (cudaGetSymbolAddress(&a, g_noalloc_part) == cudaSuccess) g_noalloc_addr[dev] = static_cast<double*>(a);
+      else st = NDS_E_CUDA;
+    }
+    part = g_noalloc_addr[dev];
+  }
+  if (st == NDS_OK) {
+    cudaStream_t cs = static_cast<cudaStream_t>(stream);
+    nds::k::continuity<double><<<grid, nds::kBlock, 0, cs>>>(nc, ref, bco, fdiv, u0, u1, u2, r, part);
+    nds::k::reduce_partials<1><<<1, nds::kBlock, 0, cs>>>(part, grid, norm);
+    sqrt_in_place<<<1, 1, 0, cs>>>(norm);
+    nds::g_launches += 3;
+    if (cudaGetLastError() != cudaSuccess) st = NDS_E_CUDA;
+  }
+  if (prev != dev) cudaSetDevice(prev);
+  return st;
+}
 
 int nds_profile_enable(nds_solver* s, int on) {
   if (!s) return fail(NDS_E_INVALID, "null solver");
