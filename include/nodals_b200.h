@@ -82,6 +82,10 @@ typedef struct nds_options {
   int threads;     /* host threads for setup; 0 = all */
   int device;      /* CUDA device ordinal */
   int verbose;     /* 1: print the reference's NODALS_GPU_* markers to stdout */
+  /* laminar SUPG stabilisation of the momentum operator, implicit form with
+   * the 64-point collapsed rule (h8_supg_main_cli.inc, h7_momentum_assembly.cuh:100-226) */
+  int supg;
+  double supg_tau_scale, supg_magic;
 } nds_options;
 
 /* One SIMPLE outer iteration (h8_main_base.cu:2046-2119). */

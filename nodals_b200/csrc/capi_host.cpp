@@ -86,6 +86,9 @@ void nds_options_default(nds_options* o) {
   o->threads = 0;
   o->device = 0;
   o->verbose = 0;
+  o->supg = 0;
+  o->supg_tau_scale = 0.05;
+  o->supg_magic = 9.0;
 }
 
 int nds_mesh_read_polymesh(const char* dir, nds_mesh** out) {
@@ -161,6 +164,9 @@ int nds_problem_create(const nds_mesh* mm, const nds_options* o, nds_problem** o
     so.inlet = o->inlet;
     so.outlet = o->outlet;
     so.threads = o->threads;
+    so.supg = o->supg != 0;
+    so.supg_tau_scale = o->supg_tau_scale;
+    so.supg_magic = o->supg_magic;
     P->setup = nds::build_setup(P->mesh, so);
     P->power_its = nds::effective_amg_power_its(*o);
     nds::AmgOptions ao;
@@ -252,7 +258,10 @@ namespace nds {
 
 int effective_amg_power_its(const nds_options& o) {
   if (o.amg_spectrum_policy == NDS_SPEC_ALWAYS) return o.amg_power_its;
-  if (o.amg_spectrum_policy == NDS_SPEC_AUTO && o.amg_smoother == NDS_SM_CHEB2) return o.amg_power_its;
+  // the SUPG entry also estimates the spectrum for smoothed aggregation
+  // (h8_supg_main_setup.inc:10-14)
+  const bool need = o.amg_smoother == NDS_SM_CHEB2 || (o.supg && o.amg_hierarchy == NDS_AMG_SA);
+  if (o.amg_spectrum_policy == NDS_SPEC_AUTO && need) return o.amg_power_its;
   return 0;
 }
 
@@ -298,6 +307,14 @@ bool validate_options(const nds_options& o, std::string& why) {
   if (o.run_mode == NDS_RUN_FIXED10 && o.max_outer != 10) return bad("H8 fixed10 requires maxOuter=10");
   if (o.amg_smoother == NDS_SM_CHEB2 && effective_amg_power_its(o) <= 0) return bad("H8 Chebyshev AMG smoother requires spectrum estimation");
   if (o.precision < 0 || o.precision > 2) return bad("precision must be fp64, fp32 or amg_fp32");
+  if (o.supg != 0 && o.supg != 1) return bad("H8 supg must be 0 or 1");
+  if (o.supg) {  // h8_supg_main_cli.inc:92-124
+    if (!(o.supg_tau_scale > 0.0)) return bad("H8 SUPG tau scale must be positive");
+    if (!(o.supg_magic > 0.0)) return bad("H8 SUPG magic must be positive");
+    if (o.amg_hierarchy == NDS_AMG_SA && effective_amg_power_its(o) <= 0)
+      return bad("P7D smoothed aggregation requires spectrum estimation to smooth interpolation");
+    if (o.momentum_work != NDS_MOM_FGS1) return bad("H8 requires momentum-work=fgs1");
+  }
   return true;
 }
 
@@ -365,6 +382,16 @@ void Problem::index_arrays() {
   for (int d = 0; d < 3; ++d) A["staticRhs" + std::to_string(d)] = view(S.static_rhs[(size_t)d], 0);
   A["fixedDiv"] = view(S.fixed_div, 0);
   A["volume"] = view(S.volume, 0);
+  A["cell.h2"] = view(S.h2, 0);
+  {
+    const auto& q = tet_rule_64();
+    supg_rule.clear();
+    for (const auto& x : q) {
+      for (int k = 0; k < 4; ++k) supg_rule.push_back(x.lam[(size_t)k]);
+      supg_rule.push_back(x.w);
+    }
+    A["supg.rule"] = view(supg_rule, 0);  // 64 x (lambda0..3, weight)
+  }
   A["initRau"] = view(S.init_rau, 0);
   A["initDelta"] = view(S.init_delta, 0);
   A["fine.row"] = view(S.fine.row, 1);

@@ -26,6 +26,7 @@ struct Problem {
   std::map<std::string, nds_array> arrays;
   std::map<std::string, std::vector<double>> scalars;
   std::vector<int32_t> mesh_tets, mesh_opp;
+  std::vector<double> supg_rule;  // 64 x (lambda0..3, weight) of the SUPG quadrature
   void index_arrays();
 };
 

@@ -69,8 +69,8 @@ int run(int argc, char** argv) {
     else if (a == "--wall-reference-f") (void)dv();
     else if (a == "--wall-diag-csv") (void)sv();
     else if (a == "--supg") supg = iv();
-    else if (a == "--supg-tau-scale") (void)dv();
-    else if (a == "--supg-magic") (void)dv();
+    else if (a == "--supg-tau-scale") o.supg_tau_scale = dv();
+    else if (a == "--supg-magic") o.supg_magic = dv();
     else if (a == "--supg-form") supgForm = sv();
     else if (a == "--supg-quad-points") supgQuad = iv();
     else if (a == "--simple-tol") o.simple_tol = dv();
@@ -128,9 +128,13 @@ int run(int argc, char** argv) {
   }
   if (mesh.empty()) throw Fail("--mesh required");
   if (mixlen || dg || weak) throw Fail("RANS closures (--mixing-length/--dg-inlet/--weak-wall) are not part of this solver");
-  if (supg) throw Fail("SUPG stabilisation is not part of this solver");
-  (void)supgForm;
-  (void)supgQuad;
+  o.supg = supg != 0 ? 1 : 0;
+  if (o.supg) {  // laminar SUPG entry checks (h8_supg_main_cli.inc:92-95)
+    if (!(o.supg_tau_scale > 0.0)) throw Fail("H8 SUPG tau scale must be positive");
+    if (!(o.supg_magic > 0.0)) throw Fail("H8 SUPG magic must be positive");
+    if (supgForm != "implicit") throw Fail("H8 GPU SUPG currently supports form=implicit");
+    if (supgQuad != 64) throw Fail("H8 GPU SUPG currently supports quad-points=64");
+  }
   (void)wallMode;
   auto pick = [](const std::string& v, std::initializer_list<const char*> names, const char* err) {
     int k = 0;
@@ -176,6 +180,10 @@ int run(int argc, char** argv) {
               "pressureSolver=%s hostSetupSeconds=%.6f deviceSetupSeconds=%.6f status=PASS\n",
               tag.c_str(), nc, nv, ncolors, levels, hierarchy.c_str(), smoother.c_str(), psolver.c_str(), setup_s,
               upload_s);
+  if (o.supg)
+    std::printf("NODALS_GPU_H8_SUPG tag=%s enabled=1 form=%s quadPoints=%d tauScale=%.8g magic=%.8g "
+                "setupSnapshotIncludesSUPG=1 status=PASS\n",
+                tag.c_str(), supgForm.c_str(), supgQuad, o.supg_tau_scale, o.supg_magic);
   std::fflush(stdout);
 
   bool converged = false, pressureAll = true, finiteAll = true;

@@ -61,15 +61,88 @@ __device__ __forceinline__ void write_partials(double (&v)[NV], double* part) {
 // the same pass.
 // ---------------------------------------------------------------------------
 
-// 8 lanes per cell; lane b computes column b of the cell's block.
+// Laminar SUPG terms, implicit form (h7_momentum_assembly.cuh:100-226; host
+// twin g4_host.hpp:324-419): column b of the cell block
+//   S[a][b] = sum_q tau_q w_q det (adv_q . grad phi_a) strong_b(q),
+//   strong_b = adv . grad phi_b (- nu lap phi_b for the bubbles),
+//   tau_q = tau_scale / sqrt(max(4 |adv_q|^2 / h^2 + magic (4 nu / h^2)^2, 1e-30)),
+// over the 64-point collapsed rule (rule: 64 x (lambda0..3, weight)).
+// Lane m of the 8-lane group holds the velocity q of basis m; lane b returns
+// S[0..7][b].
+struct SupgArgs {
+  double nu, tau_scale, magic;
+};
+template <class T>
+__device__ __forceinline__ void supg_column(const T* __restrict__ I, T h2, T dc, T q0, T q1, T q2,
+                                            const T* __restrict__ rule, const SupgArgs& sa, int lane8,
+                                            unsigned gmask, T S[8]) {
+  T gl[4][3], gd[4][4];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    gl[0][d] = -(I[d] + I[3 + d] + I[6 + d]);
+    gl[1][d] = I[d];
+    gl[2][d] = I[3 + d];
+    gl[3][d] = I[6 + d];
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = i; j < 4; ++j) {
+      T v = 0;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) v += gl[i][d] * gl[j][d];
+      gd[i][j] = gd[j][i] = v;
+    }
+  // this lane's basis function: vertex i = lane8 (< 4) or the bubble on the
+  // face opposite vertex i = lane8 - 4, with the other vertices j0 < j1 < j2
+  const int i = lane8 & 3;
+  const int j0 = i == 0 ? 1 : 0, j1 = i <= 1 ? 2 : 1, j2 = i <= 2 ? 3 : 2;
+  const bool bubble = lane8 >= 4;
+  const T nu = T(sa.nu), diff = T(4) * nu / h2;
+#pragma unroll
+  for (int a = 0; a < 8; ++a) S[a] = 0;
+  for (int qp = 0; qp < 64; ++qp) {
+    const T* lam = rule + 5 * qp;
+    const T l0 = lam[j0], l1 = lam[j1], l2 = lam[j2];
+    const T phi = bubble ? T(27) * l0 * l1 * l2 : lam[i];
+    const T a0 = group_sum<8>(q0 * phi, gmask), a1 = group_sum<8>(q1 * phi, gmask), a2 = group_sum<8>(q2 * phi, gmask);
+    T g0, g1, g2, lap = 0;
+    if (!bubble) {
+      g0 = gl[i][0];
+      g1 = gl[i][1];
+      g2 = gl[i][2];
+    } else {
+      g0 = T(27) * (l1 * l2 * gl[j0][0] + l0 * l2 * gl[j1][0] + l0 * l1 * gl[j2][0]);
+      g1 = T(27) * (l1 * l2 * gl[j0][1] + l0 * l2 * gl[j1][1] + l0 * l1 * gl[j2][1]);
+      g2 = T(27) * (l1 * l2 * gl[j0][2] + l0 * l2 * gl[j1][2] + l0 * l1 * gl[j2][2]);
+      lap = T(54) * (l2 * gd[j0][j1] + l1 * gd[j0][j2] + l0 * gd[j1][j2]);
+    }
+    const T stream = a0 * g0 + a1 * g1 + a2 * g2;
+    const T strong = bubble ? -nu * lap + stream : stream;
+    const T speed2 = a0 * a0 + a1 * a1 + a2 * a2;
+    const T den = fmax(T(4) * speed2 / h2 + T(sa.magic) * diff * diff, T(1e-30));
+    const T w = T(sa.tau_scale) / sqrt(den) * lam[4] * dc;
+    const T ta = w * stream;
+#pragma unroll
+    for (int a = 0; a < 8; ++a) S[a] += __shfl_sync(gmask, ta, a, 8) * strong;
+  }
+}
+
+// 8 lanes per cell; lane b computes column b of the cell's block (convection,
+// plus the SUPG terms when supg_rule is not null).
 template <class T>
 __global__ void __launch_bounds__(kBlock) mom_cell_conv(int nc, const int32_t* __restrict__ ref,
                                                         const T* __restrict__ fixed, const T* __restrict__ u0,
                                                         const T* __restrict__ u1, const T* __restrict__ u2,
                                                         const T* __restrict__ invJ, const T* __restrict__ det,
-                                                        const T* __restrict__ centT, T* __restrict__ C) {
+                                                        const T* __restrict__ centT, T* __restrict__ C,
+                                                        const T* __restrict__ supg_rule, const T* __restrict__ h2,
+                                                        SupgArgs sa) {
   __shared__ T sT[1536];
+  __shared__ T sQ[320];
   for (int k = threadIdx.x; k < 1536; k += blockDim.x) sT[k] = centT[k];
+  if (supg_rule)
+    for (int k = threadIdx.x; k < 320; k += blockDim.x) sQ[k] = supg_rule[k];
   __syncthreads();
   const int lane8 = threadIdx.x & 7;
   const int groups = blockDim.x >> 3;
@@ -101,6 +174,8 @@ __global__ void __launch_bounds__(kBlock) mom_cell_conv(int nc, const int32_t* _
     }
     const T dc = det[c];
     T* out = C + 64 * (size_t)c + lane8;
+    T S[8];
+    if (supg_rule) supg_column<T>(I, h2[c], dc, q0, q1, q2, sQ, sa, lane8, gmask, S);
 #pragma unroll 2
     for (int a = 0; a < 8; ++a) {
       T cv = 0;
@@ -109,7 +184,7 @@ __global__ void __launch_bounds__(kBlock) mom_cell_conv(int nc, const int32_t* _
         const T* t = sT + ((a * 8 + m) * 8 + lane8) * 3;
         cv += w[m][0] * t[0] + w[m][1] * t[1] + w[m][2] * t[2];
       }
-      out[8 * a] = cv * dc;
+      out[8 * a] = supg_rule ? cv * dc + S[a] : cv * dc;
     }
   }
 }
@@ -162,55 +237,48 @@ __global__ void __launch_bounds__(kBlock) mom_assemble(MomArgs<T> g) {
     __syncwarp(gmask);
     T conv0 = 0, conv1 = 0, conv2 = 0, bt0 = 0, bt1 = 0, bt2 = 0;
     const int z0 = g.inc_off[i], z1 = g.inc_off[i + 1];
-    for (int zb = z0; zb < z1; zb += 8) {
-      // up to 8 incidence words in one coalesced load, then the gathers of
-      // four incidences in flight before their (ordered) updates
-      const int zn = min(8, z1 - zb);
-      const uint32_t mine = lane8 < zn ? g.inc[zb + lane8] : 0u;
-      for (int k0 = 0; k0 < zn; k0 += 4) {
-        int gk[4], sk[4];
-        T vk[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          const bool ok = k0 + u < zn;
-          const uint32_t pk = __shfl_sync(gmask, mine, (k0 + u) & 7, 8);
-          const int c = (int)(pk >> 3), a = (int)(pk & 7u);
-          const size_t e = 64 * (size_t)c + 8 * a + lane8;
-          gk[u] = ok ? g.ref[8 * (size_t)c + lane8] : 0;
-          vk[u] = ok ? g.C[e] : T(0);
-          sk[u] = ok ? (int)g.slot[e] : 0;
+    for (int z = z0; z < z1; z += 2) {
+      // two incidences in flight; applied in order
+      const bool two = z + 1 < z1;
+      const uint32_t pa = g.inc[z], pb = two ? g.inc[z + 1] : pa;
+      const int ca = (int)(pa >> 3), aa = (int)(pa & 7u), cb = (int)(pb >> 3), ab = (int)(pb & 7u);
+      const int ga = g.ref[8 * (size_t)ca + lane8], gb = g.ref[8 * (size_t)cb + lane8];
+      const T va = g.C[64 * (size_t)ca + 8 * aa + lane8], vb = g.C[64 * (size_t)cb + 8 * ab + lane8];
+      const int sa = g.slot[64 * (size_t)ca + 8 * aa + lane8], sb = g.slot[64 * (size_t)cb + 8 * ab + lane8];
+      if (ga >= 0) {
+        buf[sa] += va;
+      } else {
+        const T* f = g.fixed + 3 * (size_t)(-ga - 1);
+        conv0 -= va * f[0];
+        conv1 -= va * f[1];
+        conv2 -= va * f[2];
+      }
+      if (lane8 == 0) {
+        const T pv = g.p[ca];
+        const T* B = g.bco + 24 * (size_t)ca + 3 * aa;
+        bt0 += B[0] * pv;
+        bt1 += B[1] * pv;
+        bt2 += B[2] * pv;
+      }
+      __syncwarp(gmask);
+      if (two) {
+        if (gb >= 0) {
+          buf[sb] += vb;
+        } else {
+          const T* f = g.fixed + 3 * (size_t)(-gb - 1);
+          conv0 -= vb * f[0];
+          conv1 -= vb * f[1];
+          conv2 -= vb * f[2];
         }
-        // lane u < 4: the B^T p terms of incidence k0 + u
-        T t0 = 0, t1 = 0, t2 = 0;
-        {
-          const uint32_t pk = __shfl_sync(gmask, mine, (k0 + (lane8 & 3)) & 7, 8);
-          if (lane8 < 4 && k0 + lane8 < zn) {
-            const int c = (int)(pk >> 3), a = (int)(pk & 7u);
-            const T* B = g.bco + 24 * (size_t)c + 3 * a;
-            const T pv = g.p[c];
-            t0 = B[0] * pv;
-            t1 = B[1] * pv;
-            t2 = B[2] * pv;
-          }
-        }
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          if (k0 + u < zn) {
-            if (gk[u] >= 0) {
-              buf[sk[u]] += vk[u];
-            } else {
-              const T* f = g.fixed + 3 * (size_t)(-gk[u] - 1);
-              conv0 -= vk[u] * f[0];
-              conv1 -= vk[u] * f[1];
-              conv2 -= vk[u] * f[2];
-            }
-            bt0 += __shfl_sync(gmask, t0, u, 8);
-            bt1 += __shfl_sync(gmask, t1, u, 8);
-            bt2 += __shfl_sync(gmask, t2, u, 8);
-            __syncwarp(gmask);
-          }
+        if (lane8 == 0) {
+          const T pv = g.p[cb];
+          const T* B = g.bco + 24 * (size_t)cb + 3 * ab;
+          bt0 += B[0] * pv;
+          bt1 += B[1] * pv;
+          bt2 += B[2] * pv;
         }
       }
+      __syncwarp(gmask);
     }
     conv0 = group_sum<8>(conv0, gmask);
     conv1 = group_sum<8>(conv1, gmask);
@@ -239,9 +307,11 @@ __global__ void __launch_bounds__(kBlock) mom_assemble(MomArgs<T> g) {
 
 // One multicolour Gauss-Seidel colour pass on the shared momentum matrix,
 // three right-hand sides (g5e_fp32_kernels.cuh:106-116).  8 lanes per row.
+// rows: the colour's rows; span: their (begin, end) in the CSR, in the same
+// order, so the row's entries and its own data load in parallel.
 template <class T>
 __global__ void __launch_bounds__(kBlock) mom_gs_color(int count, const int32_t* __restrict__ rows,
-                                                       const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                                       const int2* __restrict__ span, const int32_t* __restrict__ ci,
                                                        const T* __restrict__ av, const T* __restrict__ diag,
                                                        const T* __restrict__ b0, const T* __restrict__ b1,
                                                        const T* __restrict__ b2, T* __restrict__ x0, T* __restrict__ x1,
@@ -251,8 +321,19 @@ __global__ void __launch_bounds__(kBlock) mom_gs_color(int count, const int32_t*
   if (q >= count) return;
   const unsigned gmask = group8_mask();
   const int i = rows[q];
+  const int2 sp = span[q];
+  T d = 0, c0 = 0, c1 = 0, c2 = 0, y0 = 0, y1 = 0, y2 = 0;
+  if (lane8 == 0) {
+    d = diag[i];
+    c0 = b0[i];
+    c1 = b1[i];
+    c2 = b2[i];
+    y0 = x0[i];
+    y1 = x1[i];
+    y2 = x2[i];
+  }
   T s0 = 0, s1 = 0, s2 = 0;
-  for (int k = rp[i] + lane8; k < rp[i + 1]; k += 8) {
+  for (int k = sp.x + lane8; k < sp.y; k += 8) {
     const int j = ci[k];
     if (j == i) continue;
     const T a = av[k];
@@ -264,10 +345,10 @@ __global__ void __launch_bounds__(kBlock) mom_gs_color(int count, const int32_t*
   s1 = group_sum<8>(s1, gmask);
   s2 = group_sum<8>(s2, gmask);
   if (lane8 == 0) {
-    const T iv = T(1) / diag[i];
-    x0[i] = (T(1) - omega) * x0[i] + omega * ((b0[i] - s0) * iv);
-    x1[i] = (T(1) - omega) * x1[i] + omega * ((b1[i] - s1) * iv);
-    x2[i] = (T(1) - omega) * x2[i] + omega * ((b2[i] - s2) * iv);
+    const T iv = T(1) / d;
+    x0[i] = (T(1) - omega) * y0 + omega * ((c0 - s0) * iv);
+    x1[i] = (T(1) - omega) * y1 + omega * ((c1 - s1) * iv);
+    x2[i] = (T(1) - omega) * y2 + omega * ((c2 - s2) * iv);
   }
 }
 
@@ -338,13 +419,30 @@ __global__ void __launch_bounds__(kBlock) continuity(int nc, const int32_t* __re
 // ---------------------------------------------------------------------------
 // CSR SpMV family, warp per row (h2b_fine_csr.cuh:579-596, h6_coarse_spmv.cuh:10-32)
 // ---------------------------------------------------------------------------
+// Lane l sums entries rb+l, rb+l+32, ... in that order; the loads of four
+// entries are issued before their products are added (same order, same
+// result, a quarter of the dependent memory round trips).
+template <class T>
+__device__ __forceinline__ T lane_strided_dot(int rb, int re, const int32_t* __restrict__ ci, const T* __restrict__ v,
+                                              const T* __restrict__ x, int lane) {
+  T s = 0;
+  int k = rb + lane;
+  for (; k + 96 < re; k += 128) {
+    const int c0 = ci[k], c1 = ci[k + 32], c2 = ci[k + 64], c3 = ci[k + 96];
+    const T a0 = v[k], a1 = v[k + 32], a2 = v[k + 64], a3 = v[k + 96];
+    const T x0 = x[c0], x1 = x[c1], x2 = x[c2], x3 = x[c3];
+    s += a0 * x0;
+    s += a1 * x1;
+    s += a2 * x2;
+    s += a3 * x3;
+  }
+  for (; k < re; k += 32) s += v[k] * x[ci[k]];
+  return s;
+}
 template <class T>
 __device__ __forceinline__ T warp_row_dot(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
                                           const T* __restrict__ v, const T* __restrict__ x, int i, int lane) {
-  T s = 0;
-  const int rb = rp[i], re = rp[i + 1];
-  for (int k = rb + lane; k < re; k += 32) s += v[k] * x[ci[k]];
-  return warp_sum(s);
+  return warp_sum(lane_strided_dot(rp[i], rp[i + 1], ci, v, x, lane));
 }
 
 // y = A x
@@ -361,14 +459,17 @@ __global__ void __launch_bounds__(kBlock) spmv(int n, const int32_t* __restrict_
 template <class T>
 __global__ void __launch_bounds__(kBlock) spmv_resid(int n, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
                                                      const T* __restrict__ v, const T* __restrict__ x,
-                                                     const T* __restrict__ b, T* __restrict__ r, T* __restrict__ r2) {
+                                                     const T* __restrict__ b, T* __restrict__ r, T* __restrict__ r2,
+                                                     const T* __restrict__ den, T w) {
   const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (i >= n) return;
   const T s = warp_row_dot(rp, ci, v, x, i, lane);
   if (lane == 0) {
+    // r; r2 = r (den null) or the first Jacobi step w r / den
     const T q = b[i] - s;
     r[i] = q;
-    if (r2) r2[i] = q;
+    if (den) r2[i] = w * q / den[i];
+    else if (r2) r2[i] = q;
   }
 }
 
@@ -377,13 +478,17 @@ template <class T>
 __global__ void __launch_bounds__(kBlock) spmv_smooth(int n, const int32_t* __restrict__ rp,
                                                       const int32_t* __restrict__ ci, const T* __restrict__ v,
                                                       const T* __restrict__ xin, const T* __restrict__ b,
-                                                      const T* __restrict__ den, T w, T* __restrict__ xout) {
+                                                      const T* __restrict__ den, T w, T* __restrict__ xout,
+                                                      T* __restrict__ add_to) {
   const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (i >= n) return;
   const T s = warp_row_dot(rp, ci, v, xin, i, lane);
   if (lane == 0) {
+    // with add_to the step is added to add_to instead of stored in xout
     const T r = b[i] - s;
-    xout[i] = xin[i] + w * r / den[i];
+    const T val = xin[i] + w * r / den[i];
+    if (add_to) add_to[i] += val;
+    else xout[i] = val;
   }
 }
 
@@ -534,8 +639,20 @@ __global__ void prolong_add(int nf, const int32_t* __restrict__ pr, const int32_
                             const T* __restrict__ pv, const T* __restrict__ c, T* __restrict__ f) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nf) return;
+  // sequential sum; loads of four entries issued ahead of their products
   T s = 0;
-  for (int k = pr[i]; k < pr[i + 1]; ++k) s += pv[k] * c[pc[k]];
+  int k = pr[i];
+  const int ke = pr[i + 1];
+  for (; k + 3 < ke; k += 4) {
+    const int c0 = pc[k], c1 = pc[k + 1], c2 = pc[k + 2], c3 = pc[k + 3];
+    const T a0 = pv[k], a1 = pv[k + 1], a2 = pv[k + 2], a3 = pv[k + 3];
+    const T x0 = c[c0], x1 = c[c1], x2 = c[c2], x3 = c[c3];
+    s += a0 * x0;
+    s += a1 * x1;
+    s += a2 * x2;
+    s += a3 * x3;
+  }
+  for (; k < ke; ++k) s += pv[k] * c[pc[k]];
   f[i] += s;
 }
 // x = Ainv b, dense row-major, warp per row
@@ -606,8 +723,7 @@ enum SellMode { SELL_Y = 0, SELL_RESID = 1, SELL_SMOOTH = 2, SELL_DOT = 3 };
 // accumulators, fixed order -> deterministic.
 template <class T, bool D16>
 __device__ __forceinline__ T sell_row(const Sell& A, const T* __restrict__ v, const T* __restrict__ x, int i) {
-  // entries in flight per thread: 8 for 8-byte values, 16 for 4-byte ones
-  constexpr int U = sizeof(T) == 4 ? 16 : 8;
+  constexpr int U = 8;  // entries in flight per thread
   const int s = i >> 5;
   const int b = A.base[s] + (i & 31);
   const int w = A.width[s];
@@ -662,11 +778,16 @@ __global__ void __launch_bounds__(kBlock) sell_spmv(Sell A, const T* __restrict_
   if (MODE == SELL_Y) {
     y[i] = s;
   } else if (MODE == SELL_RESID) {
+    // y = r; y2 = r (den null) or the first Jacobi step w r / den
     const T q = b[i] - s;
     y[i] = q;
-    if (y2) y2[i] = q;
+    if (den) y2[i] = w * q / den[i];
+    else if (y2) y2[i] = q;
   } else {
-    y[i] = x[i] + w * (b[i] - s) / den[i];
+    // smoothing step; with y2 the step is added to y2 instead of stored
+    const T val = x[i] + w * (b[i] - s) / den[i];
+    if (y2) y2[i] += val;
+    else y[i] = val;
   }
 }
 
@@ -688,82 +809,103 @@ __global__ void refresh_geometry(int nc, const int32_t* __restrict__ coff, const
   }
 }
 
-// Fine Schur numeric refresh A_p = B diag(rau) B^T (h8_precomputed_b.cuh:37-91),
-// warp per pressure row, written into the SELL layout.  Each value is
-// sum_q rau_{g(c,a_q)} G_q over the row's contributions to that entry.  The
-// contributions of a row were sorted by destination slot at setup (stable,
-// from the reference's (basis, incidence) order of h2b_fine_csr.cuh:480-520).
-// Lanes take one contribution each (a coalesced stream of G and cs), then
-// every slot is summed sequentially in that order by a shuffle chain: lane L
-// adds its product to the final running sum of lane L-1 when both belong to
-// the same slot, so each value is the reference's serial sum; no atomics.
-// Slots are written by the lane holding their last contribution.  Values go
-// to val (operator precision T) and, in the mixed mode, also to valA (AMG
-// precision TA); the diagonal and L1 row sums feed the AMG smoothers.
+// Fine Schur numeric refresh A_p = B diag(rau) B^T (h8_precomputed_b.cuh:37-91)
+// into the SELL layout.  Each value is sum_q rau_{g(c,a_q)} G_q over the
+// row's contributions to that entry.  The contributions of a row were sorted
+// by destination slot at setup (stable, from the reference's (basis,
+// incidence) order of h2b_fine_csr.cuh:480-520).
+//
+// One block per SELL slice (32 rows), 4 rows per warp.  For a row, lanes take
+// one contribution each (a coalesced stream of G and cs), then every slot is
+// summed sequentially in that order by a shuffle chain: lane L adds its
+// product to the final running sum of lane L-1 when both belong to the same
+// slot, so each value is the reference's serial sum; no atomics.  The lane
+// holding a slot's last contribution puts the value into the slice's
+// shared-memory image ([entry][row], row stride 33 against bank conflicts),
+// which the block then writes out contiguously in SELL order (padding and
+// slots without contributions as zeros).  Values go to val (operator
+// precision T) and, in the mixed mode, also to valA (AMG precision TA); the
+// diagonal and L1 row sums feed the AMG smoothers.
+// Dynamic shared memory: 33 * max slice width * sizeof(T).
 template <class T, class TA>
 __global__ void __launch_bounds__(kBlock) sell_refresh(int nc, const int32_t* __restrict__ coff,
                                                        const uint16_t* __restrict__ cs, const T* __restrict__ G,
                                                        const int32_t* __restrict__ ref, const T* __restrict__ rau,
                                                        const int32_t* __restrict__ dslot, const int32_t* __restrict__ sbase,
-                                                       T* __restrict__ val, TA* __restrict__ valA, TA* __restrict__ diag,
+                                                       const int32_t* __restrict__ swidth, T* __restrict__ val,
+                                                       TA* __restrict__ valA, TA* __restrict__ diag,
                                                        TA* __restrict__ l1) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* sv = reinterpret_cast<T*>(smem_raw);
   __shared__ T sR[kWarps][8];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (c >= nc) return;
-  if (lane < 8) {
-    const int g = ref[8 * (size_t)c + lane];
-    sR[w][lane] = g >= 0 ? rau[g] : T(0);
-  }
-  __syncwarp();
-  const int qb = coff[c], qe = coff[c + 1];
-  const int out = sbase[c >> 5] + (c & 31);
-  const int ds = dslot[c];
-  T asum = 0, carry = 0;
-  int carry_slot = -1;
+  const int slice = blockIdx.x;
+  const int width = swidth[slice];
+  for (int t = threadIdx.x; t < 33 * width; t += blockDim.x) sv[t] = T(0);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
   const unsigned below = (1u << lane) - 1u;
-  for (int q0 = qb; q0 < qe; q0 += 32) {
-    const int q = q0 + lane;
-    const bool live = q < qe;
-    int sl = -1;
-    T p = 0;
-    if (live) {
-      const unsigned v = cs[q];
-      sl = (int)(v >> 3);
-      p = sR[w][v & 7u] * G[q];
+  for (int rr = 0; rr < 32 / kWarps; ++rr) {
+    const int r = wp * (32 / kWarps) + rr;
+    const int c = slice * 32 + r;
+    if (c >= nc) break;  // warp-uniform
+    if (lane < 8) {
+      const int g = ref[8 * (size_t)c + lane];
+      sR[wp][lane] = g >= 0 ? rau[g] : T(0);
     }
-    const int prev = __shfl_up_sync(0xffffffffu, sl, 1);
-    const int next = __shfl_down_sync(0xffffffffu, sl, 1);
-    // lane 31's run continues into the next chunk when the next contribution
-    // has the same slot
-    const bool cont = lane == 31 && live && q + 1 < qe && (int)(cs[q + 1] >> 3) == sl;
-    const bool head = !live || (lane == 0 ? sl != carry_slot : sl != prev);
-    const bool tail = live && (lane == 31 ? !cont : next != sl);
-    const unsigned heads = __ballot_sync(0xffffffffu, head) | 1u;
-    // position of this lane inside its slot's run within this chunk
-    const int pos = lane - (31 - __clz(heads & (below | (1u << lane))));
-    T acc = (lane == 0 && !head) ? carry + p : p;
-    int maxpos = pos;
+    __syncwarp();
+    const int qb = coff[c], qe = coff[c + 1];
+    const int ds = dslot[c];
+    T asum = 0, carry = 0;
+    int carry_slot = -1;
+    for (int q0 = qb; q0 < qe; q0 += 32) {
+      const int q = q0 + lane;
+      const bool live = q < qe;
+      int sl = -1;
+      T p = 0;
+      if (live) {
+        const unsigned v = cs[q];
+        sl = (int)(v >> 3);
+        p = sR[wp][v & 7u] * G[q];
+      }
+      const int prev = __shfl_up_sync(0xffffffffu, sl, 1);
+      const int next = __shfl_down_sync(0xffffffffu, sl, 1);
+      // lane 31's run continues into the next chunk when the next
+      // contribution has the same slot
+      const bool cont = lane == 31 && live && q + 1 < qe && (int)(cs[q + 1] >> 3) == sl;
+      const bool head = !live || (lane == 0 ? sl != carry_slot : sl != prev);
+      const bool tail = live && (lane == 31 ? !cont : next != sl);
+      const unsigned heads = __ballot_sync(0xffffffffu, head) | 1u;
+      // position of this lane inside its slot's run within this chunk
+      const int pos = lane - (31 - __clz(heads & (below | (1u << lane))));
+      T acc = (lane == 0 && !head) ? carry + p : p;
+      int maxpos = pos;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) maxpos = max(maxpos, __shfl_xor_sync(0xffffffffu, maxpos, o));
-    for (int j = 1; j <= maxpos; ++j) {
-      const T up = __shfl_up_sync(0xffffffffu, acc, 1);
-      if (pos == j) acc = up + p;
+      for (int o = 16; o > 0; o >>= 1) maxpos = max(maxpos, __shfl_xor_sync(0xffffffffu, maxpos, o));
+      for (int j = 1; j <= maxpos; ++j) {
+        const T up = __shfl_up_sync(0xffffffffu, acc, 1);
+        if (pos == j) acc = up + p;
+      }
+      if (tail) {
+        sv[sl * 33 + r] = acc;
+        if (sl == ds) diag[c] = TA(acc);
+        asum += fabs(acc);
+      }
+      // a slot run cut by the chunk end continues from lane 31's running sum
+      carry = __shfl_sync(0xffffffffu, acc, 31);
+      carry_slot = __shfl_sync(0xffffffffu, sl, 31);
     }
-    if (tail) {
-      const size_t o = (size_t)out + 32 * (size_t)sl;
-      val[o] = acc;
-      if (valA) valA[o] = TA(acc);
-      if (sl == ds) diag[c] = TA(acc);
-      asum += fabs(acc);
+    if (l1) {
+      asum = warp_sum(asum);
+      if (lane == 0) l1[c] = TA(asum);
     }
-    // a slot run cut by the chunk end continues from lane 31's running sum
-    carry = __shfl_sync(0xffffffffu, acc, 31);
-    carry_slot = __shfl_sync(0xffffffffu, sl, 31);
+    __syncwarp();
   }
-  if (l1) {
-    asum = warp_sum(asum);
-    if (lane == 0) l1[c] = TA(asum);
+  __syncthreads();
+  const size_t base = (size_t)sbase[slice];
+  for (int t = threadIdx.x; t < 32 * width; t += blockDim.x) {
+    const T v = sv[(t >> 5) * 33 + (t & 31)];
+    val[base + t] = v;
+    if (valA) valA[base + t] = TA(v);
   }
 }
 
@@ -771,6 +913,17 @@ template <class Tin, class Tout>
 __global__ void cast_copy(int n, const Tin* __restrict__ a, Tout* __restrict__ b) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) b[i] = Tout(a[i]);
+}
+// b = a in the other precision, and the fine pre-smoother's diagonal step
+// x1 = w0 b / den0
+template <class Tin, class Tout>
+__global__ void cast_jacobi(int n, const Tin* __restrict__ a, Tout* __restrict__ b, Tout w0,
+                            const Tout* __restrict__ den0, Tout* __restrict__ x1) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const Tout v = Tout(a[i]);
+  b[i] = v;
+  x1[i] = w0 * v / den0[i];
 }
 
 // multicolour GS colour pass on the SELL fine operator (thread per row)
@@ -797,13 +950,16 @@ __global__ void sell_gs_color(int count, const int32_t* __restrict__ rows, Sell 
 template <class T>
 __global__ void __launch_bounds__(kBlock) restrict_warp(int nc, const int32_t* __restrict__ rr,
                                                         const int32_t* __restrict__ rc, const T* __restrict__ rv,
-                                                        const T* __restrict__ f, T* __restrict__ c) {
+                                                        const T* __restrict__ f, T* __restrict__ c,
+                                                        const T* __restrict__ den0, T w0, T* __restrict__ x1) {
   const int I = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (I >= nc) return;
-  T s = 0;
-  for (int k = rr[I] + lane; k < rr[I + 1]; k += 32) s += rv[k] * f[rc[k]];
-  s = warp_sum(s);
-  if (lane == 0) c[I] = s;
+  T s = warp_sum(lane_strided_dot(rr[I], rr[I + 1], rc, rv, f, lane));
+  if (lane == 0) {
+    c[I] = s;
+    // with x1: the coarse pre-smoother's diagonal step w0 c / den0
+    if (x1) x1[I] = w0 * s / den0[I];
+  }
 }
 
 }  // namespace k

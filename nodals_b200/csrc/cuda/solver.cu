@@ -77,10 +77,13 @@ struct DBuf {
 
 // Optional per-category CUDA-event timing of kernel launches on the solver's
 // stream (the analogue of the reference's H0Profiler, h8_main_base.cu:58-99).
+// fine_spmv: the physical fine operator (Krylov A p, power iterations);
+// fine_spmv_amg: the fine-level operator inside the V-cycle
 enum ProfCat { P_FINE_SPMV = 0, P_COARSE_SPMV, P_REFRESH, P_ASSEMBLE, P_GS, P_CONTINUITY, P_TRANSFER, P_TERMINAL,
-               P_VECTOR, P_NCAT };
+               P_VECTOR, P_FINE_AMG, P_NCAT };
 static const char* const kProfNames[P_NCAT] = {"fine_spmv", "coarse_spmv", "fine_refresh", "mom_assemble", "mom_gs",
-                                               "continuity", "transfer", "terminal_dense", "vector_reduce"};
+                                               "continuity", "transfer", "terminal_dense", "vector_reduce",
+                                               "fine_spmv_amg"};
 struct Profiler {
   bool on = false;
   std::vector<cudaEvent_t> ev;
@@ -266,6 +269,14 @@ class Solver final : public ISolver {
     color_rows_.upload(S.color_rows);
     color_off_ = S.color_off;
     {
+      std::vector<int2> span(S.color_rows.size());
+      for (size_t q = 0; q < span.size(); ++q) {
+        const int i = S.color_rows[q];
+        span[q] = make_int2((int)S.mom.row[(size_t)i], (int)S.mom.row[(size_t)i + 1]);
+      }
+      color_span_.upload(span);
+    }
+    {
       const RefTensors& RT = ref_tensors();
       std::vector<double> t(1536);
       std::memcpy(t.data(), &RT.T[0][0][0][0], sizeof(double) * 1536);
@@ -278,6 +289,15 @@ class Solver final : public ISolver {
     if (mom_smem_ > 200 * 1024) throw std::runtime_error("momentum row too long for the shared-memory assembly buffer");
     NDS_CUDA(cudaFuncSetAttribute(k::mom_assemble<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mom_smem_));
     cconv_.alloc(64 * (size_t)nc_);
+    if (o_.supg) {
+      h2_.upload(S.h2);
+      std::vector<double> rule;
+      for (const auto& q : tet_rule_64()) {
+        for (int k = 0; k < 4; ++k) rule.push_back(q.lam[(size_t)k]);
+        rule.push_back(q.w);
+      }
+      supg_rule_.upload(rule);
+    }
 
     // fine Schur CSR with contributions regrouped by destination slot
     const FineTopo& F = S.fine;
@@ -347,6 +367,11 @@ class Solver final : public ISolver {
         for (int q = 0; q < width[(size_t)s0]; ++q) scol[(size_t)base[(size_t)s0] + 32 * (size_t)q + l] = 0;
       }
       swidth_.upload(width);
+      const int wmax = *std::max_element(width.begin(), width.end());
+      refresh_smem_ = (size_t)33 * wmax * sizeof(T);
+      if (refresh_smem_ > 200 * 1024) throw std::runtime_error("fine Schur row too long for the refresh slice buffer");
+      NDS_CUDA(cudaFuncSetAttribute(k::sell_refresh<T, TA>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)refresh_smem_));
       sbase_.upload(base);
       fdslot_.upload(dslot);
       fval_.alloc(scol.size());
@@ -570,6 +595,15 @@ class Solver final : public ISolver {
   void amg_T(const T* b, T* z) {
     if constexpr (kSame) {
       amg_apply(b, z);
+    } else if (o_.amg_smoother != NDS_SM_MCGS) {
+      // the cast also takes the fine pre-smoother's diagonal step
+      const PolyPlan pl = fine_plan();
+      k::cast_jacobi<T, TA><<<grid_for(nc_), kBlock, 0, st_>>>(nc_, b, rA_.p, TA(pl.w0), pl.den0,
+                                                               poly_first(pl, zA_.p, fpong_.p));
+      NDS_LAUNCH();
+      amg_apply(rA_.p, zA_.p, true);
+      k::cast_copy<TA, T><<<grid_for(nc_), kBlock, 0, st_>>>(nc_, zA_.p, z);
+      NDS_LAUNCH();
     } else {
       k::cast_copy<T, TA><<<grid_for(nc_), kBlock, 0, st_>>>(nc_, b, rA_.p);
       NDS_LAUNCH();
@@ -621,6 +655,7 @@ class Solver final : public ISolver {
     const int32_t* rp;
     const int32_t* ci;
     const V* v;
+    int cat;  // profiler category
   };
   template <int MODE, class V>
   void sell_launch(const OpView<V>& A, int grid, const V* x, const V* b, const V* den, double w, V* y, V* y2) {
@@ -630,31 +665,39 @@ class Solver final : public ISolver {
       k::sell_spmv<V, MODE, false><<<grid, kBlock, 0, st_>>>(A.s, A.v, x, b, den, V(w), y, y2, part_.p);
   }
   // physical operator (precision T) and the AMG's fine operator (precision TA)
-  OpView<T> fine_op() const { return {nc_, true, sell_, nullptr, nullptr, fval_.p}; }
+  OpView<T> fine_op() const { return {nc_, true, sell_, nullptr, nullptr, fval_.p, P_FINE_SPMV}; }
   OpView<TA> fine_opA() const {
-    if constexpr (kSame) return {nc_, true, sell_, nullptr, nullptr, fval_.p};
-    else return {nc_, true, sell_, nullptr, nullptr, fvalA_.p};
+    if constexpr (kSame) return {nc_, true, sell_, nullptr, nullptr, fval_.p, P_FINE_AMG};
+    else return {nc_, true, sell_, nullptr, nullptr, fvalA_.p, P_FINE_AMG};
   }
-  OpView<TA> level_op(const Level& A) const { return {A.n, false, k::Sell{}, A.row.p, A.col.p, A.val.p}; }
+  OpView<TA> level_op(const Level& A) const {
+    return {A.n, false, k::Sell{}, A.row.p, A.col.p, A.val.p, P_COARSE_SPMV};
+  }
   template <class V>
   void op_spmv(const OpView<V>& A, const V* x, V* y) {
-    ProfScope ps(prof, st_, A.sell ? P_FINE_SPMV : P_COARSE_SPMV);
+    ProfScope ps(prof, st_, A.cat);
     if (A.sell) sell_launch<k::SELL_Y, V>(A, grid_for(A.n), x, nullptr, nullptr, 0.0, y, nullptr);
     else k::spmv<V><<<grid_for((long long)A.n * 32), kBlock, 0, st_>>>(A.n, A.rp, A.ci, A.v, x, y);
     NDS_LAUNCH();
   }
+  // r = b - A x; r2 = r, or (den given) the first Jacobi step w r / den
   template <class V>
-  void op_resid(const OpView<V>& A, const V* x, const V* b, V* r, V* r2 = nullptr) {
-    ProfScope ps(prof, st_, A.sell ? P_FINE_SPMV : P_COARSE_SPMV);
-    if (A.sell) sell_launch<k::SELL_RESID, V>(A, grid_for(A.n), x, b, nullptr, 0.0, r, r2);
-    else k::spmv_resid<V><<<grid_for((long long)A.n * 32), kBlock, 0, st_>>>(A.n, A.rp, A.ci, A.v, x, b, r, r2);
+  void op_resid(const OpView<V>& A, const V* x, const V* b, V* r, V* r2 = nullptr, const V* den = nullptr,
+                double w = 0.0) {
+    ProfScope ps(prof, st_, A.cat);
+    if (A.sell) sell_launch<k::SELL_RESID, V>(A, grid_for(A.n), x, b, den, w, r, r2);
+    else
+      k::spmv_resid<V><<<grid_for((long long)A.n * 32), kBlock, 0, st_>>>(A.n, A.rp, A.ci, A.v, x, b, r, r2, den, V(w));
     NDS_LAUNCH();
   }
+  // xout = xin + w (b - A xin) / den, or (add_to given) add_to += that
   template <class V>
-  void op_smooth(const OpView<V>& A, const V* xin, const V* b, const V* den, double w, V* xout) {
-    ProfScope ps(prof, st_, A.sell ? P_FINE_SPMV : P_COARSE_SPMV);
-    if (A.sell) sell_launch<k::SELL_SMOOTH, V>(A, grid_for(A.n), xin, b, den, w, xout, nullptr);
-    else k::spmv_smooth<V><<<grid_for((long long)A.n * 32), kBlock, 0, st_>>>(A.n, A.rp, A.ci, A.v, xin, b, den, V(w), xout);
+  void op_smooth(const OpView<V>& A, const V* xin, const V* b, const V* den, double w, V* xout, V* add_to = nullptr) {
+    ProfScope ps(prof, st_, A.cat);
+    if (A.sell) sell_launch<k::SELL_SMOOTH, V>(A, grid_for(A.n), xin, b, den, w, xout, add_to);
+    else
+      k::spmv_smooth<V><<<grid_for((long long)A.n * 32), kBlock, 0, st_>>>(A.n, A.rp, A.ci, A.v, xin, b, den, V(w), xout,
+                                                                          add_to);
     NDS_LAUNCH();
   }
   template <class V>
@@ -671,8 +714,8 @@ class Solver final : public ISolver {
   // fine Schur operator
   void refresh_fine(const T* rau) {
     ProfScope ps(prof, st_, P_REFRESH);
-    k::sell_refresh<T, TA><<<grid_for((long long)nc_ * 32), kBlock, 0, st_>>>(
-        nc_, fcoff_.p, fcs_.p, fgeo_.p, ref_.p, rau, fdslot_.p, sbase_.p, fval_.p,
+    k::sell_refresh<T, TA><<<(nc_ + 31) / 32, kBlock, refresh_smem_, st_>>>(
+        nc_, fcoff_.p, fcs_.p, fgeo_.p, ref_.p, rau, fdslot_.p, sbase_.p, swidth_.p, fval_.p,
         kSame ? nullptr : fvalA_.p, fdiag_.p, fl1_.p);
     NDS_LAUNCH();
   }
@@ -681,33 +724,45 @@ class Solver final : public ISolver {
   // ------------------------------------------------------------- smoothers
   // x = S(b) from a zero initial guess.  Jacobi-type steps write to a second
   // buffer (xin is read by every row), then the result is copied back.
-  void poly_smooth(const OpView<TA>& A, const TA* diag, const TA* b, TA* x, TA* pong, double lambda, bool cheb,
-                   const TA* den_jac, int sweeps) {
-    // x = S(b) from a zero guess: one diagonal step, then m Jacobi-type steps
-    // ping-ponging between two buffers; the first buffer is chosen by the
-    // parity of m so that the last step writes x (no copy-back).
-    const int n = A.n;
-    const int deg = o_.amg_cheb_degree;
-    const int m = cheb ? deg - 1 : sweeps - 1;
-    TA* cur = (m % 2 == 0) ? x : pong;
-    TA* nxt = (m % 2 == 0) ? pong : x;
+  // Polynomial (Chebyshev or damped-Jacobi) smoother from a zero guess:
+  // x = S(b).  One diagonal step, then m Jacobi-type steps ping-ponging
+  // between two buffers; the first buffer is chosen by the parity of m so
+  // that the last step writes x (no copy-back).
+  struct PolyPlan {
+    int m;            // Jacobi-type steps after the diagonal one
+    double w0;        // weight of the diagonal step
+    const TA* den0;   // its denominator
+  };
+  PolyPlan poly_plan(double lambda, bool cheb, const TA* diag, const TA* den_jac, int sweeps) const {
     if (cheb) {
+      const int deg = o_.amg_cheb_degree;
       const double lo = o_.amg_lambda_low_fraction * lambda;
       if (!(lambda > lo && lo > 0)) throw SolveFailure(NDS_E_BREAKDOWN, "Chebyshev smoother interval invalid");
-      k::jacobi_zero<TA><<<grid_for(n), kBlock, 0, st_>>>(n, TA(1.0 / cheb_root(lambda, lo, 0, deg)), b, diag, cur);
-      NDS_LAUNCH();
-      for (int kk = 1; kk < deg; ++kk) {
-        op_smooth(A, cur, b, diag, 1.0 / cheb_root(lambda, lo, kk, deg), nxt);
-        std::swap(cur, nxt);
-      }
-    } else {
-      k::jacobi_zero<TA><<<grid_for(n), kBlock, 0, st_>>>(n, TA(o_.amg_jacobi_omega), b, den_jac, cur);
-      NDS_LAUNCH();
-      for (int q = 1; q < sweeps; ++q) {
-        op_smooth(A, cur, b, den_jac, o_.amg_jacobi_omega, nxt);
-        std::swap(cur, nxt);
-      }
+      return {deg - 1, 1.0 / cheb_root(lambda, lo, 0, deg), diag};
     }
+    return {sweeps - 1, o_.amg_jacobi_omega, den_jac};
+  }
+  static TA* poly_first(const PolyPlan& pl, TA* x, TA* pong) { return (pl.m % 2 == 0) ? x : pong; }
+  // first_done: the diagonal step is already in poly_first(x, pong) (written
+  // by the residual kernel); add_to: the result is added to add_to instead
+  // of stored in x.
+  void poly_smooth(const OpView<TA>& A, const TA* diag, const TA* b, TA* x, TA* pong, double lambda, bool cheb,
+                   const TA* den_jac, int sweeps, bool first_done = false, TA* add_to = nullptr) {
+    const int n = A.n;
+    const PolyPlan pl = poly_plan(lambda, cheb, diag, den_jac, sweeps);
+    TA* cur = poly_first(pl, x, pong);
+    TA* nxt = (pl.m % 2 == 0) ? pong : x;
+    if (!first_done) {
+      k::jacobi_zero<TA><<<grid_for(n), kBlock, 0, st_>>>(n, TA(pl.w0), b, pl.den0, cur);
+      NDS_LAUNCH();
+    }
+    const double lo = cheb ? o_.amg_lambda_low_fraction * lambda : 0.0;
+    for (int kk = 1; kk <= pl.m; ++kk) {
+      const double w = cheb ? 1.0 / cheb_root(lambda, lo, kk, o_.amg_cheb_degree) : o_.amg_jacobi_omega;
+      op_smooth(A, cur, b, cheb ? diag : den_jac, w, nxt, kk == pl.m ? add_to : nullptr);
+      std::swap(cur, nxt);
+    }
+    if (pl.m == 0 && add_to) vaxpy(n, 1.0, (const TA*)x, add_to);
   }
   void mcgs(const OpView<TA>& A, const TA* diag, const TA* b, TA* x, const DBuf<int32_t>& crows,
             const std::vector<int>& coff, int sweeps) {
@@ -737,27 +792,59 @@ class Solver final : public ISolver {
       else { pass(false); pass(true); }
     }
   }
-  void smooth_fine(const TA* b, TA* x) {
+  // first_done: the diagonal step of the polynomial smoother is already in
+  // place (taken by the kernel that produced b); never set for MCGS
+  void smooth_fine(const TA* b, TA* x, bool first_done = false) {
     const int sm = o_.amg_smoother;
     if (sm == NDS_SM_MCGS) {
       mcgs(fine_opA(), fdiag_.p, b, x, fine_crows_, fine_coff_, o_.amg_mcgs_fine_sweeps);
       return;
     }
     const TA* den = sm == NDS_SM_L1JACOBI ? fl1_.p : fdiag_.p;
-    poly_smooth(fine_opA(), fdiag_.p, b, x, fpong_.p, fine_lambda_, sm == NDS_SM_CHEB2, den, o_.amg_jacobi_fine_sweeps);
+    poly_smooth(fine_opA(), fdiag_.p, b, x, fpong_.p, fine_lambda_, sm == NDS_SM_CHEB2, den, o_.amg_jacobi_fine_sweeps,
+                first_done);
   }
-  void smooth_level(Level& A, const TA* b, TA* x, double lambda) {
+  void smooth_level(Level& A, const TA* b, TA* x, double lambda, bool first_done = false) {
     const int sm = o_.amg_smoother;
     if (sm == NDS_SM_MCGS) {
       mcgs(level_op(A), A.diag.p, b, x, A.crows, A.coff, o_.amg_mcgs_coarse_sweeps);
       return;
     }
     const TA* den = sm == NDS_SM_L1JACOBI ? A.l1.p : A.diag.p;
-    poly_smooth(level_op(A), A.diag.p, b, x, A.pong.p, lambda, sm == NDS_SM_CHEB2, den, o_.amg_jacobi_coarse_sweeps);
+    poly_smooth(level_op(A), A.diag.p, b, x, A.pong.p, lambda, sm == NDS_SM_CHEB2, den, o_.amg_jacobi_coarse_sweeps,
+                first_done);
   }
-  void restrict_to(const Xfer& X, const TA* f, TA* c) {
+  // plan of the pre-smoother of level l (polynomial smoothers only)
+  PolyPlan level_plan(int l) const {
+    const Level& A = L_[(size_t)l];
+    const int sm = o_.amg_smoother;
+    const TA* den = sm == NDS_SM_L1JACOBI ? A.l1.p : A.diag.p;
+    return poly_plan(level_lambda_[(size_t)l], sm == NDS_SM_CHEB2, A.diag.p, den, o_.amg_jacobi_coarse_sweeps);
+  }
+  PolyPlan fine_plan() const {
+    const int sm = o_.amg_smoother;
+    const TA* den = sm == NDS_SM_L1JACOBI ? fl1_.p : fdiag_.p;
+    return poly_plan(fine_lambda_, sm == NDS_SM_CHEB2, fdiag_.p, den, o_.amg_jacobi_fine_sweeps);
+  }
+  // whether the pre-smoother of level l can take its diagonal step in the
+  // restriction that feeds it (a polynomial smoother, not the terminal level)
+  bool fuse_pre(int l) const { return o_.amg_smoother != NDS_SM_MCGS && l < (int)L_.size() - 1; }
+  // c = R f; with level >= 0 also the diagonal step of that level's
+  // pre-smoother (see fuse_pre)
+  void restrict_to(const Xfer& X, const TA* f, TA* c, int level = -1) {
     ProfScope ps(prof, st_, P_TRANSFER);
-    k::restrict_warp<TA><<<grid_for((long long)X.nc * 32), kBlock, 0, st_>>>(X.nc, X.rrow.p, X.rcol.p, X.rval.p, f, c);
+    const TA* den0 = nullptr;
+    TA* x1 = nullptr;
+    double w0 = 0.0;
+    if (level >= 0) {
+      Level& C = L_[(size_t)level];
+      const PolyPlan pl = level_plan(level);
+      den0 = pl.den0;
+      w0 = pl.w0;
+      x1 = poly_first(pl, C.x.p, C.pong.p);
+    }
+    k::restrict_warp<TA><<<grid_for((long long)X.nc * 32), kBlock, 0, st_>>>(X.nc, X.rrow.p, X.rcol.p, X.rval.p, f, c,
+                                                                            den0, TA(w0), x1);
     NDS_LAUNCH();
   }
   void prolong(const Xfer& X, const TA* c, TA* f) {
@@ -767,7 +854,9 @@ class Solver final : public ISolver {
   }
 
   // -------------------------------------------------------------- V-cycle
-  void vcycle(int l, const TA* b, TA* x) {
+  // pre_done: the diagonal step of this level's pre-smoother is already in
+  // place (taken by the restriction that produced b)
+  void vcycle(int l, const TA* b, TA* x, bool pre_done = false) {
     Level& A = L_[(size_t)l];
     if (l == (int)L_.size() - 1) {
       ProfScope ps(prof, st_, P_TERMINAL);
@@ -775,27 +864,55 @@ class Solver final : public ISolver {
       NDS_LAUNCH();
       return;
     }
-    smooth_level(A, b, x, level_lambda_[(size_t)l]);
+    smooth_level(A, b, x, level_lambda_[(size_t)l], pre_done);
     op_resid(level_op(A), x, b, A.r.p);
     Level& C = L_[(size_t)l + 1];
-    restrict_to(X_[(size_t)l + 1], A.r.p, C.b.p);
-    vcycle(l + 1, C.b.p, C.x.p);
+    const bool fuse = fuse_pre(l + 1);
+    restrict_to(X_[(size_t)l + 1], A.r.p, C.b.p, fuse ? l + 1 : -1);
+    vcycle(l + 1, C.b.p, C.x.p, fuse);
     prolong(X_[(size_t)l + 1], C.x.p, x);
-    // r = b - A x, then the post-smoother solves A corr = r (b is no longer needed)
-    op_resid(level_op(A), x, b, A.r.p, A.b.p);
-    smooth_level(A, A.b.p, A.corr.p, level_lambda_[(size_t)l]);
-    vaxpy(A.n, 1.0, A.corr.p, x);
+    // r = b - A x into b (b is no longer needed), then the post-smoother
+    // solves A corr = r and x += corr
+    const double lam = level_lambda_[(size_t)l];
+    const int sm = o_.amg_smoother;
+    if (sm == NDS_SM_MCGS) {
+      op_resid(level_op(A), x, b, A.r.p, A.b.p);
+      smooth_level(A, A.b.p, A.corr.p, lam);
+      vaxpy(A.n, 1.0, A.corr.p, x);
+      return;
+    }
+    // the residual kernel also takes the smoother's diagonal step, and the
+    // last smoothing step adds the correction to x
+    const bool cheb = sm == NDS_SM_CHEB2;
+    const TA* den = sm == NDS_SM_L1JACOBI ? A.l1.p : A.diag.p;
+    const PolyPlan pl = poly_plan(lam, cheb, A.diag.p, den, o_.amg_jacobi_coarse_sweeps);
+    op_resid(level_op(A), x, b, A.b.p, poly_first(pl, A.corr.p, A.pong.p), pl.den0, pl.w0);
+    poly_smooth(level_op(A), A.diag.p, A.b.p, A.corr.p, A.pong.p, lam, cheb, den, o_.amg_jacobi_coarse_sweeps, true, x);
   }
-  void amg_apply(const TA* b, TA* z) {
-    smooth_fine(b, z);
+  // pre_done: the fine pre-smoother's diagonal step is already in place
+  void amg_apply(const TA* b, TA* z, bool pre_done = false) {
+    smooth_fine(b, z, pre_done);
     op_resid(fine_opA(), z, b, fr_.p);
     Level& C = L_[0];
-    restrict_to(X_[0], fr_.p, C.b.p);
-    vcycle(0, C.b.p, C.x.p);
+    const bool fuse = fuse_pre(0);
+    restrict_to(X_[0], fr_.p, C.b.p, fuse ? 0 : -1);
+    vcycle(0, C.b.p, C.x.p, fuse);
     prolong(X_[0], C.x.p, z);
-    op_resid(fine_opA(), z, b, fr_.p, frhs_.p);
-    smooth_fine(frhs_.p, fcorr_.p);
-    vaxpy(nc_, 1.0, fcorr_.p, z);
+    const int sm = o_.amg_smoother;
+    if (sm == NDS_SM_MCGS) {
+      op_resid(fine_opA(), z, b, fr_.p, frhs_.p);
+      smooth_fine(frhs_.p, fcorr_.p);
+      vaxpy(nc_, 1.0, fcorr_.p, z);
+      return;
+    }
+    // post-smoothing as on the levels: residual with the diagonal step, last
+    // step added to z
+    const bool cheb = sm == NDS_SM_CHEB2;
+    const TA* den = sm == NDS_SM_L1JACOBI ? fl1_.p : fdiag_.p;
+    const PolyPlan pl = poly_plan(fine_lambda_, cheb, fdiag_.p, den, o_.amg_jacobi_fine_sweeps);
+    op_resid(fine_opA(), z, b, frhs_.p, poly_first(pl, fcorr_.p, fpong_.p), pl.den0, pl.w0);
+    poly_smooth(fine_opA(), fdiag_.p, frhs_.p, fcorr_.p, fpong_.p, fine_lambda_, cheb, den, o_.amg_jacobi_fine_sweeps,
+                true, z);
   }
 
   // ------------------------------------------------------ spectrum estimates
@@ -1086,8 +1203,10 @@ class Solver final : public ISolver {
     a.b2 = b_[2].p;
     ProfScope ps(prof, st_, P_ASSEMBLE);
     // cell blocks: a grid of 8 blocks per SM amortises the shared tensor load
+    k::SupgArgs sa{P_.setup.pipe.nu, o_.supg_tau_scale, o_.supg_magic};
     k::mom_cell_conv<T><<<std::min(grid_for(nc_, kBlock / 8), 8 * 148), kBlock, 0, st_>>>(
-        nc_, ref_.p, fixed_.p, u_[0].p, u_[1].p, u_[2].p, invJ_.p, det_.p, centT_.p, cconv_.p);
+        nc_, ref_.p, fixed_.p, u_[0].p, u_[1].p, u_[2].p, invJ_.p, det_.p, centT_.p, cconv_.p,
+        o_.supg ? supg_rule_.p : nullptr, h2_.p, sa);
     NDS_LAUNCH();
     k::mom_assemble<T><<<grid_for(nv_, kBlock / 8), kBlock, mom_smem_, st_>>>(a);
     NDS_LAUNCH();
@@ -1099,7 +1218,7 @@ class Solver final : public ISolver {
       const int s = color_off_[(size_t)c], n = color_off_[(size_t)c + 1] - s;
       if (!n) continue;
       ProfScope ps(prof, st_, P_GS);
-      k::mom_gs_color<T><<<grid_for((long long)n * 8), kBlock, 0, st_>>>(n, color_rows_.p + s, mrow_.p, mcol_.p, A_.p,
+      k::mom_gs_color<T><<<grid_for((long long)n * 8), kBlock, 0, st_>>>(n, color_rows_.p + s, color_span_.p + s, mcol_.p, A_.p,
                                                                        diag_.p, b_[0].p, b_[1].p, b_[2].p, u_[0].p,
                                                                        u_[1].p, u_[2].p, T(o_.mom_omega));
       NDS_LAUNCH();
@@ -1312,7 +1431,7 @@ class Solver final : public ISolver {
   cudaStream_t st_ = nullptr;
   cudaEvent_t ev_[7] = {};
   int nc_ = 0, nv_ = 0, row_cap_ = 0, it_ = 0;
-  size_t mom_smem_ = 0;
+  size_t mom_smem_ = 0, refresh_smem_ = 0;
   double cont0_ = -1, cont_rel_ = 1, fine_lambda_ = 1, p_cheb_lambda_ = 1;
   bool finite_all_ = true;
   std::vector<double> level_lambda_;
@@ -1321,8 +1440,10 @@ class Solver final : public ISolver {
   DBuf<uint32_t> inc_;
   DBuf<uint8_t> slot_;
   DBuf<T> K_, A_, diag_, delta_, rau_, rau_pc_, det_, invJ_, bco_, fixed_, fixed_div_, centT_, cconv_, fgeo_, p_;
+  DBuf<T> h2_, supg_rule_;
   DBuf<T> u_[3], b_[3], s_[3], v_[3];
   std::vector<int> color_off_;
+  DBuf<int2> color_span_;
   // pressure
   DBuf<int32_t> fcoff_, fine_crows_, sbase_, swidth_, scol_, fdslot_;
   DBuf<int16_t> sdcol_;

@@ -67,23 +67,33 @@ void gauss_jacobi01(int n, int alpha, std::vector<double>& xo, std::vector<doubl
   }
 }
 
+namespace {
+// n^3-point collapsed rule: Gauss-Jacobi (1-r)^2, (1-s)^1, Gauss-Legendre t
+std::vector<QuadPoint> collapsed_rule(int n) {
+  std::vector<double> rn, rw, sn, sw, tn, tw;
+  gauss_jacobi01(n, 2, rn, rw);
+  gauss_jacobi01(n, 1, sn, sw);
+  gauss_jacobi01(n, 0, tn, tw);
+  std::vector<QuadPoint> out;
+  out.reserve((size_t)n * n * n);
+  for (int ir = 0; ir < n; ++ir)
+    for (int is = 0; is < n; ++is)
+      for (int it = 0; it < n; ++it) {
+        const double r = rn[(size_t)ir], s = sn[(size_t)is], t = tn[(size_t)it];
+        const double omr = 1 - r, oms = 1 - s;
+        out.push_back({{omr * oms * (1 - t), r, omr * s, omr * oms * t}, rw[(size_t)ir] * sw[(size_t)is] * tw[(size_t)it]});
+      }
+  return out;
+}
+}  // namespace
+
 const std::vector<QuadPoint>& tet_rule_125() {
-  static const std::vector<QuadPoint> q = [] {
-    std::vector<double> rn, rw, sn, sw, tn, tw;
-    gauss_jacobi01(5, 2, rn, rw);
-    gauss_jacobi01(5, 1, sn, sw);
-    gauss_jacobi01(5, 0, tn, tw);
-    std::vector<QuadPoint> out;
-    out.reserve(125);
-    for (int ir = 0; ir < 5; ++ir)
-      for (int is = 0; is < 5; ++is)
-        for (int it = 0; it < 5; ++it) {
-          const double r = rn[(size_t)ir], s = sn[(size_t)is], t = tn[(size_t)it];
-          const double omr = 1 - r, oms = 1 - s;
-          out.push_back({{omr * oms * (1 - t), r, omr * s, omr * oms * t}, rw[(size_t)ir] * sw[(size_t)is] * tw[(size_t)it]});
-        }
-    return out;
-  }();
+  static const std::vector<QuadPoint> q = collapsed_rule(5);
+  return q;
+}
+
+const std::vector<QuadPoint>& tet_rule_64() {
+  static const std::vector<QuadPoint> q = collapsed_rule(4);
   return q;
 }
 

@@ -26,6 +26,10 @@ void gauss_jacobi01(int n, int alpha, std::vector<double>& x, std::vector<double
 
 // 125-point collapsed rule on the reference tetrahedron (weights sum to 1/6).
 const std::vector<QuadPoint>& tet_rule_125();
+// 64-point (4x4x4) collapsed rule of the SUPG terms, same construction
+// (h7_momentum_assembly.cuh:100-226, g4_host.hpp:324-419), ordered r-major:
+// point 16 ir + 4 is + it.
+const std::vector<QuadPoint>& tet_rule_64();
 
 // Reference tensors of the element:
 //   D[a][b][j][k] = sum_q w_q dphi_a/dxi_j dphi_b/dxi_k            (diffusion)

@@ -535,6 +535,9 @@ Setup build_setup(const Mesh& m, const SetupOptions& o) {
     for (auto& u : U0) u.assign((size_t)nv, 0.0);
     std::vector<double> a;
     host_assemble_central(S, U0, a, conv);
+    // the SUPG entry's snapshot includes the SUPG terms (h8_supg_main_setup.inc:6-7):
+    // the Dirichlet inlet values convect even at U = 0
+    if (o.supg) host_add_supg(S, U0, o.supg_tau_scale, o.supg_magic, a, conv);
     S.init_rau = host_finalize_relax(S, a, o.alpha_u, &S.init_delta);
     if (o.rau_scale != 1.0)
       for (double& q : S.init_rau) q *= o.rau_scale;
@@ -578,6 +581,91 @@ void host_assemble_central(const Setup& S, const std::array<std::vector<double>,
         } else {
           const double* fv = &S.fixed_value[3 * (size_t)(-rf[b] - 1)];
           for (int d = 0; d < 3; ++d) conv[(size_t)d][(size_t)r] -= C * fv[d];
+        }
+      }
+    }
+  }
+}
+
+void supg_cell_block(const Setup& S, int c, const std::array<std::vector<double>, 3>& U, double tau_scale, double magic,
+                     double out[64]) {
+  const int32_t* rf = &S.ref[8 * (size_t)c];
+  double coeff[3][8];
+  for (int m = 0; m < 8; ++m)
+    for (int d = 0; d < 3; ++d)
+      coeff[d][m] = rf[m] >= 0 ? U[(size_t)d][(size_t)rf[m]] : S.fixed_value[3 * (size_t)(-rf[m] - 1) + d];
+  const double* I = &S.invJ[9 * (size_t)c];
+  double gl[4][3], gd[4][4];
+  for (int d = 0; d < 3; ++d) {
+    gl[0][d] = -(I[d] + I[3 + d] + I[6 + d]);
+    gl[1][d] = I[d];
+    gl[2][d] = I[3 + d];
+    gl[3][d] = I[6 + d];
+  }
+  for (int i = 0; i < 4; ++i)
+    for (int j = i; j < 4; ++j) {
+      double q = 0.0;
+      for (int d = 0; d < 3; ++d) q += gl[i][d] * gl[j][d];
+      gd[i][j] = gd[j][i] = q;
+    }
+  for (int k = 0; k < 64; ++k) out[k] = 0.0;
+  const double nu = S.pipe.nu, h2 = S.h2[(size_t)c], diff = 4.0 * nu / h2;
+  for (const QuadPoint& qp : tet_rule_64()) {
+    const auto& lam = qp.lam;
+    int js[4][3];
+    double phi[8];
+    for (int i = 0; i < 4; ++i) {
+      int kk = 0;
+      for (int j = 0; j < 4; ++j)
+        if (j != i) js[i][kk++] = j;
+      phi[i] = lam[(size_t)i];
+      phi[4 + i] = 27.0 * lam[(size_t)js[i][0]] * lam[(size_t)js[i][1]] * lam[(size_t)js[i][2]];
+    }
+    double adv[3] = {0, 0, 0};
+    for (int d = 0; d < 3; ++d)
+      for (int m = 0; m < 8; ++m) adv[d] += coeff[d][m] * phi[m];
+    const double speed2 = adv[0] * adv[0] + adv[1] * adv[1] + adv[2] * adv[2];
+    double stream[8], strong[8];
+    for (int a = 0; a < 4; ++a) stream[a] = strong[a] = adv[0] * gl[a][0] + adv[1] * gl[a][1] + adv[2] * gl[a][2];
+    for (int i = 0; i < 4; ++i) {
+      const int* j = js[i];
+      const double l0 = lam[(size_t)j[0]], l1 = lam[(size_t)j[1]], l2 = lam[(size_t)j[2]];
+      double gb[3];
+      for (int d = 0; d < 3; ++d) gb[d] = 27.0 * (l1 * l2 * gl[j[0]][d] + l0 * l2 * gl[j[1]][d] + l0 * l1 * gl[j[2]][d]);
+      stream[4 + i] = adv[0] * gb[0] + adv[1] * gb[1] + adv[2] * gb[2];
+      const double lap = 54.0 * (l2 * gd[j[0]][j[1]] + l1 * gd[j[0]][j[2]] + l0 * gd[j[1]][j[2]]);
+      strong[4 + i] = -nu * lap + stream[4 + i];
+    }
+    const double den = std::max(4.0 * speed2 / h2 + magic * diff * diff, 1.0e-30);
+    const double w = tau_scale / std::sqrt(den) * qp.w * S.det[(size_t)c];
+    for (int a = 0; a < 8; ++a) {
+      const double ta = w * stream[a];
+      for (int b = 0; b < 8; ++b) out[8 * a + b] += ta * strong[b];
+    }
+  }
+}
+
+void host_add_supg(const Setup& S, const std::array<std::vector<double>, 3>& U, double tau_scale, double magic,
+                   std::vector<double>& aval, std::array<std::vector<double>, 3>& conv) {
+  std::vector<double> blk(64 * (size_t)S.nc);
+#pragma omp parallel for schedule(static)
+  for (int c = 0; c < S.nc; ++c) supg_cell_block(S, c, U, tau_scale, magic, &blk[64 * (size_t)c]);
+  // row gather in ascending cell order: the order of the cell loop of the
+  // reference's host twin
+  const FineTopo& F = S.fine;
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int r = 0; r < S.nv; ++r) {
+    const int64_t rb = S.mom.row[(size_t)r];
+    for (int z = F.inc_off[(size_t)r]; z < F.inc_off[(size_t)r + 1]; ++z) {
+      const int c = (int)(F.packed[(size_t)z] >> 3), a = (int)(F.packed[(size_t)z] & 7u);
+      const int32_t* rf = &S.ref[8 * (size_t)c];
+      for (int b = 0; b < 8; ++b) {
+        const double v = blk[64 * (size_t)c + 8 * a + b];
+        if (rf[b] >= 0) {
+          aval[(size_t)(rb + S.row_slot[64 * (size_t)c + 8 * a + b])] += v;
+        } else {
+          const double* fv = &S.fixed_value[3 * (size_t)(-rf[b] - 1)];
+          for (int d = 0; d < 3; ++d) conv[(size_t)d][(size_t)r] -= v * fv[d];
         }
       }
     }

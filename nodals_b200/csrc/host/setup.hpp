@@ -93,6 +93,8 @@ struct Setup {
 
 struct SetupOptions {
   double re = 20.0, bulk = 1.0, alpha_u = 0.5, rau_scale = 1.0;
+  bool supg = false;  // laminar SUPG terms in the setup snapshot
+  double supg_tau_scale = 0.05, supg_magic = 9.0;
   std::string wall = "patch_0_0", inlet = "patch_2_0", outlet = "patch_1_0";
   int threads = 0;  // 0: all hardware threads
 };
@@ -106,6 +108,13 @@ double bcoeff(double det, const double* invJ, int a, int d);
 // A = K + C(U) with Dirichlet convection into conv (g4_host.hpp:326-340)
 void host_assemble_central(const Setup& S, const std::array<std::vector<double>, 3>& U, std::vector<double>& aval,
                            std::array<std::vector<double>, 3>& conv);
+// adds the implicit SUPG terms at U (g4_host.hpp:324-419): entries in
+// ascending cell order after the convection, Dirichlet columns into conv
+void host_add_supg(const Setup& S, const std::array<std::vector<double>, 3>& U, double tau_scale, double magic,
+                   std::vector<double>& aval, std::array<std::vector<double>, 3>& conv);
+// the implicit SUPG block S[a][b] of cell c at U (64 values, row-major)
+void supg_cell_block(const Setup& S, int c, const std::array<std::vector<double>, 3>& U, double tau_scale, double magic,
+                     double out[64]);
 // row-L1 relaxation (g4_host.hpp:422): returns rAU; writes delta if non-null
 std::vector<double> host_finalize_relax(const Setup& S, std::vector<double>& aval, double alpha_u,
                                         std::vector<double>* delta);

@@ -65,6 +65,7 @@ class Options(C.Structure):
         ("cf_pmax", C.c_int), ("cf_interp", C.c_int), ("cf_aggressive_first", C.c_int),
         ("wall", C.c_char * 64), ("inlet", C.c_char * 64), ("outlet", C.c_char * 64),
         ("precision", C.c_int), ("threads", C.c_int), ("device", C.c_int), ("verbose", C.c_int),
+        ("supg", C.c_int), ("supg_tau_scale", C.c_double), ("supg_magic", C.c_double),
     ]
 
     @classmethod

@@ -26,6 +26,7 @@ struct ora_state {
   double* level_lambda;
   /* momentum */
   double *A, *delta, *diag, *rau, *u[3], *b[3];
+  double* supg; /* 64 per cell when SUPG is on */
   /* pressure */
   double *p, *rhs, *fval, *fdiag, *fl1;
   double *x, *r, *z, *pp, *q, *fr, *fcorr, *frhs, *ftmp, *fpong;
@@ -55,9 +56,76 @@ static void cell_ur(const ora_problem* P, int c, double* const u[3], double ur[8
   }
 }
 
+/* implicit SUPG block S[a][b] of cell c at the lagged velocity u
+ * (g4_host.hpp:324-419, the host twin of h7_momentum_assembly.cuh:100-226):
+ * S[a][b] = sum_q tau_q w_q det (adv_q . grad phi_a)(adv_q . grad phi_b - nu lap phi_b [bubbles]) */
+static void supg_block(const ora_problem* P, int c, double* const u[3], double out[64]) {
+  double coeff[3][8];
+  for (int m = 0; m < 8; ++m) {
+    const int g = P->ref[8L * c + m];
+    for (int d = 0; d < 3; ++d) coeff[d][m] = g >= 0 ? u[d][g] : P->fixed[3L * (-g - 1) + d];
+  }
+  const double* I = P->invJ + 9L * c;
+  double gl[4][3], gd[4][4];
+  for (int d = 0; d < 3; ++d) {
+    gl[0][d] = -(I[d] + I[3 + d] + I[6 + d]);
+    gl[1][d] = I[d];
+    gl[2][d] = I[3 + d];
+    gl[3][d] = I[6 + d];
+  }
+  for (int i = 0; i < 4; ++i)
+    for (int j = i; j < 4; ++j) {
+      double q = 0.0;
+      for (int d = 0; d < 3; ++d) q += gl[i][d] * gl[j][d];
+      gd[i][j] = gd[j][i] = q;
+    }
+  for (int k = 0; k < 64; ++k) out[k] = 0.0;
+  const double h2 = P->h2[c], diff = 4.0 * P->nu / h2;
+  for (int qp = 0; qp < 64; ++qp) {
+    const double* lam = P->supg_rule + 5 * qp;
+    const double qw = lam[4];
+    double phi[8];
+    int js[4][3];
+    for (int i = 0; i < 4; ++i) {
+      int kk = 0;
+      for (int j = 0; j < 4; ++j)
+        if (j != i) js[i][kk++] = j;
+      phi[i] = lam[i];
+      phi[4 + i] = 27.0 * lam[js[i][0]] * lam[js[i][1]] * lam[js[i][2]];
+    }
+    double adv[3] = {0, 0, 0};
+    for (int d = 0; d < 3; ++d)
+      for (int m = 0; m < 8; ++m) adv[d] += coeff[d][m] * phi[m];
+    const double speed2 = adv[0] * adv[0] + adv[1] * adv[1] + adv[2] * adv[2];
+    double stream[8], strong[8];
+    for (int a = 0; a < 4; ++a) stream[a] = adv[0] * gl[a][0] + adv[1] * gl[a][1] + adv[2] * gl[a][2];
+    for (int i = 0; i < 4; ++i) {
+      const int* j = js[i];
+      double gb[3];
+      for (int d = 0; d < 3; ++d)
+        gb[d] = 27.0 * (lam[j[1]] * lam[j[2]] * gl[j[0]][d] + lam[j[0]] * lam[j[2]] * gl[j[1]][d] +
+                        lam[j[0]] * lam[j[1]] * gl[j[2]][d]);
+      stream[4 + i] = adv[0] * gb[0] + adv[1] * gb[1] + adv[2] * gb[2];
+      const double lap = 54.0 * (lam[j[2]] * gd[j[0]][j[1]] + lam[j[1]] * gd[j[0]][j[2]] + lam[j[0]] * gd[j[1]][j[2]]);
+      strong[4 + i] = -P->nu * lap + stream[4 + i];
+    }
+    for (int a = 0; a < 4; ++a) strong[a] = stream[a];
+    const double den = fmax(4.0 * speed2 / h2 + P->supg_magic * diff * diff, 1.0e-30);
+    const double w = P->supg_tau_scale / sqrt(den) * qw * P->det[c];
+    for (int a = 0; a < 8; ++a) {
+      const double ta = w * stream[a];
+      for (int b = 0; b < 8; ++b) out[8 * a + b] += ta * strong[b];
+    }
+  }
+}
+
 static void assemble(ora_state* S) {
   const ora_problem* P = S->P;
   const double fac = 1.0 / P->alpha_u - 1.0;
+  if (P->supg) {
+#pragma omp parallel for schedule(static)
+    for (int c = 0; c < P->nc; ++c) supg_block(P, c, S->u, S->supg + 64L * c);
+  }
 #pragma omp parallel for schedule(dynamic, 256)
   for (int i = 0; i < P->nv; ++i) {
     const int64_t rb = P->mrow[i], re = P->mrow[i + 1];
@@ -71,7 +139,7 @@ static void assemble(ora_state* S) {
         double v = 0.0;
         for (int m = 0; m < 8; ++m)
           for (int j = 0; j < 3; ++j) v += ur[m][j] * P->centT[((a * 8 + m) * 8 + b) * 3 + j];
-        const double C = P->det[c] * v;
+        const double C = P->supg ? P->det[c] * v + S->supg[64L * c + 8 * a + b] : P->det[c] * v;
         if (P->ref[8L * c + b] >= 0) {
           S->A[rb + P->row_slot[64L * c + 8 * a + b]] += C;
         } else {
@@ -465,6 +533,7 @@ ora_state* ora_create(const ora_problem* P) {
     S->b[d] = dalloc(P->nv);
   }
   const int n = P->nc;
+  if (P->supg) S->supg = dalloc(64L * n);
   S->p = dalloc(n);
   S->rhs = dalloc(n);
   S->fval = dalloc(P->frow[n]);
@@ -569,7 +638,7 @@ void ora_set(ora_state* S, const double* u0, const double* u1, const double* u2,
 
 void ora_destroy(ora_state* S) {
   if (!S) return;
-  free(S->A); free(S->delta); free(S->diag); free(S->rau);
+  free(S->A); free(S->delta); free(S->diag); free(S->rau); free(S->supg);
   for (int d = 0; d < 3; ++d) { free(S->u[d]); free(S->b[d]); }
   free(S->p); free(S->rhs); free(S->fval); free(S->fdiag); free(S->fl1);
   double* vs[] = {S->x, S->r, S->z, S->pp, S->q, S->fr, S->fcorr, S->frhs, S->ftmp, S->fpong};

@@ -84,6 +84,11 @@ typedef struct ora_problem {
   double amg_lambda_safety, amg_lambda_low_fraction, amg_jacobi_omega;
   int amg_jacobi_fine_sweeps, amg_jacobi_coarse_sweeps;
   int threads;
+  /* laminar SUPG (0: off) */
+  int supg;
+  double nu, supg_tau_scale, supg_magic;
+  const double* h2;         /* per cell */
+  const double* supg_rule;  /* 64 x (lambda0..3, weight) */
 } ora_problem;
 
 typedef struct ora_report {

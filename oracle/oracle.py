@@ -43,7 +43,9 @@ class _Problem(C.Structure):
                  ("amg_smoother", C.c_int), ("amg_cheb_degree", C.c_int),
                  ("amg_lambda_safety", C.c_double), ("amg_lambda_low_fraction", C.c_double),
                  ("amg_jacobi_omega", C.c_double), ("amg_jacobi_fine_sweeps", C.c_int),
-                 ("amg_jacobi_coarse_sweeps", C.c_int), ("threads", C.c_int)])
+                 ("amg_jacobi_coarse_sweeps", C.c_int), ("threads", C.c_int),
+                 ("supg", C.c_int), ("nu", C.c_double), ("supg_tau_scale", C.c_double), ("supg_magic", C.c_double),
+                 ("h2", C.c_void_p), ("supg_rule", C.c_void_p)])
 
 
 class Report(C.Structure):
@@ -134,6 +136,11 @@ class Oracle:
                   "amg_lambda_low_fraction", "amg_jacobi_omega", "amg_jacobi_fine_sweeps", "amg_jacobi_coarse_sweeps"):
             setattr(P, k, getattr(o, k))
         P.threads = threads
+        P.supg = o.supg
+        P.nu = problem.scalar("pipe.nu")
+        P.supg_tau_scale, P.supg_magic = o.supg_tau_scale, o.supg_magic
+        P.h2 = _ptr(arr("cell.h2"))
+        P.supg_rule = _ptr(arr("supg.rule"))
         self._P = P
         self.nc, self.nv = P.nc, P.nv
         self._h = lib().ora_create(C.byref(P))

@@ -61,7 +61,8 @@ int main(int argc, char** argv) {
     std::string mesh, out, hierarchy = "sa", interp = "exti";
     std::string wall = "patch_0_0", inlet = "patch_2_0", outlet = "patch_1_0";
     double re = 20, bulk = 1, alphaU = 0.5, theta = 0.25, safety = 1.5, lowFrac = 0.05, rauScale = 1.0;
-    int pmax = 8, terminal = 1000, powerIts = 16, aggressive = 0;
+    int pmax = 8, terminal = 1000, powerIts = 16, aggressive = 0, supg = 0;
+    double supgTau = 0.05, supgMagic = 9.0;
     for (int i = 1; i < argc; ++i) {
       std::string a = argv[i];
       auto nx = [&]() -> std::string { if (i + 1 >= argc) throw std::runtime_error("missing value for " + a); return argv[++i]; };
@@ -83,6 +84,9 @@ int main(int argc, char** argv) {
       else if (a == "--wall") wall = nx();
       else if (a == "--inlet") inlet = nx();
       else if (a == "--outlet") outlet = nx();
+      else if (a == "--supg") supg = std::atoi(nx().c_str());
+      else if (a == "--supg-tau-scale") supgTau = std::atof(nx().c_str());
+      else if (a == "--supg-magic") supgMagic = std::atof(nx().c_str());
       else throw std::runtime_error("usage: unknown flag " + a);
     }
     if (mesh.empty() || out.empty()) throw std::runtime_error("--mesh and --out are required");
@@ -94,6 +98,8 @@ int main(int argc, char** argv) {
     std::vector<double> hostA, initDelta;
     std::array<std::vector<double>, 3> hostConv;
     host_assemble_central_g4(S, U0, hostA, hostConv);
+    // the SUPG entry adds its host SUPG twin before relaxing (h8_supg_main_setup.inc:6-7)
+    if (supg) host_add_supg64_g4(S, U0, supgTau, supgMagic, hostA, hostConv);
     auto initRau = host_finalize_relax_g4(S, hostA, alphaU, &initDelta);
     if (rauScale != 1.0) for (double& q : initRau) q *= rauScale;
     S.pressure.rAU = initRau;

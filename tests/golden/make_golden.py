@@ -80,9 +80,22 @@ CASES = {
     # SA + PCG: the reference's per-iteration profiler overflows (2048 records)
     # with CF + Richardson at this tolerance on this mesh
     "m40k_sa_fixed10": ("pipe40k", "fp64", ["--run-mode", "fixed10", "--max-outer", "10"], _CFG1 + _SA),
+    # laminar SUPG (the reference's separate SUPG entry, implicit 64-point form)
+    "tiny_supg_fixed10": ("pipe_tiny", "fp64", ["--run-mode", "fixed10", "--max-outer", "10"],
+                          _CFG1 + _SA + ["--amg-terminal", "60", "--supg", "1"]),
+    "small_supg_fixed10": ("pipe_small", "fp64", ["--run-mode", "fixed10", "--max-outer", "10"],
+                           _CFG1 + _SA + ["--amg-terminal", "100", "--supg", "1"]),
+    "small_supg_cf_fixed10": ("pipe_small", "fp64", ["--run-mode", "fixed10", "--max-outer", "10"],
+                              _CFG1 + _CF + ["--amg-terminal", "100", "--supg", "1", "--supg-tau-scale", "0.1",
+                                             "--supg-magic", "4"]),
+    "small_supg_converge": ("pipe_small", "fp64", ["--run-mode", "converge", "--max-outer", "400", "--simple-tol", "1e-3"],
+                            _CFG1 + _SA + ["--amg-terminal", "100", "--supg", "1"]),
 }
 
 _SIMPLE = re.compile(r"NODALS_GPU_H8_SIMPLE .*?it=(\d+) relCont=(\S+) .*?pCG=(\d+) pTrueRel=(\S+)")
+# the SUPG entry writes no VTU; its field check is the analytic-error line
+_HP = re.compile(r"NODALS_GPU_H8_HP_ERROR .*?hEff=(\S+) U_L2=(\S+) U_relL2=(\S+) P_shifted_L2=(\S+) "
+                 r"P_shifted_relL2=(\S+) pressureShift=(\S+) pressureDropFit=(\S+)")
 _AUDIT = re.compile(r"auditInitRel=\[(\S+?),(\S+?),(\S+?)\]")
 
 
@@ -151,18 +164,42 @@ def make_runs(out: Path, only=None):
                 meshes[mesh] = write_mesh(mesh, td)
             exe = REF / f"nodals_gpu_h8_{prec}"
             vtu = td / f"{case}.vtu"
-            cmd = [str(exe), "--mesh", str(meshes[mesh]), "--tag", case, "--vtu-out", str(vtu), *mode, *flags]
+            out_flags = [] if "--supg" in flags else ["--vtu-out", str(vtu)]
+            cmd = [str(exe), "--mesh", str(meshes[mesh]), "--tag", case, *out_flags, *mode, *flags]
             r = subprocess.run(cmd, capture_output=True, text=True, timeout=900)
             (out / f"run_{case}.log").write_text(r.stdout + r.stderr)
             if r.returncode not in (0, 35):
                 print("FAILED", case, r.returncode, r.stderr[-2000:])
                 continue
             its, rel, pcg, prel, audit = parse_log(r.stdout)
-            p, u0 = parse_vtu(vtu)
+            fields = {}
+            if out_flags:
+                fields["p"], fields["u_cell"] = parse_vtu(vtu)
+            m = _HP.search(r.stdout)
+            if m:
+                fields["hp"] = np.array([float(v) for v in m.groups()])
             np.savez_compressed(out / f"run_{case}.npz", it=its, rel_cont=rel, p_its=pcg, p_rel=prel, audit=audit,
-                                p=p, u_cell=u0, rc=np.array([r.returncode]),
-                                cmd=np.array(" ".join(cmd[3:])))
+                                rc=np.array([r.returncode]), cmd=np.array(" ".join(cmd[3:])), **fields)
             print("wrote", case, "rc", r.returncode, "its", len(its))
+
+
+def add_hp(out: Path, logdirs):
+    """Add the analytic-error line (hp) to existing run fixtures from the
+    logs of the reference runs that produced them (run_<case>.log)."""
+    for f in sorted(out.glob("run_*.npz")):
+        case = f.stem[4:]
+        g = dict(np.load(f))
+        if "hp" in g:
+            continue
+        for d in logdirs:
+            log = Path(d) / f"run_{case}.log"
+            if log.exists():
+                m = _HP.search(log.read_text())
+                if m:
+                    g["hp"] = np.array([float(v) for v in m.groups()])
+                    np.savez_compressed(f, **g)
+                    print("added hp to", f.name)
+                break
 
 
 if __name__ == "__main__":
@@ -170,6 +207,7 @@ if __name__ == "__main__":
     ap.add_argument("--setup", action="store_true")
     ap.add_argument("--runs", action="store_true")
     ap.add_argument("--only", nargs="*")
+    ap.add_argument("--add-hp", nargs="*", metavar="LOGDIR", help="add hp to existing fixtures from reference logs")
     ap.add_argument("--out", default=str(Path(__file__).resolve().parent))
     ns = ap.parse_args()
     out = Path(ns.out)
@@ -178,3 +216,5 @@ if __name__ == "__main__":
         make_setup(out)
     if ns.runs:
         make_runs(out, ns.only)
+    if ns.add_hp:
+        add_hp(out, ns.add_hp)

@@ -25,6 +25,8 @@ ORACLE_CASES = {
                        amg_terminal=100),
     "sa_sgs": dict(CFG1, **SA, amg_terminal=100, momentum_work="sgs1"),
     "defaults": dict(amg_terminal=100),
+    "sa_supg": dict(CFG1, **SA, amg_terminal=100, supg=1),
+    "cf_supg": dict(CFG1, **CF, amg_terminal=100, supg=1, supg_tau_scale=0.1, supg_magic=4.0),
 }
 
 
@@ -107,12 +109,13 @@ def _options_from_cmd(cmd: str):
     o = {}
     num = {"--re": "re", "--alpha-u": "alpha_u", "--alpha-p": "alpha_p", "--p-rtol": "p_rtol", "--p-max": "p_max",
            "--amg-terminal": "amg_terminal", "--max-outer": "max_outer", "--simple-tol": "simple_tol",
-           "--cf-pmax": "cf_pmax"}
+           "--cf-pmax": "cf_pmax", "--supg": "supg", "--supg-tau-scale": "supg_tau_scale",
+           "--supg-magic": "supg_magic"}
     enum = {"--amg-hierarchy": "amg_hierarchy", "--amg-smoother": "amg_smoother", "--pressure-solver": "pressure_solver",
             "--cf-interp": "cf_interp", "--run-mode": "run_mode", "--momentum-work": "momentum_work"}
     for k, v in kv.items():
         if k in num:
-            o[num[k]] = int(v) if num[k] in ("p_max", "amg_terminal", "max_outer", "cf_pmax") else float(v)
+            o[num[k]] = int(v) if num[k] in ("p_max", "amg_terminal", "max_outer", "cf_pmax", "supg") else float(v)
         elif k in enum:
             o[enum[k]] = v
     return o
@@ -141,9 +144,22 @@ def test_gpu_matches_reference_fixture(native, meshes, case):
                 assert r.p_its == int(g["p_its"][k]), (it, r.p_its, int(g["p_its"][k]))
         last = r
     u0, u1, u2, p = S.fields()
-    uc = np.zeros((P.counts()["nc"], 3))
-    native.cell_average_velocity(P, u0, u1, u2, uc)
     ftol = 1e-3 if fp32 else 1e-8
-    assert rel_l2(p, g["p"]) <= ftol
-    assert rel_l2(uc, g["u_cell"]) <= ftol
+    if "p" in g.files:
+        uc = np.zeros((P.counts()["nc"], 3))
+        native.cell_average_velocity(P, u0, u1, u2, uc)
+        assert rel_l2(p, g["p"]) <= ftol
+        assert rel_l2(uc, g["u_cell"]) <= ftol
+    if "hp" in g.files:
+        check_hp(native.hp_errors(P, u0, u1, u2, p), g["hp"], ftol)
     assert last is not None
+
+
+HP_KEYS = ("h_eff", "u_l2", "u_rel_l2", "p_shifted_l2", "p_shifted_rel_l2", "pressure_shift", "dp_fit")
+
+
+def check_hp(got: dict, want, tol: float):
+    """The reference's NODALS_GPU_H8_HP_ERROR values (12 printed digits):
+    errors against Hagen-Poiseuille and the pressure-drop fit."""
+    for k, w in zip(HP_KEYS, want):
+        assert abs(got[k] - w) <= tol * abs(w) + 1e-12, (k, got[k], w)

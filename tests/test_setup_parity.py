@@ -107,6 +107,14 @@ def _ref_dump_available():
     ("pipe_small", ["--amg-hierarchy", "cf", "--cf-pmax", "4", "--cf-interp", "direct", "--power-its", "16"],
      dict(amg_hierarchy="cf", cf_pmax=4, cf_interp="direct", amg_smoother="cheb2")),
     ("reference40k", ["--amg-hierarchy", "sa", "--alpha-u", "0.5"], dict(amg_hierarchy="sa", alpha_u=0.5)),
+    # the SUPG entry: its setup snapshot includes the SUPG terms of the
+    # convecting Dirichlet values (h8_supg_main_setup.inc:6-7)
+    ("pipe_small", ["--amg-hierarchy", "sa", "--amg-terminal", "100", "--alpha-u", "0.7", "--supg", "1"],
+     dict(amg_hierarchy="sa", amg_terminal=100, alpha_u=0.7, supg=1)),
+    ("pipe_small", ["--amg-hierarchy", "cf", "--cf-pmax", "8", "--cf-interp", "exti", "--power-its", "16", "--supg", "1",
+                    "--supg-tau-scale", "0.1", "--supg-magic", "4"],
+     dict(amg_hierarchy="cf", cf_pmax=8, cf_interp="exti", amg_smoother="cheb2", supg=1, supg_tau_scale=0.1,
+          supg_magic=4.0)),
 ])
 def test_setup_matches_reference_builders_directly(native, meshes, tmp_path, mesh, flags, opts):
     from nodals_b200 import meshgen
