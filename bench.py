@@ -169,15 +169,17 @@ def fine_spmv_bytes(problem, s: int) -> float:
 
 
 def sell_format_bytes(problem, s: int) -> float:
-    """Bytes the SELL-32 fine operator actually streams per SpMV: padded
-    values (s B) and 16-bit column deltas, slice offsets/widths, x and y."""
+    """Bytes the SELL-32x4 fine operator actually streams per SpMV: padded
+    values (s B) and 16-bit column deltas (slice width rounded up to a
+    multiple of 4), slice offsets/widths, x and y."""
     row = problem.array("fine.row")
     n = len(row) - 1
     lens = np.diff(row)
     ns = (n + 31) // 32
     w = np.zeros(ns * 32, dtype=np.int64)
     w[:n] = lens
-    padded = int(w.reshape(ns, 32).max(axis=1).sum()) * 32
+    widths = (w.reshape(ns, 32).max(axis=1) + 3) // 4 * 4
+    padded = int(widths.sum()) * 32
     return padded * (s + 2) + 8 * ns + 2 * s * n
 
 
@@ -240,7 +242,7 @@ def run_nodals(args):
         achieved = alg / (avg_launch_ms * 1e-3) / 1e9
         roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": _traffic(), "peak_kind": peak_kind,
-                "kernel": "fine Schur SpMV of the PCG step, q = A p with p.q (SELL-32, FP64, sell_spmv<double,3>)",
+                "kernel": "fine Schur SpMV of the PCG step, q = A p with p.q (SELL-32x4, FP64, sell_spmv<double,3>)",
                 "algorithmic_bytes_per_launch": int(alg),
                 "algorithmic_bytes_rule": "nnz*(8+4) + 4(n+1) + 2*8*n (CSR index 4 B, value 8 B, x and y once)",
                 "format_bytes_per_launch": int(fmt),

@@ -633,26 +633,31 @@ __global__ void pcg_check(const double* __restrict__ sc, int rn2_slot, int r0_sl
 // ---------------------------------------------------------------------------
 // transfers and terminal solve (g5e_fp32_kernels.cuh:140-150)
 // ---------------------------------------------------------------------------
-// f += P c (one thread per fine row)
+// f += P c (one thread per fine row; P in ELL with entry k of row i at
+// k nf + i, so a warp's loads of P are coalesced).  Sequential sum over k
+// with the loads of four entries issued ahead; padding adds 0 c[0].
 template <class T>
-__global__ void prolong_add(int nf, const int32_t* __restrict__ pr, const int32_t* __restrict__ pc,
-                            const T* __restrict__ pv, const T* __restrict__ c, T* __restrict__ f) {
+__global__ void prolong_add(int nf, int pw, const int32_t* __restrict__ pc, const T* __restrict__ pv,
+                            const T* __restrict__ c, T* __restrict__ f) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nf) return;
-  // sequential sum; loads of four entries issued ahead of their products
   T s = 0;
-  int k = pr[i];
-  const int ke = pr[i + 1];
-  for (; k + 3 < ke; k += 4) {
-    const int c0 = pc[k], c1 = pc[k + 1], c2 = pc[k + 2], c3 = pc[k + 3];
-    const T a0 = pv[k], a1 = pv[k + 1], a2 = pv[k + 2], a3 = pv[k + 3];
+  int k = 0;
+  const size_t n = (size_t)nf;
+  for (; k + 3 < pw; k += 4) {
+    const size_t o = (size_t)k * n + i;
+    const int c0 = pc[o], c1 = pc[o + n], c2 = pc[o + 2 * n], c3 = pc[o + 3 * n];
+    const T a0 = pv[o], a1 = pv[o + n], a2 = pv[o + 2 * n], a3 = pv[o + 3 * n];
     const T x0 = c[c0], x1 = c[c1], x2 = c[c2], x3 = c[c3];
     s += a0 * x0;
     s += a1 * x1;
     s += a2 * x2;
     s += a3 * x3;
   }
-  for (; k < ke; ++k) s += pv[k] * c[pc[k]];
+  for (; k < pw; ++k) {
+    const size_t o = (size_t)k * n + i;
+    s += pv[o] * c[pc[o]];
+  }
   f[i] += s;
 }
 // x = Ainv b, dense row-major, warp per row
@@ -696,11 +701,14 @@ namespace nds {
 namespace k {
 
 // ---------------------------------------------------------------------------
-// Fine Schur operator in sliced ELL (SELL-32): rows grouped in slices of 32;
-// entry k of row i (slice s = i/32, lane l = i%32) lives at
-// base[s] + 32 k + l, k < width[s].  Padding entries carry value 0 and the
-// row's own column.  One thread owns a row: fully coalesced value / column
-// streams, a sequential per-row sum in column order (deterministic).
+// Fine Schur operator in sliced ELL with 4-wide lanes (SELL-32x4): rows are
+// grouped in slices of 32 (one warp); each row's entries are padded to a
+// multiple of 4 and entry k of row i (slice s = i/32, lane l = i%32) lives at
+//   base[s] + 128 (k/4) + 4 l + (k%4),
+// so every thread reads four consecutive entries of its own row with one
+// vector load while the warp's loads stay fully coalesced (512 B of FP32
+// values per instruction).  width[s] is the slice's longest row; padding
+// entries carry value 0 and the row's own column.  One thread owns a row.
 // ---------------------------------------------------------------------------
 struct Sell {
   int n;
@@ -710,6 +718,44 @@ struct Sell {
   const int16_t* __restrict__ dcol;  // column - row, when every |column - row| < 2^15
 };
 
+__device__ __forceinline__ int sell_offset(int base, int lane, int k) { return base + 128 * (k >> 2) + 4 * lane + (k & 3); }
+
+// the four column indices of entries o..o+3 of row i (o a multiple of 4)
+template <bool D16>
+__device__ __forceinline__ void sell_col4(const Sell& A, int o, int i, int j[4]) {
+  if (D16) {
+    const short4 d = *reinterpret_cast<const short4*>(A.dcol + o);
+    j[0] = i + d.x;
+    j[1] = i + d.y;
+    j[2] = i + d.z;
+    j[3] = i + d.w;
+  } else {
+    const int4 c = *reinterpret_cast<const int4*>(A.col + o);
+    j[0] = c.x;
+    j[1] = c.y;
+    j[2] = c.z;
+    j[3] = c.w;
+  }
+}
+template <class T>
+__device__ __forceinline__ void sell_val4(const T* __restrict__ v, int o, T a[4]);
+template <>
+__device__ __forceinline__ void sell_val4<float>(const float* __restrict__ v, int o, float a[4]) {
+  const float4 q = *reinterpret_cast<const float4*>(v + o);
+  a[0] = q.x;
+  a[1] = q.y;
+  a[2] = q.z;
+  a[3] = q.w;
+}
+template <>
+__device__ __forceinline__ void sell_val4<double>(const double* __restrict__ v, int o, double a[4]) {
+  const double2 p = *reinterpret_cast<const double2*>(v + o);
+  const double2 q = *reinterpret_cast<const double2*>(v + o + 2);
+  a[0] = p.x;
+  a[1] = p.y;
+  a[2] = q.x;
+  a[3] = q.y;
+}
 template <bool D16>
 __device__ __forceinline__ int sell_col(const Sell& A, int o, int i) {
   if (D16) return i + (int)A.dcol[o];
@@ -718,38 +764,43 @@ __device__ __forceinline__ int sell_col(const Sell& A, int o, int i) {
 
 enum SellMode { SELL_Y = 0, SELL_RESID = 1, SELL_SMOOTH = 2, SELL_DOT = 3 };
 
-// Row dot product with 8 independent entries in flight per thread (column
-// and value streams first, then the x gathers) to cover HBM latency; two
-// accumulators, fixed order -> deterministic.
+// Row dot product: entries in batches of 8 (two vector loads of values and
+// of columns, then the 8 x gathers), even entries into s0 and odd ones into
+// s1; the last w mod 8 entries (and the zero padding) go to s0 in order.
+// Fixed order -> deterministic.
 template <class T, bool D16>
 __device__ __forceinline__ T sell_row(const Sell& A, const T* __restrict__ v, const T* __restrict__ x, int i) {
-  constexpr int U = 8;  // entries in flight per thread
-  const int s = i >> 5;
-  const int b = A.base[s] + (i & 31);
+  const int s = i >> 5, lane = i & 31;
+  const int b = A.base[s];
   const int w = A.width[s];
+  const int w8 = w & ~7, wp = (w + 3) & ~3;
   T s0 = 0, s1 = 0;
   int k = 0;
-  for (; k + U <= w; k += U) {
-    int j[U];
-    T a[U];
+  for (; k < w8; k += 8) {
+    int j[8];
+    T a[8];
+    const int o0 = sell_offset(b, lane, k), o1 = o0 + 128;
+    sell_col4<D16>(A, o0, i, j);
+    sell_col4<D16>(A, o1, i, j + 4);
+    sell_val4<T>(v, o0, a);
+    sell_val4<T>(v, o1, a + 4);
+    T xv[8];
 #pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const int o = b + 32 * (k + u);
-      j[u] = sell_col<D16>(A, o, i);
-      a[u] = v[o];
-    }
-    T xv[U];
+    for (int u = 0; u < 8; ++u) xv[u] = x[j[u]];
 #pragma unroll
-    for (int u = 0; u < U; ++u) xv[u] = x[j[u]];
-#pragma unroll
-    for (int u = 0; u < U; u += 2) {
+    for (int u = 0; u < 8; u += 2) {
       s0 += a[u] * xv[u];
       s1 += a[u + 1] * xv[u + 1];
     }
   }
-  for (; k < w; ++k) {
-    const int o = b + 32 * k;
-    s0 += v[o] * x[sell_col<D16>(A, o, i)];
+  for (; k < wp; k += 4) {
+    int j[4];
+    T a[4];
+    const int o = sell_offset(b, lane, k);
+    sell_col4<D16>(A, o, i, j);
+    sell_val4<T>(v, o, a);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) s0 += a[u] * x[j[u]];
   }
   return s0 + s1;
 }
@@ -759,7 +810,7 @@ __device__ __forceinline__ T sell_row(const Sell& A, const T* __restrict__ v, co
 // MODE SELL_SMOOTH: y = x + w (b - A x) / den
 // MODE SELL_DOT:    y = A x, partials of x.y (grid-stride; blockDim = kBlock)
 template <class T, int MODE, bool D16>
-__global__ void __launch_bounds__(kBlock) sell_spmv(Sell A, const T* __restrict__ v, const T* __restrict__ x,
+__global__ void __launch_bounds__(kBlock, 8) sell_spmv(Sell A, const T* __restrict__ v, const T* __restrict__ x,
                                                     const T* __restrict__ b, const T* __restrict__ den, T w,
                                                     T* __restrict__ y, T* __restrict__ y2, double* __restrict__ part) {
   if (MODE == SELL_DOT) {
@@ -794,7 +845,7 @@ __global__ void __launch_bounds__(kBlock) sell_spmv(Sell A, const T* __restrict_
 // Static part of the fine Schur refresh: for every directed contribution q of
 // row c (basis a of c, incidence (c2, b) of the shared velocity dof), the
 // geometric factor G_q = B[c][a] . B[c2][b].  Evaluated once at setup.
-// cs[q] = slot << 3 | a; cpk[q] = c2 << 3 | b.
+// cs[q]: basis a in bits 0-2 (0xFFFF: pad entry, G = 0); cpk[q] = c2 << 3 | b.
 template <class T>
 __global__ void refresh_geometry(int nc, const int32_t* __restrict__ coff, const uint32_t* __restrict__ cpk,
                                  const uint16_t* __restrict__ cs, const T* __restrict__ bco, T* __restrict__ G) {
@@ -802,6 +853,10 @@ __global__ void refresh_geometry(int nc, const int32_t* __restrict__ coff, const
   if (c >= nc) return;
   const T* Bc = bco + 24 * (size_t)c;
   for (int q = coff[c]; q < coff[c + 1]; ++q) {
+    if (cs[q] == 0xFFFFu) {
+      G[q] = T(0);
+      continue;
+    }
     const int a = cs[q] & 7;
     const uint32_t pk = cpk[q];
     const T* bb = bco + 24 * (size_t)(pk >> 3) + 3 * (pk & 7u);
@@ -811,99 +866,86 @@ __global__ void refresh_geometry(int nc, const int32_t* __restrict__ coff, const
 
 // Fine Schur numeric refresh A_p = B diag(rau) B^T (h8_precomputed_b.cuh:37-91)
 // into the SELL layout.  Each value is sum_q rau_{g(c,a_q)} G_q over the
-// row's contributions to that entry.  The contributions of a row were sorted
-// by destination slot at setup (stable, from the reference's (basis,
-// incidence) order of h2b_fine_csr.cuh:480-520).
+// row's contributions to that entry, in the reference's (basis, incidence)
+// order (h2b_fine_csr.cuh:480-520).  The contributions of a row are stored
+// as runs, one per fine entry, that never straddle a 32-entry chunk; the
+// code word cs gives the basis a (bits 0-2), the position in the run (bits
+// 3-5), the run's last entry (bit 6) and the entry's slot (bits 7-15); pads
+// are 0xFFFF.
 //
-// One block per SELL slice (32 rows), 4 rows per warp.  For a row, lanes take
-// one contribution each (a coalesced stream of G and cs), then every slot is
-// summed sequentially in that order by a shuffle chain: lane L adds its
-// product to the final running sum of lane L-1 when both belong to the same
-// slot, so each value is the reference's serial sum; no atomics.  The lane
-// holding a slot's last contribution puts the value into the slice's
-// shared-memory image ([entry][row], row stride 33 against bank conflicts),
-// which the block then writes out contiguously in SELL order (padding and
-// slots without contributions as zeros).  Values go to val (operator
-// precision T) and, in the mixed mode, also to valA (AMG precision TA); the
-// diagonal and L1 row sums feed the AMG smoothers.
-// Dynamic shared memory: 33 * max slice width * sizeof(T).
+// One block of 32 warps per SELL slice, a warp per row, a lane per
+// contribution: a shuffle chain sums every run sequentially (the lane at
+// position j adds its product to the finished sum of position j-1), so each
+// value is the reference's serial sum; no atomics.  The run's last lane
+// puts the value into the slice's shared-memory image ([entry][row], row
+// stride 33 against bank conflicts), which the block then writes out
+// contiguously in SELL order (padding as zeros).  Values go to val
+// (operator precision T) and, in the mixed mode, also to valA (AMG precision
+// TA); the diagonal and L1 row sums feed the AMG smoothers.
+// Launch: blockDim 1024; dynamic shared memory 33 * padded max width * sizeof(T).
+constexpr int kRefreshBlock = 1024;
 template <class T, class TA>
-__global__ void __launch_bounds__(kBlock) sell_refresh(int nc, const int32_t* __restrict__ coff,
-                                                       const uint16_t* __restrict__ cs, const T* __restrict__ G,
-                                                       const int32_t* __restrict__ ref, const T* __restrict__ rau,
-                                                       const int32_t* __restrict__ dslot, const int32_t* __restrict__ sbase,
-                                                       const int32_t* __restrict__ swidth, T* __restrict__ val,
-                                                       TA* __restrict__ valA, TA* __restrict__ diag,
-                                                       TA* __restrict__ l1) {
+__global__ void __launch_bounds__(kRefreshBlock) sell_refresh(int nc, const int32_t* __restrict__ coff,
+                                                              const uint16_t* __restrict__ cs, const T* __restrict__ G,
+                                                              const int32_t* __restrict__ ref, const T* __restrict__ rau,
+                                                              const int32_t* __restrict__ dslot,
+                                                              const int32_t* __restrict__ sbase,
+                                                              const int32_t* __restrict__ swidth, T* __restrict__ val,
+                                                              TA* __restrict__ valA, TA* __restrict__ diag,
+                                                              TA* __restrict__ l1) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* sv = reinterpret_cast<T*>(smem_raw);
-  __shared__ T sR[kWarps][8];
+  __shared__ T sR[32][8];
   const int slice = blockIdx.x;
-  const int width = swidth[slice];
+  const int width = (swidth[slice] + 3) & ~3;  // padded to the 4-wide lanes
   for (int t = threadIdx.x; t < 33 * width; t += blockDim.x) sv[t] = T(0);
-  __syncthreads();
-  const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
-  const unsigned below = (1u << lane) - 1u;
-  for (int rr = 0; rr < 32 / kWarps; ++rr) {
-    const int r = wp * (32 / kWarps) + rr;
-    const int c = slice * 32 + r;
-    if (c >= nc) break;  // warp-uniform
+  const int lane = threadIdx.x & 31, r = threadIdx.x >> 5;
+  const int c = slice * 32 + r;
+  const bool live_row = c < nc;
+  int qb = 0, qe = 0, ds = -1;
+  if (live_row) {
     if (lane < 8) {
       const int g = ref[8 * (size_t)c + lane];
-      sR[wp][lane] = g >= 0 ? rau[g] : T(0);
+      sR[r][lane] = g >= 0 ? rau[g] : T(0);
     }
-    __syncwarp();
-    const int qb = coff[c], qe = coff[c + 1];
-    const int ds = dslot[c];
-    T asum = 0, carry = 0;
-    int carry_slot = -1;
-    for (int q0 = qb; q0 < qe; q0 += 32) {
-      const int q = q0 + lane;
-      const bool live = q < qe;
-      int sl = -1;
-      T p = 0;
-      if (live) {
-        const unsigned v = cs[q];
-        sl = (int)(v >> 3);
-        p = sR[wp][v & 7u] * G[q];
-      }
-      const int prev = __shfl_up_sync(0xffffffffu, sl, 1);
-      const int next = __shfl_down_sync(0xffffffffu, sl, 1);
-      // lane 31's run continues into the next chunk when the next
-      // contribution has the same slot
-      const bool cont = lane == 31 && live && q + 1 < qe && (int)(cs[q + 1] >> 3) == sl;
-      const bool head = !live || (lane == 0 ? sl != carry_slot : sl != prev);
-      const bool tail = live && (lane == 31 ? !cont : next != sl);
-      const unsigned heads = __ballot_sync(0xffffffffu, head) | 1u;
-      // position of this lane inside its slot's run within this chunk
-      const int pos = lane - (31 - __clz(heads & (below | (1u << lane))));
-      T acc = (lane == 0 && !head) ? carry + p : p;
-      int maxpos = pos;
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) maxpos = max(maxpos, __shfl_xor_sync(0xffffffffu, maxpos, o));
-      for (int j = 1; j <= maxpos; ++j) {
-        const T up = __shfl_up_sync(0xffffffffu, acc, 1);
-        if (pos == j) acc = up + p;
-      }
-      if (tail) {
-        sv[sl * 33 + r] = acc;
-        if (sl == ds) diag[c] = TA(acc);
-        asum += fabs(acc);
-      }
-      // a slot run cut by the chunk end continues from lane 31's running sum
-      carry = __shfl_sync(0xffffffffu, acc, 31);
-      carry_slot = __shfl_sync(0xffffffffu, sl, 31);
+    qb = coff[c];
+    qe = coff[c + 1];
+    ds = dslot[c];
+  }
+  __syncthreads();  // image zeroed, rAU of every row staged
+  T asum = 0;
+  for (int q0 = qb; q0 < qe; q0 += 32) {  // warp-uniform bounds
+    const int q = q0 + lane;
+    unsigned v = 0xFFFFu;
+    T p = 0;
+    if (q < qe) {
+      v = cs[q];
+      if (v != 0xFFFFu) p = sR[r][v & 7u] * G[q];
     }
-    if (l1) {
-      asum = warp_sum(asum);
-      if (lane == 0) l1[c] = TA(asum);
+    const bool real = v != 0xFFFFu;
+    const int pos = real ? (int)((v >> 3) & 7u) : 0;
+    const int maxpos = __reduce_max_sync(0xffffffffu, pos);
+    T acc = p;
+    for (int j = 1; j <= maxpos; ++j) {
+      const T up = __shfl_up_sync(0xffffffffu, acc, 1);
+      if (pos == j) acc = up + p;
     }
-    __syncwarp();
+    if (real && (v & 64u)) {
+      const int sl = (int)(v >> 7);
+      sv[sl * 33 + r] = acc;
+      if (sl == ds) diag[c] = TA(acc);
+      asum += fabs(acc);
+    }
+  }
+  if (l1 && live_row) {
+    asum = warp_sum(asum);
+    if (lane == 0) l1[c] = TA(asum);
   }
   __syncthreads();
   const size_t base = (size_t)sbase[slice];
   for (int t = threadIdx.x; t < 32 * width; t += blockDim.x) {
-    const T v = sv[(t >> 5) * 33 + (t & 31)];
+    // element t of the slice is entry 4 (t/128) + t%4 of row (t/4)%32
+    const T v = sv[(4 * (t >> 7) + (t & 3)) * 33 + ((t >> 2) & 31)];
     val[base + t] = v;
     if (valA) valA[base + t] = TA(v);
   }
@@ -934,10 +976,10 @@ __global__ void sell_gs_color(int count, const int32_t* __restrict__ rows, Sell 
   if (q >= count) return;
   const int i = rows[q];
   const int s = i >> 5;
-  const int base = A.base[s] + (i & 31);
+  const int base = A.base[s];
   T off = 0;
   for (int k = 0; k < A.width[s]; ++k) {
-    const int o = base + 32 * k;
+    const int o = sell_offset(base, i & 31, k);
     const int j = sell_col<D16>(A, o, i);
     if (j != i) off += v[o] * x[j];
   }

@@ -155,6 +155,28 @@ struct SolveFailure : std::runtime_error {
 
 namespace {
 
+// Exceptions cannot leave an OpenMP region: the first message is kept and
+// rethrown after the region.
+struct OmpErr {
+  bool bad = false;
+  std::string msg;
+  template <class F>
+  void run(F&& f) {
+    try {
+      f();
+    } catch (const std::exception& e) {
+#pragma omp critical(nds_solver_omp_error)
+      if (!bad) {
+        bad = true;
+        msg = e.what();
+      }
+    }
+  }
+  void rethrow() const {
+    if (bad) throw std::runtime_error(msg);
+  }
+};
+
 std::vector<int32_t> to_i32(const std::vector<int64_t>& v, const char* what) {
   std::vector<int32_t> o(v.size());
   for (size_t i = 0; i < v.size(); ++i) {
@@ -215,9 +237,9 @@ class Solver final : public ISolver {
     std::vector<int> coff;
     DBuf<TA> val, diag, l1, b, x, r, tmp, corr, pong;
   };
-  struct Xfer {  // P (fine rows) and R = P^T (coarse rows)
-    int nf = 0, nc = 0;
-    DBuf<int32_t> prow, pcol, rrow, rcol;
+  struct Xfer {  // P (fine rows, ELL k-major) and R = P^T (coarse rows, CSR)
+    int nf = 0, nc = 0, pw = 0;
+    DBuf<int32_t> pcol, rrow, rcol;
     DBuf<TA> pval, rval;
   };
 
@@ -239,6 +261,7 @@ class Solver final : public ISolver {
   void upload() {
     const Setup& S = P_.setup;
     const Hierarchy& H = P_.hier;
+    StageTimer tm("device_upload");
     nc_ = S.nc;
     nv_ = S.nv;
     mrow_.upload(to_i32(S.mom.row, "momentum CSR"));
@@ -299,50 +322,91 @@ class Solver final : public ISolver {
       supg_rule_.upload(rule);
     }
 
-    // fine Schur CSR with contributions regrouped by destination slot
+    tm.mark("momentum_and_cells");
+    // fine Schur refresh contributions, regrouped by destination slot in the
+    // reference's order and laid out in runs (one run per fine entry) that
+    // never straddle a 32-contribution chunk of the row: a run that would
+    // cross a chunk boundary starts the next chunk, the gap is filled with
+    // pad entries.  Per contribution: the code word cs (basis a bits 0-2,
+    // position in its run bits 3-5, run tail bit 6, slot bits 7-15; pads are
+    // 0xFFFF) and the packed incidence (c2 << 3 | b) for the geometry.
     const FineTopo& F = S.fine;
-    fcoff_.upload(F.contrib_off);
     {
-      std::vector<uint8_t> cnt(F.col.size(), 0), ca(F.slot.size()), csl(F.slot.size());
-      std::vector<uint32_t> cpk(F.slot.size());
-      std::vector<int32_t> cur;
+      std::vector<int32_t> plen((size_t)nc_ + 1, 0);
+      std::vector<int32_t> poff((size_t)nc_ + 1, 0);
+      OmpErr oerr;
+      // pass 1: counts per slot and padded row lengths
+      std::vector<uint8_t> cnt(F.col.size(), 0);
+#pragma omp parallel for schedule(dynamic, 1024)
       for (int c = 0; c < nc_; ++c) {
-        const int rb = F.row[(size_t)c], len = F.row[(size_t)c + 1] - rb;
-        const int q0 = F.contrib_off[(size_t)c];
-        // counts per slot, then stable placement (the order of (a, incidence))
-        for (int q = q0; q < F.contrib_off[(size_t)c + 1]; ++q) {
-          if (cnt[(size_t)rb + F.slot[(size_t)q]] == 255) throw std::runtime_error("more than 255 contributions to one fine entry");
-          ++cnt[(size_t)rb + F.slot[(size_t)q]];
-        }
-        if (cnt[(size_t)F.diag_pos[(size_t)c]] == 0) throw std::runtime_error("fine Schur row without a diagonal contribution");
-        cur.assign((size_t)len + 1, 0);
-        for (int s = 0; s < len; ++s) cur[(size_t)s + 1] = cur[(size_t)s] + cnt[(size_t)rb + s];
-        int q = q0;
-        for (int a = 0; a < 8; ++a) {
-          const int g = S.ref[8 * (size_t)c + a];
-          if (g < 0) continue;
-          for (int k = F.inc_off[(size_t)g]; k < F.inc_off[(size_t)g + 1]; ++k, ++q) {
-            const int pos = q0 + cur[(size_t)F.slot[(size_t)q]]++;
-            cpk[(size_t)pos] = F.packed[(size_t)k];
-            ca[(size_t)pos] = (uint8_t)a;
-            csl[(size_t)pos] = F.slot[(size_t)q];
+        oerr.run([&] {
+          const int rb = F.row[(size_t)c], len = F.row[(size_t)c + 1] - rb;
+          for (int q = F.contrib_off[(size_t)c]; q < F.contrib_off[(size_t)c + 1]; ++q) {
+            if (cnt[(size_t)rb + F.slot[(size_t)q]] == 32)
+              throw std::runtime_error("more than 32 contributions to one fine entry");
+            ++cnt[(size_t)rb + F.slot[(size_t)q]];
+          }
+          if (cnt[(size_t)F.diag_pos[(size_t)c]] == 0) throw std::runtime_error("fine Schur row without a diagonal contribution");
+          int L = 0;
+          for (int sl = 0; sl < len; ++sl) {
+            const int n = cnt[(size_t)rb + sl];
+            if (!n) continue;
+            if ((L & 31) + n > 32) L = (L + 31) & ~31;
+            L += n;
+          }
+          plen[(size_t)c + 1] = L;
+        });
+      }
+      oerr.rethrow();
+      for (int c = 0; c < nc_; ++c) poff[(size_t)c + 1] = poff[(size_t)c] + plen[(size_t)c + 1];
+      const size_t nq = (size_t)poff[(size_t)nc_];
+      std::vector<uint16_t> cs(nq, 0xFFFF);
+      std::vector<uint32_t> cpk(nq, 0);
+      // pass 2: stable placement (the order of (a, incidence)) into the runs
+#pragma omp parallel
+      {
+        std::vector<int32_t> start, fill;
+#pragma omp for schedule(dynamic, 1024)
+        for (int c = 0; c < nc_; ++c) {
+          const int rb = F.row[(size_t)c], len = F.row[(size_t)c + 1] - rb;
+          start.assign((size_t)len, 0);
+          fill.assign((size_t)len, 0);
+          int L = 0;
+          for (int sl = 0; sl < len; ++sl) {
+            const int n = cnt[(size_t)rb + sl];
+            if (!n) continue;
+            if ((L & 31) + n > 32) L = (L + 31) & ~31;
+            start[(size_t)sl] = L;
+            L += n;
+          }
+          const size_t o = (size_t)poff[(size_t)c];
+          int q = F.contrib_off[(size_t)c];
+          for (int a = 0; a < 8; ++a) {
+            const int g = S.ref[8 * (size_t)c + a];
+            if (g < 0) continue;
+            for (int k = F.inc_off[(size_t)g]; k < F.inc_off[(size_t)g + 1]; ++k, ++q) {
+              const int sl = F.slot[(size_t)q], n = cnt[(size_t)rb + sl];
+              const int pos = fill[(size_t)sl]++;
+              const size_t at = o + (size_t)(start[(size_t)sl] + pos);
+              cpk[at] = F.packed[(size_t)k];
+              cs[at] = (uint16_t)(((unsigned)sl << 7) | ((pos == n - 1) ? 64u : 0u) | ((unsigned)pos << 3) | (unsigned)a);
+            }
           }
         }
       }
-      // (slot << 3 | basis) per contribution, and its static geometric factor
-      // B[c][a] . B[c2][b], evaluated once on the device
-      std::vector<uint16_t> cs(ca.size());
-      for (size_t q = 0; q < cs.size(); ++q) cs[q] = (uint16_t)(((unsigned)csl[q] << 3) | ca[q]);
+      fcoff_.upload(poff);
       fcs_.upload(cs);
       DBuf<uint32_t> cpk_d;
       cpk_d.upload(cpk);
-      fgeo_.alloc(cpk.size());
+      fgeo_.alloc(nq);
       k::refresh_geometry<T><<<grid_for(nc_), kBlock, 0, st_>>>(nc_, fcoff_.p, cpk_d.p, fcs_.p, bco_.p, fgeo_.p);
       NDS_LAUNCH();
       NDS_CUDA(cudaStreamSynchronize(st_));
     }
     {
-      // SELL-32 layout of the fine pattern
+      tm.mark("refresh_contributions");
+      // SELL-32x4 layout of the fine pattern (entry k of row 32 s + l at
+      // base[s] + 128 (k/4) + 4 l + k%4, rows padded to a multiple of 4)
       const int ns = (nc_ + 31) / 32;
       std::vector<int32_t> width((size_t)ns, 0), base((size_t)ns + 1, 0), dslot((size_t)nc_);
       for (int c = 0; c < nc_; ++c) {
@@ -350,24 +414,28 @@ class Solver final : public ISolver {
         width[(size_t)(c >> 5)] = std::max(width[(size_t)(c >> 5)], len);
         dslot[(size_t)c] = F.diag_pos[(size_t)c] - F.row[(size_t)c];
       }
+      auto padded = [&](int q) { return (width[(size_t)q] + 3) & ~3; };
+      auto offset = [&](int q, int l, int k) {
+        return (size_t)base[(size_t)q] + 128 * (size_t)(k >> 2) + 4 * (size_t)l + (size_t)(k & 3);
+      };
       for (int q = 0; q < ns; ++q) {
-        const int64_t nb = (int64_t)base[(size_t)q] + 32LL * width[(size_t)q];
+        const int64_t nb = (int64_t)base[(size_t)q] + 32LL * padded(q);
         if (nb > INT32_MAX) throw std::runtime_error("SELL fine operator exceeds int32 offsets");
         base[(size_t)q + 1] = (int32_t)nb;
       }
+      // padding entries point at their own row; lanes past the last row of
+      // the final slice point at row 0 (never read by a live thread)
       std::vector<int32_t> scol((size_t)base[(size_t)ns]);
-      for (int c = 0; c < nc_; ++c) {
-        const int s0 = c >> 5, l = c & 31, rb = F.row[(size_t)c], len = F.row[(size_t)c + 1] - rb;
-        for (int q = 0; q < width[(size_t)s0]; ++q)
-          scol[(size_t)base[(size_t)s0] + 32 * (size_t)q + l] = q < len ? F.col[(size_t)rb + q] : c;
-      }
-      // lanes past the last row of the final slice point at row 0 (never read by a live thread)
-      for (int c = nc_; c < ns * 32; ++c) {
-        const int s0 = c >> 5, l = c & 31;
-        for (int q = 0; q < width[(size_t)s0]; ++q) scol[(size_t)base[(size_t)s0] + 32 * (size_t)q + l] = 0;
-      }
+#pragma omp parallel for schedule(static)
+      for (int q = 0; q < ns; ++q)
+        for (int l = 0; l < 32; ++l) {
+          const int c = 32 * q + l;
+          const int rb = c < nc_ ? F.row[(size_t)c] : 0, len = c < nc_ ? F.row[(size_t)c + 1] - rb : 0;
+          for (int kk = 0; kk < padded(q); ++kk) scol[offset(q, l, kk)] = kk < len ? F.col[(size_t)rb + kk] : (c < nc_ ? c : 0);
+        }
       swidth_.upload(width);
-      const int wmax = *std::max_element(width.begin(), width.end());
+      int wmax = 0;
+      for (int q = 0; q < ns; ++q) wmax = std::max(wmax, padded(q));
       refresh_smem_ = (size_t)33 * wmax * sizeof(T);
       if (refresh_smem_ > 200 * 1024) throw std::runtime_error("fine Schur row too long for the refresh slice buffer");
       NDS_CUDA(cudaFuncSetAttribute(k::sell_refresh<T, TA>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -381,17 +449,20 @@ class Solver final : public ISolver {
         NDS_CUDA(cudaMemset(fvalA_.p, 0, fvalA_.bytes()));
       }
       // 16-bit column deltas when the ordering keeps every |column - row| < 2^15
-      bool fits = true;
+      int too_far = 0;
       std::vector<int16_t> dcol(scol.size());
-      for (int q = 0; q < ns && fits; ++q)
-        for (int kk = 0; kk < width[(size_t)q] && fits; ++kk)
-          for (int l = 0; l < 32; ++l) {
-            const int row = 32 * q + l;
-            const size_t o = (size_t)base[(size_t)q] + 32 * (size_t)kk + l;
+#pragma omp parallel for schedule(static) reduction(| : too_far)
+      for (int q = 0; q < ns; ++q)
+        for (int l = 0; l < 32; ++l) {
+          const int row = 32 * q + l;
+          for (int kk = 0; kk < padded(q); ++kk) {
+            const size_t o = offset(q, l, kk);
             const int d = row < nc_ ? scol[o] - row : 0;
-            if (d < -32767 || d > 32767) { fits = false; break; }
-            dcol[o] = (int16_t)d;
+            if (d < -32767 || d > 32767) too_far = 1;
+            else dcol[o] = (int16_t)d;
           }
+        }
+      const bool fits = too_far == 0;
       if (fits && !std::getenv("NDS_SELL_COL32")) {
         sdcol_.upload(dcol);
         sell_ = k::Sell{nc_, sbase_.p, swidth_.p, nullptr, sdcol_.p};
@@ -401,6 +472,7 @@ class Solver final : public ISolver {
       }
       sell_nnz_ = (long long)scol.size();
     }
+    tm.mark("sell_layout");
     fdiag_.upload(H.fine_diag);
     const bool l1 = o_.amg_smoother == NDS_SM_L1JACOBI;
     if (l1) fl1_.alloc((size_t)nc_);
@@ -447,9 +519,23 @@ class Solver final : public ISolver {
       Xfer& X = X_[l];
       X.nf = Ph.nf;
       X.nc = Ph.nc;
-      X.prow.upload(to_i32(Ph.row, "transfer"));
-      X.pcol.upload(Ph.col);
-      X.pval.upload(Ph.val);
+      {
+        // P in ELL, entry k of fine row i at k nf + i (coalesced across rows);
+        // padding entries carry value 0 and coarse column 0
+        int pw = 0;
+        for (int i = 0; i < Ph.nf; ++i) pw = std::max<int>(pw, (int)(Ph.row[(size_t)i + 1] - Ph.row[(size_t)i]));
+        std::vector<int32_t> ec((size_t)pw * Ph.nf, 0);
+        std::vector<double> ev((size_t)pw * Ph.nf, 0.0);
+        for (int i = 0; i < Ph.nf; ++i)
+          for (int64_t q = Ph.row[(size_t)i]; q < Ph.row[(size_t)i + 1]; ++q) {
+            const size_t o = (size_t)(q - Ph.row[(size_t)i]) * Ph.nf + i;
+            ec[o] = Ph.col[(size_t)q];
+            ev[o] = Ph.val[(size_t)q];
+          }
+        X.pw = pw;
+        X.pcol.upload(ec);
+        X.pval.upload(ev);
+      }
       // R = P^T, entries of each coarse row in ascending fine row
       std::vector<int32_t> rr((size_t)Ph.nc + 1, 0), rc(Ph.col.size());
       std::vector<double> rv(Ph.col.size());
@@ -480,6 +566,7 @@ class Solver final : public ISolver {
     NDS_CUDA(cudaMemsetAsync(flags_.p, 0, sizeof(int), st_));
 
     // setup-time state: fine CSR refreshed with the initial rAU
+    tm.mark("levels_and_transfers");
     refresh_fine(rau_.p);
     if (P_.power_its > 0) {
       fine_lambda_ = power_fine(P_.power_its, o_.amg_lambda_safety);
@@ -490,6 +577,7 @@ class Solver final : public ISolver {
     }
     if (o_.pressure_solver == NDS_P_CHEB) p_cheb_lambda_ = precond_power(o_.p_power_its, o_.p_power_safety);
     NDS_CUDA(cudaStreamSynchronize(st_));
+    tm.mark("refresh_and_spectrum");
     reset();
   }
 
@@ -714,7 +802,7 @@ class Solver final : public ISolver {
   // fine Schur operator
   void refresh_fine(const T* rau) {
     ProfScope ps(prof, st_, P_REFRESH);
-    k::sell_refresh<T, TA><<<(nc_ + 31) / 32, kBlock, refresh_smem_, st_>>>(
+    k::sell_refresh<T, TA><<<(nc_ + 31) / 32, k::kRefreshBlock, refresh_smem_, st_>>>(
         nc_, fcoff_.p, fcs_.p, fgeo_.p, ref_.p, rau, fdslot_.p, sbase_.p, swidth_.p, fval_.p,
         kSame ? nullptr : fvalA_.p, fdiag_.p, fl1_.p);
     NDS_LAUNCH();
@@ -849,7 +937,7 @@ class Solver final : public ISolver {
   }
   void prolong(const Xfer& X, const TA* c, TA* f) {
     ProfScope ps(prof, st_, P_TRANSFER);
-    k::prolong_add<TA><<<grid_for(X.nf), kBlock, 0, st_>>>(X.nf, X.prow.p, X.pcol.p, X.pval.p, c, f);
+    k::prolong_add<TA><<<grid_for(X.nf), kBlock, 0, st_>>>(X.nf, X.pw, X.pcol.p, X.pval.p, c, f);
     NDS_LAUNCH();
   }
 

@@ -98,6 +98,14 @@ def test_device_loop_matches_host_loop(native, meshes, precision):
         assert np.array_equal(x, y)
 
 
+# The reference's default SUPG kernel ("mixed64_8", h8_supg_support.inc:49,
+# h7_momentum_assembly.cuh:829-845) evaluates the per-quadrature-point terms
+# in FP32 even in the FP64 build; this package evaluates them in FP64 like the
+# reference's host twin (g4_host.hpp:324-419), so SUPG runs agree with the
+# reference binary to 1e-7 instead of 1e-8.
+SUPG_TOL = 1e-7
+
+
 def _golden_cases():
     return sorted(p.stem[4:] for p in GOLDEN.glob("run_*.npz"))
 
@@ -133,7 +141,7 @@ def test_gpu_matches_reference_fixture(native, meshes, case):
     S = native.Solver(P)
     its = {int(i): k for k, i in enumerate(g["it"])}
     fp32 = opts.get("precision") == "fp32"
-    tol = 2e-3 if fp32 else 1e-8
+    tol = 2e-3 if fp32 else (SUPG_TOL if opts.get("supg") else 1e-8)
     last = None
     for it in range(1, int(g["it"].max()) + 1):
         r = S.step()
@@ -144,7 +152,7 @@ def test_gpu_matches_reference_fixture(native, meshes, case):
                 assert r.p_its == int(g["p_its"][k]), (it, r.p_its, int(g["p_its"][k]))
         last = r
     u0, u1, u2, p = S.fields()
-    ftol = 1e-3 if fp32 else 1e-8
+    ftol = 1e-3 if fp32 else (SUPG_TOL if opts.get("supg") else 1e-8)
     if "p" in g.files:
         uc = np.zeros((P.counts()["nc"], 3))
         native.cell_average_velocity(P, u0, u1, u2, uc)
