@@ -129,8 +129,8 @@ __device__ __forceinline__ void supg_column(const T* __restrict__ I, T h2, T dc,
 }
 
 // 8 lanes per cell; lane b computes column b of the cell's block (convection,
-// plus the SUPG terms when supg_rule is not null).
-template <class T>
+// plus the SUPG terms when SUPG; supg_rule and h2 are read only then).
+template <class T, bool SUPG>
 __global__ void __launch_bounds__(kBlock) mom_cell_conv(int nc, const int32_t* __restrict__ ref,
                                                         const T* __restrict__ fixed, const T* __restrict__ u0,
                                                         const T* __restrict__ u1, const T* __restrict__ u2,
@@ -139,9 +139,9 @@ __global__ void __launch_bounds__(kBlock) mom_cell_conv(int nc, const int32_t* _
                                                         const T* __restrict__ supg_rule, const T* __restrict__ h2,
                                                         SupgArgs sa) {
   __shared__ T sT[1536];
-  __shared__ T sQ[320];
+  __shared__ T sQ[SUPG ? 320 : 1];
   for (int k = threadIdx.x; k < 1536; k += blockDim.x) sT[k] = centT[k];
-  if (supg_rule)
+  if (SUPG)
     for (int k = threadIdx.x; k < 320; k += blockDim.x) sQ[k] = supg_rule[k];
   __syncthreads();
   const int lane8 = threadIdx.x & 7;
@@ -175,7 +175,7 @@ __global__ void __launch_bounds__(kBlock) mom_cell_conv(int nc, const int32_t* _
     const T dc = det[c];
     T* out = C + 64 * (size_t)c + lane8;
     T S[8];
-    if (supg_rule) supg_column<T>(I, h2[c], dc, q0, q1, q2, sQ, sa, lane8, gmask, S);
+    if (SUPG) supg_column<T>(I, h2[c], dc, q0, q1, q2, sQ, sa, lane8, gmask, S);
 #pragma unroll 2
     for (int a = 0; a < 8; ++a) {
       T cv = 0;
@@ -184,7 +184,7 @@ __global__ void __launch_bounds__(kBlock) mom_cell_conv(int nc, const int32_t* _
         const T* t = sT + ((a * 8 + m) * 8 + lane8) * 3;
         cv += w[m][0] * t[0] + w[m][1] * t[1] + w[m][2] * t[2];
       }
-      out[8 * a] = supg_rule ? cv * dc + S[a] : cv * dc;
+      out[8 * a] = SUPG ? cv * dc + S[a] : cv * dc;
     }
   }
 }

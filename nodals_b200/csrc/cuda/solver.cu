@@ -312,6 +312,7 @@ class Solver final : public ISolver {
     if (mom_smem_ > 200 * 1024) throw std::runtime_error("momentum row too long for the shared-memory assembly buffer");
     NDS_CUDA(cudaFuncSetAttribute(k::mom_assemble<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mom_smem_));
     cconv_.alloc(64 * (size_t)nc_);
+
     if (o_.supg) {
       h2_.upload(S.h2);
       std::vector<double> rule;
@@ -1292,9 +1293,13 @@ class Solver final : public ISolver {
     ProfScope ps(prof, st_, P_ASSEMBLE);
     // cell blocks: a grid of 8 blocks per SM amortises the shared tensor load
     k::SupgArgs sa{P_.setup.pipe.nu, o_.supg_tau_scale, o_.supg_magic};
-    k::mom_cell_conv<T><<<std::min(grid_for(nc_, kBlock / 8), 8 * 148), kBlock, 0, st_>>>(
-        nc_, ref_.p, fixed_.p, u_[0].p, u_[1].p, u_[2].p, invJ_.p, det_.p, centT_.p, cconv_.p,
-        o_.supg ? supg_rule_.p : nullptr, h2_.p, sa);
+    const int gc = std::min(grid_for(nc_, kBlock / 8), 8 * 148);
+    if (o_.supg)
+      k::mom_cell_conv<T, true><<<gc, kBlock, 0, st_>>>(nc_, ref_.p, fixed_.p, u_[0].p, u_[1].p, u_[2].p, invJ_.p,
+                                                       det_.p, centT_.p, cconv_.p, supg_rule_.p, h2_.p, sa);
+    else
+      k::mom_cell_conv<T, false><<<gc, kBlock, 0, st_>>>(nc_, ref_.p, fixed_.p, u_[0].p, u_[1].p, u_[2].p, invJ_.p,
+                                                        det_.p, centT_.p, cconv_.p, nullptr, nullptr, sa);
     NDS_LAUNCH();
     k::mom_assemble<T><<<grid_for(nv_, kBlock / 8), kBlock, mom_smem_, st_>>>(a);
     NDS_LAUNCH();

@@ -171,3 +171,19 @@ def check_hp(got: dict, want, tol: float):
     errors against Hagen-Poiseuille and the pressure-drop fit."""
     for k, w in zip(HP_KEYS, want):
         assert abs(got[k] - w) <= tol * abs(w) + 1e-12, (k, got[k], w)
+
+
+@pytest.mark.gpu
+def test_sell_column_formats_agree(native, meshes, monkeypatch):
+    """The fine operator keeps 16-bit column deltas when the ordering allows
+    and absolute 32-bit columns otherwise (NDS_SELL_COL32 forces the latter):
+    both formats give bitwise-equal solves."""
+    P = _make(native, meshes, "pipe_small", precision="amg_fp32", **ORACLE_CASES["sa_pcg"])
+    A = native.Solver(P)
+    monkeypatch.setenv("NDS_SELL_COL32", "1")
+    B = native.Solver(P)
+    for _ in range(4):
+        a, b = A.step(), B.step()
+        assert a.p_its == b.p_its and a.rel_cont == b.rel_cont
+    for x, y in zip(A.fields(), B.fields()):
+        assert np.array_equal(x, y)
