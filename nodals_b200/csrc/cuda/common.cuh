@@ -49,6 +49,11 @@ __device__ __forceinline__ T group_sum(T v, unsigned mask) {
 }
 // lanes of the aligned 8-lane group of the calling thread
 __device__ __forceinline__ unsigned group8_mask() { return 0xffu << (threadIdx.x & 24); }
+// lanes of the aligned G-lane group of the calling thread (G = 8, 16 or 32)
+template <int G>
+__device__ __forceinline__ unsigned group_mask() {
+  return G == 32 ? 0xffffffffu : (((1u << G) - 1u) << (threadIdx.x & (32 - G)));
+}
 
 // Deterministic block reduction of NV doubles; thread 0 holds the sums.
 template <int NV>

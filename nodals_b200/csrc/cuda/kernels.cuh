@@ -419,39 +419,50 @@ __global__ void __launch_bounds__(kBlock) continuity(int nc, const int32_t* __re
 // ---------------------------------------------------------------------------
 // CSR SpMV family, warp per row (h2b_fine_csr.cuh:579-596, h6_coarse_spmv.cuh:10-32)
 // ---------------------------------------------------------------------------
-// Lane l sums entries rb+l, rb+l+32, ... in that order; the loads of four
-// entries are issued before their products are added (same order, same
-// result, a quarter of the dependent memory round trips).
-template <class T>
+// Lane l of a G-lane group sums entries rb+l, rb+l+G, ... in that order;
+// the loads of eight entries are issued before their products are added
+// (same order, an eighth of the dependent memory round trips).
+template <int G, class T>
 __device__ __forceinline__ T lane_strided_dot(int rb, int re, const int32_t* __restrict__ ci, const T* __restrict__ v,
                                               const T* __restrict__ x, int lane) {
   T s = 0;
   int k = rb + lane;
-  for (; k + 96 < re; k += 128) {
-    const int c0 = ci[k], c1 = ci[k + 32], c2 = ci[k + 64], c3 = ci[k + 96];
-    const T a0 = v[k], a1 = v[k + 32], a2 = v[k + 64], a3 = v[k + 96];
-    const T x0 = x[c0], x1 = x[c1], x2 = x[c2], x3 = x[c3];
-    s += a0 * x0;
-    s += a1 * x1;
-    s += a2 * x2;
-    s += a3 * x3;
+  for (; k + 7 * G < re; k += 8 * G) {
+    int c[8];
+    T a[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      c[u] = ci[k + u * G];
+      a[u] = v[k + u * G];
+    }
+    T xv[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) xv[u] = x[c[u]];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) s += a[u] * xv[u];
   }
-  for (; k < re; k += 32) s += v[k] * x[ci[k]];
+  for (; k < re; k += G) s += v[k] * x[ci[k]];
   return s;
 }
+// Coarse-level CSR rows (a few hundred entries at most) go to groups of
+// kRowLanes lanes: two rows per warp keep twice the loads in flight of a
+// warp per row.
+constexpr int kRowLanes = 16;
 template <class T>
-__device__ __forceinline__ T warp_row_dot(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
-                                          const T* __restrict__ v, const T* __restrict__ x, int i, int lane) {
-  return warp_sum(lane_strided_dot(rp[i], rp[i + 1], ci, v, x, lane));
+__device__ __forceinline__ T group_row_dot(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                           const T* __restrict__ v, const T* __restrict__ x, int i, int lane,
+                                           unsigned mask) {
+  return group_sum<kRowLanes>(lane_strided_dot<kRowLanes>(rp[i], rp[i + 1], ci, v, x, lane), mask);
 }
 
 // y = A x
 template <class T>
 __global__ void __launch_bounds__(kBlock) spmv(int n, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
                                                const T* __restrict__ v, const T* __restrict__ x, T* __restrict__ y) {
-  const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = t / kRowLanes, lane = t % kRowLanes;
   if (i >= n) return;
-  const T s = warp_row_dot(rp, ci, v, x, i, lane);
+  const T s = group_row_dot(rp, ci, v, x, i, lane, group_mask<kRowLanes>());
   if (lane == 0) y[i] = s;
 }
 
@@ -461,9 +472,10 @@ __global__ void __launch_bounds__(kBlock) spmv_resid(int n, const int32_t* __res
                                                      const T* __restrict__ v, const T* __restrict__ x,
                                                      const T* __restrict__ b, T* __restrict__ r, T* __restrict__ r2,
                                                      const T* __restrict__ den, T w) {
-  const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = t / kRowLanes, lane = t % kRowLanes;
   if (i >= n) return;
-  const T s = warp_row_dot(rp, ci, v, x, i, lane);
+  const T s = group_row_dot(rp, ci, v, x, i, lane, group_mask<kRowLanes>());
   if (lane == 0) {
     // r; r2 = r (den null) or the first Jacobi step w r / den
     const T q = b[i] - s;
@@ -480,9 +492,10 @@ __global__ void __launch_bounds__(kBlock) spmv_smooth(int n, const int32_t* __re
                                                       const T* __restrict__ xin, const T* __restrict__ b,
                                                       const T* __restrict__ den, T w, T* __restrict__ xout,
                                                       T* __restrict__ add_to) {
-  const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = t / kRowLanes, lane = t % kRowLanes;
   if (i >= n) return;
-  const T s = warp_row_dot(rp, ci, v, xin, i, lane);
+  const T s = group_row_dot(rp, ci, v, xin, i, lane, group_mask<kRowLanes>());
   if (lane == 0) {
     // with add_to the step is added to add_to instead of stored in xout
     const T r = b[i] - s;
@@ -988,15 +1001,17 @@ __global__ void sell_gs_color(int count, const int32_t* __restrict__ rows, Sell 
   x[i] = old + omega * (gs - old);
 }
 
-// c = P^T f, warp per coarse row over R = P^T (deterministic tree per row)
+// c = P^T f, a kRowLanes group per coarse row over R = P^T (deterministic
+// tree per row)
 template <class T>
-__global__ void __launch_bounds__(kBlock) restrict_warp(int nc, const int32_t* __restrict__ rr,
+__global__ void __launch_bounds__(kBlock) restrict_rows(int nc, const int32_t* __restrict__ rr,
                                                         const int32_t* __restrict__ rc, const T* __restrict__ rv,
                                                         const T* __restrict__ f, T* __restrict__ c,
                                                         const T* __restrict__ den0, T w0, T* __restrict__ x1) {
-  const int I = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int I = t / kRowLanes, lane = t % kRowLanes;
   if (I >= nc) return;
-  T s = warp_sum(lane_strided_dot(rr[I], rr[I + 1], rc, rv, f, lane));
+  const T s = group_row_dot(rr, rc, rv, f, I, lane, group_mask<kRowLanes>());
   if (lane == 0) {
     c[I] = s;
     // with x1: the coarse pre-smoother's diagonal step w0 c / den0

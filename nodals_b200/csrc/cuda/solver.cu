@@ -766,7 +766,7 @@ class Solver final : public ISolver {
   void op_spmv(const OpView<V>& A, const V* x, V* y) {
     ProfScope ps(prof, st_, A.cat);
     if (A.sell) sell_launch<k::SELL_Y, V>(A, grid_for(A.n), x, nullptr, nullptr, 0.0, y, nullptr);
-    else k::spmv<V><<<grid_for((long long)A.n * 32), kBlock, 0, st_>>>(A.n, A.rp, A.ci, A.v, x, y);
+    else k::spmv<V><<<grid_for((long long)A.n * k::kRowLanes), kBlock, 0, st_>>>(A.n, A.rp, A.ci, A.v, x, y);
     NDS_LAUNCH();
   }
   // r = b - A x; r2 = r, or (den given) the first Jacobi step w r / den
@@ -776,7 +776,7 @@ class Solver final : public ISolver {
     ProfScope ps(prof, st_, A.cat);
     if (A.sell) sell_launch<k::SELL_RESID, V>(A, grid_for(A.n), x, b, den, w, r, r2);
     else
-      k::spmv_resid<V><<<grid_for((long long)A.n * 32), kBlock, 0, st_>>>(A.n, A.rp, A.ci, A.v, x, b, r, r2, den, V(w));
+      k::spmv_resid<V><<<grid_for((long long)A.n * k::kRowLanes), kBlock, 0, st_>>>(A.n, A.rp, A.ci, A.v, x, b, r, r2, den, V(w));
     NDS_LAUNCH();
   }
   // xout = xin + w (b - A xin) / den, or (add_to given) add_to += that
@@ -785,7 +785,7 @@ class Solver final : public ISolver {
     ProfScope ps(prof, st_, A.cat);
     if (A.sell) sell_launch<k::SELL_SMOOTH, V>(A, grid_for(A.n), xin, b, den, w, xout, add_to);
     else
-      k::spmv_smooth<V><<<grid_for((long long)A.n * 32), kBlock, 0, st_>>>(A.n, A.rp, A.ci, A.v, xin, b, den, V(w), xout,
+      k::spmv_smooth<V><<<grid_for((long long)A.n * k::kRowLanes), kBlock, 0, st_>>>(A.n, A.rp, A.ci, A.v, xin, b, den, V(w), xout,
                                                                           add_to);
     NDS_LAUNCH();
   }
@@ -932,7 +932,7 @@ class Solver final : public ISolver {
       w0 = pl.w0;
       x1 = poly_first(pl, C.x.p, C.pong.p);
     }
-    k::restrict_warp<TA><<<grid_for((long long)X.nc * 32), kBlock, 0, st_>>>(X.nc, X.rrow.p, X.rcol.p, X.rval.p, f, c,
+    k::restrict_rows<TA><<<grid_for((long long)X.nc * k::kRowLanes), kBlock, 0, st_>>>(X.nc, X.rrow.p, X.rcol.p, X.rval.p, f, c,
                                                                             den0, TA(w0), x1);
     NDS_LAUNCH();
   }
