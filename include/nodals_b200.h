@@ -100,7 +100,9 @@ typedef struct nds_iter_report {
   int all_momentum_met;
   int converged;
   double ms_assembly, ms_momentum, ms_continuity, ms_pressure, ms_update;
-  double ms_refresh;        /* fine Schur refresh, the first part of ms_pressure */
+  double ms_refresh;        /* the part of the fine Schur refresh (run beside the momentum
+                               sweep and continuity) still pending when the pressure stage
+                               starts; the first part of ms_pressure */
 } nds_iter_report;
 
 typedef struct nds_solve_report {

@@ -246,6 +246,8 @@ class Solver final : public ISolver {
   Solver(const Problem& P) : P_(P), o_(P.opt) {
     NDS_CUDA(cudaSetDevice(o_.device));
     NDS_CUDA(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
+    NDS_CUDA(cudaStreamCreateWithFlags(&st2_, cudaStreamNonBlocking));
+    for (auto& e : ev_side_) NDS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     for (auto& e : ev_) NDS_CUDA(cudaEventCreate(&e));
     upload();
   }
@@ -254,6 +256,9 @@ class Solver final : public ISolver {
       if (e) cudaEventDestroy(e);
     if (hsc_) cudaFreeHost(hsc_);
     if (hflags_) cudaFreeHost(hflags_);
+    for (auto& e : ev_side_)
+      if (e) cudaEventDestroy(e);
+    if (st2_) cudaStreamDestroy(st2_);
     if (st_) cudaStreamDestroy(st_);
   }
 
@@ -801,9 +806,10 @@ class Solver final : public ISolver {
   }
 
   // fine Schur operator
-  void refresh_fine(const T* rau) {
-    ProfScope ps(prof, st_, P_REFRESH);
-    k::sell_refresh<T, TA><<<(nc_ + 31) / 32, k::kRefreshBlock, refresh_smem_, st_>>>(
+  void refresh_fine(const T* rau, cudaStream_t s = nullptr) {
+    if (!s) s = st_;
+    ProfScope ps(prof, s, P_REFRESH);
+    k::sell_refresh<T, TA><<<(nc_ + 31) / 32, k::kRefreshBlock, refresh_smem_, s>>>(
         nc_, fcoff_.p, fcs_.p, fgeo_.p, ref_.p, rau, fdslot_.p, sbase_.p, swidth_.p, fval_.p,
         kSame ? nullptr : fvalA_.p, fdiag_.p, fl1_.p);
     NDS_LAUNCH();
@@ -1363,6 +1369,14 @@ class Solver final : public ISolver {
     NDS_CUDA(cudaEventRecord(ev_[0], st_));
     assemble();
     NDS_CUDA(cudaEventRecord(ev_[1], st_));
+    // The fine Schur refresh needs only rAU from the assembly: it runs on the
+    // side stream while the momentum sweep and the continuity residual run
+    // on the main stream (it writes only the pressure operator, which
+    // nothing reads until the pressure solve waits for it).
+    NDS_CUDA(cudaEventRecord(ev_side_[0], st_));
+    NDS_CUDA(cudaStreamWaitEvent(st2_, ev_side_[0], 0));
+    refresh_fine(rau_.p, st2_);
+    NDS_CUDA(cudaEventRecord(ev_side_[1], st2_));
     if (it == 1) {
       const double rr = rau_snapshot_rel();
       if (!(rr < o_.snapshot_tol))
@@ -1393,7 +1407,7 @@ class Solver final : public ISolver {
     R.cont_norm = cn;
     R.rel_cont = cont_rel_;
     NDS_CUDA(cudaEventRecord(ev_[3], st_));
-    refresh_fine(rau_.p);
+    NDS_CUDA(cudaStreamWaitEvent(st_, ev_side_[1], 0));
     NDS_CUDA(cudaEventRecord(ev_[6], st_));
     PRes pr;
     if (o_.pressure_solver == NDS_P_PCG) pr = pcg(rhs_.p);
@@ -1522,6 +1536,8 @@ class Solver final : public ISolver {
   const Problem& P_;
   nds_options o_;
   cudaStream_t st_ = nullptr;
+  cudaStream_t st2_ = nullptr;      // side stream of the fine Schur refresh
+  cudaEvent_t ev_side_[2] = {};     // assembly done -> refresh; refresh done -> pressure
   cudaEvent_t ev_[7] = {};
   int nc_ = 0, nv_ = 0, row_cap_ = 0, it_ = 0;
   size_t mom_smem_ = 0, refresh_smem_ = 0;
