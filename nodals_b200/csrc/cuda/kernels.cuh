@@ -40,6 +40,32 @@ __device__ __forceinline__ void write_partials(double (&v)[NV], double* part) {
     for (int k = 0; k < NV; ++k) part[(size_t)blockIdx.x * NV + k] = v[k];
 }
 
+// The velocity state is stored interleaved, component d of dof g at
+// u[kVel g + d]: the momentum sweep, the cell pass and the continuity
+// residual gather all three components of a dof, which then share a sector.
+// Kernels take the three component pointers u, u + 1, u + 2.
+constexpr int kVel = 3;
+
+// u[3 i + d] = a_d[i] for the components given (null: left as is)
+template <class T>
+__global__ void interleave3(int n, const T* __restrict__ a0, const T* __restrict__ a1, const T* __restrict__ a2,
+                            T* __restrict__ u) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (a0) u[kVel * (size_t)i] = a0[i];
+  if (a1) u[kVel * (size_t)i + 1] = a1[i];
+  if (a2) u[kVel * (size_t)i + 2] = a2[i];
+}
+template <class T>
+__global__ void deinterleave3(int n, const T* __restrict__ u, T* __restrict__ a0, T* __restrict__ a1,
+                              T* __restrict__ a2) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  a0[i] = u[kVel * (size_t)i];
+  a1[i] = u[kVel * (size_t)i + 1];
+  a2[i] = u[kVel * (size_t)i + 2];
+}
+
 // ---------------------------------------------------------------------------
 // Momentum assembly (a9 + a10 + a11 + a12) in two passes
 //
@@ -152,9 +178,9 @@ __global__ void __launch_bounds__(kBlock) mom_cell_conv(int nc, const int32_t* _
     const int gm = ref[8 * (size_t)c + lane8];
     T q0, q1, q2;
     if (gm >= 0) {
-      q0 = u0[gm];
-      q1 = u1[gm];
-      q2 = u2[gm];
+      q0 = u0[kVel * (size_t)gm];
+      q1 = u1[kVel * (size_t)gm];
+      q2 = u2[kVel * (size_t)gm];
     } else {
       const T* f = fixed + 3 * (size_t)(-gm - 1);
       q0 = f[0];
@@ -297,9 +323,9 @@ __global__ void __launch_bounds__(kBlock) mom_assemble(MomArgs<T> g) {
       g.delta[i] = de;
       g.diag[i] = d;
       g.rau[i] = (T(1) / d) * g.rau_scale;
-      g.b0[i] = g.s0[i] + conv0 + bt0 + de * g.u0[i];
-      g.b1[i] = g.s1[i] + conv1 + bt1 + de * g.u1[i];
-      g.b2[i] = g.s2[i] + conv2 + bt2 + de * g.u2[i];
+      g.b0[i] = g.s0[i] + conv0 + bt0 + de * g.u0[kVel * (size_t)i];
+      g.b1[i] = g.s1[i] + conv1 + bt1 + de * g.u1[kVel * (size_t)i];
+      g.b2[i] = g.s2[i] + conv2 + bt2 + de * g.u2[kVel * (size_t)i];
     }
     __syncwarp(gmask);
   }
@@ -323,32 +349,34 @@ __global__ void __launch_bounds__(kBlock) mom_gs_color(int count, const int32_t*
   const int i = rows[q];
   const int2 sp = span[q];
   T d = 0, c0 = 0, c1 = 0, c2 = 0, y0 = 0, y1 = 0, y2 = 0;
+  const size_t vi = kVel * (size_t)i;
   if (lane8 == 0) {
     d = diag[i];
     c0 = b0[i];
     c1 = b1[i];
     c2 = b2[i];
-    y0 = x0[i];
-    y1 = x1[i];
-    y2 = x2[i];
+    y0 = x0[vi];
+    y1 = x1[vi];
+    y2 = x2[vi];
   }
   T s0 = 0, s1 = 0, s2 = 0;
   for (int k = sp.x + lane8; k < sp.y; k += 8) {
     const int j = ci[k];
     if (j == i) continue;
     const T a = av[k];
-    s0 += a * x0[j];
-    s1 += a * x1[j];
-    s2 += a * x2[j];
+    const size_t vj = kVel * (size_t)j;
+    s0 += a * x0[vj];
+    s1 += a * x1[vj];
+    s2 += a * x2[vj];
   }
   s0 = group_sum<8>(s0, gmask);
   s1 = group_sum<8>(s1, gmask);
   s2 = group_sum<8>(s2, gmask);
   if (lane8 == 0) {
     const T iv = T(1) / d;
-    x0[i] = (T(1) - omega) * y0 + omega * ((c0 - s0) * iv);
-    x1[i] = (T(1) - omega) * y1 + omega * ((c1 - s1) * iv);
-    x2[i] = (T(1) - omega) * y2 + omega * ((c2 - s2) * iv);
+    x0[vi] = (T(1) - omega) * y0 + omega * ((c0 - s0) * iv);
+    x1[vi] = (T(1) - omega) * y1 + omega * ((c1 - s1) * iv);
+    x2[vi] = (T(1) - omega) * y2 + omega * ((c2 - s2) * iv);
   }
 }
 
@@ -366,11 +394,11 @@ __global__ void __launch_bounds__(kBlock) mom_audit(int n, const int32_t* __rest
   for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 3; i < n; i += groups_total) {
     T a0 = 0, a1 = 0, a2 = 0;
     for (int k = rp[i] + lane8; k < rp[i + 1]; k += 8) {
-      const int j = ci[k];
+      const size_t vj = kVel * (size_t)ci[k];
       const T a = av[k];
-      a0 += a * x0[j];
-      a1 += a * x1[j];
-      a2 += a * x2[j];
+      a0 += a * x0[vj];
+      a1 += a * x1[vj];
+      a2 += a * x2[vj];
     }
     a0 = group_sum<8>(a0, gmask);
     a1 = group_sum<8>(a1, gmask);
@@ -392,8 +420,10 @@ __global__ void __launch_bounds__(kBlock) mom_audit(int n, const int32_t* __rest
 // ---------------------------------------------------------------------------
 // Continuity r_c = fixedDiv_c + sum_a B[c][a] . u(ref a)  (h8_precomputed_b.cuh:140-163),
 // stored negated as the pressure right-hand side, with sum r^2 partials.
+// Component d of velocity dof g is ud[VS g]: VS = kVel for the solver's
+// interleaved state, 1 for three separate arrays.
 // ---------------------------------------------------------------------------
-template <class T>
+template <class T, int VS = kVel>
 __global__ void __launch_bounds__(kBlock) continuity(int nc, const int32_t* __restrict__ ref, const T* __restrict__ bco,
                                                      const T* __restrict__ fixed_div, const T* __restrict__ u0,
                                                      const T* __restrict__ u1, const T* __restrict__ u2,
@@ -407,7 +437,8 @@ __global__ void __launch_bounds__(kBlock) continuity(int nc, const int32_t* __re
     for (int a = 0; a < 8; ++a) {
       const int g = rf[a];
       if (g < 0) continue;
-      s += B[3 * a] * u0[g] + B[3 * a + 1] * u1[g] + B[3 * a + 2] * u2[g];
+      const size_t vg = (size_t)VS * g;
+      s += B[3 * a] * u0[vg] + B[3 * a + 1] * u1[vg] + B[3 * a + 2] * u2[vg];
     }
     const T sr = s;
     acc[0] += (double)sr * (double)sr;

@@ -289,10 +289,11 @@ class Solver final : public ISolver {
     fixed_div_.upload(S.fixed_div);
     for (int d = 0; d < 3; ++d) {
       s_[d].upload(S.static_rhs[(size_t)d]);
-      u_[d].alloc((size_t)nv_);
       b_[d].alloc((size_t)nv_);
       v_[d].alloc((size_t)nv_);
     }
+    u3_.alloc((size_t)kVelComponents * nv_);
+    NDS_CUDA(cudaMemset(u3_.p, 0, u3_.bytes()));
     p_.alloc((size_t)nc_);
     color_rows_.upload(S.color_rows);
     color_off_ = S.color_off;
@@ -1279,9 +1280,9 @@ class Solver final : public ISolver {
     a.C = cconv_.p;
     a.bco = bco_.p;
     a.fixed = fixed_.p;
-    a.u0 = u_[0].p;
-    a.u1 = u_[1].p;
-    a.u2 = u_[2].p;
+    a.u0 = uc(0);
+    a.u1 = uc(1);
+    a.u2 = uc(2);
     a.p = p_.p;
     a.s0 = s_[0].p;
     a.s1 = s_[1].p;
@@ -1301,10 +1302,10 @@ class Solver final : public ISolver {
     k::SupgArgs sa{P_.setup.pipe.nu, o_.supg_tau_scale, o_.supg_magic};
     const int gc = std::min(grid_for(nc_, kBlock / 8), 8 * 148);
     if (o_.supg)
-      k::mom_cell_conv<T, true><<<gc, kBlock, 0, st_>>>(nc_, ref_.p, fixed_.p, u_[0].p, u_[1].p, u_[2].p, invJ_.p,
+      k::mom_cell_conv<T, true><<<gc, kBlock, 0, st_>>>(nc_, ref_.p, fixed_.p, uc(0), uc(1), uc(2), invJ_.p,
                                                        det_.p, centT_.p, cconv_.p, supg_rule_.p, h2_.p, sa);
     else
-      k::mom_cell_conv<T, false><<<gc, kBlock, 0, st_>>>(nc_, ref_.p, fixed_.p, u_[0].p, u_[1].p, u_[2].p, invJ_.p,
+      k::mom_cell_conv<T, false><<<gc, kBlock, 0, st_>>>(nc_, ref_.p, fixed_.p, uc(0), uc(1), uc(2), invJ_.p,
                                                         det_.p, centT_.p, cconv_.p, nullptr, nullptr, sa);
     NDS_LAUNCH();
     k::mom_assemble<T><<<grid_for(nv_, kBlock / 8), kBlock, mom_smem_, st_>>>(a);
@@ -1318,15 +1319,15 @@ class Solver final : public ISolver {
       if (!n) continue;
       ProfScope ps(prof, st_, P_GS);
       k::mom_gs_color<T><<<grid_for((long long)n * 8), kBlock, 0, st_>>>(n, color_rows_.p + s, color_span_.p + s, mcol_.p, A_.p,
-                                                                       diag_.p, b_[0].p, b_[1].p, b_[2].p, u_[0].p,
-                                                                       u_[1].p, u_[2].p, T(o_.mom_omega));
+                                                                       diag_.p, b_[0].p, b_[1].p, b_[2].p, uc(0),
+                                                                       uc(1), uc(2), T(o_.mom_omega));
       NDS_LAUNCH();
     }
   }
   std::array<double, 3> audit() {
     const int g = red_grid((long long)nv_ * 8);
-    k::mom_audit<T><<<g, kBlock, 0, st_>>>(nv_, mrow_.p, mcol_.p, A_.p, b_[0].p, b_[1].p, b_[2].p, u_[0].p, u_[1].p,
-                                           u_[2].p, part_.p);
+    k::mom_audit<T><<<g, kBlock, 0, st_>>>(nv_, mrow_.p, mcol_.p, A_.p, b_[0].p, b_[1].p, b_[2].p, uc(0), uc(1),
+                                           uc(2), part_.p);
     NDS_LAUNCH();
     reduce_to<6>(g, S_AUDIT);
     fetch(S_AUDIT, 6);
@@ -1354,7 +1355,7 @@ class Solver final : public ISolver {
   }
 
   void reset() override {
-    for (int d = 0; d < 3; ++d) u_[d].zero(st_);
+    u3_.zero(st_);
     p_.zero(st_);
     it_ = 0;
     cont0_ = -1.0;
@@ -1395,7 +1396,7 @@ class Solver final : public ISolver {
     {
       const int g = red_grid(nc_);
       ProfScope ps(prof, st_, P_CONTINUITY);
-      k::continuity<T><<<g, kBlock, 0, st_>>>(nc_, ref_.p, bco_.p, fixed_div_.p, u_[0].p, u_[1].p, u_[2].p, rhs_.p,
+      k::continuity<T><<<g, kBlock, 0, st_>>>(nc_, ref_.p, bco_.p, fixed_div_.p, uc(0), uc(1), uc(2), rhs_.p,
                                              part_.p);
       NDS_LAUNCH();
       reduce_to<1>(g, S_CONT2);
@@ -1507,9 +1508,13 @@ class Solver final : public ISolver {
       NDS_CUDA(cudaStreamSynchronize(st_));
       for (size_t i = 0; i < b.n; ++i) out[i] = (double)h[i];
     };
-    get(u_[0], u0);
-    get(u_[1], u1);
-    get(u_[2], u2);
+    if (u0 || u1 || u2) {
+      k::deinterleave3<T><<<grid_for(nv_), kBlock, 0, st_>>>(nv_, u3_.p, v_[0].p, v_[1].p, v_[2].p);
+      NDS_LAUNCH();
+    }
+    get(v_[0], u0);
+    get(v_[1], u1);
+    get(v_[2], u2);
     get(p_, p);
   }
   void set_fields(const double* u0, const double* u1, const double* u2, const double* p) override {
@@ -1524,9 +1529,15 @@ class Solver final : public ISolver {
       NDS_CUDA(cudaMemcpyAsync(b.p, h.data(), b.bytes(), cudaMemcpyHostToDevice, st_));
       NDS_CUDA(cudaStreamSynchronize(st_));
     };
-    put(u_[0], u0);
-    put(u_[1], u1);
-    put(u_[2], u2);
+    put(v_[0], u0);
+    put(v_[1], u1);
+    put(v_[2], u2);
+    if (u0 || u1 || u2) {
+      k::interleave3<T><<<grid_for(nv_), kBlock, 0, st_>>>(nv_, u0 ? v_[0].p : nullptr, u1 ? v_[1].p : nullptr,
+                                                           u2 ? v_[2].p : nullptr, u3_.p);
+      NDS_LAUNCH();
+      NDS_CUDA(cudaStreamSynchronize(st_));
+    }
     put(p_, p);
   }
 
@@ -1550,7 +1561,9 @@ class Solver final : public ISolver {
   DBuf<uint8_t> slot_;
   DBuf<T> K_, A_, diag_, delta_, rau_, rau_pc_, det_, invJ_, bco_, fixed_, fixed_div_, centT_, cconv_, fgeo_, p_;
   DBuf<T> h2_, supg_rule_;
-  DBuf<T> u_[3], b_[3], s_[3], v_[3];
+  DBuf<T> u3_, b_[3], s_[3], v_[3];  // u3_: interleaved velocity; v_: staging of get/set fields
+  static constexpr int kVelComponents = k::kVel;
+  T* uc(int d) const { return u3_.p + d; }
   std::vector<int> color_off_;
   DBuf<int2> color_span_;
   // pressure
@@ -1698,7 +1711,7 @@ int nds_continuity_noalloc(nds_solver* s, const double* u0, const double* u1, co
   }
   if (st == NDS_OK) {
     cudaStream_t cs = static_cast<cudaStream_t>(stream);
-    nds::k::continuity<double><<<grid, nds::kBlock, 0, cs>>>(nc, ref, bco, fdiv, u0, u1, u2, r, part);
+    nds::k::continuity<double, 1><<<grid, nds::kBlock, 0, cs>>>(nc, ref, bco, fdiv, u0, u1, u2, r, part);
     nds::k::reduce_partials<1><<<1, nds::kBlock, 0, cs>>>(part, grid, norm);
     sqrt_in_place<<<1, 1, 0, cs>>>(norm);
     nds::g_launches += 3;
