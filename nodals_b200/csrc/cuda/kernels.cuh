@@ -453,37 +453,39 @@ __global__ void __launch_bounds__(kBlock) continuity(int nc, const int32_t* __re
 // Lane l of a G-lane group sums entries rb+l, rb+l+G, ... in that order;
 // the loads of eight entries are issued before their products are added
 // (same order, an eighth of the dependent memory round trips).
+// Coarse-level CSR rows (one to a few hundred entries) go to a warp each.
+// Lane l takes entries rb + l + 32u; one round of predicated loads (eight
+// per lane: columns and values, then the x gathers) covers a row of up to
+// 256 entries, so a row costs three dependent round trips (row bounds,
+// columns and values, gathers).  Longer rows take further rounds.
 template <int G, class T>
-__device__ __forceinline__ T lane_strided_dot(int rb, int re, const int32_t* __restrict__ ci, const T* __restrict__ v,
+__device__ __forceinline__ T lane_batched_dot(int rb, int re, const int32_t* __restrict__ ci, const T* __restrict__ v,
                                               const T* __restrict__ x, int lane) {
   T s = 0;
-  int k = rb + lane;
-  for (; k + 7 * G < re; k += 8 * G) {
+  for (int k0 = rb + lane; k0 < re; k0 += 8 * G) {
     int c[8];
     T a[8];
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
-      c[u] = ci[k + u * G];
-      a[u] = v[k + u * G];
+      const int k = k0 + u * G;
+      c[u] = k < re ? ci[k] : -1;
+      a[u] = k < re ? v[k] : T(0);
     }
     T xv[8];
 #pragma unroll
-    for (int u = 0; u < 8; ++u) xv[u] = x[c[u]];
+    for (int u = 0; u < 8; ++u) xv[u] = c[u] >= 0 ? x[c[u]] : T(0);
 #pragma unroll
-    for (int u = 0; u < 8; ++u) s += a[u] * xv[u];
+    for (int u = 0; u < 8; ++u)
+      if (c[u] >= 0) s += a[u] * xv[u];
   }
-  for (; k < re; k += G) s += v[k] * x[ci[k]];
   return s;
 }
-// Coarse-level CSR rows (a few hundred entries at most) go to groups of
-// kRowLanes lanes: two rows per warp keep twice the loads in flight of a
-// warp per row.
-constexpr int kRowLanes = 16;
+constexpr int kRowLanes = 32;
 template <class T>
 __device__ __forceinline__ T group_row_dot(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
                                            const T* __restrict__ v, const T* __restrict__ x, int i, int lane,
                                            unsigned mask) {
-  return group_sum<kRowLanes>(lane_strided_dot<kRowLanes>(rp[i], rp[i + 1], ci, v, x, lane), mask);
+  return group_sum<kRowLanes>(lane_batched_dot<kRowLanes>(rp[i], rp[i + 1], ci, v, x, lane), mask);
 }
 
 // y = A x
