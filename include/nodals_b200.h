@@ -169,6 +169,18 @@ int nds_simple_step(nds_solver* s, nds_iter_report* rep);
 int nds_solve(nds_solver* s, nds_solve_report* rep);         /* the run_mode loop */
 int nds_get_fields(nds_solver* s, double* u0, double* u1, double* u2, double* p);
 int nds_set_fields(nds_solver* s, const double* u0, const double* u1, const double* u2, const double* p);
+/* One SIMPLE iteration whose state goes through host memory (no reference
+ * counterpart: the reference keeps the state on the device for the whole
+ * loop).  Same result as nds_set_fields(in) + nds_simple_step +
+ * nds_get_fields(out); any input or output pointer may be NULL (that field
+ * is kept / not read back), and an input may alias an output.  With an FP64
+ * state and page-locked outputs (cudaMallocHost / cudaHostRegister) the
+ * velocity read-back runs under the pressure solve instead of after it.
+ * Returns once every copy into the outputs has finished; after a failure
+ * their contents are unspecified. */
+int nds_simple_step_io(nds_solver* s, const double* u0_in, const double* u1_in, const double* u2_in,
+                       const double* p_in, double* u0_out, double* u1_out, double* u2_out, double* p_out,
+                       nds_iter_report* rep);
 void nds_solver_destroy(nds_solver* s);
 
 /* ---- kernel timing by category with CUDA events on the solver's stream

@@ -141,6 +141,9 @@ struct ISolver {
   virtual void solve(nds_solve_report* rep) = 0;
   virtual void get_fields(double* u0, double* u1, double* u2, double* p) = 0;
   virtual void set_fields(const double* u0, const double* u1, const double* u2, const double* p) = 0;
+  // set_fields(in), step, get_fields(out), with the read-back overlapped
+  // with the step where the state type and the output memory allow it
+  virtual void step_io(const double* const in[4], double* const out[4], nds_iter_report* rep) = 0;
   // device cell-plan arrays read by nds_continuity_noalloc; false unless the
   // state type is double
   virtual bool cell_arrays(const int32_t** ref, const double** bco, const double** fixed_div, int* nc,
@@ -247,6 +250,8 @@ class Solver final : public ISolver {
     NDS_CUDA(cudaSetDevice(o_.device));
     NDS_CUDA(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
     NDS_CUDA(cudaStreamCreateWithFlags(&st2_, cudaStreamNonBlocking));
+    NDS_CUDA(cudaStreamCreateWithFlags(&st_io_, cudaStreamNonBlocking));
+    NDS_CUDA(cudaEventCreateWithFlags(&ev_io_, cudaEventDisableTiming));
     for (auto& e : ev_side_) NDS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     for (auto& e : ev_) NDS_CUDA(cudaEventCreate(&e));
     upload();
@@ -258,6 +263,8 @@ class Solver final : public ISolver {
     if (hflags_) cudaFreeHost(hflags_);
     for (auto& e : ev_side_)
       if (e) cudaEventDestroy(e);
+    if (ev_io_) cudaEventDestroy(ev_io_);
+    if (st_io_) cudaStreamDestroy(st_io_);
     if (st2_) cudaStreamDestroy(st2_);
     if (st_) cudaStreamDestroy(st_);
   }
@@ -1189,6 +1196,7 @@ class Solver final : public ISolver {
   }
   PRes pcg(const T* rhs) {
     const double r0 = p_start(rhs);
+    start_readback();
     if (r0 <= o_.p_atol) return {0, 0.0, true};
     // device loop unless the category profiler needs per-kernel events (or
     // graphs are off / the conditional graph could not be built)
@@ -1231,6 +1239,7 @@ class Solver final : public ISolver {
   // Richardson (omega fixed) and outer Chebyshev (omega = 1/root_k)
   PRes stationary(const T* rhs, bool cheb) {
     const double r0 = p_start(rhs);
+    start_readback();
     if (r0 <= o_.p_atol) return {0, 0.0, true};
     const double target = std::max(o_.p_atol, o_.p_rtol * r0);
     double centre = 0, radius = 0;
@@ -1422,7 +1431,14 @@ class Solver final : public ISolver {
     }
     vaxpy(nc_, o_.alpha_p, x_.p, p_.p);
     NDS_CUDA(cudaEventRecord(ev_[5], st_));
-    NDS_CUDA(cudaEventSynchronize(ev_[5]));
+    if constexpr (std::is_same<T, double>::value) {
+      if (io_out_ && io_out_[3]) NDS_CUDA(cudaMemcpyAsync(io_out_[3], p_.p, p_.bytes(), cudaMemcpyDeviceToHost, st_));
+    }
+    NDS_CUDA(cudaStreamSynchronize(st_));
+    if (io_pending_) {
+      NDS_CUDA(cudaEventSynchronize(ev_io_));
+      io_pending_ = false;
+    }
     prof.collect();
     float ms[5];
     for (int q = 0; q < 5; ++q) NDS_CUDA(cudaEventElapsedTime(&ms[q], ev_[q], ev_[q + 1]));
@@ -1541,6 +1557,63 @@ class Solver final : public ISolver {
     put(p_, p);
   }
 
+  // step_io: the velocity is final after the momentum sweep (event ev_[2]);
+  // it is read back on the I/O stream once the pressure solve has read its
+  // initial norm, so that the copy runs under the device-side Krylov loop.
+  // (Issued earlier, it would hold up the small reads the host waits for
+  // between the sweep and the loop: they share the copy engine.)
+  void start_readback() {
+    if constexpr (std::is_same<T, double>::value) {
+      if (!io_out_ || io_issued_ || !(io_out_[0] || io_out_[1] || io_out_[2])) return;
+      io_issued_ = true;
+      NDS_CUDA(cudaStreamWaitEvent(st_io_, ev_[2], 0));
+      k::deinterleave3<T><<<grid_for(nv_), kBlock, 0, st_io_>>>(nv_, u3_.p, v_[0].p, v_[1].p, v_[2].p);
+      NDS_LAUNCH();
+      for (int d = 0; d < 3; ++d)
+        if (io_out_[d]) NDS_CUDA(cudaMemcpyAsync(io_out_[d], v_[d].p, v_[d].bytes(), cudaMemcpyDeviceToHost, st_io_));
+      NDS_CUDA(cudaEventRecord(ev_io_, st_io_));
+      io_pending_ = true;
+    }
+  }
+  void step_io(const double* const in[4], double* const out[4], nds_iter_report* rep) override {
+    set_fields(in[0], in[1], in[2], in[3]);
+    // Overlapped read-back needs an FP64 state (no host-side conversion) and
+    // page-locked outputs (a copy into pageable memory would block the host
+    // before the rest of the step is queued).
+    bool overlap = std::is_same<T, double>::value;
+    for (int q = 0; q < 4 && overlap; ++q) {
+      if (!out[q]) continue;
+      cudaPointerAttributes a{};
+      if (cudaPointerGetAttributes(&a, out[q]) != cudaSuccess || a.type != cudaMemoryTypeHost) {
+        cudaGetLastError();
+        overlap = false;
+      }
+    }
+    if (!overlap) {
+      step(rep);
+      get_fields(out[0], out[1], out[2], out[3]);
+      return;
+    }
+    io_out_ = out;
+    io_issued_ = false;
+    try {
+      step(rep);
+      start_readback();  // no-op unless the pressure stage did not issue it
+      if (io_pending_) {
+        NDS_CUDA(cudaEventSynchronize(ev_io_));
+        io_pending_ = false;
+      }
+    } catch (...) {
+      // no copy may write the caller's arrays after the call returns
+      io_out_ = nullptr;
+      cudaStreamSynchronize(st_io_);
+      cudaStreamSynchronize(st_);
+      io_pending_ = false;
+      throw;
+    }
+    io_out_ = nullptr;
+  }
+
   nds_iter_report last_{};
 
  private:
@@ -1549,6 +1622,10 @@ class Solver final : public ISolver {
   cudaStream_t st_ = nullptr;
   cudaStream_t st2_ = nullptr;      // side stream of the fine Schur refresh
   cudaEvent_t ev_side_[2] = {};     // assembly done -> refresh; refresh done -> pressure
+  cudaStream_t st_io_ = nullptr;    // read-back of step_io
+  cudaEvent_t ev_io_ = nullptr;
+  double* const* io_out_ = nullptr;  // outputs of the step_io call in progress
+  bool io_pending_ = false, io_issued_ = false;
   cudaEvent_t ev_[7] = {};
   int nc_ = 0, nv_ = 0, row_cap_ = 0, it_ = 0;
   size_t mom_smem_ = 0, refresh_smem_ = 0;
@@ -1648,6 +1725,16 @@ int nds_get_fields(nds_solver* s, double* u0, double* u1, double* u2, double* p)
 int nds_set_fields(nds_solver* s, const double* u0, const double* u1, const double* u2, const double* p) {
   if (!s) return fail(NDS_E_INVALID, "null solver");
   return guarded([&] { s->impl->set_fields(u0, u1, u2, p); });
+}
+int nds_simple_step_io(nds_solver* s, const double* u0_in, const double* u1_in, const double* u2_in,
+                       const double* p_in, double* u0_out, double* u1_out, double* u2_out, double* p_out,
+                       nds_iter_report* r) {
+  if (!s) return fail(NDS_E_INVALID, "null solver");
+  return guarded([&] {
+    const double* in[4] = {u0_in, u1_in, u2_in, p_in};
+    double* const out[4] = {u0_out, u1_out, u2_out, p_out};
+    s->impl->step_io(in, out, r);
+  });
 }
 void nds_solver_destroy(nds_solver* s) { delete s; }
 

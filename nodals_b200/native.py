@@ -145,6 +145,7 @@ def lib():
             L.nds_solve.argtypes = [vp, C.POINTER(SolveReport)]
             L.nds_get_fields.argtypes = [vp] * 5
             L.nds_set_fields.argtypes = [vp] * 5
+            L.nds_simple_step_io.argtypes = [vp] * 9 + [C.POINTER(IterReport)]
             L.nds_solver_destroy.argtypes = [vp]
             L.nds_profile_enable.argtypes = [vp, C.c_int]
             L.nds_launch_count.restype = C.c_ulonglong
@@ -269,6 +270,22 @@ class Solver:
     def set_fields(self, u0, u1, u2, p):
         arrs = [np.ascontiguousarray(x, dtype=np.float64) for x in (u0, u1, u2, p)]
         _check(lib().nds_set_fields(self._h, *[_p(x) for x in arrs]))
+
+    def step_io(self, inputs, outputs) -> IterReport:
+        """One SIMPLE iteration with the state passed through host memory:
+        inputs and outputs are (u0, u1, u2, p) sequences of float64 arrays
+        (or None entries, or raw addresses of page-locked buffers as ints)."""
+        def ptr(x):
+            if x is None:
+                return None
+            if isinstance(x, int):
+                return C.c_void_p(x)
+            if x.dtype != np.float64 or not x.flags.c_contiguous:
+                raise ValueError("step_io arrays must be contiguous float64")
+            return _p(x)
+        r = IterReport()
+        _check(lib().nds_simple_step_io(self._h, *[ptr(x) for x in inputs], *[ptr(x) for x in outputs], C.byref(r)))
+        return r
 
     def profile(self, enable: bool = True):
         _check(lib().nds_profile_enable(self._h, int(enable)))
