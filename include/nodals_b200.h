@@ -131,6 +131,11 @@ void nds_options_default(nds_options* o);
 /* ---- meshes: replace load_foam_tet_mesh (foam_mesh_g2.hpp:55) ---------- */
 int nds_mesh_read_polymesh(const char* polymesh_dir, nds_mesh** out);
 int nds_mesh_read_msh2(const char* path, nds_mesh** out);
+/* binary HXT1 mesh (hybrid_hxt1/hxt1_mesh.hpp:19-103, as written by the
+ * reference's turbulence/sst_gpu_v2/tools/msh2_to_hxt1.py): files without
+ * hex cells; inlet/outlet from the tet boundary records, every other
+ * exterior face wall */
+int nds_mesh_read_hxt1(const char* path, nds_mesh** out);
 int nds_mesh_from_arrays(int n_points, const double* xyz, int n_cells, const int32_t* tets, int n_bfaces,
                          const int32_t* btri, const int32_t* bpatch, int n_patches, const char* const* patch_names,
                          nds_mesh** out);

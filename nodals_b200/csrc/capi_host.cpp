@@ -112,6 +112,16 @@ int nds_mesh_read_msh2(const char* path, nds_mesh** out) {
     return NDS_E_SETUP;
   }
 }
+int nds_mesh_read_hxt1(const char* path, nds_mesh** out) {
+  if (!path || !out) { set_error("null argument"); return NDS_E_INVALID; }
+  try {
+    *out = reinterpret_cast<nds_mesh*>(new nds::Mesh(nds::read_hxt1(path)));
+    return NDS_OK;
+  } catch (const std::exception& e) {
+    set_error(e.what());
+    return NDS_E_SETUP;
+  }
+}
 
 int nds_mesh_from_arrays(int n_points, const double* xyz, int n_cells, const int32_t* tets, int n_bfaces,
                          const int32_t* btri, const int32_t* bpatch, int n_patches, const char* const* patch_names,

@@ -32,6 +32,16 @@ bool ends_with(const std::string& s, const std::string& t) {
   return s.size() >= t.size() && s.compare(s.size() - t.size(), t.size(), t) == 0;
 }
 
+// a regular file that starts with the HXT1 magic
+bool is_hxt1(const std::string& path) {
+  std::FILE* f = std::fopen(path.c_str(), "rb");
+  if (!f) return false;
+  char m[8] = {};
+  const bool ok = std::fread(m, 1, 8, f) == 8 && std::memcmp(m, "HXT1BIN1", 8) == 0;
+  std::fclose(f);
+  return ok;
+}
+
 int run(int argc, char** argv) {
   nds_options o;
   nds_options_default(&o);
@@ -159,6 +169,7 @@ int run(int argc, char** argv) {
   const auto t0 = std::chrono::steady_clock::now();
   nds_mesh* M = nullptr;
   if (ends_with(mesh, ".msh")) ck(nds_mesh_read_msh2(mesh.c_str(), &M), "mesh");
+  else if (is_hxt1(mesh)) ck(nds_mesh_read_hxt1(mesh.c_str(), &M), "mesh");
   else ck(nds_mesh_read_polymesh(mesh.c_str(), &M), "mesh");
   nds_problem* P = nullptr;
   ck(nds_problem_create(M, &o, &P), "setup");

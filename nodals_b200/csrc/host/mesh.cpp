@@ -500,4 +500,106 @@ Mesh read_msh2(const std::string& path) {
                           (int)bpatch.size(), btri.data(), bpatch.data(), names);
 }
 
+// HXT1 layout (hxt1_mesh.hpp:19-103, writer hybrid_hxt1/prepare_hxt1.py):
+// 8-byte magic, u32 version, u32 reserved, 13 u64 counts
+//   nv nhex ntet nhexface ntetface nvel npressure ninterface
+//   nwallhex ninhex nintet nouthex nouttet,
+// then, little-endian and packed: points (3 f64), hexes (8 i32), tets (4 i32),
+// hex velocity dofs (14 i32), tet velocity dofs (8 i32), hex and tet
+// pressure ids (i32), hex geometry (82 f64), tet geometry (12 f64),
+// interface records (9 i32) and the wall-hex, inlet-hex, inlet-tet,
+// outlet-hex, outlet-tet boundary records (cell, local face, bubble: 3 i32),
+// and nothing after them.  Local face lf of a tet is its vertices
+// kTetFace[lf] (the face opposite vertex lf).
+Mesh read_hxt1(const std::string& path) {
+  static const int kTetFace[4][3] = {{1, 2, 3}, {0, 3, 2}, {0, 1, 3}, {0, 2, 1}};
+  std::ifstream in(path, std::ios::binary);
+  if (!in) throw std::runtime_error("cannot open " + path);
+  char magic[8];
+  in.read(magic, 8);
+  if (!in || std::memcmp(magic, "HXT1BIN1", 8) != 0) throw std::runtime_error("bad HXT1 magic in " + path);
+  uint32_t version = 0, reserved = 0;
+  in.read(reinterpret_cast<char*>(&version), 4);
+  in.read(reinterpret_cast<char*>(&reserved), 4);
+  if (!in) throw std::runtime_error("short read: HXT1 version in " + path);
+  if (version != 1) throw std::runtime_error("unsupported HXT1 version " + std::to_string(version) + " in " + path);
+  uint64_t h[13];
+  in.read(reinterpret_cast<char*>(h), sizeof(h));
+  if (!in) throw std::runtime_error("short read: HXT1 header counts in " + path);
+  const uint64_t nv = h[0], nhex = h[1], ntet = h[2], nwallhex = h[8], ninhex = h[9], nintet = h[10],
+                 nouthex = h[11], nouttet = h[12], ninterface = h[7];
+  if (nhex || ninterface || nwallhex || ninhex || nouthex)
+    throw std::runtime_error("HXT1 mesh " + path + " has " + std::to_string(nhex) +
+                             " hex cells: the tetrahedral solver needs a pure-tet HXT1 file");
+  if (ntet == 0) throw std::runtime_error("no tetrahedra in " + path);
+  if (nv > (uint64_t)INT32_MAX || ntet > (uint64_t)INT32_MAX) throw std::runtime_error("HXT1 mesh too large: " + path);
+  auto read = [&](void* dst, uint64_t n, size_t size, const char* what) {
+    if (n) in.read(reinterpret_cast<char*>(dst), (std::streamsize)(n * size));
+    if (!in) throw std::runtime_error(std::string("short read: HXT1 ") + what + " in " + path);
+  };
+  auto skip = [&](uint64_t n, size_t size, const char* what) {
+    std::vector<char> junk(n * size);
+    read(junk.data(), n, size, what);
+  };
+  std::vector<double> xyz(3 * (size_t)nv);
+  read(xyz.data(), nv, 3 * sizeof(double), "points");
+  std::vector<int32_t> tets(4 * (size_t)ntet);
+  read(tets.data(), ntet, 4 * sizeof(int32_t), "tets");
+  skip(ntet, 8 * sizeof(int32_t), "tet velocity dofs");
+  skip(ntet, sizeof(int32_t), "tet pressure ids");
+  skip(ntet, 12 * sizeof(double), "tet geometry");
+  std::vector<int32_t> inrec(3 * (size_t)nintet), outrec(3 * (size_t)nouttet);
+  read(inrec.data(), nintet, 3 * sizeof(int32_t), "inlet tet records");
+  read(outrec.data(), nouttet, 3 * sizeof(int32_t), "outlet tet records");
+  char extra = 0;
+  in.read(&extra, 1);
+  if (in.gcount() != 0) throw std::runtime_error("trailing bytes in HXT1 mesh " + path);
+  for (int32_t v : tets)
+    if (v < 0 || (uint64_t)v >= nv) throw std::runtime_error("HXT1 tet references an unknown point in " + path);
+  // exterior faces: used by exactly one tet
+  using Key = std::array<int32_t, 3>;
+  auto key_of = [&](int c, int lf) {
+    Key k{tets[4 * (size_t)c + kTetFace[lf][0]], tets[4 * (size_t)c + kTetFace[lf][1]],
+          tets[4 * (size_t)c + kTetFace[lf][2]]};
+    std::sort(k.begin(), k.end());
+    return k;
+  };
+  std::vector<std::pair<Key, int64_t>> all;  // face, 4 cell + lf
+  all.reserve(4 * (size_t)ntet);
+  for (int c = 0; c < (int)ntet; ++c)
+    for (int lf = 0; lf < 4; ++lf) all.push_back({key_of(c, lf), 4 * (int64_t)c + lf});
+  std::sort(all.begin(), all.end());
+  std::vector<int8_t> label(4 * (size_t)ntet, -1);  // patch of each exterior (cell, lf); -2 interior
+  for (size_t a = 0; a < all.size();) {
+    size_t b = a;
+    while (b < all.size() && all[b].first == all[a].first) ++b;
+    if (b - a > 2) throw std::runtime_error("non-manifold face in HXT1 mesh " + path);
+    for (size_t q = a; q < b; ++q) label[(size_t)all[q].second] = (b - a == 1) ? 0 : -2;  // exterior: wall unless tagged
+    a = b;
+  }
+  auto tag = [&](const std::vector<int32_t>& rec, int patch, const char* what) {
+    for (size_t r = 0; r < rec.size() / 3; ++r) {
+      const int32_t c = rec[3 * r], lf = rec[3 * r + 1];
+      if (c < 0 || (uint64_t)c >= ntet || lf < 0 || lf > 3)
+        throw std::runtime_error(std::string("HXT1 ") + what + " record out of range in " + path);
+      int8_t& l = label[4 * (size_t)c + (size_t)lf];
+      if (l != 0) throw std::runtime_error(std::string("HXT1 ") + what + " face is not an untagged exterior face in " + path);
+      l = (int8_t)patch;
+    }
+  };
+  tag(inrec, 1, "inlet");
+  tag(outrec, 2, "outlet");
+  std::vector<int32_t> btri, bpatch;
+  for (int c = 0; c < (int)ntet; ++c)
+    for (int lf = 0; lf < 4; ++lf) {
+      const int8_t l = label[4 * (size_t)c + (size_t)lf];
+      if (l < 0) continue;
+      for (int k = 0; k < 3; ++k) btri.push_back(tets[4 * (size_t)c + kTetFace[lf][k]]);
+      bpatch.push_back(l);
+    }
+  std::vector<std::string> names(kCanonicalPatches, kCanonicalPatches + 3);
+  return mesh_from_arrays((int)nv, xyz.data(), (int)ntet, tets.data(), (int)bpatch.size(), btri.data(), bpatch.data(),
+                          names);
+}
+
 }  // namespace nds

@@ -51,6 +51,11 @@ Mesh read_polymesh(const std::string& dir);
 // Gmsh MSH 2.2 ASCII: tetrahedra (type 4) and tagged boundary triangles
 // (type 2); physical tag 1 = inlet, 2 = outlet, 3 = wall.
 Mesh read_msh2(const std::string& path);
+// Binary HXT1 ("HXT1BIN1", version 1): the mixed hex/tet mesh format of the
+// reference's hybrid and SST solvers (gpu/serial_cuda/hybrid_hxt1/
+// hxt1_mesh.hpp:19-103).  Files without hex cells only: points, tets, and the
+// inlet/outlet tet boundary records; every other exterior face is wall.
+Mesh read_hxt1(const std::string& path);
 // Raw arrays: points, tets (any orientation), boundary triangles with a patch
 // index into patch_names.
 Mesh mesh_from_arrays(int np, const double* xyz, int nc, const int32_t* tets, int nb,

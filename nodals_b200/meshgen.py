@@ -18,9 +18,9 @@ this module generates stand-ins of the named shapes:
   spacing with a splitmix64 stream seeded per configuration; nodes on the
   wall keep their radius, nodes on the inlet/outlet keep their z.
 
-Writers: ASCII polyMesh (faces ordered canonically, see ``canonical_faces``)
-and Gmsh MSH 2.2 with physical tags inlet=1, outlet=2, wall=3, volume=4
-(turbulence/sst_gpu_v2/tools/msh2_to_hxt1.py:9-42).  The C++ readers build
+Writers: ASCII polyMesh (faces ordered canonically, see ``canonical_faces``),
+Gmsh MSH 2.2 with physical tags inlet=1, outlet=2, wall=3, volume=4
+(turbulence/sst_gpu_v2/tools/msh2_to_hxt1.py:9-42), and binary HXT1.  The C++ readers build
 the same canonical face order from either file, so both formats number the
 velocity and pressure unknowns identically.
 """
@@ -364,6 +364,73 @@ def write_msh2(m: TetMesh, path: str | os.PathLike) -> Path:
             e += 1
         f.write("\n".join(lines))
         f.write("\n$EndElements\n")
+    return p
+
+
+# Binary HXT1, the mixed hex/tet mesh format of the reference's hybrid and
+# SST solvers (gpu/serial_cuda/hybrid_hxt1/hxt1_mesh.hpp:19-103), written
+# here for pure-tet meshes as the reference's converter does
+# (turbulence/sst_gpu_v2/tools/msh2_to_hxt1.py: positively oriented tets,
+# inlet and outlet tet records, no wall records).
+HXT1_MAGIC = b"HXT1BIN1"
+HXT1_TET_FACE = ((1, 2, 3), (0, 3, 2), (0, 1, 3), (0, 2, 1))  # face opposite local vertex lf
+
+
+def _det3_cols(a, b, c):
+    """Determinant of the 3x3 matrices with columns a, b, c (rows of (n, 3) arrays)."""
+    return (a[:, 0] * (b[:, 1] * c[:, 2] - b[:, 2] * c[:, 1])
+            - b[:, 0] * (a[:, 1] * c[:, 2] - a[:, 2] * c[:, 1])
+            + c[:, 0] * (a[:, 1] * b[:, 2] - a[:, 2] * b[:, 1]))
+
+
+def write_hxt1(m: TetMesh, path: str | os.PathLike) -> Path:
+    """HXT1 version 1 for a tetrahedral mesh: points; tets with a positive
+    Jacobian (vertices 2 and 3 swapped otherwise); per tet the 8 velocity
+    unknowns (4 vertices, then the bubbles of the faces opposite vertices
+    0..3, a face's bubble numbered n_points + the rank of its sorted vertex
+    triple); pressure ids 0..nt-1; geometry (volume, squared longest edge,
+    det J, J^-1 row-major, J = [X1-X0 | X2-X0 | X3-X0]); the inlet and
+    outlet faces as (tet, local face, bubble) records in boundary-list
+    order.  All other counts are zero."""
+    pts = np.ascontiguousarray(m.points, dtype=np.float64)
+    tets = np.array(m.tets, dtype=np.int32)
+    nv, nt = len(pts), len(tets)
+    x = pts[tets]
+    det = _det3_cols(x[:, 1] - x[:, 0], x[:, 2] - x[:, 0], x[:, 3] - x[:, 0])
+    flip = det < 0
+    tets[flip, 2], tets[flip, 3] = tets[flip, 3].copy(), tets[flip, 2].copy()
+    x = pts[tets]
+    e1, e2, e3 = x[:, 1] - x[:, 0], x[:, 2] - x[:, 0], x[:, 3] - x[:, 0]
+    det = _det3_cols(e1, e2, e3)
+    # J^-1 = adj(J) / det; with J's columns e1, e2, e3 the rows of J^-1 are
+    # e2 x e3, e3 x e1, e1 x e2 divided by det
+    inv = np.stack((np.cross(e2, e3), np.cross(e3, e1), np.cross(e1, e2)), axis=1) / det[:, None, None]
+    h2 = np.zeros(nt)
+    for a in range(4):
+        for b in range(a + 1, 4):
+            d = x[:, a] - x[:, b]
+            h2 = np.maximum(h2, np.einsum("ij,ij->i", d, d))
+    geom = np.column_stack((det / 6.0, h2, det, inv.reshape(nt, 9)))
+    keys = np.sort(tets[:, np.asarray(HXT1_TET_FACE)], axis=2).reshape(-1, 3)
+    uniq, rank = np.unique(keys, axis=0, return_inverse=True)
+    bubble = (nv + rank.reshape(nt, 4)).astype(np.int32)
+    tvel = np.concatenate((tets, bubble), axis=1)
+    lookup = {tuple(k): (i // 4, i % 4) for i, k in enumerate(map(tuple, keys))}
+
+    def records(tag):
+        out = []
+        for tri in m.bfaces[m.btag == tag]:
+            c, lf = lookup[tuple(sorted(int(v) for v in tri))]
+            out.append((c, lf, int(bubble[c, lf])))
+        return np.asarray(out, dtype=np.int32).reshape(-1, 3)
+    rin, rout = records(PATCHES.index("patch_2_0")), records(PATCHES.index("patch_1_0"))
+    header = (nv, 0, nt, 0, len(uniq), nv + len(uniq), nt, 0, 0, 0, len(rin), 0, len(rout))
+    p = Path(path)
+    p.parent.mkdir(parents=True, exist_ok=True)
+    with open(p, "wb") as f:
+        f.write(HXT1_MAGIC + np.asarray([1, 0], dtype="<u4").tobytes() + np.asarray(header, dtype="<u8").tobytes())
+        for a in (pts, tets, tvel, np.arange(nt, dtype=np.int32), geom, rin, rout):
+            f.write(np.ascontiguousarray(a).astype(a.dtype.newbyteorder("<"), copy=False).tobytes())
     return p
 
 

@@ -127,6 +127,7 @@ def lib():
         L.nds_options_default.argtypes = [C.POINTER(Options)]
         L.nds_mesh_read_polymesh.argtypes = [C.c_char_p, C.POINTER(vp)]
         L.nds_mesh_read_msh2.argtypes = [C.c_char_p, C.POINTER(vp)]
+        L.nds_mesh_read_hxt1.argtypes = [C.c_char_p, C.POINTER(vp)]
         L.nds_mesh_from_arrays.argtypes = [C.c_int, vp, C.c_int, vp, C.c_int, vp, vp, C.c_int, C.POINTER(C.c_char_p),
                                            C.POINTER(vp)]
         L.nds_mesh_counts.argtypes = [vp] + [C.POINTER(C.c_int)] * 4
@@ -177,6 +178,12 @@ class Mesh:
     def read_msh2(cls, path) -> "Mesh":
         h = C.c_void_p()
         _check(lib().nds_mesh_read_msh2(str(path).encode(), C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def read_hxt1(cls, path) -> "Mesh":
+        h = C.c_void_p()
+        _check(lib().nds_mesh_read_hxt1(str(path).encode(), C.byref(h)))
         return cls(h)
 
     @classmethod

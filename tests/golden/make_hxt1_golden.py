@@ -1,0 +1,37 @@
+"""Golden HXT1 file made by the reference's own converter.
+
+Writes the seeded ``pipe_tiny`` mesh as MSH 2.2 with this package's writer,
+converts it with the reference's ``turbulence/sst_gpu_v2/tools/msh2_to_hxt1.py``
+(which runs its ``prepare_hxt1.py``) and keeps the resulting
+``HXT1_mesh.bin`` as ``tests/golden/hxt1_pipe_tiny.bin``.  Needs the
+reference tree (first argument, default /root/reference); the tests only read
+the committed file.
+"""
+from __future__ import annotations
+
+import shutil
+import subprocess
+import sys
+import tempfile
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+ROOT = HERE.parents[1]
+sys.path.insert(0, str(ROOT))
+
+from nodals_b200 import meshgen  # noqa: E402
+
+
+def main() -> None:
+    ref = Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference")
+    conv = ref / "turbulence" / "sst_gpu_v2" / "tools" / "msh2_to_hxt1.py"
+    with tempfile.TemporaryDirectory() as tmp:
+        msh = meshgen.write_msh2(meshgen.named("pipe_tiny"), Path(tmp) / "pipe_tiny.msh")
+        subprocess.run([sys.executable, str(conv), "--msh", str(msh), "--out", str(Path(tmp) / "out")], check=True,
+                       stdout=subprocess.DEVNULL)
+        shutil.copy(Path(tmp) / "out" / "HXT1_mesh.bin", HERE / "hxt1_pipe_tiny.bin")
+    print("wrote", HERE / "hxt1_pipe_tiny.bin")
+
+
+if __name__ == "__main__":
+    main()

@@ -65,3 +65,20 @@ def test_executable_reproduces_reference_run(case, tmp_path):
         ftol = 1e-3 if fp32 else 1e-8
         assert rel_l2(p, g["p"]) <= ftol
         assert rel_l2(u0, g["u_cell"]) <= ftol
+
+
+@pytest.mark.gpu
+def test_executable_reads_hxt1(tmp_path):
+    """--mesh given the HXT1 file the reference's converter made from the
+    pipe_tiny mesh: every NODALS_GPU_H8_SIMPLE line equals the one of the
+    MSH 2.2 run of the same mesh."""
+    from nodals_b200 import meshgen
+    msh = meshgen.write_msh2(meshgen.named("pipe_tiny"), tmp_path / "m.msh")
+    exe = LIB / "nodals_gpu_h8_fp64"
+    common = ["--run-mode", "fixed10", "--max-outer", "10", "--amg-terminal", "60", "--p-rtol", "1e-6", "--p-max", "200"]
+    outs = []
+    for mesh in (msh, GOLDEN / "hxt1_pipe_tiny.bin"):
+        r = subprocess.run([str(exe), "--mesh", str(mesh), *common], capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stderr[-2000:]
+        outs.append([l for l in r.stdout.splitlines() if l.startswith("NODALS_GPU_H8_SIMPLE")])
+    assert len(outs[0]) == 10 and outs[0] == outs[1]
