@@ -219,6 +219,36 @@ unsigned long long nds_launch_count(void);
 int nds_continuity_noalloc(nds_solver* s, const double* u0, const double* u1, const double* u2, double* r,
                            double* norm, void* stream);
 
+/* ---- mixed hexahedron/tetrahedron Stokes gate: replaces the reference's
+ *      HXT4A executable (gpu/serial_cuda/hybrid_hxt4a/hxt4a_main.cu:405-518,
+ *      operators from hybrid_hxt2/hxt2_main.cu and hybrid_hxt3a/hxt3a_main.cu).
+ * Reads a binary HXT1 mesh with hex and tet cells (Q1+BF2 hex and P1+BF3
+ * tet velocity, P0 pressure, Nitsche-coupled interface), sets the
+ * manufactured axial pressure p* (cell centroid z, 0 at cell 0) and runs the
+ * SIMPLE loop of the gate: three Jacobi-PCG momentum solves with forcing
+ * B^T p* - B^T p, one Jacobi-PCG solve of B diag(rAU) B^T (rAU = rau_scale /
+ * penalty-free diag A), p += alpha_p dp, until relCont <= simple_tol.
+ * verbose = 1 prints the reference's NODALS_HXT4A_* lines.  Returns NDS_OK
+ * when the loop ran to convergence (pass tells whether the gate's
+ * accuracy criteria hold), NDS_E_SETUP for a bad mesh or a failed solve,
+ * NDS_E_CUDA without a device. */
+typedef struct nds_hybrid_report {
+  int outer_its, converged, pass;
+  int n_hex, n_tet, n_interface, n_velocity;
+  double final_rel_cont, pressure_rel_l2, slope, slope_exact, delta, delta_exact, velocity_rel;
+  double avg_momentum_cg, avg_pressure_cg;
+  double a_norm, b_norm, s_norm;   /* operator audit: ||A a||, ||B b||, ||S p|| on fixed vectors */
+  double loop_ms;                  /* wall time of the SIMPLE loop and final predictor */
+} nds_hybrid_report;
+int nds_hybrid_stokes_gate(const char* hxt1_path, double nu, double gamma, double rau_scale, double alpha_p,
+                           double simple_tol, int max_outer, int device, int verbose, nds_hybrid_report* out);
+/* Host-only operator audit of the same gate (no device needed): norms[0..2] =
+ * ||A a||, ||B b||, ||S p|| for the gate's fixed vectors a_g = sin(0.00113
+ * (g+1)), b = (cos(0.00131 (g+1)), sin(0.00091 (g+1) + 0.2), cos(0.00157
+ * (g+1) - 0.1)), p_i = sin(0.00107 (i+1)), as the reference prints them in
+ * NODALS_HXT4A_OPERATOR_AUDIT (hxt4a_main.cu:429-437). */
+int nds_hybrid_operator_audit(const char* hxt1_path, double nu, double gamma, double rau_scale, double norms[3]);
+
 #ifdef __cplusplus
 }
 #endif

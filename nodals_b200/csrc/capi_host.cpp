@@ -1,6 +1,7 @@
 // Host half of the C ABI: meshes, options and the host setup ("problem").
 // No CUDA call is made here, so these entry points work on CPU-only hosts.
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -10,6 +11,7 @@
 
 #include "../../include/nodals_b200.h"
 #include "capi_internal.hpp"
+#include "host/hybrid.hpp"
 #include "host/amg.hpp"
 #include "host/diagnostics.hpp"
 #include "host/fem.hpp"
@@ -112,6 +114,64 @@ int nds_mesh_read_msh2(const char* path, nds_mesh** out) {
     return NDS_E_SETUP;
   }
 }
+int nds_hybrid_operator_audit(const char* path, double nu, double gamma, double rau_scale, double norms[3]) {
+  if (!path || !norms || !(nu > 0) || !(gamma > 0) || !(rau_scale > 0)) {
+    set_error("nds_hybrid_operator_audit: bad argument");
+    return NDS_E_INVALID;
+  }
+  try {
+    const nds::HybridMesh m = nds::read_hxt1_hybrid(path);
+    const nds::HybridStokes H = nds::build_hybrid_stokes(m, nds::interface_plans(m), nu, gamma);
+    const int nv = H.nvel, np = H.np;
+    std::vector<double> a((size_t)nv), b0((size_t)nv), b1((size_t)nv), b2((size_t)nv), p((size_t)np);
+    for (int g = 0; g < nv; ++g) {
+      const double q = g + 1;
+      a[(size_t)g] = std::sin(0.00113 * q);
+      b0[(size_t)g] = std::cos(.00131 * q);
+      b1[(size_t)g] = std::sin(.00091 * q + .2);
+      b2[(size_t)g] = std::cos(.00157 * q - .1);
+    }
+    for (int i = 0; i < np; ++i) p[(size_t)i] = std::sin(.00107 * (i + 1));
+    auto norm = [](const std::vector<double>& x) {
+      long double s = 0;
+      for (double v : x) s += (long double)v * v;
+      return (double)std::sqrt(s);
+    };
+    std::vector<double> y((size_t)nv, 0.0), c((size_t)np, 0.0), v[3];
+    for (int i = 0; i < nv; ++i)
+      for (int32_t k = H.a_row[(size_t)i]; k < H.a_row[(size_t)i + 1]; ++k) y[(size_t)i] += H.a_val[(size_t)k] * a[(size_t)H.a_col[(size_t)k]];
+    norms[0] = norm(y);
+    for (int i = 0; i < np; ++i)
+      for (int32_t k = H.b_row[(size_t)i]; k < H.b_row[(size_t)i + 1]; ++k) {
+        const size_t g = (size_t)H.b_col[(size_t)k];
+        c[(size_t)i] += H.bx[(size_t)k] * b0[g] + H.by[(size_t)k] * b1[g] + H.bz[(size_t)k] * b2[g];
+      }
+    norms[1] = norm(c);
+    for (auto& q : v) q.assign((size_t)nv, 0.0);
+    for (int g = 0; g < nv; ++g) {
+      const double r = H.fixed[(size_t)g] ? 0.0 : rau_scale / H.diag_rau[(size_t)g];
+      for (int32_t k = H.bt_row[(size_t)g]; k < H.bt_row[(size_t)g + 1]; ++k) {
+        const double q = p[(size_t)H.bt_col[(size_t)k]];
+        v[0][(size_t)g] += H.btx[(size_t)k] * q;
+        v[1][(size_t)g] += H.bty[(size_t)k] * q;
+        v[2][(size_t)g] += H.btz[(size_t)k] * q;
+      }
+      for (auto& q : v) q[(size_t)g] *= r;
+    }
+    std::fill(c.begin(), c.end(), 0.0);
+    for (int i = 1; i < np; ++i)  // row 0 is the pressure pin
+      for (int32_t k = H.b_row[(size_t)i]; k < H.b_row[(size_t)i + 1]; ++k) {
+        const size_t g = (size_t)H.b_col[(size_t)k];
+        c[(size_t)i] += H.bx[(size_t)k] * v[0][g] + H.by[(size_t)k] * v[1][g] + H.bz[(size_t)k] * v[2][g];
+      }
+    norms[2] = norm(c);
+    return NDS_OK;
+  } catch (const std::exception& e) {
+    set_error(e.what());
+    return NDS_E_SETUP;
+  }
+}
+
 int nds_mesh_read_hxt1(const char* path, nds_mesh** out) {
   if (!path || !out) { set_error("null argument"); return NDS_E_INVALID; }
   try {

@@ -1,0 +1,585 @@
+#include "hybrid.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <fstream>
+#include <map>
+#include <stdexcept>
+#include <tuple>
+
+#include "fem.hpp"
+
+namespace nds {
+namespace {
+
+// Reference hexahedron [-1,1]^3: vertex a sits at kHexSign[a]; local face f
+// is kHexFace[f] (z-, z+, y-, x+, y+, x-), bubble 8 + f lives on it.  A
+// tet's local face lf is kTetFace[lf], the face opposite vertex lf.
+// (hybrid_hxt2/hxt2_main.cu:18-27, hybrid_hxt1/prepare_hxt1.py)
+const int kHexSign[8][3] = {{-1, -1, -1}, {1, -1, -1}, {1, 1, -1}, {-1, 1, -1},
+                            {-1, -1, 1},  {1, -1, 1},  {1, 1, 1},  {-1, 1, 1}};
+const int kHexFace[6][4] = {{0, 1, 2, 3}, {4, 5, 6, 7}, {0, 1, 5, 4}, {1, 2, 6, 5}, {2, 3, 7, 6}, {3, 0, 4, 7}};
+const int kTetFace[4][3] = {{1, 2, 3}, {0, 3, 2}, {0, 1, 3}, {0, 2, 1}};
+
+// trilinear (Q1) values and reference gradients
+void hex_q1(double x, double y, double z, double phi[8], double g[8][3]) {
+  for (int a = 0; a < 8; ++a) {
+    const double sx = kHexSign[a][0], sy = kHexSign[a][1], sz = kHexSign[a][2];
+    const double ax = 1.0 + sx * x, ay = 1.0 + sy * y, az = 1.0 + sz * z;
+    phi[a] = 0.125 * ax * ay * az;
+    g[a][0] = 0.125 * sx * ay * az;
+    g[a][1] = 0.125 * sy * ax * az;
+    g[a][2] = 0.125 * sz * ax * ay;
+  }
+}
+
+// Q1 + BF2: the bubble of face f is the Q1 factor of the face-normal
+// coordinate that is 1 on f times the quadratic bubbles (1 - t^2) of the two
+// tangential coordinates (value 1 at the face centre, 1/2 at the cell centre)
+// (hybrid_hxt2/hxt2_main.cu:176-187, prepare_hxt1.py bf2_value)
+void hex_basis(double x, double y, double z, double phi[14], double g[14][3]) {
+  hex_q1(x, y, z, phi, g);
+  const double bx = 1 - x * x, by = 1 - y * y, bz = 1 - z * z;
+  const double dx = -2 * x, dy = -2 * y, dz = -2 * z;
+  // normal coordinate n in {x, y, z}, side sgn = -1 / +1
+  auto face = [&](int f, int n, double sgn) {
+    const double c[3] = {x, y, z}, b[3] = {bx, by, bz}, d[3] = {dx, dy, dz};
+    const int t1 = n == 0 ? 1 : 0, t2 = n == 2 ? 1 : 2;
+    const double s = 0.5 * (1.0 + sgn * c[n]);
+    phi[8 + f] = s * b[t1] * b[t2];
+    g[8 + f][n] = 0.5 * sgn * b[t1] * b[t2];
+    g[8 + f][t1] = s * d[t1] * b[t2];
+    g[8 + f][t2] = s * b[t1] * d[t2];
+  };
+  face(0, 2, -1.0);
+  face(1, 2, 1.0);
+  face(2, 1, -1.0);
+  face(3, 0, 1.0);
+  face(4, 1, 1.0);
+  face(5, 0, -1.0);
+}
+
+// J^-1 (row-major, I[3 j + d] = d xi_j / d x_d) and det J at (x, y, z)
+void hex_metric(const HybridMesh& m, int c, double x, double y, double z, double I[9], double& det) {
+  double phi[8], g[8][3];
+  hex_q1(x, y, z, phi, g);
+  double J[9] = {};
+  for (int a = 0; a < 8; ++a) {
+    const double* p = &m.xyz[3 * (size_t)m.hexes[(size_t)c][(size_t)a]];
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) J[3 * i + j] += p[i] * g[a][j];
+  }
+  det = J[0] * (J[4] * J[8] - J[5] * J[7]) - J[1] * (J[3] * J[8] - J[5] * J[6]) + J[2] * (J[3] * J[7] - J[4] * J[6]);
+  if (!(det > 0)) throw std::runtime_error("hybrid mesh: non-positive hex Jacobian in cell " + std::to_string(c));
+  const double q = 1.0 / det;
+  I[0] = (J[4] * J[8] - J[5] * J[7]) * q;
+  I[1] = (J[2] * J[7] - J[1] * J[8]) * q;
+  I[2] = (J[1] * J[5] - J[2] * J[4]) * q;
+  I[3] = (J[5] * J[6] - J[3] * J[8]) * q;
+  I[4] = (J[0] * J[8] - J[2] * J[6]) * q;
+  I[5] = (J[2] * J[3] - J[0] * J[5]) * q;
+  I[6] = (J[3] * J[7] - J[4] * J[6]) * q;
+  I[7] = (J[1] * J[6] - J[0] * J[7]) * q;
+  I[8] = (J[0] * J[4] - J[1] * J[3]) * q;
+}
+
+template <int N>
+void phys_grad(const double g[][3], const double I[9], double gp[][3]) {
+  for (int a = 0; a < N; ++a)
+    for (int d = 0; d < 3; ++d) gp[a][d] = g[a][0] * I[d] + g[a][1] * I[3 + d] + g[a][2] * I[6 + d];
+}
+
+struct V3 {
+  double x, y, z;
+};
+V3 point(const HybridMesh& m, int v) { return {m.xyz[3 * (size_t)v], m.xyz[3 * (size_t)v + 1], m.xyz[3 * (size_t)v + 2]}; }
+V3 sub(V3 a, V3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+V3 cross(V3 a, V3 b) { return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
+double dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+double tri_area(V3 a, V3 b, V3 c) { return 0.5 * std::sqrt(dot(cross(sub(b, a), sub(c, a)), cross(sub(b, a), sub(c, a)))); }
+V3 hex_centroid(const HybridMesh& m, int c) {
+  V3 q{0, 0, 0};
+  for (int a = 0; a < 8; ++a) {
+    const V3 p = point(m, m.hexes[(size_t)c][(size_t)a]);
+    q = {q.x + p.x, q.y + p.y, q.z + p.z};
+  }
+  return {q.x / 8, q.y / 8, q.z / 8};
+}
+V3 tet_centroid(const HybridMesh& m, int c) {
+  V3 q{0, 0, 0};
+  for (int a = 0; a < 4; ++a) {
+    const V3 p = point(m, m.tets[(size_t)c][(size_t)a]);
+    q = {q.x + p.x, q.y + p.y, q.z + p.z};
+  }
+  return {q.x / 4, q.y / 4, q.z / 4};
+}
+
+// tensor-product rules: 3-point Gauss on [-1,1] for hex volumes; the
+// collapsed 5 x 5 rule on interface triangles (Gauss-Legendre on [0,1] in
+// both directions, weight (1 - r) folded in by the Duffy map)
+struct Rules {
+  double g3x[3], g3w[3];
+  std::vector<double> q5x, q5w;
+  Rules() {
+    const double a = std::sqrt(0.6);
+    g3x[0] = -a; g3x[1] = 0.0; g3x[2] = a;
+    g3w[0] = 5.0 / 9.0; g3w[1] = 8.0 / 9.0; g3w[2] = 5.0 / 9.0;
+    gauss_jacobi01(5, 0, q5x, q5w);
+  }
+};
+const Rules& rules() {
+  static const Rules r;
+  return r;
+}
+
+// The 25 points of interface triangle s of plan p, each with the hex and
+// tet basis values and physical gradients there.
+template <class F>
+void for_interface_points(const HybridMesh& m, const InterfacePlan& p, int s, F&& f) {
+  const Rules& R = rules();
+  const auto& tg = m.tet_geom[(size_t)p.tet_cell[s]];
+  for (int ia = 0; ia < 5; ++ia)
+    for (int ib = 0; ib < 5; ++ib) {
+      const double rr = R.q5x[(size_t)ia], ss = R.q5x[(size_t)ib], om = 1.0 - rr;
+      const double L[3] = {om * (1.0 - ss), rr, om * ss};
+      const double w = R.q5w[(size_t)ia] * R.q5w[(size_t)ib] * om * 2.0 * p.area_tri[s];
+      double xr = 0, yr = 0, zr = 0;
+      for (int k = 0; k < 3; ++k) {
+        const int hl = p.hex_tri_local[s][k];
+        xr += L[k] * kHexSign[hl][0];
+        yr += L[k] * kHexSign[hl][1];
+        zr += L[k] * kHexSign[hl][2];
+      }
+      double ph[14], gh[14][3], gph[14][3], I[9], det;
+      hex_basis(xr, yr, zr, ph, gh);
+      hex_metric(m, p.hex_cell, xr, yr, zr, I, det);
+      phys_grad<14>(gh, I, gph);
+      std::array<double, 4> lam{0, 0, 0, 0};
+      for (int k = 0; k < 3; ++k) lam[(size_t)kTetFace[p.tet_face[s]][k]] = L[k];
+      double pt[8], gt[8][3], gpt[8][3];
+      basis_eval(lam, pt, gt);
+      phys_grad<8>(gt, tg.data() + 3, gpt);
+      f(w, ph, gph, pt, gpt);
+    }
+}
+
+}  // namespace
+
+HybridMesh read_hxt1_hybrid(const std::string& path) {
+  std::ifstream in(path, std::ios::binary);
+  if (!in) throw std::runtime_error("cannot open " + path);
+  char magic[8];
+  in.read(magic, 8);
+  if (!in || std::memcmp(magic, "HXT1BIN1", 8) != 0) throw std::runtime_error("bad HXT1 magic in " + path);
+  uint32_t version = 0, reserved = 0;
+  in.read(reinterpret_cast<char*>(&version), 4);
+  in.read(reinterpret_cast<char*>(&reserved), 4);
+  if (!in || version != 1) throw std::runtime_error("unsupported HXT1 version in " + path);
+  HybridMesh m;
+  in.read(reinterpret_cast<char*>(m.count), sizeof(m.count));
+  if (!in) throw std::runtime_error("short read: HXT1 header counts in " + path);
+  for (uint64_t c : m.count)
+    if (c > (uint64_t)INT32_MAX) throw std::runtime_error("HXT1 mesh too large: " + path);
+  auto read = [&](auto& v, uint64_t n, const char* what) {
+    v.resize((size_t)n);
+    if (n) in.read(reinterpret_cast<char*>(v.data()), (std::streamsize)(n * sizeof(v[0])));
+    if (!in) throw std::runtime_error(std::string("short read: HXT1 ") + what + " in " + path);
+  };
+  std::vector<int32_t> hp, tp;
+  m.xyz.resize(3 * (size_t)m.count[0]);
+  if (m.count[0]) in.read(reinterpret_cast<char*>(m.xyz.data()), (std::streamsize)(m.xyz.size() * sizeof(double)));
+  if (!in) throw std::runtime_error("short read: HXT1 points in " + path);
+  read(m.hexes, m.count[1], "hexes");
+  read(m.tets, m.count[2], "tets");
+  read(m.hex_dofs, m.count[1], "hex velocity dofs");
+  read(m.tet_dofs, m.count[2], "tet velocity dofs");
+  read(hp, m.count[1], "hex pressure ids");
+  read(tp, m.count[2], "tet pressure ids");
+  read(m.hex_geom, m.count[1], "hex geometry");
+  read(m.tet_geom, m.count[2], "tet geometry");
+  read(m.interface, m.count[7], "interface");
+  read(m.wall_hex, m.count[8], "wall hex");
+  read(m.in_hex, m.count[9], "inlet hex");
+  read(m.in_tet, m.count[10], "inlet tet");
+  read(m.out_hex, m.count[11], "outlet hex");
+  read(m.out_tet, m.count[12], "outlet tet");
+  char extra = 0;
+  in.read(&extra, 1);
+  if (in.gcount() != 0) throw std::runtime_error("trailing bytes in HXT1 mesh " + path);
+  for (int c = 0; c < m.nhex(); ++c)
+    if (hp[(size_t)c] != c) throw std::runtime_error("HXT1 hex pressure ids are not 0..nhex-1 in " + path);
+  for (int c = 0; c < m.ntet(); ++c)
+    if (tp[(size_t)c] != m.nhex() + c) throw std::runtime_error("HXT1 tet pressure ids do not follow the hexes in " + path);
+  const int nvel = m.nvel();
+  auto dofs_ok = [&](const int32_t* g, int n) {
+    for (int a = 0; a < n; ++a)
+      if (g[a] < 0 || g[a] >= nvel) return false;
+    return true;
+  };
+  for (const auto& h : m.hex_dofs)
+    if (!dofs_ok(h.data(), 14)) throw std::runtime_error("HXT1 hex velocity dof out of range in " + path);
+  for (const auto& t : m.tet_dofs)
+    if (!dofs_ok(t.data(), 8)) throw std::runtime_error("HXT1 tet velocity dof out of range in " + path);
+  return m;
+}
+
+std::vector<InterfacePlan> interface_plans(const HybridMesh& m) {
+  std::vector<InterfacePlan> P;
+  P.reserve(m.interface.size());
+  for (const auto& r : m.interface) {
+    InterfacePlan p{};
+    p.hex_cell = r[0];
+    p.hex_face = r[1];
+    p.tet_cell[0] = r[3];
+    p.tet_face[0] = r[4];
+    p.tet_cell[1] = r[6];
+    p.tet_face[1] = r[7];
+    if (p.hex_cell < 0 || p.hex_cell >= m.nhex() || p.hex_face < 0 || p.hex_face > 5)
+      throw std::runtime_error("HXT1 interface record out of range");
+    const auto& hc = m.hexes[(size_t)p.hex_cell];
+    V3 q[4];
+    for (int k = 0; k < 4; ++k) q[k] = point(m, hc[(size_t)kHexFace[p.hex_face][k]]);
+    p.area_quad = tri_area(q[0], q[1], q[2]) + tri_area(q[0], q[2], q[3]);
+    V3 n = cross(sub(q[1], q[0]), sub(q[3], q[0]));
+    const double nn = std::sqrt(dot(n, n));
+    if (!(nn > 0)) throw std::runtime_error("hybrid mesh: zero interface quad normal");
+    n = {n.x / nn, n.y / nn, n.z / nn};
+    if (p.tet_cell[0] < 0 || p.tet_cell[0] >= m.ntet() || p.tet_cell[1] < 0 || p.tet_cell[1] >= m.ntet())
+      throw std::runtime_error("HXT1 interface record out of range");
+    if (dot(n, sub(tet_centroid(m, p.tet_cell[0]), hex_centroid(m, p.hex_cell))) < 0) n = {-n.x, -n.y, -n.z};
+    p.normal[0] = n.x;
+    p.normal[1] = n.y;
+    p.normal[2] = n.z;
+    const double vh = m.hex_geom[(size_t)p.hex_cell][0];
+    if (!(vh > 0)) throw std::runtime_error("hybrid mesh: non-positive hex volume");
+    p.inv_h_hex = p.area_quad / (2.0 * vh);
+    for (int s = 0; s < 2; ++s) {
+      const auto& tc = m.tets[(size_t)p.tet_cell[s]];
+      V3 tp[3];
+      for (int k = 0; k < 3; ++k) {
+        const int gv = tc[(size_t)kTetFace[p.tet_face[s]][k]];
+        tp[k] = point(m, gv);
+        int hl = -1;
+        for (int a = 0; a < 8; ++a)
+          if (hc[(size_t)a] == gv) hl = a;
+        bool on_face = false;
+        for (int a = 0; a < 4; ++a)
+          if (kHexFace[p.hex_face][a] == hl) on_face = true;
+        if (!on_face) throw std::runtime_error("hybrid mesh: interface triangle vertex not on its hex face");
+        p.hex_tri_local[s][k] = hl;
+      }
+      p.area_tri[s] = tri_area(tp[0], tp[1], tp[2]);
+      const double vt = m.tet_geom[(size_t)p.tet_cell[s]][0];
+      if (!(vt > 0 && p.area_tri[s] > 0)) throw std::runtime_error("hybrid mesh: bad interface tet geometry");
+      p.inv_h_tet[s] = p.area_tri[s] / (2.0 * vt);
+    }
+    if (std::abs(p.area_tri[0] + p.area_tri[1] - p.area_quad) > 1e-12 * p.area_quad)
+      throw std::runtime_error("hybrid mesh: interface quad and triangle areas differ (non-planar quad)");
+    P.push_back(p);
+  }
+  return P;
+}
+
+HybridStokes build_hybrid_stokes(const HybridMesh& m, const std::vector<InterfacePlan>& plans, double nu,
+                                 double gamma) {
+  const Rules& R = rules();
+  HybridStokes H;
+  H.nvel = m.nvel();
+  H.np = m.np();
+  const int nv = H.nvel;
+  // ---- velocity operator as (row, col, value) triples in generation order;
+  // a stable sort by (row, col) then sums equal positions in that order
+  struct Trip {
+    int32_t r, c;
+    double v;
+  };
+  std::vector<Trip> t;
+  t.reserve((size_t)m.nhex() * 196 + (size_t)m.ntet() * 64 + plans.size() * 2 * 484);
+  H.diag_full.assign((size_t)nv, 0.0);
+  H.diag_rau.assign((size_t)nv, 0.0);
+  // hex volumes: K_ab = sum_q nu det w grad phi_a . grad phi_b (27 points)
+  for (int c = 0; c < m.nhex(); ++c) {
+    double K[14][14] = {};
+    for (int ix = 0; ix < 3; ++ix)
+      for (int iy = 0; iy < 3; ++iy)
+        for (int iz = 0; iz < 3; ++iz) {
+          const double x = R.g3x[ix], y = R.g3x[iy], z = R.g3x[iz], w = R.g3w[ix] * R.g3w[iy] * R.g3w[iz];
+          double ph[14], g[14][3], gp[14][3], I[9], det;
+          hex_basis(x, y, z, ph, g);
+          hex_metric(m, c, x, y, z, I, det);
+          phys_grad<14>(g, I, gp);
+          const double q = nu * det * w;
+          for (int a = 0; a < 14; ++a)
+            for (int b = 0; b < 14; ++b) K[a][b] += q * (gp[a][0] * gp[b][0] + gp[a][1] * gp[b][1] + gp[a][2] * gp[b][2]);
+        }
+    const auto& g = m.hex_dofs[(size_t)c];
+    for (int a = 0; a < 14; ++a) {
+      H.diag_rau[(size_t)g[(size_t)a]] += K[a][a];
+      for (int b = 0; b < 14; ++b) t.push_back({g[(size_t)a], g[(size_t)b], K[a][b]});
+    }
+  }
+  // tet volumes: K_ab = nu det sum_jk D[a][b][j][k] (J^-T J^-1)_jk
+  const auto& D = ref_tensors().D;
+  for (int c = 0; c < m.ntet(); ++c) {
+    const auto& tg = m.tet_geom[(size_t)c];
+    double M[3][3] = {};
+    for (int j = 0; j < 3; ++j)
+      for (int k = 0; k < 3; ++k)
+        for (int d = 0; d < 3; ++d) M[j][k] += tg[3 + 3 * (size_t)j + d] * tg[3 + 3 * (size_t)k + d];
+    const auto& g = m.tet_dofs[(size_t)c];
+    for (int a = 0; a < 8; ++a)
+      for (int b = 0; b < 8; ++b) {
+        double kd = 0;
+        for (int j = 0; j < 3; ++j)
+          for (int k = 0; k < 3; ++k) kd += D[a][b][j][k] * M[j][k];
+        const double v = nu * tg[2] * kd;
+        if (a == b) H.diag_rau[(size_t)g[(size_t)a]] += v;
+        t.push_back({g[(size_t)a], g[(size_t)b], v});
+      }
+  }
+  // Nitsche coupling on each interface triangle.  Over the union u of the
+  // hex's and the tet's unknowns, the jump coefficient J_i = phi^hex_i -
+  // phi^tet_i and the averaged flux coefficient F_i = nu/2 (grad phi^hex_i +
+  // grad phi^tet_i) . n give K_ij = w (-J_i F_j - F_i J_j + tau J_i J_j),
+  // tau = gamma nu max(1/h_hex, 1/h_tet)  (hybrid_hxt4b/hxt4b_main.cu
+  // interface_assemble; hybrid_hxt2/hxt2_main.cu interface_kernel)
+  for (const auto& p : plans)
+    for (int s = 0; s < 2; ++s) {
+      const auto& hg = m.hex_dofs[(size_t)p.hex_cell];
+      const auto& tgd = m.tet_dofs[(size_t)p.tet_cell[s]];
+      int u[22], hu[14], tu[8], nu_ = 0;
+      for (int a = 0; a < 14; ++a) {
+        hu[a] = nu_;
+        u[nu_++] = hg[(size_t)a];
+      }
+      for (int b = 0; b < 8; ++b) {
+        int at = -1;
+        for (int q = 0; q < nu_; ++q)
+          if (u[q] == tgd[(size_t)b]) at = q;
+        if (at < 0) {
+          at = nu_;
+          u[nu_++] = tgd[(size_t)b];
+        }
+        tu[b] = at;
+      }
+      const double tau = gamma * nu * std::max(p.inv_h_hex, p.inv_h_tet[s]);
+      const double* n = p.normal;
+      double K[22][22] = {}, cons[22] = {};
+      for_interface_points(m, p, s, [&](double w, const double* ph, const double (*gph)[3], const double* pt,
+                                        const double (*gpt)[3]) {
+        double J[22] = {}, F[22] = {};
+        for (int a = 0; a < 14; ++a) {
+          J[hu[a]] += ph[a];
+          F[hu[a]] += 0.5 * nu * (gph[a][0] * n[0] + gph[a][1] * n[1] + gph[a][2] * n[2]);
+        }
+        for (int b = 0; b < 8; ++b) {
+          J[tu[b]] -= pt[b];
+          F[tu[b]] += 0.5 * nu * (gpt[b][0] * n[0] + gpt[b][1] * n[1] + gpt[b][2] * n[2]);
+        }
+        for (int i = 0; i < nu_; ++i) {
+          for (int j = 0; j < nu_; ++j) K[i][j] += w * (-F[j] * J[i] - F[i] * J[j] + tau * J[i] * J[j]);
+          cons[i] += w * (-2.0 * F[i] * J[i]);
+        }
+      });
+      for (int i = 0; i < nu_; ++i) {
+        H.diag_rau[(size_t)u[i]] += cons[i];
+        for (int j = 0; j < nu_; ++j) t.push_back({u[i], u[j], K[i][j]});
+      }
+    }
+  std::stable_sort(t.begin(), t.end(), [](const Trip& a, const Trip& b) { return std::tie(a.r, a.c) < std::tie(b.r, b.c); });
+  // fixed unknowns: every vertex and bubble of the wall, inlet and outlet faces
+  H.fixed.assign((size_t)nv, 0);
+  auto fix_hex = [&](const std::array<int32_t, 3>& r) {
+    H.fixed[(size_t)r[2]] = 1;
+    for (int k = 0; k < 4; ++k) H.fixed[(size_t)m.hexes[(size_t)r[0]][(size_t)kHexFace[r[1]][k]]] = 1;
+  };
+  auto fix_tet = [&](const std::array<int32_t, 3>& r) {
+    H.fixed[(size_t)r[2]] = 1;
+    for (int k = 0; k < 3; ++k) H.fixed[(size_t)m.tets[(size_t)r[0]][(size_t)kTetFace[r[1]][k]]] = 1;
+  };
+  for (const auto& r : m.wall_hex) fix_hex(r);
+  for (const auto& r : m.in_hex) fix_hex(r);
+  for (const auto& r : m.out_hex) fix_hex(r);
+  for (const auto& r : m.in_tet) fix_tet(r);
+  for (const auto& r : m.out_tet) fix_tet(r);
+  H.a_row.assign((size_t)nv + 1, 0);
+  for (size_t a = 0; a < t.size();) {
+    size_t b = a;
+    double v = 0;
+    while (b < t.size() && t[b].r == t[a].r && t[b].c == t[a].c) v += t[b++].v;
+    const int r = t[a].r, c = t[a].c;
+    if (r == c) H.diag_full[(size_t)r] = v;
+    if (!H.fixed[(size_t)r]) {
+      H.a_col.push_back(c);
+      H.a_val.push_back(v);
+      ++H.a_row[(size_t)r + 1];
+    }
+    a = b;
+  }
+  // identity rows for the fixed unknowns, inserted in place
+  {
+    std::vector<int32_t> row((size_t)nv + 1, 0), col;
+    std::vector<double> val;
+    col.reserve(H.a_col.size() + (size_t)nv);
+    val.reserve(H.a_val.size() + (size_t)nv);
+    int32_t k = 0;
+    for (int i = 0; i < nv; ++i) {
+      const int32_t n = H.a_row[(size_t)i + 1];
+      if (H.fixed[(size_t)i]) {
+        col.push_back(i);
+        val.push_back(1.0);
+      } else {
+        for (int32_t q = 0; q < n; ++q) {
+          col.push_back(H.a_col[(size_t)(k + q)]);
+          val.push_back(H.a_val[(size_t)(k + q)]);
+        }
+        k += n;
+      }
+      row[(size_t)i + 1] = (int32_t)col.size();
+    }
+    H.a_row.swap(row);
+    H.a_col.swap(col);
+    H.a_val.swap(val);
+  }
+  // ---- divergence rows: cell volume integrals, then the averaged traces
+  // on interface triangles (hybrid_hxt3a/hxt3a_main.cu:132-246)
+  std::vector<std::map<int32_t, std::array<double, 3>>> rows((size_t)H.np);
+  auto add = [](std::map<int32_t, std::array<double, 3>>& r, int32_t g, double x, double y, double z) {
+    auto& e = r[g];
+    e[0] += x;
+    e[1] += y;
+    e[2] += z;
+  };
+  for (int c = 0; c < m.nhex(); ++c) {
+    double Bv[14][3] = {};
+    for (int ix = 0; ix < 3; ++ix)
+      for (int iy = 0; iy < 3; ++iy)
+        for (int iz = 0; iz < 3; ++iz) {
+          const double x = R.g3x[ix], y = R.g3x[iy], z = R.g3x[iz], w = R.g3w[ix] * R.g3w[iy] * R.g3w[iz];
+          double ph[14], g[14][3], gp[14][3], I[9], det;
+          hex_basis(x, y, z, ph, g);
+          hex_metric(m, c, x, y, z, I, det);
+          phys_grad<14>(g, I, gp);
+          for (int a = 0; a < 14; ++a)
+            for (int d = 0; d < 3; ++d) Bv[a][d] += w * det * gp[a][d];
+        }
+    for (int a = 0; a < 14; ++a) add(rows[(size_t)c], m.hex_dofs[(size_t)c][(size_t)a], Bv[a][0], Bv[a][1], Bv[a][2]);
+  }
+  static const double gl[4][3] = {{-1, -1, -1}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+  for (int c = 0; c < m.ntet(); ++c) {
+    const auto& tg = m.tet_geom[(size_t)c];
+    double Bv[8][3];
+    for (int i = 0; i < 4; ++i)
+      for (int d = 0; d < 3; ++d) {
+        Bv[i][d] = tg[0] * (gl[i][0] * tg[3 + d] + gl[i][1] * tg[6 + d] + gl[i][2] * tg[9 + d]);
+        Bv[4 + i][d] = (-27.0 / 20.0) * Bv[i][d];
+      }
+    for (int a = 0; a < 8; ++a)
+      add(rows[(size_t)(m.nhex() + c)], m.tet_dofs[(size_t)c][(size_t)a], Bv[a][0], Bv[a][1], Bv[a][2]);
+  }
+  for (const auto& p : plans)
+    for (int s = 0; s < 2; ++s) {
+      double TH[14] = {}, TT[8] = {};
+      for_interface_points(m, p, s, [&](double w, const double* ph, const double (*)[3], const double* pt,
+                                        const double (*)[3]) {
+        for (int a = 0; a < 14; ++a) TH[a] += w * ph[a];
+        for (int a = 0; a < 8; ++a) TT[a] += w * pt[a];
+      });
+      auto& rh = rows[(size_t)p.hex_cell];
+      auto& rt = rows[(size_t)(m.nhex() + p.tet_cell[s])];
+      const double* n = p.normal;
+      for (int a = 0; a < 14; ++a) {
+        const double q = 0.5 * TH[a];
+        const int32_t g = m.hex_dofs[(size_t)p.hex_cell][(size_t)a];
+        add(rh, g, -q * n[0], -q * n[1], -q * n[2]);
+        add(rt, g, -q * n[0], -q * n[1], -q * n[2]);
+      }
+      for (int a = 0; a < 8; ++a) {
+        const double q = 0.5 * TT[a];
+        const int32_t g = m.tet_dofs[(size_t)p.tet_cell[s]][(size_t)a];
+        add(rh, g, q * n[0], q * n[1], q * n[2]);
+        add(rt, g, q * n[0], q * n[1], q * n[2]);
+      }
+    }
+  H.b_row.assign((size_t)H.np + 1, 0);
+  for (int i = 0; i < H.np; ++i) {
+    for (const auto& [g, v] : rows[(size_t)i]) {
+      if (std::max({std::abs(v[0]), std::abs(v[1]), std::abs(v[2])}) < 1e-28) continue;
+      H.b_col.push_back(g);
+      H.bx.push_back(v[0]);
+      H.by.push_back(v[1]);
+      H.bz.push_back(v[2]);
+    }
+    H.b_row[(size_t)i + 1] = (int32_t)H.b_col.size();
+  }
+  // transpose, rows ascending in pressure index
+  H.bt_row.assign((size_t)nv + 1, 0);
+  for (int32_t g : H.b_col) ++H.bt_row[(size_t)g + 1];
+  for (int i = 0; i < nv; ++i) H.bt_row[(size_t)i + 1] += H.bt_row[(size_t)i];
+  H.bt_col.resize(H.b_col.size());
+  H.btx.resize(H.b_col.size());
+  H.bty.resize(H.b_col.size());
+  H.btz.resize(H.b_col.size());
+  {
+    std::vector<int32_t> next(H.bt_row.begin(), H.bt_row.end() - 1);
+    for (int i = 0; i < H.np; ++i)
+      for (int32_t k = H.b_row[(size_t)i]; k < H.b_row[(size_t)i + 1]; ++k) {
+        const int32_t q = next[(size_t)H.b_col[(size_t)k]]++;
+        H.bt_col[(size_t)q] = i;
+        H.btx[(size_t)q] = H.bx[(size_t)k];
+        H.bty[(size_t)q] = H.by[(size_t)k];
+        H.btz[(size_t)q] = H.bz[(size_t)k];
+      }
+  }
+  // manufactured pressure: (z_centroid - zmin) / L, shifted to 0 at cell 0
+  double zmin = 1e300, zmax = -1e300;
+  for (int v = 0; v < m.nv(); ++v) {
+    zmin = std::min(zmin, m.xyz[3 * (size_t)v + 2]);
+    zmax = std::max(zmax, m.xyz[3 * (size_t)v + 2]);
+  }
+  const double L = zmax - zmin;
+  H.p_exact.resize((size_t)H.np);
+  for (int c = 0; c < m.nhex(); ++c) H.p_exact[(size_t)c] = (hex_centroid(m, c).z - zmin) / L;
+  for (int c = 0; c < m.ntet(); ++c) H.p_exact[(size_t)(m.nhex() + c)] = (tet_centroid(m, c).z - zmin) / L;
+  const double sh = H.p_exact[0];
+  for (double& q : H.p_exact) q -= sh;
+  return H;
+}
+
+double hybrid_pressure_slope(const HybridMesh& m, const std::vector<double>& p) {
+  long double W = 0, Wz = 0, Wp = 0, Wzz = 0, Wzp = 0;
+  for (int c = 0; c < m.np(); ++c) {
+    const bool h = c < m.nhex();
+    const int lc = h ? c : c - m.nhex();
+    const double z = h ? hex_centroid(m, lc).z : tet_centroid(m, lc).z;
+    const double v = h ? m.hex_geom[(size_t)lc][0] : m.tet_geom[(size_t)lc][0];
+    W += v;
+    Wz += v * z;
+    Wp += v * p[(size_t)c];
+    Wzz += v * z * z;
+    Wzp += v * z * p[(size_t)c];
+  }
+  return (double)((W * Wzp - Wz * Wp) / (W * Wzz - Wz * Wz));
+}
+
+double hybrid_boundary_pressure(const HybridMesh& m, const std::vector<double>& p, bool inlet) {
+  long double num = 0, den = 0;
+  for (const auto& r : inlet ? m.in_hex : m.out_hex) {
+    V3 q[4];
+    for (int k = 0; k < 4; ++k) q[k] = point(m, m.hexes[(size_t)r[0]][(size_t)kHexFace[r[1]][k]]);
+    const double A = tri_area(q[0], q[1], q[2]) + tri_area(q[0], q[2], q[3]);
+    num += (long double)A * p[(size_t)r[0]];
+    den += A;
+  }
+  for (const auto& r : inlet ? m.in_tet : m.out_tet) {
+    V3 q[3];
+    for (int k = 0; k < 3; ++k) q[k] = point(m, m.tets[(size_t)r[0]][(size_t)kTetFace[r[1]][k]]);
+    const double A = tri_area(q[0], q[1], q[2]);
+    num += (long double)A * p[(size_t)(m.nhex() + r[0])];
+    den += A;
+  }
+  return (double)(num / den);
+}
+
+}  // namespace nds

@@ -1,0 +1,79 @@
+// Mixed hexahedron/tetrahedron Stokes operators (the reference's HXT gates,
+// gpu/serial_cuda/hybrid_hxt2, hybrid_hxt3a, hybrid_hxt4a).
+//
+// Velocity: Q1 + six face bubbles ("BF2", 14 unknowns) on hexahedra, P1 +
+// four cubic face bubbles (8 unknowns) on tetrahedra; one P0 pressure per
+// cell.  Hexahedra and tetrahedra meet on quads, each covered by two tet
+// faces; the two sides are coupled weakly by symmetric two-sided Nitsche
+// terms (arithmetic flux average, penalty gamma nu / h with h = 2 V / A).
+// The divergence of a cell uses its volume integral, with the trace on an
+// interface triangle replaced by the average of the two sides' traces.
+//
+// The reference applies these operators matrix-free with atomic scatter;
+// here they are assembled once on the host, row by row in a fixed order
+// (the gate's operators do not change during its solve), so that the device
+// only runs sparse products.
+#pragma once
+#include <array>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace nds {
+
+struct HybridMesh {
+  // nv nhex ntet nhexface ntetface nvel npressure ninterface
+  // nwallhex ninhex nintet nouthex nouttet
+  uint64_t count[13] = {};
+  std::vector<double> xyz;                         // 3 * nv
+  std::vector<std::array<int32_t, 8>> hexes;       // bottom quad, then top quad
+  std::vector<std::array<int32_t, 4>> tets;
+  std::vector<std::array<int32_t, 14>> hex_dofs;   // 8 vertices, 6 face bubbles
+  std::vector<std::array<int32_t, 8>> tet_dofs;    // 4 vertices, 4 face bubbles
+  std::vector<std::array<double, 82>> hex_geom;    // volume, h2, det J at 8 Gauss points, J^-1 (8 x 9)
+  std::vector<std::array<double, 12>> tet_geom;    // volume, h2, det J, J^-1
+  std::vector<std::array<int32_t, 9>> interface;   // hex cell/face/bubble, tet0 cell/face/bubble, tet1 ...
+  std::vector<std::array<int32_t, 3>> wall_hex, in_hex, in_tet, out_hex, out_tet;  // cell, local face, bubble
+  int nv() const { return (int)count[0]; }
+  int nhex() const { return (int)count[1]; }
+  int ntet() const { return (int)count[2]; }
+  int nvel() const { return (int)count[5]; }
+  int np() const { return nhex() + ntet(); }
+};
+
+// binary HXT1 with hex cells (hybrid_hxt1/hxt1_mesh.hpp:19-103)
+HybridMesh read_hxt1_hybrid(const std::string& path);
+
+struct InterfacePlan {
+  int hex_cell, hex_face;
+  int tet_cell[2], tet_face[2];
+  int hex_tri_local[2][3];  // hex local vertex of each corner of the two triangles
+  double normal[3];         // unit, from the hex into the tets
+  double area_quad, area_tri[2];
+  double inv_h_hex, inv_h_tet[2];  // A / (2 V)
+};
+std::vector<InterfacePlan> interface_plans(const HybridMesh& m);
+
+struct HybridStokes {
+  int nvel = 0, np = 0;
+  // velocity operator: rows of fixed unknowns are identity rows
+  std::vector<int32_t> a_row, a_col;
+  std::vector<double> a_val;
+  std::vector<double> diag_full, diag_rau;  // diag(A) and diag(A) without the Nitsche penalty
+  std::vector<uint8_t> fixed;
+  // divergence B (np rows, sorted columns) and its transpose (nvel rows)
+  std::vector<int32_t> b_row, b_col;
+  std::vector<double> bx, by, bz;
+  std::vector<int32_t> bt_row, bt_col;
+  std::vector<double> btx, bty, btz;
+  std::vector<double> p_exact;  // manufactured pressure: axial linear, p_exact[0] = 0
+};
+HybridStokes build_hybrid_stokes(const HybridMesh& m, const std::vector<InterfacePlan>& plans, double nu,
+                                 double gamma);
+
+// least-squares axial pressure slope and area-weighted inlet/outlet pressure
+// of a P0 field (hybrid_hxt4a/hxt4a_main.cu:339-357)
+double hybrid_pressure_slope(const HybridMesh& m, const std::vector<double>& p);
+double hybrid_boundary_pressure(const HybridMesh& m, const std::vector<double>& p, bool inlet);
+
+}  // namespace nds

@@ -434,6 +434,103 @@ def write_hxt1(m: TetMesh, path: str | os.PathLike) -> Path:
     return p
 
 
+# ---------------------------------------------------------------------------
+# hybrid hex/tet pipes (the mixed meshes of the reference's HXT solvers)
+# ---------------------------------------------------------------------------
+HXT1_HEX_FACE = ((0, 1, 2, 3), (4, 5, 6, 7), (0, 1, 5, 4), (1, 2, 6, 5), (2, 3, 7, 6), (3, 0, 4, 7))
+
+
+@dataclass
+class HybridMesh:
+    """Mixed mesh in the array form the reference's HXT1 preparer reads
+    (gpu/serial_cuda/hybrid_hxt1/prepare_hxt1.py: HXT0 arrays)."""
+    points: np.ndarray                # (np, 3)
+    hexes: np.ndarray                 # (nh, 8): bottom quad counter-clockwise, then the top quad
+    tets: np.ndarray                  # (nt, 4) positively oriented
+    interface_quads: np.ndarray       # (ni, 4) hex faces shared with the tet region
+    interface_triangles: np.ndarray   # (ni, 2, 3) the two tet faces covering each
+    wall_quads: np.ndarray
+    inlet_hex_quads: np.ndarray
+    inlet_tet_triangles: np.ndarray
+    outlet_hex_quads: np.ndarray
+    outlet_tet_triangles: np.ndarray
+    meta: dict = field(default_factory=dict)
+
+    def arrays(self) -> dict:
+        return {k: getattr(self, k) for k in ("points", "hexes", "tets", "interface_quads", "interface_triangles",
+                                              "wall_quads", "inlet_hex_quads", "inlet_tet_triangles",
+                                              "outlet_hex_quads", "outlet_tet_triangles")}
+
+
+def hybrid_pipe(nr: int = 4, ntheta: int = 16, nz: int = 40, radius: float = 0.5, length: float = 10.0) -> HybridMesh:
+    """Straight pipe with the cross-section of ``pipe_mesh``: its ``nr`` rings
+    of quads are extruded into hexahedra (they carry the wall), its square
+    core into prisms split into tetrahedra by the minimum-vertex rule.  The
+    hex/tet interface is the core boundary: each of its quads is a hex face
+    covered by two tet faces.  No jitter, so every face is planar."""
+    xy, quads, _on_wall, _ = _cross_section(nr, ntheta, radius)
+    k = ntheta // 4
+    core, ring = quads[: k * k], quads[k * k:]
+    # hex bottoms counter-clockwise seen from +z (positive Jacobian)
+    e1, e2 = xy[ring[:, 1]] - xy[ring[:, 0]], xy[ring[:, 3]] - xy[ring[:, 0]]
+    cw = e1[:, 0] * e2[:, 1] - e1[:, 1] * e2[:, 0] < 0
+    ring = np.where(cw[:, None], ring[:, [0, 3, 2, 1]], ring)
+    n2, nl = len(xy), nz + 1
+    z = np.linspace(0.0, length, nl)
+    pts = np.zeros((n2 * nl, 3))
+    pts[:, 0] = np.tile(xy[:, 0], nl)
+    pts[:, 1] = np.tile(xy[:, 1], nl)
+    pts[:, 2] = np.repeat(z, n2)
+    hexes = np.concatenate([np.concatenate([ring + s * n2, ring + (s + 1) * n2], axis=1) for s in range(nz)])
+    tri = _split_quads(xy, core)
+    tets = _orient(pts, np.concatenate([_prism_tets(tri + s * n2, tri + (s + 1) * n2) for s in range(nz)]))
+    faces = {}
+    for c, t in enumerate(tets):
+        for f in HXT1_TET_FACE:
+            tri3 = tuple(int(t[i]) for i in f)
+            faces[tuple(sorted(tri3))] = tri3
+    # interface: the inner side faces of the first ring's hexes
+    # inner edge of a first-ring quad: its two vertices on the core boundary
+    core_nodes = set(int(v) for v in core.reshape(-1))
+    ring0 = ring[:ntheta]
+    iq, it = [], []
+    for s in range(nz):
+        for q in ring0:
+            a, b = [int(v) + s * n2 for v in q if int(v) in core_nodes]
+            quad = (a, b, b + n2, a + n2)
+            for t1, t2 in (((quad[0], quad[1], quad[2]), (quad[0], quad[2], quad[3])),
+                           ((quad[0], quad[1], quad[3]), (quad[1], quad[2], quad[3]))):
+                k1, k2 = tuple(sorted(t1)), tuple(sorted(t2))
+                if k1 in faces and k2 in faces:
+                    iq.append(quad)
+                    it.append((faces[k1], faces[k2]))
+                    break
+            else:
+                raise RuntimeError("interface quad not covered by two tet faces")
+    wall_nodes = set(int(v) for v in ring[-ntheta:].reshape(-1)) - set(int(v) for v in ring[-2 * ntheta:-ntheta].reshape(-1)) \
+        if nr > 1 else set(int(v) for v in ring.reshape(-1)) - core_nodes
+    wall = []
+    for s in range(nz):
+        for q in ring[-ntheta:]:
+            a, b = [int(v) + s * n2 for v in q if int(v) in wall_nodes]
+            wall.append((a, b, b + n2, a + n2))
+    as32 = lambda a, w: np.asarray(a, dtype=np.int32).reshape(-1, *w)
+    return HybridMesh(
+        points=pts, hexes=as32(hexes, (8,)), tets=as32(tets, (4,)),
+        interface_quads=as32(iq, (4,)), interface_triangles=as32(it, (2, 3)), wall_quads=as32(wall, (4,)),
+        inlet_hex_quads=as32(ring, (4,)), inlet_tet_triangles=as32(tri, (3,)),
+        outlet_hex_quads=as32(ring + nz * n2, (4,)), outlet_tet_triangles=as32(tri + nz * n2, (3,)),
+        meta=dict(nr=nr, ntheta=ntheta, nz=nz, radius=radius, length=length))
+
+
+def write_hxt0(m: HybridMesh, path: str | os.PathLike) -> Path:
+    """The HXT0 ``.npz`` the reference's HXT1 preparer takes as input."""
+    p = Path(path)
+    p.parent.mkdir(parents=True, exist_ok=True)
+    np.savez(p, **m.arrays())
+    return p
+
+
 # named workloads: (nr, ntheta, nz, radius, length, jitter, seed)
 CONFIGS = {
     # ~40k-tet pipe, Re=20 (8 rings x 24 sectors x 35 slabs)

@@ -1,0 +1,77 @@
+"""Mixed hexahedron/tetrahedron Stokes gate (the reference's HXT4A,
+gpu/serial_cuda/hybrid_hxt4a/hxt4a_main.cu) against the reference binary's
+own run on the same HXT1 mesh (tests/golden/hxt4a_hybrid_r2.log, made by
+make_hxt4a_golden.py from tests/golden/hxt1_hybrid_r2.bin, itself the
+reference preparer's output for the seeded 2-ring hybrid pipe).
+
+CPU: the host-assembled operators (hex Q1+BF2 diffusion, tet P1+BF3
+diffusion, Nitsche interface, divergence with averaged interface traces,
+rAU) reproduce the reference's printed operator-audit norms to 1e-12.
+GPU: the gate executable prints the same audit, the same relCont history
+(1e-9 relative; the reference sums with atomics, so not bitwise), CG counts
+within one iteration, the same outer iteration count and the same result
+line (errors against p* and the Hagen-Poiseuille-like checks 1e-8).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import re
+import subprocess
+
+import pytest
+
+from conftest import GOLDEN, ROOT
+
+MESH = GOLDEN / "hxt1_hybrid_r2.bin"
+LOG = GOLDEN / "hxt4a_hybrid_r2.log"
+
+
+def _kv(line):
+    return dict(re.findall(r"(\w+)=(\[[^\]]*\]|\S+)", line))
+
+
+def _parse(text):
+    lines = text.splitlines()
+    audit = next(_kv(l) for l in lines if l.startswith("NODALS_HXT4A_OPERATOR_AUDIT"))
+    simple = {int(_kv(l)["it"]): _kv(l) for l in lines if l.startswith("NODALS_HXT4A_SIMPLE")}
+    result = next(_kv(l) for l in lines if l.startswith("NODALS_HXT4A_RESULT"))
+    return audit, simple, result
+
+
+def _close(a, b, tol):
+    a, b = float(a), float(b)
+    return abs(a - b) <= tol * max(abs(b), 1e-300)
+
+
+def test_host_operators_match_reference_audit(native):
+    audit, _, _ = _parse(LOG.read_text())
+    n = (C.c_double * 3)()
+    rc = native.lib().nds_hybrid_operator_audit(str(MESH).encode(), C.c_double(1.0), C.c_double(50.0), C.c_double(24.0), n)
+    assert rc == 0, native.lib().nds_last_error()
+    for got, key in zip(n, ("Anorm", "Bnorm", "Snorm")):
+        assert _close(got, audit[key], 1e-12), (key, got, audit[key])
+
+
+@pytest.mark.gpu
+def test_gate_matches_reference_run():
+    r = subprocess.run([str(ROOT / "nodals_b200" / "_lib" / "nodals_hxt4a_fp64"), "--mesh", str(MESH)],
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert "HXT4A_PRECISION_STATUS=PASS" in r.stdout
+    ga, gs, gr = _parse(r.stdout)
+    wa, ws, wr = _parse(LOG.read_text())
+    for k in ("Anorm", "Bnorm", "Snorm"):
+        assert _close(ga[k], wa[k], 1e-12), (k, ga[k], wa[k])
+    assert sorted(gs) == sorted(ws)
+    for it, w in ws.items():
+        g = gs[it]
+        assert _close(g["relCont"], w["relCont"], 1e-9), (it, g["relCont"], w["relCont"])
+        assert _close(g["velocityNorm"], w["velocityNorm"], 1e-9), (it, g["velocityNorm"], w["velocityNorm"])
+        gm, wm = eval(g["mCG"]), eval(w["mCG"])
+        assert all(abs(x - y) <= 1 for x, y in zip(gm, wm)) and abs(int(g["pCG"]) - int(w["pCG"])) <= 1, (it, g, w)
+    assert gr["outer"] == wr["outer"]
+    for k, tol in (("finalRelCont", 1e-9), ("pressureRelL2", 1e-8), ("slope", 1e-10), ("delta", 1e-10),
+                   ("velocityRel", 1e-8)):
+        assert _close(gr[k], wr[k], tol), (k, gr[k], wr[k])
+    assert abs(float(gr["avgMomentumCG"]) - float(wr["avgMomentumCG"])) < 0.01
+    assert abs(float(gr["avgPressureCG"]) - float(wr["avgPressureCG"])) < 0.01
