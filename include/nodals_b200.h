@@ -249,6 +249,39 @@ int nds_hybrid_stokes_gate(const char* hxt1_path, double nu, double gamma, doubl
  * NODALS_HXT4A_OPERATOR_AUDIT (hxt4a_main.cu:429-437). */
 int nds_hybrid_operator_audit(const char* hxt1_path, double nu, double gamma, double rau_scale, double norms[3]);
 
+/* ---- mixed-mesh pipe SIMPLE: replaces the reference's HXT4B executable
+ *      (gpu/serial_cuda/hybrid_hxt4b/hxt4b_main.cu:211-268).
+ * Steady Navier-Stokes in a straight pipe of 10 diameters on a binary HXT1
+ * mesh with hex and tet cells: parabolic inlet, no-slip wall (hex faces),
+ * natural outlet, nu = bulk D / Re.  Per iteration the lagged central
+ * advective convection is assembled into the velocity CSR, the diagonal is
+ * relaxed by alpha_u, rAU = rau_scale alpha_u / (penalty-free diagonal +
+ * convection diagonal), each velocity component gets the multicolour
+ * Gauss-Seidel work momentum_work (0 fgs1, 1 altgs1, 2 sgs1), and
+ * B diag(rAU) B^T dp = B u is solved by Jacobi PCG to max(p_atol, p_rtol
+ * ||r0||) within p_max iterations, p -= alpha_p dp, until relCont <=
+ * simple_tol.  mom_rtol / mom_atol are accepted and unused, as in the
+ * reference (fixed-work sweeps).  verbose = 1 prints the reference's
+ * NODALS_HXT4B_* lines. */
+typedef struct nds_hybrid_flow_options {
+  double re, bulk, gamma, alpha_u, alpha_p, rau_scale, simple_tol;
+  int max_outer, momentum_work;
+  double mom_omega, mom_rtol, mom_atol, p_rtol, p_atol;
+  int p_max;
+} nds_hybrid_flow_options;
+typedef struct nds_hybrid_flow_report {
+  int outer_its, converged, pass;
+  int n_hex, n_tet, n_velocity;
+  double final_rel_cont, avg_pressure_cg;
+  double slope, slope_exact, p_in, p_out, drop, drop_exact;   /* pressure against Hagen-Poiseuille */
+  double profile_rel_l2, transverse_rel_l2;                   /* vertex velocity against the profile */
+  double conv_norm, velocity_norm;
+  double loop_ms;
+} nds_hybrid_flow_report;
+void nds_hybrid_flow_defaults(nds_hybrid_flow_options* o);   /* the reference binary's defaults */
+int nds_hybrid_flow(const char* hxt1_path, const nds_hybrid_flow_options* o, int device, int verbose,
+                    nds_hybrid_flow_report* out);
+
 #ifdef __cplusplus
 }
 #endif

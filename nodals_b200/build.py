@@ -80,10 +80,10 @@ def build(verbose: bool = False, jobs: int | None = None) -> Path:
             _run([CXX, *CXXFLAGS, "-I", str(CSRC), "-o", str(exe), str(cli), "-L", str(LIB), "-lnodals_b200",
                   "-Wl,-rpath,$ORIGIN"])
             shutil.copy2(exe, LIB / "nodals_gpu_h8_fp32")
-    gate = CSRC / "cli" / "nodals_hxt4a.cpp"
-    if gate.exists():
-        exe = LIB / "nodals_hxt4a_fp64"
-        if not exe.exists() or exe.stat().st_mtime < max(gate.stat().st_mtime, so.stat().st_mtime, newest):
+    for name in ("nodals_hxt4a", "nodals_hxt4b"):
+        gate = CSRC / "cli" / f"{name}.cpp"
+        exe = LIB / f"{name}_fp64"
+        if gate.exists() and (not exe.exists() or exe.stat().st_mtime < max(gate.stat().st_mtime, so.stat().st_mtime, newest)):
             _run([CXX, *CXXFLAGS, "-I", str(CSRC), "-o", str(exe), str(gate), "-L", str(LIB), "-lnodals_b200",
                   "-Wl,-rpath,$ORIGIN"])
     return so

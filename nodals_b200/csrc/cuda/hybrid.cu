@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "../../../include/nodals_b200.h"
+#include "../host/fem.hpp"
 #include "../host/hybrid.hpp"
 #include "common.cuh"
 
@@ -28,6 +29,15 @@ void set_error(const std::string& m);
 namespace hy {
 
 constexpr int kTPB = 256;
+
+// 3-point Gauss rule on [-1,1]: nodes then weights
+struct Rules3 {
+  double v[6];
+};
+inline Rules3 rules3() {
+  const double a = std::sqrt(0.6);
+  return Rules3{{-a, 0.0, a, 5.0 / 9.0, 8.0 / 9.0, 5.0 / 9.0}};
+}
 
 template <class T>
 struct Buf {
@@ -455,6 +465,407 @@ void run_gate(const char* path, double nu, double gamma, double rau_scale, doubl
   if (out) *out = R;
 }
 
+// ===================================================================
+// Mixed-mesh pipe SIMPLE (the reference's HXT4B,
+// gpu/serial_cuda/hybrid_hxt4b/hxt4b_main.cu:211-268)
+// ===================================================================
+__constant__ double c_g3[6];                   // 3-point Gauss nodes, then weights
+__constant__ double c_tet_conv[8 * 8 * 8 * 3];  // T[a][m][b][j] = int phi_a phi_m dphi_b/dxi_j
+__constant__ int c_hex_sign[8][3] = {{-1, -1, -1}, {1, -1, -1}, {1, 1, -1}, {-1, 1, -1},
+                                     {-1, -1, 1},  {1, -1, 1},  {1, 1, 1},  {-1, 1, 1}};
+
+// Q1 + BF2 basis (values, reference gradients) at (x, y, z) in [-1,1]^3
+__device__ void hex_basis_dev(double x, double y, double z, double phi[14], double g[14][3]) {
+  for (int a = 0; a < 8; ++a) {
+    const double sx = c_hex_sign[a][0], sy = c_hex_sign[a][1], sz = c_hex_sign[a][2];
+    const double ax = 1.0 + sx * x, ay = 1.0 + sy * y, az = 1.0 + sz * z;
+    phi[a] = 0.125 * ax * ay * az;
+    g[a][0] = 0.125 * sx * ay * az;
+    g[a][1] = 0.125 * sy * ax * az;
+    g[a][2] = 0.125 * sz * ax * ay;
+  }
+  const double c[3] = {x, y, z}, b[3] = {1 - x * x, 1 - y * y, 1 - z * z}, d[3] = {-2 * x, -2 * y, -2 * z};
+  const int nrm[6] = {2, 2, 1, 0, 1, 0};
+  const double sgn[6] = {-1, 1, -1, 1, 1, -1};
+  for (int f = 0; f < 6; ++f) {
+    const int n = nrm[f], t1 = n == 0 ? 1 : 0, t2 = n == 2 ? 1 : 2;
+    const double s = 0.5 * (1.0 + sgn[f] * c[n]);
+    phi[8 + f] = s * b[t1] * b[t2];
+    g[8 + f][n] = 0.5 * sgn[f] * b[t1] * b[t2];
+    g[8 + f][t1] = s * d[t1] * b[t2];
+    g[8 + f][t2] = s * b[t1] * d[t2];
+  }
+}
+
+// Convection block of each hex at the lagged velocity:
+// C_ab = sum_q det w phi_a (u_q . grad phi_b), u_q = sum_m u_m phi_m(q), 27 points.
+// One block per hex; one thread per point builds that point's basis,
+// metric and velocity in shared memory, then the 196 entries.
+__global__ void __launch_bounds__(kTPB) hex_conv_local(int nh, const double* __restrict__ xyz,
+                                                        const int32_t* __restrict__ hexes,
+                                                        const int32_t* __restrict__ dofs, const double* __restrict__ u0,
+                                                        const double* __restrict__ u1, const double* __restrict__ u2,
+                                                        double* __restrict__ local, int* __restrict__ bad) {
+  __shared__ double sphi[27][14], sgp[27][14][3], sdw[27], su[27][3], sul[3][14];
+  const int c = blockIdx.x, t = threadIdx.x;
+  if (c >= nh) return;
+  if (t < 14) {
+    const int g = dofs[14 * (size_t)c + t];
+    sul[0][t] = u0[g];
+    sul[1][t] = u1[g];
+    sul[2][t] = u2[g];
+  }
+  __syncthreads();
+  if (t < 27) {
+    const int ix = t / 9, iy = (t / 3) % 3, iz = t % 3;
+    const double x = c_g3[ix], y = c_g3[iy], z = c_g3[iz], w = c_g3[3 + ix] * c_g3[3 + iy] * c_g3[3 + iz];
+    double ph[14], g[14][3];
+    hex_basis_dev(x, y, z, ph, g);
+    double J[9] = {};
+    for (int a = 0; a < 8; ++a) {
+      const double* p = xyz + 3 * (size_t)hexes[8 * (size_t)c + a];
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) J[3 * i + j] += p[i] * g[a][j];
+    }
+    const double det = J[0] * (J[4] * J[8] - J[5] * J[7]) - J[1] * (J[3] * J[8] - J[5] * J[6]) + J[2] * (J[3] * J[7] - J[4] * J[6]);
+    if (!(det > 0)) atomicAdd(bad, 1);
+    const double q = 1.0 / det;
+    const double I[9] = {(J[4] * J[8] - J[5] * J[7]) * q, (J[2] * J[7] - J[1] * J[8]) * q, (J[1] * J[5] - J[2] * J[4]) * q,
+                         (J[5] * J[6] - J[3] * J[8]) * q, (J[0] * J[8] - J[2] * J[6]) * q, (J[2] * J[3] - J[0] * J[5]) * q,
+                         (J[3] * J[7] - J[4] * J[6]) * q, (J[1] * J[6] - J[0] * J[7]) * q, (J[0] * J[4] - J[1] * J[3]) * q};
+    double uq[3] = {0, 0, 0};
+    for (int a = 0; a < 14; ++a) {
+      sphi[t][a] = ph[a];
+      for (int d = 0; d < 3; ++d) sgp[t][a][d] = g[a][0] * I[d] + g[a][1] * I[3 + d] + g[a][2] * I[6 + d];
+      for (int d = 0; d < 3; ++d) uq[d] += sul[d][a] * ph[a];
+    }
+    sdw[t] = det * w;
+    for (int d = 0; d < 3; ++d) su[t][d] = uq[d];
+  }
+  __syncthreads();
+  for (int e = t; e < 196; e += blockDim.x) {
+    const int a = e / 14, b = e % 14;
+    double s = 0;
+    for (int q = 0; q < 27; ++q)
+      s += sdw[q] * sphi[q][a] * (su[q][0] * sgp[q][b][0] + su[q][1] * sgp[q][b][1] + su[q][2] * sgp[q][b][2]);
+    local[196 * (size_t)c + e] = s;
+  }
+}
+// Convection block of each tet: C_ab = det sum_m sum_j (J^-1 u_m)_j T[a][m][b][j]
+__global__ void tet_conv_local(int nt, const double* __restrict__ geom, const int32_t* __restrict__ dofs,
+                               const double* __restrict__ u0, const double* __restrict__ u1,
+                               const double* __restrict__ u2, double* __restrict__ local) {
+  __shared__ double ur[8][3];
+  const int c = blockIdx.x, t = threadIdx.x;
+  if (c >= nt) return;
+  const double* G = geom + 12 * (size_t)c;
+  if (t < 8) {
+    const int g = dofs[8 * (size_t)c + t];
+    const double u[3] = {u0[g], u1[g], u2[g]};
+    for (int j = 0; j < 3; ++j) ur[t][j] = u[0] * G[3 + 3 * j] + u[1] * G[4 + 3 * j] + u[2] * G[5 + 3 * j];
+  }
+  __syncthreads();
+  if (t < 64) {
+    const int a = t / 8, b = t % 8;
+    double q = 0;
+    for (int m = 0; m < 8; ++m)
+      for (int j = 0; j < 3; ++j) q += ur[m][j] * c_tet_conv[((a * 8 + m) * 8 + b) * 3 + j];
+    local[64 * (size_t)c + t] = q * G[2];
+  }
+}
+// conv[k] = sum of its cells' local values, in cell order
+__global__ void conv_gather(int nnz, const int32_t* __restrict__ off, const int32_t* __restrict__ src,
+                            const double* __restrict__ local, double* __restrict__ conv) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nnz) return;
+  double s = 0;
+  for (int q = off[k]; q < off[k + 1]; ++q) s += local[src[q]];
+  conv[k] = s;
+}
+// val = base + conv; relaxed diagonal val_ii / alpha_u; rAU = scale alpha_u / (penalty-free diag + conv_ii)
+__global__ void flow_rows(int n, const int32_t* __restrict__ row, const int32_t* __restrict__ dpos,
+                          const uint8_t* __restrict__ fixed, const double* __restrict__ base,
+                          const double* __restrict__ conv, const double* __restrict__ dr, double alpha_u,
+                          double rau_scale, double* __restrict__ val, double* __restrict__ dorig,
+                          double* __restrict__ rau, int* __restrict__ bad) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (int k = row[i]; k < row[i + 1]; ++k) val[k] = base[k] + conv[k];
+  const int d = dpos[i];
+  const double orig = val[d];
+  dorig[i] = orig;
+  if (fixed[i]) {
+    rau[i] = 0.0;
+    return;
+  }
+  const double den = dr[i] + conv[d];
+  if (!(orig > 0) || !(den > 0) || !isfinite(orig) || !isfinite(den)) {
+    atomicAdd(bad, 1);
+    rau[i] = 0.0;
+    return;
+  }
+  val[d] = orig / alpha_u;
+  rau[i] = rau_scale * alpha_u / den;
+}
+// rhs = fixed ? 0 : B^T p + (1 - alpha_u) / alpha_u diag_i u_i
+__global__ void flow_rhs(int n, const uint8_t* fixed, const double* bt, const double* u, const double* dorig,
+                         double alpha_u, double* rhs) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) rhs[i] = fixed[i] ? 0.0 : bt[i] + ((1.0 - alpha_u) / alpha_u) * dorig[i] * u[i];
+}
+// Gauss-Seidel on the rows of one colour, a warp per row:
+// x_i += omega ((rhs_i - sum_{j != i} a_ij x_j) / a_ii - x_i)
+__global__ void gs_colour(int count, const int32_t* __restrict__ rows, const int32_t* __restrict__ row,
+                          const int32_t* __restrict__ col, const double* __restrict__ val,
+                          const int32_t* __restrict__ dpos, const double* __restrict__ rhs, double* x, double omega) {
+  const int q = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (q >= count) return;
+  const int i = rows[q];
+  double off = 0;
+  for (int k = row[i] + lane; k < row[i + 1]; k += 32)
+    if (col[k] != i) off += val[k] * x[col[k]];
+  off = warp_sum(off);
+  if (lane == 0) {
+    const double gs = (rhs[i] - off) / val[dpos[i]];
+    x[i] = x[i] + omega * (gs - x[i]);
+  }
+}
+__global__ void residual_free(int n, const uint8_t* fixed, const double* b, const double* Ax, double* r) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) r[i] = fixed[i] ? 0.0 : b[i] - Ax[i];
+}
+__global__ void p_update_minus(int n, int pin, double a, const double* dp, double* p) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) p[i] = (i == pin) ? 0.0 : p[i] - a * dp[i];
+}
+__global__ void twice(size_t n, const double* a, double* b) {
+  const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i < n) b[i] = a[i] + a[i];
+}
+
+// Jacobi PCG to max(atol, rtol ||r0||) from the guess in x, pin kept zero
+// (hxt4b_main.cu:197-201)
+template <class Op>
+CgResult pcg_prod(Op& A, const double* rhs, double* x, const double* invdiag, double rtol, double atol, int maxit,
+                  CgWork& W, int pin) {
+  const int n = W.n;
+  A.apply(x, W.q.p);
+  residual<<<grid(n), kTPB>>>(n, rhs, W.q.p, W.r.p);
+  NDS_LAUNCH();
+  set_at<<<1, 1>>>(pin, 0.0, W.r.p);
+  const double r0 = W.red.norm(W.r.p);
+  if (r0 == 0) return {0, 0, true};
+  const double target = std::max(atol, rtol * r0);
+  mul<<<grid(n), kTPB>>>(n, invdiag, W.r.p, W.z.p);
+  NDS_LAUNCH();
+  NDS_CUDA(cudaMemcpy(W.p.p, W.z.p, n * sizeof(double), cudaMemcpyDeviceToDevice));
+  double rho = W.red.dot(W.r.p, W.z.p);
+  CgResult R;
+  for (int k = 0; k < maxit; ++k) {
+    A.apply(W.p.p, W.q.p);
+    const double pq = W.red.dot(W.p.p, W.q.p);
+    if (!(pq > 0)) throw std::runtime_error("mixed-mesh pressure PCG pAp nonpositive");
+    axpy2<<<grid(n), kTPB>>>(n, rho / pq, W.p.p, W.q.p, x, W.r.p);
+    NDS_LAUNCH();
+    set_at<<<1, 1>>>(pin, 0.0, x);
+    set_at<<<1, 1>>>(pin, 0.0, W.r.p);
+    const double rn = W.red.norm(W.r.p);
+    R.its = k + 1;
+    R.rel = rn / r0;
+    if (rn <= target) {
+      R.ok = true;
+      break;
+    }
+    mul<<<grid(n), kTPB>>>(n, invdiag, W.r.p, W.z.p);
+    NDS_LAUNCH();
+    const double nr = W.red.dot(W.r.p, W.z.p);
+    xpby<<<grid(n), kTPB>>>(n, nr / rho, W.z.p, W.p.p);
+    NDS_LAUNCH();
+    set_at<<<1, 1>>>(pin, 0.0, W.p.p);
+    rho = nr;
+  }
+  return R;
+}
+
+void run_flow(const char* path, const nds_hybrid_flow_options& o, int verbose, nds_hybrid_flow_report* out) {
+  const HybridMesh M = read_hxt1_hybrid(path);
+  const auto P = interface_plans(M);
+  HybridFlow F = build_hybrid_flow(M, P, o.re, o.bulk, o.gamma);
+  HybridStokes Hb;
+  build_hybrid_divergence(M, P, Hb);
+  const int nv = F.nvel, np = F.np, nh = F.nhex, nt = F.ntet, nnz = (int)F.col.size(), pin = F.pin;
+  {
+    const Rules3 r = rules3();
+    NDS_CUDA(cudaMemcpyToSymbol(c_g3, r.v, sizeof(r.v)));
+    const auto& T = ref_tensors().T;
+    NDS_CUDA(cudaMemcpyToSymbol(c_tet_conv, &T[0][0][0][0], sizeof(double) * 8 * 8 * 8 * 3));
+  }
+  std::vector<int32_t> hexes(8 * (size_t)nh), hdofs(14 * (size_t)nh), tdofs(8 * (size_t)nt);
+  std::vector<double> tgeom(12 * (size_t)nt);
+  for (int c = 0; c < nh; ++c) {
+    for (int a = 0; a < 8; ++a) hexes[8 * (size_t)c + a] = M.hexes[(size_t)c][(size_t)a];
+    for (int a = 0; a < 14; ++a) hdofs[14 * (size_t)c + a] = M.hex_dofs[(size_t)c][(size_t)a];
+  }
+  for (int c = 0; c < nt; ++c) {
+    for (int a = 0; a < 8; ++a) tdofs[8 * (size_t)c + a] = M.tet_dofs[(size_t)c][(size_t)a];
+    for (int a = 0; a < 12; ++a) tgeom[12 * (size_t)c + a] = M.tet_geom[(size_t)c][(size_t)a];
+  }
+  Buf<double> d_xyz(M.xyz), d_tgeom(tgeom), d_base(F.base), d_dr(F.diag_r_base), d_local((size_t)nh * 196 + (size_t)nt * 64);
+  Buf<int32_t> d_hexes(hexes), d_hdofs(hdofs), d_tdofs(tdofs), d_row(F.row), d_col(F.col), d_dpos(F.diag_pos),
+      d_soff(F.src_off), d_src(F.src), d_crows(F.colour_rows);
+  Buf<uint8_t> d_fixed(F.fixed);
+  Buf<double> u0(F.u0), u1(F.u1), u2(F.u2), conv((size_t)nnz), val((size_t)nnz), dorig((size_t)nv), rau((size_t)nv),
+      isd((size_t)np), p((size_t)np), dp((size_t)np), cont((size_t)np), bt0((size_t)nv), bt1((size_t)nv),
+      bt2((size_t)nv), r0((size_t)nv), r1((size_t)nv), r2((size_t)nv), tmp((size_t)nv), res((size_t)nv);
+  Buf<int> d_bad((size_t)1);
+  Div B(Hb);
+  Schur S(B, rau.p, pin);
+  Reducer pred(np), ured(nv);
+  CgWork WP(np);
+  auto apply_val = [&](const double* x, double* y) {
+    csr_mv<<<grid((long long)nv * 32), kTPB>>>(nv, d_row.p, d_col.p, val.p, x, y);
+    NDS_LAUNCH();
+  };
+  const double dpdz_exact = -32 * F.nu * o.bulk / (F.diameter * F.diameter), drop_exact = -dpdz_exact * F.length;
+  const int ncol = (int)F.colour_off.size() - 1;
+  const char* work = o.momentum_work == 0 ? "fgs1" : o.momentum_work == 1 ? "altgs1" : "sgs1";
+  if (verbose) {
+    std::printf("NODALS_HXT4B_CONFIG precision=fp64 geometry=fp64 reductions=fp64 cellsHex=%d cellsTet=%d velocityDofs=%d "
+                "pressureDofs=%d csrNnz=%d colors=%d maxColor=%d Re=%.12g bulk=%.12g nu=%.12e D=%.12e L=%.12e gamma=%.6g "
+                "convection=CENTRAL_ADVECTIVE_LAGGED interfaceConvection=VOLUME_ONLY_TANGENTIAL_RE20_GATE momentumWork=%s "
+                "momOmega=%.6g momRtol=%.3e momAtol=%.3e fixedWorkIgnoresMomTolerances=1 pressureSolver=PCG_JACOBI "
+                "momentumSign=A_u_MINUS_BT_p pRtol=%.3e pAtol=%.3e pMax=%d alphaU=%.6g alphaP=%.6g rauScale=%.6g "
+                "rauPenaltyIncluded=0 simpleTol=%.3e status=PASS\n",
+                nh, nt, nv, np, nnz, ncol, F.max_colour, o.re, o.bulk, F.nu, F.diameter, F.length, o.gamma, work,
+                o.mom_omega, o.mom_rtol, o.mom_atol, o.p_rtol, o.p_atol, o.p_max, o.alpha_u, o.alpha_p, o.rau_scale,
+                o.simple_tol);
+    std::printf("NODALS_HXT4B_HAGEN_POISEUILLE expectedDpDz=%.12e expectedDropPinMinusPout=%.12e inlet=STRONG_PARABOLIC "
+                "wall=STRONG_NOSLIP outlet=NATURAL_TRACTION pressureGaugePin=%d status=PASS\n",
+                dpdz_exact, drop_exact, pin);
+  }
+  auto sweep = [&](double* x, const double* rhs, bool forward) {
+    for (int q = 0; q < ncol; ++q) {
+      const int c = forward ? q : ncol - 1 - q;
+      const int b = F.colour_off[(size_t)c], n = F.colour_off[(size_t)c + 1] - b;
+      gs_colour<<<grid((long long)n * 32), kTPB>>>(n, d_crows.p + b, d_row.p, d_col.p, val.p, d_dpos.p, rhs, x, o.mom_omega);
+      NDS_LAUNCH();
+    }
+  };
+  auto momentum_work = [&](int it, double* x, const double* rhs) {
+    if (o.momentum_work == 0) sweep(x, rhs, true);
+    else if (o.momentum_work == 1) sweep(x, rhs, (it & 1) != 0);
+    else {
+      sweep(x, rhs, true);
+      sweep(x, rhs, false);
+    }
+  };
+  const auto t0 = std::chrono::steady_clock::now();
+  double c0 = -1, rel = 1;
+  bool conv_ok = false;
+  int outer = 0;
+  long long pits = 0;
+  for (int it = 1; it <= o.max_outer; ++it) {
+    hex_conv_local<<<std::max(nh, 1), kTPB>>>(nh, d_xyz.p, d_hexes.p, d_hdofs.p, u0.p, u1.p, u2.p, d_local.p, d_bad.p);
+    NDS_LAUNCH();
+    if (nt) {
+      tet_conv_local<<<nt, 64>>>(nt, d_tgeom.p, d_tdofs.p, u0.p, u1.p, u2.p, d_local.p + 196 * (size_t)nh);
+      NDS_LAUNCH();
+    }
+    conv_gather<<<grid(nnz), kTPB>>>(nnz, d_soff.p, d_src.p, d_local.p, conv.p);
+    NDS_LAUNCH();
+    flow_rows<<<grid(nv), kTPB>>>(nv, d_row.p, d_dpos.p, d_fixed.p, d_base.p, conv.p, d_dr.p, o.alpha_u, o.rau_scale,
+                                  val.p, dorig.p, rau.p, d_bad.p);
+    NDS_LAUNCH();
+    int bad = 0;
+    NDS_CUDA(cudaMemcpy(&bad, d_bad.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (bad) throw std::runtime_error("mixed-mesh SIMPLE: nonpositive momentum diagonal or hex Jacobian");
+    schur_diag_inv<<<grid(np), kTPB>>>(np, B.row.p, B.col.p, B.bx.p, B.by.p, B.bz.p, rau.p, pin, isd.p);
+    NDS_LAUNCH();
+    B.BT(p.p, bt0.p, bt1.p, bt2.p);
+    flow_rhs<<<grid(nv), kTPB>>>(nv, d_fixed.p, bt0.p, u0.p, dorig.p, o.alpha_u, r0.p);
+    flow_rhs<<<grid(nv), kTPB>>>(nv, d_fixed.p, bt1.p, u1.p, dorig.p, o.alpha_u, r1.p);
+    flow_rhs<<<grid(nv), kTPB>>>(nv, d_fixed.p, bt2.p, u2.p, dorig.p, o.alpha_u, r2.p);
+    NDS_LAUNCH();
+    momentum_work(it, u0.p, r0.p);
+    momentum_work(it, u1.p, r1.p);
+    momentum_work(it, u2.p, r2.p);
+    B.B(u0.p, u1.p, u2.p, cont.p);
+    set_at<<<1, 1>>>(pin, 0.0, cont.p);
+    NDS_LAUNCH();
+    const double cn = pred.norm(cont.p);
+    if (it == 1) c0 = cn;
+    rel = cn / std::max(c0, 1e-300);
+    NDS_CUDA(cudaMemset(dp.p, 0, np * sizeof(double)));
+    const CgResult pr = pcg_prod(S, cont.p, dp.p, isd.p, o.p_rtol, o.p_atol, o.p_max, WP, pin);
+    if (!pr.ok) throw std::runtime_error("mixed-mesh SIMPLE: pressure PCG missed its target within p_max");
+    pits += pr.its;
+    p_update_minus<<<grid(np), kTPB>>>(np, pin, o.alpha_p, dp.p, p.p);
+    NDS_LAUNCH();
+    outer = it;
+    conv_ok = it > 1 && rel <= o.simple_tol;
+    if (verbose && (it <= 5 || it % 20 == 0 || conv_ok)) {
+      apply_val(u2.p, tmp.p);
+      residual_free<<<grid(nv), kTPB>>>(nv, d_fixed.p, r2.p, tmp.p, res.p);
+      NDS_LAUNCH();
+      const double mr = ured.norm(res.p) / std::max(ured.norm(r2.p), 1e-300);
+      std::printf("NODALS_HXT4B_SIMPLE it=%d relCont=%.12e absCont=%.12e zMomentumResidualRel=%.12e pCG=%d pRel=%.3e "
+                  "converged=%d status=PASS\n",
+                  it, rel, cn, mr, pr.its, pr.rel, (int)conv_ok);
+    }
+    if (it >= 5 && (!std::isfinite(rel) || rel > 1e8)) throw std::runtime_error("mixed-mesh SIMPLE diverged");
+    if (conv_ok) break;
+  }
+  if (!conv_ok) throw std::runtime_error("mixed-mesh SIMPLE: no convergence within max_outer");
+  const double loop_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  std::vector<double> hp((size_t)np), hu0((size_t)nv), hu1((size_t)nv), hu2((size_t)nv);
+  NDS_CUDA(cudaMemcpy(hp.data(), p.p, np * sizeof(double), cudaMemcpyDeviceToHost));
+  NDS_CUDA(cudaMemcpy(hu0.data(), u0.p, nv * sizeof(double), cudaMemcpyDeviceToHost));
+  NDS_CUDA(cudaMemcpy(hu1.data(), u1.p, nv * sizeof(double), cudaMemcpyDeviceToHost));
+  NDS_CUDA(cudaMemcpy(hu2.data(), u2.p, nv * sizeof(double), cudaMemcpyDeviceToHost));
+  nds_hybrid_flow_report R{};
+  R.outer_its = outer;
+  R.converged = 1;
+  R.n_hex = nh;
+  R.n_tet = nt;
+  R.n_velocity = nv;
+  R.final_rel_cont = rel;
+  R.slope = hybrid_pressure_slope(M, hp);
+  R.slope_exact = dpdz_exact;
+  const double pin_p = hybrid_boundary_pressure(M, hp, true), pout_p = hybrid_boundary_pressure(M, hp, false);
+  R.p_in = pin_p;
+  R.p_out = pout_p;
+  R.drop = pin_p - pout_p;
+  R.drop_exact = drop_exact;
+  long double en = 0, ed = 0, et = 0;
+  for (int v = 0; v < M.nv(); ++v) {
+    const double ex = pipe_profile(M.xyz[3 * (size_t)v], M.xyz[3 * (size_t)v + 1], F.radius, o.bulk);
+    const double e = hu2[(size_t)v] - ex;
+    en += e * e;
+    ed += ex * ex;
+    et += hu0[(size_t)v] * hu0[(size_t)v] + hu1[(size_t)v] * hu1[(size_t)v];
+  }
+  R.profile_rel_l2 = std::sqrt((double)(en / std::max((long double)1e-300, ed)));
+  R.transverse_rel_l2 = std::sqrt((double)(et / std::max((long double)1e-300, ed)));
+  // the last convection matrix applied to the axial velocity
+  twice<<<grid(nnz), kTPB>>>((size_t)nnz, conv.p, val.p);
+  NDS_LAUNCH();
+  apply_val(u2.p, tmp.p);
+  R.conv_norm = 0.5 * ured.norm(tmp.p);
+  R.velocity_norm = ured.norm(u2.p);
+  R.avg_pressure_cg = outer ? (double)pits / outer : 0.0;
+  R.loop_ms = loop_ms;
+  const double slope_err = std::abs(R.slope - dpdz_exact) / std::abs(dpdz_exact);
+  const double drop_err = std::abs(R.drop - drop_exact) / std::abs(drop_exact);
+  R.pass = drop_err < 0.05 && slope_err < 0.05 && R.profile_rel_l2 < 0.15 && std::isfinite(R.conv_norm);
+  if (verbose)
+    std::printf("NODALS_HXT4B_PHYSICS pressureSlope=%.12e exactSlope=%.12e slopeRelError=%.12e pIn=%.12e pOut=%.12e "
+                "pressureDrop=%.12e exactDrop=%.12e dropRelError=%.12e vertexVelocityProfileRelL2=%.12e "
+                "transverseVertexRelL2=%.12e convectionActionNorm=%.12e velocityNorm=%.12e avgPressureCG=%.6f status=%s\n",
+                R.slope, dpdz_exact, slope_err, pin_p, pout_p, R.drop, drop_exact, drop_err, R.profile_rel_l2,
+                R.transverse_rel_l2, R.conv_norm, R.velocity_norm, R.avg_pressure_cg, R.pass ? "PASS" : "FAIL");
+  if (out) *out = R;
+}
+
 }  // namespace hy
 }  // namespace nds
 
@@ -471,6 +882,50 @@ extern "C" int nds_hybrid_stokes_gate(const char* hxt1_path, double nu, double g
     if (e != cudaSuccess || ndev <= device) throw nds::CudaError(std::string("no CUDA device available: ") + cudaGetErrorString(e));
     NDS_CUDA(cudaSetDevice(device));
     nds::hy::run_gate(hxt1_path, nu, gamma, rau_scale, alpha_p, simple_tol, max_outer, verbose, out);
+    return NDS_OK;
+  } catch (const nds::CudaError& e) {
+    nds::set_error(e.what());
+    return NDS_E_CUDA;
+  } catch (const std::exception& e) {
+    nds::set_error(e.what());
+    return NDS_E_SETUP;
+  }
+}
+
+extern "C" void nds_hybrid_flow_defaults(nds_hybrid_flow_options* o) {
+  if (!o) return;
+  *o = nds_hybrid_flow_options{};
+  o->re = 20;
+  o->bulk = 1;
+  o->gamma = 50;
+  o->alpha_u = 0.7;
+  o->alpha_p = 1.0;
+  o->rau_scale = 2.0;
+  o->simple_tol = 1e-3;
+  o->max_outer = 3000;
+  o->momentum_work = 2;
+  o->mom_omega = 1.0;
+  o->mom_rtol = 0.5;
+  o->mom_atol = 1e-8;
+  o->p_rtol = 0.9;
+  o->p_atol = 1e-12;
+  o->p_max = 50;
+}
+
+extern "C" int nds_hybrid_flow(const char* hxt1_path, const nds_hybrid_flow_options* o, int device, int verbose,
+                               nds_hybrid_flow_report* out) {
+  if (!hxt1_path || !o || !(o->re > 0) || !(o->bulk > 0) || !(o->gamma > 0) || !(o->alpha_u > 0 && o->alpha_u <= 1) ||
+      !(o->alpha_p > 0) || !(o->rau_scale > 0) || o->max_outer < 1 || o->p_max < 1 || o->momentum_work < 0 ||
+      o->momentum_work > 2) {
+    nds::set_error("nds_hybrid_flow: bad argument");
+    return NDS_E_INVALID;
+  }
+  try {
+    int ndev = 0;
+    const cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev <= device) throw nds::CudaError(std::string("no CUDA device available: ") + cudaGetErrorString(e));
+    NDS_CUDA(cudaSetDevice(device));
+    nds::hy::run_flow(hxt1_path, *o, verbose, out);
     return NDS_OK;
   } catch (const nds::CudaError& e) {
     nds::set_error(e.what());

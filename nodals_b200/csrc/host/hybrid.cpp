@@ -281,24 +281,24 @@ std::vector<InterfacePlan> interface_plans(const HybridMesh& m) {
   return P;
 }
 
-HybridStokes build_hybrid_stokes(const HybridMesh& m, const std::vector<InterfacePlan>& plans, double nu,
-                                 double gamma) {
+namespace {
+// Velocity operator of diffusion and Nitsche coupling, merged into CSR
+// (columns sorted; equal positions summed in generation order: hexes,
+// tets, interface triangles).  diag_rau gets the diagonal without the
+// Nitsche penalty.
+struct Trip {
+  int32_t r, c;
+  double v;
+};
+void assemble_velocity(const HybridMesh& m, const std::vector<InterfacePlan>& plans, double nu, double gamma,
+                       std::vector<int32_t>& row, std::vector<int32_t>& col, std::vector<double>& val,
+                       std::vector<double>& diag_rau) {
   const Rules& R = rules();
-  HybridStokes H;
-  H.nvel = m.nvel();
-  H.np = m.np();
-  const int nv = H.nvel;
-  // ---- velocity operator as (row, col, value) triples in generation order;
-  // a stable sort by (row, col) then sums equal positions in that order
-  struct Trip {
-    int32_t r, c;
-    double v;
-  };
+  const int nv = m.nvel();
+  diag_rau.assign((size_t)nv, 0.0);
   std::vector<Trip> t;
   t.reserve((size_t)m.nhex() * 196 + (size_t)m.ntet() * 64 + plans.size() * 2 * 484);
-  H.diag_full.assign((size_t)nv, 0.0);
-  H.diag_rau.assign((size_t)nv, 0.0);
-  // hex volumes: K_ab = sum_q nu det w grad phi_a . grad phi_b (27 points)
+    // hex volumes: K_ab = sum_q nu det w grad phi_a . grad phi_b (27 points)
   for (int c = 0; c < m.nhex(); ++c) {
     double K[14][14] = {};
     for (int ix = 0; ix < 3; ++ix)
@@ -315,7 +315,7 @@ HybridStokes build_hybrid_stokes(const HybridMesh& m, const std::vector<Interfac
         }
     const auto& g = m.hex_dofs[(size_t)c];
     for (int a = 0; a < 14; ++a) {
-      H.diag_rau[(size_t)g[(size_t)a]] += K[a][a];
+      diag_rau[(size_t)g[(size_t)a]] += K[a][a];
       for (int b = 0; b < 14; ++b) t.push_back({g[(size_t)a], g[(size_t)b], K[a][b]});
     }
   }
@@ -334,7 +334,7 @@ HybridStokes build_hybrid_stokes(const HybridMesh& m, const std::vector<Interfac
         for (int j = 0; j < 3; ++j)
           for (int k = 0; k < 3; ++k) kd += D[a][b][j][k] * M[j][k];
         const double v = nu * tg[2] * kd;
-        if (a == b) H.diag_rau[(size_t)g[(size_t)a]] += v;
+        if (a == b) diag_rau[(size_t)g[(size_t)a]] += v;
         t.push_back({g[(size_t)a], g[(size_t)b], v});
       }
   }
@@ -383,11 +383,62 @@ HybridStokes build_hybrid_stokes(const HybridMesh& m, const std::vector<Interfac
         }
       });
       for (int i = 0; i < nu_; ++i) {
-        H.diag_rau[(size_t)u[i]] += cons[i];
+        diag_rau[(size_t)u[i]] += cons[i];
         for (int j = 0; j < nu_; ++j) t.push_back({u[i], u[j], K[i][j]});
       }
     }
   std::stable_sort(t.begin(), t.end(), [](const Trip& a, const Trip& b) { return std::tie(a.r, a.c) < std::tie(b.r, b.c); });
+  row.assign((size_t)nv + 1, 0);
+  col.clear();
+  val.clear();
+  for (size_t a = 0; a < t.size();) {
+    size_t b = a;
+    double v = 0;
+    while (b < t.size() && t[b].r == t[a].r && t[b].c == t[a].c) v += t[b++].v;
+    col.push_back(t[a].c);
+    val.push_back(v);
+    ++row[(size_t)t[a].r + 1];
+    a = b;
+  }
+  for (int i = 0; i < nv; ++i) row[(size_t)i + 1] += row[(size_t)i];
+}
+
+int32_t csr_find(const std::vector<int32_t>& row, const std::vector<int32_t>& col, int i, int j) {
+  const auto b = col.begin() + row[(size_t)i], e = col.begin() + row[(size_t)i + 1];
+  const auto it = std::lower_bound(b, e, j);
+  if (it == e || *it != j) throw std::runtime_error("hybrid velocity CSR: missing entry");
+  return (int32_t)(it - col.begin());
+}
+}  // namespace
+
+namespace {
+// manufactured pressure: (z_centroid - zmin) / L, shifted to 0 at cell 0
+void p_exact_of(const HybridMesh& m, HybridStokes& H) {
+  double zmin = 1e300, zmax = -1e300;
+  for (int v = 0; v < m.nv(); ++v) {
+    zmin = std::min(zmin, m.xyz[3 * (size_t)v + 2]);
+    zmax = std::max(zmax, m.xyz[3 * (size_t)v + 2]);
+  }
+  const double L = zmax - zmin;
+  H.p_exact.resize((size_t)H.np);
+  for (int c = 0; c < m.nhex(); ++c) H.p_exact[(size_t)c] = (hex_centroid(m, c).z - zmin) / L;
+  for (int c = 0; c < m.ntet(); ++c) H.p_exact[(size_t)(m.nhex() + c)] = (tet_centroid(m, c).z - zmin) / L;
+  const double sh = H.p_exact[0];
+  for (double& q : H.p_exact) q -= sh;
+}
+}  // namespace
+
+HybridStokes build_hybrid_stokes(const HybridMesh& m, const std::vector<InterfacePlan>& plans, double nu,
+                                 double gamma) {
+  HybridStokes H;
+  H.nvel = m.nvel();
+  H.np = m.np();
+  const int nv = H.nvel;
+  std::vector<int32_t> arow, acol;
+  std::vector<double> aval;
+  assemble_velocity(m, plans, nu, gamma, arow, acol, aval, H.diag_rau);
+  H.diag_full.assign((size_t)nv, 0.0);
+  for (int i = 0; i < nv; ++i) H.diag_full[(size_t)i] = aval[(size_t)csr_find(arow, acol, i, i)];
   // fixed unknowns: every vertex and bubble of the wall, inlet and outlet faces
   H.fixed.assign((size_t)nv, 0);
   auto fix_hex = [&](const std::array<int32_t, 3>& r) {
@@ -403,45 +454,30 @@ HybridStokes build_hybrid_stokes(const HybridMesh& m, const std::vector<Interfac
   for (const auto& r : m.out_hex) fix_hex(r);
   for (const auto& r : m.in_tet) fix_tet(r);
   for (const auto& r : m.out_tet) fix_tet(r);
+  // free rows as assembled, identity rows for the fixed unknowns
   H.a_row.assign((size_t)nv + 1, 0);
-  for (size_t a = 0; a < t.size();) {
-    size_t b = a;
-    double v = 0;
-    while (b < t.size() && t[b].r == t[a].r && t[b].c == t[a].c) v += t[b++].v;
-    const int r = t[a].r, c = t[a].c;
-    if (r == c) H.diag_full[(size_t)r] = v;
-    if (!H.fixed[(size_t)r]) {
-      H.a_col.push_back(c);
-      H.a_val.push_back(v);
-      ++H.a_row[(size_t)r + 1];
-    }
-    a = b;
-  }
-  // identity rows for the fixed unknowns, inserted in place
-  {
-    std::vector<int32_t> row((size_t)nv + 1, 0), col;
-    std::vector<double> val;
-    col.reserve(H.a_col.size() + (size_t)nv);
-    val.reserve(H.a_val.size() + (size_t)nv);
-    int32_t k = 0;
-    for (int i = 0; i < nv; ++i) {
-      const int32_t n = H.a_row[(size_t)i + 1];
-      if (H.fixed[(size_t)i]) {
-        col.push_back(i);
-        val.push_back(1.0);
-      } else {
-        for (int32_t q = 0; q < n; ++q) {
-          col.push_back(H.a_col[(size_t)(k + q)]);
-          val.push_back(H.a_val[(size_t)(k + q)]);
-        }
-        k += n;
+  for (int i = 0; i < nv; ++i) {
+    if (H.fixed[(size_t)i]) {
+      H.a_col.push_back(i);
+      H.a_val.push_back(1.0);
+    } else {
+      for (int32_t k = arow[(size_t)i]; k < arow[(size_t)i + 1]; ++k) {
+        H.a_col.push_back(acol[(size_t)k]);
+        H.a_val.push_back(aval[(size_t)k]);
       }
-      row[(size_t)i + 1] = (int32_t)col.size();
     }
-    H.a_row.swap(row);
-    H.a_col.swap(col);
-    H.a_val.swap(val);
+    H.a_row[(size_t)i + 1] = (int32_t)H.a_col.size();
   }
+  build_hybrid_divergence(m, plans, H);
+  p_exact_of(m, H);
+  return H;
+}
+
+void build_hybrid_divergence(const HybridMesh& m, const std::vector<InterfacePlan>& plans, HybridStokes& H) {
+  const Rules& R = rules();
+  H.nvel = m.nvel();
+  H.np = m.np();
+  const int nv = H.nvel;
   // ---- divergence rows: cell volume integrals, then the averaged traces
   // on interface triangles (hybrid_hxt3a/hxt3a_main.cu:132-246)
   std::vector<std::map<int32_t, std::array<double, 3>>> rows((size_t)H.np);
@@ -532,19 +568,140 @@ HybridStokes build_hybrid_stokes(const HybridMesh& m, const std::vector<Interfac
         H.btz[(size_t)q] = H.bz[(size_t)k];
       }
   }
-  // manufactured pressure: (z_centroid - zmin) / L, shifted to 0 at cell 0
-  double zmin = 1e300, zmax = -1e300;
+}
+
+HybridFlow build_hybrid_flow(const HybridMesh& m, const std::vector<InterfacePlan>& plans, double re, double bulk,
+                             double gamma) {
+  HybridFlow F;
+  F.nvel = m.nvel();
+  F.np = m.np();
+  F.nhex = m.nhex();
+  F.ntet = m.ntet();
+  const int nv = F.nvel;
+  // pipe geometry from the mesh (hxt4b_main.cu:233-236)
+  double zmin = 1e300, zmax = -1e300, R = 0;
   for (int v = 0; v < m.nv(); ++v) {
-    zmin = std::min(zmin, m.xyz[3 * (size_t)v + 2]);
-    zmax = std::max(zmax, m.xyz[3 * (size_t)v + 2]);
+    const double x = m.xyz[3 * (size_t)v], y = m.xyz[3 * (size_t)v + 1], z = m.xyz[3 * (size_t)v + 2];
+    zmin = std::min(zmin, z);
+    zmax = std::max(zmax, z);
+    R = std::max(R, std::sqrt(x * x + y * y));
   }
-  const double L = zmax - zmin;
-  H.p_exact.resize((size_t)H.np);
-  for (int c = 0; c < m.nhex(); ++c) H.p_exact[(size_t)c] = (hex_centroid(m, c).z - zmin) / L;
-  for (int c = 0; c < m.ntet(); ++c) H.p_exact[(size_t)(m.nhex() + c)] = (tet_centroid(m, c).z - zmin) / L;
-  const double sh = H.p_exact[0];
-  for (double& q : H.p_exact) q -= sh;
-  return H;
+  F.radius = R;
+  F.length = zmax - zmin;
+  F.diameter = 2 * R;
+  F.nu = bulk * F.diameter / re;
+  if (std::abs(F.length / F.diameter - 10) > 1e-6)
+    throw std::runtime_error("the mixed-mesh pipe SIMPLE expects a pipe of 10 diameters");
+  assemble_velocity(m, plans, F.nu, gamma, F.row, F.col, F.base, F.diag_r_base);
+  F.diag_pos.resize((size_t)nv);
+  for (int i = 0; i < nv; ++i) F.diag_pos[(size_t)i] = csr_find(F.row, F.col, i, i);
+  // convection gather lists: (entry, local value) pairs in cell order
+  std::vector<std::pair<int32_t, int32_t>> c;
+  c.reserve((size_t)m.nhex() * 196 + (size_t)m.ntet() * 64);
+  for (int h = 0; h < m.nhex(); ++h) {
+    const auto& g = m.hex_dofs[(size_t)h];
+    for (int a = 0; a < 14; ++a)
+      for (int b = 0; b < 14; ++b)
+        c.push_back({csr_find(F.row, F.col, g[(size_t)a], g[(size_t)b]), h * 196 + a * 14 + b});
+  }
+  const int32_t tet0 = m.nhex() * 196;
+  for (int t = 0; t < m.ntet(); ++t) {
+    const auto& g = m.tet_dofs[(size_t)t];
+    for (int a = 0; a < 8; ++a)
+      for (int b = 0; b < 8; ++b)
+        c.push_back({csr_find(F.row, F.col, g[(size_t)a], g[(size_t)b]), tet0 + t * 64 + a * 8 + b});
+  }
+  std::stable_sort(c.begin(), c.end(), [](const auto& x, const auto& y) { return x.first < y.first; });
+  F.src_off.assign(F.col.size() + 1, 0);
+  F.src.resize(c.size());
+  for (size_t q = 0; q < c.size(); ++q) {
+    ++F.src_off[(size_t)c[q].first + 1];
+    F.src[q] = c[q].second;
+  }
+  for (size_t k = 0; k < F.col.size(); ++k) F.src_off[k + 1] += F.src_off[k];
+  // Dirichlet data and initial state (hxt4b_main.cu:175-186): parabolic
+  // axial velocity at every vertex; wall faces no-slip; inlet faces the
+  // profile, their bubble the profile at the face centre minus the mean of
+  // the vertex values; the outlet is natural
+  F.fixed.assign((size_t)nv, 0);
+  F.u0.assign((size_t)nv, 0.0);
+  F.u1.assign((size_t)nv, 0.0);
+  F.u2.assign((size_t)nv, 0.0);
+  for (int v = 0; v < m.nv(); ++v) F.u2[(size_t)v] = pipe_profile(m.xyz[3 * (size_t)v], m.xyz[3 * (size_t)v + 1], R, bulk);
+  for (const auto& r : m.wall_hex) {
+    F.fixed[(size_t)r[2]] = 1;
+    F.u2[(size_t)r[2]] = 0;
+    for (int k = 0; k < 4; ++k) {
+      const int g = m.hexes[(size_t)r[0]][(size_t)kHexFace[r[1]][k]];
+      F.fixed[(size_t)g] = 1;
+      F.u0[(size_t)g] = F.u1[(size_t)g] = F.u2[(size_t)g] = 0;
+    }
+  }
+  auto inlet = [&](const int32_t* v, int nvert, int bubble) {
+    double av = 0, cx = 0, cy = 0;
+    for (int k = 0; k < nvert; ++k) {
+      const double x = m.xyz[3 * (size_t)v[k]], y = m.xyz[3 * (size_t)v[k] + 1];
+      const double q = pipe_profile(x, y, R, bulk);
+      F.fixed[(size_t)v[k]] = 1;
+      F.u2[(size_t)v[k]] = q;
+      if (nvert == 4) {
+        av += .25 * q;
+        cx += .25 * x;
+        cy += .25 * y;
+      } else {
+        av += q / 3;
+        cx += x / 3;
+        cy += y / 3;
+      }
+    }
+    F.fixed[(size_t)bubble] = 1;
+    F.u2[(size_t)bubble] = pipe_profile(cx, cy, R, bulk) - av;
+  };
+  for (const auto& r : m.in_hex) {
+    int32_t v[4];
+    for (int k = 0; k < 4; ++k) v[k] = m.hexes[(size_t)r[0]][(size_t)kHexFace[r[1]][k]];
+    inlet(v, 4, r[2]);
+  }
+  for (const auto& r : m.in_tet) {
+    int32_t v[3];
+    for (int k = 0; k < 3; ++k) v[k] = m.tets[(size_t)r[0]][(size_t)kTetFace[r[1]][k]];
+    inlet(v, 3, r[2]);
+  }
+  // greedy colouring of the free rows over their lower free neighbours
+  // (hxt4b_main.cu color_free_rows)
+  std::vector<int> colour((size_t)nv, -1), mark(128, -1);
+  int nc = 0, nfree = 0;
+  for (int i = 0; i < nv; ++i) {
+    if (F.fixed[(size_t)i]) continue;
+    ++nfree;
+    for (int32_t q = F.row[(size_t)i]; q < F.row[(size_t)i + 1]; ++q) {
+      const int j = F.col[(size_t)q];
+      if (j >= i || F.fixed[(size_t)j]) continue;
+      const int cj = colour[(size_t)j];
+      if (cj >= 0) {
+        if (cj >= (int)mark.size()) mark.resize((size_t)cj + 32, -1);
+        mark[(size_t)cj] = i;
+      }
+    }
+    int cc = 0;
+    while (cc < (int)mark.size() && mark[(size_t)cc] == i) ++cc;
+    if (cc >= (int)mark.size()) mark.resize((size_t)cc + 32, -1);
+    colour[(size_t)i] = cc;
+    nc = std::max(nc, cc + 1);
+  }
+  F.colour_off.assign((size_t)nc + 1, 0);
+  for (int i = 0; i < nv; ++i)
+    if (colour[(size_t)i] >= 0) ++F.colour_off[(size_t)colour[(size_t)i] + 1];
+  for (int k = 0; k < nc; ++k) F.colour_off[(size_t)k + 1] += F.colour_off[(size_t)k];
+  F.colour_rows.resize((size_t)nfree);
+  {
+    std::vector<int32_t> next(F.colour_off.begin(), F.colour_off.end() - 1);
+    for (int i = 0; i < nv; ++i)
+      if (colour[(size_t)i] >= 0) F.colour_rows[(size_t)next[(size_t)colour[(size_t)i]]++] = i;
+  }
+  for (int k = 0; k < nc; ++k) F.max_colour = std::max(F.max_colour, F.colour_off[(size_t)k + 1] - F.colour_off[(size_t)k]);
+  F.pin = !m.out_hex.empty() ? m.out_hex[0][0] : (!m.out_tet.empty() ? m.nhex() + m.out_tet[0][0] : 0);
+  return F;
 }
 
 double hybrid_pressure_slope(const HybridMesh& m, const std::vector<double>& p) {

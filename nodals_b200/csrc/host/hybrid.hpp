@@ -71,6 +71,42 @@ struct HybridStokes {
 HybridStokes build_hybrid_stokes(const HybridMesh& m, const std::vector<InterfacePlan>& plans, double nu,
                                  double gamma);
 
+// The production mixed-mesh SIMPLE of the reference (HXT4B,
+// gpu/serial_cuda/hybrid_hxt4b/hxt4b_main.cu): steady Navier-Stokes in a
+// straight pipe (10 diameters) with a lagged central advective convection
+// term assembled into the velocity CSR each iteration, multicolour
+// Gauss-Seidel velocity sweeps, and a Jacobi-PCG pressure correction.
+struct HybridFlow {
+  int nvel = 0, np = 0, nhex = 0, ntet = 0;
+  double radius = 0, length = 0, diameter = 0, nu = 0;
+  int pin = 0;  // pressure gauge cell: the first outlet face's cell
+  // velocity CSR of all unknowns (columns sorted), the constant part of its
+  // values (diffusion + Nitsche) and the penalty-free diagonal of that part
+  std::vector<int32_t> row, col, diag_pos;
+  std::vector<double> base, diag_r_base;
+  // entry k of the convection matrix = sum of local[src[q]] over q in
+  // [src_off[k], src_off[k+1]): local holds 196 values per hex (row-major
+  // a * 14 + b), then 64 per tet, in cell order
+  std::vector<int32_t> src_off, src;
+  // wall, inlet unknowns; initial state (parabolic axial velocity at every
+  // vertex, the inlet bubbles corrected to the profile at the face centre)
+  std::vector<uint8_t> fixed;
+  std::vector<double> u0, u1, u2;
+  // colours of the free unknowns: rows of colour c are colour_rows[colour_off[c] ..)
+  std::vector<int32_t> colour_rows, colour_off;
+  int max_colour = 0;
+};
+HybridFlow build_hybrid_flow(const HybridMesh& m, const std::vector<InterfacePlan>& plans, double re, double bulk,
+                             double gamma);
+// the divergence operator alone (rows of HybridStokes::b_* and bt_*)
+void build_hybrid_divergence(const HybridMesh& m, const std::vector<InterfacePlan>& plans, HybridStokes& H);
+// axial velocity of the Hagen-Poiseuille profile
+inline double pipe_profile(double x, double y, double R, double bulk) {
+  const double r2 = x * x + y * y;
+  const double v = 2.0 * bulk * (1.0 - r2 / (R * R));
+  return v > 0 ? v : 0.0;
+}
+
 // least-squares axial pressure slope and area-weighted inlet/outlet pressure
 // of a P0 field (hybrid_hxt4a/hxt4a_main.cu:339-357)
 double hybrid_pressure_slope(const HybridMesh& m, const std::vector<double>& p);
