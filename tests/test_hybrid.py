@@ -1,4 +1,5 @@
-"""Mixed hexahedron/tetrahedron Stokes gate (the reference's HXT4A,
+"""Mixed hexahedron/tetrahedron solvers against the reference binaries' own
+runs on the same HXT1 mesh: the Stokes gate (the reference's HXT4A,
 gpu/serial_cuda/hybrid_hxt4a/hxt4a_main.cu) against the reference binary's
 own run on the same HXT1 mesh (tests/golden/hxt4a_hybrid_r2.log, made by
 make_hxt4a_golden.py from tests/golden/hxt1_hybrid_r2.bin, itself the
@@ -11,6 +12,15 @@ GPU: the gate executable prints the same audit, the same relCont history
 (1e-9 relative; the reference sums with atomics, so not bitwise), CG counts
 within one iteration, the same outer iteration count and the same result
 line (errors against p* and the Hagen-Poiseuille-like checks 1e-8).
+
+The mixed-mesh pipe SIMPLE (the reference's HXT4B,
+gpu/serial_cuda/hybrid_hxt4b/hxt4b_main.cu; logs made by
+make_hxt4b_golden.py): with tight pressure solves every printed iteration,
+the converged iteration and the physics line agree with the reference to
+3e-9.  At the default pressure tolerance (rtol 0.9) the iteration amplifies
+rounding -- the reference's own runs differ from each other, its atomic
+sums changing the last bits -- so there the first iteration agrees to 1e-10,
+the converged iteration within 5 and the physics within 5e-3.
 """
 from __future__ import annotations
 
@@ -75,3 +85,51 @@ def test_gate_matches_reference_run():
         assert _close(gr[k], wr[k], tol), (k, gr[k], wr[k])
     assert abs(float(gr["avgMomentumCG"]) - float(wr["avgMomentumCG"])) < 0.01
     assert abs(float(gr["avgPressureCG"]) - float(wr["avgPressureCG"])) < 0.01
+
+
+def _parse_4b(text):
+    lines = text.splitlines()
+    simple = {int(_kv(l)["it"]): _kv(l) for l in lines if l.startswith("NODALS_HXT4B_SIMPLE")}
+    phys = next(_kv(l) for l in lines if l.startswith("NODALS_HXT4B_PHYSICS"))
+    cfg = next(_kv(l) for l in lines if l.startswith("NODALS_HXT4B_CONFIG"))
+    cfg.update(next(_kv(l) for l in lines if l.startswith("NODALS_HXT4B_HAGEN_POISEUILLE")))
+    return cfg, simple, phys
+
+
+def _run_4b(*extra):
+    r = subprocess.run([str(ROOT / "nodals_b200" / "_lib" / "nodals_hxt4b_fp64"), "--mesh", str(MESH), *extra],
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert "HXT4B_GATE_STATUS=PASS" in r.stdout
+    return _parse_4b(r.stdout)
+
+
+PHYS = ("pressureSlope", "pIn", "pOut", "pressureDrop", "vertexVelocityProfileRelL2", "transverseVertexRelL2",
+        "convectionActionNorm", "velocityNorm")
+
+
+@pytest.mark.gpu
+def test_pipe_simple_matches_reference_tight():
+    gc, gs, gp = _run_4b("--p-rtol", "1e-10", "--p-max", "2000")
+    wc, ws, wp = _parse_4b((GOLDEN / "hxt4b_hybrid_r2_tight.log").read_text())
+    for k in ("cellsHex", "cellsTet", "velocityDofs", "pressureDofs", "csrNnz", "colors", "maxColor", "pressureGaugePin"):
+        assert gc.get(k) == wc.get(k), k
+    assert sorted(gs) == sorted(ws)
+    for it, w in ws.items():
+        g = gs[it]
+        for k in ("relCont", "absCont", "zMomentumResidualRel"):
+            assert _close(g[k], w[k], 3e-9), (it, k, g[k], w[k])
+        assert abs(int(g["pCG"]) - int(w["pCG"])) <= 1, (it, g["pCG"], w["pCG"])
+    for k in PHYS:
+        assert _close(gp[k], wp[k], 3e-9), (k, gp[k], wp[k])
+
+
+@pytest.mark.gpu
+def test_pipe_simple_default_tolerance():
+    gc, gs, gp = _run_4b("--p-max", "400")
+    wc, ws, wp = _parse_4b((GOLDEN / "hxt4b_hybrid_r2.log").read_text())
+    for k in ("relCont", "absCont", "zMomentumResidualRel"):
+        assert _close(gs[1][k], ws[1][k], 1e-10), (k, gs[1][k], ws[1][k])
+    assert abs(max(gs) - max(ws)) <= 5, (max(gs), max(ws))
+    for k in PHYS:
+        assert _close(gp[k], wp[k], 5e-3), (k, gp[k], wp[k])
