@@ -34,6 +34,7 @@ int main(int argc, char** argv) {
     nds_hybrid_report r{};
     if (nds_hybrid_stokes_gate(mesh.c_str(), nu, gamma, rau_scale, alpha_p, simple_tol, max_outer, 0, 1, &r) != NDS_OK)
       throw std::runtime_error(nds_last_error());
+    std::printf("NODALS_HXT4A_TIMING loopMs=%.3f outer=%d status=PASS\n", r.loop_ms, r.outer_its);
     std::printf("HXT4A_PRECISION_STATUS=%s\n", r.pass ? "PASS" : "FAIL");
     return r.pass ? 0 : 3;
   } catch (const std::exception& e) {

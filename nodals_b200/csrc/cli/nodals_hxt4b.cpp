@@ -49,6 +49,7 @@ int main(int argc, char** argv) {
     std::printf("NODALS_HXT4B_KERNEL_POLICY convectionBlocks=CELL_LOCAL_THEN_GATHER gsRows=WARP_PER_ROW status=PASS\n");
     nds_hybrid_flow_report r{};
     if (nds_hybrid_flow(mesh.c_str(), &o, 0, 1, &r) != NDS_OK) throw std::runtime_error(nds_last_error());
+    std::printf("NODALS_HXT4B_TIMING loopMs=%.3f outer=%d status=PASS\n", r.loop_ms, r.outer_its);
     std::printf("HXT4B_GATE_STATUS=%s\n", r.pass ? "PASS" : "FAIL");
     return r.pass ? 0 : 3;
   } catch (const std::exception& e) {
