@@ -281,6 +281,22 @@ typedef struct nds_hybrid_flow_report {
 void nds_hybrid_flow_defaults(nds_hybrid_flow_options* o);   /* the reference binary's defaults */
 int nds_hybrid_flow(const char* hxt1_path, const nds_hybrid_flow_options* o, int device, int verbose,
                     nds_hybrid_flow_report* out);
+/* The same solve, also returning the final fields: u0, u1, u2 hold
+ * counts[5] velocity unknowns each (vertices first, then face bubbles) and
+ * pressure counts[6] P0 values (hexes first), counts[] being the HXT1
+ * header read by nds_hybrid_counts.  Any of the four may be NULL. */
+int nds_hybrid_flow_fields(const char* hxt1_path, const nds_hybrid_flow_options* o, int device, int verbose,
+                           nds_hybrid_flow_report* out, double* u0, double* u1, double* u2, double* pressure);
+/* Host only: the 13 counts of a mixed-mesh HXT1 header (nv nhex ntet
+ * nhexface ntetface nvel npressure ninterface nwallhex ninhex nintet
+ * nouthex nouttet). */
+int nds_hybrid_counts(const char* hxt1_path, uint64_t counts[13]);
+/* Host only: the HXT4B VTU (hxt4b_main.cu:203-209, written for --vtu at
+ * :265): points, hex then tet connectivity (VTK types 12 and 10), vertex
+ * velocity from the first nv entries of u0/u1/u2, the P0 pressure, its
+ * volume-weighted vertex average, and region 1 (hex) / 2 (tet). */
+int nds_hybrid_write_vtu(const char* hxt1_path, const char* vtu_path, const double* u0, const double* u1,
+                         const double* u2, const double* pressure);
 
 #ifdef __cplusplus
 }

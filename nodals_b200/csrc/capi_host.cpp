@@ -172,6 +172,30 @@ int nds_hybrid_operator_audit(const char* path, double nu, double gamma, double 
   }
 }
 
+int nds_hybrid_counts(const char* path, uint64_t counts[13]) {
+  if (!path || !counts) { set_error("null argument"); return NDS_E_INVALID; }
+  try {
+    const nds::HybridMesh m = nds::read_hxt1_hybrid(path);
+    std::copy(m.count, m.count + 13, counts);
+    return NDS_OK;
+  } catch (const std::exception& e) {
+    set_error(e.what());
+    return NDS_E_SETUP;
+  }
+}
+
+int nds_hybrid_write_vtu(const char* hxt1_path, const char* vtu_path, const double* u0, const double* u1,
+                         const double* u2, const double* pressure) {
+  if (!hxt1_path || !vtu_path || !u0 || !u1 || !u2 || !pressure) { set_error("null argument"); return NDS_E_INVALID; }
+  try {
+    nds::write_hybrid_vtu(nds::read_hxt1_hybrid(hxt1_path), vtu_path, u0, u1, u2, pressure);
+    return NDS_OK;
+  } catch (const std::exception& e) {
+    set_error(e.what());
+    return NDS_E_SETUP;
+  }
+}
+
 int nds_mesh_read_hxt1(const char* path, nds_mesh** out) {
   if (!path || !out) { set_error("null argument"); return NDS_E_INVALID; }
   try {

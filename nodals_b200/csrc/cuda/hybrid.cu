@@ -687,7 +687,8 @@ CgResult pcg_prod(Op& A, const double* rhs, double* x, const double* invdiag, do
   return R;
 }
 
-void run_flow(const char* path, const nds_hybrid_flow_options& o, int verbose, nds_hybrid_flow_report* out) {
+void run_flow(const char* path, const nds_hybrid_flow_options& o, int verbose, nds_hybrid_flow_report* out,
+              double* const fields[4]) {
   const HybridMesh M = read_hxt1_hybrid(path);
   const auto P = interface_plans(M);
   HybridFlow F = build_hybrid_flow(M, P, o.re, o.bulk, o.gamma);
@@ -864,6 +865,9 @@ void run_flow(const char* path, const nds_hybrid_flow_options& o, int verbose, n
                 R.slope, dpdz_exact, slope_err, pin_p, pout_p, R.drop, drop_exact, drop_err, R.profile_rel_l2,
                 R.transverse_rel_l2, R.conv_norm, R.velocity_norm, R.avg_pressure_cg, R.pass ? "PASS" : "FAIL");
   if (out) *out = R;
+  const std::vector<double>* host[4] = {&hu0, &hu1, &hu2, &hp};
+  for (int k = 0; k < 4; ++k)
+    if (fields[k]) std::copy(host[k]->begin(), host[k]->end(), fields[k]);
 }
 
 }  // namespace hy
@@ -914,6 +918,12 @@ extern "C" void nds_hybrid_flow_defaults(nds_hybrid_flow_options* o) {
 
 extern "C" int nds_hybrid_flow(const char* hxt1_path, const nds_hybrid_flow_options* o, int device, int verbose,
                                nds_hybrid_flow_report* out) {
+  return nds_hybrid_flow_fields(hxt1_path, o, device, verbose, out, nullptr, nullptr, nullptr, nullptr);
+}
+
+extern "C" int nds_hybrid_flow_fields(const char* hxt1_path, const nds_hybrid_flow_options* o, int device, int verbose,
+                                      nds_hybrid_flow_report* out, double* u0, double* u1, double* u2,
+                                      double* pressure) {
   if (!hxt1_path || !o || !(o->re > 0) || !(o->bulk > 0) || !(o->gamma > 0) || !(o->alpha_u > 0 && o->alpha_u <= 1) ||
       !(o->alpha_p > 0) || !(o->rau_scale > 0) || o->max_outer < 1 || o->p_max < 1 || o->momentum_work < 0 ||
       o->momentum_work > 2) {
@@ -925,7 +935,8 @@ extern "C" int nds_hybrid_flow(const char* hxt1_path, const nds_hybrid_flow_opti
     const cudaError_t e = cudaGetDeviceCount(&ndev);
     if (e != cudaSuccess || ndev <= device) throw nds::CudaError(std::string("no CUDA device available: ") + cudaGetErrorString(e));
     NDS_CUDA(cudaSetDevice(device));
-    nds::hy::run_flow(hxt1_path, *o, verbose, out);
+    double* const fields[4] = {u0, u1, u2, pressure};
+    nds::hy::run_flow(hxt1_path, *o, verbose, out, fields);
     return NDS_OK;
   } catch (const nds::CudaError& e) {
     nds::set_error(e.what());

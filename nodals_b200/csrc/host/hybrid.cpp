@@ -739,4 +739,61 @@ double hybrid_boundary_pressure(const HybridMesh& m, const std::vector<double>& 
   return (double)(num / den);
 }
 
+void write_hybrid_vtu(const HybridMesh& m, const std::string& path, const double* u0, const double* u1,
+                      const double* u2, const double* p) {
+  const int nv = m.nv(), nh = m.nhex(), nt = m.ntet();
+  // vertex pressure = sum over the cells at the vertex of (V/k) p / sum of V/k,
+  // k the cell's vertex count; hexes first, then tets, in cell order
+  std::vector<long double> wsum((size_t)nv, 0.0L), psum((size_t)nv, 0.0L);
+  for (int c = 0; c < nh; ++c) {
+    const double share = m.hex_geom[(size_t)c][0] / 8;
+    for (int a = 0; a < 8; ++a) {
+      const size_t v = (size_t)m.hexes[(size_t)c][(size_t)a];
+      wsum[v] += share;
+      psum[v] += share * p[(size_t)c];
+    }
+  }
+  for (int c = 0; c < nt; ++c) {
+    const double share = m.tet_geom[(size_t)c][0] / 4;
+    for (int a = 0; a < 4; ++a) {
+      const size_t v = (size_t)m.tets[(size_t)c][(size_t)a];
+      wsum[v] += share;
+      psum[v] += share * p[(size_t)(nh + c)];
+    }
+  }
+  std::ofstream f(path);
+  if (!f) throw std::runtime_error("cannot write " + path);
+  f.precision(16);
+  f << "<?xml version=\"1.0\"?>\n<VTKFile type=\"UnstructuredGrid\" version=\"0.1\" byte_order=\"LittleEndian\">\n"
+    << "<UnstructuredGrid><Piece NumberOfPoints=\"" << nv << "\" NumberOfCells=\"" << nh + nt << "\">\n"
+    << "<Points><DataArray type=\"Float64\" NumberOfComponents=\"3\" format=\"ascii\">\n";
+  for (int v = 0; v < nv; ++v)
+    f << m.xyz[3 * (size_t)v] << ' ' << m.xyz[3 * (size_t)v + 1] << ' ' << m.xyz[3 * (size_t)v + 2] << '\n';
+  f << "</DataArray></Points><Cells><DataArray type=\"Int32\" Name=\"connectivity\" format=\"ascii\">\n";
+  for (const auto& h : m.hexes) {
+    for (int32_t v : h) f << v << ' ';
+    f << '\n';
+  }
+  for (const auto& t : m.tets) {
+    for (int32_t v : t) f << v << ' ';
+    f << '\n';
+  }
+  f << "</DataArray><DataArray type=\"Int64\" Name=\"offsets\" format=\"ascii\">\n";
+  long long end = 0;
+  for (int c = 0; c < nh + nt; ++c) f << (end += c < nh ? 8 : 4) << '\n';
+  f << "</DataArray><DataArray type=\"UInt8\" Name=\"types\" format=\"ascii\">\n";
+  for (int c = 0; c < nh + nt; ++c) f << (c < nh ? "12\n" : "10\n");
+  f << "</DataArray></Cells><PointData><DataArray type=\"Float64\" Name=\"velocity_Q1P1_vertex\" "
+       "NumberOfComponents=\"3\" format=\"ascii\">\n";
+  for (int v = 0; v < nv; ++v) f << u0[v] << ' ' << u1[v] << ' ' << u2[v] << '\n';
+  f << "</DataArray><DataArray type=\"Float64\" Name=\"pressure_Q0P0_vertex_volume_average\" format=\"ascii\">\n";
+  for (int v = 0; v < nv; ++v) f << (wsum[(size_t)v] > 0 ? (double)(psum[(size_t)v] / wsum[(size_t)v]) : 0.0) << '\n';
+  f << "</DataArray></PointData><CellData><DataArray type=\"Float64\" Name=\"pressure_Q0P0\" format=\"ascii\">\n";
+  for (int c = 0; c < nh + nt; ++c) f << p[c] << '\n';
+  f << "</DataArray><DataArray type=\"Int32\" Name=\"region\" format=\"ascii\">\n";
+  for (int c = 0; c < nh + nt; ++c) f << (c < nh ? "1\n" : "2\n");
+  f << "</DataArray></CellData></Piece></UnstructuredGrid></VTKFile>\n";
+  if (!f) throw std::runtime_error("short write to " + path);
+}
+
 }  // namespace nds

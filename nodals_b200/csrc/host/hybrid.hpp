@@ -112,4 +112,12 @@ inline double pipe_profile(double x, double y, double R, double bulk) {
 double hybrid_pressure_slope(const HybridMesh& m, const std::vector<double>& p);
 double hybrid_boundary_pressure(const HybridMesh& m, const std::vector<double>& p, bool inlet);
 
+// ASCII VTU of a mixed mesh (hybrid_hxt4b/hxt4b_main.cu:203-209): the hexes
+// (VTK type 12, region 1) then the tets (type 10, region 2); vertex velocity
+// (the first nv entries of each component), the P0 pressure per cell, and its
+// volume-weighted vertex average (each cell gives a quarter or an eighth of
+// its volume to every vertex).  Values are printed with 16 significant digits.
+void write_hybrid_vtu(const HybridMesh& m, const std::string& path, const double* u0, const double* u1,
+                      const double* u2, const double* p);
+
 }  // namespace nds

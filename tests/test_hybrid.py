@@ -21,16 +21,25 @@ the converged iteration and the physics line agree with the reference to
 rounding -- the reference's own runs differ from each other, its atomic
 sums changing the last bits -- so there the first iteration agrees to 1e-10,
 the converged iteration within 5 and the physics within 5e-3.
+
+The VTU of --vtu (hxt4b_main.cu:203-209): on the CPU the C-ABI writer, given
+seeded fields, produces byte for byte the text of the oracle's restatement
+of the reference writer; on the GPU the tight run's file has the reference
+run's layout and integer blocks exactly and its values to 3e-9 of each
+block's largest magnitude (tests/golden/hxt4b_hybrid_r2_tight.vtu.gz).
 """
 from __future__ import annotations
 
 import ctypes as C
+import gzip
 import re
 import subprocess
 
+import numpy as np
 import pytest
 
 from conftest import GOLDEN, ROOT
+from oracle import hybrid_vtu
 
 MESH = GOLDEN / "hxt1_hybrid_r2.bin"
 LOG = GOLDEN / "hxt4a_hybrid_r2.log"
@@ -96,11 +105,42 @@ def _parse_4b(text):
     return cfg, simple, phys
 
 
-def _run_4b(*extra):
-    r = subprocess.run([str(ROOT / "nodals_b200" / "_lib" / "nodals_hxt4b_fp64"), "--mesh", str(MESH), *extra],
-                       capture_output=True, text=True, timeout=600)
+def test_vtu_writer_matches_reference_layout(native, tmp_path):
+    m = hybrid_vtu.read_mixed_hxt1(MESH)
+    counts = (C.c_uint64 * 13)()
+    assert native.lib().nds_hybrid_counts(str(MESH).encode(), counts) == 0
+    assert tuple(counts) == tuple(m["counts"])
+    nvel, npr = int(counts[5]), int(counts[6])
+    rng = np.random.default_rng(7)
+    u = [rng.standard_normal(nvel) * 10.0 ** rng.integers(-12, 3, nvel) for _ in range(3)]
+    p = rng.standard_normal(npr) * 16.0
+    out = tmp_path / "seeded.vtu"
+    dp = C.POINTER(C.c_double)
+    args = [np.ascontiguousarray(a).ctypes.data_as(dp) for a in (*u, p)]
+    assert native.lib().nds_hybrid_write_vtu(str(MESH).encode(), str(out).encode(), *args) == 0
+    assert out.read_text() == hybrid_vtu.vtu_text(m, *u, p)
+    assert native.lib().nds_hybrid_write_vtu(str(MESH).encode(), str(tmp_path / "no" / "x.vtu").encode(), *args) != 0
+
+
+def _same_vtu(got: str, want: str, tol: float):
+    number = re.compile(r"(?<=\n)[-+0-9.eE ]+(?=\n)")
+    assert number.sub("#", got) == number.sub("#", want)
+    g, w = hybrid_vtu.parse_vtu(got), hybrid_vtu.parse_vtu(want)
+    assert sorted(g) == sorted(w)
+    for name in ("points", "connectivity", "offsets", "types", "region"):
+        assert np.array_equal(g[name], w[name]), name
+    for name in ("velocity_Q1P1_vertex", "pressure_Q0P0_vertex_volume_average", "pressure_Q0P0"):
+        scale = np.abs(w[name]).max()
+        err = np.abs(g[name] - w[name]).max()
+        assert err <= tol * scale, (name, err, scale)
+
+
+def _run_4b(vtu, *extra):
+    r = subprocess.run([str(ROOT / "nodals_b200" / "_lib" / "nodals_hxt4b_fp64"), "--mesh", str(MESH), "--vtu", str(vtu),
+                        *extra], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
     assert "HXT4B_GATE_STATUS=PASS" in r.stdout
+    assert f"NODALS_HXT4B_OUTPUT vtu={vtu} status=PASS" in r.stdout
     return _parse_4b(r.stdout)
 
 
@@ -109,8 +149,9 @@ PHYS = ("pressureSlope", "pIn", "pOut", "pressureDrop", "vertexVelocityProfileRe
 
 
 @pytest.mark.gpu
-def test_pipe_simple_matches_reference_tight():
-    gc, gs, gp = _run_4b("--p-rtol", "1e-10", "--p-max", "2000")
+def test_pipe_simple_matches_reference_tight(tmp_path):
+    vtu = tmp_path / "r2.vtu"
+    gc, gs, gp = _run_4b(vtu, "--p-rtol", "1e-10", "--p-max", "2000")
     wc, ws, wp = _parse_4b((GOLDEN / "hxt4b_hybrid_r2_tight.log").read_text())
     for k in ("cellsHex", "cellsTet", "velocityDofs", "pressureDofs", "csrNnz", "colors", "maxColor", "pressureGaugePin"):
         assert gc.get(k) == wc.get(k), k
@@ -122,11 +163,12 @@ def test_pipe_simple_matches_reference_tight():
         assert abs(int(g["pCG"]) - int(w["pCG"])) <= 1, (it, g["pCG"], w["pCG"])
     for k in PHYS:
         assert _close(gp[k], wp[k], 3e-9), (k, gp[k], wp[k])
+    _same_vtu(vtu.read_text(), gzip.decompress((GOLDEN / "hxt4b_hybrid_r2_tight.vtu.gz").read_bytes()).decode(), 3e-9)
 
 
 @pytest.mark.gpu
-def test_pipe_simple_default_tolerance():
-    gc, gs, gp = _run_4b("--p-max", "400")
+def test_pipe_simple_default_tolerance(tmp_path):
+    gc, gs, gp = _run_4b(tmp_path / "r2.vtu", "--p-max", "400")
     wc, ws, wp = _parse_4b((GOLDEN / "hxt4b_hybrid_r2.log").read_text())
     for k in ("relCont", "absCont", "zMomentumResidualRel"):
         assert _close(gs[1][k], ws[1][k], 1e-10), (k, gs[1][k], ws[1][k])
