@@ -268,6 +268,20 @@ typedef struct nds_hybrid_flow_options {
   int max_outer, momentum_work;
   double mom_omega, mom_rtol, mom_atol, p_rtol, p_atol;
   int p_max;
+  /* Pressure preconditioner: 0 Jacobi (the HXT4B solver), 1 the classical
+   * AMG V-cycle of the reference's turbulent entry (hxt4c::HybridAMG,
+   * hybrid_hxt5b/hybrid_amg.cuh:353-533; options and defaults of
+   * hxt5b_main.cu:49-86, 195-210).  The hierarchy is built once from the
+   * initial rAU; the fine matrix B diag(rAU) B^T is refreshed every
+   * iteration, the coarse levels are kept. */
+  int pressure_solver;
+  int amg_smoother;                 /* enum nds_amg_smoother */
+  int amg_spectrum_policy;          /* enum nds_spectrum_policy (auto: power iterations for cheb2 only) */
+  int amg_terminal, amg_power_its, amg_cheb_degree;
+  int amg_jacobi_fine_sweeps, amg_jacobi_coarse_sweeps;
+  int amg_mcgs_fine_sweeps, amg_mcgs_coarse_sweeps, amg_mcgs_order; /* enum nds_mcgs_order */
+  int cf_pmax, cf_interp, cf_aggressive_first;                       /* enum nds_cf_interp */
+  double cf_theta, amg_lambda_safety, amg_lambda_low_fraction, amg_jacobi_omega, amg_mcgs_omega;
 } nds_hybrid_flow_options;
 typedef struct nds_hybrid_flow_report {
   int outer_its, converged, pass;
@@ -297,6 +311,18 @@ int nds_hybrid_counts(const char* hxt1_path, uint64_t counts[13]);
  * volume-weighted vertex average, and region 1 (hex) / 2 (tet). */
 int nds_hybrid_write_vtu(const char* hxt1_path, const char* vtu_path, const double* u0, const double* u1,
                          const double* u2, const double* pressure);
+/* Host only: the pressure preconditioner's setup for a given rAU (nvel
+ * values): the pressure matrix (pin = the first outlet face's cell) and its
+ * CF hierarchy, as hxt4c::build_hybrid_fine_host (hybrid_amg.cuh:63) and
+ * build_cf_hierarchy_from_csr (hybrid_cf_overload.inc:5) build them.  Named
+ * arrays: "pin", "fine.row|col|val|diag|entryRow|diagPos", "amg.levels",
+ * "amg.fineLambda", "amg.levelLambda", "amg.P<l>.row|col|val|nCoarse",
+ * "amg.A<l>.row|col|val|diag", "amg.terminal_inv". */
+typedef struct nds_hybrid_amg nds_hybrid_amg;
+int nds_hybrid_amg_create(const char* hxt1_path, const double* rau, const nds_hybrid_flow_options* o,
+                          nds_hybrid_amg** out);
+int nds_hybrid_amg_array(const nds_hybrid_amg* h, const char* name, nds_array* out);
+void nds_hybrid_amg_destroy(nds_hybrid_amg* h);
 
 #ifdef __cplusplus
 }

@@ -28,6 +28,17 @@ void set_error(const std::string& e) { g_err = e; }
 
 using nds::set_error;
 
+namespace {
+struct HybridAmgHandle {
+  nds::HybridSchurCsr fine;
+  nds::Hierarchy H;
+  std::vector<double> scalars[4];
+  std::vector<int64_t> ncoarse;
+  std::map<std::string, nds_array> arrays;
+};
+template <class T> nds_array view_of(const std::vector<T>& v, int dtype) { return nds_array{v.data(), (int64_t)v.size(), dtype}; }
+}  // namespace
+
 extern "C" {
 
 const char* nds_last_error(void) { return g_err.c_str(); }
@@ -183,6 +194,73 @@ int nds_hybrid_counts(const char* path, uint64_t counts[13]) {
     return NDS_E_SETUP;
   }
 }
+
+int nds_hybrid_amg_create(const char* path, const double* rau, const nds_hybrid_flow_options* o, nds_hybrid_amg** out) {
+  if (!path || !rau || !o || !out) { set_error("null argument"); return NDS_E_INVALID; }
+  try {
+    const nds::AmgOptions ao = nds::hybrid_amg_options(*o);
+    const nds::HybridMesh m = nds::read_hxt1_hybrid(path);
+    nds::HybridStokes B;
+    nds::build_hybrid_divergence(m, nds::interface_plans(m), B);
+    auto h = std::make_unique<HybridAmgHandle>();
+    const int pin = nds::hybrid_pin(m);
+    h->fine = nds::hybrid_schur_csr(B, pin, std::vector<double>(rau, rau + B.nvel));
+    h->H = nds::build_cf_hierarchy(h->fine.A, ao);
+    auto& A = h->arrays;
+    h->scalars[0] = {(double)pin};
+    h->scalars[1] = {(double)h->H.A.size()};
+    h->scalars[2] = {h->H.fine_lambda};
+    A["pin"] = view_of(h->scalars[0], 0);
+    A["amg.levels"] = view_of(h->scalars[1], 0);
+    A["amg.fineLambda"] = view_of(h->scalars[2], 0);
+    A["fine.row"] = view_of(h->fine.A.row, 2);
+    A["fine.col"] = view_of(h->fine.A.col, 1);
+    A["fine.val"] = view_of(h->fine.A.val, 0);
+    A["fine.diag"] = view_of(h->fine.A.diag, 0);
+    A["fine.entryRow"] = view_of(h->fine.entry_row, 1);
+    A["fine.diagPos"] = view_of(h->fine.diag_pos, 1);
+    A["amg.levelLambda"] = view_of(h->H.level_lambda, 0);
+    A["amg.terminal_inv"] = view_of(h->H.terminal_inv, 0);
+    h->ncoarse.resize(h->H.P.size());
+    for (size_t l = 0; l < h->H.P.size(); ++l) {
+      const std::string p = "amg.P" + std::to_string(l) + ".";
+      h->ncoarse[l] = h->H.P[l].nc;
+      A[p + "nCoarse"] = nds_array{&h->ncoarse[l], 1, 2};
+      A[p + "row"] = view_of(h->H.P[l].row, 2);
+      A[p + "col"] = view_of(h->H.P[l].col, 1);
+      A[p + "val"] = view_of(h->H.P[l].val, 0);
+    }
+    for (size_t l = 0; l < h->H.A.size(); ++l) {
+      const std::string p = "amg.A" + std::to_string(l) + ".";
+      A[p + "row"] = view_of(h->H.A[l].row, 2);
+      A[p + "col"] = view_of(h->H.A[l].col, 1);
+      A[p + "val"] = view_of(h->H.A[l].val, 0);
+      A[p + "diag"] = view_of(h->H.A[l].diag, 0);
+    }
+    *out = reinterpret_cast<nds_hybrid_amg*>(h.release());
+    return NDS_OK;
+  } catch (const std::invalid_argument& e) {
+    set_error(e.what());
+    return NDS_E_INVALID;
+  } catch (const std::exception& e) {
+    set_error(e.what());
+    return NDS_E_SETUP;
+  }
+}
+
+int nds_hybrid_amg_array(const nds_hybrid_amg* hh, const char* name, nds_array* out) {
+  if (!hh || !name || !out) { set_error("null argument"); return NDS_E_INVALID; }
+  const auto* h = reinterpret_cast<const HybridAmgHandle*>(hh);
+  auto it = h->arrays.find(name);
+  if (it == h->arrays.end()) {
+    set_error(std::string("unknown hybrid AMG array ") + name);
+    return NDS_E_INVALID;
+  }
+  *out = it->second;
+  return NDS_OK;
+}
+
+void nds_hybrid_amg_destroy(nds_hybrid_amg* h) { delete reinterpret_cast<HybridAmgHandle*>(h); }
 
 int nds_hybrid_write_vtu(const char* hxt1_path, const char* vtu_path, const double* u0, const double* u1,
                          const double* u2, const double* pressure) {

@@ -914,6 +914,25 @@ extern "C" void nds_hybrid_flow_defaults(nds_hybrid_flow_options* o) {
   o->p_rtol = 0.9;
   o->p_atol = 1e-12;
   o->p_max = 50;
+  o->pressure_solver = 0;
+  o->amg_smoother = NDS_SM_CHEB2;
+  o->amg_spectrum_policy = NDS_SPEC_AUTO;
+  o->amg_terminal = 1000;
+  o->amg_power_its = 16;
+  o->amg_cheb_degree = 4;
+  o->amg_jacobi_fine_sweeps = 1;
+  o->amg_jacobi_coarse_sweeps = 1;
+  o->amg_mcgs_fine_sweeps = 1;
+  o->amg_mcgs_coarse_sweeps = 1;
+  o->amg_mcgs_order = NDS_MCGS_SYMMETRIC;
+  o->cf_pmax = 8;
+  o->cf_interp = NDS_CF_EXTI;
+  o->cf_aggressive_first = 0;
+  o->cf_theta = 0.25;
+  o->amg_lambda_safety = 1.5;
+  o->amg_lambda_low_fraction = 0.05;
+  o->amg_jacobi_omega = 0.7;
+  o->amg_mcgs_omega = 1.0;
 }
 
 extern "C" int nds_hybrid_flow(const char* hxt1_path, const nds_hybrid_flow_options* o, int device, int verbose,

@@ -744,6 +744,54 @@ std::vector<double> dense_inverse_cholesky(const CsrHost& A) {
   return inv;
 }
 
+Hierarchy build_cf_hierarchy(CsrHost A, const AmgOptions& o) {
+  StageTimer tm("amg");
+  Hierarchy H;
+  H.fine_diag = A.diag;
+  H.fine_lambda = o.power_its > 0 ? power_csr(A, o.power_its, o.lambda_safety) : 1.0;
+  int logical = 0;
+  if (o.cf_aggressive_first && A.n > o.terminal) {
+    Split s0 = pmis_split(A, o.cf_theta);
+    Transfer P01 = cf_transfer(A, s0, o.cf_pmax, o.cf_interp);
+    CsrHost A1 = galerkin(A, P01);
+    if (A1.n <= o.terminal) {
+      H.P.push_back(std::move(P01));
+      H.A.push_back(std::move(A1));
+    } else {
+      Split s1 = pmis_split(A1, o.cf_theta);
+      Transfer P12 = cf_transfer(A1, s1, o.cf_pmax, o.cf_interp);
+      CsrHost A2 = galerkin(A1, P12);
+      H.P.push_back(compose(P01, P12));
+      H.A.push_back(std::move(A2));
+    }
+    if (H.A.back().n > o.terminal) {
+      H.level_lambda.resize(H.A.size(), 0.0);
+      H.level_lambda[0] = o.power_its > 0 ? power_csr(H.A.back(), o.power_its, o.lambda_safety) : 1.0;
+    }
+    A = H.A.back();
+    logical = 1;
+  }
+  while (H.A.empty() || H.A.back().n > o.terminal) {
+    Split s = pmis_split(A, o.cf_theta);
+    tm.mark("pmis");
+    H.P.push_back(cf_transfer(A, s, o.cf_pmax, o.cf_interp));
+    tm.mark("interpolation");
+    H.A.push_back(galerkin(A, H.P.back()));
+    tm.mark("galerkin");
+    if (H.A.back().n <= o.terminal) break;
+    const size_t idx = H.A.size() - 1;
+    if (H.level_lambda.size() < H.A.size()) H.level_lambda.resize(H.A.size(), 0.0);
+    H.level_lambda[idx] = o.power_its > 0 ? power_csr(H.A.back(), o.power_its, o.lambda_safety) : 1.0;
+    A = H.A.back();
+    if (++logical > 20) throw std::runtime_error("CF hierarchy excessive levels");
+  }
+  if (H.level_lambda.size() < H.A.size()) H.level_lambda.resize(H.A.size(), 1.0);
+  H.terminal_n = H.A.back().n;
+  H.terminal_inv = dense_inverse_cholesky(H.A.back());
+  tm.mark("terminal_inverse");
+  return H;
+}
+
 Hierarchy build_hierarchy(const Mesh& m, const Setup& S, const std::vector<double>& rau, const AmgOptions& o) {
   StageTimer tm("amg");
   Hierarchy H;
@@ -789,47 +837,7 @@ Hierarchy build_hierarchy(const Mesh& m, const Setup& S, const std::vector<doubl
     }
     if (H.level_lambda.size() < H.A.size()) H.level_lambda.resize(H.A.size(), 0.0);
   } else if (o.hierarchy == "cf") {
-    CsrHost A = host_fine_csr(S, rau);
-    H.fine_diag = A.diag;
-    tm.mark("fine_csr");
-    H.fine_lambda = o.power_its > 0 ? power_csr(A, o.power_its, o.lambda_safety) : 1.0;
-    int logical = 0;
-    if (o.cf_aggressive_first && A.n > o.terminal) {
-      Split s0 = pmis_split(A, o.cf_theta);
-      Transfer P01 = cf_transfer(A, s0, o.cf_pmax, o.cf_interp);
-      CsrHost A1 = galerkin(A, P01);
-      if (A1.n <= o.terminal) {
-        H.P.push_back(std::move(P01));
-        H.A.push_back(std::move(A1));
-      } else {
-        Split s1 = pmis_split(A1, o.cf_theta);
-        Transfer P12 = cf_transfer(A1, s1, o.cf_pmax, o.cf_interp);
-        CsrHost A2 = galerkin(A1, P12);
-        H.P.push_back(compose(P01, P12));
-        H.A.push_back(std::move(A2));
-      }
-      if (H.A.back().n > o.terminal) {
-        H.level_lambda.resize(H.A.size(), 0.0);
-        H.level_lambda[0] = o.power_its > 0 ? power_csr(H.A.back(), o.power_its, o.lambda_safety) : 1.0;
-      }
-      A = H.A.back();
-      logical = 1;
-    }
-    while (H.A.empty() || H.A.back().n > o.terminal) {
-      Split s = pmis_split(A, o.cf_theta);
-      tm.mark("pmis");
-      H.P.push_back(cf_transfer(A, s, o.cf_pmax, o.cf_interp));
-      tm.mark("interpolation");
-      H.A.push_back(galerkin(A, H.P.back()));
-      tm.mark("galerkin");
-      if (H.A.back().n <= o.terminal) break;
-      const size_t idx = H.A.size() - 1;
-      if (H.level_lambda.size() < H.A.size()) H.level_lambda.resize(H.A.size(), 0.0);
-      H.level_lambda[idx] = o.power_its > 0 ? power_csr(H.A.back(), o.power_its, o.lambda_safety) : 1.0;
-      A = H.A.back();
-      if (++logical > 20) throw std::runtime_error("CF hierarchy excessive levels");
-    }
-    if (H.level_lambda.size() < H.A.size()) H.level_lambda.resize(H.A.size(), 1.0);
+    return build_cf_hierarchy(host_fine_csr(S, rau), o);
   } else {
     throw std::runtime_error("amg hierarchy must be sa or cf");
   }

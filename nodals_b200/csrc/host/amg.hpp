@@ -55,6 +55,9 @@ struct AmgOptions {
 };
 
 Hierarchy build_hierarchy(const Mesh& m, const Setup& S, const std::vector<double>& rau, const AmgOptions& o);
+// classical C/F hierarchy of any symmetric CSR with a positive diagonal (the
+// reference's build_cf_hierarchy_from_csr, hybrid_hxt5b/hybrid_cf_overload.inc)
+Hierarchy build_cf_hierarchy(CsrHost A, const AmgOptions& o);
 
 // pieces exposed for tests
 std::vector<int32_t> aggregate_graph(const std::vector<std::vector<int32_t>>& g, int target, int minsz, int softmax,

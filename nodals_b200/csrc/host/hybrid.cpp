@@ -8,6 +8,7 @@
 #include <stdexcept>
 #include <tuple>
 
+#include "../../../include/nodals_b200.h"
 #include "fem.hpp"
 
 namespace nds {
@@ -700,7 +701,7 @@ HybridFlow build_hybrid_flow(const HybridMesh& m, const std::vector<InterfacePla
       if (colour[(size_t)i] >= 0) F.colour_rows[(size_t)next[(size_t)colour[(size_t)i]]++] = i;
   }
   for (int k = 0; k < nc; ++k) F.max_colour = std::max(F.max_colour, F.colour_off[(size_t)k + 1] - F.colour_off[(size_t)k]);
-  F.pin = !m.out_hex.empty() ? m.out_hex[0][0] : (!m.out_tet.empty() ? m.nhex() + m.out_tet[0][0] : 0);
+  F.pin = hybrid_pin(m);
   return F;
 }
 
@@ -737,6 +738,97 @@ double hybrid_boundary_pressure(const HybridMesh& m, const std::vector<double>& 
     den += A;
   }
   return (double)(num / den);
+}
+
+HybridSchurCsr hybrid_schur_csr(const HybridStokes& B, int pin, const std::vector<double>& rau) {
+  const int np = B.np;
+  if ((int)rau.size() != B.nvel) throw std::runtime_error("hybrid pressure matrix: rAU size mismatch");
+  auto entry = [&](int i, int j) {
+    int32_t a = B.b_row[(size_t)i], b = B.b_row[(size_t)j];
+    const int32_t ae = B.b_row[(size_t)i + 1], be = B.b_row[(size_t)j + 1];
+    long double s = 0;
+    while (a < ae && b < be) {
+      const int32_t ga = B.b_col[(size_t)a], gb = B.b_col[(size_t)b];
+      if (ga < gb) { ++a; continue; }
+      if (gb < ga) { ++b; continue; }
+      s += (long double)rau[(size_t)ga] * ((long double)B.bx[(size_t)a] * B.bx[(size_t)b] +
+                                           (long double)B.by[(size_t)a] * B.by[(size_t)b] +
+                                           (long double)B.bz[(size_t)a] * B.bz[(size_t)b]);
+      ++a;
+      ++b;
+    }
+    return (double)s;
+  };
+  HybridSchurCsr H;
+  CsrHost& A = H.A;
+  A.n = np;
+  A.row.assign((size_t)np + 1, 0);
+  std::vector<int32_t> nb;
+  for (int i = 0; i < np; ++i) {
+    nb.assign(1, i);
+    if (i != pin) {
+      for (int32_t k = B.b_row[(size_t)i]; k < B.b_row[(size_t)i + 1]; ++k) {
+        const int32_t g = B.b_col[(size_t)k];
+        for (int32_t q = B.bt_row[(size_t)g]; q < B.bt_row[(size_t)g + 1]; ++q)
+          if (B.bt_col[(size_t)q] != pin) nb.push_back(B.bt_col[(size_t)q]);
+      }
+      std::sort(nb.begin(), nb.end());
+      nb.erase(std::unique(nb.begin(), nb.end()), nb.end());
+    }
+    A.col.insert(A.col.end(), nb.begin(), nb.end());
+    A.row[(size_t)i + 1] = (int64_t)A.col.size();
+  }
+  A.val.resize(A.col.size());
+  A.diag.resize((size_t)np);
+  H.entry_row.resize(A.col.size());
+  H.diag_pos.assign((size_t)np, -1);
+  for (int i = 0; i < np; ++i) {
+    for (int64_t k = A.row[(size_t)i]; k < A.row[(size_t)i + 1]; ++k) {
+      const int j = A.col[(size_t)k];
+      H.entry_row[(size_t)k] = i;
+      const double v = i == pin ? (j == pin ? 1.0 : 0.0) : entry(i, j);
+      A.val[(size_t)k] = v;
+      if (j == i) {
+        H.diag_pos[(size_t)i] = (int32_t)k;
+        A.diag[(size_t)i] = v;
+      }
+    }
+    if (!(A.diag[(size_t)i] > 0.0) || !std::isfinite(A.diag[(size_t)i]))
+      throw std::runtime_error("hybrid pressure matrix: nonpositive diagonal");
+  }
+  return H;
+}
+
+int hybrid_pin(const HybridMesh& m) {
+  return !m.out_hex.empty() ? m.out_hex[0][0] : (!m.out_tet.empty() ? m.nhex() + m.out_tet[0][0] : 0);
+}
+
+AmgOptions hybrid_amg_options(const nds_hybrid_flow_options& o) {
+  auto bad = [](const char* what) { throw std::invalid_argument(what); };
+  if (o.amg_smoother < NDS_SM_CHEB2 || o.amg_smoother > NDS_SM_MCGS) bad("unknown AMG smoother");
+  if (o.cf_interp != NDS_CF_DIRECT && o.cf_interp != NDS_CF_EXTI) bad("CF interp must be direct or exti");
+  if (o.amg_mcgs_order < NDS_MCGS_SYMMETRIC || o.amg_mcgs_order > NDS_MCGS_BACKWARD) bad("bad MCGS order");
+  if (o.pressure_solver == 1 && o.amg_smoother == NDS_SM_MCGS && o.amg_mcgs_order != NDS_MCGS_SYMMETRIC)
+    bad("PCG requires symmetric MCGS");
+  if (o.amg_spectrum_policy < NDS_SPEC_AUTO || o.amg_spectrum_policy > NDS_SPEC_OFF) bad("bad AMG spectrum policy");
+  if (o.amg_terminal < 1 || o.cf_pmax < 1 || !(o.cf_theta > 0) || o.amg_cheb_degree < 1 || o.amg_power_its < 0 ||
+      o.amg_jacobi_fine_sweeps < 1 || o.amg_jacobi_coarse_sweeps < 1 || o.amg_mcgs_fine_sweeps < 1 ||
+      o.amg_mcgs_coarse_sweeps < 1 || !(o.amg_lambda_safety > 0) || !(o.amg_lambda_low_fraction > 0))
+    bad("bad AMG option value");
+  AmgOptions a;
+  a.hierarchy = "cf";
+  a.terminal = o.amg_terminal;
+  a.power_its = o.amg_spectrum_policy == NDS_SPEC_ALWAYS || (o.amg_spectrum_policy == NDS_SPEC_AUTO &&
+                                                             o.amg_smoother == NDS_SM_CHEB2)
+                    ? o.amg_power_its
+                    : 0;
+  if (o.amg_smoother == NDS_SM_CHEB2 && a.power_its <= 0) bad("Chebyshev requires spectrum estimation");
+  a.lambda_safety = o.amg_lambda_safety;
+  a.cf_theta = o.cf_theta;
+  a.cf_pmax = o.cf_pmax;
+  a.cf_interp = o.cf_interp == NDS_CF_EXTI ? "exti" : "direct";
+  a.cf_aggressive_first = o.cf_aggressive_first != 0;
+  return a;
 }
 
 void write_hybrid_vtu(const HybridMesh& m, const std::string& path, const double* u0, const double* u1,

@@ -19,6 +19,11 @@
 #include <string>
 #include <vector>
 
+#include "amg.hpp"
+#include "setup.hpp"
+
+struct nds_hybrid_flow_options;
+
 namespace nds {
 
 struct HybridMesh {
@@ -100,6 +105,23 @@ HybridFlow build_hybrid_flow(const HybridMesh& m, const std::vector<InterfacePla
                              double gamma);
 // the divergence operator alone (rows of HybridStokes::b_* and bt_*)
 void build_hybrid_divergence(const HybridMesh& m, const std::vector<InterfacePlan>& plans, HybridStokes& H);
+// Pressure matrix of the mixed-mesh SIMPLE for the AMG preconditioner
+// (hybrid_hxt5b/hybrid_amg.cuh:63-125): S = B diag(rAU) B^T with the pin row
+// replaced by the identity and the pin column dropped.  Row i holds i and
+// every cell sharing a velocity unknown with it, sorted; each value is the
+// merge of the two sorted B rows summed in extended precision.
+struct HybridSchurCsr {
+  CsrHost A;
+  std::vector<int32_t> entry_row, diag_pos;
+};
+HybridSchurCsr hybrid_schur_csr(const HybridStokes& B, int pin, const std::vector<double>& rau);
+// pressure gauge cell of the pipe solvers: the first outlet face's cell
+// (hybrid_hxt4b/hxt4b_main.cu:236)
+int hybrid_pin(const HybridMesh& m);
+// hierarchy options of a mixed-mesh run, checked as the reference's
+// turbulent entry checks them (hxt5b_main.cu:76-86, 195-200); throws
+// std::invalid_argument on a bad combination
+AmgOptions hybrid_amg_options(const nds_hybrid_flow_options& o);
 // axial velocity of the Hagen-Poiseuille profile
 inline double pipe_profile(double x, double y, double R, double bulk) {
   const double r2 = x * x + y * y;

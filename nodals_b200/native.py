@@ -115,6 +115,47 @@ class _Array(C.Structure):
 _DT = {0: np.float64, 1: np.int32, 2: np.int64, 3: np.uint8, 4: np.uint32}
 
 
+class HybridFlowOptions(C.Structure):
+    """nds_hybrid_flow_options: the mixed-mesh pipe SIMPLE and its pressure
+    preconditioner (defaults: the reference HXT4B binary, AMG fields those of
+    its turbulent entry)."""
+    _fields_ = ([(n, C.c_double) for n in ("re", "bulk", "gamma", "alpha_u", "alpha_p", "rau_scale", "simple_tol")]
+                + [("max_outer", C.c_int), ("momentum_work", C.c_int)]
+                + [(n, C.c_double) for n in ("mom_omega", "mom_rtol", "mom_atol", "p_rtol", "p_atol")]
+                + [("p_max", C.c_int)]
+                + [(n, C.c_int) for n in ("pressure_solver", "amg_smoother", "amg_spectrum_policy", "amg_terminal",
+                                          "amg_power_its", "amg_cheb_degree", "amg_jacobi_fine_sweeps",
+                                          "amg_jacobi_coarse_sweeps", "amg_mcgs_fine_sweeps", "amg_mcgs_coarse_sweeps",
+                                          "amg_mcgs_order", "cf_pmax", "cf_interp", "cf_aggressive_first")]
+                + [(n, C.c_double) for n in ("cf_theta", "amg_lambda_safety", "amg_lambda_low_fraction",
+                                             "amg_jacobi_omega", "amg_mcgs_omega")])
+
+    @classmethod
+    def make(cls, **kw) -> "HybridFlowOptions":
+        o = cls()
+        lib().nds_hybrid_flow_defaults(C.byref(o))
+        for k, v in kw.items():
+            if not hasattr(o, k):
+                raise AttributeError(f"no hybrid flow option {k}")
+            setattr(o, k, v)
+        return o
+
+
+class HybridFlowReport(C.Structure):
+    _fields_ = ([(n, C.c_int) for n in ("outer_its", "converged", "pass_", "n_hex", "n_tet", "n_velocity")]
+                + [(n, C.c_double) for n in ("final_rel_cont", "avg_pressure_cg", "slope", "slope_exact", "p_in",
+                                             "p_out", "drop", "drop_exact", "profile_rel_l2", "transverse_rel_l2",
+                                             "conv_norm", "velocity_norm", "loop_ms")])
+
+
+def _array_copy(a) -> np.ndarray:
+    dt = np.dtype(_DT[a.dtype])
+    if a.count == 0:
+        return np.zeros(0, dtype=dt)
+    buf = (C.c_char * (a.count * dt.itemsize)).from_address(a.data)
+    return np.frombuffer(buf, dtype=dt).copy()
+
+
 def lib():
     global _lib
     if _lib is None:
@@ -139,6 +180,15 @@ def lib():
         L.nds_write_vtu.argtypes = [vp, C.c_char_p, vp, vp, vp, vp, C.c_int, C.c_int]
         L.nds_compute_hp_errors.argtypes = [vp, vp, vp, vp, vp, C.POINTER(HpErrors)]
         L.nds_cell_average_velocity.argtypes = [vp, vp, vp, vp, vp]
+        L.nds_hybrid_flow_defaults.argtypes = [C.POINTER(HybridFlowOptions)]
+        L.nds_hybrid_counts.argtypes = [C.c_char_p, C.POINTER(C.c_uint64)]
+        L.nds_hybrid_write_vtu.argtypes = [C.c_char_p, C.c_char_p, vp, vp, vp, vp]
+        L.nds_hybrid_amg_create.argtypes = [C.c_char_p, vp, C.POINTER(HybridFlowOptions), C.POINTER(vp)]
+        L.nds_hybrid_amg_array.argtypes = [vp, C.c_char_p, C.POINTER(_Array)]
+        L.nds_hybrid_amg_destroy.argtypes = [vp]
+        if hasattr(L, "nds_hybrid_flow_fields"):
+            L.nds_hybrid_flow_fields.argtypes = [C.c_char_p, C.POINTER(HybridFlowOptions), C.c_int, C.c_int,
+                                                 C.POINTER(HybridFlowReport), vp, vp, vp, vp]
         if hasattr(L, "nds_solver_create"):
             L.nds_solver_create.argtypes = [vp, C.POINTER(vp)]
             L.nds_solver_reset.argtypes = [vp]
@@ -208,6 +258,45 @@ class Mesh:
     def __del__(self):
         if getattr(self, "_h", None) and _lib is not None:
             _lib.nds_mesh_destroy(self._h)
+            self._h = None
+
+
+def hybrid_counts(path) -> tuple:
+    c = (C.c_uint64 * 13)()
+    _check(lib().nds_hybrid_counts(str(path).encode(), c))
+    return tuple(int(x) for x in c)
+
+
+def hybrid_flow(path, options: HybridFlowOptions | None = None, device: int = 0, verbose: int = 0, **kw):
+    """Mixed-mesh pipe SIMPLE on the GPU; returns (report, u0, u1, u2, p)."""
+    o = options if options is not None else HybridFlowOptions.make(**kw)
+    n = hybrid_counts(path)
+    u = [np.zeros(n[5]) for _ in range(3)]
+    p = np.zeros(n[6])
+    r = HybridFlowReport()
+    _check(lib().nds_hybrid_flow_fields(str(path).encode(), C.byref(o), device, verbose, C.byref(r),
+                                        *[_p(x) for x in (*u, p)]))
+    return r, u[0], u[1], u[2], p
+
+
+class HybridAmg:
+    """Host setup of the mixed-mesh pressure preconditioner for a given rAU."""
+
+    def __init__(self, path, rau: np.ndarray, options: HybridFlowOptions | None = None, **kw):
+        o = options if options is not None else HybridFlowOptions.make(**kw)
+        r = np.ascontiguousarray(rau, dtype=np.float64)
+        h = C.c_void_p()
+        _check(lib().nds_hybrid_amg_create(str(path).encode(), _p(r), C.byref(o), C.byref(h)))
+        self._h = h
+
+    def array(self, name: str) -> np.ndarray:
+        a = _Array()
+        _check(lib().nds_hybrid_amg_array(self._h, name.encode(), C.byref(a)))
+        return _array_copy(a)
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.nds_hybrid_amg_destroy(self._h)
             self._h = None
 
 
