@@ -282,6 +282,12 @@ typedef struct nds_hybrid_flow_options {
   int amg_mcgs_fine_sweeps, amg_mcgs_coarse_sweeps, amg_mcgs_order; /* enum nds_mcgs_order */
   int cf_pmax, cf_interp, cf_aggressive_first;                       /* enum nds_cf_interp */
   double cf_theta, amg_lambda_safety, amg_lambda_low_fraction, amg_jacobi_omega, amg_mcgs_omega;
+  /* 0: the reference's V-cycle, whose post-smoothing calls pass one work
+   * vector as both the result and the Chebyshev product (and on the fine
+   * level the right-hand side as the scaled right-hand side), which makes
+   * its cheb2 V-cycle nonsymmetric; 1: separate work vectors there, a
+   * symmetric V-cycle (same result for jacobi with one sweep and mcgs). */
+  int amg_separate_post;
 } nds_hybrid_flow_options;
 typedef struct nds_hybrid_flow_report {
   int outer_its, converged, pass;
@@ -323,6 +329,12 @@ int nds_hybrid_amg_create(const char* hxt1_path, const double* rau, const nds_hy
                           nds_hybrid_amg** out);
 int nds_hybrid_amg_array(const nds_hybrid_amg* h, const char* name, nds_array* out);
 void nds_hybrid_amg_destroy(nds_hybrid_amg* h);
+/* One application of that preconditioner on the device: the hierarchy is
+ * built from rau, the fine matrix refreshed from rau on the device, and
+ * z = M^-1 b (np values each) computed by the reference's V-cycle
+ * (hxt4c::HybridAMG::apply, hybrid_amg.cuh:519-533). */
+int nds_hybrid_amg_vcycle(const char* hxt1_path, const double* rau, const nds_hybrid_flow_options* o, int device,
+                          const double* b, double* z);
 
 #ifdef __cplusplus
 }

@@ -15,6 +15,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <memory>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -687,6 +688,413 @@ CgResult pcg_prod(Op& A, const double* rhs, double* x, const double* invdiag, do
   return R;
 }
 
+// ---- classical AMG preconditioner of the pressure correction (the
+// reference's hxt4c::HybridAMG, hybrid_hxt5b/hybrid_amg.cuh:127-533).  The
+// hierarchy is built once on the host from the initial rAU; the fine matrix
+// B diag(rAU) B^T is refreshed on the device every SIMPLE iteration.
+// Restriction gathers through the explicit transpose of each transfer, so
+// the V-cycle sums in a fixed order (the reference scatters with atomics).
+
+// entry k of the fine matrix: merge of the sorted B rows i and j
+__global__ void amg_fine_refresh(int nnz, const int32_t* __restrict__ erow, const int32_t* __restrict__ acol,
+                                 const int32_t* __restrict__ brow, const int32_t* __restrict__ bcol,
+                                 const double* __restrict__ bx, const double* __restrict__ by,
+                                 const double* __restrict__ bz, const double* __restrict__ rau, int pin,
+                                 double* __restrict__ aval) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nnz) return;
+  const int i = erow[k], j = acol[k];
+  if (i == pin || j == pin) {
+    aval[k] = (i == pin && j == pin) ? 1.0 : 0.0;
+    return;
+  }
+  int a = brow[i], b = brow[j];
+  const int ae = brow[i + 1], be = brow[j + 1];
+  double s = 0;
+  while (a < ae && b < be) {
+    const int ga = bcol[a], gb = bcol[b];
+    if (ga < gb) {
+      ++a;
+    } else if (gb < ga) {
+      ++b;
+    } else {
+      s += rau[ga] * (bx[a] * bx[b] + by[a] * by[b] + bz[a] * bz[b]);
+      ++a;
+      ++b;
+    }
+  }
+  aval[k] = s;
+}
+// diagonal and absolute row sum; flags a nonpositive or non-finite one
+__global__ void amg_diag_l1(int n, const int32_t* __restrict__ row, const int32_t* __restrict__ dpos,
+                            const double* __restrict__ val, double* __restrict__ diag, double* __restrict__ l1,
+                            int* __restrict__ bad) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double d = val[dpos[i]];
+  double s = 0;
+  for (int k = row[i]; k < row[i + 1]; ++k) s += fabs(val[k]);
+  diag[i] = d;
+  l1[i] = s;
+  if (!(d > 0) || !isfinite(d) || !(s > 0) || !isfinite(s)) atomicAdd(bad, 1);
+}
+__global__ void amg_jacobi_set(int n, double w, const double* b, const double* den, double* x) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) x[i] = w * b[i] / den[i];
+}
+__global__ void amg_jacobi_add(int n, double w, const double* r, const double* den, double* x) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) x[i] += w * r[i] / den[i];
+}
+// symmetric Chebyshev on D^-1/2 A D^-1/2: bs = b / sqrt(d) (b may be bs)
+__global__ void amg_scale_rhs(int n, const double* b, const double* d, double* bs) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) bs[i] = b[i] / sqrt(d[i]);
+}
+__global__ void amg_scaled_copy(int n, double w, const double* bs, double* y) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) y[i] = w * bs[i];
+}
+__global__ void amg_unscale(int n, const double* y, const double* d, double* x) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) x[i] = y[i] / sqrt(d[i]);
+}
+__global__ void amg_unscale_inplace(int n, double* x, const double* d) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) x[i] /= sqrt(d[i]);
+}
+// y += w (bs - Hy); Hy may be y itself
+__global__ void amg_cheb_add(int n, double w, const double* bs, const double* Hy, double* y) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) y[i] += w * (bs[i] - Hy[i]);
+}
+// one colour of a Gauss-Seidel sweep, one warp per row
+__global__ void amg_gs_colour(int count, const int32_t* __restrict__ rows, const int32_t* __restrict__ row,
+                              const int32_t* __restrict__ col, const double* __restrict__ val,
+                              const double* __restrict__ diag, const double* __restrict__ b, double* x, double w) {
+  const int q = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (q >= count) return;
+  const int i = rows[q];
+  double off = 0;
+  for (int k = row[i] + lane; k < row[i + 1]; k += 32) {
+    const int j = col[k];
+    if (j != i) off += val[k] * x[j];
+  }
+  off = warp_sum(off);
+  if (lane == 0) {
+    const double old = x[i];
+    x[i] = old + w * ((b[i] - off) / diag[i] - old);
+  }
+}
+// y += A x (prolongation) or y = A x (restriction through P^T), warp per row
+__global__ void amg_csr_add(int n, const int32_t* __restrict__ row, const int32_t* __restrict__ col,
+                            const double* __restrict__ val, const double* __restrict__ x, double* __restrict__ y,
+                            int accumulate) {
+  const int i = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (i >= n) return;
+  double s = 0;
+  for (int k = row[i] + lane; k < row[i + 1]; k += 32) s += val[k] * x[col[k]];
+  s = warp_sum(s);
+  if (lane == 0) y[i] = accumulate ? y[i] + s : s;
+}
+// x = inv b with a dense row-major inverse, warp per row
+__global__ void amg_dense(int n, const double* __restrict__ inv, const double* __restrict__ b, double* __restrict__ x) {
+  const int i = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (i >= n) return;
+  double s = 0;
+  for (int j = lane; j < n; j += 32) s += inv[(size_t)i * n + j] * b[j];
+  s = warp_sum(s);
+  if (lane == 0) x[i] = s;
+}
+__global__ void amg_axpy(int n, const double* x, double* y) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) y[i] += x[i];
+}
+
+// greedy colouring of a symmetric pattern: each row takes the smallest colour
+// not held by a lower-numbered neighbour (hybrid_amg.cuh:195-215)
+void amg_colours(const CsrHost& A, std::vector<int32_t>& off, std::vector<int32_t>& rows) {
+  std::vector<int> colour((size_t)A.n, -1), mark;
+  int nc = 0;
+  for (int i = 0; i < A.n; ++i) {
+    for (int64_t k = A.row[(size_t)i]; k < A.row[(size_t)i + 1]; ++k) {
+      const int j = A.col[(size_t)k];
+      if (j >= i) continue;
+      const int c = colour[(size_t)j];
+      if (c >= (int)mark.size()) mark.resize((size_t)c + 32, -1);
+      mark[(size_t)c] = i;
+    }
+    int c = 0;
+    while (c < (int)mark.size() && mark[(size_t)c] == i) ++c;
+    colour[(size_t)i] = c;
+    nc = std::max(nc, c + 1);
+  }
+  off.assign((size_t)nc + 1, 0);
+  for (int c : colour) ++off[(size_t)c + 1];
+  for (int c = 0; c < nc; ++c) off[(size_t)c + 1] += off[(size_t)c];
+  rows.resize((size_t)A.n);
+  std::vector<int32_t> next(off.begin(), off.end() - 1);
+  for (int i = 0; i < A.n; ++i) rows[(size_t)next[(size_t)colour[(size_t)i]]++] = i;
+}
+
+std::vector<int32_t> rows32(const std::vector<int64_t>& r) {
+  std::vector<int32_t> o(r.size());
+  for (size_t i = 0; i < r.size(); ++i) {
+    if (r[i] > INT32_MAX) throw std::runtime_error("AMG level too large for 32-bit row offsets");
+    o[i] = (int32_t)r[i];
+  }
+  return o;
+}
+
+struct AmgLevel {
+  int n = 0;
+  Buf<int32_t> row, col, dpos, crows;
+  Buf<double> val, diag, l1, b, x, r, tmp, corr;
+  Buf<double> r2, corr2;  // post-smoothing work vectors of the separate-buffer V-cycle
+  std::vector<int32_t> coff;
+  AmgLevel(const CsrHost& A, bool colour)
+      : n(A.n), row(rows32(A.row)), col(A.col), val(A.val), diag(A.diag), b((size_t)A.n), x((size_t)A.n),
+        r((size_t)A.n), tmp((size_t)A.n), corr((size_t)A.n), r2((size_t)A.n), corr2((size_t)A.n) {
+    std::vector<int32_t> dp((size_t)n, -1);
+    std::vector<double> l((size_t)n, 0.0);
+    for (int i = 0; i < n; ++i)
+      for (int64_t k = A.row[(size_t)i]; k < A.row[(size_t)i + 1]; ++k) {
+        if (A.col[(size_t)k] == i) dp[(size_t)i] = (int32_t)k;
+        l[(size_t)i] += std::abs(A.val[(size_t)k]);
+      }
+    for (int v : dp)
+      if (v < 0) throw std::runtime_error("AMG level without a diagonal entry");
+    dpos.upload(dp);
+    l1.upload(l);
+    if (colour) {
+      std::vector<int32_t> rows;
+      amg_colours(A, coff, rows);
+      crows.upload(rows);
+    }
+  }
+  void apply(const double* in, double* out) const {
+    amg_csr_add<<<grid((long long)n * 32), kTPB>>>(n, row.p, col.p, val.p, in, out, 0);
+    NDS_LAUNCH();
+  }
+};
+struct AmgTransfer {
+  int nf, nc;
+  Buf<int32_t> prow, pcol, rrow, rcol;
+  Buf<double> pval, rval;
+  explicit AmgTransfer(const Transfer& P) : nf(P.nf), nc(P.nc), prow(rows32(P.row)), pcol(P.col), pval(P.val) {
+    // R = P^T, rows ascending in the fine index
+    std::vector<int32_t> rr((size_t)nc + 1, 0), rc(P.col.size());
+    std::vector<double> rv(P.col.size());
+    for (int32_t c : P.col) ++rr[(size_t)c + 1];
+    for (int c = 0; c < nc; ++c) rr[(size_t)c + 1] += rr[(size_t)c];
+    std::vector<int32_t> next(rr.begin(), rr.end() - 1);
+    for (int i = 0; i < nf; ++i)
+      for (int64_t k = P.row[(size_t)i]; k < P.row[(size_t)i + 1]; ++k) {
+        const int32_t q = next[(size_t)P.col[(size_t)k]]++;
+        rc[(size_t)q] = i;
+        rv[(size_t)q] = P.val[(size_t)k];
+      }
+    rrow.upload(rr);
+    rcol.upload(rc);
+    rval.upload(rv);
+  }
+  void restrict_to(const double* f, double* c) const {
+    amg_csr_add<<<grid((long long)nc * 32), kTPB>>>(nc, rrow.p, rcol.p, rval.p, f, c, 0);
+    NDS_LAUNCH();
+  }
+  void prolong_add(const double* c, double* f) const {
+    amg_csr_add<<<grid((long long)nf * 32), kTPB>>>(nf, prow.p, pcol.p, pval.p, c, f, 1);
+    NDS_LAUNCH();
+  }
+};
+
+struct HybridAmgDevice {
+  const nds_hybrid_flow_options& o;
+  int pin;
+  std::unique_ptr<AmgLevel> fine;
+  Buf<int32_t> erow;
+  std::vector<std::unique_ptr<AmgLevel>> L;
+  std::vector<std::unique_ptr<AmgTransfer>> P;
+  Buf<double> tinv;
+  int tn = 0;
+  double fine_lambda = 0;
+  std::vector<double> level_lambda;
+  HybridAmgDevice(const HybridSchurCsr& F, const Hierarchy& H, int pin_, const nds_hybrid_flow_options& opt)
+      : o(opt), pin(pin_), erow(F.entry_row), tinv(H.terminal_inv), tn(H.terminal_n), fine_lambda(H.fine_lambda),
+        level_lambda(H.level_lambda) {
+    const bool mc = o.amg_smoother == NDS_SM_MCGS;
+    fine = std::make_unique<AmgLevel>(F.A, mc);
+    for (size_t l = 0; l < H.A.size(); ++l) L.push_back(std::make_unique<AmgLevel>(H.A[l], mc && l + 1 < H.A.size()));
+    for (const auto& t : H.P) P.push_back(std::make_unique<AmgTransfer>(t));
+    if (L.empty() || P.size() != L.size() || tn != L.back()->n) throw std::runtime_error("AMG hierarchy shape");
+  }
+  void refresh(const Div& B, const double* rau, int* bad) {
+    const int nnz = (int)fine->val.n;
+    amg_fine_refresh<<<grid(nnz), kTPB>>>(nnz, erow.p, fine->col.p, B.row.p, B.col.p, B.bx.p, B.by.p, B.bz.p, rau,
+                                          pin, fine->val.p);
+    amg_diag_l1<<<grid(fine->n), kTPB>>>(fine->n, fine->row.p, fine->dpos.p, fine->val.p, fine->diag.p, fine->l1.p,
+                                         bad);
+    NDS_LAUNCH();
+  }
+  static double cheb_root(double hi, double lo, int k, int degree) {
+    const double centre = 0.5 * (hi + lo), radius = 0.5 * (hi - lo), pi = 3.141592653589793238462643383279502884;
+    return centre - radius * std::cos(pi * (2.0 * k + 1.0) / (2.0 * degree));
+  }
+  // zero initial guess: x = S b.  The work vectors are passed as the
+  // reference passes them (hybrid_amg.cuh:445-506): its post-smoothing calls
+  // hand the same vector as x and corr (and, on the fine level, as b and r),
+  // and the in-place updates below reproduce what that aliasing computes.
+  void smooth(AmgLevel& A, const double* b, double* x, double* tmp, double* r, double* corr, int sweeps,
+              double lambda) {
+    const int n = A.n;
+    if (o.amg_smoother == NDS_SM_MCGS) {
+      NDS_CUDA(cudaMemsetAsync(x, 0, (size_t)n * sizeof(double)));
+      auto one = [&](bool forward) {
+        const int nc = (int)A.coff.size() - 1;
+        for (int q = 0; q < nc; ++q) {
+          const int c = forward ? q : nc - 1 - q;
+          const int beg = A.coff[(size_t)c], cnt = A.coff[(size_t)c + 1] - beg;
+          amg_gs_colour<<<grid((long long)cnt * 32), kTPB>>>(cnt, A.crows.p + beg, A.row.p, A.col.p, A.val.p,
+                                                             A.diag.p, b, x, o.amg_mcgs_omega);
+        }
+      };
+      for (int s = 0; s < sweeps; ++s) {
+        if (o.amg_mcgs_order == NDS_MCGS_SYMMETRIC) {
+          one(true);
+          one(false);
+        } else {
+          one(o.amg_mcgs_order == NDS_MCGS_FORWARD);
+        }
+      }
+      NDS_LAUNCH();
+      return;
+    }
+    if (o.amg_smoother == NDS_SM_JACOBI || o.amg_smoother == NDS_SM_L1JACOBI) {
+      const double* den = o.amg_smoother == NDS_SM_L1JACOBI ? A.l1.p : A.diag.p;
+      amg_jacobi_set<<<grid(n), kTPB>>>(n, o.amg_jacobi_omega, b, den, x);
+      for (int s = 1; s < sweeps; ++s) {
+        A.apply(x, tmp);
+        residual<<<grid(n), kTPB>>>(n, b, tmp, r);
+        amg_jacobi_add<<<grid(n), kTPB>>>(n, o.amg_jacobi_omega, r, den, x);
+      }
+      NDS_LAUNCH();
+      return;
+    }
+    const double lo = o.amg_lambda_low_fraction * lambda;
+    if (!(lambda > lo && lo > 0)) throw std::runtime_error("AMG Chebyshev interval invalid");
+    const int deg = o.amg_cheb_degree;
+    amg_scale_rhs<<<grid(n), kTPB>>>(n, b, A.diag.p, r);
+    amg_scaled_copy<<<grid(n), kTPB>>>(n, 1.0 / cheb_root(lambda, lo, 0, deg), r, x);
+    for (int k = 1; k < deg; ++k) {
+      amg_unscale<<<grid(n), kTPB>>>(n, x, A.diag.p, tmp);
+      A.apply(tmp, corr);
+      amg_unscale_inplace<<<grid(n), kTPB>>>(n, corr, A.diag.p);
+      amg_cheb_add<<<grid(n), kTPB>>>(n, 1.0 / cheb_root(lambda, lo, k, deg), r, corr, x);
+    }
+    amg_unscale<<<grid(n), kTPB>>>(n, x, A.diag.p, x);
+    NDS_LAUNCH();
+  }
+  // post = true: the post-smoothing call; with amg_separate_post it gets work
+  // vectors of its own, which makes the V-cycle symmetric
+  void smooth_fine(const double* b, double* x, bool post = false) {
+    AmgLevel& F = *fine;
+    const bool sep = post && o.amg_separate_post;
+    smooth(F, b, x, F.tmp.p, sep ? F.r2.p : F.r.p, sep ? F.corr2.p : F.corr.p,
+           o.amg_smoother == NDS_SM_MCGS ? o.amg_mcgs_fine_sweeps : o.amg_jacobi_fine_sweeps, fine_lambda);
+  }
+  void smooth_coarse(size_t l, const double* b, double* x, bool post = false) {
+    AmgLevel& A = *L[l];
+    const bool sep = post && o.amg_separate_post;
+    smooth(A, b, x, A.tmp.p, sep ? A.r2.p : A.r.p, sep ? A.corr2.p : A.corr.p,
+           o.amg_smoother == NDS_SM_MCGS ? o.amg_mcgs_coarse_sweeps : o.amg_jacobi_coarse_sweeps,
+           l < level_lambda.size() ? level_lambda[l] : 0.0);
+  }
+  void vcycle(size_t l, const double* b, double* x) {
+    AmgLevel& A = *L[l];
+    if (l + 1 == L.size()) {
+      amg_dense<<<grid((long long)A.n * 32), kTPB>>>(A.n, tinv.p, b, x);
+      NDS_LAUNCH();
+      return;
+    }
+    smooth_coarse(l, b, x);
+    A.apply(x, A.tmp.p);
+    residual<<<grid(A.n), kTPB>>>(A.n, b, A.tmp.p, A.r.p);
+    AmgLevel& Cn = *L[l + 1];
+    P[l + 1]->restrict_to(A.r.p, Cn.b.p);
+    vcycle(l + 1, Cn.b.p, Cn.x.p);
+    P[l + 1]->prolong_add(Cn.x.p, x);
+    A.apply(x, A.tmp.p);
+    residual<<<grid(A.n), kTPB>>>(A.n, b, A.tmp.p, A.r.p);
+    NDS_CUDA(cudaMemcpyAsync(A.b.p, A.r.p, (size_t)A.n * sizeof(double), cudaMemcpyDeviceToDevice));
+    smooth_coarse(l, A.b.p, A.corr.p, true);
+    amg_axpy<<<grid(A.n), kTPB>>>(A.n, A.corr.p, x);
+    NDS_LAUNCH();
+  }
+  // z = V-cycle(b) with the fine smoother on both sides
+  void apply(const double* b, double* z) {
+    AmgLevel& F = *fine;
+    smooth_fine(b, z);
+    F.apply(z, F.tmp.p);
+    residual<<<grid(F.n), kTPB>>>(F.n, b, F.tmp.p, F.r.p);
+    AmgLevel& C0 = *L[0];
+    P[0]->restrict_to(F.r.p, C0.b.p);
+    vcycle(0, C0.b.p, C0.x.p);
+    P[0]->prolong_add(C0.x.p, z);
+    F.apply(z, F.tmp.p);
+    residual<<<grid(F.n), kTPB>>>(F.n, b, F.tmp.p, F.r.p);
+    smooth_fine(F.r.p, F.corr.p, true);
+    amg_axpy<<<grid(F.n), kTPB>>>(F.n, F.corr.p, z);
+    NDS_LAUNCH();
+  }
+};
+
+// AMG-preconditioned CG on the pinned pressure system
+// (hybrid_amg.cuh:535-580): stops at max(atol, rtol ||r0||)
+template <class Op>
+CgResult pcg_amg(Op& A, HybridAmgDevice& M, const double* rhs, double* x, double rtol, double atol, int maxit,
+                 CgWork& W, int pin) {
+  const int n = W.n;
+  A.apply(x, W.q.p);
+  residual<<<grid(n), kTPB>>>(n, rhs, W.q.p, W.r.p);
+  NDS_LAUNCH();
+  set_at<<<1, 1>>>(pin, 0.0, W.r.p);
+  const double r0 = W.red.norm(W.r.p);
+  if (!std::isfinite(r0)) throw std::runtime_error("mixed-mesh pressure PCG: initial residual not finite");
+  if (r0 <= atol) return {0, 0, true};
+  const double target = std::max(atol, rtol * r0);
+  M.apply(W.r.p, W.z.p);
+  set_at<<<1, 1>>>(pin, 0.0, W.z.p);
+  NDS_CUDA(cudaMemcpy(W.p.p, W.z.p, n * sizeof(double), cudaMemcpyDeviceToDevice));
+  double rho = W.red.dot(W.r.p, W.z.p);
+  if (!(rho > 0) || !std::isfinite(rho)) throw std::runtime_error("mixed-mesh pressure PCG: initial rho nonpositive");
+  CgResult R;
+  for (int k = 0; k < maxit; ++k) {
+    A.apply(W.p.p, W.q.p);
+    const double pq = W.red.dot(W.p.p, W.q.p);
+    if (!(pq > 0) || !std::isfinite(pq)) throw std::runtime_error("mixed-mesh pressure PCG pAp nonpositive");
+    axpy2<<<grid(n), kTPB>>>(n, rho / pq, W.p.p, W.q.p, x, W.r.p);
+    NDS_LAUNCH();
+    set_at<<<1, 1>>>(pin, 0.0, x);
+    set_at<<<1, 1>>>(pin, 0.0, W.r.p);
+    const double rn = W.red.norm(W.r.p);
+    R.its = k + 1;
+    R.rel = rn / r0;
+    if (rn <= target) {
+      R.ok = true;
+      break;
+    }
+    M.apply(W.r.p, W.z.p);
+    set_at<<<1, 1>>>(pin, 0.0, W.z.p);
+    const double nr = W.red.dot(W.r.p, W.z.p);
+    if (!(nr > 0) || !std::isfinite(nr)) throw std::runtime_error("mixed-mesh pressure PCG rho nonpositive");
+    xpby<<<grid(n), kTPB>>>(n, nr / rho, W.z.p, W.p.p);
+    NDS_LAUNCH();
+    set_at<<<1, 1>>>(pin, 0.0, W.p.p);
+    rho = nr;
+  }
+  return R;
+}
+
 void run_flow(const char* path, const nds_hybrid_flow_options& o, int verbose, nds_hybrid_flow_report* out,
               double* const fields[4]) {
   const HybridMesh M = read_hxt1_hybrid(path);
@@ -718,7 +1126,7 @@ void run_flow(const char* path, const nds_hybrid_flow_options& o, int verbose, n
   Buf<double> u0(F.u0), u1(F.u1), u2(F.u2), conv((size_t)nnz), val((size_t)nnz), dorig((size_t)nv), rau((size_t)nv),
       isd((size_t)np), p((size_t)np), dp((size_t)np), cont((size_t)np), bt0((size_t)nv), bt1((size_t)nv),
       bt2((size_t)nv), r0((size_t)nv), r1((size_t)nv), r2((size_t)nv), tmp((size_t)nv), res((size_t)nv);
-  Buf<int> d_bad((size_t)1);
+  Buf<int> d_bad((size_t)2);  // [0] momentum rows / hex Jacobians, [1] refreshed pressure matrix
   Div B(Hb);
   Schur S(B, rau.p, pin);
   Reducer pred(np), ured(nv);
@@ -734,12 +1142,12 @@ void run_flow(const char* path, const nds_hybrid_flow_options& o, int verbose, n
     std::printf("NODALS_HXT4B_CONFIG precision=fp64 geometry=fp64 reductions=fp64 cellsHex=%d cellsTet=%d velocityDofs=%d "
                 "pressureDofs=%d csrNnz=%d colors=%d maxColor=%d Re=%.12g bulk=%.12g nu=%.12e D=%.12e L=%.12e gamma=%.6g "
                 "convection=CENTRAL_ADVECTIVE_LAGGED interfaceConvection=VOLUME_ONLY_TANGENTIAL_RE20_GATE momentumWork=%s "
-                "momOmega=%.6g momRtol=%.3e momAtol=%.3e fixedWorkIgnoresMomTolerances=1 pressureSolver=PCG_JACOBI "
+                "momOmega=%.6g momRtol=%.3e momAtol=%.3e fixedWorkIgnoresMomTolerances=1 pressureSolver=%s "
                 "momentumSign=A_u_MINUS_BT_p pRtol=%.3e pAtol=%.3e pMax=%d alphaU=%.6g alphaP=%.6g rauScale=%.6g "
                 "rauPenaltyIncluded=0 simpleTol=%.3e status=PASS\n",
                 nh, nt, nv, np, nnz, ncol, F.max_colour, o.re, o.bulk, F.nu, F.diameter, F.length, o.gamma, work,
-                o.mom_omega, o.mom_rtol, o.mom_atol, o.p_rtol, o.p_atol, o.p_max, o.alpha_u, o.alpha_p, o.rau_scale,
-                o.simple_tol);
+                o.mom_omega, o.mom_rtol, o.mom_atol, o.pressure_solver == 1 ? "PCG_AMG" : "PCG_JACOBI", o.p_rtol,
+                o.p_atol, o.p_max, o.alpha_u, o.alpha_p, o.rau_scale, o.simple_tol);
     std::printf("NODALS_HXT4B_HAGEN_POISEUILLE expectedDpDz=%.12e expectedDropPinMinusPout=%.12e inlet=STRONG_PARABOLIC "
                 "wall=STRONG_NOSLIP outlet=NATURAL_TRACTION pressureGaugePin=%d status=PASS\n",
                 dpdz_exact, drop_exact, pin);
@@ -760,12 +1168,8 @@ void run_flow(const char* path, const nds_hybrid_flow_options& o, int verbose, n
       sweep(x, rhs, false);
     }
   };
-  const auto t0 = std::chrono::steady_clock::now();
-  double c0 = -1, rel = 1;
-  bool conv_ok = false;
-  int outer = 0;
-  long long pits = 0;
-  for (int it = 1; it <= o.max_outer; ++it) {
+  // lagged convection of the current velocity, relaxed rows and rAU
+  auto assemble = [&]() {
     hex_conv_local<<<std::max(nh, 1), kTPB>>>(nh, d_xyz.p, d_hexes.p, d_hdofs.p, u0.p, u1.p, u2.p, d_local.p, d_bad.p);
     NDS_LAUNCH();
     if (nt) {
@@ -777,11 +1181,50 @@ void run_flow(const char* path, const nds_hybrid_flow_options& o, int verbose, n
     flow_rows<<<grid(nv), kTPB>>>(nv, d_row.p, d_dpos.p, d_fixed.p, d_base.p, conv.p, d_dr.p, o.alpha_u, o.rau_scale,
                                   val.p, dorig.p, rau.p, d_bad.p);
     NDS_LAUNCH();
-    int bad = 0;
-    NDS_CUDA(cudaMemcpy(&bad, d_bad.p, sizeof(int), cudaMemcpyDeviceToHost));
-    if (bad) throw std::runtime_error("mixed-mesh SIMPLE: nonpositive momentum diagonal or hex Jacobian");
-    schur_diag_inv<<<grid(np), kTPB>>>(np, B.row.p, B.col.p, B.bx.p, B.by.p, B.bz.p, rau.p, pin, isd.p);
-    NDS_LAUNCH();
+  };
+  auto check_bad = [&]() {
+    int bad[2] = {0, 0};
+    NDS_CUDA(cudaMemcpy(bad, d_bad.p, sizeof(bad), cudaMemcpyDeviceToHost));
+    if (bad[0]) throw std::runtime_error("mixed-mesh SIMPLE: nonpositive momentum diagonal or hex Jacobian");
+    if (bad[1]) throw std::runtime_error("mixed-mesh SIMPLE: refreshed pressure matrix has an invalid diagonal");
+  };
+  // AMG preconditioner: hierarchy from the initial rAU, as the reference's
+  // turbulent entry builds it before its loop (hxt5b_main.cu:185-212)
+  std::unique_ptr<HybridAmgDevice> amg;
+  if (o.pressure_solver == 1) {
+    const AmgOptions ao = hybrid_amg_options(o);
+    assemble();
+    check_bad();
+    std::vector<double> rau_h((size_t)nv);
+    NDS_CUDA(cudaMemcpy(rau_h.data(), rau.p, nv * sizeof(double), cudaMemcpyDeviceToHost));
+    const HybridSchurCsr FS = hybrid_schur_csr(Hb, pin, rau_h);
+    const Hierarchy HH = build_cf_hierarchy(FS.A, ao);
+    amg = std::make_unique<HybridAmgDevice>(FS, HH, pin, o);
+    if (verbose) {
+      static const char* sm[] = {"cheb2", "jacobi", "l1jacobi", "mcgs"};
+      std::printf("NODALS_HXT4C_FINE_HOST rows=%d nnz=%zu avgNnz=%.6f pin=%d source=B_DIAG_RAU_BT_REDUCED_PIN "
+                  "status=PASS\n",
+                  FS.A.n, FS.A.val.size(), FS.A.n ? (double)FS.A.val.size() / FS.A.n : 0.0, pin);
+      std::printf("NODALS_HXT4C_AMG_UPLOAD levels=%zu transfers=%zu terminal=%d smoother=%s chebScaling=%s "
+                  "status=PASS\n",
+                  HH.A.size(), HH.P.size(), HH.terminal_n, sm[o.amg_smoother],
+                  o.amg_smoother == NDS_SM_CHEB2 ? "SYMMETRIC_D_HALF" : "NA");
+    }
+  }
+  const auto t0 = std::chrono::steady_clock::now();
+  double c0 = -1, rel = 1;
+  bool conv_ok = false;
+  int outer = 0;
+  long long pits = 0;
+  for (int it = 1; it <= o.max_outer; ++it) {
+    assemble();
+    if (amg) {
+      amg->refresh(B, rau.p, d_bad.p + 1);
+    } else {
+      schur_diag_inv<<<grid(np), kTPB>>>(np, B.row.p, B.col.p, B.bx.p, B.by.p, B.bz.p, rau.p, pin, isd.p);
+      NDS_LAUNCH();
+    }
+    check_bad();
     B.BT(p.p, bt0.p, bt1.p, bt2.p);
     flow_rhs<<<grid(nv), kTPB>>>(nv, d_fixed.p, bt0.p, u0.p, dorig.p, o.alpha_u, r0.p);
     flow_rhs<<<grid(nv), kTPB>>>(nv, d_fixed.p, bt1.p, u1.p, dorig.p, o.alpha_u, r1.p);
@@ -797,7 +1240,8 @@ void run_flow(const char* path, const nds_hybrid_flow_options& o, int verbose, n
     if (it == 1) c0 = cn;
     rel = cn / std::max(c0, 1e-300);
     NDS_CUDA(cudaMemset(dp.p, 0, np * sizeof(double)));
-    const CgResult pr = pcg_prod(S, cont.p, dp.p, isd.p, o.p_rtol, o.p_atol, o.p_max, WP, pin);
+    const CgResult pr = amg ? pcg_amg(S, *amg, cont.p, dp.p, o.p_rtol, o.p_atol, o.p_max, WP, pin)
+                            : pcg_prod(S, cont.p, dp.p, isd.p, o.p_rtol, o.p_atol, o.p_max, WP, pin);
     if (!pr.ok) throw std::runtime_error("mixed-mesh SIMPLE: pressure PCG missed its target within p_max");
     pits += pr.its;
     p_update_minus<<<grid(np), kTPB>>>(np, pin, o.alpha_p, dp.p, p.p);
@@ -873,6 +1317,57 @@ void run_flow(const char* path, const nds_hybrid_flow_options& o, int verbose, n
 }  // namespace hy
 }  // namespace nds
 
+namespace nds {
+namespace hy {
+void run_amg_vcycle(const char* path, const double* rau_in, const nds_hybrid_flow_options& o, const double* b,
+                    double* z) {
+  const AmgOptions ao = hybrid_amg_options(o);
+  const HybridMesh M = read_hxt1_hybrid(path);
+  HybridStokes Hb;
+  build_hybrid_divergence(M, interface_plans(M), Hb);
+  const int pin = hybrid_pin(M), np = Hb.np;
+  const std::vector<double> rau_h(rau_in, rau_in + Hb.nvel);
+  const HybridSchurCsr FS = hybrid_schur_csr(Hb, pin, rau_h);
+  const Hierarchy HH = build_cf_hierarchy(FS.A, ao);
+  HybridAmgDevice amg(FS, HH, pin, o);
+  Div B(Hb);
+  Buf<double> rau(rau_h), db(std::vector<double>(b, b + np)), dz((size_t)np);
+  Buf<int> bad((size_t)1);
+  amg.refresh(B, rau.p, bad.p);
+  int nb = 0;
+  NDS_CUDA(cudaMemcpy(&nb, bad.p, sizeof(int), cudaMemcpyDeviceToHost));
+  if (nb) throw std::runtime_error("pressure matrix has an invalid diagonal");
+  amg.apply(db.p, dz.p);
+  NDS_CUDA(cudaMemcpy(z, dz.p, np * sizeof(double), cudaMemcpyDeviceToHost));
+}
+}  // namespace hy
+}  // namespace nds
+
+extern "C" int nds_hybrid_amg_vcycle(const char* hxt1_path, const double* rau, const nds_hybrid_flow_options* o,
+                                     int device, const double* b, double* z) {
+  if (!hxt1_path || !rau || !o || !b || !z) {
+    nds::set_error("nds_hybrid_amg_vcycle: null argument");
+    return NDS_E_INVALID;
+  }
+  try {
+    int ndev = 0;
+    const cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev <= device) throw nds::CudaError(std::string("no CUDA device available: ") + cudaGetErrorString(e));
+    NDS_CUDA(cudaSetDevice(device));
+    nds::hy::run_amg_vcycle(hxt1_path, rau, *o, b, z);
+    return NDS_OK;
+  } catch (const std::invalid_argument& e) {
+    nds::set_error(e.what());
+    return NDS_E_INVALID;
+  } catch (const nds::CudaError& e) {
+    nds::set_error(e.what());
+    return NDS_E_CUDA;
+  } catch (const std::exception& e) {
+    nds::set_error(e.what());
+    return NDS_E_SETUP;
+  }
+}
+
 extern "C" int nds_hybrid_stokes_gate(const char* hxt1_path, double nu, double gamma, double rau_scale, double alpha_p,
                                       double simple_tol, int max_outer, int device, int verbose,
                                       nds_hybrid_report* out) {
@@ -933,6 +1428,7 @@ extern "C" void nds_hybrid_flow_defaults(nds_hybrid_flow_options* o) {
   o->amg_lambda_low_fraction = 0.05;
   o->amg_jacobi_omega = 0.7;
   o->amg_mcgs_omega = 1.0;
+  o->amg_separate_post = 0;
 }
 
 extern "C" int nds_hybrid_flow(const char* hxt1_path, const nds_hybrid_flow_options* o, int device, int verbose,
@@ -945,7 +1441,7 @@ extern "C" int nds_hybrid_flow_fields(const char* hxt1_path, const nds_hybrid_fl
                                       double* pressure) {
   if (!hxt1_path || !o || !(o->re > 0) || !(o->bulk > 0) || !(o->gamma > 0) || !(o->alpha_u > 0 && o->alpha_u <= 1) ||
       !(o->alpha_p > 0) || !(o->rau_scale > 0) || o->max_outer < 1 || o->p_max < 1 || o->momentum_work < 0 ||
-      o->momentum_work > 2) {
+      o->momentum_work > 2 || o->pressure_solver < 0 || o->pressure_solver > 1) {
     nds::set_error("nds_hybrid_flow: bad argument");
     return NDS_E_INVALID;
   }
@@ -957,6 +1453,9 @@ extern "C" int nds_hybrid_flow_fields(const char* hxt1_path, const nds_hybrid_fl
     double* const fields[4] = {u0, u1, u2, pressure};
     nds::hy::run_flow(hxt1_path, *o, verbose, out, fields);
     return NDS_OK;
+  } catch (const std::invalid_argument& e) {
+    nds::set_error(e.what());
+    return NDS_E_INVALID;
   } catch (const nds::CudaError& e) {
     nds::set_error(e.what());
     return NDS_E_CUDA;

@@ -128,7 +128,8 @@ class HybridFlowOptions(C.Structure):
                                           "amg_jacobi_coarse_sweeps", "amg_mcgs_fine_sweeps", "amg_mcgs_coarse_sweeps",
                                           "amg_mcgs_order", "cf_pmax", "cf_interp", "cf_aggressive_first")]
                 + [(n, C.c_double) for n in ("cf_theta", "amg_lambda_safety", "amg_lambda_low_fraction",
-                                             "amg_jacobi_omega", "amg_mcgs_omega")])
+                                             "amg_jacobi_omega", "amg_mcgs_omega")]
+                + [("amg_separate_post", C.c_int)])
 
     @classmethod
     def make(cls, **kw) -> "HybridFlowOptions":
@@ -186,6 +187,8 @@ def lib():
         L.nds_hybrid_amg_create.argtypes = [C.c_char_p, vp, C.POINTER(HybridFlowOptions), C.POINTER(vp)]
         L.nds_hybrid_amg_array.argtypes = [vp, C.c_char_p, C.POINTER(_Array)]
         L.nds_hybrid_amg_destroy.argtypes = [vp]
+        if hasattr(L, "nds_hybrid_amg_vcycle"):
+            L.nds_hybrid_amg_vcycle.argtypes = [C.c_char_p, vp, C.POINTER(HybridFlowOptions), C.c_int, vp, vp]
         if hasattr(L, "nds_hybrid_flow_fields"):
             L.nds_hybrid_flow_fields.argtypes = [C.c_char_p, C.POINTER(HybridFlowOptions), C.c_int, C.c_int,
                                                  C.POINTER(HybridFlowReport), vp, vp, vp, vp]
@@ -277,6 +280,17 @@ def hybrid_flow(path, options: HybridFlowOptions | None = None, device: int = 0,
     _check(lib().nds_hybrid_flow_fields(str(path).encode(), C.byref(o), device, verbose, C.byref(r),
                                         *[_p(x) for x in (*u, p)]))
     return r, u[0], u[1], u[2], p
+
+
+def hybrid_amg_vcycle(path, rau: np.ndarray, b: np.ndarray, options: HybridFlowOptions | None = None, device: int = 0,
+                      **kw) -> np.ndarray:
+    """z = M^-1 b for the mixed-mesh pressure AMG built and refreshed from rau (GPU)."""
+    o = options if options is not None else HybridFlowOptions.make(**kw)
+    r = np.ascontiguousarray(rau, dtype=np.float64)
+    bb = np.ascontiguousarray(b, dtype=np.float64)
+    z = np.zeros_like(bb)
+    _check(lib().nds_hybrid_amg_vcycle(str(path).encode(), _p(r), C.byref(o), device, _p(bb), _p(z)))
+    return z
 
 
 class HybridAmg:

@@ -10,7 +10,11 @@
 //   hxt4c::build_hybrid_fine_host          hybrid_hxt5b/hybrid_amg.cuh:63
 //   nodals_gpu::build_cf_hierarchy_from_csr hybrid_hxt5b/hybrid_cf_overload.inc:5
 // with the HXT4B pressure pin (hybrid_hxt4b/hxt4b_main.cu:236) and an rAU
-// vector read from a file of nvel doubles.  No CUDA runtime call is made.
+// vector read from a file of nvel doubles.  No CUDA runtime call is made
+// unless --apply is given: then the reference's device preconditioner
+// (hxt4c::HybridAMG, hybrid_amg.cuh:353-533) is built from that hierarchy,
+// refreshed from rAU on the device and applied once to the np doubles of the
+// --apply file, and the result is written to --z-out (needs a CUDA device).
 #define HXT4B_EMBED_MAIN hxt4b_embedded_main
 #include "hybrid_hxt4b/hxt4b_main.cu"
 #undef HXT4B_EMBED_MAIN
@@ -50,7 +54,10 @@ struct Writer {
 
 int main(int argc, char** argv) {
   try {
-    std::string mesh, rauPath, out, interp = "exti";
+    std::string mesh, rauPath, out, interp = "exti", applyPath, zPath;
+    hxt4c::AMGOptions AO;
+    AO.smoother = "cheb2";
+    AO.chebDegree = 4;
     double theta = 0.25, safety = 1.5, lowFrac = 0.05;
     int pmax = 8, terminal = 1000, powerIts = 16, aggressive = 0;
     for (int i = 1; i < argc; ++i) {
@@ -65,6 +72,14 @@ int main(int argc, char** argv) {
       else if (a == "--cf-aggressive-first") aggressive = std::atoi(nx().c_str());
       else if (a == "--amg-terminal") terminal = std::atoi(nx().c_str());
       else if (a == "--amg-power-its") powerIts = std::atoi(nx().c_str());
+      else if (a == "--apply") applyPath = nx();
+      else if (a == "--z-out") zPath = nx();
+      else if (a == "--amg-smoother") AO.smoother = nx();
+      else if (a == "--amg-cheb-degree") AO.chebDegree = std::atoi(nx().c_str());
+      else if (a == "--amg-jacobi-omega") AO.jacobiOmega = std::atof(nx().c_str());
+      else if (a == "--amg-jacobi-fine-sweeps") AO.jacobiFineSweeps = std::atoi(nx().c_str());
+      else if (a == "--amg-jacobi-coarse-sweeps") AO.jacobiCoarseSweeps = std::atoi(nx().c_str());
+      else if (a == "--amg-mcgs-omega") AO.mcgsOmega = std::atof(nx().c_str());
       else throw std::runtime_error("unknown arg " + a);
     }
     if (mesh.empty() || rauPath.empty() || out.empty()) throw std::runtime_error("--mesh, --rau and --out required");
@@ -117,6 +132,29 @@ int main(int argc, char** argv) {
       w.f64(p + "diag", H.csr[l].diag);
     }
     w.f64("amg.terminal_inv", H.terminal_inv);
+    if (!applyPath.empty()) {
+      AO.lambdaLowFraction = lowFrac;
+      std::vector<double> b((std::size_t)B.np), z((std::size_t)B.np);
+      FILE* f = std::fopen(applyPath.c_str(), "rb");
+      if (!f) throw std::runtime_error("cannot open " + applyPath);
+      const size_t got = std::fread(b.data(), sizeof(double), b.size(), f);
+      std::fclose(f);
+      if (got != b.size()) throw std::runtime_error("--apply file holds fewer than np doubles");
+      hxt4a::BDevice<double> Bd(B);
+      hxt4c::HybridAMG<double> PC(F, H, pin, AO);
+      hxt4c::Buf<double> dr, db, dz;
+      dr.upload(rau);
+      db.upload(b);
+      dz.alloc(b.size());
+      PC.refresh(Bd, dr.p);
+      PC.apply(db.p, dz.p);
+      HXT1_CUDA(cudaDeviceSynchronize());
+      dz.download(z);
+      FILE* g = std::fopen(zPath.c_str(), "wb");
+      if (!g) throw std::runtime_error("cannot open " + zPath);
+      std::fwrite(z.data(), sizeof(double), z.size(), g);
+      std::fclose(g);
+    }
     std::printf("NDS_REF_HYBRID_AMG_DUMP np=%d nv=%d pin=%d fineNnz=%zu levels=%zu status=PASS\n", B.np, B.nv, pin,
                 F.A.val.size(), H.csr.size());
     return 0;

@@ -8,6 +8,11 @@ vector ``rau(g) = 0.02 (1.5 + sin(0.37 (g + 1)))`` and keeps, per case, the
 pressure matrix (first case only) and the CF hierarchy as
 ``hybrid_amg_r2.npz`` (keys ``<case>/<array>``).  Runs on the CPU; needs
 the reference tree only through the built harness.
+
+With ``--vcycle`` (needs a CUDA device) it also applies the reference's device
+preconditioner once, for each smoother case of ``VCYCLES``, to the seeded
+vector ``b`` (standard normal from seed 11, zero at the pin) and keeps ``b``
+and each ``z = M^-1 b`` as ``hybrid_amg_vcycle_r2.npz``.
 """
 from __future__ import annotations
 
@@ -33,6 +38,17 @@ CASES = {
 }
 
 
+# V-cycle case -> (hierarchy case, harness smoother flags)
+VCYCLES = {
+    "cheb2": ("exti_t60", ["--amg-smoother", "cheb2"]),
+    "cheb2_deg3_aggr": ("direct_aggr_t40", ["--amg-smoother", "cheb2", "--amg-cheb-degree", "3"]),
+    "jacobi_2sweeps": ("exti_t60", ["--amg-smoother", "jacobi", "--amg-jacobi-fine-sweeps", "2",
+                                    "--amg-jacobi-coarse-sweeps", "2", "--amg-jacobi-omega", "0.6"]),
+    "l1jacobi": ("exti_t60", ["--amg-smoother", "l1jacobi"]),
+    "mcgs": ("exti_t60", ["--amg-smoother", "mcgs", "--amg-mcgs-omega", "0.9"]),
+}
+
+
 def rau_of(nvel: int) -> np.ndarray:
     g = np.arange(nvel, dtype=np.float64)
     return 0.02 * (1.5 + np.sin(0.37 * (g + 1)))
@@ -54,6 +70,28 @@ def main() -> None:
                 if not k.startswith("b.") and (case == "exti_t60" or not k.startswith("fine.")):
                     out[f"{case}/{k}"] = v
     np.savez_compressed(HERE / "hybrid_amg_r2.npz", **out)
+    if "--vcycle" in sys.argv[1:]:
+        vcycles(nvel)
+
+
+def vcycles(nvel: int) -> None:
+    z = np.load(HERE / "hybrid_amg_r2.npz")
+    pin = int(z["exti_t60/pin"][0])
+    npres = len(z["exti_t60/fine.diag"])
+    b = np.random.default_rng(11).standard_normal(npres)
+    b[pin] = 0.0
+    out = {"b": b}
+    with tempfile.TemporaryDirectory() as td:
+        rp, bp = Path(td) / "rau.bin", Path(td) / "b.bin"
+        rau_of(nvel).astype("<f8").tofile(rp)
+        b.astype("<f8").tofile(bp)
+        for name, (case, flags) in VCYCLES.items():
+            zp = Path(td) / f"{name}.z"
+            subprocess.run([str(ROOT / "oracle" / "_ref" / "ref_hybrid_amg_dump"), "--mesh", str(MESH), "--rau", str(rp),
+                            "--out", str(Path(td) / "dump.bin"), *CASES[case], *flags, "--apply", str(bp),
+                            "--z-out", str(zp)], check=True, stdout=subprocess.DEVNULL)
+            out[name] = np.fromfile(zp, dtype="<f8")
+    np.savez_compressed(HERE / "hybrid_amg_vcycle_r2.npz", **out)
 
 
 if __name__ == "__main__":

@@ -27,6 +27,12 @@ seeded fields, produces byte for byte the text of the oracle's restatement
 of the reference writer; on the GPU the tight run's file has the reference
 run's layout and integer blocks exactly and its values to 3e-9 of each
 block's largest magnitude (tests/golden/hxt4b_hybrid_r2_tight.vtu.gz).
+
+The AMG-preconditioned pressure solve (--pressure-solver pcg_amg, the
+preconditioner of the reference's turbulent entry) with tight pressure
+solves follows the same tight history with a fifth of the pressure
+iterations or fewer; the reference's own cheb2 V-cycle makes PCG break down on this
+matrix and the run fails as the reference's would.
 """
 from __future__ import annotations
 
@@ -175,3 +181,38 @@ def test_pipe_simple_default_tolerance(tmp_path):
     assert abs(max(gs) - max(ws)) <= 5, (max(gs), max(ws))
     for k in PHYS:
         assert _close(gp[k], wp[k], 5e-3), (k, gp[k], wp[k])
+
+
+AMG = ["--pressure-solver", "pcg_amg"]
+AMG_VARIANTS = {"cheb2_separate_post": AMG + ["--amg-separate-post", "1"], "mcgs": AMG + ["--amg-smoother", "mcgs"]}
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("variant", sorted(AMG_VARIANTS))
+def test_pipe_simple_amg_pressure_tight(tmp_path, variant):
+    """With tight pressure solves the SIMPLE iterates do not depend on the
+    pressure preconditioner: the AMG-preconditioned runs follow the
+    reference's (Jacobi-preconditioned) tight history to 3e-9, with a fifth
+    of its pressure iterations or fewer."""
+    gc, gs, gp = _run_4b(tmp_path / "r2.vtu", "--p-rtol", "1e-10", "--p-max", "400", *AMG_VARIANTS[variant])
+    wc, ws, wp = _parse_4b((GOLDEN / "hxt4b_hybrid_r2_tight.log").read_text())
+    assert gc["pressureSolver"] == "PCG_AMG"
+    assert sorted(gs) == sorted(ws)
+    for it, w in ws.items():
+        for k in ("relCont", "absCont", "zMomentumResidualRel"):
+            assert _close(gs[it][k], w[k], 3e-9), (it, k, gs[it][k], w[k])
+        assert int(gs[it]["pCG"]) * 5 <= int(w["pCG"]), (it, gs[it]["pCG"], w["pCG"])
+    for k in PHYS:
+        assert _close(gp[k], wp[k], 3e-9), (k, gp[k], wp[k])
+
+
+@pytest.mark.gpu
+def test_pipe_simple_reference_cheb2_vcycle_breaks_pcg(tmp_path):
+    """The reference's cheb2 V-cycle (post-smoothing aliasing) is not a
+    positive definite preconditioner of this pressure matrix: PCG reports a
+    nonpositive rho and the executable exits 2, as the reference's pcg_amg
+    throws."""
+    r = subprocess.run([str(ROOT / "nodals_b200" / "_lib" / "nodals_hxt4b_fp64"), "--mesh", str(MESH), "--vtu",
+                        str(tmp_path / "x.vtu"), "--p-max", "400", *AMG], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 2
+    assert "nonpositive" in r.stderr and "HXT4B_GATE_STATUS=FAIL" in r.stderr

@@ -63,3 +63,84 @@ def test_pressure_options_rejected(native, bad):
     with pytest.raises(native.NdsError) as e:
         native.HybridAmg(MESH, _rau(nvel), pressure_solver=1, **bad)
     assert e.value.code == -1  # NDS_E_INVALID
+
+
+# V-cycle cases: (hierarchy case, product options, oracle options); the
+# reference's own device V-cycle results are in hybrid_amg_vcycle_r2.npz
+VCYCLES = {
+    "cheb2": ("exti_t60", {}, {}),
+    "cheb2_deg3_aggr": ("direct_aggr_t40", dict(amg_cheb_degree=3), dict(cheb_degree=3)),
+    "jacobi_2sweeps": ("exti_t60", dict(amg_smoother=1, amg_jacobi_fine_sweeps=2, amg_jacobi_coarse_sweeps=2,
+                                        amg_jacobi_omega=0.6),
+                       dict(smoother="jacobi", jacobi_fine_sweeps=2, jacobi_coarse_sweeps=2, jacobi_omega=0.6)),
+    "l1jacobi": ("exti_t60", dict(amg_smoother=2), dict(smoother="l1jacobi")),
+    "mcgs": ("exti_t60", dict(amg_smoother=3, amg_mcgs_omega=0.9), dict(smoother="mcgs", mcgs_omega=0.9)),
+}
+VGOLD = GOLDEN / "hybrid_amg_vcycle_r2.npz"
+
+
+def _hierarchy(case):
+    z = np.load(GOLD)
+    arr = {k.split("/", 1)[1]: z[k] for k in z.files if k.startswith(case + "/")}
+    for k in z.files:
+        if k.startswith("exti_t60/fine."):
+            arr.setdefault(k.split("/", 1)[1], z[k])
+    return arr
+
+
+def _rel(got, want):
+    return float(np.abs(got - want).max() / np.abs(want).max())
+
+
+@pytest.mark.parametrize("name", sorted(VCYCLES))
+def test_vcycle_oracle_matches_reference_vcycle(name):
+    """The oracle's V-cycle on the reference's hierarchy reproduces the
+    reference's device V-cycle (its restriction sums with atomics: 1e-12)."""
+    from oracle.hybrid_amg import VCycle
+    case, _, oo = VCYCLES[name]
+    v = np.load(VGOLD)
+    z = VCycle(_hierarchy(case), oo).apply(v["b"])
+    assert _rel(z, v[name]) < 1e-12, (name, _rel(z, v[name]))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", sorted(VCYCLES))
+def test_device_vcycle_matches_reference_vcycle(native, name):
+    case, po, _ = VCYCLES[name]
+    v = np.load(VGOLD)
+    nvel = native.hybrid_counts(MESH)[5]
+    z = native.hybrid_amg_vcycle(MESH, _rau(nvel), v["b"], pressure_solver=1, **CASES[case], **po)
+    assert _rel(z, v[name]) < 1e-12, (name, _rel(z, v[name]))
+
+
+def test_separate_post_vcycle_is_symmetric():
+    """With its own post-smoothing work vectors the cheb2 V-cycle is a
+    symmetric operator (x.My = y.Mx); the reference's, whose post-smoothing
+    aliases the result and the Chebyshev product, is not."""
+    from oracle.hybrid_amg import VCycle
+    arr = _hierarchy("exti_t60")
+    pin = int(arr["pin"][0])
+    rng = np.random.default_rng(5)
+    x, y = rng.standard_normal((2, len(arr["fine.diag"])))
+    x[pin] = y[pin] = 0.0
+
+    def gap(opt):
+        V = VCycle(arr, opt)
+        My, Mx = V.apply(y), V.apply(x)
+        return abs(x @ My - y @ Mx) / (np.linalg.norm(x) * np.linalg.norm(My))
+
+    assert gap(dict(separate_post=True)) < 1e-13
+    assert gap({}) > 1e-3
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["cheb2", "jacobi_2sweeps"])
+def test_device_separate_post_vcycle_matches_oracle(native, name):
+    from oracle.hybrid_amg import VCycle
+    case, po, oo = VCYCLES[name]
+    v = np.load(VGOLD)
+    nvel = native.hybrid_counts(MESH)[5]
+    z = native.hybrid_amg_vcycle(MESH, _rau(nvel), v["b"], pressure_solver=1, amg_separate_post=1, **CASES[case],
+                                 **po)
+    want = VCycle(_hierarchy(case), dict(oo, separate_post=True)).apply(v["b"])
+    assert _rel(z, want) < 1e-12, (name, _rel(z, want))
