@@ -65,7 +65,9 @@ def build(verbose: bool = False, jobs: int | None = None) -> Path:
         o = BUILD / (s.stem + ".cu.o")
         objs.append(o)
         if _stale(o, s, newest):
-            jobs_.append([NVCC, *NVFLAGS, "-I", str(CSRC), "-c", str(s), "-o", str(o)])
+            # the mixed-mesh solvers capture their default-stream launches into graphs
+            extra = ["--default-stream", "per-thread"] if s.name == "hybrid.cu" else []
+            jobs_.append([NVCC, *NVFLAGS, *extra, "-I", str(CSRC), "-c", str(s), "-o", str(o)])
     with cf.ThreadPoolExecutor(max_workers=jobs or os.cpu_count() or 4) as ex:
         for out in ex.map(_run, jobs_):
             if verbose and out.strip():

@@ -15,6 +15,8 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstring>
+#include <cstdlib>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -249,23 +251,234 @@ struct Schur {
     NDS_LAUNCH();
   }
 };
+// ---- CG with its iteration loop on the device.  This file is compiled with
+// the per-thread default stream, so every launch below can be captured: the
+// loop is one graph whose conditional while node runs one iteration per
+// pass, with the scalars (rho, alpha, beta, ||r||) kept on the device and
+// each partial-sum vector reduced by one block in a fixed order.  Per solve
+// the host waits twice (initial norm, final state) instead of three times
+// per iteration.
+enum { CG_RHO = 0, CG_BETA = 1, CG_ALPHA = 2, CG_RN = 3, CG_TARGET = 4 };
+enum { CG_ITS = 0, CG_CONV = 1, CG_FIRST = 2, CG_MAXIT = 3, CG_FLAGS = 4 };
+// flags: 1 pAp nonpositive, 2 rho nonpositive, 4 residual not finite, 8 initial rho nonpositive
+
+__device__ double sum_partials(const double* __restrict__ part, int nb) {
+  double s = 0;
+  for (int k = 0; k < nb; ++k) s += part[k];
+  return s;
+}
+// rho = r.z: the first pass takes it as the initial rho, later passes form beta
+__global__ void cg_rho(const double* __restrict__ part, int nb, double* __restrict__ sc, int* __restrict__ ctl) {
+  const double nr = sum_partials(part, nb);
+  const bool bad = !(nr > 0) || !isfinite(nr);
+  if (ctl[CG_FIRST]) {
+    if (bad) ctl[CG_FLAGS] |= 8;
+    sc[CG_BETA] = 0;
+  } else {
+    if (bad) ctl[CG_FLAGS] |= 2;
+    sc[CG_BETA] = bad ? 0.0 : nr / sc[CG_RHO];
+  }
+  sc[CG_RHO] = nr;
+}
+// p = z on the first pass, else z + beta p; zero at the pin
+__global__ void cg_p(int n, const double* __restrict__ sc, const int* __restrict__ ctl, const double* __restrict__ z,
+                     double* __restrict__ p, int pin) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  p[i] = i == pin ? 0.0 : (ctl[CG_FIRST] ? z[i] : z[i] + sc[CG_BETA] * p[i]);
+}
+__global__ void cg_alpha(const double* __restrict__ part, int nb, double* __restrict__ sc, int* __restrict__ ctl) {
+  const double pq = sum_partials(part, nb);
+  ctl[CG_FIRST] = 0;
+  if (!(pq > 0) || !isfinite(pq)) {
+    ctl[CG_FLAGS] |= 1;
+    sc[CG_ALPHA] = 0;
+  } else {
+    sc[CG_ALPHA] = sc[CG_RHO] / pq;
+  }
+}
+__global__ void cg_xr(int n, const double* __restrict__ sc, const double* __restrict__ p, const double* __restrict__ q,
+                      double* __restrict__ x, double* __restrict__ r, int pin) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double a = sc[CG_ALPHA];
+  x[i] = i == pin ? 0.0 : x[i] + a * p[i];
+  r[i] = i == pin ? 0.0 : r[i] - a * q[i];
+}
+// end of a pass: ||r||, the iteration count and the stopping test; the loop
+// always ends, at the latest when the count reaches max_it
+__global__ void cg_check(const double* __restrict__ part, int nb, double* __restrict__ sc, int* __restrict__ ctl,
+                         cudaGraphConditionalHandle loop) {
+  const double q = sum_partials(part, nb);
+  const double rn = isfinite(q) ? sqrt(fmax(0.0, q)) : NAN;
+  const int it = ++ctl[CG_ITS];
+  sc[CG_RN] = rn;
+  if (!isfinite(rn)) ctl[CG_FLAGS] |= 4;
+  const int conv = rn <= sc[CG_TARGET];
+  ctl[CG_CONV] = conv;
+  cudaGraphSetConditional(loop, (conv || ctl[CG_FLAGS] != 0 || it >= ctl[CG_MAXIT]) ? 0u : 1u);
+}
+// z = r / d with zero at the pin
+__global__ void cg_jacobi(int n, const double* __restrict__ inv, const double* __restrict__ r, double* __restrict__ z,
+                          int pin) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) z[i] = i == pin ? 0.0 : inv[i] * r[i];
+}
+
+struct CgLoop {
+  cudaGraphExec_t exec = nullptr;
+  const void* bound = nullptr;  // x of the captured body
+  unsigned long long body_kernels = 0;
+  bool failed = false;
+  CgLoop() = default;
+  CgLoop(const CgLoop&) = delete;
+  ~CgLoop() {
+    if (exec) cudaGraphExecDestroy(exec);
+  }
+};
 struct CgWork {
   int n;
-  Buf<double> r, z, p, q;
+  Buf<double> r, z, p, q, sc;
+  Buf<int> ctl;
   Reducer red;
-  explicit CgWork(int n_) : n(n_), r((size_t)n_), z((size_t)n_), p((size_t)n_), q((size_t)n_), red(n_) {}
+  CgLoop loop;
+  double* hsc = nullptr;
+  int* hctl = nullptr;
+  explicit CgWork(int n_)
+      : n(n_), r((size_t)n_), z((size_t)n_), p((size_t)n_), q((size_t)n_), sc((size_t)8), ctl((size_t)8), red(n_) {
+    NDS_CUDA(cudaMallocHost((void**)&hsc, 8 * sizeof(double)));
+    NDS_CUDA(cudaMallocHost((void**)&hctl, 8 * sizeof(int)));
+  }
+  CgWork(const CgWork&) = delete;
+  ~CgWork() {
+    if (hsc) cudaFreeHost(hsc);
+    if (hctl) cudaFreeHost(hctl);
+  }
 };
 struct CgResult {
   int its = 0;
   double rel = 1;
   bool ok = false;
 };
+bool hybrid_graphs_enabled() {
+  static const bool on = std::getenv("NDS_NO_GRAPHS") == nullptr;
+  return on;
+}
+
+// Preconditioned CG on the device from the guess in x: r = rhs - A x (zero at
+// pin, pin < 0 for none), r0 = ||r||; returns at once when r0 <= floor, else
+// iterates to ||r|| <= max(atol, rtol r0) within maxit.  pre(r, z) applies
+// the preconditioner (zero at the pin included).  Arithmetic and stopping
+// rule as the host loops below; false when the graph could not be built.
+template <class Op, class Pre>
+bool cg_device(Op& A, Pre&& pre, const double* rhs, double* x, double rtol, double atol, double floor, int maxit,
+               CgWork& W, int pin, CgResult& R) {
+  CgLoop& L = W.loop;
+  if (!hybrid_graphs_enabled() || L.failed) return false;
+  const int n = W.n, nb = W.red.blocks;
+  A.apply(x, W.q.p);
+  residual<<<grid(n), kTPB>>>(n, rhs, W.q.p, W.r.p);
+  NDS_LAUNCH();
+  if (pin >= 0) set_at<<<1, 1>>>(pin, 0.0, W.r.p);
+  const double r0 = W.red.norm(W.r.p);
+  if (!std::isfinite(r0)) throw std::runtime_error("mixed-mesh CG: initial residual not finite");
+  R = CgResult{};
+  if (r0 <= floor) {
+    R.rel = 0;
+    R.ok = true;
+    return true;
+  }
+  if (L.exec && L.bound != x) {
+    cudaGraphExecDestroy(L.exec);
+    L.exec = nullptr;
+  }
+  if (!L.exec) {
+    cudaGraph_t graph = nullptr;
+    bool ok = cudaGraphCreate(&graph, 0) == cudaSuccess;
+    cudaGraphConditionalHandle h{};
+    cudaGraphNodeParams cp{};
+    cudaGraphNode_t node{};
+    if (ok) ok = cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault) == cudaSuccess;
+    if (ok) {
+      cp.type = cudaGraphNodeTypeConditional;
+      cp.conditional.handle = h;
+      cp.conditional.type = cudaGraphCondTypeWhile;
+      cp.conditional.size = 1;
+      ok = cudaGraphAddNode(&node, graph, nullptr, 0, &cp) == cudaSuccess;
+    }
+    const unsigned long long l0 = g_launches;
+    if (ok)
+      ok = cudaStreamBeginCaptureToGraph(cudaStreamPerThread, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                         cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+    if (ok) {
+      bool body_ok = true;
+      try {
+        pre(W.r.p, W.z.p);
+        dot_blocks<<<nb, kTPB>>>(W.r.p, W.z.p, n, W.red.part.p);
+        cg_rho<<<1, 1>>>(W.red.part.p, nb, W.sc.p, W.ctl.p);
+        cg_p<<<grid(n), kTPB>>>(n, W.sc.p, W.ctl.p, W.z.p, W.p.p, pin);
+        A.apply(W.p.p, W.q.p);
+        dot_blocks<<<nb, kTPB>>>(W.p.p, W.q.p, n, W.red.part.p);
+        cg_alpha<<<1, 1>>>(W.red.part.p, nb, W.sc.p, W.ctl.p);
+        cg_xr<<<grid(n), kTPB>>>(n, W.sc.p, W.p.p, W.q.p, x, W.r.p, pin);
+        dot_blocks<<<nb, kTPB>>>(W.r.p, W.r.p, n, W.red.part.p);
+        cg_check<<<1, 1>>>(W.red.part.p, nb, W.sc.p, W.ctl.p, h);
+        g_launches += 8;
+        body_ok = cudaGetLastError() == cudaSuccess;
+      } catch (...) {
+        body_ok = false;
+      }
+      cudaGraph_t captured = nullptr;
+      ok = cudaStreamEndCapture(cudaStreamPerThread, &captured) == cudaSuccess && body_ok;
+    }
+    L.body_kernels = g_launches - l0;
+    g_launches = l0;
+    if (ok) ok = cudaGraphInstantiate(&L.exec, graph, 0) == cudaSuccess;
+    if (graph) cudaGraphDestroy(graph);
+    if (!ok) {
+      if (L.exec) cudaGraphExecDestroy(L.exec);
+      L.exec = nullptr;
+      L.failed = true;
+      cudaGetLastError();
+      return false;
+    }
+    L.bound = x;
+  }
+  W.hsc[CG_TARGET] = std::max(atol, rtol * r0);
+  const int init[5] = {0, 0, 1, maxit, 0};
+  std::memcpy(W.hctl, init, sizeof(init));
+  NDS_CUDA(cudaMemcpyAsync(W.sc.p + CG_TARGET, W.hsc + CG_TARGET, sizeof(double), cudaMemcpyHostToDevice,
+                           cudaStreamPerThread));
+  NDS_CUDA(cudaMemcpyAsync(W.ctl.p, W.hctl, 5 * sizeof(int), cudaMemcpyHostToDevice, cudaStreamPerThread));
+  NDS_CUDA(cudaGraphLaunch(L.exec, cudaStreamPerThread));
+  NDS_CUDA(cudaMemcpyAsync(W.hctl, W.ctl.p, 5 * sizeof(int), cudaMemcpyDeviceToHost, cudaStreamPerThread));
+  NDS_CUDA(cudaMemcpyAsync(W.hsc + CG_RN, W.sc.p + CG_RN, sizeof(double), cudaMemcpyDeviceToHost, cudaStreamPerThread));
+  NDS_CUDA(cudaStreamSynchronize(cudaStreamPerThread));
+  const int f = W.hctl[CG_FLAGS];
+  g_launches += (unsigned long long)W.hctl[CG_ITS] * L.body_kernels;
+  if (f & 8) throw std::runtime_error("mixed-mesh CG: initial rho nonpositive");
+  if (f & 1) throw std::runtime_error("mixed-mesh CG: pAp nonpositive");
+  if (f & 2) throw std::runtime_error("mixed-mesh CG: rho nonpositive");
+  if (f & 4) throw std::runtime_error("mixed-mesh CG: residual not finite");
+  R.its = W.hctl[CG_ITS];
+  R.rel = W.hsc[CG_RN] / r0;
+  R.ok = W.hctl[CG_CONV] != 0;
+  return true;
+}
 // Jacobi-preconditioned CG to ||r|| <= rtol ||r0|| from the guess in x
 // (hybrid_hxt4a/hxt4a_main.cu:309-326; pin >= 0 keeps x, r, p zero there)
 template <class Op>
 CgResult cg(Op& A, const double* rhs, double* x, const double* invdiag, double rtol, int maxit, CgWork& W,
             int pin = -1) {
   const int n = W.n;
+  {
+    CgResult D;
+    auto jac = [&](const double* r, double* z) {
+      cg_jacobi<<<grid(n), kTPB>>>(n, invdiag, r, z, pin);
+      NDS_LAUNCH();
+    };
+    if (cg_device(A, jac, rhs, x, rtol, 0.0, 0.0, maxit, W, pin, D)) return D;
+  }
   A.apply(x, W.q.p);
   residual<<<grid(n), kTPB>>>(n, rhs, W.q.p, W.r.p);
   NDS_LAUNCH();
@@ -650,6 +863,14 @@ template <class Op>
 CgResult pcg_prod(Op& A, const double* rhs, double* x, const double* invdiag, double rtol, double atol, int maxit,
                   CgWork& W, int pin) {
   const int n = W.n;
+  {
+    CgResult D;
+    auto jac = [&](const double* r, double* z) {
+      cg_jacobi<<<grid(n), kTPB>>>(n, invdiag, r, z, pin);
+      NDS_LAUNCH();
+    };
+    if (cg_device(A, jac, rhs, x, rtol, atol, 0.0, maxit, W, pin, D)) return D;
+  }
   A.apply(x, W.q.p);
   residual<<<grid(n), kTPB>>>(n, rhs, W.q.p, W.r.p);
   NDS_LAUNCH();
@@ -1054,6 +1275,15 @@ template <class Op>
 CgResult pcg_amg(Op& A, HybridAmgDevice& M, const double* rhs, double* x, double rtol, double atol, int maxit,
                  CgWork& W, int pin) {
   const int n = W.n;
+  {
+    CgResult D;
+    auto vc = [&](const double* r, double* z) {
+      M.apply(r, z);
+      set_at<<<1, 1>>>(pin, 0.0, z);
+      NDS_LAUNCH();
+    };
+    if (cg_device(A, vc, rhs, x, rtol, atol, atol, maxit, W, pin, D)) return D;
+  }
   A.apply(x, W.q.p);
   residual<<<grid(n), kTPB>>>(n, rhs, W.q.p, W.r.p);
   NDS_LAUNCH();
