@@ -523,6 +523,128 @@ def hybrid_pipe(nr: int = 4, ntheta: int = 16, nz: int = 40, radius: float = 0.5
         meta=dict(nr=nr, ntheta=ntheta, nz=nz, radius=radius, length=length))
 
 
+_HEX_SIGN = np.array([[-1, -1, -1], [1, -1, -1], [1, 1, -1], [-1, 1, -1],
+                      [-1, -1, 1], [1, -1, 1], [1, 1, 1], [-1, 1, 1]], dtype=np.float64)
+
+
+def _face_table(cells: np.ndarray, faces) -> tuple:
+    """Sorted vertex keys of every local face (cell-major), the unique keys in
+    lexicographic order and each local face's rank among them."""
+    k = np.sort(cells[:, np.asarray(faces)], axis=2).reshape(-1, len(faces[0]))
+    uniq, inv, cnt = np.unique(k, axis=0, return_inverse=True, return_counts=True)
+    if np.any(cnt > 2):
+        raise ValueError("non-manifold face")
+    return k, uniq, inv.reshape(len(cells), len(faces)), cnt
+
+
+def _locate(uniq: np.ndarray, rank: np.ndarray, cnt: np.ndarray, recs: np.ndarray, what: str) -> np.ndarray:
+    """(cell, local face, rank) of the faces of recs (vertex lists), each of
+    which must have exactly one owner."""
+    recs = np.asarray(recs, dtype=np.int64).reshape(-1, uniq.shape[1])
+    if len(recs) == 0:
+        return np.zeros((0, 3), dtype=np.int64)
+    keys = np.sort(recs, axis=1)
+    # row of each key in uniq: as big-endian unsigned bytes, the byte order
+    # of a key is its lexicographic order, so a void view searches sorted
+    big = np.dtype(">u4")
+    vu = np.ascontiguousarray(uniq.astype(big)).view(np.dtype((np.void, 4 * uniq.shape[1]))).ravel()
+    vk = np.ascontiguousarray(keys.astype(big)).view(vu.dtype).ravel()
+    pos = np.searchsorted(vu, vk)
+    if np.any(pos >= len(vu)) or np.any(vu[np.minimum(pos, len(vu) - 1)] != vk):
+        raise ValueError(f"{what} face not found in the mesh")
+    if np.any(cnt[pos] != 1):
+        raise ValueError(f"{what} face owner count != 1")
+    flat = np.full(len(uniq), -1, dtype=np.int64)
+    flat[rank.ravel()] = np.arange(rank.size)
+    owner = flat[pos]  # the single owner's (cell * nfaces + local face)
+    nf = rank.shape[1]
+    return np.stack((owner // nf, owner % nf, pos), axis=1)
+
+
+def write_hxt1_hybrid(m: HybridMesh, path: str | os.PathLike) -> Path:
+    """HXT1 version 1 of a mixed mesh, laid out as the reference's preparer
+    writes it (gpu/serial_cuda/hybrid_hxt1/prepare_hxt1.py:110-246): the face
+    bubbles of hex faces numbered n_points + the rank of the sorted vertex
+    quadruple, then those of tet faces after them; per hex the 8 vertices and
+    6 face bubbles, per tet 4 vertices and 4; pressure ids hexes then tets;
+    hex geometry (volume = sum of det J at the 2x2x2 Gauss points, squared
+    longest vertex distance, the 8 det J, the 8 J^-1 row-major), tet geometry
+    (volume, squared longest edge, det J, J^-1); interface records (hex cell,
+    face, bubble, then the two tets'); wall, inlet and outlet records (cell,
+    local face, bubble) in the order of the mesh's lists."""
+    pts = np.ascontiguousarray(m.points, dtype=np.float64)
+    hexes = np.ascontiguousarray(m.hexes, dtype=np.int32)
+    tets = np.ascontiguousarray(m.tets, dtype=np.int32)
+    nv, nh, nt = len(pts), len(hexes), len(tets)
+    _, hu, hrank, hcnt = _face_table(hexes, HXT1_HEX_FACE)
+    _, tu, trank, tcnt = _face_table(tets, HXT1_TET_FACE)
+    nhf, ntf = len(hu), len(tu)
+    hvel = np.concatenate((hexes, nv + hrank), axis=1).astype(np.int32)
+    tvel = np.concatenate((tets, nv + nhf + trank), axis=1).astype(np.int32)
+    iq = np.asarray(m.interface_quads).reshape(-1, 4)
+    itr = np.asarray(m.interface_triangles).reshape(-1, 2, 3)
+    if len(iq) != len(itr):
+        raise ValueError("interface quad/triangle record mismatch")
+    hrec = _locate(hu, hrank, hcnt, iq, "interface hex")
+    t0 = _locate(tu, trank, tcnt, itr[:, 0], "interface tet")
+    t1 = _locate(tu, trank, tcnt, itr[:, 1], "interface tet")
+    off_h, off_t = np.array([0, 0, nv]), np.array([0, 0, nv + nhf])
+    irec = np.concatenate((hrec + off_h, t0 + off_t, t1 + off_t), axis=1).astype(np.int32)
+    recs = [_locate(hu, hrank, hcnt, m.wall_quads, "wall") + off_h,
+            _locate(hu, hrank, hcnt, m.inlet_hex_quads, "inlet hex") + off_h,
+            _locate(tu, trank, tcnt, m.inlet_tet_triangles, "inlet tet") + off_t,
+            _locate(hu, hrank, hcnt, m.outlet_hex_quads, "outlet hex") + off_h,
+            _locate(tu, trank, tcnt, m.outlet_tet_triangles, "outlet tet") + off_t]
+    recs = [r.astype(np.int32) for r in recs]
+    # hex geometry at the 2x2x2 Gauss points, xi slowest
+    x = pts[hexes]  # (nh, 8, 3)
+    g = 1.0 / np.sqrt(3.0)
+    dets, invs = [], []
+    for xi in (-g, g):
+        for eta in (-g, g):
+            for zeta in (-g, g):
+                sx, sy, sz = _HEX_SIGN[:, 0], _HEX_SIGN[:, 1], _HEX_SIGN[:, 2]
+                dxi = 0.125 * sx * (1.0 + sy * eta) * (1.0 + sz * zeta)
+                deta = 0.125 * sy * (1.0 + sx * xi) * (1.0 + sz * zeta)
+                dzeta = 0.125 * sz * (1.0 + sx * xi) * (1.0 + sy * eta)
+                # J[:, i, j] = d x_i / d xi_j, each column one 8-term product
+                J = np.stack((np.matmul(dxi, x), np.matmul(deta, x), np.matmul(dzeta, x)), axis=2)
+                dets.append(np.linalg.det(J))
+                invs.append(np.linalg.inv(J).reshape(nh, 9))
+    dets = np.stack(dets, axis=1) if nh else np.zeros((0, 8))
+    invs = np.concatenate(invs, axis=1) if nh else np.zeros((0, 72))
+    h2h = np.zeros(nh)
+    for a in range(8):
+        for b in range(a + 1, 8):
+            dd = x[:, a] - x[:, b]
+            h2h = np.maximum(h2h, dd[:, 0] * dd[:, 0] + dd[:, 1] * dd[:, 1] + dd[:, 2] * dd[:, 2])
+    vol = np.zeros(nh)
+    for k in range(8):  # summed in Gauss-point order
+        vol = vol + dets[:, k]
+    hgeom = np.column_stack((vol, h2h, dets, invs)) if nh else np.zeros((0, 82))
+    y = pts[tets]
+    Jt = np.stack((y[:, 1] - y[:, 0], y[:, 2] - y[:, 0], y[:, 3] - y[:, 0]), axis=2)  # columns
+    dt = np.linalg.det(Jt) if nt else np.zeros(0)
+    it_ = np.linalg.inv(Jt).reshape(nt, 9) if nt else np.zeros((0, 9))
+    h2t = np.zeros(nt)
+    for a in range(4):
+        for b in range(a + 1, 4):
+            dd = y[:, a] - y[:, b]
+            h2t = np.maximum(h2t, np.einsum("ij,ij->i", dd, dd))
+    tgeom = np.column_stack((dt / 6.0, h2t, dt, it_)) if nt else np.zeros((0, 12))
+    if nh and np.min(dets) <= 0 or nt and np.min(dt) <= 0:
+        raise ValueError("non-positive Jacobian")
+    header = (nv, nh, nt, nhf, ntf, nv + nhf + ntf, nh + nt, len(irec), *(len(r) for r in recs))
+    p = Path(path)
+    p.parent.mkdir(parents=True, exist_ok=True)
+    with open(p, "wb") as f:
+        f.write(HXT1_MAGIC + np.asarray([1, 0], dtype="<u4").tobytes() + np.asarray(header, dtype="<u8").tobytes())
+        for a in (pts, hexes, tets, hvel, tvel, np.arange(nh, dtype=np.int32), np.arange(nh, nh + nt, dtype=np.int32),
+                  hgeom, tgeom, irec, *recs):
+            f.write(np.ascontiguousarray(a).astype(a.dtype.newbyteorder("<"), copy=False).tobytes())
+    return p
+
+
 def write_hxt0(m: HybridMesh, path: str | os.PathLike) -> Path:
     """The HXT0 ``.npz`` the reference's HXT1 preparer takes as input."""
     p = Path(path)

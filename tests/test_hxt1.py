@@ -91,3 +91,39 @@ def test_reader_rejects(native, tmp_path, case, message):
     with pytest.raises(native.NdsError) as e:
         native.Mesh.read_hxt1(_bad(tmp_path, bytes(b), case + ".bin"))
     assert e.value.code == -2 and message in str(e.value)
+
+
+def test_hybrid_writer_matches_reference_preparer(tmp_path):
+    """meshgen.write_hxt1_hybrid against the reference preparer's file of the
+    same mixed pipe (tests/golden/hxt1_hybrid_r2.bin, made by
+    make_hxt1_golden.py): every count, index and record identical, points and
+    geometry to 1e-13 of each record's largest entry (here the files are
+    byte-identical; the reference takes det J and J^-1 from LAPACK through
+    numpy, so a different LAPACK build may move the last bit)."""
+    import sys
+    from oracle.hybrid_vtu import read_mixed_hxt1
+    from nodals_b200 import meshgen
+    sys.path.insert(0, str(GOLDEN))
+    from make_hxt1_golden import HYBRID
+    p = meshgen.write_hxt1_hybrid(meshgen.hybrid_pipe(**HYBRID), tmp_path / "r2.bin")
+    got, want = read_mixed_hxt1(p), read_mixed_hxt1(GOLDEN / "hxt1_hybrid_r2.bin")
+    assert got["counts"] == want["counts"]
+    for k, w in want.items():
+        if k == "counts":
+            continue
+        g = got[k]
+        assert g.shape == w.shape, k
+        if w.dtype.kind == "f":
+            scale = np.maximum(np.abs(w).max(axis=1, keepdims=True), 1e-300) if w.size else 1.0
+            assert np.all(np.abs(g - w) <= 1e-13 * scale), k
+        else:
+            assert np.array_equal(g, w), k
+
+
+def test_hybrid_writer_rejects_bad_records(tmp_path):
+    from nodals_b200 import meshgen
+    m = meshgen.hybrid_pipe(nr=2, ntheta=8, nz=4, radius=0.5, length=2.0)
+    # the top face of a hex in the first slab is shared with the next slab's hex
+    m.wall_quads = np.concatenate((m.wall_quads, m.hexes[:1, 4:8]))
+    with pytest.raises(ValueError, match="owner count"):
+        meshgen.write_hxt1_hybrid(m, tmp_path / "bad.bin")
