@@ -713,78 +713,130 @@ __device__ void hex_basis_dev(double x, double y, double z, double phi[14], doub
 
 // Convection block of each hex at the lagged velocity:
 // C_ab = sum_q det w phi_a (u_q . grad phi_b), u_q = sum_m u_m phi_m(q), 27 points.
-// One block per hex; one thread per point builds that point's basis,
-// metric and velocity in shared memory, then the 196 entries.
+// Persistent blocks walk the hexes.  Each block first copies the basis
+// values and reference gradients at the 27 points into shared memory (the
+// same for every hex); per hex, 27 threads build the metric of their point
+// and the velocity there, all threads then form, per (point, function),
+// det w phi and u . grad phi, and finally the 196 entries, summed over the
+// points in order.
+struct HexConvShared {
+  double phi[27][14], gref[27][14][3], inv[27][9], dw[27], u[27][3], ul[3][14], v[8][3];
+  double dwphi[27][14], ugrad[27][14];  // det w phi_a and u_q . grad phi_b at each point
+};
+// basis values and reference gradients at the 27 points: tab[q][a][0] = phi,
+// tab[q][a][1..3] = gradient (filled once per run)
+__global__ void hex_point_table(double* __restrict__ tab) {
+  const int t = threadIdx.x;
+  if (t >= 27) return;
+  const int ix = t / 9, iy = (t / 3) % 3, iz = t % 3;
+  double ph[14], g[14][3];
+  hex_basis_dev(c_g3[ix], c_g3[iy], c_g3[iz], ph, g);
+  for (int a = 0; a < 14; ++a) {
+    double* o = tab + (t * 14 + a) * 4;
+    o[0] = ph[a];
+    for (int d = 0; d < 3; ++d) o[1 + d] = g[a][d];
+  }
+}
 __global__ void __launch_bounds__(kTPB) hex_conv_local(int nh, const double* __restrict__ xyz,
                                                         const int32_t* __restrict__ hexes,
                                                         const int32_t* __restrict__ dofs, const double* __restrict__ u0,
                                                         const double* __restrict__ u1, const double* __restrict__ u2,
-                                                        double* __restrict__ local, int* __restrict__ bad) {
-  __shared__ double sphi[27][14], sgp[27][14][3], sdw[27], su[27][3], sul[3][14];
-  const int c = blockIdx.x, t = threadIdx.x;
-  if (c >= nh) return;
-  if (t < 14) {
-    const int g = dofs[14 * (size_t)c + t];
-    sul[0][t] = u0[g];
-    sul[1][t] = u1[g];
-    sul[2][t] = u2[g];
+                                                        const double* __restrict__ tab, double* __restrict__ local,
+                                                        int* __restrict__ bad) {
+  __shared__ HexConvShared S;
+  const int t = threadIdx.x;
+  for (int k = t; k < 27 * 14; k += blockDim.x) {
+    const int q = k / 14, a = k % 14;
+    S.phi[q][a] = tab[4 * k];
+    for (int d = 0; d < 3; ++d) S.gref[q][a][d] = tab[4 * k + 1 + d];
   }
-  __syncthreads();
-  if (t < 27) {
-    const int ix = t / 9, iy = (t / 3) % 3, iz = t % 3;
-    const double x = c_g3[ix], y = c_g3[iy], z = c_g3[iz], w = c_g3[3 + ix] * c_g3[3 + iy] * c_g3[3 + iz];
-    double ph[14], g[14][3];
-    hex_basis_dev(x, y, z, ph, g);
-    double J[9] = {};
-    for (int a = 0; a < 8; ++a) {
-      const double* p = xyz + 3 * (size_t)hexes[8 * (size_t)c + a];
-      for (int i = 0; i < 3; ++i)
-        for (int j = 0; j < 3; ++j) J[3 * i + j] += p[i] * g[a][j];
+  for (int c = blockIdx.x; c < nh; c += gridDim.x) {
+    __syncthreads();  // the previous hex's entries are written; tables are ready
+    if (t < 14) {
+      const int g = dofs[14 * (size_t)c + t];
+      S.ul[0][t] = u0[g];
+      S.ul[1][t] = u1[g];
+      S.ul[2][t] = u2[g];
+    } else if (t >= 32 && t < 56) {
+      const int a = (t - 32) / 3, i = (t - 32) % 3;
+      S.v[a][i] = xyz[3 * (size_t)hexes[8 * (size_t)c + a] + i];
     }
-    const double det = J[0] * (J[4] * J[8] - J[5] * J[7]) - J[1] * (J[3] * J[8] - J[5] * J[6]) + J[2] * (J[3] * J[7] - J[4] * J[6]);
-    if (!(det > 0)) atomicAdd(bad, 1);
-    const double q = 1.0 / det;
-    const double I[9] = {(J[4] * J[8] - J[5] * J[7]) * q, (J[2] * J[7] - J[1] * J[8]) * q, (J[1] * J[5] - J[2] * J[4]) * q,
-                         (J[5] * J[6] - J[3] * J[8]) * q, (J[0] * J[8] - J[2] * J[6]) * q, (J[2] * J[3] - J[0] * J[5]) * q,
-                         (J[3] * J[7] - J[4] * J[6]) * q, (J[1] * J[6] - J[0] * J[7]) * q, (J[0] * J[4] - J[1] * J[3]) * q};
-    double uq[3] = {0, 0, 0};
-    for (int a = 0; a < 14; ++a) {
-      sphi[t][a] = ph[a];
-      for (int d = 0; d < 3; ++d) sgp[t][a][d] = g[a][0] * I[d] + g[a][1] * I[3 + d] + g[a][2] * I[6 + d];
-      for (int d = 0; d < 3; ++d) uq[d] += sul[d][a] * ph[a];
+    __syncthreads();
+    if (t < 27) {
+      const int ix = t / 9, iy = (t / 3) % 3, iz = t % 3;
+      const double w = c_g3[3 + ix] * c_g3[3 + iy] * c_g3[3 + iz];
+      double J[9] = {};
+      for (int a = 0; a < 8; ++a)
+        for (int i = 0; i < 3; ++i)
+          for (int j = 0; j < 3; ++j) J[3 * i + j] += S.v[a][i] * S.gref[t][a][j];
+      const double det = J[0] * (J[4] * J[8] - J[5] * J[7]) - J[1] * (J[3] * J[8] - J[5] * J[6]) + J[2] * (J[3] * J[7] - J[4] * J[6]);
+      if (!(det > 0)) atomicAdd(bad, 1);
+      const double q = 1.0 / det;
+      S.inv[t][0] = (J[4] * J[8] - J[5] * J[7]) * q;
+      S.inv[t][1] = (J[2] * J[7] - J[1] * J[8]) * q;
+      S.inv[t][2] = (J[1] * J[5] - J[2] * J[4]) * q;
+      S.inv[t][3] = (J[5] * J[6] - J[3] * J[8]) * q;
+      S.inv[t][4] = (J[0] * J[8] - J[2] * J[6]) * q;
+      S.inv[t][5] = (J[2] * J[3] - J[0] * J[5]) * q;
+      S.inv[t][6] = (J[3] * J[7] - J[4] * J[6]) * q;
+      S.inv[t][7] = (J[1] * J[6] - J[0] * J[7]) * q;
+      S.inv[t][8] = (J[0] * J[4] - J[1] * J[3]) * q;
+      S.dw[t] = det * w;
+      double uq[3] = {0, 0, 0};
+      for (int a = 0; a < 14; ++a)
+        for (int d = 0; d < 3; ++d) uq[d] += S.ul[d][a] * S.phi[t][a];
+      for (int d = 0; d < 3; ++d) S.u[t][d] = uq[d];
     }
-    sdw[t] = det * w;
-    for (int d = 0; d < 3; ++d) su[t][d] = uq[d];
-  }
-  __syncthreads();
-  for (int e = t; e < 196; e += blockDim.x) {
-    const int a = e / 14, b = e % 14;
-    double s = 0;
-    for (int q = 0; q < 27; ++q)
-      s += sdw[q] * sphi[q][a] * (su[q][0] * sgp[q][b][0] + su[q][1] * sgp[q][b][1] + su[q][2] * sgp[q][b][2]);
-    local[196 * (size_t)c + e] = s;
+    __syncthreads();
+    for (int e = t; e < 27 * 14; e += blockDim.x) {
+      const int q = e / 14, a = e % 14;
+      const double* g = S.gref[q][a];
+      const double* I = S.inv[q];
+      double gp[3];
+      for (int d = 0; d < 3; ++d) gp[d] = g[0] * I[d] + g[1] * I[3 + d] + g[2] * I[6 + d];
+      S.ugrad[q][a] = S.u[q][0] * gp[0] + S.u[q][1] * gp[1] + S.u[q][2] * gp[2];
+      S.dwphi[q][a] = S.dw[q] * S.phi[q][a];
+    }
+    __syncthreads();
+    for (int e = t; e < 196; e += blockDim.x) {
+      const int a = e / 14, b = e % 14;
+      double s = 0;
+      for (int q = 0; q < 27; ++q) s += S.dwphi[q][a] * S.ugrad[q][b];
+      local[196 * (size_t)c + e] = s;
+    }
   }
 }
-// Convection block of each tet: C_ab = det sum_m sum_j (J^-1 u_m)_j T[a][m][b][j]
-__global__ void tet_conv_local(int nt, const double* __restrict__ geom, const int32_t* __restrict__ dofs,
-                               const double* __restrict__ u0, const double* __restrict__ u1,
-                               const double* __restrict__ u2, double* __restrict__ local) {
-  __shared__ double ur[8][3];
-  const int c = blockIdx.x, t = threadIdx.x;
-  if (c >= nt) return;
-  const double* G = geom + 12 * (size_t)c;
-  if (t < 8) {
-    const int g = dofs[8 * (size_t)c + t];
-    const double u[3] = {u0[g], u1[g], u2[g]};
-    for (int j = 0; j < 3; ++j) ur[t][j] = u[0] * G[3 + 3 * j] + u[1] * G[4 + 3 * j] + u[2] * G[5 + 3 * j];
+// Convection block of each tet: C_ab = det sum_m sum_j (J^-1 u_m)_j T[a][m][b][j].
+// Persistent blocks of 256 threads take four tets at a time (64 threads
+// each, one per entry); the tensor is staged once per block in shared memory
+// as [m][j][a][b], so a warp's 32 entries read 32 consecutive values.
+__global__ void __launch_bounds__(kTPB) tet_conv_local(int nt, const double* __restrict__ geom,
+                                                        const int32_t* __restrict__ dofs,
+                                                        const double* __restrict__ u0, const double* __restrict__ u1,
+                                                        const double* __restrict__ u2, double* __restrict__ local) {
+  __shared__ double T[8 * 3 * 64];
+  __shared__ double ur[4][8][3];
+  const int t = threadIdx.x, slot = t / 64, e = t % 64, a = e / 8, b = e % 8;
+  for (int k = t; k < 8 * 3 * 64; k += blockDim.x) {
+    const int mj = k / 64, ab = k % 64, m = mj / 3, j = mj % 3, aa = ab / 8, bb = ab % 8;
+    T[k] = c_tet_conv[((aa * 8 + m) * 8 + bb) * 3 + j];
   }
-  __syncthreads();
-  if (t < 64) {
-    const int a = t / 8, b = t % 8;
-    double q = 0;
-    for (int m = 0; m < 8; ++m)
-      for (int j = 0; j < 3; ++j) q += ur[m][j] * c_tet_conv[((a * 8 + m) * 8 + b) * 3 + j];
-    local[64 * (size_t)c + t] = q * G[2];
+  for (int c0 = 4 * blockIdx.x; c0 < nt; c0 += 4 * gridDim.x) {
+    const int c = c0 + slot;
+    __syncthreads();  // T staged; the previous tets' velocities are no longer read
+    if (c < nt && e < 8) {
+      const double* G = geom + 12 * (size_t)c;
+      const int g = dofs[8 * (size_t)c + e];
+      const double u[3] = {u0[g], u1[g], u2[g]};
+      for (int j = 0; j < 3; ++j) ur[slot][e][j] = u[0] * G[3 + 3 * j] + u[1] * G[4 + 3 * j] + u[2] * G[5 + 3 * j];
+    }
+    __syncthreads();
+    if (c < nt) {
+      double q = 0;
+      for (int m = 0; m < 8; ++m)
+        for (int j = 0; j < 3; ++j) q += ur[slot][m][j] * T[(m * 3 + j) * 64 + a * 8 + b];
+      local[64 * (size_t)c + e] = q * geom[12 * (size_t)c + 2];
+    }
   }
 }
 // conv[k] = sum of its cells' local values, in cell order
@@ -829,19 +881,36 @@ __global__ void flow_rhs(int n, const uint8_t* fixed, const double* bt, const do
 }
 // Gauss-Seidel on the rows of one colour, a warp per row:
 // x_i += omega ((rhs_i - sum_{j != i} a_ij x_j) / a_ii - x_i)
-__global__ void gs_colour(int count, const int32_t* __restrict__ rows, const int32_t* __restrict__ row,
-                          const int32_t* __restrict__ col, const double* __restrict__ val,
-                          const int32_t* __restrict__ dpos, const double* __restrict__ rhs, double* x, double omega) {
+// the same colour step for the three velocity components at once: they share
+// the matrix, so each row is read once; per component the arithmetic is
+// gs_colour's
+__global__ void gs_colour3(int count, const int32_t* __restrict__ rows, const int32_t* __restrict__ row,
+                           const int32_t* __restrict__ col, const double* __restrict__ val,
+                           const int32_t* __restrict__ dpos, const double* __restrict__ r0,
+                           const double* __restrict__ r1, const double* __restrict__ r2, double* x0, double* x1,
+                           double* x2, double omega) {
   const int q = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
   if (q >= count) return;
   const int i = rows[q];
-  double off = 0;
-  for (int k = row[i] + lane; k < row[i + 1]; k += 32)
-    if (col[k] != i) off += val[k] * x[col[k]];
-  off = warp_sum(off);
+  double o0 = 0, o1 = 0, o2 = 0;
+  for (int k = row[i] + lane; k < row[i + 1]; k += 32) {
+    const int j = col[k];
+    if (j != i) {
+      const double v = val[k];
+      o0 += v * x0[j];
+      o1 += v * x1[j];
+      o2 += v * x2[j];
+    }
+  }
+  o0 = warp_sum(o0);
+  o1 = warp_sum(o1);
+  o2 = warp_sum(o2);
   if (lane == 0) {
-    const double gs = (rhs[i] - off) / val[dpos[i]];
-    x[i] = x[i] + omega * (gs - x[i]);
+    const double d = val[dpos[i]];
+    const double g0 = (r0[i] - o0) / d, g1 = (r1[i] - o1) / d, g2 = (r2[i] - o2) / d;
+    x0[i] = x0[i] + omega * (g0 - x0[i]);
+    x1[i] = x1[i] + omega * (g1 - x1[i]);
+    x2[i] = x2[i] + omega * (g2 - x2[i]);
   }
 }
 __global__ void residual_free(int n, const uint8_t* fixed, const double* b, const double* Ax, double* r) {
@@ -1382,28 +1451,46 @@ void run_flow(const char* path, const nds_hybrid_flow_options& o, int verbose, n
                 "wall=STRONG_NOSLIP outlet=NATURAL_TRACTION pressureGaugePin=%d status=PASS\n",
                 dpdz_exact, drop_exact, pin);
   }
-  auto sweep = [&](double* x, const double* rhs, bool forward) {
+  auto sweep3 = [&](bool forward) {
     for (int q = 0; q < ncol; ++q) {
       const int c = forward ? q : ncol - 1 - q;
       const int b = F.colour_off[(size_t)c], n = F.colour_off[(size_t)c + 1] - b;
-      gs_colour<<<grid((long long)n * 32), kTPB>>>(n, d_crows.p + b, d_row.p, d_col.p, val.p, d_dpos.p, rhs, x, o.mom_omega);
+      gs_colour3<<<grid((long long)n * 32), kTPB>>>(n, d_crows.p + b, d_row.p, d_col.p, val.p, d_dpos.p, r0.p, r1.p,
+                                                    r2.p, u0.p, u1.p, u2.p, o.mom_omega);
       NDS_LAUNCH();
     }
   };
-  auto momentum_work = [&](int it, double* x, const double* rhs) {
-    if (o.momentum_work == 0) sweep(x, rhs, true);
-    else if (o.momentum_work == 1) sweep(x, rhs, (it & 1) != 0);
+  // the momentum work of the three components (independent systems with one
+  // matrix), swept together
+  auto momentum_work3 = [&](int it) {
+    if (o.momentum_work == 0) sweep3(true);
+    else if (o.momentum_work == 1) sweep3((it & 1) != 0);
     else {
-      sweep(x, rhs, true);
-      sweep(x, rhs, false);
+      sweep3(true);
+      sweep3(false);
     }
   };
+  // persistent grids of the convection kernels: 8 blocks of 256 threads per SM
+  int conv_blocks = 0;
+  {
+    int dev = 0, sms = 0;
+    NDS_CUDA(cudaGetDevice(&dev));
+    NDS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    conv_blocks = 8 * std::max(sms, 1);
+  }
+  Buf<double> d_ptab((size_t)27 * 14 * 4);
+  hex_point_table<<<1, 32>>>(d_ptab.p);
+  NDS_LAUNCH();
   // lagged convection of the current velocity, relaxed rows and rAU
   auto assemble = [&]() {
-    hex_conv_local<<<std::max(nh, 1), kTPB>>>(nh, d_xyz.p, d_hexes.p, d_hdofs.p, u0.p, u1.p, u2.p, d_local.p, d_bad.p);
-    NDS_LAUNCH();
+    if (nh) {
+      hex_conv_local<<<std::min(nh, conv_blocks), kTPB>>>(nh, d_xyz.p, d_hexes.p, d_hdofs.p, u0.p, u1.p, u2.p,
+                                                          d_ptab.p, d_local.p, d_bad.p);
+      NDS_LAUNCH();
+    }
     if (nt) {
-      tet_conv_local<<<nt, 64>>>(nt, d_tgeom.p, d_tdofs.p, u0.p, u1.p, u2.p, d_local.p + 196 * (size_t)nh);
+      tet_conv_local<<<std::min((nt + 3) / 4, conv_blocks), kTPB>>>(nt, d_tgeom.p, d_tdofs.p, u0.p, u1.p, u2.p,
+                                                                    d_local.p + 196 * (size_t)nh);
       NDS_LAUNCH();
     }
     conv_gather<<<grid(nnz), kTPB>>>(nnz, d_soff.p, d_src.p, d_local.p, conv.p);
@@ -1460,9 +1547,7 @@ void run_flow(const char* path, const nds_hybrid_flow_options& o, int verbose, n
     flow_rhs<<<grid(nv), kTPB>>>(nv, d_fixed.p, bt1.p, u1.p, dorig.p, o.alpha_u, r1.p);
     flow_rhs<<<grid(nv), kTPB>>>(nv, d_fixed.p, bt2.p, u2.p, dorig.p, o.alpha_u, r2.p);
     NDS_LAUNCH();
-    momentum_work(it, u0.p, r0.p);
-    momentum_work(it, u1.p, r1.p);
-    momentum_work(it, u2.p, r2.p);
+    momentum_work3(it);
     B.B(u0.p, u1.p, u2.p, cont.p);
     set_at<<<1, 1>>>(pin, 0.0, cont.p);
     NDS_LAUNCH();

@@ -1,6 +1,7 @@
 #include "hybrid.hpp"
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstring>
 #include <fstream>
@@ -291,38 +292,97 @@ struct Trip {
   int32_t r, c;
   double v;
 };
+// Stable sort of triplets by (row, column): a counting sort by row, then a
+// stable sort of each row's run by column, so duplicates keep the order in
+// which the cells produced them.
+void sort_trips(std::vector<Trip>& t, int nrows) {
+  std::vector<int64_t> off((size_t)nrows + 1, 0);
+  for (const Trip& x : t) ++off[(size_t)x.r + 1];
+  for (int r = 0; r < nrows; ++r) off[(size_t)r + 1] += off[(size_t)r];
+  std::vector<Trip> o(t.size());
+  {
+    std::vector<int64_t> next(off.begin(), off.end() - 1);
+    for (const Trip& x : t) o[(size_t)next[(size_t)x.r]++] = x;
+  }
+#pragma omp parallel for schedule(dynamic, 512)
+  for (int r = 0; r < nrows; ++r)
+    std::stable_sort(o.begin() + off[(size_t)r], o.begin() + off[(size_t)r + 1],
+                     [](const Trip& x, const Trip& y) { return x.c < y.c; });
+  t.swap(o);
+}
+
+// The element loops run in parallel, each cell (and interface triangle)
+// writing its block into its own slots in cell order; the diagonal sums and
+// the merge of duplicates then follow that order, as a serial loop would.
 void assemble_velocity(const HybridMesh& m, const std::vector<InterfacePlan>& plans, double nu, double gamma,
                        std::vector<int32_t>& row, std::vector<int32_t>& col, std::vector<double>& val,
                        std::vector<double>& diag_rau) {
   const Rules& R = rules();
-  const int nv = m.nvel();
+  const int nv = m.nvel(), nh = m.nhex(), nt = m.ntet(), np2 = 2 * (int)plans.size();
   diag_rau.assign((size_t)nv, 0.0);
-  std::vector<Trip> t;
-  t.reserve((size_t)m.nhex() * 196 + (size_t)m.ntet() * 64 + plans.size() * 2 * 484);
-    // hex volumes: K_ab = sum_q nu det w grad phi_a . grad phi_b (27 points)
-  for (int c = 0; c < m.nhex(); ++c) {
-    double K[14][14] = {};
-    for (int ix = 0; ix < 3; ++ix)
-      for (int iy = 0; iy < 3; ++iy)
-        for (int iz = 0; iz < 3; ++iz) {
-          const double x = R.g3x[ix], y = R.g3x[iy], z = R.g3x[iz], w = R.g3w[ix] * R.g3w[iy] * R.g3w[iz];
-          double ph[14], g[14][3], gp[14][3], I[9], det;
-          hex_basis(x, y, z, ph, g);
-          hex_metric(m, c, x, y, z, I, det);
-          phys_grad<14>(g, I, gp);
-          const double q = nu * det * w;
-          for (int a = 0; a < 14; ++a)
-            for (int b = 0; b < 14; ++b) K[a][b] += q * (gp[a][0] * gp[b][0] + gp[a][1] * gp[b][1] + gp[a][2] * gp[b][2]);
-        }
-    const auto& g = m.hex_dofs[(size_t)c];
+  // union of the hex's and the tet's unknowns of each interface triangle
+  std::vector<std::array<int, 22>> iu((size_t)np2);
+  std::vector<std::array<int, 14>> ihu((size_t)np2);
+  std::vector<std::array<int, 8>> itu((size_t)np2);
+  std::vector<int> inu((size_t)np2);
+  std::vector<int64_t> ioff((size_t)np2 + 1, 0), coff((size_t)np2 + 1, 0);
+  for (int k = 0; k < np2; ++k) {
+    const InterfacePlan& p = plans[(size_t)(k / 2)];
+    const auto& hg = m.hex_dofs[(size_t)p.hex_cell];
+    const auto& tgd = m.tet_dofs[(size_t)p.tet_cell[k % 2]];
+    int n = 0;
     for (int a = 0; a < 14; ++a) {
-      diag_rau[(size_t)g[(size_t)a]] += K[a][a];
-      for (int b = 0; b < 14; ++b) t.push_back({g[(size_t)a], g[(size_t)b], K[a][b]});
+      ihu[(size_t)k][(size_t)a] = n;
+      iu[(size_t)k][(size_t)n++] = hg[(size_t)a];
     }
+    for (int b = 0; b < 8; ++b) {
+      int at = -1;
+      for (int q = 0; q < n; ++q)
+        if (iu[(size_t)k][(size_t)q] == tgd[(size_t)b]) at = q;
+      if (at < 0) {
+        at = n;
+        iu[(size_t)k][(size_t)n++] = tgd[(size_t)b];
+      }
+      itu[(size_t)k][(size_t)b] = at;
+    }
+    inu[(size_t)k] = n;
+    ioff[(size_t)k + 1] = ioff[(size_t)k] + (int64_t)n * n;
+    coff[(size_t)k + 1] = coff[(size_t)k] + n;
   }
+  const int64_t tet0 = (int64_t)nh * 196, if0 = tet0 + (int64_t)nt * 64;
+  std::vector<Trip> t((size_t)(if0 + ioff[(size_t)np2]));
+  std::vector<double> cons((size_t)coff[(size_t)np2]);
+  int bad_hex = -1;
+  // hex volumes: K_ab = sum_q nu det w grad phi_a . grad phi_b (27 points)
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int c = 0; c < nh; ++c) {
+    double K[14][14] = {};
+    try {
+      for (int ix = 0; ix < 3; ++ix)
+        for (int iy = 0; iy < 3; ++iy)
+          for (int iz = 0; iz < 3; ++iz) {
+            const double x = R.g3x[ix], y = R.g3x[iy], z = R.g3x[iz], w = R.g3w[ix] * R.g3w[iy] * R.g3w[iz];
+            double ph[14], g[14][3], gp[14][3], I[9], det;
+            hex_basis(x, y, z, ph, g);
+            hex_metric(m, c, x, y, z, I, det);
+            phys_grad<14>(g, I, gp);
+            const double q = nu * det * w;
+            for (int a = 0; a < 14; ++a)
+              for (int b = 0; b < 14; ++b) K[a][b] += q * (gp[a][0] * gp[b][0] + gp[a][1] * gp[b][1] + gp[a][2] * gp[b][2]);
+          }
+    } catch (...) {
+#pragma omp critical(hybrid_bad_hex)
+      bad_hex = bad_hex < 0 ? c : std::min(bad_hex, c);
+    }
+    const auto& g = m.hex_dofs[(size_t)c];
+    for (int a = 0; a < 14; ++a)
+      for (int b = 0; b < 14; ++b) t[(size_t)(196 * (int64_t)c + a * 14 + b)] = {g[(size_t)a], g[(size_t)b], K[a][b]};
+  }
+  if (bad_hex >= 0) throw std::runtime_error("hybrid mesh: non-positive hex Jacobian in cell " + std::to_string(bad_hex));
   // tet volumes: K_ab = nu det sum_jk D[a][b][j][k] (J^-T J^-1)_jk
   const auto& D = ref_tensors().D;
-  for (int c = 0; c < m.ntet(); ++c) {
+#pragma omp parallel for schedule(static)
+  for (int c = 0; c < nt; ++c) {
     const auto& tg = m.tet_geom[(size_t)c];
     double M[3][3] = {};
     for (int j = 0; j < 3; ++j)
@@ -334,9 +394,7 @@ void assemble_velocity(const HybridMesh& m, const std::vector<InterfacePlan>& pl
         double kd = 0;
         for (int j = 0; j < 3; ++j)
           for (int k = 0; k < 3; ++k) kd += D[a][b][j][k] * M[j][k];
-        const double v = nu * tg[2] * kd;
-        if (a == b) diag_rau[(size_t)g[(size_t)a]] += v;
-        t.push_back({g[(size_t)a], g[(size_t)b], v});
+        t[(size_t)(tet0 + 64 * (int64_t)c + a * 8 + b)] = {g[(size_t)a], g[(size_t)b], nu * tg[2] * kd};
       }
   }
   // Nitsche coupling on each interface triangle.  Over the union u of the
@@ -345,50 +403,54 @@ void assemble_velocity(const HybridMesh& m, const std::vector<InterfacePlan>& pl
   // grad phi^tet_i) . n give K_ij = w (-J_i F_j - F_i J_j + tau J_i J_j),
   // tau = gamma nu max(1/h_hex, 1/h_tet)  (hybrid_hxt4b/hxt4b_main.cu
   // interface_assemble; hybrid_hxt2/hxt2_main.cu interface_kernel)
-  for (const auto& p : plans)
-    for (int s = 0; s < 2; ++s) {
-      const auto& hg = m.hex_dofs[(size_t)p.hex_cell];
-      const auto& tgd = m.tet_dofs[(size_t)p.tet_cell[s]];
-      int u[22], hu[14], tu[8], nu_ = 0;
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int k = 0; k < np2; ++k) {
+    const InterfacePlan& p = plans[(size_t)(k / 2)];
+    const int s = k % 2, nu_ = inu[(size_t)k];
+    const int* hu = ihu[(size_t)k].data();
+    const int* tu = itu[(size_t)k].data();
+    const double tau = gamma * nu * std::max(p.inv_h_hex, p.inv_h_tet[s]);
+    const double* n = p.normal;
+    double K[22][22] = {}, cn[22] = {};
+    try {
+    for_interface_points(m, p, s, [&](double w, const double* ph, const double (*gph)[3], const double* pt,
+                                      const double (*gpt)[3]) {
+      double J[22] = {}, F[22] = {};
       for (int a = 0; a < 14; ++a) {
-        hu[a] = nu_;
-        u[nu_++] = hg[(size_t)a];
+        J[hu[a]] += ph[a];
+        F[hu[a]] += 0.5 * nu * (gph[a][0] * n[0] + gph[a][1] * n[1] + gph[a][2] * n[2]);
       }
       for (int b = 0; b < 8; ++b) {
-        int at = -1;
-        for (int q = 0; q < nu_; ++q)
-          if (u[q] == tgd[(size_t)b]) at = q;
-        if (at < 0) {
-          at = nu_;
-          u[nu_++] = tgd[(size_t)b];
-        }
-        tu[b] = at;
+        J[tu[b]] -= pt[b];
+        F[tu[b]] += 0.5 * nu * (gpt[b][0] * n[0] + gpt[b][1] * n[1] + gpt[b][2] * n[2]);
       }
-      const double tau = gamma * nu * std::max(p.inv_h_hex, p.inv_h_tet[s]);
-      const double* n = p.normal;
-      double K[22][22] = {}, cons[22] = {};
-      for_interface_points(m, p, s, [&](double w, const double* ph, const double (*gph)[3], const double* pt,
-                                        const double (*gpt)[3]) {
-        double J[22] = {}, F[22] = {};
-        for (int a = 0; a < 14; ++a) {
-          J[hu[a]] += ph[a];
-          F[hu[a]] += 0.5 * nu * (gph[a][0] * n[0] + gph[a][1] * n[1] + gph[a][2] * n[2]);
-        }
-        for (int b = 0; b < 8; ++b) {
-          J[tu[b]] -= pt[b];
-          F[tu[b]] += 0.5 * nu * (gpt[b][0] * n[0] + gpt[b][1] * n[1] + gpt[b][2] * n[2]);
-        }
-        for (int i = 0; i < nu_; ++i) {
-          for (int j = 0; j < nu_; ++j) K[i][j] += w * (-F[j] * J[i] - F[i] * J[j] + tau * J[i] * J[j]);
-          cons[i] += w * (-2.0 * F[i] * J[i]);
-        }
-      });
       for (int i = 0; i < nu_; ++i) {
-        diag_rau[(size_t)u[i]] += cons[i];
-        for (int j = 0; j < nu_; ++j) t.push_back({u[i], u[j], K[i][j]});
+        for (int j = 0; j < nu_; ++j) K[i][j] += w * (-F[j] * J[i] - F[i] * J[j] + tau * J[i] * J[j]);
+        cn[i] += w * (-2.0 * F[i] * J[i]);
       }
+    });
+    } catch (...) {
+#pragma omp critical(hybrid_bad_hex)
+      bad_hex = bad_hex < 0 ? p.hex_cell : std::min(bad_hex, p.hex_cell);
     }
-  std::stable_sort(t.begin(), t.end(), [](const Trip& a, const Trip& b) { return std::tie(a.r, a.c) < std::tie(b.r, b.c); });
+    const auto& u = iu[(size_t)k];
+    for (int i = 0; i < nu_; ++i) {
+      cons[(size_t)(coff[(size_t)k] + i)] = cn[i];
+      for (int j = 0; j < nu_; ++j) t[(size_t)(if0 + ioff[(size_t)k] + i * nu_ + j)] = {u[(size_t)i], u[(size_t)j], K[i][j]};
+    }
+  }
+  if (bad_hex >= 0) throw std::runtime_error("hybrid mesh: non-positive hex Jacobian in cell " + std::to_string(bad_hex));
+  // penalty-free diagonal, summed in cell order: hex, tet, then interface
+  for (int c = 0; c < nh; ++c)
+    for (int a = 0; a < 14; ++a) diag_rau[(size_t)t[(size_t)(196 * (int64_t)c + 15 * a)].r] += t[(size_t)(196 * (int64_t)c + 15 * a)].v;
+  for (int c = 0; c < nt; ++c)
+    for (int a = 0; a < 8; ++a) {
+      const Trip& x = t[(size_t)(tet0 + 64 * (int64_t)c + 9 * a)];
+      diag_rau[(size_t)x.r] += x.v;
+    }
+  for (int k = 0; k < np2; ++k)
+    for (int i = 0; i < inu[(size_t)k]; ++i) diag_rau[(size_t)iu[(size_t)k][(size_t)i]] += cons[(size_t)(coff[(size_t)k] + i)];
+  sort_trips(t, nv);
   row.assign((size_t)nv + 1, 0);
   col.clear();
   val.clear();
@@ -596,30 +658,41 @@ HybridFlow build_hybrid_flow(const HybridMesh& m, const std::vector<InterfacePla
   assemble_velocity(m, plans, F.nu, gamma, F.row, F.col, F.base, F.diag_r_base);
   F.diag_pos.resize((size_t)nv);
   for (int i = 0; i < nv; ++i) F.diag_pos[(size_t)i] = csr_find(F.row, F.col, i, i);
-  // convection gather lists: (entry, local value) pairs in cell order
-  std::vector<std::pair<int32_t, int32_t>> c;
-  c.reserve((size_t)m.nhex() * 196 + (size_t)m.ntet() * 64);
+  // convection gather lists: the CSR entry of each local value (local value
+  // q: 196 per hex, row-major, then 64 per tet), then the values of each entry
+  // in cell order (a stable counting sort by entry)
+  const int64_t tet0 = (int64_t)m.nhex() * 196, nloc = tet0 + (int64_t)m.ntet() * 64;
+  if (nloc > INT32_MAX) throw std::runtime_error("mixed mesh too large for 32-bit convection gather lists");
+  std::vector<int32_t> entry((size_t)nloc);
+  auto find = [&](int i, int j) -> int32_t {
+    const auto b = F.col.begin() + F.row[(size_t)i], e = F.col.begin() + F.row[(size_t)i + 1];
+    const auto it = std::lower_bound(b, e, j);
+    return it == e || *it != j ? -1 : (int32_t)(it - F.col.begin());
+  };
+#pragma omp parallel for schedule(static)
   for (int h = 0; h < m.nhex(); ++h) {
     const auto& g = m.hex_dofs[(size_t)h];
     for (int a = 0; a < 14; ++a)
       for (int b = 0; b < 14; ++b)
-        c.push_back({csr_find(F.row, F.col, g[(size_t)a], g[(size_t)b]), h * 196 + a * 14 + b});
+        entry[(size_t)(196 * (int64_t)h + a * 14 + b)] = find(g[(size_t)a], g[(size_t)b]);
   }
-  const int32_t tet0 = m.nhex() * 196;
+#pragma omp parallel for schedule(static)
   for (int t = 0; t < m.ntet(); ++t) {
     const auto& g = m.tet_dofs[(size_t)t];
     for (int a = 0; a < 8; ++a)
       for (int b = 0; b < 8; ++b)
-        c.push_back({csr_find(F.row, F.col, g[(size_t)a], g[(size_t)b]), tet0 + t * 64 + a * 8 + b});
+        entry[(size_t)(tet0 + 64 * (int64_t)t + a * 8 + b)] = find(g[(size_t)a], g[(size_t)b]);
   }
-  std::stable_sort(c.begin(), c.end(), [](const auto& x, const auto& y) { return x.first < y.first; });
+  for (int32_t k : entry)
+    if (k < 0) throw std::runtime_error("hybrid velocity CSR: missing entry");
   F.src_off.assign(F.col.size() + 1, 0);
-  F.src.resize(c.size());
-  for (size_t q = 0; q < c.size(); ++q) {
-    ++F.src_off[(size_t)c[q].first + 1];
-    F.src[q] = c[q].second;
-  }
+  F.src.resize((size_t)nloc);
+  for (int32_t k : entry) ++F.src_off[(size_t)k + 1];
   for (size_t k = 0; k < F.col.size(); ++k) F.src_off[k + 1] += F.src_off[k];
+  {
+    std::vector<int32_t> next(F.src_off.begin(), F.src_off.end() - 1);
+    for (int64_t q = 0; q < nloc; ++q) F.src[(size_t)next[(size_t)entry[(size_t)q]]++] = (int32_t)q;
+  }
   // Dirichlet data and initial state (hxt4b_main.cu:175-186): parabolic
   // axial velocity at every vertex; wall faces no-slip; inlet faces the
   // profile, their bubble the profile at the face centre minus the mean of
@@ -763,8 +836,11 @@ HybridSchurCsr hybrid_schur_csr(const HybridStokes& B, int pin, const std::vecto
   CsrHost& A = H.A;
   A.n = np;
   A.row.assign((size_t)np + 1, 0);
-  std::vector<int32_t> nb;
+  // rows are independent: patterns, then values, in parallel
+  std::vector<std::vector<int32_t>> nbs((size_t)np);
+#pragma omp parallel for schedule(dynamic, 256)
   for (int i = 0; i < np; ++i) {
+    std::vector<int32_t>& nb = nbs[(size_t)i];
     nb.assign(1, i);
     if (i != pin) {
       for (int32_t k = B.b_row[(size_t)i]; k < B.b_row[(size_t)i + 1]; ++k) {
@@ -775,14 +851,17 @@ HybridSchurCsr hybrid_schur_csr(const HybridStokes& B, int pin, const std::vecto
       std::sort(nb.begin(), nb.end());
       nb.erase(std::unique(nb.begin(), nb.end()), nb.end());
     }
-    A.col.insert(A.col.end(), nb.begin(), nb.end());
-    A.row[(size_t)i + 1] = (int64_t)A.col.size();
   }
+  for (int i = 0; i < np; ++i) A.row[(size_t)i + 1] = A.row[(size_t)i] + (int64_t)nbs[(size_t)i].size();
+  A.col.resize((size_t)A.row[(size_t)np]);
   A.val.resize(A.col.size());
-  A.diag.resize((size_t)np);
+  A.diag.assign((size_t)np, 0.0);
   H.entry_row.resize(A.col.size());
   H.diag_pos.assign((size_t)np, -1);
+  int bad = 0;
+#pragma omp parallel for schedule(dynamic, 256) reduction(+ : bad)
   for (int i = 0; i < np; ++i) {
+    std::copy(nbs[(size_t)i].begin(), nbs[(size_t)i].end(), A.col.begin() + A.row[(size_t)i]);
     for (int64_t k = A.row[(size_t)i]; k < A.row[(size_t)i + 1]; ++k) {
       const int j = A.col[(size_t)k];
       H.entry_row[(size_t)k] = i;
@@ -793,9 +872,9 @@ HybridSchurCsr hybrid_schur_csr(const HybridStokes& B, int pin, const std::vecto
         A.diag[(size_t)i] = v;
       }
     }
-    if (!(A.diag[(size_t)i] > 0.0) || !std::isfinite(A.diag[(size_t)i]))
-      throw std::runtime_error("hybrid pressure matrix: nonpositive diagonal");
+    if (!(A.diag[(size_t)i] > 0.0) || !std::isfinite(A.diag[(size_t)i])) ++bad;
   }
+  if (bad) throw std::runtime_error("hybrid pressure matrix: nonpositive diagonal");
   return H;
 }
 
