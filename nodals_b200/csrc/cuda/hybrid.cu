@@ -94,23 +94,35 @@ __global__ void b_mv(int n, const int32_t* __restrict__ row, const int32_t* __re
   s = warp_sum(s);
   if (lane == 0) y[i] = s;
 }
+// sum over the L lanes of an aligned lane group; every lane of the warp calls it
+template <int L>
+__device__ __forceinline__ double group_sum(double v) {
+#pragma unroll
+  for (int o = L / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+// (v0, v1, v2) = B^T p: the transposed rows are short (a velocity unknown
+// touches a few cells), so eight lanes take a row
+constexpr int kBtLanes = 8;
 __global__ void bt_mv(int n, const int32_t* __restrict__ row, const int32_t* __restrict__ col,
                       const double* __restrict__ bx, const double* __restrict__ by, const double* __restrict__ bz,
                       const double* __restrict__ p, double* __restrict__ v0, double* __restrict__ v1,
                       double* __restrict__ v2) {
-  const int i = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
-  if (i >= n) return;
+  const long long gt = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const int i = (int)(gt / kBtLanes), lane = (int)(gt % kBtLanes);
+  const bool live = i < n;
   double s0 = 0, s1 = 0, s2 = 0;
-  for (int k = row[i] + lane; k < row[i + 1]; k += 32) {
-    const double q = p[col[k]];
-    s0 += bx[k] * q;
-    s1 += by[k] * q;
-    s2 += bz[k] * q;
-  }
-  s0 = warp_sum(s0);
-  s1 = warp_sum(s1);
-  s2 = warp_sum(s2);
-  if (lane == 0) {
+  if (live)
+    for (int k = row[i] + lane; k < row[i + 1]; k += kBtLanes) {
+      const double q = p[col[k]];
+      s0 += bx[k] * q;
+      s1 += by[k] * q;
+      s2 += bz[k] * q;
+    }
+  s0 = group_sum<kBtLanes>(s0);
+  s1 = group_sum<kBtLanes>(s1);
+  s2 = group_sum<kBtLanes>(s2);
+  if (live && lane == 0) {
     v0[i] = s0;
     v1[i] = s1;
     v2[i] = s2;
@@ -231,7 +243,7 @@ struct Div {
     NDS_LAUNCH();
   }
   void BT(const double* p, double* v0, double* v1, double* v2) {
-    bt_mv<<<grid((long long)nv * 32), kTPB>>>(nv, trow.p, tcol.p, tx.p, ty.p, tz.p, p, v0, v1, v2);
+    bt_mv<<<grid((long long)nv * kBtLanes), kTPB>>>(nv, trow.p, tcol.p, tx.p, ty.p, tz.p, p, v0, v1, v2);
     NDS_LAUNCH();
   }
 };
@@ -1076,16 +1088,20 @@ __global__ void amg_gs_colour(int count, const int32_t* __restrict__ rows, const
     x[i] = old + w * ((b[i] - off) / diag[i] - old);
   }
 }
-// y += A x (prolongation) or y = A x (restriction through P^T), warp per row
+// y += A x (prolongation) or y = A x (levels, restriction through P^T), L
+// lanes per row (8 for the short rows of P, 32 otherwise)
+template <int L>
 __global__ void amg_csr_add(int n, const int32_t* __restrict__ row, const int32_t* __restrict__ col,
                             const double* __restrict__ val, const double* __restrict__ x, double* __restrict__ y,
                             int accumulate) {
-  const int i = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
-  if (i >= n) return;
+  const long long gt = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const int i = (int)(gt / L), lane = (int)(gt % L);
+  const bool live = i < n;
   double s = 0;
-  for (int k = row[i] + lane; k < row[i + 1]; k += 32) s += val[k] * x[col[k]];
-  s = warp_sum(s);
-  if (lane == 0) y[i] = accumulate ? y[i] + s : s;
+  if (live)
+    for (int k = row[i] + lane; k < row[i + 1]; k += L) s += val[k] * x[col[k]];
+  s = group_sum<L>(s);
+  if (live && lane == 0) y[i] = accumulate ? y[i] + s : s;
 }
 // x = inv b with a dense row-major inverse, warp per row
 __global__ void amg_dense(int n, const double* __restrict__ inv, const double* __restrict__ b, double* __restrict__ x) {
@@ -1163,7 +1179,7 @@ struct AmgLevel {
     }
   }
   void apply(const double* in, double* out) const {
-    amg_csr_add<<<grid((long long)n * 32), kTPB>>>(n, row.p, col.p, val.p, in, out, 0);
+    amg_csr_add<32><<<grid((long long)n * 32), kTPB>>>(n, row.p, col.p, val.p, in, out, 0);
     NDS_LAUNCH();
   }
 };
@@ -1189,11 +1205,11 @@ struct AmgTransfer {
     rval.upload(rv);
   }
   void restrict_to(const double* f, double* c) const {
-    amg_csr_add<<<grid((long long)nc * 32), kTPB>>>(nc, rrow.p, rcol.p, rval.p, f, c, 0);
+    amg_csr_add<32><<<grid((long long)nc * 32), kTPB>>>(nc, rrow.p, rcol.p, rval.p, f, c, 0);
     NDS_LAUNCH();
   }
   void prolong_add(const double* c, double* f) const {
-    amg_csr_add<<<grid((long long)nf * 32), kTPB>>>(nf, prow.p, pcol.p, pval.p, c, f, 1);
+    amg_csr_add<8><<<grid((long long)nf * 8), kTPB>>>(nf, prow.p, pcol.p, pval.p, c, f, 1);
     NDS_LAUNCH();
   }
 };
