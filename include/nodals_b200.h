@@ -307,6 +307,16 @@ int nds_hybrid_flow(const char* hxt1_path, const nds_hybrid_flow_options* o, int
  * header read by nds_hybrid_counts.  Any of the four may be NULL. */
 int nds_hybrid_flow_fields(const char* hxt1_path, const nds_hybrid_flow_options* o, int device, int verbose,
                            nds_hybrid_flow_report* out, double* u0, double* u1, double* u2, double* pressure);
+/* Host only: the patch and symmetry audit of the mixed-mesh velocity
+ * operator that the reference's HXT2 gate prints (hybrid_hxt2/hxt2_main.cu:
+ * 296-315), on the operator without boundary conditions (nu-scaled
+ * diffusion, with or without the Nitsche interface terms):
+ * out[0] max |A 1| (constant patch, with interface); out[1..3] and out[4..6]
+ * max |A u| over the interface bubbles for the three affine fields, without
+ * and with the interface terms; out[7..10] x.Ax, y.Ay, x.Ay, y.Ax for x, y
+ * supported on the interface bubbles (x_g = sin(0.001731 (g+1)), y_g =
+ * cos(0.002117 (g+3))); out[11] the number of interface bubble unknowns. */
+int nds_hybrid_operator_patch(const char* hxt1_path, double nu, double gamma, double out[12]);
 /* Host only: the 13 counts of a mixed-mesh HXT1 header (nv nhex ntet
  * nhexface ntetface nvel npressure ninterface nwallhex ninhex nintet
  * nouthex nouttet). */

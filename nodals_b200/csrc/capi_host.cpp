@@ -183,6 +183,75 @@ int nds_hybrid_operator_audit(const char* path, double nu, double gamma, double 
   }
 }
 
+int nds_hybrid_operator_patch(const char* path, double nu, double gamma, double out[12]) {
+  if (!path || !out || !(nu > 0) || !(gamma > 0)) { set_error("nds_hybrid_operator_patch: bad argument"); return NDS_E_INVALID; }
+  try {
+    const nds::HybridMesh m = nds::read_hxt1_hybrid(path);
+    const auto P = nds::interface_plans(m);
+    std::vector<int32_t> fr, fc, vr, vc;
+    std::vector<double> fv, vv;
+    nds::hybrid_velocity_operator(m, P, nu, gamma, true, fr, fc, fv);
+    nds::hybrid_velocity_operator(m, P, nu, gamma, false, vr, vc, vv);
+    const int nv = m.nvel();
+    auto apply = [&](const std::vector<int32_t>& r, const std::vector<int32_t>& c, const std::vector<double>& v,
+                     const std::vector<double>& x) {
+      std::vector<double> y((size_t)nv, 0.0);
+      for (int i = 0; i < nv; ++i)
+        for (int32_t k = r[(size_t)i]; k < r[(size_t)i + 1]; ++k) y[(size_t)i] += v[(size_t)k] * x[(size_t)c[(size_t)k]];
+      return y;
+    };
+    // vertex values c + a . x, bubbles zero (the field is in both spaces)
+    auto affine = [&](double c0, double ax, double ay, double az) {
+      std::vector<double> u((size_t)nv, 0.0);
+      for (int i = 0; i < m.nv(); ++i)
+        u[(size_t)i] = c0 + ax * m.xyz[3 * (size_t)i] + ay * m.xyz[3 * (size_t)i + 1] + az * m.xyz[3 * (size_t)i + 2];
+      return u;
+    };
+    std::vector<int32_t> ids;
+    for (const auto& r : m.interface) {
+      ids.push_back(r[2]);
+      ids.push_back(r[5]);
+      ids.push_back(r[8]);
+    }
+    std::sort(ids.begin(), ids.end());
+    ids.erase(std::unique(ids.begin(), ids.end()), ids.end());
+    auto bubble_max = [&](const std::vector<double>& y) {
+      double q = 0;
+      for (int32_t g : ids) q = std::max(q, std::abs(y[(size_t)g]));
+      return q;
+    };
+    double cmax = 0;
+    for (double v : apply(fr, fc, fv, affine(1.0, 0, 0, 0))) cmax = std::max(cmax, std::abs(v));
+    out[0] = cmax;
+    const double coeff[3][4] = {{0.7, 1.0, 0.20, -0.10}, {-0.4, 0.30, 1.10, 0.15}, {0.2, -0.25, 0.35, 0.90}};
+    for (int k = 0; k < 3; ++k) {
+      const auto u = affine(coeff[k][0], coeff[k][1], coeff[k][2], coeff[k][3]);
+      out[1 + k] = bubble_max(apply(vr, vc, vv, u));
+      out[4 + k] = bubble_max(apply(fr, fc, fv, u));
+    }
+    std::vector<double> x((size_t)nv, 0.0), y((size_t)nv, 0.0);
+    for (int32_t g : ids) {
+      x[(size_t)g] = std::sin(0.001731 * (g + 1));
+      y[(size_t)g] = std::cos(0.002117 * (g + 3));
+    }
+    const auto Ax = apply(fr, fc, fv, x), Ay = apply(fr, fc, fv, y);
+    auto dot = [&](const std::vector<double>& a, const std::vector<double>& b) {
+      long double q = 0;
+      for (int i = 0; i < nv; ++i) q += (long double)a[(size_t)i] * b[(size_t)i];
+      return (double)q;
+    };
+    out[7] = dot(x, Ax);
+    out[8] = dot(y, Ay);
+    out[9] = dot(x, Ay);
+    out[10] = dot(y, Ax);
+    out[11] = (double)ids.size();
+    return NDS_OK;
+  } catch (const std::exception& e) {
+    set_error(e.what());
+    return NDS_E_SETUP;
+  }
+}
+
 int nds_hybrid_counts(const char* path, uint64_t counts[13]) {
   if (!path || !counts) { set_error("null argument"); return NDS_E_INVALID; }
   try {

@@ -316,9 +316,9 @@ void sort_trips(std::vector<Trip>& t, int nrows) {
 // the merge of duplicates then follow that order, as a serial loop would.
 void assemble_velocity(const HybridMesh& m, const std::vector<InterfacePlan>& plans, double nu, double gamma,
                        std::vector<int32_t>& row, std::vector<int32_t>& col, std::vector<double>& val,
-                       std::vector<double>& diag_rau) {
+                       std::vector<double>& diag_rau, bool with_interface = true) {
   const Rules& R = rules();
-  const int nv = m.nvel(), nh = m.nhex(), nt = m.ntet(), np2 = 2 * (int)plans.size();
+  const int nv = m.nvel(), nh = m.nhex(), nt = m.ntet(), np2 = with_interface ? 2 * (int)plans.size() : 0;
   diag_rau.assign((size_t)nv, 0.0);
   // union of the hex's and the tet's unknowns of each interface triangle
   std::vector<std::array<int, 22>> iu((size_t)np2);
@@ -876,6 +876,13 @@ HybridSchurCsr hybrid_schur_csr(const HybridStokes& B, int pin, const std::vecto
   }
   if (bad) throw std::runtime_error("hybrid pressure matrix: nonpositive diagonal");
   return H;
+}
+
+void hybrid_velocity_operator(const HybridMesh& m, const std::vector<InterfacePlan>& plans, double nu, double gamma,
+                              bool with_interface, std::vector<int32_t>& row, std::vector<int32_t>& col,
+                              std::vector<double>& val) {
+  std::vector<double> diag;
+  assemble_velocity(m, plans, nu, gamma, row, col, val, diag, with_interface);
 }
 
 int hybrid_pin(const HybridMesh& m) {

@@ -115,6 +115,12 @@ struct HybridSchurCsr {
   std::vector<int32_t> entry_row, diag_pos;
 };
 HybridSchurCsr hybrid_schur_csr(const HybridStokes& B, int pin, const std::vector<double>& rau);
+// velocity operator without boundary conditions: nu-scaled diffusion of the
+// hex (Q1+BF2) and tet (P1+BF3) cells, plus the Nitsche coupling of the
+// interface when with_interface (CSR, columns sorted)
+void hybrid_velocity_operator(const HybridMesh& m, const std::vector<InterfacePlan>& plans, double nu, double gamma,
+                              bool with_interface, std::vector<int32_t>& row, std::vector<int32_t>& col,
+                              std::vector<double>& val);
 // pressure gauge cell of the pipe solvers: the first outlet face's cell
 // (hybrid_hxt4b/hxt4b_main.cu:236)
 int hybrid_pin(const HybridMesh& m);

@@ -216,3 +216,27 @@ def test_pipe_simple_reference_cheb2_vcycle_breaks_pcg(tmp_path):
                         str(tmp_path / "x.vtu"), "--p-max", "400", *AMG], capture_output=True, text=True, timeout=600)
     assert r.returncode == 2
     assert "nonpositive" in r.stderr and "HXT4B_GATE_STATUS=FAIL" in r.stderr
+
+
+def test_operator_patch_matches_reference_hxt2_gate(native):
+    """The velocity operator without boundary conditions (nu 1, gamma 20)
+    against the reference's HXT2 gate run on the same mesh
+    (tests/golden/hxt2_hybrid_r2.log, made by make_hxt2_golden.py): the
+    volume-only residual of each affine field at the interface bubbles and
+    the energies x.Ax, y.Ay, x.Ay, y.Ax to 1e-11 (12 printed digits); the
+    gate's own criteria for the round-off quantities (constant patch below
+    1e-11, Nitsche cancelling the affine interface residual to 1e-7 of it,
+    symmetry)."""
+    lines = (GOLDEN / "hxt2_hybrid_r2.log").read_text().splitlines()
+    aff = [_kv(l) for l in lines if l.startswith("NODALS_HXT2_AFFINE_PATCH")]
+    sym = next(_kv(l) for l in lines if l.startswith("NODALS_HXT2_SYMMETRY_ENERGY"))
+    out = (C.c_double * 12)()
+    assert native.lib().nds_hybrid_operator_patch(str(MESH).encode(), C.c_double(1.0), C.c_double(20.0), out) == 0
+    assert out[0] < 1e-11
+    for k, a in enumerate(aff):
+        assert _close(out[1 + k], a["volumeInterfaceBubbleMax"], 1e-11), (k, out[1 + k], a)
+        assert out[4 + k] < 1e-7 * out[1 + k]
+    for i, key in enumerate(("xAx", "yAy", "xAy", "yAx")):
+        assert _close(out[7 + i], sym[key], 1e-11), (key, out[7 + i], sym[key])
+    assert int(out[11]) == int(sym["interfaceBubbleDofs"])
+    assert abs(out[9] - out[10]) <= 1e-12 * abs(out[9])
