@@ -317,6 +317,16 @@ int nds_hybrid_flow_fields(const char* hxt1_path, const nds_hybrid_flow_options*
  * supported on the interface bubbles (x_g = sin(0.001731 (g+1)), y_g =
  * cos(0.002117 (g+3))); out[11] the number of interface bubble unknowns. */
 int nds_hybrid_operator_patch(const char* hxt1_path, double nu, double gamma, double out[12]);
+/* Host only: the divergence audit that the reference's HXT3A gate prints
+ * (hybrid_hxt3a/hxt3a_main.cu main), with its synthetic rAU_g = 0.8 + 0.2
+ * (0.5 + 0.5 sin(0.000731 (g+1))): out[0] nnz of B; out[1] max |B u| over
+ * the three constant fields; out[2], out[3] max abs / rel error of B (x,y,z)
+ * against 3 V; out[4], out[5] p.Bu and u.B^T p; out[6..9] x.Sx, y.Sy, x.Sy,
+ * y.Sx with S = B diag(rAU) B^T; out[10], out[11] min / max norm of the
+ * cross-region trace coefficients of each interface triangle pair; out[12],
+ * out[13] min / max |S_ht| of those pairs; out[14] the number of pairs;
+ * out[15] pairs missing a cross trace or with S_ht = 0. */
+int nds_hybrid_divergence_audit(const char* hxt1_path, double out[16]);
 /* Host only: the 13 counts of a mixed-mesh HXT1 header (nv nhex ntet
  * nhexface ntetface nvel npressure ninterface nwallhex ninhex nintet
  * nouthex nouttet). */

@@ -252,6 +252,162 @@ int nds_hybrid_operator_patch(const char* path, double nu, double gamma, double 
   }
 }
 
+int nds_hybrid_divergence_audit(const char* path, double out[16]) {
+  if (!path || !out) { set_error("nds_hybrid_divergence_audit: null argument"); return NDS_E_INVALID; }
+  try {
+    const nds::HybridMesh m = nds::read_hxt1_hybrid(path);
+    const auto P = nds::interface_plans(m);
+    nds::HybridStokes B;
+    nds::build_hybrid_divergence(m, P, B);
+    const int nv = B.nvel, np = B.np, nh = m.nhex();
+    std::vector<double> rau((size_t)nv);
+    for (int g = 0; g < nv; ++g) rau[(size_t)g] = 0.8 + 0.2 * (0.5 + 0.5 * std::sin(0.000731 * (g + 1)));
+    auto Bu = [&](const std::vector<double>& u0, const std::vector<double>& u1, const std::vector<double>& u2) {
+      std::vector<double> y((size_t)np, 0.0);
+      for (int i = 0; i < np; ++i)
+        for (int32_t k = B.b_row[(size_t)i]; k < B.b_row[(size_t)i + 1]; ++k) {
+          const size_t g = (size_t)B.b_col[(size_t)k];
+          y[(size_t)i] += B.bx[(size_t)k] * u0[g] + B.by[(size_t)k] * u1[g] + B.bz[(size_t)k] * u2[g];
+        }
+      return y;
+    };
+    auto BTp = [&](const std::vector<double>& p, std::vector<double> v[3]) {
+      for (int d = 0; d < 3; ++d) v[d].assign((size_t)nv, 0.0);
+      for (int g = 0; g < nv; ++g)
+        for (int32_t k = B.bt_row[(size_t)g]; k < B.bt_row[(size_t)g + 1]; ++k) {
+          const double q = p[(size_t)B.bt_col[(size_t)k]];
+          v[0][(size_t)g] += B.btx[(size_t)k] * q;
+          v[1][(size_t)g] += B.bty[(size_t)k] * q;
+          v[2][(size_t)g] += B.btz[(size_t)k] * q;
+        }
+    };
+    auto dot = [](const std::vector<double>& a, const std::vector<double>& b) {
+      long double q = 0;
+      for (size_t i = 0; i < a.size(); ++i) q += (long double)a[i] * b[i];
+      return (double)q;
+    };
+    out[0] = (double)B.b_col.size();
+    double cmax = 0;
+    for (int d = 0; d < 3; ++d) {
+      std::vector<double> u[3] = {std::vector<double>((size_t)nv, 0.0), std::vector<double>((size_t)nv, 0.0),
+                                  std::vector<double>((size_t)nv, 0.0)};
+      for (int v = 0; v < m.nv(); ++v) u[d][(size_t)v] = 1.0;
+      for (double y : Bu(u[0], u[1], u[2])) cmax = std::max(cmax, std::abs(y));
+    }
+    out[1] = cmax;
+    {
+      std::vector<double> u[3] = {std::vector<double>((size_t)nv, 0.0), std::vector<double>((size_t)nv, 0.0),
+                                  std::vector<double>((size_t)nv, 0.0)};
+      for (int v = 0; v < m.nv(); ++v)
+        for (int d = 0; d < 3; ++d) u[d][(size_t)v] = m.xyz[3 * (size_t)v + d];
+      const auto dv = Bu(u[0], u[1], u[2]);
+      double ma = 0, mr = 0;
+      for (int c = 0; c < np; ++c) {
+        const double V = c < nh ? m.hex_geom[(size_t)c][0] : m.tet_geom[(size_t)(c - nh)][0];
+        const double e = std::abs(dv[(size_t)c] - 3.0 * V);
+        ma = std::max(ma, e);
+        mr = std::max(mr, e / std::max(std::abs(3.0 * V), 1e-300));
+      }
+      out[2] = ma;
+      out[3] = mr;
+    }
+    {
+      std::vector<double> r[3] = {std::vector<double>((size_t)nv), std::vector<double>((size_t)nv),
+                                  std::vector<double>((size_t)nv)};
+      std::vector<double> pp((size_t)np), bt[3];
+      for (int g = 0; g < nv; ++g) {
+        const double q = g + 1;
+        r[0][(size_t)g] = std::sin(.00113 * q);
+        r[1][(size_t)g] = std::cos(.00171 * q);
+        r[2][(size_t)g] = std::sin(.00091 * q + .3);
+      }
+      for (int i = 0; i < np; ++i) pp[(size_t)i] = std::cos(.00137 * (i + 1) + .2);
+      BTp(pp, bt);
+      out[4] = dot(pp, Bu(r[0], r[1], r[2]));
+      out[5] = dot(r[0], bt[0]) + dot(r[1], bt[1]) + dot(r[2], bt[2]);
+    }
+    {
+      std::vector<double> px((size_t)np), py((size_t)np);
+      for (int i = 0; i < np; ++i) {
+        const double q = i + 1;
+        px[(size_t)i] = std::sin(.00073 * q);
+        py[(size_t)i] = std::cos(.00109 * q + .17);
+      }
+      auto S = [&](const std::vector<double>& x) {
+        std::vector<double> v[3];
+        BTp(x, v);
+        for (int d = 0; d < 3; ++d)
+          for (int g = 0; g < nv; ++g) v[d][(size_t)g] *= rau[(size_t)g];
+        return Bu(v[0], v[1], v[2]);
+      };
+      const auto Sx = S(px), Sy = S(py);
+      out[6] = dot(px, Sx);
+      out[7] = dot(py, Sy);
+      out[8] = dot(px, Sy);
+      out[9] = dot(py, Sx);
+    }
+    // interface sensitivity: each hex row carries the tet's traces and the
+    // other way round, and the direct Schur entry of the pair is nonzero
+    auto coeff = [&](int row, int g, double b[3]) {
+      const auto bg = B.b_col.begin() + B.b_row[(size_t)row], en = B.b_col.begin() + B.b_row[(size_t)row + 1];
+      const auto it = std::lower_bound(bg, en, g);
+      if (it == en || *it != g) return false;
+      const size_t k = (size_t)(it - B.b_col.begin());
+      b[0] = B.bx[k];
+      b[1] = B.by[k];
+      b[2] = B.bz[k];
+      return true;
+    };
+    double cmin = 1e300, cmx = 0, smin = 1e300, smx = 0;
+    int missing = 0;
+    for (const auto& p : P)
+      for (int s2 = 0; s2 < 2; ++s2) {
+        const int rh = p.hex_cell, rt = nh + p.tet_cell[s2];
+        const auto& tv = m.tet_dofs[(size_t)p.tet_cell[s2]];
+        const auto& hv = m.hex_dofs[(size_t)p.hex_cell];
+        bool h_has_t = false, t_has_h = false;
+        double cm = 0, b[3];
+        for (int a = 0; a < 8; ++a)
+          if (coeff(rh, tv[(size_t)a], b)) {
+            h_has_t = true;
+            cm = std::max(cm, std::sqrt(b[0] * b[0] + b[1] * b[1] + b[2] * b[2]));
+          }
+        for (int a = 0; a < 14; ++a)
+          if (coeff(rt, hv[(size_t)a], b)) {
+            t_has_h = true;
+            cm = std::max(cm, std::sqrt(b[0] * b[0] + b[1] * b[1] + b[2] * b[2]));
+          }
+        long double ss = 0;
+        for (int32_t k = B.b_row[(size_t)rh]; k < B.b_row[(size_t)rh + 1]; ++k) {
+          double bt[3];
+          if (coeff(rt, B.b_col[(size_t)k], bt))
+            ss += (long double)rau[(size_t)B.b_col[(size_t)k]] *
+                  (B.bx[(size_t)k] * bt[0] + B.by[(size_t)k] * bt[1] + B.bz[(size_t)k] * bt[2]);
+        }
+        const double sa = std::abs((double)ss);
+        if (!(h_has_t && t_has_h) || !(sa > 0)) ++missing;
+        if (sa > 0) {
+          smin = std::min(smin, sa);
+          smx = std::max(smx, sa);
+        }
+        if (cm > 0) {
+          cmin = std::min(cmin, cm);
+          cmx = std::max(cmx, cm);
+        }
+      }
+    out[10] = cmin;
+    out[11] = cmx;
+    out[12] = smin;
+    out[13] = smx;
+    out[14] = 2.0 * (double)P.size();
+    out[15] = missing;
+    return NDS_OK;
+  } catch (const std::exception& e) {
+    set_error(e.what());
+    return NDS_E_SETUP;
+  }
+}
+
 int nds_hybrid_counts(const char* path, uint64_t counts[13]) {
   if (!path || !counts) { set_error("null argument"); return NDS_E_INVALID; }
   try {

@@ -240,3 +240,33 @@ def test_operator_patch_matches_reference_hxt2_gate(native):
         assert _close(out[7 + i], sym[key], 1e-11), (key, out[7 + i], sym[key])
     assert int(out[11]) == int(sym["interfaceBubbleDofs"])
     assert abs(out[9] - out[10]) <= 1e-12 * abs(out[9])
+
+
+def test_divergence_audit_matches_reference_hxt3a_gate(native):
+    """The divergence B of the mixed mesh against the reference's HXT3A gate
+    run on the same mesh (tests/golden/hxt3a_hybrid_r2.log, made by
+    make_hxt3a_golden.py): the nonzero count exactly, p.Bu, u.B^T p, the four
+    Schur energies, the cross-region trace norms and direct Schur entries to
+    1e-11; the round-off quantities (constant and affine divergence) within
+    1e-15.  (The reference gate itself reports FAIL on this mesh: its
+    constant-divergence bound of 2e-18 is below the 4.9e-17 round-off that
+    both codes give.)"""
+    kv = {}
+    for l in (GOLDEN / "hxt3a_hybrid_r2.log").read_text().splitlines():
+        if l.startswith("NODALS_HXT3A_"):
+            kv[l.split()[0]] = _kv(l)
+    out = (C.c_double * 16)()
+    assert native.lib().nds_hybrid_divergence_audit(str(MESH).encode(), out) == 0
+    assert int(out[0]) == int(kv["NODALS_HXT3A_BCSR"]["nnz"])
+    assert abs(out[1] - float(kv["NODALS_HXT3A_CONSTANT_DIVERGENCE"]["cellResidualMax"])) < 1e-15
+    aff = kv["NODALS_HXT3A_AFFINE_DIVERGENCE"]
+    assert abs(out[2] - float(aff["maxAbs"])) < 1e-15 and out[3] < 2e-10
+    t = kv["NODALS_HXT3A_TRANSPOSE"]
+    assert _close(out[4], t["pDotBu"], 1e-11) and _close(out[5], t["uDotBTp"], 1e-11)
+    sc = kv["NODALS_HXT3A_SCHUR"]
+    for i, key in enumerate(("xSx", "ySy", "xSy", "ySx")):
+        assert _close(out[6 + i], sc[key], 1e-11), (key, out[6 + i], sc[key])
+    s = kv["NODALS_HXT3A_INTERFACE_SENSITIVITY"]
+    for i, key in enumerate(("crossCoeffNormMin", "crossCoeffNormMax", "directSchurAbsMin", "directSchurAbsMax")):
+        assert _close(out[10 + i], s[key], 1e-11), (key, out[10 + i], s[key])
+    assert int(out[14]) == int(s["trianglePairs"]) and int(out[15]) == 0
