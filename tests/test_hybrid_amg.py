@@ -144,3 +144,25 @@ def test_device_separate_post_vcycle_matches_oracle(native, name):
                                  **po)
     want = VCycle(_hierarchy(case), dict(oo, separate_post=True)).apply(v["b"])
     assert _rel(z, want) < 1e-12, (name, _rel(z, want))
+
+
+@pytest.mark.parametrize("args, message", [
+    (["--bogus", "1"], "unknown argument --bogus"),
+    (["--pressure-solver", "pcg_gmres"], "pressure solver must be pcg_amg or pcg_jacobi"),
+    (["--amg-hierarchy", "sa"], "--amg-hierarchy must be cf"),
+    (["--amg-smoother", "ilu"], "unknown AMG smoother"),
+    (["--cf-interp", "classical"], "CF interp must be direct or exti"),
+    (["--momentum-work", "sgs2"], "momentum-work must be fgs1, altgs1, or sgs1"),
+    (["--alpha-u", "1.5"], "bad relaxation"),
+    (["--p-max"], "missing value for --p-max"),
+])
+def test_hxt4b_executable_rejects_bad_flags(native, args, message):
+    """Flag errors end the run before any device work, with exit code 2 and
+    the reference's HXT4B_ERROR / HXT4B_GATE_STATUS=FAIL lines on stderr
+    (hybrid_hxt4b/hxt4b_main.cu:218, 269)."""
+    import subprocess
+    from conftest import ROOT
+    exe = ROOT / "nodals_b200" / "_lib" / "nodals_hxt4b_fp64"
+    r = subprocess.run([str(exe), "--mesh", str(MESH), *args], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 2
+    assert message in r.stderr and "HXT4B_GATE_STATUS=FAIL" in r.stderr
