@@ -1681,6 +1681,7 @@ extern "C" int nds_hybrid_amg_vcycle(const char* hxt1_path, const double* rau, c
     return NDS_E_INVALID;
   }
   try {
+    nds::hybrid_amg_options(*o);  // option errors before any device work
     int ndev = 0;
     const cudaError_t e = cudaGetDeviceCount(&ndev);
     if (e != cudaSuccess || ndev <= device) throw nds::CudaError(std::string("no CUDA device available: ") + cudaGetErrorString(e));
@@ -1777,6 +1778,7 @@ extern "C" int nds_hybrid_flow_fields(const char* hxt1_path, const nds_hybrid_fl
     return NDS_E_INVALID;
   }
   try {
+    if (o->pressure_solver == 1) nds::hybrid_amg_options(*o);  // option errors before any device work
     int ndev = 0;
     const cudaError_t e = cudaGetDeviceCount(&ndev);
     if (e != cudaSuccess || ndev <= device) throw nds::CudaError(std::string("no CUDA device available: ") + cudaGetErrorString(e));

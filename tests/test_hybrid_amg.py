@@ -166,3 +166,17 @@ def test_hxt4b_executable_rejects_bad_flags(native, args, message):
     r = subprocess.run([str(exe), "--mesh", str(MESH), *args], capture_output=True, text=True, timeout=60)
     assert r.returncode == 2
     assert message in r.stderr and "HXT4B_GATE_STATUS=FAIL" in r.stderr
+
+
+def test_flow_rejects_bad_pressure_options_before_device_work(native):
+    """nds_hybrid_flow_fields checks its options before it looks for a
+    device, so a bad preconditioner option is NDS_E_INVALID on any host."""
+    import ctypes as C
+    o = native.HybridFlowOptions.make(pressure_solver=1, amg_smoother=3, amg_mcgs_order=2)
+    r = native.HybridFlowReport()
+    rc = native.lib().nds_hybrid_flow_fields(str(MESH).encode(), C.byref(o), 0, 0, C.byref(r), None, None, None, None)
+    assert rc == -1, native.lib().nds_last_error()
+    assert b"symmetric MCGS" in native.lib().nds_last_error()
+    o2 = native.HybridFlowOptions.make(pressure_solver=7)
+    assert native.lib().nds_hybrid_flow_fields(str(MESH).encode(), C.byref(o2), 0, 0, C.byref(r), None, None, None,
+                                               None) == -1
