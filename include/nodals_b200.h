@@ -349,6 +349,14 @@ int nds_hybrid_amg_create(const char* hxt1_path, const double* rau, const nds_hy
                           nds_hybrid_amg** out);
 int nds_hybrid_amg_array(const nds_hybrid_amg* h, const char* name, nds_array* out);
 void nds_hybrid_amg_destroy(nds_hybrid_amg* h);
+/* Host only: the mixed-mesh pipe SIMPLE's host setup, as a handle of the same
+ * kind (read with nds_hybrid_amg_array, free with nds_hybrid_amg_destroy):
+ * "flow.scalars" (pin, R, L, D, nu, nhex, ntet), the velocity CSR
+ * "flow.row|col|diagPos", its constant values "flow.base" and penalty-free
+ * diagonal "flow.diagRBase", the convection gather lists "flow.srcOff|src",
+ * "flow.fixed", the initial state "flow.u0|u1|u2", the colours
+ * "flow.colourOff|colourRows" and the divergence "b.row|col|bx|by|bz". */
+int nds_hybrid_flow_setup(const char* hxt1_path, const nds_hybrid_flow_options* o, nds_hybrid_amg** out);
 /* One application of that preconditioner on the device: the hierarchy is
  * built from rau, the fine matrix refreshed from rau on the device, and
  * z = M^-1 b (np values each) computed by the reference's V-cycle

@@ -32,6 +32,8 @@ namespace {
 struct HybridAmgHandle {
   nds::HybridSchurCsr fine;
   nds::Hierarchy H;
+  nds::HybridFlow flow;
+  nds::HybridStokes div;
   std::vector<double> scalars[4];
   std::vector<int64_t> ncoarse;
   std::map<std::string, nds_array> arrays;
@@ -467,6 +469,49 @@ int nds_hybrid_amg_create(const char* path, const double* rau, const nds_hybrid_
   } catch (const std::invalid_argument& e) {
     set_error(e.what());
     return NDS_E_INVALID;
+  } catch (const std::exception& e) {
+    set_error(e.what());
+    return NDS_E_SETUP;
+  }
+}
+
+int nds_hybrid_flow_setup(const char* path, const nds_hybrid_flow_options* o, nds_hybrid_amg** out) {
+  if (!path || !o || !out) { set_error("null argument"); return NDS_E_INVALID; }
+  try {
+    auto h = std::make_unique<HybridAmgHandle>();
+    const nds::HybridMesh m = nds::read_hxt1_hybrid(path);
+    const auto P = nds::interface_plans(m);
+    nds::HybridFlow& F = h->flow;
+    F = nds::build_hybrid_flow(m, P, o->re, o->bulk, o->gamma);
+    nds::build_hybrid_divergence(m, P, h->div);
+    auto& A = h->arrays;
+    h->scalars[0] = {(double)F.pin, F.radius, F.length, F.diameter, F.nu, (double)F.nhex, (double)F.ntet};
+    A["flow.scalars"] = view_of(h->scalars[0], 0);  // pin, R, L, D, nu, nhex, ntet
+    A["flow.row"] = view_of(F.row, 1);
+    A["flow.col"] = view_of(F.col, 1);
+    A["flow.diagPos"] = view_of(F.diag_pos, 1);
+    A["flow.base"] = view_of(F.base, 0);
+    A["flow.diagRBase"] = view_of(F.diag_r_base, 0);
+    A["flow.srcOff"] = view_of(F.src_off, 1);
+    A["flow.src"] = view_of(F.src, 1);
+    A["flow.fixed"] = view_of(F.fixed, 3);
+    A["flow.u0"] = view_of(F.u0, 0);
+    A["flow.u1"] = view_of(F.u1, 0);
+    A["flow.u2"] = view_of(F.u2, 0);
+    A["flow.colourOff"] = view_of(F.colour_off, 1);
+    A["flow.colourRows"] = view_of(F.colour_rows, 1);
+    A["b.row"] = view_of(h->div.b_row, 1);
+    A["b.col"] = view_of(h->div.b_col, 1);
+    A["b.bx"] = view_of(h->div.bx, 0);
+    A["b.by"] = view_of(h->div.by, 0);
+    A["b.bz"] = view_of(h->div.bz, 0);
+    {
+      const auto& T = nds::ref_tensors().T;
+      h->scalars[1].assign(&T[0][0][0][0], &T[0][0][0][0] + 8 * 8 * 8 * 3);
+      A["centT"] = view_of(h->scalars[1], 0);  // T[a][m][b][j] = int phi_a phi_m dphi_b/dxi_j on the reference tet
+    }
+    *out = reinterpret_cast<nds_hybrid_amg*>(h.release());
+    return NDS_OK;
   } catch (const std::exception& e) {
     set_error(e.what());
     return NDS_E_SETUP;

@@ -187,6 +187,7 @@ def lib():
         L.nds_hybrid_amg_create.argtypes = [C.c_char_p, vp, C.POINTER(HybridFlowOptions), C.POINTER(vp)]
         L.nds_hybrid_amg_array.argtypes = [vp, C.c_char_p, C.POINTER(_Array)]
         L.nds_hybrid_amg_destroy.argtypes = [vp]
+        L.nds_hybrid_flow_setup.argtypes = [C.c_char_p, C.POINTER(HybridFlowOptions), C.POINTER(vp)]
         if hasattr(L, "nds_hybrid_amg_vcycle"):
             L.nds_hybrid_amg_vcycle.argtypes = [C.c_char_p, vp, C.POINTER(HybridFlowOptions), C.c_int, vp, vp]
         if hasattr(L, "nds_hybrid_flow_fields"):
@@ -294,13 +295,17 @@ def hybrid_amg_vcycle(path, rau: np.ndarray, b: np.ndarray, options: HybridFlowO
 
 
 class HybridAmg:
-    """Host setup of the mixed-mesh pressure preconditioner for a given rAU."""
+    """Host setup of the mixed-mesh pressure preconditioner for a given rAU
+    (``rau`` given) or of the whole pipe SIMPLE (``rau`` None)."""
 
-    def __init__(self, path, rau: np.ndarray, options: HybridFlowOptions | None = None, **kw):
+    def __init__(self, path, rau: np.ndarray | None, options: HybridFlowOptions | None = None, **kw):
         o = options if options is not None else HybridFlowOptions.make(**kw)
-        r = np.ascontiguousarray(rau, dtype=np.float64)
         h = C.c_void_p()
-        _check(lib().nds_hybrid_amg_create(str(path).encode(), _p(r), C.byref(o), C.byref(h)))
+        if rau is None:
+            _check(lib().nds_hybrid_flow_setup(str(path).encode(), C.byref(o), C.byref(h)))
+        else:
+            r = np.ascontiguousarray(rau, dtype=np.float64)
+            _check(lib().nds_hybrid_amg_create(str(path).encode(), _p(r), C.byref(o), C.byref(h)))
         self._h = h
 
     def array(self, name: str) -> np.ndarray:

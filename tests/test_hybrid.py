@@ -270,3 +270,36 @@ def test_divergence_audit_matches_reference_hxt3a_gate(native):
     for i, key in enumerate(("crossCoeffNormMin", "crossCoeffNormMax", "directSchurAbsMin", "directSchurAbsMax")):
         assert _close(out[10 + i], s[key], 1e-11), (key, out[10 + i], s[key])
     assert int(out[14]) == int(s["trianglePairs"]) and int(out[15]) == 0
+
+
+def _oracle_history(native, n, **opts):
+    from oracle.hybrid_flow import HybridFlowOracle
+    return HybridFlowOracle(native, MESH, **opts).run(n)
+
+
+def test_flow_oracle_matches_reference_tight(native):
+    """The CPU restatement of the mixed-mesh pipe SIMPLE (oracle/hybrid_flow.py)
+    on the product's host setup follows the reference's tight run: relCont
+    and absCont of the first five iterations to 1e-11, the same pressure
+    iteration counts."""
+    hist = _oracle_history(native, 5, p_rtol=1e-10, p_max=2000)
+    _, ws, _ = _parse_4b((GOLDEN / "hxt4b_hybrid_r2_tight.log").read_text())
+    for it in range(1, 6):
+        rel, cn, its = hist[it - 1]
+        assert _close(rel, ws[it]["relCont"], 1e-11), (it, rel, ws[it]["relCont"])
+        assert _close(cn, ws[it]["absCont"], 1e-11), (it, cn, ws[it]["absCont"])
+        assert its == int(ws[it]["pCG"]), (it, its, ws[it]["pCG"])
+
+
+@pytest.mark.gpu
+def test_pipe_simple_device_matches_oracle(native, tmp_path):
+    """The device run against the oracle on the same host setup: the first
+    five iterations' relCont and absCont to 3e-9, pressure iterations within
+    one (tight pressure solves)."""
+    _, gs, _ = _run_4b(tmp_path / "r2.vtu", "--p-rtol", "1e-10", "--p-max", "2000")
+    hist = _oracle_history(native, 5, p_rtol=1e-10, p_max=2000)
+    for it in range(1, 6):
+        rel, cn, its = hist[it - 1]
+        assert _close(gs[it]["relCont"], rel, 3e-9), (it, gs[it]["relCont"], rel)
+        assert _close(gs[it]["absCont"], cn, 3e-9), (it, gs[it]["absCont"], cn)
+        assert abs(int(gs[it]["pCG"]) - its) <= 1, (it, gs[it]["pCG"], its)
