@@ -303,3 +303,28 @@ def test_pipe_simple_device_matches_oracle(native, tmp_path):
         assert _close(gs[it]["relCont"], rel, 3e-9), (it, gs[it]["relCont"], rel)
         assert _close(gs[it]["absCont"], cn, 3e-9), (it, gs[it]["absCont"], cn)
         assert abs(int(gs[it]["pCG"]) - its) <= 1, (it, gs[it]["pCG"], its)
+
+
+def test_flow_setup_properties(native):
+    """Host setup of the pipe SIMPLE: no two rows of a colour are coupled (so a
+    colour's rows update independently), fixed rows are in no colour, every
+    local convection value is gathered into exactly one entry, and each
+    diagonal position points at the row's own column."""
+    import numpy as np
+    h = native.HybridAmg(MESH, None)
+    row, col, dpos = h.array("flow.row"), h.array("flow.col"), h.array("flow.diagPos")
+    n = len(row) - 1
+    assert np.array_equal(col[dpos], np.arange(n))
+    off, rows = h.array("flow.colourOff"), h.array("flow.colourRows")
+    fixed = h.array("flow.fixed").astype(bool)
+    colour = np.full(n, -1)
+    for c in range(len(off) - 1):
+        colour[rows[off[c]:off[c + 1]]] = c
+    assert np.all((colour >= 0) == ~fixed)
+    r_of = np.repeat(np.arange(n), np.diff(row))
+    coupled = (r_of != col) & (colour[r_of] >= 0) & (colour[r_of] == colour[col])
+    assert not coupled.any()
+    src, soff = h.array("flow.src"), h.array("flow.srcOff")
+    sc = h.array("flow.scalars")
+    assert np.array_equal(np.sort(src), np.arange(int(sc[5]) * 196 + int(sc[6]) * 64))
+    assert soff[-1] == len(src) and len(soff) == len(col) + 1
