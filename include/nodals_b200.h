@@ -201,21 +201,27 @@ int nds_profile_read(nds_solver* s, nds_profile_entry* out, int max_entries, int
 unsigned long long nds_launch_count(void);
 
 /* ---- allocation-free continuity residual (no counterpart in the
- *      reference, which computes this only inside its SIMPLE loop,
- *      h8_precomputed_b.cuh:140-163).
- * For callers that must not allocate device memory.  u0..u2 (nv doubles
- * each), r (nc doubles) and norm (1 double) are caller-owned DEVICE
- * pointers on the solver's device; stream is a cudaStream_t (NULL: the
- * legacy default stream).  Enqueues r = -(B u + fixedDiv) and
- * *norm = ||B u + fixedDiv||_2, the quantity nds_simple_step reports as
- * cont_norm, and returns without synchronising.  Needs a solver whose state
- * is FP64 (precision fp64 or amg_fp32).  Makes no cudaMalloc/cudaFree or
- * other allocating call: the partial sums live in a 16 KiB device array of
- * the library (at most 1184 blocks).  The first call on a device resolves
- * that array's address (cudaGetSymbolAddress), so make it before any stream
- * capture.  Calls that overlap in time on one device race on the array, and
- * so do calls overlapping an nds_simple_step of the same solver.  Failures
- * return a status only: nds_last_error() is not updated. */
+ *      reference).
+ * For callers that must not allocate device memory: code that runs between
+ * the steps of its own captured or real-time loop, or under an allocator
+ * that forbids cudaMalloc once it has started.  u0..u2 (nv doubles each),
+ * r (nc doubles) and norm (1 double) are caller-owned DEVICE pointers on the
+ * solver's device; stream is a cudaStream_t (NULL: the legacy default
+ * stream).  Enqueues r = -(B u + fixedDiv) and *norm = ||B u + fixedDiv||_2,
+ * the quantity nds_simple_step reports as cont_norm, and returns without
+ * synchronising.  Needs a solver whose state is FP64 (precision fp64,
+ * amg_fp32 or mixed); any mesh size and any device ordinal the solver runs
+ * on.  Makes no cudaMalloc/cudaFree or other allocating call: the block
+ * partial sums live in a 16 KiB device array of the library (at most 1184
+ * blocks, whatever the mesh size), held on every device that loads the
+ * library until the process exits.  Each call looks that array's address up
+ * (cudaGetSymbolAddress, which allocates nothing) with the solver's device
+ * current.  Calls that overlap in time on one device race on the array, and
+ * so do calls overlapping an nds_simple_step of the same solver.  Launches
+ * are checked with cudaPeekAtLastError, so an error still pending from the
+ * caller's own earlier CUDA work is reported as NDS_E_CUDA too (and left
+ * pending).  Failures return a status only: nds_last_error() is not
+ * updated. */
 int nds_continuity_noalloc(nds_solver* s, const double* u0, const double* u1, const double* u2, double* r,
                            double* norm, void* stream);
 

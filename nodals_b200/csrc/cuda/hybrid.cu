@@ -337,9 +337,16 @@ __global__ void cg_jacobi(int n, const double* __restrict__ inv, const double* _
   if (i < n) z[i] = i == pin ? 0.0 : inv[i] * r[i];
 }
 
+// The captured loop body bakes in x, the pin, the operator's buffers and the
+// preconditioner's buffers (its closure).  It is rebuilt when x, the pin or
+// the operator object changes; the preconditioner is not compared, so every
+// CgWork serves one (operator, preconditioner) pair for its whole life (each
+// solve site of this file owns its own CgWork).
 struct CgLoop {
   cudaGraphExec_t exec = nullptr;
-  const void* bound = nullptr;  // x of the captured body
+  const void* bound = nullptr;     // x of the captured body
+  const void* bound_op = nullptr;  // operator object of the captured body
+  int bound_pin = -2;
   unsigned long long body_kernels = 0;
   bool failed = false;
   CgLoop() = default;
@@ -400,7 +407,7 @@ bool cg_device(Op& A, Pre&& pre, const double* rhs, double* x, double rtol, doub
     R.ok = true;
     return true;
   }
-  if (L.exec && L.bound != x) {
+  if (L.exec && (L.bound != x || L.bound_op != (const void*)&A || L.bound_pin != pin)) {
     cudaGraphExecDestroy(L.exec);
     L.exec = nullptr;
   }
@@ -455,6 +462,8 @@ bool cg_device(Op& A, Pre&& pre, const double* rhs, double* x, double rtol, doub
       return false;
     }
     L.bound = x;
+    L.bound_op = (const void*)&A;
+    L.bound_pin = pin;
   }
   W.hsc[CG_TARGET] = std::max(atol, rtol * r0);
   const int init[5] = {0, 0, 1, maxit, 0};

@@ -1756,14 +1756,16 @@ unsigned long long nds_launch_count(void) { return nds::g_launches; }
 // nothing has to start at zero.  The array is shared by all calls on a
 // device: calls that overlap in time (two host threads, or two streams
 // without ordering between them) race on it.
+//
+// The array's device address is looked up (cudaGetSymbolAddress) on every
+// call with the solver's device current: the lookup allocates nothing, and
+// an address kept from an earlier call could be stale once the caller has
+// torn the context down (cudaDeviceReset) and the module was loaded again.
 // ---------------------------------------------------------------------------
 namespace {
 constexpr int kNoAllocBlocks = 1184;
 constexpr int kNoAllocScratch = 2048;  // doubles; >= kNoAllocBlocks
-constexpr int kNoAllocMaxDevices = 64;
 static_assert(kNoAllocScratch >= kNoAllocBlocks, "scratch too small for the block cap");
-std::mutex g_noalloc_mu;
-double* g_noalloc_addr[kNoAllocMaxDevices] = {};
 
 __global__ void sqrt_in_place(double* x) { *x = sqrt(*x); }
 }  // namespace
@@ -1779,7 +1781,7 @@ int nds_continuity_noalloc(nds_solver* s, const double* u0, const double* u1, co
   const double *bco = nullptr, *fdiv = nullptr;
   int nc = 0, dev = 0;
   if (!s->impl->cell_arrays(&ref, &bco, &fdiv, &nc, &dev)) return NDS_E_INVALID;
-  if (nc < 1 || dev < 0 || dev >= kNoAllocMaxDevices) return NDS_E_INVALID;
+  if (nc < 1 || dev < 0) return NDS_E_INVALID;
   const int grid = std::min(nds::grid_for(nc), kNoAllocBlocks);
   if (grid > kNoAllocScratch) return NDS_E_INVALID;
   int prev = -1;
@@ -1788,21 +1790,27 @@ int nds_continuity_noalloc(nds_solver* s, const double* u0, const double* u1, co
   int st = NDS_OK;
   double* part = nullptr;
   {
-    std::lock_guard<std::mutex> lk(g_noalloc_mu);
-    if (!g_noalloc_addr[dev]) {
-      void* a = nullptr;
-      if (cudaGetSymbolAddress(&a, g_noalloc_part) == cudaSuccess) g_noalloc_addr[dev] = static_cast<double*>(a);
-      else st = NDS_E_CUDA;
-    }
-    part = g_noalloc_addr[dev];
+    void* a = nullptr;
+    if (cudaGetSymbolAddress(&a, g_noalloc_part) == cudaSuccess) part = static_cast<double*>(a);
+    else st = NDS_E_CUDA;
+  }
+  // every launch is checked with cudaPeekAtLastError, which leaves an error
+  // pending from the caller's own earlier work in place for the caller
+  cudaStream_t cs = static_cast<cudaStream_t>(stream);
+  if (st == NDS_OK) {
+    nds::k::continuity<double, 1><<<grid, nds::kBlock, 0, cs>>>(nc, ref, bco, fdiv, u0, u1, u2, r, part);
+    ++nds::g_launches;
+    if (cudaPeekAtLastError() != cudaSuccess) st = NDS_E_CUDA;
   }
   if (st == NDS_OK) {
-    cudaStream_t cs = static_cast<cudaStream_t>(stream);
-    nds::k::continuity<double, 1><<<grid, nds::kBlock, 0, cs>>>(nc, ref, bco, fdiv, u0, u1, u2, r, part);
     nds::k::reduce_partials<1><<<1, nds::kBlock, 0, cs>>>(part, grid, norm);
+    ++nds::g_launches;
+    if (cudaPeekAtLastError() != cudaSuccess) st = NDS_E_CUDA;
+  }
+  if (st == NDS_OK) {
     sqrt_in_place<<<1, 1, 0, cs>>>(norm);
-    nds::g_launches += 3;
-    if (cudaGetLastError() != cudaSuccess) st = NDS_E_CUDA;
+    ++nds::g_launches;
+    if (cudaPeekAtLastError() != cudaSuccess) st = NDS_E_CUDA;
   }
   if (prev != dev) cudaSetDevice(prev);
   return st;

@@ -445,22 +445,3 @@ def hp_errors(problem: Problem, u0, u1, u2, p) -> dict:
 def write_vtu(problem: Problem, path, u0, u1, u2, p, converged: bool = False, outer_its: int = 0):
     a = [_f64(x) for x in (u0, u1, u2, p)]
     _check(lib().nds_write_vtu(problem._h, str(path).encode(), *[_p(x) for x in a], int(converged), int(outer_its)))
-
-
-def read_dump(path) -> dict:
-    """Reader of the flat record files written by oracle/ref_setup_dump."""
-    dt = {"f64": np.float64, "i32": np.int32, "i64": np.int64, "u8": np.uint8, "u32": np.uint32}
-    out = {}
-    with open(path, "rb") as f:
-        if f.read(8) != b"NDSDUMP1":
-            raise ValueError("not an NDSDUMP1 file")
-        while True:
-            nm = f.read(48)
-            if len(nm) < 48:
-                break
-            name = nm.split(b"\0", 1)[0].decode()
-            d = f.read(8).split(b"\0", 1)[0].decode()
-            n = int(np.frombuffer(f.read(8), dtype=np.int64)[0])
-            t = np.dtype(dt[d])
-            out[name] = np.frombuffer(f.read(n * t.itemsize), dtype=t).copy()
-    return out

@@ -11,7 +11,10 @@ ROOT = Path(__file__).resolve().parents[1]
 if str(ROOT) not in sys.path:
     sys.path.insert(0, str(ROOT))
 GOLDEN = ROOT / "tests" / "golden"
-REFERENCE = Path("/root/reference")
+from oracle.refpath import reference_root  # noqa: E402
+
+# the reference checkout (None when absent: the steps that read it skip)
+REFERENCE = reference_root()
 
 
 def pytest_configure(config):

@@ -12,6 +12,14 @@ into the git-ignored ``oracle/_ref/``:
   cases in ``CASES``; the NODALS_GPU_H8_SIMPLE history and the VTU fields
   (P0 pressure, cell-average velocity, 17 digits) are stored as
   ``run_<case>.npz``.
+* ``--configs`` (needs a GPU): the reference H8 FP64 binary on the two
+  benchmark configurations, ``CONFIG_CASES``: the ~40k-tet pipe at Re 20 for
+  300 outer iterations and the ~1M-tet pipe at Re 100 to steady state.  Stored
+  as ``cfg_<case>.npz``: the printed history (every iteration up to 10, then
+  every 25th, audits and the converged one), the FULLCONV summary line, and
+  the VTU fields -- all of them for the 40k mesh; for the 1M mesh (whose
+  fields would be ~40 MB) every ``FIELD_STRIDE``-th cell plus the L2 norm and
+  sum of each full field.
 
 Meshes are regenerated from ``nodals_b200.meshgen`` (deterministic, seeded),
 so the fixtures only hold reference outputs, never mesh files.
@@ -35,7 +43,7 @@ ROOT = Path(__file__).resolve().parents[2]
 sys.path.insert(0, str(ROOT))
 
 from nodals_b200 import meshgen  # noqa: E402
-from nodals_b200.native import read_dump  # noqa: E402
+from oracle.dump import read_dump  # noqa: E402
 
 REF = ROOT / "oracle" / "_ref"
 
@@ -91,6 +99,23 @@ CASES = {
     "small_supg_converge": ("pipe_small", "fp64", ["--run-mode", "converge", "--max-outer", "400", "--simple-tol", "1e-3"],
                             _CFG1 + _SA + ["--amg-terminal", "100", "--supg", "1"]),
 }
+
+# Benchmark configurations: 300 outer iterations of the ~40k pipe at Re 20
+# (converge mode with a tolerance it does not reach, so the run is exactly 300
+# iterations; fixed10 only allows 10), and the ~1M pipe at Re 100 to steady
+# state (relCont and the momentum audit <= 1e-6).
+_SA_RUN = ["--amg-hierarchy", "sa", "--amg-smoother", "cheb2", "--pressure-solver", "pcg"]
+CONFIG_CASES = {
+    "pipe40k_re20_300": ("pipe40k", ["--run-mode", "converge", "--max-outer", "300", "--simple-tol", "1e-12"],
+                         ["--re", "20", "--alpha-u", "0.7", "--alpha-p", "0.3", "--p-rtol", "1e-6",
+                          "--p-max", "400"] + _SA_RUN),
+    "pipe1m_re100_steady": ("pipe1m", ["--run-mode", "converge", "--max-outer", "6000", "--simple-tol", "1e-6"],
+                            ["--re", "100", "--alpha-u", "0.7", "--alpha-p", "0.3", "--p-rtol", "1e-6",
+                             "--p-max", "400"] + _SA_RUN),
+}
+FIELD_STRIDE = 61  # cells kept from fields of meshes above 100k cells
+_FULLCONV = re.compile(r"NODALS_GPU_H8_FULLCONV .*?outerIts=(\d+) converged=(\d+) finalRelCont=(\S+) "
+                       r".*?avgPressureIts=(\S+) pressureDropFit=(\S+)")
 
 _SIMPLE = re.compile(r"NODALS_GPU_H8_SIMPLE .*?it=(\d+) relCont=(\S+) .*?pCG=(\d+) pTrueRel=(\S+)")
 # the SUPG entry writes no VTU; its field check is the analytic-error line
@@ -183,6 +208,44 @@ def make_runs(out: Path, only=None):
             print("wrote", case, "rc", r.returncode, "its", len(its))
 
 
+def make_configs(out: Path, only=None):
+    with tempfile.TemporaryDirectory() as td:
+        td = Path(td)
+        for case, (mesh, mode, flags) in CONFIG_CASES.items():
+            if only and case not in only:
+                continue
+            pm = write_mesh(mesh, td)
+            vtu = td / f"{case}.vtu"
+            cmd = [str(REF / "nodals_gpu_h8_fp64"), "--mesh", str(pm), "--tag", case, "--vtu-out", str(vtu),
+                   *mode, *flags]
+            r = subprocess.run(cmd, capture_output=True, text=True, timeout=1800)
+            if r.returncode not in (0, 35):
+                print("FAILED", case, r.returncode, r.stderr[-2000:])
+                continue
+            its, rel, pcg, prel, audit = parse_log(r.stdout)
+            p, uc = parse_vtu(vtu)
+            keep = {}
+            if len(p) > 100_000:
+                idx = np.arange(0, len(p), FIELD_STRIDE)
+                keep.update(p_sample=p[idx], u_cell_sample=uc[idx], field_stride=np.array([FIELD_STRIDE]))
+            else:
+                keep.update(p=p, u_cell=uc)
+            keep.update(p_norm=np.array([np.linalg.norm(p)]), p_sum=np.array([p.sum()]),
+                        u_cell_norm=np.linalg.norm(uc, axis=0), u_cell_sum=uc.sum(axis=0),
+                        n_cells=np.array([len(p)]))
+            m = _FULLCONV.search(r.stdout)
+            if m:
+                keep["fullconv"] = np.array([float(v) for v in m.groups()])
+            m = _HP.search(r.stdout)
+            if m:
+                keep["hp"] = np.array([float(v) for v in m.groups()])
+            lines = [l for l in r.stdout.splitlines() if l.startswith(("NODALS_GPU_H8_FULLCONV", "NODALS_GPU_RESULT"))]
+            np.savez_compressed(out / f"cfg_{case}.npz", it=its, rel_cont=rel, p_its=pcg, p_rel=prel, audit=audit,
+                                rc=np.array([r.returncode]), cmd=np.array(" ".join(cmd[3:])),
+                                summary=np.array("\n".join(lines)), **keep)
+            print("wrote", case, "rc", r.returncode, "printed its", len(its), flush=True)
+
+
 def add_hp(out: Path, logdirs):
     """Add the analytic-error line (hp) to existing run fixtures from the
     logs of the reference runs that produced them (run_<case>.log)."""
@@ -206,6 +269,7 @@ if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--setup", action="store_true")
     ap.add_argument("--runs", action="store_true")
+    ap.add_argument("--configs", action="store_true")
     ap.add_argument("--only", nargs="*")
     ap.add_argument("--add-hp", nargs="*", metavar="LOGDIR", help="add hp to existing fixtures from reference logs")
     ap.add_argument("--out", default=str(Path(__file__).resolve().parent))
@@ -216,5 +280,7 @@ if __name__ == "__main__":
         make_setup(out)
     if ns.runs:
         make_runs(out, ns.only)
+    if ns.configs:
+        make_configs(out, ns.only)
     if ns.add_hp:
         add_hp(out, ns.add_hp)

@@ -6,8 +6,8 @@ converts it with the reference's ``turbulence/sst_gpu_v2/tools/msh2_to_hxt1.py``
 ``HXT1_mesh.bin`` as ``tests/golden/hxt1_pipe_tiny.bin``; writes the small
 mixed hex/tet pipe ``HYBRID`` as HXT0 arrays and keeps the reference
 preparer's ``HXT1_mesh.bin`` of it as ``tests/golden/hxt1_hybrid_r2.bin``.  Needs the
-reference tree (first argument, default /root/reference); the tests only read
-the committed file.
+reference tree (first argument, default: oracle.refpath.reference_root()); the
+tests only read the committed file.
 """
 from __future__ import annotations
 
@@ -22,6 +22,7 @@ ROOT = HERE.parents[1]
 sys.path.insert(0, str(ROOT))
 
 from nodals_b200 import meshgen  # noqa: E402
+from oracle.refpath import reference_root  # noqa: E402
 
 
 # the small mixed pipe: 2 hex rings, 8 sectors, 20 slabs, R = 0.5, L = 10 (10 D)
@@ -29,7 +30,9 @@ HYBRID = dict(nr=2, ntheta=8, nz=20, radius=0.5, length=10.0)
 
 
 def main() -> None:
-    ref = Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference")
+    ref = Path(sys.argv[1]) if len(sys.argv) > 1 else reference_root()
+    if ref is None:
+        raise SystemExit("reference tree not found: pass its path or set NODALS_REFERENCE")
     conv = ref / "turbulence" / "sst_gpu_v2" / "tools" / "msh2_to_hxt1.py"
     with tempfile.TemporaryDirectory() as tmp:
         msh = meshgen.write_msh2(meshgen.named("pipe_tiny"), Path(tmp) / "pipe_tiny.msh")

@@ -27,7 +27,7 @@ HERE = Path(__file__).resolve().parent
 ROOT = HERE.parents[1]
 sys.path.insert(0, str(ROOT))
 
-from nodals_b200.native import read_dump  # noqa: E402
+from oracle.dump import read_dump  # noqa: E402
 
 MESH = HERE / "hxt1_hybrid_r2.bin"
 # case -> harness flags (the product's options of the same meaning are set by the test)

@@ -5,8 +5,11 @@ Checked against nds_simple_step on the same velocity: the norm must equal the
 step's reported cont_norm bit for bit (same kernel, same fixed-order
 reduction); r against a numpy evaluation of -(B u + fixedDiv) to 1e-12
 relative.  Each input is evaluated by two calls in a row, so a scratch value
-left over from the first call would show up in the second.  Collected last
-(file name) and also run on its own.
+left over from the first call would show up in the second.  The device's free
+memory (cudaMemGetInfo) and torch's allocator counters must not move across
+the calls.  pipe400k has more cells than 1184 blocks x 256 threads, so the
+grid-stride loop and every slot of the scratch array are used.  Collected
+last (file name) and also run on its own.
 """
 from __future__ import annotations
 
@@ -38,10 +41,14 @@ def _numpy_residual(P, u):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("precision", ["fp64", "amg_fp32"])
-def test_noalloc_continuity_matches_step(native, meshes, precision):
+@pytest.mark.parametrize("precision,mesh", [("fp64", "pipe_small"), ("amg_fp32", "pipe_small"),
+                                            ("fp64", "pipe400k")])
+def test_noalloc_continuity_matches_step(native, meshes, precision, mesh):
     import torch
-    P = native.Problem(native.Mesh.from_tetmesh(meshes("pipe_small")), precision=precision, **CFG)
+    kw = dict(CFG, amg_terminal=300) if mesh == "pipe400k" else CFG
+    P = native.Problem(native.Mesh.from_tetmesh(meshes(mesh)), precision=precision, **kw)
+    if mesh == "pipe400k":
+        assert P.counts()["nc"] > 1184 * 256
     S = native.Solver(P)
     f = _fn(native)
     for _ in range(2):
@@ -49,9 +56,14 @@ def test_noalloc_continuity_matches_step(native, meshes, precision):
         u0, u1, u2, p = S.fields()
         du = [torch.from_numpy(x).cuda() for x in (u0, u1, u2)]
         want_r = _numpy_residual(P, (u0, u1, u2))
+        r = torch.full((len(p),), float("nan"), dtype=torch.float64, device="cuda")
+        nrm = torch.full((1,), float("nan"), dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        free0 = torch.cuda.mem_get_info()[0]
+        stats0 = torch.cuda.memory_stats()
         for _call in range(2):
-            r = torch.full((len(p),), float("nan"), dtype=torch.float64, device="cuda")
-            nrm = torch.full((1,), float("nan"), dtype=torch.float64, device="cuda")
+            r.fill_(float("nan"))
+            nrm.fill_(float("nan"))
             l0 = native.launch_count()
             st = f(S._h, *[C.c_void_p(x.data_ptr()) for x in du], C.c_void_p(r.data_ptr()),
                    C.c_void_p(nrm.data_ptr()), None)
@@ -61,6 +73,12 @@ def test_noalloc_continuity_matches_step(native, meshes, precision):
             assert nrm.item() == rep.cont_norm
             got = r.cpu().numpy()
             assert np.linalg.norm(got - want_r) <= 1e-12 * np.linalg.norm(want_r)
+        # nothing was allocated on the device by the two calls (the checks in
+        # between only fill existing tensors and copy to the host)
+        assert torch.cuda.mem_get_info()[0] == free0
+        stats1 = torch.cuda.memory_stats()
+        for key in ("allocation.all.allocated", "segment.all.allocated"):
+            assert stats1.get(key, 0) == stats0.get(key, 0), key
 
 
 @pytest.mark.gpu
