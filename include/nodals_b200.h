@@ -43,8 +43,16 @@ typedef struct nds_solver nds_solver;
  * 0 / 1, gpu/serial_cuda/h8_main.cu).  NDS_AMG_FP32 has no reference build:
  * state, momentum, continuity and the Krylov method (including its A*p) stay
  * FP64 while the AMG V-cycle -- levels, transfers, smoothers and an FP32 copy
- * of the fine Schur operator written by the same refresh -- runs in FP32. */
-enum nds_precision { NDS_FP64 = 0, NDS_FP32 = 1, NDS_AMG_FP32 = 2 };
+ * of the fine Schur operator written by the same refresh -- runs in FP32.
+ * NDS_MIXED has no reference build either: state, momentum, continuity and
+ * the outer residual of an FP64 defect-correction loop around each pressure
+ * solve stay FP64; each inner solve (PCG or FGMRES, options p_krylov ...)
+ * runs in FP32 on the FP32 operator copy with the FP32 V-cycle, with FP64
+ * reductions, FGMRES Gram-Schmidt and Hessenberg least squares.  The
+ * pressure solve meets the same FP64 target max(p_atol, p_rtol ||b||). */
+enum nds_precision { NDS_FP64 = 0, NDS_FP32 = 1, NDS_AMG_FP32 = 2, NDS_MIXED = 3 };
+/* inner Krylov method of NDS_MIXED */
+enum nds_krylov { NDS_KRYLOV_PCG = 0, NDS_KRYLOV_FGMRES = 1 };
 enum nds_run_mode { NDS_RUN_FIXED10 = 0, NDS_RUN_CONVERGE = 1 };
 enum nds_momentum_work { NDS_MOM_FGS1 = 0, NDS_MOM_ALTGS1 = 1, NDS_MOM_SGS1 = 2 };
 enum nds_pressure_solver { NDS_P_PCG = 0, NDS_P_RICHARDSON = 1, NDS_P_CHEB = 2 };
@@ -86,6 +94,17 @@ typedef struct nds_options {
    * the 64-point collapsed rule (h8_supg_main_cli.inc, h7_momentum_assembly.cuh:100-226) */
   int supg;
   double supg_tau_scale, supg_magic;
+  /* pressure solve of NDS_MIXED (no reference counterpart; ignored by the
+   * other precisions).  p_max caps the inner iterations of one solve. */
+  int p_krylov;          /* enum nds_krylov (default PCG) */
+  int p_restart;         /* FGMRES basis vectors per pass, 1..64 (default 30) */
+  double p_inner_rtol;   /* relative target of one FP32 inner pass (default 1e-3) */
+  int p_refine_max;      /* FP64 defect-correction passes per solve (default 8) */
+  int p_guess;           /* earlier corrections spanning a Galerkin initial guess, 0..4 (0: zero guess) */
+  int learned;           /* 1: learned stage ahead of the V-cycle (FGMRES only; nds_solver_load_stage) */
+  /* 1: pipe centre and radius from the inlet patch instead of the bounding
+   * box (bent pipes); 0: the reference's bounding-box rule (g4_host.hpp:37-49) */
+  int geom_from_inlet;
 } nds_options;
 
 /* One SIMPLE outer iteration (h8_main_base.cu:2046-2119). */

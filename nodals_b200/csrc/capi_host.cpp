@@ -104,6 +104,13 @@ void nds_options_default(nds_options* o) {
   o->supg = 0;
   o->supg_tau_scale = 0.05;
   o->supg_magic = 9.0;
+  o->p_krylov = NDS_KRYLOV_PCG;
+  o->p_restart = 30;
+  o->p_inner_rtol = 1e-3;
+  o->p_refine_max = 8;
+  o->p_guess = 0;
+  o->learned = 0;
+  o->geom_from_inlet = 0;
 }
 
 int nds_mesh_read_polymesh(const char* dir, nds_mesh** out) {
@@ -609,6 +616,7 @@ int nds_problem_create(const nds_mesh* mm, const nds_options* o, nds_problem** o
     so.supg = o->supg != 0;
     so.supg_tau_scale = o->supg_tau_scale;
     so.supg_magic = o->supg_magic;
+    so.geom_from_inlet = o->geom_from_inlet != 0;
     P->setup = nds::build_setup(P->mesh, so);
     P->power_its = nds::effective_amg_power_its(*o);
     nds::AmgOptions ao;
@@ -748,7 +756,18 @@ bool validate_options(const nds_options& o, std::string& why) {
   if (o.run_mode != NDS_RUN_FIXED10 && o.run_mode != NDS_RUN_CONVERGE) return bad("H8 run-mode must be fixed10 or converge");
   if (o.run_mode == NDS_RUN_FIXED10 && o.max_outer != 10) return bad("H8 fixed10 requires maxOuter=10");
   if (o.amg_smoother == NDS_SM_CHEB2 && effective_amg_power_its(o) <= 0) return bad("H8 Chebyshev AMG smoother requires spectrum estimation");
-  if (o.precision < 0 || o.precision > 2) return bad("precision must be fp64, fp32 or amg_fp32");
+  if (o.precision < 0 || o.precision > 3) return bad("precision must be fp64, fp32, amg_fp32 or mixed");
+  if (o.p_krylov < 0 || o.p_krylov > 1) return bad("p_krylov must be pcg or fgmres");
+  if (o.p_restart < 1 || o.p_restart > 64) return bad("p_restart must be in 1..64");
+  if (!(o.p_inner_rtol > 0.0 && o.p_inner_rtol < 1.0)) return bad("p_inner_rtol must be in (0, 1)");
+  if (o.p_refine_max < 1) return bad("p_refine_max must be >= 1");
+  if (o.p_guess < 0 || o.p_guess > 4) return bad("p_guess must be in 0..4");
+  if (o.learned && (o.precision != NDS_MIXED || o.p_krylov != NDS_KRYLOV_FGMRES))
+    return bad("the learned stage needs precision mixed and p_krylov fgmres (a varying preconditioner)");
+  if (o.precision == NDS_MIXED && o.pressure_solver != NDS_P_PCG)
+    return bad("precision mixed runs its own Krylov solve: pressure_solver must be pcg (the default)");
+  if (o.precision == NDS_MIXED && o.amg_smoother == NDS_SM_MCGS)
+    return bad("precision mixed supports the polynomial smoothers (cheb2, jacobi, l1jacobi)");
   if (o.supg != 0 && o.supg != 1) return bad("H8 supg must be 0 or 1");
   if (o.supg) {  // h8_supg_main_cli.inc:92-124
     if (!(o.supg_tau_scale > 0.0)) return bad("H8 SUPG tau scale must be positive");

@@ -663,9 +663,12 @@ __global__ void p_update_dev(int n, const double* __restrict__ beta_dev, const i
 // the host loop does (sqrt, then compare); stop on convergence, on any flag
 // or at max_its.  The loop always ends: every body pass runs this kernel and
 // the count reaches max_its.
+// max_its < 0: the cap is ctl[3] (set per solve by the host).  in_graph = 0:
+// launched outside a graph (host-driven loop), no condition to set.
 __global__ void pcg_check(const double* __restrict__ sc, int rn2_slot, int r0_slot, int target_slot,
                           int* __restrict__ flags, int* __restrict__ ctl, int max_its,
-                          cudaGraphConditionalHandle loop) {
+                          cudaGraphConditionalHandle loop, int in_graph = 1) {
+  if (max_its < 0) max_its = ctl[3];
   const int it = ++ctl[0];
   ctl[2] = 0;
   const double rn = sqrt(sc[rn2_slot]);
@@ -673,7 +676,7 @@ __global__ void pcg_check(const double* __restrict__ sc, int rn2_slot, int r0_sl
   const int conv = rn <= sc[target_slot];
   ctl[1] = conv;
   const bool stop = conv || *flags != 0 || it >= max_its;
-  cudaGraphSetConditional(loop, stop ? 0u : 1u);
+  if (in_graph) cudaGraphSetConditional(loop, stop ? 0u : 1u);
 }
 
 // ---------------------------------------------------------------------------

@@ -26,6 +26,7 @@
 #include "../host/fem.hpp"
 #include "common.cuh"
 #include "kernels.cuh"
+#include "krylov.cuh"
 
 namespace nds {
 
@@ -579,6 +580,10 @@ class Solver final : public ISolver {
     NDS_CUDA(cudaMallocHost((void**)&hflags_, sizeof(int) * 8));
     NDS_CUDA(cudaMemsetAsync(flags_.p, 0, sizeof(int), st_));
 
+    if constexpr (!kSame) {
+      mixed_ = o_.precision == NDS_MIXED;
+      if (mixed_) alloc_mixed();
+    }
     // setup-time state: fine CSR refreshed with the initial rAU
     tm.mark("levels_and_transfers");
     refresh_fine(rau_.p);
@@ -597,10 +602,12 @@ class Solver final : public ISolver {
 
   // ------------------------------------------------------------------ helpers
   static constexpr int kMaxPartBlocks = 1184;  // 8 x 148 SMs
-  static constexpr int kScalars = 32;
+  static constexpr int kScalars = 64;
   enum { S_RHO = 0, S_PQ = 1, S_ALPHA = 2, S_RN2 = 3, S_RHON = 4, S_BETA = 5, S_R0 = 6, S_TARGET = 7, S_TMP = 8,
-         S_TMP2 = 9, S_CONT2 = 10,
-         S_AUDIT = 16 };
+         S_TMP2 = 9, S_CONT2 = 10, S_WN = 11,
+         S_AUDIT = 16,
+         S_GUESS = 24,  // 14 slots: Galerkin matrix (upper triangle) and right-hand side of the guess
+         S_COEF = 40 };  // 4 slots: guess coefficients
 
   // CUDA graphs of fixed launch sequences (no host decisions inside)
   struct Graph {
@@ -1173,7 +1180,7 @@ class Solver final : public ISolver {
     hsc_[S_R0] = r0;
     hsc_[S_TARGET] = target;
     NDS_CUDA(cudaMemcpyAsync(sc_.p + S_R0, hsc_ + S_R0, 2 * sizeof(double), cudaMemcpyHostToDevice, st_));
-    const int init[4] = {0, 0, 1, 0};
+    const int init[4] = {0, 0, 1, o_.p_max};
     std::memcpy(hflags_ + 4, init, sizeof(init));
     NDS_CUDA(cudaMemcpyAsync(ctl_.p, hflags_ + 4, 4 * sizeof(int), cudaMemcpyHostToDevice, st_));
     NDS_CUDA(cudaMemsetAsync(flags_.p, 0, sizeof(int), st_));
@@ -1275,6 +1282,312 @@ class Solver final : public ISolver {
     return R;
   }
 
+  // ------------------------------------------- mixed-precision pressure solve
+  // (precision NDS_MIXED: Solver<double, float>).  No reference counterpart.
+  // FP64 defect correction around FP32 inner Krylov solves:
+  //   target = max(atol, rtol ||b||); x = Galerkin guess (or 0); r = b - A x
+  //   while ||r|| > target:  solve A d = r / ||r|| in FP32 (PCG or FGMRES,
+  //   FP32 operator copy and V-cycle) to max(inner_rtol, target / (2 ||r||));
+  //   x += ||r|| d;  r = b - A x in FP64 on the FP64 operator.
+  // The stopping rule is the reference's ||r|| <= max(atol, rtol ||r0||)
+  // with r0 = b (its zero initial guess), checked on the FP64 residual.
+  void alloc_mixed() {
+    const size_t n = (size_t)nc_;
+    for (auto* b : {&xf_, &rf_, &zf_, &pf_, &qf_}) b->alloc(n);
+    fg_m_ = o_.p_krylov == NDS_KRYLOV_FGMRES ? o_.p_restart : 0;
+    if (fg_m_ > 0) {
+      fgV_.alloc((size_t)(fg_m_ + 1) * n);
+      fgZ_.alloc((size_t)fg_m_ * n);
+      fg_.alloc((size_t)k::FgLayout{fg_m_}.size());
+      fg_.zero(st_);
+    }
+    fgpart_.alloc((size_t)kMaxPartBlocks * std::max(fg_m_ + 1, 16));
+    if (o_.p_guess > 0) {
+      gY_.alloc((size_t)o_.p_guess * n);
+      gW_.alloc((size_t)o_.p_guess * n);
+    }
+  }
+  // the preconditioner of the inner solves: z = M v (FP32)
+  void precond_f(const float* v, float* z) {
+    if constexpr (!kSame) amg_apply(v, z);
+  }
+  // one pass of the FP32 PCG loop: z = M r; rho; p; q = A p; alpha; x, r; check
+  void pcgf_body(cudaGraphConditionalHandle h) {
+    if constexpr (!kSame) {
+      precond_f(rf_.p, zf_.p);
+      dot_dev(rf_.p, zf_.p, nc_, S_RHON);
+      k::pcg_rho_dev<<<1, 1, 0, st_>>>(sc_.p, flags_.p, ctl_.p);
+      NDS_LAUNCH();
+      k::p_update_dev<float><<<grid_for(nc_), kBlock, 0, st_>>>(nc_, sc_.p + S_BETA, ctl_.p, zf_.p, pf_.p);
+      NDS_LAUNCH();
+      const int g = red_grid(nc_);
+      sell_launch<k::SELL_DOT, float>(fine_opA(), g, pf_.p, nullptr, nullptr, 0.0, qf_.p, nullptr);
+      NDS_LAUNCH();
+      reduce_to<1>(g, S_PQ);
+      k::pcg_alpha<<<1, 1, 0, st_>>>(sc_.p, flags_.p);
+      NDS_LAUNCH();
+      k::xr_update<float><<<g, kBlock, 0, st_>>>(nc_, 0.0, sc_.p + S_ALPHA, pf_.p, qf_.p, xf_.p, rf_.p, part_.p);
+      NDS_LAUNCH();
+      reduce_to<1>(g, S_RN2);
+      k::pcg_check<<<1, 1, 0, st_>>>(sc_.p, S_RN2, S_R0, S_TARGET, flags_.p, ctl_.p, -1, h, in_graph_);
+      NDS_LAUNCH();
+    }
+  }
+  // one Arnoldi step of FGMRES: z_j = M v_j, w = A z_j, classical Gram-Schmidt
+  // with FP64 dot products, Givens update of the least-squares problem
+  void fg_body(cudaGraphConditionalHandle h) {
+    if constexpr (!kSame) {
+      const int g = red_grid(nc_);
+      const k::FgLayout L{fg_m_};
+      k::fg_fetch<<<grid_for(nc_), kBlock, 0, st_>>>(nc_, fgV_.p, ctl_.p, rf_.p);
+      NDS_LAUNCH();
+      precond_f(rf_.p, zf_.p);
+      k::fg_store<<<grid_for(nc_), kBlock, 0, st_>>>(nc_, zf_.p, ctl_.p, fgZ_.p);
+      NDS_LAUNCH();
+      op_spmv(fine_opA(), (const float*)zf_.p, qf_.p);
+      k::fg_dots<<<dim3(g, fg_m_ + 1), kBlock, 0, st_>>>(nc_, fgV_.p, qf_.p, ctl_.p, fgpart_.p);
+      NDS_LAUNCH();
+      k::fg_reduce_h<<<fg_m_ + 1, kBlock, 0, st_>>>(fgpart_.p, g, ctl_.p, L, fg_.p);
+      NDS_LAUNCH();
+      k::fg_orth<<<g, kBlock, 0, st_>>>(nc_, fgV_.p, fg_.p, L, ctl_.p, qf_.p, part_.p);
+      NDS_LAUNCH();
+      reduce_to<1>(g, S_RN2);
+      k::fg_givens<<<1, 1, 0, st_>>>(fg_.p, L, sc_.p, S_RN2, S_WN, S_TARGET, ctl_.p, flags_.p, h, in_graph_);
+      NDS_LAUNCH();
+      k::fg_normalize<<<grid_for(nc_), kBlock, 0, st_>>>(nc_, qf_.p, sc_.p, S_WN, ctl_.p, fgV_.p);
+      NDS_LAUNCH();
+    }
+  }
+  template <class Body>
+  bool build_loop(LoopGraph& G, Body&& body) {
+    const bool was = prof.on;
+    prof.on = false;
+    cudaGraph_t graph = nullptr;
+    bool ok = cudaGraphCreate(&graph, 0) == cudaSuccess;
+    cudaGraphConditionalHandle h{};
+    cudaGraphNodeParams cp{};
+    cudaGraphNode_t node{};
+    if (ok) ok = cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault) == cudaSuccess;
+    if (ok) {
+      cp.type = cudaGraphNodeTypeConditional;
+      cp.conditional.handle = h;
+      cp.conditional.type = cudaGraphCondTypeWhile;
+      cp.conditional.size = 1;
+      ok = cudaGraphAddNode(&node, graph, nullptr, 0, &cp) == cudaSuccess;
+    }
+    const unsigned long long l0 = g_launches;
+    if (ok) ok = cudaStreamBeginCaptureToGraph(st_, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                               cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+    if (ok) {
+      bool body_ok = true;
+      in_graph_ = 1;
+      try {
+        body(h);
+      } catch (...) {
+        body_ok = false;
+      }
+      in_graph_ = 0;
+      ok = cudaStreamEndCapture(st_, nullptr) == cudaSuccess && body_ok;
+    }
+    G.body_kernels = g_launches - l0;
+    g_launches = l0;
+    if (ok) ok = cudaGraphInstantiate(&G.exec, graph, 0) == cudaSuccess;
+    if (graph) cudaGraphDestroy(graph);
+    if (!ok) {
+      if (G.exec) cudaGraphExecDestroy(G.exec);
+      G.exec = nullptr;
+      G.failed = true;
+      cudaGetLastError();
+    }
+    prof.on = was;
+    return ok;
+  }
+  // Runs a device loop (or, with graphs off or the profiler on, the same
+  // body launch by launch with a host-side test of the loop condition).
+  // ctl[0..3] must be set by the caller; returns after the loop ends.
+  template <class Body>
+  void run_loop(LoopGraph& G, Body&& body) {
+    if (use_graphs_ && !prof.on && !G.failed && (G.exec || build_loop(G, body))) {
+      NDS_CUDA(cudaGraphLaunch(G.exec, st_));
+      NDS_CUDA(cudaMemcpyAsync(hflags_ + 4, ctl_.p, 4 * sizeof(int), cudaMemcpyDeviceToHost, st_));
+      NDS_CUDA(cudaMemcpyAsync(hflags_, flags_.p, sizeof(int), cudaMemcpyDeviceToHost, st_));
+      NDS_CUDA(cudaStreamSynchronize(st_));
+      g_launches += (unsigned long long)hflags_[4] * G.body_kernels;
+      return;
+    }
+    // host-driven: the body's check kernel (launched with in_graph_ = 0)
+    // leaves the decision to this loop, which reads ctl and the flags
+    for (;;) {
+      body(cudaGraphConditionalHandle{});
+      NDS_CUDA(cudaMemcpyAsync(hflags_ + 4, ctl_.p, 4 * sizeof(int), cudaMemcpyDeviceToHost, st_));
+      NDS_CUDA(cudaMemcpyAsync(hflags_, flags_.p, sizeof(int), cudaMemcpyDeviceToHost, st_));
+      NDS_CUDA(cudaStreamSynchronize(st_));
+      prof.collect();
+      const int its = hflags_[4], conv = hflags_[5], cap = hflags_[7];
+      if (conv || hflags_[0] != 0 || its >= cap) break;
+    }
+  }
+  void set_target(double tol, double r0) {
+    hsc_[S_R0] = r0;
+    hsc_[S_TARGET] = tol;
+    NDS_CUDA(cudaMemcpyAsync(sc_.p + S_R0, hsc_ + S_R0, 2 * sizeof(double), cudaMemcpyHostToDevice, st_));
+  }
+  void set_ctl(int a, int b, int c, int d) {
+    const int init[4] = {a, b, c, d};
+    std::memcpy(hflags_ + 4, init, sizeof(init));
+    NDS_CUDA(cudaMemcpyAsync(ctl_.p, hflags_ + 4, 4 * sizeof(int), cudaMemcpyHostToDevice, st_));
+    NDS_CUDA(cudaMemsetAsync(flags_.p, 0, sizeof(int), st_));
+  }
+  // inner FP32 PCG on rf_ (unit norm) from xf_ = 0 to ||r|| <= tol within
+  // cap iterations; returns the iterations
+  int inner_pcg(double tol, int cap) {
+    xf_.zero(st_);
+    set_target(tol, 1.0);
+    set_ctl(0, 0, 1, cap);
+    run_loop(g_loopf_, [&](cudaGraphConditionalHandle h) { pcgf_body(h); });
+    const int f = hflags_[0];
+    if (f & 8) throw SolveFailure(NDS_E_BREAKDOWN, "inner FP32 PCG initial rho nonpositive");
+    if (f & 1) throw SolveFailure(NDS_E_BREAKDOWN, "inner FP32 PCG pAp nonpositive");
+    if (f & 2) throw SolveFailure(NDS_E_BREAKDOWN, "inner FP32 PCG rho nonpositive");
+    if (f & 4) throw SolveFailure(NDS_E_BREAKDOWN, "inner FP32 PCG residual nonfinite");
+    return hflags_[4];
+  }
+  // one FGMRES pass on V_0 = r / rn: x += rn sum y_i z_i; returns the
+  // Arnoldi steps taken
+  int inner_fgmres(double rn, double tol, int cap) {
+    const k::FgLayout L{fg_m_};
+    k::scale_to_float<<<grid_for(nc_), kBlock, 0, st_>>>(nc_, r_.p, 1.0 / rn, fgV_.p);
+    NDS_LAUNCH();
+    set_target(tol, 1.0);
+    set_ctl(0, 0, 0, cap);
+    k::fg_start<<<1, 1, 0, st_>>>(fg_.p, L, ctl_.p, cap);
+    NDS_LAUNCH();
+    run_loop(g_fgmres_, [&](cudaGraphConditionalHandle h) { fg_body(h); });
+    if (hflags_[0] & 16) throw SolveFailure(NDS_E_BREAKDOWN, "inner FGMRES breakdown or nonfinite value");
+    const int k_done = hflags_[4];
+    k::fg_backsolve<<<1, 1, 0, st_>>>(fg_.p, L, ctl_.p);
+    NDS_LAUNCH();
+    k::fg_combine<<<grid_for(nc_), kBlock, 0, st_>>>(nc_, fgZ_.p, fg_.p, L, ctl_.p, rn, x_.p);
+    NDS_LAUNCH();
+    return k_done;
+  }
+  // Galerkin guess over the stored corrections: sets x_, r_; returns ||r||
+  // (or a negative value when the guess is not usable and x_ = 0, r_ = b)
+  template <int K>
+  double guess_k(const double* rhs) {
+    const size_t n = (size_t)nc_;
+    for (int a = 0; a < K; ++a) op_spmv(fine_op(), (const double*)(gY_.p + a * n), gW_.p + a * n);
+    constexpr int NG = K * (K + 1) / 2 + K;
+    const int g = red_grid(nc_);
+    k::guess_dots<K><<<g, kBlock, 0, st_>>>(nc_, gY_.p, gW_.p, rhs, fgpart_.p);
+    NDS_LAUNCH();
+    k::reduce_partials<NG><<<1, kBlock, 0, st_>>>(fgpart_.p, g, sc_.p + S_GUESS);
+    NDS_LAUNCH();
+    fetch(S_GUESS, NG);
+    // G c = f by Cholesky (G symmetric positive definite unless the stored
+    // corrections are dependent; then no guess)
+    double G[K][K], f[K], c[K];
+    int q = 0;
+    for (int a = 0; a < K; ++a)
+      for (int b = a; b < K; ++b) G[a][b] = G[b][a] = hsc_[S_GUESS + q++];
+    for (int a = 0; a < K; ++a) f[a] = hsc_[S_GUESS + q++];
+    double Lc[K][K] = {};
+    for (int a = 0; a < K; ++a) {
+      for (int b = 0; b <= a; ++b) {
+        double sum = G[a][b];
+        for (int e = 0; e < b; ++e) sum -= Lc[a][e] * Lc[b][e];
+        if (a == b) {
+          if (!(sum > 1e-14 * std::max(G[a][a], 1e-300)) || !std::isfinite(sum)) return -1.0;
+          Lc[a][a] = std::sqrt(sum);
+        } else {
+          Lc[a][b] = sum / Lc[b][b];
+        }
+      }
+    }
+    for (int a = 0; a < K; ++a) {
+      double sum = f[a];
+      for (int e = 0; e < a; ++e) sum -= Lc[a][e] * c[e];
+      c[a] = sum / Lc[a][a];
+    }
+    for (int a = K - 1; a >= 0; --a) {
+      double sum = c[a];
+      for (int e = a + 1; e < K; ++e) sum -= Lc[e][a] * c[e];
+      c[a] = sum / Lc[a][a];
+    }
+    for (int a = 0; a < K; ++a) hsc_[S_COEF + a] = c[a];
+    NDS_CUDA(cudaMemcpyAsync(sc_.p + S_COEF, hsc_ + S_COEF, K * sizeof(double), cudaMemcpyHostToDevice, st_));
+    k::guess_apply<K><<<g, kBlock, 0, st_>>>(nc_, gY_.p, gW_.p, rhs, sc_.p + S_COEF, x_.p, r_.p, part_.p);
+    NDS_LAUNCH();
+    reduce_to<1>(g, S_TMP);
+    fetch(S_TMP, 1);
+    return std::sqrt(hsc_[S_TMP]);
+  }
+  double apply_guess(const double* rhs) {
+    switch (std::min(o_.p_guess, nguess_)) {
+      case 1: return guess_k<1>(rhs);
+      case 2: return guess_k<2>(rhs);
+      case 3: return guess_k<3>(rhs);
+      case 4: return guess_k<4>(rhs);
+      default: return -1.0;
+    }
+  }
+  void store_guess() {
+    if (o_.p_guess <= 0) return;
+    vcopy(nc_, (const double*)x_.p, gY_.p + (size_t)guess_head_ * nc_);
+    guess_head_ = (guess_head_ + 1) % o_.p_guess;
+    nguess_ = std::min(nguess_ + 1, o_.p_guess);
+  }
+  PRes mixed_solve(const T* rhs_t) {
+    PRes R;
+    if constexpr (!kSame) {
+      const double* rhs = rhs_t;
+      const double bn = std::sqrt(dot_fetch(rhs, rhs, nc_, S_TMP));
+      if (!std::isfinite(bn)) throw SolveFailure(NDS_E_BREAKDOWN, "pressure initial norm nonfinite");
+      const double target = std::max(o_.p_atol, o_.p_rtol * bn);
+      start_readback();
+      if (bn <= o_.p_atol) {
+        x_.zero(st_);
+        R.ok = true;
+        R.rel = 0.0;
+        return R;
+      }
+      double rn = -1.0;
+      if (o_.p_guess > 0 && nguess_ > 0) rn = apply_guess(rhs);
+      if (!(rn >= 0.0) || !std::isfinite(rn)) {
+        x_.zero(st_);
+        vcopy(nc_, rhs, r_.p);
+        rn = bn;
+      }
+      int passes = 0;
+      for (;;) {
+        if (rn <= target) {
+          R.ok = true;
+          break;
+        }
+        if (passes >= o_.p_refine_max || R.its >= o_.p_max) break;
+        const double tol = std::max(o_.p_inner_rtol, 0.5 * target / rn);
+        const int cap = o_.p_max - R.its;
+        if (fg_m_ > 0) {
+          R.its += inner_fgmres(rn, tol, std::min(cap, fg_m_));
+        } else {
+          k::scale_to_float<<<grid_for(nc_), kBlock, 0, st_>>>(nc_, r_.p, 1.0 / rn, rf_.p);
+          NDS_LAUNCH();
+          R.its += inner_pcg(tol, cap);
+          k::axpy_from_float<<<grid_for(nc_), kBlock, 0, st_>>>(nc_, rn, xf_.p, x_.p);
+          NDS_LAUNCH();
+        }
+        ++passes;
+        op_resid(fine_op(), (const double*)x_.p, rhs, r_.p);
+        rn = std::sqrt(dot_fetch((const double*)r_.p, (const double*)r_.p, nc_, S_TMP));
+        if (!std::isfinite(rn)) throw SolveFailure(NDS_E_BREAKDOWN, "pressure defect nonfinite");
+      }
+      R.rel = rn / std::max(bn, 1e-300);
+      last_passes_ = passes;
+      if (R.ok) store_guess();
+    }
+    return R;
+  }
+
   // ------------------------------------------------------ SIMPLE iteration
   void assemble() {
     k::MomArgs<T> a;
@@ -1367,6 +1680,8 @@ class Solver final : public ISolver {
     u3_.zero(st_);
     p_.zero(st_);
     it_ = 0;
+    nguess_ = 0;
+    guess_head_ = 0;
     cont0_ = -1.0;
     cont_rel_ = 1.0;
     NDS_CUDA(cudaStreamSynchronize(st_));
@@ -1420,7 +1735,8 @@ class Solver final : public ISolver {
     NDS_CUDA(cudaStreamWaitEvent(st_, ev_side_[1], 0));
     NDS_CUDA(cudaEventRecord(ev_[6], st_));
     PRes pr;
-    if (o_.pressure_solver == NDS_P_PCG) pr = pcg(rhs_.p);
+    if (mixed_) pr = mixed_solve(rhs_.p);
+    else if (o_.pressure_solver == NDS_P_PCG) pr = pcg(rhs_.p);
     else pr = stationary(rhs_.p, o_.pressure_solver == NDS_P_CHEB);
     R.p_its = pr.its;
     R.p_rel = pr.rel;
@@ -1656,6 +1972,15 @@ class Solver final : public ISolver {
   DBuf<TA> fvalA_, fdiag_, fl1_, fr_, ftmp_, fcorr_, frhs_, fpong_, tinv_, rA_, zA_;
   std::vector<Level> L_;
   std::vector<Xfer> X_;
+  // mixed precision (NDS_MIXED): inner FP32 Krylov vectors, FGMRES basis
+  // V (m+1 vectors) and preconditioned vectors Z (m), its FP64 work array,
+  // and the stored corrections Y (and A Y) of the Galerkin guess
+  bool mixed_ = false;
+  int in_graph_ = 0;  // 1 while a loop body is being captured (its check kernel sets the graph condition)
+  int fg_m_ = 0, nguess_ = 0, guess_head_ = 0, last_passes_ = 0;
+  DBuf<float> xf_, rf_, zf_, pf_, qf_, fgV_, fgZ_;
+  DBuf<double> fg_, fgpart_, gY_, gW_;
+  LoopGraph g_loopf_, g_fgmres_;
   DBuf<double> part_, sc_;
   DBuf<int> flags_;
   double* hsc_ = nullptr;

@@ -77,11 +77,22 @@ PipeBC make_pipe(const Mesh& m, const SetupOptions& o) {
     ymin = std::min(ymin, m.y(v)); ymax = std::max(ymax, m.y(v));
     zmin = std::min(zmin, m.z(v)); zmax = std::max(zmax, m.z(v));
   }
-  P.cx = 0.5 * (xmin + xmax);
-  P.cy = 0.5 * (ymin + ymax);
   P.z_in = zmin;
   P.z_out = zmax;
   P.L = zmax - zmin;
+  if (o.geom_from_inlet) {
+    // the inlet disk's own extent (its rim vertices lie on the pipe wall)
+    const auto& pin0 = m.patches[(size_t)P.inlet];
+    xmin = ymin = 1e300;
+    xmax = ymax = -1e300;
+    for (int f = pin0.start; f < pin0.start + pin0.count; ++f)
+      for (int v : m.faces[(size_t)f]) {
+        xmin = std::min(xmin, m.x(v)); xmax = std::max(xmax, m.x(v));
+        ymin = std::min(ymin, m.y(v)); ymax = std::max(ymax, m.y(v));
+      }
+  }
+  P.cx = 0.5 * (xmin + xmax);
+  P.cy = 0.5 * (ymin + ymax);
   P.R = 0.5 * std::max(xmax - xmin, ymax - ymin);
   P.D = 2 * P.R;
   if (!(P.R > 0 && P.L > 0 && o.re > 0 && o.bulk > 0)) throw std::runtime_error("invalid pipe geometry or flow parameters");

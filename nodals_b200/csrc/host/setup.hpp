@@ -97,6 +97,10 @@ struct SetupOptions {
   double supg_tau_scale = 0.05, supg_magic = 9.0;
   std::string wall = "patch_0_0", inlet = "patch_2_0", outlet = "patch_1_0";
   int threads = 0;  // 0: all hardware threads
+  // pipe centre and radius from the inlet patch's vertices instead of the
+  // bounding box of the whole mesh (bent pipes, whose bounding box is not
+  // the inlet disk's); the reference's rule is the bounding box
+  bool geom_from_inlet = false;
 };
 
 Setup build_setup(const Mesh& m, const SetupOptions& o);

@@ -19,7 +19,8 @@ NDS_OK = 0
 ERRORS = {-1: "NDS_E_INVALID", -2: "NDS_E_SETUP", -3: "NDS_E_CUDA", -4: "NDS_E_BREAKDOWN",
           -5: "NDS_E_NOT_CONVERGED", -6: "NDS_E_STATE"}
 
-PRECISION = {"fp64": 0, "fp32": 1, "amg_fp32": 2}
+PRECISION = {"fp64": 0, "fp32": 1, "amg_fp32": 2, "mixed": 3}
+KRYLOV = {"pcg": 0, "fgmres": 1}
 RUN_MODE = {"fixed10": 0, "converge": 1}
 MOMENTUM_WORK = {"fgs1": 0, "altgs1": 1, "sgs1": 2}
 PRESSURE_SOLVER = {"pcg": 0, "richardson": 1, "cheb": 2}
@@ -30,7 +31,8 @@ MCGS_ORDER = {"symmetric": 0, "forward": 1, "backward": 2}
 CF_INTERP = {"direct": 0, "exti": 1}
 _ENUMS = {"precision": PRECISION, "run_mode": RUN_MODE, "momentum_work": MOMENTUM_WORK,
           "pressure_solver": PRESSURE_SOLVER, "amg_hierarchy": AMG_HIERARCHY, "amg_smoother": AMG_SMOOTHER,
-          "amg_spectrum_policy": SPECTRUM, "amg_mcgs_order": MCGS_ORDER, "cf_interp": CF_INTERP}
+          "amg_spectrum_policy": SPECTRUM, "amg_mcgs_order": MCGS_ORDER, "cf_interp": CF_INTERP,
+          "p_krylov": KRYLOV}
 
 
 class NdsError(RuntimeError):
@@ -66,6 +68,8 @@ class Options(C.Structure):
         ("wall", C.c_char * 64), ("inlet", C.c_char * 64), ("outlet", C.c_char * 64),
         ("precision", C.c_int), ("threads", C.c_int), ("device", C.c_int), ("verbose", C.c_int),
         ("supg", C.c_int), ("supg_tau_scale", C.c_double), ("supg_magic", C.c_double),
+        ("p_krylov", C.c_int), ("p_restart", C.c_int), ("p_inner_rtol", C.c_double), ("p_refine_max", C.c_int),
+        ("p_guess", C.c_int), ("learned", C.c_int), ("geom_from_inlet", C.c_int),
     ]
 
     @classmethod
