@@ -100,7 +100,7 @@ typedef struct nds_options {
   int p_restart;         /* FGMRES basis vectors per pass, 1..64 (default 30) */
   double p_inner_rtol;   /* relative target of one FP32 inner pass (default 1e-3) */
   int p_refine_max;      /* FP64 defect-correction passes per solve (default 8) */
-  int p_guess;           /* earlier corrections spanning a Galerkin initial guess, 0..4 (0: zero guess) */
+  int p_guess;           /* earlier corrections spanning a Galerkin initial guess, 0..8 (0: zero guess) */
   int learned;           /* 1: learned stage ahead of the V-cycle (FGMRES only; nds_solver_load_stage) */
   /* 1: pipe centre and radius from the inlet patch instead of the bounding
    * box (bent pipes); 0: the reference's bounding-box rule (g4_host.hpp:37-49) */
@@ -243,6 +243,61 @@ unsigned long long nds_launch_count(void);
  * updated. */
 int nds_continuity_noalloc(nds_solver* s, const double* u0, const double* u1, const double* u2, double* r,
                            double* norm, void* stream);
+
+/* ---- learned pressure stage (no counterpart in the reference) ----------
+ * A message-passing network on the face graph of the pressure cells (3
+ * layers of width 64, BF16 weights, tcgen05 tensor-core GEMMs with FP32
+ * accumulation) that maps a pressure-correction residual v to an
+ * approximate correction z.  With options learned = 1 (precision mixed,
+ * p_krylov fgmres) it is a flexible-preconditioner stage ahead of the AMG
+ * V-cycle: z = N(v) + V(v - A N(v)), or the plain V(v) whenever the stage
+ * does not reduce the residual (||v - A N(v)|| >= ||v||).
+ * The graph: n nodes, nbr[4 n] face neighbours (-1: boundary face), ew[4 n]
+ * edge weights a_ij / sqrt(a_ii a_jj) of the Jacobi-scaled pressure
+ * operator, dscale[n] = 1 / sqrt(a_ii); device pointers.  Parameter vector
+ * (FP32, NDS_MPNN_NPARAM values): We[64][2], be[64], then for l = 1..3
+ * W_l[64][128] (out x in, input [h ; sum_j e_ij h_j]), b_l[64], then
+ * wd[64], bd, cs (out = wd . h3 + bd + cs s). */
+#define NDS_MPNN_NPARAM 25026
+typedef struct nds_mpnn_graph {
+  int n;
+  const int32_t* nbr;
+  const float* ew;
+  const float* dscale;
+} nds_mpnn_graph;
+typedef struct nds_mpnn nds_mpnn;
+int nds_mpnn_param_count(void);
+/* device state for graphs of up to n_max nodes; training = 1 keeps the
+ * activations, gradients and Adam moments */
+int nds_mpnn_create(int n_max, int training, int device, nds_mpnn** out);
+int nds_mpnn_set_params(nds_mpnn* m, const float* host_params, int count);
+int nds_mpnn_get_params(nds_mpnn* m, float* host_params, int count);
+/* z = N(v) (device pointers); the graph may hold nseg independent segments
+ * (seg_off[0..nseg] host offsets, each normalised on its own; nseg = 0: one) */
+int nds_mpnn_forward(nds_mpnn* m, const nds_mpnn_graph* g, int nseg, const int32_t* seg_off, const float* v,
+                     float* z);
+/* forward, loss and backward for pairs (v, x) of right-hand sides and
+ * solutions: loss = mean over segments of sum_i (out_i - t_i)^2 / sum_i t_i^2,
+ * t_i = x_i / (dscale_i sigma_s); gradients kept for nds_mpnn_get_grads and
+ * nds_mpnn_adam_step */
+int nds_mpnn_loss_backward(nds_mpnn* m, const nds_mpnn_graph* g, int nseg, const int32_t* seg_off, const float* v,
+                           const float* x, double* loss);
+int nds_mpnn_get_grads(nds_mpnn* m, float* host_grads, int count);
+int nds_mpnn_adam_step(nds_mpnn* m, float lr, float beta1, float beta2, float eps, int step);
+/* BF16 activations h^layer (n_max x 64, row-major) into a device buffer */
+int nds_mpnn_activations(nds_mpnn* m, int layer, void* out_dev);
+void nds_mpnn_destroy(nds_mpnn* m);
+/* the solver's side of the stage: load its parameters (host array); copy the
+ * current graph (face neighbours, edge weights and scaling from the operator
+ * of the last refresh) into device arrays of nc (4 nc) entries; copy the
+ * last pressure solve's right-hand side and solution as FP32 (device arrays
+ * of nc entries) -- the training pairs */
+int nds_solver_load_stage(nds_solver* s, const float* host_params, int count);
+int nds_solver_stage_graph(nds_solver* s, int32_t* nbr, float* ew, float* dscale);
+int nds_solver_pressure_pair(nds_solver* s, float* rhs, float* x);
+/* counters of the learned stage since the solver was created: applications
+ * and fallbacks to the plain V-cycle */
+int nds_solver_stage_counts(nds_solver* s, long long* applied, long long* fallbacks);
 
 /* ---- mixed hexahedron/tetrahedron Stokes gate: replaces the reference's
  *      HXT4A executable (gpu/serial_cuda/hybrid_hxt4a/hxt4a_main.cu:405-518,

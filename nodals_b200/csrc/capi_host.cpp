@@ -761,7 +761,7 @@ bool validate_options(const nds_options& o, std::string& why) {
   if (o.p_restart < 1 || o.p_restart > 64) return bad("p_restart must be in 1..64");
   if (!(o.p_inner_rtol > 0.0 && o.p_inner_rtol < 1.0)) return bad("p_inner_rtol must be in (0, 1)");
   if (o.p_refine_max < 1) return bad("p_refine_max must be >= 1");
-  if (o.p_guess < 0 || o.p_guess > 4) return bad("p_guess must be in 0..4");
+  if (o.p_guess < 0 || o.p_guess > 8) return bad("p_guess must be in 0..8");
   if (o.learned && (o.precision != NDS_MIXED || o.p_krylov != NDS_KRYLOV_FGMRES))
     return bad("the learned stage needs precision mixed and p_krylov fgmres (a varying preconditioner)");
   if (o.precision == NDS_MIXED && o.pressure_solver != NDS_P_PCG)

@@ -27,6 +27,7 @@
 #include "common.cuh"
 #include "kernels.cuh"
 #include "krylov.cuh"
+#include "mpnn.hpp"
 
 namespace nds {
 
@@ -149,6 +150,11 @@ struct ISolver {
   // state type is double
   virtual bool cell_arrays(const int32_t** ref, const double** bco, const double** fixed_div, int* nc,
                            int* device) const = 0;
+  // learned pressure stage (precision mixed, FGMRES)
+  virtual void load_stage(const float* host_params) = 0;
+  virtual void stage_graph(int32_t* nbr, float* ew, float* dscale) = 0;
+  virtual void pressure_pair(float* rhs, float* x) = 0;
+  virtual void stage_counts(long long* applied, long long* fallbacks) = 0;
   Profiler prof;
 };
 
@@ -218,6 +224,42 @@ void greedy_color(int n, const std::vector<int32_t>& row, const std::vector<int3
   rows_out.resize((size_t)n);
   std::vector<int> next(off_out.begin(), off_out.end() - 1);
   for (int i = 0; i < n; ++i) rows_out[(size_t)next[(size_t)color[(size_t)i]]++] = i;
+}
+
+// Jacobi scaling and edge weights of the learned stage's graph from the
+// current FP32 operator: dscale_i = 1 / sqrt(a_ii), e_ij = a_ij dscale_i dscale_j
+// (a_ij read at its SELL offset off[4 i + k]; 0 for a boundary slot)
+__global__ void stage_dscale(int n, const float* __restrict__ diag, float* __restrict__ dscale) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dscale[i] = diag[i] > 0.f ? rsqrtf(diag[i]) : 0.f;
+}
+__global__ void stage_edges(int n, const int32_t* __restrict__ nbr, const int32_t* __restrict__ off,
+                            const float* __restrict__ val, const float* __restrict__ dscale, float* __restrict__ ew) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 4 * n) return;
+  const int i = t >> 2, j = nbr[t];
+  ew[t] = j >= 0 ? val[off[t]] * dscale[i] * dscale[j] : 0.f;
+}
+// after t = v - A z1: keep (t, z1) when ||t|| < ||v||, else fall back to the
+// plain V-cycle (t = v, z1 = 0); counters: [0] applications, [1] fallbacks
+__global__ void stage_select(int n, const float* __restrict__ v, float* __restrict__ t, float* __restrict__ z1,
+                             const double* __restrict__ sc, int tt_slot, int vv_slot,
+                             unsigned long long* __restrict__ cnt) {
+  const bool bad = !(sc[tt_slot] < sc[vv_slot]);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    cnt[0] += 1;
+    if (bad) cnt[1] += 1;
+  }
+  if (!bad) return;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    t[i] = v[i];
+    z1[i] = 0.f;
+  }
+}
+template <class Tin>
+__global__ void to_float(int n, const Tin* __restrict__ a, float* __restrict__ b) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) b[i] = (float)a[i];
 }
 
 double cheb_root(double hi, double lo, int k, int degree) {
@@ -602,12 +644,12 @@ class Solver final : public ISolver {
 
   // ------------------------------------------------------------------ helpers
   static constexpr int kMaxPartBlocks = 1184;  // 8 x 148 SMs
-  static constexpr int kScalars = 64;
+  static constexpr int kScalars = 128;
   enum { S_RHO = 0, S_PQ = 1, S_ALPHA = 2, S_RN2 = 3, S_RHON = 4, S_BETA = 5, S_R0 = 6, S_TARGET = 7, S_TMP = 8,
          S_TMP2 = 9, S_CONT2 = 10, S_WN = 11,
-         S_AUDIT = 16,
-         S_GUESS = 24,  // 14 slots: Galerkin matrix (upper triangle) and right-hand side of the guess
-         S_COEF = 40 };  // 4 slots: guess coefficients
+         S_AUDIT = 16, S_ST_T = 20, S_ST_V = 21,
+         S_GUESS = 24,  // 44 slots: Galerkin matrix (upper triangle) and right-hand side of the guess
+         S_COEF = 72 };  // 8 slots: guess coefficients
 
   // CUDA graphs of fixed launch sequences (no host decisions inside)
   struct Graph {
@@ -1301,15 +1343,122 @@ class Solver final : public ISolver {
       fg_.alloc((size_t)k::FgLayout{fg_m_}.size());
       fg_.zero(st_);
     }
-    fgpart_.alloc((size_t)kMaxPartBlocks * std::max(fg_m_ + 1, 16));
+    fgpart_.alloc((size_t)kMaxPartBlocks * std::max(fg_m_ + 1, 48));
     if (o_.p_guess > 0) {
       gY_.alloc((size_t)o_.p_guess * n);
       gW_.alloc((size_t)o_.p_guess * n);
     }
   }
-  // the preconditioner of the inner solves: z = M v (FP32)
+  // the preconditioner of the inner solves: z = M v (FP32).  With the
+  // learned stage: z1 = N(v), t = v - A z1; the V-cycle then solves for t and
+  // z = z1 + V(t) -- or, when the stage did not reduce the residual
+  // (||t|| >= ||v||), z = V(v) (the plain preconditioner as fallback).
   void precond_f(const float* v, float* z) {
-    if constexpr (!kSame) amg_apply(v, z);
+    if constexpr (!kSame) {
+      if (!stage_) {
+        amg_apply(v, z);
+        return;
+      }
+      mpnn_forward(*stage_, stage_view(), v, st_z1_.p);
+      op_resid(fine_opA(), (const float*)st_z1_.p, v, st_t_.p);
+      dot_dev((const float*)st_t_.p, (const float*)st_t_.p, nc_, S_ST_T);
+      dot_dev(v, v, nc_, S_ST_V);
+      stage_select<<<red_grid(nc_), kBlock, 0, st_>>>(nc_, v, st_t_.p, st_z1_.p, sc_.p, S_ST_T, S_ST_V, st_cnt_.p);
+      NDS_LAUNCH();
+      amg_apply(st_t_.p, z);
+      vaxpy(nc_, 1.0, (const float*)st_z1_.p, z);
+    }
+  }
+  nds_mpnn_graph stage_view() const { return nds_mpnn_graph{nc_, sg_nbr_.p, sg_ew_.p, sg_dscale_.p}; }
+  // face graph of the cells and the SELL offsets of its edges
+  void build_stage_graph() {
+    const Mesh& M = P_.mesh;
+    const FineTopo& F = P_.setup.fine;
+    std::vector<int32_t> nbr(4 * (size_t)nc_, -1), off(4 * (size_t)nc_, -1);
+    std::vector<int> cnt((size_t)nc_, 0);
+    auto add = [&](int a, int b) {
+      if (cnt[(size_t)a] >= 4) throw std::runtime_error("learned stage: a cell with more than four face neighbours");
+      nbr[4 * (size_t)a + cnt[(size_t)a]++] = b;
+    };
+    for (size_t f = 0; f < M.neighbour.size(); ++f) {
+      add(M.owner[f], M.neighbour[f]);
+      add(M.neighbour[f], M.owner[f]);
+    }
+    std::vector<int32_t> base((size_t)(nc_ + 31) / 32 + 1);
+    NDS_CUDA(cudaMemcpy(base.data(), sbase_.p, sizeof(int32_t) * base.size(), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < nc_; ++i)
+      for (int k = 0; k < 4; ++k) {
+        const int j = nbr[4 * (size_t)i + k];
+        if (j < 0) continue;
+        int pos = -1;
+        for (int q = F.row[(size_t)i]; q < F.row[(size_t)i + 1]; ++q)
+          if (F.col[(size_t)q] == j) pos = q - F.row[(size_t)i];
+        if (pos < 0) throw std::runtime_error("learned stage: face neighbour missing from the pressure operator");
+        off[4 * (size_t)i + k] = base[(size_t)(i >> 5)] + 128 * (pos >> 2) + 4 * (i & 31) + (pos & 3);
+      }
+    sg_nbr_.upload(nbr);
+    sg_off_.upload(off);
+    sg_ew_.alloc(4 * (size_t)nc_);
+    sg_dscale_.alloc((size_t)nc_);
+    st_z1_.alloc((size_t)nc_);
+    st_t_.alloc((size_t)nc_);
+    st_cnt_.alloc(2);
+    st_cnt_.zero(st_);
+  }
+  // edge weights and scaling from the operator of the last refresh
+  void update_stage_graph() {
+    if constexpr (!kSame) {
+      stage_dscale<<<grid_for(nc_), kBlock, 0, st_>>>(nc_, fdiag_.p, sg_dscale_.p);
+      NDS_LAUNCH();
+      stage_edges<<<grid_for(4LL * nc_), kBlock, 0, st_>>>(nc_, sg_nbr_.p, sg_off_.p, fvalA_.p, sg_dscale_.p, sg_ew_.p);
+      NDS_LAUNCH();
+    }
+  }
+  void load_stage(const float* host) override {
+    if constexpr (kSame) {
+      throw SolveFailure(NDS_E_INVALID, "the learned stage needs precision mixed");
+    } else {
+      if (!mixed_ || fg_m_ == 0) throw SolveFailure(NDS_E_INVALID, "the learned stage needs precision mixed and FGMRES");
+      if (!sg_nbr_.p) build_stage_graph();
+      if (!stage_) stage_ = make_mpnn(nc_, false, st_);
+      mpnn_set_params(*stage_, host);
+      // the FGMRES loop body is captured with the stage: rebuild it
+      if (g_fgmres_.exec) cudaGraphExecDestroy(g_fgmres_.exec);
+      g_fgmres_.exec = nullptr;
+      g_fgmres_.failed = false;
+    }
+  }
+  void stage_graph(int32_t* nbr, float* ew, float* dscale) override {
+    if constexpr (kSame) {
+      throw SolveFailure(NDS_E_INVALID, "the learned stage needs precision mixed");
+    } else {
+      if (!sg_nbr_.p) build_stage_graph();
+      update_stage_graph();
+      if (nbr) NDS_CUDA(cudaMemcpyAsync(nbr, sg_nbr_.p, sg_nbr_.bytes(), cudaMemcpyDeviceToDevice, st_));
+      if (ew) NDS_CUDA(cudaMemcpyAsync(ew, sg_ew_.p, sg_ew_.bytes(), cudaMemcpyDeviceToDevice, st_));
+      if (dscale) NDS_CUDA(cudaMemcpyAsync(dscale, sg_dscale_.p, sg_dscale_.bytes(), cudaMemcpyDeviceToDevice, st_));
+      NDS_CUDA(cudaStreamSynchronize(st_));
+    }
+  }
+  void pressure_pair(float* rhs, float* x) override {
+    if (rhs) {
+      to_float<T><<<grid_for(nc_), kBlock, 0, st_>>>(nc_, rhs_.p, rhs);
+      NDS_LAUNCH();
+    }
+    if (x) {
+      to_float<T><<<grid_for(nc_), kBlock, 0, st_>>>(nc_, x_.p, x);
+      NDS_LAUNCH();
+    }
+    NDS_CUDA(cudaStreamSynchronize(st_));
+  }
+  void stage_counts(long long* applied, long long* fallbacks) override {
+    unsigned long long c[2] = {0, 0};
+    if (st_cnt_.p) {
+      NDS_CUDA(cudaMemcpyAsync(c, st_cnt_.p, sizeof(c), cudaMemcpyDeviceToHost, st_));
+      NDS_CUDA(cudaStreamSynchronize(st_));
+    }
+    if (applied) *applied = (long long)c[0];
+    if (fallbacks) *fallbacks = (long long)c[1];
   }
   // one pass of the FP32 PCG loop: z = M r; rho; p; q = A p; alpha; x, r; check
   void pcgf_body(cudaGraphConditionalHandle h) {
@@ -1471,12 +1620,11 @@ class Solver final : public ISolver {
     NDS_LAUNCH();
     return k_done;
   }
-  // Galerkin guess over the stored corrections: sets x_, r_; returns ||r||
-  // (or a negative value when the guess is not usable and x_ = 0, r_ = b)
+  // Galerkin guess over the stored corrections and their stored products:
+  // sets x_ and the exact FP64 residual r_ = b - A x_; returns ||r|| (or a
+  // negative value when the guess is not usable: then nothing is set)
   template <int K>
   double guess_k(const double* rhs) {
-    const size_t n = (size_t)nc_;
-    for (int a = 0; a < K; ++a) op_spmv(fine_op(), (const double*)(gY_.p + a * n), gW_.p + a * n);
     constexpr int NG = K * (K + 1) / 2 + K;
     const int g = red_grid(nc_);
     k::guess_dots<K><<<g, kBlock, 0, st_>>>(nc_, gY_.p, gW_.p, rhs, fgpart_.p);
@@ -1484,8 +1632,8 @@ class Solver final : public ISolver {
     k::reduce_partials<NG><<<1, kBlock, 0, st_>>>(fgpart_.p, g, sc_.p + S_GUESS);
     NDS_LAUNCH();
     fetch(S_GUESS, NG);
-    // G c = f by Cholesky (G symmetric positive definite unless the stored
-    // corrections are dependent; then no guess)
+    // G c = f by Cholesky (no guess when G is not numerically positive
+    // definite, e.g. for dependent corrections)
     double G[K][K], f[K], c[K];
     int q = 0;
     for (int a = 0; a < K; ++a)
@@ -1497,7 +1645,7 @@ class Solver final : public ISolver {
         double sum = G[a][b];
         for (int e = 0; e < b; ++e) sum -= Lc[a][e] * Lc[b][e];
         if (a == b) {
-          if (!(sum > 1e-14 * std::max(G[a][a], 1e-300)) || !std::isfinite(sum)) return -1.0;
+          if (!(sum > 1e-12 * std::max(G[a][a], 1e-300)) || !std::isfinite(sum)) return -1.0;
           Lc[a][a] = std::sqrt(sum);
         } else {
           Lc[a][b] = sum / Lc[b][b];
@@ -1514,13 +1662,15 @@ class Solver final : public ISolver {
       for (int e = a + 1; e < K; ++e) sum -= Lc[e][a] * c[e];
       c[a] = sum / Lc[a][a];
     }
-    for (int a = 0; a < K; ++a) hsc_[S_COEF + a] = c[a];
+    for (int a = 0; a < K; ++a) {
+      if (!std::isfinite(c[a])) return -1.0;
+      hsc_[S_COEF + a] = c[a];
+    }
     NDS_CUDA(cudaMemcpyAsync(sc_.p + S_COEF, hsc_ + S_COEF, K * sizeof(double), cudaMemcpyHostToDevice, st_));
-    k::guess_apply<K><<<g, kBlock, 0, st_>>>(nc_, gY_.p, gW_.p, rhs, sc_.p + S_COEF, x_.p, r_.p, part_.p);
+    k::guess_combine<K><<<grid_for(nc_), kBlock, 0, st_>>>(nc_, gY_.p, sc_.p + S_COEF, x_.p);
     NDS_LAUNCH();
-    reduce_to<1>(g, S_TMP);
-    fetch(S_TMP, 1);
-    return std::sqrt(hsc_[S_TMP]);
+    op_resid(fine_op(), (const double*)x_.p, rhs, r_.p);
+    return std::sqrt(dot_fetch((const double*)r_.p, (const double*)r_.p, nc_, S_TMP));
   }
   double apply_guess(const double* rhs) {
     switch (std::min(o_.p_guess, nguess_)) {
@@ -1528,12 +1678,20 @@ class Solver final : public ISolver {
       case 2: return guess_k<2>(rhs);
       case 3: return guess_k<3>(rhs);
       case 4: return guess_k<4>(rhs);
+      case 5: return guess_k<5>(rhs);
+      case 6: return guess_k<6>(rhs);
+      case 7: return guess_k<7>(rhs);
+      case 8: return guess_k<8>(rhs);
       default: return -1.0;
     }
   }
-  void store_guess() {
+  // keep the solution and its product with this iteration's operator,
+  // w = b - r (r_ holds the final FP64 defect b - A x)
+  void store_guess(const double* rhs) {
     if (o_.p_guess <= 0) return;
-    vcopy(nc_, (const double*)x_.p, gY_.p + (size_t)guess_head_ * nc_);
+    const size_t o = (size_t)guess_head_ * nc_;
+    k::guess_store<<<grid_for(nc_), kBlock, 0, st_>>>(nc_, x_.p, rhs, r_.p, gY_.p + o, gW_.p + o);
+    NDS_LAUNCH();
     guess_head_ = (guess_head_ + 1) % o_.p_guess;
     nguess_ = std::min(nguess_ + 1, o_.p_guess);
   }
@@ -1551,9 +1709,12 @@ class Solver final : public ISolver {
         R.rel = 0.0;
         return R;
       }
+      if (o_.learned && !stage_) throw SolveFailure(NDS_E_STATE, "learned stage enabled but no parameters loaded");
+      if (stage_) update_stage_graph();
       double rn = -1.0;
       if (o_.p_guess > 0 && nguess_ > 0) rn = apply_guess(rhs);
-      if (!(rn >= 0.0) || !std::isfinite(rn)) {
+      // a guess that does not reduce the residual is dropped
+      if (!(rn >= 0.0) || !std::isfinite(rn) || rn >= bn) {
         x_.zero(st_);
         vcopy(nc_, rhs, r_.p);
         rn = bn;
@@ -1583,7 +1744,8 @@ class Solver final : public ISolver {
       }
       R.rel = rn / std::max(bn, 1e-300);
       last_passes_ = passes;
-      if (R.ok) store_guess();
+      if (stage_) mpnn_check(*stage_);
+      if (R.ok) store_guess(rhs);
     }
     return R;
   }
@@ -1981,6 +2143,12 @@ class Solver final : public ISolver {
   DBuf<float> xf_, rf_, zf_, pf_, qf_, fgV_, fgZ_;
   DBuf<double> fg_, fgpart_, gY_, gW_;
   LoopGraph g_loopf_, g_fgmres_;
+  // learned stage: network state, face graph (neighbours, SELL offsets of
+  // the edges, edge weights, Jacobi scaling), work vectors, counters
+  MpnnPtr stage_;
+  DBuf<int32_t> sg_nbr_, sg_off_;
+  DBuf<float> sg_ew_, sg_dscale_, st_z1_, st_t_;
+  DBuf<unsigned long long> st_cnt_;
   DBuf<double> part_, sc_;
   DBuf<int> flags_;
   double* hsc_ = nullptr;
@@ -2062,6 +2230,22 @@ int nds_simple_step_io(nds_solver* s, const double* u0_in, const double* u1_in, 
   });
 }
 void nds_solver_destroy(nds_solver* s) { delete s; }
+int nds_solver_load_stage(nds_solver* s, const float* host_params, int count) {
+  if (!s || !host_params || count != NDS_MPNN_NPARAM) return fail(NDS_E_INVALID, "nds_solver_load_stage: bad argument");
+  return guarded([&] { s->impl->load_stage(host_params); });
+}
+int nds_solver_stage_graph(nds_solver* s, int32_t* nbr, float* ew, float* dscale) {
+  if (!s) return fail(NDS_E_INVALID, "null solver");
+  return guarded([&] { s->impl->stage_graph(nbr, ew, dscale); });
+}
+int nds_solver_pressure_pair(nds_solver* s, float* rhs, float* x) {
+  if (!s) return fail(NDS_E_INVALID, "null solver");
+  return guarded([&] { s->impl->pressure_pair(rhs, x); });
+}
+int nds_solver_stage_counts(nds_solver* s, long long* applied, long long* fallbacks) {
+  if (!s) return fail(NDS_E_INVALID, "null solver");
+  return guarded([&] { s->impl->stage_counts(applied, fallbacks); });
+}
 
 unsigned long long nds_launch_count(void) { return nds::g_launches; }
 

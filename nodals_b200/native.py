@@ -209,6 +209,20 @@ def lib():
             L.nds_profile_enable.argtypes = [vp, C.c_int]
             L.nds_launch_count.restype = C.c_ulonglong
             L.nds_profile_read.argtypes = [vp, C.POINTER(ProfileEntry), C.c_int, C.POINTER(C.c_int)]
+        if hasattr(L, "nds_mpnn_create"):
+            L.nds_mpnn_create.argtypes = [C.c_int, C.c_int, C.c_int, C.POINTER(vp)]
+            L.nds_mpnn_set_params.argtypes = [vp, vp, C.c_int]
+            L.nds_mpnn_get_params.argtypes = [vp, vp, C.c_int]
+            L.nds_mpnn_get_grads.argtypes = [vp, vp, C.c_int]
+            L.nds_mpnn_forward.argtypes = [vp, C.c_void_p, C.c_int, vp, vp, vp]
+            L.nds_mpnn_loss_backward.argtypes = [vp, C.c_void_p, C.c_int, vp, vp, vp, C.POINTER(C.c_double)]
+            L.nds_mpnn_adam_step.argtypes = [vp, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int]
+            L.nds_mpnn_activations.argtypes = [vp, C.c_int, vp]
+            L.nds_mpnn_destroy.argtypes = [vp]
+            L.nds_solver_load_stage.argtypes = [vp, vp, C.c_int]
+            L.nds_solver_stage_graph.argtypes = [vp, vp, vp, vp]
+            L.nds_solver_pressure_pair.argtypes = [vp, vp, vp]
+            L.nds_solver_stage_counts.argtypes = [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
         _lib = L
     return _lib
 
@@ -449,3 +463,96 @@ def hp_errors(problem: Problem, u0, u1, u2, p) -> dict:
 def write_vtu(problem: Problem, path, u0, u1, u2, p, converged: bool = False, outer_its: int = 0):
     a = [_f64(x) for x in (u0, u1, u2, p)]
     _check(lib().nds_write_vtu(problem._h, str(path).encode(), *[_p(x) for x in a], int(converged), int(outer_its)))
+
+
+# ---------------------------------------------------------------- learned stage
+class MpnnGraph(C.Structure):
+    _fields_ = [("n", C.c_int), ("nbr", C.c_void_p), ("ew", C.c_void_p), ("dscale", C.c_void_p)]
+
+
+MPNN_NPARAM = 25026
+
+
+class Mpnn:
+    """Device state of the learned stage's network (nds_mpnn_*): graphs of up
+    to n_max nodes; training=True keeps activations, gradients, Adam moments.
+    Arrays passed in are device addresses (ints) or objects with data_ptr()."""
+
+    def __init__(self, n_max: int, training: bool = False, device: int = 0):
+        h = C.c_void_p()
+        _check(lib().nds_mpnn_create(int(n_max), int(training), int(device), C.byref(h)))
+        self._h = h
+
+    @staticmethod
+    def _addr(x):
+        if x is None:
+            return None
+        return C.c_void_p(x if isinstance(x, int) else x.data_ptr())
+
+    def graph(self, n, nbr, ew, dscale) -> MpnnGraph:
+        return MpnnGraph(int(n), self._addr(nbr), self._addr(ew), self._addr(dscale))
+
+    def set_params(self, p: np.ndarray):
+        a = np.ascontiguousarray(p, dtype=np.float32)
+        _check(lib().nds_mpnn_set_params(self._h, a.ctypes.data_as(C.c_void_p), MPNN_NPARAM))
+
+    def params(self) -> np.ndarray:
+        a = np.zeros(MPNN_NPARAM, dtype=np.float32)
+        _check(lib().nds_mpnn_get_params(self._h, a.ctypes.data_as(C.c_void_p), MPNN_NPARAM))
+        return a
+
+    def grads(self) -> np.ndarray:
+        a = np.zeros(MPNN_NPARAM, dtype=np.float32)
+        _check(lib().nds_mpnn_get_grads(self._h, a.ctypes.data_as(C.c_void_p), MPNN_NPARAM))
+        return a
+
+    @staticmethod
+    def _segs(segs):
+        if segs is None:
+            return 0, None
+        s = np.ascontiguousarray(segs, dtype=np.int32)
+        return len(s) - 1, s
+
+    def forward(self, g: MpnnGraph, v, z, segs=None):
+        ns, s = self._segs(segs)
+        _check(lib().nds_mpnn_forward(self._h, C.byref(g), ns, None if s is None else s.ctypes.data_as(C.c_void_p),
+                                      self._addr(v), self._addr(z)))
+
+    def loss_backward(self, g: MpnnGraph, v, x, segs=None) -> float:
+        ns, s = self._segs(segs)
+        loss = C.c_double()
+        _check(lib().nds_mpnn_loss_backward(self._h, C.byref(g), ns,
+                                            None if s is None else s.ctypes.data_as(C.c_void_p), self._addr(v),
+                                            self._addr(x), C.byref(loss)))
+        return loss.value
+
+    def adam_step(self, lr: float, step: int, beta1=0.9, beta2=0.999, eps=1e-8):
+        _check(lib().nds_mpnn_adam_step(self._h, C.c_float(lr), C.c_float(beta1), C.c_float(beta2), C.c_float(eps),
+                                        int(step)))
+
+    def activations(self, layer: int, out):
+        _check(lib().nds_mpnn_activations(self._h, int(layer), self._addr(out)))
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.nds_mpnn_destroy(self._h)
+            self._h = None
+
+
+def solver_load_stage(solver: "Solver", params: np.ndarray):
+    a = np.ascontiguousarray(params, dtype=np.float32)
+    _check(lib().nds_solver_load_stage(solver._h, a.ctypes.data_as(C.c_void_p), MPNN_NPARAM))
+
+
+def solver_stage_graph(solver: "Solver", nbr, ew, dscale):
+    _check(lib().nds_solver_stage_graph(solver._h, Mpnn._addr(nbr), Mpnn._addr(ew), Mpnn._addr(dscale)))
+
+
+def solver_pressure_pair(solver: "Solver", rhs, x):
+    _check(lib().nds_solver_pressure_pair(solver._h, Mpnn._addr(rhs), Mpnn._addr(x)))
+
+
+def solver_stage_counts(solver: "Solver"):
+    a, f = C.c_longlong(), C.c_longlong()
+    _check(lib().nds_solver_stage_counts(solver._h, C.byref(a), C.byref(f)))
+    return a.value, f.value
