@@ -1,37 +1,38 @@
 #!/usr/bin/env python3
 """Benchmark of the steady SIMPLE hot path on one B200 (one process per GPU).
 
-Workload (named by the benchmark's metric): the ~1M-tet straight pipe,
-O-grid 24 rings x 72 sectors (+ an 18x18 square core) x 100 slabs, 6 tets per
-quad and slab = 1,231,200 tets, seed-1 jitter of +-5 % local spacing, Re = 100,
-alpha_u 0.7, alpha_p 0.3, pressure PCG rtol 1e-6 with the smoothed-aggregation
-AMG + Chebyshev(2) V-cycle.  Precision: amg_fp32 (FP64 state, momentum,
-operator and Krylov method; FP32 V-cycle) by default, --precision fp64 for the
-plain path.
+Workload (the benchmark metric's): the ~1M-tet straight pipe, O-grid 24 rings
+x 72 sectors (+ an 18x18 square core) x 100 slabs, 6 tets per quad and slab =
+1,231,200 tets, seed-1 jitter of +-5 % local spacing, Re = 100, alpha_u 0.7,
+alpha_p 0.3, pressure rtol 1e-6 with the smoothed-aggregation AMG +
+Chebyshev(2) V-cycle, converged when relCont <= 1e-6 and the pre-sweep
+momentum audit <= 1e-6 (4193 SIMPLE iterations).
 
-Metric: seconds to steady state (relCont <= 1e-6 and the pre-sweep momentum
-audit <= 1e-6).  A complete solve takes 4193 SIMPLE iterations and 75k
-pressure PCG iterations, so a benchmark "step" is one SIMPLE outer iteration
-(assembly, momentum sweep, continuity, fine Schur refresh, AMG-PCG pressure
-solve, pressure update) and the timed steps calibrate
+Metric: seconds to steady state.  ``value`` is a measured complete solve of
+the fast configuration (FAST below: FP64 state, momentum and outer residual;
+FP64 defect correction around FP32 inner Krylov solves with the FP32 V-cycle;
+Galerkin initial guess over earlier pressure corrections), device-timed (the
+sum of the per-iteration CUDA-event times of the SIMPLE loop) with the
+problem already on the device.  The same solve runs through the public C ABI
+from host arrays: ``e2e`` is its wall time from the host mesh arrays
+(nds_mesh_from_arrays) through host setup, upload, the solve and the
+read-back of the fields (nds_get_fields).  Then the plain FP64 path solves
+the same problem (untimed) and the line states the relative L2 error of u,
+v, w and p of the fast solve against it.
 
-    value = N_outer x t_outer + N_pcg x t_pcg
-
-where t_outer is the mean device time of a step outside its PCG iterations,
-t_pcg the device time per PCG iteration (pressure-solve time / iterations
-over the timed steps), and N_outer, N_pcg the outer and PCG iteration counts
-of a complete solve of this exact configuration by this solver (the CPU
-oracle follows the same iteration history, see tests/), recorded in
-profiles/steady_state_pipe1m.md beside the measured complete-solve times.
-The per-iteration working set (fine operator ~1 GB) is larger than the 126 MB
+Steps: W warm-up and K timed SIMPLE iterations of the fast configuration on
+a separate solver give ``ms_per_step`` (barrier + synchronize around the K
+steps, max over ranks); a profiled pass of further iterations (per-kernel
+CUDA events, launch-by-launch loops) times the roofline kernel live.  The
+per-iteration working set (fine operator ~1 GB) is larger than the 126 MB
 L2, so no flush is inserted.
 
 Modes:
   python bench.py [--gpus N --steps K --warmup W]     this package (CUDA path)
   python bench.py --impl reference [...]                the CPU restatement of
-      the reference's SIMPLE loop (oracle/, FP64, all host threads), same
-      metric, workload and projection, each step one SIMPLE iteration
-      (bounded sample).
+      the reference's FP64 SIMPLE loop (oracle/, all host threads), same
+      metric and workload, each step one SIMPLE iteration (bounded sample),
+      projected to steady state with the FP64 iteration counts.
 """
 from __future__ import annotations
 
@@ -53,19 +54,22 @@ sys.path.insert(0, str(ROOT))
 METRIC = "s to steady state (resid 1e-6): FP32+learned vs plain FP64 AMG-FGMRES, 1 B200"
 WORKLOAD = "pipe1m"
 OPTIONS = dict(re=100.0, alpha_u=0.7, alpha_p=0.3, p_rtol=1e-6, p_max=400, run_mode="converge", simple_tol=1e-6,
-               max_outer=100000, amg_hierarchy="sa", amg_smoother="cheb2", pressure_solver="pcg")
-# Complete solves of OPTIONS on WORKLOAD to relCont <= 1e-6 plus the momentum
-# audit (profiles/steady_state_pipe1m.md): outer and total PCG iterations.
-STEADY_STATE = {"fp64": {"outer": 4193, "pcg": 75316}, "amg_fp32": {"outer": 4193, "pcg": 75402}}
-STEADY_STATE_SOURCE = "profiles/steady_state_pipe1m.md"
-PRECISION_NOTE = {"fp64": "FP64 throughout (the reference's FP64 build)",
-                  "amg_fp32": "FP64 state, momentum, fine operator and PCG; FP32 AMG V-cycle"}
+               max_outer=6000, amg_hierarchy="sa", amg_smoother="cheb2", pressure_solver="pcg")
+# the fast configuration of the metric
+FAST = dict(precision="mixed", p_krylov="pcg", p_guess=4)
+FAST_NOTE = ("mixed: FP64 state, momentum, continuity and outer pressure residual; FP64 defect correction around "
+             "FP32 inner PCG (FP32 operator copy, FP32 SA+cheb2 V-cycle, FP64 reductions), inner rtol 1e-3; "
+             "Galerkin initial guess over the last 4 pressure corrections; learned stage: off (see DESIGN)")
+# Complete FP64 solves of OPTIONS on WORKLOAD (tests/golden/cfg_pipe1m_re100_steady.npz,
+# the reference's own run): outer and total PCG iterations, for the CPU projection.
+STEADY_STATE_FP64 = {"outer": 4193, "pcg": 75316}
 
 
-def project(outer_ms, pcg_ms, pcg_its, prec):
-    """Seconds to steady state from per-step times outside PCG (outer_ms),
-    per-step PCG times (pcg_ms) and per-step PCG iteration counts."""
-    ss = STEADY_STATE[prec]
+def project_fp64(outer_ms, pcg_ms, pcg_its):
+    """Seconds to steady state of the FP64 loop from per-step times outside
+    the pressure iterations (outer_ms), per-step pressure times (pcg_ms) and
+    per-step pressure iteration counts (the CPU baseline's sample)."""
+    ss = STEADY_STATE_FP64
     t_outer = float(np.mean(outer_ms))
     t_pcg = float(np.sum(pcg_ms)) / max(int(np.sum(pcg_its)), 1)
     return (ss["outer"] * t_outer + ss["pcg"] * t_pcg) / 1e3, t_outer, t_pcg
@@ -79,11 +83,12 @@ def _peaks():
     return 6650.0, "fallback"
 
 
-def _traffic():
+def _traffic(key):
+    """DRAM bytes of one launch from the committed ncu summary (scaled to the
+    benchmark workload there), or None."""
     p = ROOT / "profiles" / "fine_spmv_traffic.json"
     if p.exists():
-        d = json.loads(p.read_text())
-        return d.get("bytes_per_launch_pipe1m_fp64")
+        return json.loads(p.read_text()).get(key)
     return None
 
 
@@ -161,7 +166,8 @@ def _barrier_max(x: float, ws: int, device: int) -> float:
 
 
 def fine_spmv_bytes(problem, s: int) -> float:
-    """Compulsory bytes of one fine Schur SpMV: values + columns + row offsets + x + y."""
+    """Compulsory bytes of one fine Schur SpMV in CSR terms: values (s B) and
+    column indices (4 B) of every entry, row offsets, x and y once."""
     row = problem.array("fine.row")
     n = len(row) - 1
     nnz = int(row[-1])
@@ -183,6 +189,10 @@ def sell_format_bytes(problem, s: int) -> float:
     return padded * (s + 2) + 8 * ns + 2 * s * n
 
 
+def _rel(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
 def run_nodals(args):
     from nodals_b200 import meshgen
     from nodals_b200 import native as N
@@ -191,135 +201,131 @@ def run_nodals(args):
         import torch
         import torch.distributed as dist
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=600))
-    prec = args.precision
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=900))
     tm = meshgen.named(WORKLOAD)
-    mesh = N.Mesh.from_tetmesh(tm)
-    t0 = time.perf_counter()
-    P = N.Problem(mesh, precision=prec, device=local, **OPTIONS)
-    setup_s = time.perf_counter() - t0
+    fast = dict(OPTIONS, **FAST, device=local)
+    stage = None
+    if fast.get("learned"):
+        from nodals_b200.stage import load_params
+        stage = load_params()
+
+    # --- per-iteration timing (warm-up, K timed steps, profiled steps) -------
+    P = N.Problem(N.Mesh.from_tetmesh(tm), **fast)
     S = N.Solver(P)
+    if stage is not None:
+        N.solver_load_stage(S, stage)
     for _ in range(args.warmup):
         S.step()
     l0 = N.launch_count()
     _barrier_max(0.0, ws, local)
     with Clocks(local) as clk:
-        dev_ms, outer_ms, pcg_ms, pcg_its = [], [], [], []
-        w0 = time.perf_counter()
+        dev_ms, p_its = [], []
         for _ in range(args.steps):
             r = S.step()
-            total = r.ms_assembly + r.ms_momentum + r.ms_continuity + r.ms_pressure + r.ms_update
-            solve = r.ms_pressure - r.ms_refresh
-            dev_ms.append(total)
-            outer_ms.append(total - solve)
-            pcg_ms.append(solve)
-            pcg_its.append(r.p_its)
-        wall = time.perf_counter() - w0
-    launches = N.launch_count() - l0
-    # Per-kernel CUDA events need the launch-by-launch path of the Krylov
-    # loop, so the roofline kernel is timed in a profiled pass of further
-    # steps of the same solve right after the timed region.
-    S.profile(True)
-    for _ in range(args.profile_steps):
-        S.step()
-    prof = S.profile_read()
-    S.profile(False)
-    mean_ms = float(np.mean(dev_ms))
-    value, t_outer, t_pcg = project(outer_ms, pcg_ms, pcg_its, prec)
-    if WORKLOAD != "pipe1m":
-        value = 0.0  # the steady-state counts belong to pipe1m; smaller pipes serve profiling only
-    value = _barrier_max(value, ws, local)
-    mean_ms = _barrier_max(mean_ms, ws, local)
-    calls, tot = prof["fine_spmv"]
+            dev_ms.append(r.ms_assembly + r.ms_momentum + r.ms_continuity + r.ms_pressure + r.ms_update)
+            p_its.append(r.p_its)
+        step_launches = N.launch_count() - l0
+        mean_ms = _barrier_max(float(np.mean(dev_ms)), ws, local)
+        # profiled pass: per-kernel CUDA events need the launch-by-launch loops
+        S.profile(True)
+        for _ in range(args.profile_steps):
+            S.step()
+        prof = S.profile_read()
+        S.profile(False)
+        counts = P.counts()
+        del S, P
+
+        # --- the metric: a complete solve through the C ABI from host arrays --
+        _barrier_max(0.0, ws, local)
+        l1 = N.launch_count()
+        w0 = time.perf_counter()
+        mesh = N.Mesh.from_tetmesh(tm)
+        P = N.Problem(mesh, **fast)
+        S = N.Solver(P)
+        if stage is not None:
+            N.solver_load_stage(S, stage)
+        setup_s = time.perf_counter() - w0
+        rep = S.solve()
+        fields = S.fields()
+        e2e_s = time.perf_counter() - w0
+        solve_launches = N.launch_count() - l1
+    value = _barrier_max(rep.loop_ms / 1e3, ws, local)
+    e2e_s = _barrier_max(e2e_s, ws, local)
+    if not rep.converged:
+        raise RuntimeError(f"the fast solve did not converge ({rep.outer_its} iterations)")
+    del S
+
+    # --- roofline: the FP32 fine-level SELL SpMV (V-cycle and inner Krylov) --
     roof = None
-    if args.profile_steps > 0:
-        if calls == 0:
-            raise RuntimeError("no fine SpMV launch was timed in the profiled pass")
-        avg_launch_ms = tot / calls
-        alg = fine_spmv_bytes(P, 8)
-        fmt = sell_format_bytes(P, 8)
+    calls, tot = prof["fine_spmv_amg"]
+    if args.profile_steps > 0 and calls > 0:
+        avg_ms = tot / calls
+        alg = fine_spmv_bytes(P, 4)
+        fmt = sell_format_bytes(P, 4)
         peak, peak_kind = _peaks()
-        achieved = alg / (avg_launch_ms * 1e-3) / 1e9
+        achieved = alg / (avg_ms * 1e-3) / 1e9
+        c64, t64 = prof["fine_spmv"]
         roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                "frac": round(achieved / peak, 4), "traffic": _traffic(), "peak_kind": peak_kind,
-                "kernel": "fine Schur SpMV of the PCG step, q = A p with p.q (SELL-32x4, FP64, sell_spmv<double,3>)",
+                "frac": round(achieved / peak, 4), "traffic": _traffic("bytes_per_launch_pipe1m_fp32"),
+                "peak_kind": peak_kind,
+                "kernel": "fine Schur SELL-32x4 SpMV in FP32 (sell_spmv<float,*>): V-cycle fine-level smoothing "
+                          "and residual steps and the inner Krylov A p",
                 "algorithmic_bytes_per_launch": int(alg),
-                "algorithmic_bytes_rule": "nnz*(8+4) + 4(n+1) + 2*8*n (CSR index 4 B, value 8 B, x and y once)",
+                "algorithmic_bytes_rule": "nnz*(4+4) + 4(n+1) + 2*4*n (CSR index 4 B, value 4 B, x and y once)",
                 "format_bytes_per_launch": int(fmt),
-                "format_frac": round(fmt / (avg_launch_ms * 1e-3) / 1e9 / peak, 4),
-                "avg_launch_ms": round(avg_launch_ms, 5), "launches": calls,
-                "timed_in": f"profiled pass of {args.profile_steps} steps after the timed region"}
+                "format_frac": round(fmt / (avg_ms * 1e-3) / 1e9 / peak, 4),
+                "avg_launch_ms": round(avg_ms, 5), "launches": calls,
+                "timed_in": f"profiled pass of {args.profile_steps} steps after the timed steps",
+                "fp64_defect_spmv": None if c64 == 0 else {
+                    "avg_launch_ms": round(t64 / c64, 5), "launches": c64,
+                    "achieved": round(fine_spmv_bytes(P, 8) / (t64 / c64 * 1e-3) / 1e9, 1)}}
 
-    # e2e: the public C ABI from host arrays: mesh -> setup -> device upload,
-    # then per step (nds_simple_step_io) H2D of the state (u, p) from pinned
-    # host memory, one SIMPLE iteration, D2H of the new state into the same
-    # pinned arrays (the velocity read-back runs beside the pressure solve).
-    # Projected like value, with the copies counted in the per-step part.
-    e2e = None
-    if args.e2e:
-        import torch
-        torch.cuda.set_device(local)
-        del S
-        t0 = time.perf_counter()
-        mesh2 = N.Mesh.from_tetmesh(tm)
-        P2 = N.Problem(mesh2, precision=prec, device=local, **OPTIONS)
-        S2 = N.Solver(P2)
-        fixed_s = time.perf_counter() - t0
-        c = P2.counts()
-        hu = [torch.zeros(c["nv"], dtype=torch.float64).pin_memory() for _ in range(3)]
-        hp = torch.zeros(c["nc"], dtype=torch.float64).pin_memory()
-        ptrs = [x.data_ptr() for x in hu] + [hp.data_ptr()]
-        import ctypes as C
-        L = N.lib()
-
-        def e2e_step():
-            r = N.IterReport()
-            N._check(L.nds_simple_step_io(S2._h, *[C.c_void_p(p) for p in ptrs], *[C.c_void_p(p) for p in ptrs],
-                                          C.byref(r)))
-            return r
-        for _ in range(args.warmup):
-            e2e_step()
-        e_outer, e_pcg, e_its = [], [], []
-        for _ in range(args.steps):
-            w = time.perf_counter()
-            r = e2e_step()
-            step_ms = (time.perf_counter() - w) * 1e3
-            solve = r.ms_pressure - r.ms_refresh
-            e_outer.append(step_ms - solve)
-            e_pcg.append(solve)
-            e_its.append(r.p_its)
-        ev, _, _ = project(e_outer, e_pcg, e_its, prec)
-        ev = _barrier_max(fixed_s + ev, ws, local)
-        bytes_state = 8 * (3 * c["nv"] + c["nc"])
-        e2e = {"value": round(ev, 3), "unit": "s", "h2d_bytes_per_step": bytes_state,
-               "d2h_bytes_per_step": bytes_state, "fixed_setup_s": round(fixed_s, 3),
-               "outer_ms": round(float(np.mean(e_outer)), 4)}
-        P = P2
+    # --- field error against the plain FP64 path (untimed) -------------------
+    errors = None
+    if args.fp64_check:
+        P64 = N.Problem(mesh, **dict(OPTIONS, precision="fp64", device=local))
+        S64 = N.Solver(P64)
+        r64 = S64.solve()
+        f64 = S64.fields()
+        errors = {"u": _rel(fields[0], f64[0]), "v": _rel(fields[1], f64[1]), "w": _rel(fields[2], f64[2]),
+                  "p": _rel(fields[3], f64[3]), "fp64_outer_its": r64.outer_its,
+                  "fp64_loop_s": round(r64.loop_ms / 1e3, 3),
+                  "speedup_vs_fp64_loop": round(r64.loop_ms / rep.loop_ms, 3)}
+        del S64, P64
 
     cpu = None
     if rank == 0 and ws == 1 and args.cpu_baseline:
-        cpu = cpu_baseline(P)
+        cpu = cpu_baseline(N.Problem(N.Mesh.from_tetmesh(tm), **dict(OPTIONS, precision="fp64")))
     if rank == 0:
-        ss = STEADY_STATE[prec]
+        nbytes_in = tm.points.nbytes + tm.tets.astype(np.int32).nbytes + tm.bfaces.astype(np.int32).nbytes \
+            + tm.btag.astype(np.int32).nbytes
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(mean_ms, 4), "higher_is_better": False, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64" if prec == "fp64" else "f64/f32",
-            "data": "synthetic (seeded pipe mesh)",
-            "config": {"workload": f"{WORKLOAD}: straight pipe R=0.5 L=10, 1,231,200 tets (24x72 O-grid + 18x18 core, "
-                                   f"100 slabs), Re=100, alpha_u=0.7, alpha_p=0.3, SA+cheb2 PCG rtol 1e-6",
-                       "precision": f"{prec}: {PRECISION_NOTE[prec]}",
-                       "cells": int(P.counts()["nc"]), "velocity_dofs": int(P.counts()["nv"]),
-                       "step": "one SIMPLE outer iteration of the steady-state solve",
-                       "projection": "N_outer x t_outer + N_pcg x t_pcg",
-                       "steady_state_outer_iterations": ss["outer"], "steady_state_pcg_iterations": ss["pcg"],
-                       "t_outer_ms": round(t_outer, 4), "t_pcg_ms": round(t_pcg, 5),
-                       "timed_pcg_iterations_per_step": round(float(np.mean(pcg_its)), 2),
-                       "steady_state_source": STEADY_STATE_SOURCE,
+            "vs_baseline": None, "dtype": "f64/f32", "data": "synthetic (seeded pipe mesh)",
+            "config": {"workload": f"{WORKLOAD}: straight pipe R=0.5 L=10, 1,231,200 tets (24x72 O-grid + 18x18 "
+                                   f"core, 100 slabs), Re=100, alpha_u=0.7, alpha_p=0.3, SA+cheb2 V-cycle, "
+                                   f"pressure rtol 1e-6, steady state at relCont and momentum audit <= 1e-6",
+                       "precision": FAST_NOTE, "krylov": FAST.get("p_krylov", "pcg"),
+                       "learned_stage": bool(FAST.get("learned")),
+                       "cells": int(counts["nc"]), "velocity_dofs": int(counts["nv"]),
+                       "value_is": "device time of one complete solve (sum of the per-iteration CUDA-event times)",
+                       "steady_state_outer_iterations": int(rep.outer_its),
+                       "avg_pressure_iterations": round(rep.avg_pressure_its, 3),
+                       "pressure_s": round(rep.pressure_ms / 1e3, 3),
+                       "step": "one SIMPLE outer iteration (ms_per_step: K timed iterations after W warm-up)",
+                       "timed_steps_pressure_iterations": round(float(np.mean(p_its)), 2),
                        "l2": "working set per step > 126 MB L2 (fine operator ~1 GB); no flush",
-                       "parallelism": "replicas" if ws > 1 else "single GPU", "host_setup_s": round(setup_s, 3),
-                       "wall_ms_per_step": round(wall / args.steps * 1e3, 4)},
-            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
+                       "parallelism": "replicas" if ws > 1 else "single GPU", "host_setup_s": round(setup_s, 3)},
+            "field_rel_l2_vs_fp64": errors,
+            "roofline": roof, "cpu_baseline": cpu,
+            "e2e": {"value": round(e2e_s, 3), "unit": "s", "h2d_bytes_per_step": int(nbytes_in),
+                    "d2h_bytes_per_step": int(8 * (3 * counts["nv"] + counts["nc"])),
+                    "what": "wall time of mesh host arrays -> host setup -> device upload -> complete solve -> "
+                            "fields read back to host, through the C ABI (ctypes); h2d counts the mesh arrays "
+                            "passed in (the library uploads its setup from them), d2h the fields"},
+            "gpu_launches": int(step_launches),
+            "gpu_launches_complete_solve": int(solve_launches),
             "clocks": clk.summary(),
             "kernel_ms_profiled_pass": {k: round(v[1], 3) for k, v in prof.items()},
         }
@@ -344,7 +350,7 @@ def _oracle_sample(P, threads, warmup, max_steps, max_seconds):
         outer.append(r.ms_total - r.ms_pressure)
         pcg.append(r.ms_pressure)
         its.append(r.p_its)
-    value, t_outer, t_pcg = project(outer, pcg, its, "fp64")
+    value, t_outer, t_pcg = project_fp64(outer, pcg, its)
     sample = (f"{len(tot)} SIMPLE iterations of the {WORKLOAD} solve after {warmup} warm-up "
               f"({np.mean(tot) / 1e3:.3f} s each, {np.mean(its):.1f} PCG iterations each), projected as "
               f"N_outer x t_outer + N_pcg x t_pcg with t_outer {t_outer:.1f} ms, t_pcg {t_pcg:.1f} ms")
@@ -370,7 +376,7 @@ def run_reference(args):
     warm = min(args.warmup, 1)
     value, tot, sample = _oracle_sample(P, threads, warm, args.steps, args.ref_seconds)
     value = round(value, 3) if WORKLOAD == "pipe1m" else 0.0
-    ss = STEADY_STATE["fp64"]
+    ss = STEADY_STATE_FP64
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "s", "n_gpus": ws,
             "steps": len(tot), "warmup": warm, "ms_per_step": round(float(np.mean(tot)), 3),
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -389,10 +395,10 @@ def main():
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="nodals", choices=["nodals", "reference"])
-    ap.add_argument("--precision", default="amg_fp32", choices=["amg_fp32", "fp64"])
     ap.add_argument("--workload", default=WORKLOAD, choices=["pipe1m", "pipe400k", "pipe40k"],
                     help="pipe1m is the benchmark; the smaller pipes serve kernel profiling only")
-    ap.add_argument("--no-e2e", dest="e2e", action="store_false")
+    ap.add_argument("--no-fp64-check", dest="fp64_check", action="store_false",
+                    help="skip the FP64 solve that gives the field errors")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--ref-seconds", type=float, default=60.0)
     ap.add_argument("--profile-steps", type=int, default=3, help="profiled steps after the timed region")

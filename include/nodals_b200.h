@@ -105,6 +105,14 @@ typedef struct nds_options {
   /* 1: pipe centre and radius from the inlet patch instead of the bounding
    * box (bent pipes); 0: the reference's bounding-box rule (g4_host.hpp:37-49) */
   int geom_from_inlet;
+  /* products A y of the guess: 0 kept from the solve that made each y
+   * (w = b - r, free, from an operator up to p_guess iterations old), 1
+   * recomputed with the current FP32 operator copy every solve */
+  int p_guess_fresh;
+  /* 1: the V-cycle's fine-level operator in FP16 (values scaled by a power of
+   * two into FP16 range, FP32 arithmetic); precision mixed only -- the
+   * inner Krylov product keeps the FP32 copy, the outer residual FP64 */
+  int amg_half;
 } nds_options;
 
 /* One SIMPLE outer iteration (h8_main_base.cu:2046-2119). */

@@ -111,6 +111,8 @@ void nds_options_default(nds_options* o) {
   o->p_guess = 0;
   o->learned = 0;
   o->geom_from_inlet = 0;
+  o->p_guess_fresh = 0;
+  o->amg_half = 0;
 }
 
 int nds_mesh_read_polymesh(const char* dir, nds_mesh** out) {
@@ -766,6 +768,7 @@ bool validate_options(const nds_options& o, std::string& why) {
     return bad("the learned stage needs precision mixed and p_krylov fgmres (a varying preconditioner)");
   if (o.precision == NDS_MIXED && o.pressure_solver != NDS_P_PCG)
     return bad("precision mixed runs its own Krylov solve: pressure_solver must be pcg (the default)");
+  if (o.amg_half && o.precision != NDS_MIXED) return bad("amg_half needs precision mixed");
   if (o.precision == NDS_MIXED && o.amg_smoother == NDS_SM_MCGS)
     return bad("precision mixed supports the polynomial smoothers (cheb2, jacobi, l1jacobi)");
   if (o.supg != 0 && o.supg != 1) return bad("H8 supg must be 0 or 1");

@@ -6,9 +6,11 @@
 // (double for the FP64 path, float for FP32); reductions and Krylov scalars
 // are double in both, as in the reference (gpu/serial_cuda/precision.hpp:7-36).
 #pragma once
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <type_traits>
 
 #include "common.cuh"
 
@@ -332,9 +334,9 @@ __global__ void __launch_bounds__(kBlock) mom_assemble(MomArgs<T> g) {
 }
 
 // One multicolour Gauss-Seidel colour pass on the shared momentum matrix,
-// three right-hand sides (g5e_fp32_kernels.cuh:106-116).  8 lanes per row.
-// rows: the colour's rows; span: their (begin, end) in the CSR, in the same
-// order, so the row's entries and its own data load in parallel.
+// three right-hand sides (g5e_fp32_kernels.cuh:106-116).  rows: the colour's
+// rows; span: their (begin, end) in the CSR, in the same order, so the row's
+// entries and its own data load in parallel.
 template <class T>
 __global__ void __launch_bounds__(kBlock) mom_gs_color(int count, const int32_t* __restrict__ rows,
                                                        const int2* __restrict__ span, const int32_t* __restrict__ ci,
@@ -342,25 +344,42 @@ __global__ void __launch_bounds__(kBlock) mom_gs_color(int count, const int32_t*
                                                        const T* __restrict__ b0, const T* __restrict__ b1,
                                                        const T* __restrict__ b2, T* __restrict__ x0, T* __restrict__ x1,
                                                        T* __restrict__ x2, T omega) {
-  const int lane8 = threadIdx.x & 7;
-  const int q = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
+  // one thread per row of the colour; the off-diagonal sum runs over the
+  // row in CSR order (the reference's and the oracle's order), with the
+  // loads of four entries and their gathers issued before the sums
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= count) return;
-  const unsigned gmask = group8_mask();
   const int i = rows[q];
   const int2 sp = span[q];
-  T d = 0, c0 = 0, c1 = 0, c2 = 0, y0 = 0, y1 = 0, y2 = 0;
   const size_t vi = kVel * (size_t)i;
-  if (lane8 == 0) {
-    d = diag[i];
-    c0 = b0[i];
-    c1 = b1[i];
-    c2 = b2[i];
-    y0 = x0[vi];
-    y1 = x1[vi];
-    y2 = x2[vi];
-  }
+  const T d = diag[i], c0 = b0[i], c1 = b1[i], c2 = b2[i];
+  const T y0 = x0[vi], y1 = x1[vi], y2 = x2[vi];
   T s0 = 0, s1 = 0, s2 = 0;
-  for (int k = sp.x + lane8; k < sp.y; k += 8) {
+  int k = sp.x;
+  for (; k + 4 <= sp.y; k += 4) {
+    int j[4];
+    T a[4], u0[4], u1[4], u2[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      j[e] = ci[k + e];
+      a[e] = av[k + e];
+    }
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const size_t vj = kVel * (size_t)j[e];
+      u0[e] = x0[vj];
+      u1[e] = x1[vj];
+      u2[e] = x2[vj];
+    }
+#pragma unroll
+    for (int e = 0; e < 4; ++e)
+      if (j[e] != i) {
+        s0 += a[e] * u0[e];
+        s1 += a[e] * u1[e];
+        s2 += a[e] * u2[e];
+      }
+  }
+  for (; k < sp.y; ++k) {
     const int j = ci[k];
     if (j == i) continue;
     const T a = av[k];
@@ -369,15 +388,10 @@ __global__ void __launch_bounds__(kBlock) mom_gs_color(int count, const int32_t*
     s1 += a * x1[vj];
     s2 += a * x2[vj];
   }
-  s0 = group_sum<8>(s0, gmask);
-  s1 = group_sum<8>(s1, gmask);
-  s2 = group_sum<8>(s2, gmask);
-  if (lane8 == 0) {
-    const T iv = T(1) / d;
-    x0[vi] = (T(1) - omega) * y0 + omega * ((c0 - s0) * iv);
-    x1[vi] = (T(1) - omega) * y1 + omega * ((c1 - s1) * iv);
-    x2[vi] = (T(1) - omega) * y2 + omega * ((c2 - s2) * iv);
-  }
+  const T iv = T(1) / d;
+  x0[vi] = (T(1) - omega) * y0 + omega * ((c0 - s0) * iv);
+  x1[vi] = (T(1) - omega) * y1 + omega * ((c1 - s1) * iv);
+  x2[vi] = (T(1) - omega) * y2 + omega * ((c2 - s2) * iv);
 }
 
 // ||b_d||^2 and ||b_d - A u_d||^2 (g5e_fp32_kernels.cuh:117-126); 6 partials per block.
@@ -805,6 +819,22 @@ __device__ __forceinline__ void sell_val4<double>(const double* __restrict__ v, 
   a[2] = q.x;
   a[3] = q.y;
 }
+// FP16 operator copy (values scaled by a power of two into FP16 range): four
+// values of one 8-byte load, widened
+__device__ __forceinline__ void sell_val4h(const __half* __restrict__ v, int o, float a[4]) {
+  const uint2 q = *reinterpret_cast<const uint2*>(v + o);
+  const float2 lo = __half22float2(*reinterpret_cast<const __half2*>(&q.x));
+  const float2 hi = __half22float2(*reinterpret_cast<const __half2*>(&q.y));
+  a[0] = lo.x;
+  a[1] = lo.y;
+  a[2] = hi.x;
+  a[3] = hi.y;
+}
+template <class T, class MT>
+__device__ __forceinline__ void sell_vals4(const MT* __restrict__ v, int o, T a[4]) {
+  if constexpr (std::is_same<MT, __half>::value) sell_val4h(v, o, a);
+  else sell_val4<T>(v, o, a);
+}
 template <bool D16>
 __device__ __forceinline__ int sell_col(const Sell& A, int o, int i) {
   if (D16) return i + (int)A.dcol[o];
@@ -817,8 +847,8 @@ enum SellMode { SELL_Y = 0, SELL_RESID = 1, SELL_SMOOTH = 2, SELL_DOT = 3 };
 // of columns, then the 8 x gathers), even entries into s0 and odd ones into
 // s1; the last w mod 8 entries (and the zero padding) go to s0 in order.
 // Fixed order -> deterministic.
-template <class T, bool D16>
-__device__ __forceinline__ T sell_row(const Sell& A, const T* __restrict__ v, const T* __restrict__ x, int i) {
+template <class T, bool D16, class MT = T>
+__device__ __forceinline__ T sell_row(const Sell& A, const MT* __restrict__ v, const T* __restrict__ x, int i) {
   const int s = i >> 5, lane = i & 31;
   const int b = A.base[s];
   const int w = A.width[s];
@@ -831,8 +861,8 @@ __device__ __forceinline__ T sell_row(const Sell& A, const T* __restrict__ v, co
     const int o0 = sell_offset(b, lane, k), o1 = o0 + 128;
     sell_col4<D16>(A, o0, i, j);
     sell_col4<D16>(A, o1, i, j + 4);
-    sell_val4<T>(v, o0, a);
-    sell_val4<T>(v, o1, a + 4);
+    sell_vals4<T, MT>(v, o0, a);
+    sell_vals4<T, MT>(v, o1, a + 4);
     T xv[8];
 #pragma unroll
     for (int u = 0; u < 8; ++u) xv[u] = x[j[u]];
@@ -847,7 +877,7 @@ __device__ __forceinline__ T sell_row(const Sell& A, const T* __restrict__ v, co
     T a[4];
     const int o = sell_offset(b, lane, k);
     sell_col4<D16>(A, o, i, j);
-    sell_val4<T>(v, o, a);
+    sell_vals4<T, MT>(v, o, a);
 #pragma unroll
     for (int u = 0; u < 4; ++u) s0 += a[u] * x[j[u]];
   }
@@ -858,14 +888,18 @@ __device__ __forceinline__ T sell_row(const Sell& A, const T* __restrict__ v, co
 // MODE SELL_RESID:  y = b - A x (and y2 = y when y2 != null)
 // MODE SELL_SMOOTH: y = x + w (b - A x) / den
 // MODE SELL_DOT:    y = A x, partials of x.y (grid-stride; blockDim = kBlock)
-template <class T, int MODE, bool D16>
-__global__ void __launch_bounds__(kBlock, 8) sell_spmv(Sell A, const T* __restrict__ v, const T* __restrict__ x,
+// MT: the operator's value type (T, or __half for the FP16 copy whose values
+// are a s, with vinv = 1 / s: a power of two, so the product is exact)
+template <class T, int MODE, bool D16, class MT = T>
+__global__ void __launch_bounds__(kBlock, 8) sell_spmv(Sell A, const MT* __restrict__ v, const T* __restrict__ x,
                                                     const T* __restrict__ b, const T* __restrict__ den, T w,
-                                                    T* __restrict__ y, T* __restrict__ y2, double* __restrict__ part) {
+                                                    T* __restrict__ y, T* __restrict__ y2, double* __restrict__ part,
+                                                    T vinv = T(1)) {
   if (MODE == SELL_DOT) {
     double acc[1] = {0.0};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n; i += gridDim.x * blockDim.x) {
-      const T s = sell_row<T, D16>(A, v, x, i);
+      T s = sell_row<T, D16, MT>(A, v, x, i);
+      if constexpr (!std::is_same<MT, T>::value) s *= vinv;
       y[i] = s;
       acc[0] += (double)x[i] * (double)s;
     }
@@ -874,7 +908,8 @@ __global__ void __launch_bounds__(kBlock, 8) sell_spmv(Sell A, const T* __restri
   }
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= A.n) return;
-  const T s = sell_row<T, D16>(A, v, x, i);
+  T s = sell_row<T, D16, MT>(A, v, x, i);
+  if constexpr (!std::is_same<MT, T>::value) s *= vinv;
   if (MODE == SELL_Y) {
     y[i] = s;
   } else if (MODE == SELL_RESID) {
@@ -941,7 +976,8 @@ __global__ void __launch_bounds__(kRefreshBlock) sell_refresh(int nc, const int3
                                                               const int32_t* __restrict__ sbase,
                                                               const int32_t* __restrict__ swidth, T* __restrict__ val,
                                                               TA* __restrict__ valA, TA* __restrict__ diag,
-                                                              TA* __restrict__ l1) {
+                                                              TA* __restrict__ l1, __half* __restrict__ valH = nullptr,
+                                                              float hscale = 1.f) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* sv = reinterpret_cast<T*>(smem_raw);
   __shared__ T sR[32][8];
@@ -997,6 +1033,7 @@ __global__ void __launch_bounds__(kRefreshBlock) sell_refresh(int nc, const int3
     const T v = sv[(4 * (t >> 7) + (t & 3)) * 33 + ((t >> 2) & 31)];
     val[base + t] = v;
     if (valA) valA[base + t] = TA(v);
+    if (valH) valH[base + t] = __float2half_rn(fminf(fmaxf((float)v * hscale, -65504.f), 65504.f));
   }
 }
 

@@ -144,15 +144,21 @@ __global__ void scaled_input(int n, const float* __restrict__ v, const float* __
   if (i >= n) return;
   s[i] = v[i] * dscale[i] / sigma[seg_of(i, seg_off, nseg)];
 }
-// f_i = (s_i, sum_j e_ij s_j)
+// f_i = (s_i, sum_j e_ij s_j).  A neighbour index outside [-1, n) is an
+// error of the caller's graph: it sets err bit 2 and is skipped (the layer
+// kernels skip such entries too).
 __global__ void features(int n, const float* __restrict__ s, const int32_t* __restrict__ nbr,
-                         const float* __restrict__ ew, float2* __restrict__ f) {
+                         const float* __restrict__ ew, float2* __restrict__ f, int* __restrict__ err) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   float m = 0.f;
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
     const int j = nbr[4 * (size_t)i + k];
+    if (j >= n || j < -1) {
+      atomicOr(err, 2);
+      continue;
+    }
     if (j >= 0) m += ew[4 * (size_t)i + k] * s[j];
   }
   f[i] = make_float2(s[i], m);
@@ -199,7 +205,7 @@ __device__ void build_row(const LayerIn& in, int row, uint8_t* __restrict__ X, i
 #pragma unroll 1
     for (int k = 0; k < 4; ++k) {
       const int j = in.nbr[4 * (size_t)row + k];
-      if (j < 0) continue;
+      if (j < 0 || j >= in.n) continue;
       const float w = in.ew[4 * (size_t)row + k];
       encoder_row<true>(in.f[j], s_we, s_be, h);
 #pragma unroll
@@ -212,7 +218,7 @@ __device__ void build_row(const LayerIn& in, int row, uint8_t* __restrict__ X, i
 #pragma unroll 1
     for (int k = 0; k < 4; ++k) {
       const int j = in.nbr[4 * (size_t)row + k];
-      if (j < 0) continue;
+      if (j < 0 || j >= in.n) continue;
       const float w = in.ew[4 * (size_t)row + k];
       const uint4* hj = reinterpret_cast<const uint4*>(in.hin + (size_t)j * kH);
       uint4 u[8];
@@ -526,7 +532,7 @@ __global__ void scatter_bwd(int n, const int32_t* __restrict__ nbr, const float*
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
     const int j = nbr[4 * (size_t)i + k];
-    if (j < 0) continue;
+    if (j < 0 || j >= n) continue;
     const float w = ew[4 * (size_t)i + k];
     const float4 d = reinterpret_cast<const float4*>(dm + (size_t)j * kH)[c];
     s.x = fmaf(w, d.x, s.x);
@@ -756,6 +762,8 @@ struct MpnnImpl {
     int e = 0;
     NDS_CUDA(cudaMemcpyAsync(&e, err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     NDS_CUDA(cudaStreamSynchronize(st));
+    NDS_CUDA(cudaMemsetAsync(err.p, 0, sizeof(int), st));
+    if (e & 2) throw std::runtime_error("learned stage: a neighbour index of the graph is out of range");
     if (e) throw std::runtime_error("learned stage: a tensor-core wait ran out (error flag set)");
   }
   std::vector<int32_t> seg_host;  // segment offsets last uploaded to seg_dev
@@ -781,7 +789,7 @@ struct MpnnImpl {
     }
     mp::scaled_input<<<grid_for(g.n), kBlock, 0, st>>>(g.n, v, g.dscale, sigma.p, seg_dev.p, nseg, s.p);
     NDS_LAUNCH();
-    mp::features<<<grid_for(g.n), kBlock, 0, st>>>(g.n, s.p, g.nbr, g.ew, f.p);
+    mp::features<<<grid_for(g.n), kBlock, 0, st>>>(g.n, s.p, g.nbr, g.ew, f.p, err.p);
     NDS_LAUNCH();
   }
   mp::FwdArgs fwd_args(const nds_mpnn_graph& g, int layer, int nseg) {

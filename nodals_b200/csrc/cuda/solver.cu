@@ -7,6 +7,7 @@
 //   pressure_precond_power                 :613-668
 //   g5_gpu_spectrum_refresh                :873-906
 //   SIMPLE iteration                       :2046-2119
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -629,6 +630,20 @@ class Solver final : public ISolver {
     // setup-time state: fine CSR refreshed with the initial rAU
     tm.mark("levels_and_transfers");
     refresh_fine(rau_.p);
+    if (mixed_ && o_.amg_half) {
+      // FP16 copy: scale by a power of two that puts the largest setup-time
+      // diagonal at 2^11 (the diagonal dominates its row; 2^4 headroom below
+      // the FP16 maximum for later growth of rAU, values beyond saturate)
+      std::vector<TA> d((size_t)nc_);
+      NDS_CUDA(cudaMemcpyAsync(d.data(), fdiag_.p, sizeof(TA) * d.size(), cudaMemcpyDeviceToHost, st_));
+      NDS_CUDA(cudaStreamSynchronize(st_));
+      double dmax = 0.0;
+      for (TA v : d) dmax = std::max(dmax, std::abs((double)v));
+      if (!(dmax > 0.0) || !std::isfinite(dmax)) throw std::runtime_error("FP16 operator copy: no positive diagonal");
+      hscale_ = std::ldexp(1.0, (int)std::floor(std::log2(2048.0 / dmax)));
+      fvalH_.alloc(fval_.n);
+      refresh_fine(rau_.p);
+    }
     if (P_.power_its > 0) {
       fine_lambda_ = power_fine(P_.power_its, o_.amg_lambda_safety);
       for (size_t l = 0; l + 1 < L_.size(); ++l) level_lambda_[l] = power_level(L_[l], P_.power_its, o_.amg_lambda_safety);
@@ -806,10 +821,23 @@ class Solver final : public ISolver {
     const int32_t* rp;
     const int32_t* ci;
     const V* v;
-    int cat;  // profiler category
+    int cat;                     // profiler category
+    const __half* vh = nullptr;  // FP16 copy of the values (SELL only), scaled by 1 / vinv
+    double vinv = 1.0;
   };
   template <int MODE, class V>
   void sell_launch(const OpView<V>& A, int grid, const V* x, const V* b, const V* den, double w, V* y, V* y2) {
+    if constexpr (std::is_same<V, float>::value) {
+      if (A.vh) {
+        if (A.s.dcol)
+          k::sell_spmv<V, MODE, true, __half><<<grid, kBlock, 0, st_>>>(A.s, A.vh, x, b, den, V(w), y, y2, part_.p,
+                                                                          V(A.vinv));
+        else
+          k::sell_spmv<V, MODE, false, __half><<<grid, kBlock, 0, st_>>>(A.s, A.vh, x, b, den, V(w), y, y2, part_.p,
+                                                                           V(A.vinv));
+        return;
+      }
+    }
     if (A.s.dcol)
       k::sell_spmv<V, MODE, true><<<grid, kBlock, 0, st_>>>(A.s, A.v, x, b, den, V(w), y, y2, part_.p);
     else
@@ -820,6 +848,15 @@ class Solver final : public ISolver {
   OpView<TA> fine_opA() const {
     if constexpr (kSame) return {nc_, true, sell_, nullptr, nullptr, fval_.p, P_FINE_AMG};
     else return {nc_, true, sell_, nullptr, nullptr, fvalA_.p, P_FINE_AMG};
+  }
+  // the fine operator of the V-cycle: the FP16 copy when amg_half is on
+  OpView<TA> fine_opV() const {
+    OpView<TA> A = fine_opA();
+    if (fvalH_.p) {
+      A.vh = fvalH_.p;
+      A.vinv = 1.0 / hscale_;
+    }
+    return A;
   }
   OpView<TA> level_op(const Level& A) const {
     return {A.n, false, k::Sell{}, A.row.p, A.col.p, A.val.p, P_COARSE_SPMV};
@@ -868,7 +905,7 @@ class Solver final : public ISolver {
     ProfScope ps(prof, s, P_REFRESH);
     k::sell_refresh<T, TA><<<(nc_ + 31) / 32, k::kRefreshBlock, refresh_smem_, s>>>(
         nc_, fcoff_.p, fcs_.p, fgeo_.p, ref_.p, rau, fdslot_.p, sbase_.p, swidth_.p, fval_.p,
-        kSame ? nullptr : fvalA_.p, fdiag_.p, fl1_.p);
+        kSame ? nullptr : fvalA_.p, fdiag_.p, fl1_.p, fvalH_.p, (float)hscale_);
     NDS_LAUNCH();
   }
   void fine_apply(const T* x, T* y) { op_spmv(fine_op(), x, y); }
@@ -949,11 +986,11 @@ class Solver final : public ISolver {
   void smooth_fine(const TA* b, TA* x, bool first_done = false) {
     const int sm = o_.amg_smoother;
     if (sm == NDS_SM_MCGS) {
-      mcgs(fine_opA(), fdiag_.p, b, x, fine_crows_, fine_coff_, o_.amg_mcgs_fine_sweeps);
+      mcgs(fine_opV(), fdiag_.p, b, x, fine_crows_, fine_coff_, o_.amg_mcgs_fine_sweeps);
       return;
     }
     const TA* den = sm == NDS_SM_L1JACOBI ? fl1_.p : fdiag_.p;
-    poly_smooth(fine_opA(), fdiag_.p, b, x, fpong_.p, fine_lambda_, sm == NDS_SM_CHEB2, den, o_.amg_jacobi_fine_sweeps,
+    poly_smooth(fine_opV(), fdiag_.p, b, x, fpong_.p, fine_lambda_, sm == NDS_SM_CHEB2, den, o_.amg_jacobi_fine_sweeps,
                 first_done);
   }
   void smooth_level(Level& A, const TA* b, TA* x, double lambda, bool first_done = false) {
@@ -1044,7 +1081,7 @@ class Solver final : public ISolver {
   // pre_done: the fine pre-smoother's diagonal step is already in place
   void amg_apply(const TA* b, TA* z, bool pre_done = false) {
     smooth_fine(b, z, pre_done);
-    op_resid(fine_opA(), z, b, fr_.p);
+    op_resid(fine_opV(), z, b, fr_.p);
     Level& C = L_[0];
     const bool fuse = fuse_pre(0);
     restrict_to(X_[0], fr_.p, C.b.p, fuse ? 0 : -1);
@@ -1052,7 +1089,7 @@ class Solver final : public ISolver {
     prolong(X_[0], C.x.p, z);
     const int sm = o_.amg_smoother;
     if (sm == NDS_SM_MCGS) {
-      op_resid(fine_opA(), z, b, fr_.p, frhs_.p);
+      op_resid(fine_opV(), z, b, fr_.p, frhs_.p);
       smooth_fine(frhs_.p, fcorr_.p);
       vaxpy(nc_, 1.0, fcorr_.p, z);
       return;
@@ -1062,8 +1099,8 @@ class Solver final : public ISolver {
     const bool cheb = sm == NDS_SM_CHEB2;
     const TA* den = sm == NDS_SM_L1JACOBI ? fl1_.p : fdiag_.p;
     const PolyPlan pl = poly_plan(fine_lambda_, cheb, fdiag_.p, den, o_.amg_jacobi_fine_sweeps);
-    op_resid(fine_opA(), z, b, frhs_.p, poly_first(pl, fcorr_.p, fpong_.p), pl.den0, pl.w0);
-    poly_smooth(fine_opA(), fdiag_.p, frhs_.p, fcorr_.p, fpong_.p, fine_lambda_, cheb, den, o_.amg_jacobi_fine_sweeps,
+    op_resid(fine_opV(), z, b, frhs_.p, poly_first(pl, fcorr_.p, fpong_.p), pl.den0, pl.w0);
+    poly_smooth(fine_opV(), fdiag_.p, frhs_.p, fcorr_.p, fpong_.p, fine_lambda_, cheb, den, o_.amg_jacobi_fine_sweeps,
                 true, z);
   }
 
@@ -1081,7 +1118,7 @@ class Solver final : public ISolver {
     double ray = 0.0;
     for (int it = 0; it < its; ++it) {
       k::div_sqrt<TA><<<grid_for(nc_), kBlock, 0, st_>>>(nc_, v, fdiag_.p, u);
-      op_spmv(fine_opA(), (const TA*)u, au);
+      op_spmv(fine_opV(), (const TA*)u, au);
       k::div_sqrt<TA><<<grid_for(nc_), kBlock, 0, st_>>>(nc_, au, fdiag_.p, w);
       NDS_LAUNCH();
       const double num = dot_fetch((const TA*)v, (const TA*)w, nc_, S_TMP),
@@ -1347,6 +1384,7 @@ class Solver final : public ISolver {
     if (o_.p_guess > 0) {
       gY_.alloc((size_t)o_.p_guess * n);
       gW_.alloc((size_t)o_.p_guess * n);
+      if (o_.p_guess_fresh) gYf_.alloc((size_t)o_.p_guess * n);
     }
   }
   // the preconditioner of the inner solves: z = M v (FP32).  With the
@@ -1470,8 +1508,11 @@ class Solver final : public ISolver {
       k::p_update_dev<float><<<grid_for(nc_), kBlock, 0, st_>>>(nc_, sc_.p + S_BETA, ctl_.p, zf_.p, pf_.p);
       NDS_LAUNCH();
       const int g = red_grid(nc_);
-      sell_launch<k::SELL_DOT, float>(fine_opA(), g, pf_.p, nullptr, nullptr, 0.0, qf_.p, nullptr);
-      NDS_LAUNCH();
+      {
+        ProfScope ps(prof, st_, P_FINE_AMG);
+        sell_launch<k::SELL_DOT, float>(fine_opA(), g, pf_.p, nullptr, nullptr, 0.0, qf_.p, nullptr);
+        NDS_LAUNCH();
+      }
       reduce_to<1>(g, S_PQ);
       k::pcg_alpha<<<1, 1, 0, st_>>>(sc_.p, flags_.p);
       NDS_LAUNCH();
@@ -1627,6 +1668,17 @@ class Solver final : public ISolver {
   double guess_k(const double* rhs) {
     constexpr int NG = K * (K + 1) / 2 + K;
     const int g = red_grid(nc_);
+    if constexpr (!kSame) {
+      if (o_.p_guess_fresh) {
+        // products with this iteration's operator (FP32 copy), widened to FP64
+        const size_t n = (size_t)nc_;
+        for (int a = 0; a < K; ++a) {
+          op_spmv(fine_opA(), (const float*)(gYf_.p + a * n), qf_.p);
+          k::cast_copy<float, double><<<grid_for(nc_), kBlock, 0, st_>>>(nc_, qf_.p, gW_.p + a * n);
+          NDS_LAUNCH();
+        }
+      }
+    }
     k::guess_dots<K><<<g, kBlock, 0, st_>>>(nc_, gY_.p, gW_.p, rhs, fgpart_.p);
     NDS_LAUNCH();
     k::reduce_partials<NG><<<1, kBlock, 0, st_>>>(fgpart_.p, g, sc_.p + S_GUESS);
@@ -1692,6 +1744,10 @@ class Solver final : public ISolver {
     const size_t o = (size_t)guess_head_ * nc_;
     k::guess_store<<<grid_for(nc_), kBlock, 0, st_>>>(nc_, x_.p, rhs, r_.p, gY_.p + o, gW_.p + o);
     NDS_LAUNCH();
+    if (gYf_.p) {
+      k::cast_copy<double, float><<<grid_for(nc_), kBlock, 0, st_>>>(nc_, x_.p, gYf_.p + o);
+      NDS_LAUNCH();
+    }
     guess_head_ = (guess_head_ + 1) % o_.p_guess;
     nguess_ = std::min(nguess_ + 1, o_.p_guess);
   }
@@ -1802,7 +1858,7 @@ class Solver final : public ISolver {
       const int s = color_off_[(size_t)c], n = color_off_[(size_t)c + 1] - s;
       if (!n) continue;
       ProfScope ps(prof, st_, P_GS);
-      k::mom_gs_color<T><<<grid_for((long long)n * 8), kBlock, 0, st_>>>(n, color_rows_.p + s, color_span_.p + s, mcol_.p, A_.p,
+      k::mom_gs_color<T><<<grid_for(n), kBlock, 0, st_>>>(n, color_rows_.p + s, color_span_.p + s, mcol_.p, A_.p,
                                                                        diag_.p, b_[0].p, b_[1].p, b_[2].p, uc(0),
                                                                        uc(1), uc(2), T(o_.mom_omega));
       NDS_LAUNCH();
@@ -2140,7 +2196,9 @@ class Solver final : public ISolver {
   bool mixed_ = false;
   int in_graph_ = 0;  // 1 while a loop body is being captured (its check kernel sets the graph condition)
   int fg_m_ = 0, nguess_ = 0, guess_head_ = 0, last_passes_ = 0;
-  DBuf<float> xf_, rf_, zf_, pf_, qf_, fgV_, fgZ_;
+  DBuf<float> xf_, rf_, zf_, pf_, qf_, fgV_, fgZ_, gYf_;
+  DBuf<__half> fvalH_;  // FP16 copy of the fine operator for the V-cycle (amg_half)
+  double hscale_ = 1.0;
   DBuf<double> fg_, fgpart_, gY_, gW_;
   LoopGraph g_loopf_, g_fgmres_;
   // learned stage: network state, face graph (neighbours, SELL offsets of

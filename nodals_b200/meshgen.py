@@ -182,8 +182,11 @@ def _orient(points: np.ndarray, tets: np.ndarray) -> np.ndarray:
 
 
 def pipe_mesh(nr: int = 8, ntheta: int = 24, nz: int = 35, radius: float = 0.5,
-              length: float = 10.0, jitter: float = 0.05, seed: int = 0) -> TetMesh:
-    """Straight circular pipe along +z from z=0 (inlet) to z=length (outlet)."""
+              length: float = 10.0, jitter: float = 0.05, seed: int = 0, bend_deg: float = 0.0) -> TetMesh:
+    """Circular pipe from the inlet disk at z=0 to the outlet at axial length
+    `length`: straight along +z, or (bend_deg > 0) with its axis bent in the
+    x-z plane along a circular arc that turns by bend_deg over the length (the
+    cross-sections stay normal to the axis; the inlet disk is unchanged)."""
     xy, quads, on_wall, wall_edges = _cross_section(nr, ntheta, radius)
     h2 = _local_spacing_2d(xy, quads)
     tri = _split_quads(xy, quads)
@@ -204,6 +207,16 @@ def pipe_mesh(nr: int = 8, ntheta: int = 24, nz: int = 35, radius: float = 0.5,
         pts[:, 0] += np.where(free_xy, jitter * hxy * u[:, 0], 0.0)
         pts[:, 1] += np.where(free_xy, jitter * hxy * u[:, 1], 0.0)
         pts[:, 2] += np.where(free_z, jitter * hz * u[:, 2], 0.0)
+    if bend_deg > 0.0:
+        # axis point at arc length z: (Rc (1 - cos phi), 0, Rc sin phi), phi = z / Rc;
+        # the section's x direction turns with the axis: (cos phi, 0, -sin phi)
+        rc = length / np.deg2rad(bend_deg)
+        if rc <= radius:
+            raise ValueError("bend radius must exceed the pipe radius")
+        phi = pts[:, 2] / rc
+        x = pts[:, 0].copy()
+        pts[:, 0] = rc * (1.0 - np.cos(phi)) + x * np.cos(phi)
+        pts[:, 2] = rc * np.sin(phi) - x * np.sin(phi)
     tets = []
     for s in range(nz):
         tets.append(_prism_tets(tri + s * n2, tri + (s + 1) * n2))
@@ -226,7 +239,7 @@ def pipe_mesh(nr: int = 8, ntheta: int = 24, nz: int = 35, radius: float = 0.5,
     wall = np.concatenate(wall, axis=0)
     bfaces = np.concatenate([wall, inlet, outlet], axis=0).astype(np.int32)
     btag = np.concatenate([np.zeros(len(wall)), np.ones(len(inlet)), 2 * np.ones(len(outlet))]).astype(np.int32)
-    meta = dict(nr=nr, ntheta=ntheta, nz=nz, radius=radius, length=length, jitter=jitter, seed=seed)
+    meta = dict(nr=nr, ntheta=ntheta, nz=nz, radius=radius, length=length, jitter=jitter, seed=seed, bend_deg=bend_deg)
     return TetMesh(points=pts, tets=tets, bfaces=bfaces, btag=btag, meta=meta)
 
 
@@ -669,6 +682,22 @@ CONFIGS = {
 
 def named(name: str) -> TetMesh:
     return pipe_mesh(**CONFIGS[name])
+
+
+# The learned stage's pipe family: members 0..63 train, 64..79 are held out.
+# Radius U[0.4, 0.6], length U[8, 12], axial bend U[0, 60] degrees, Re
+# U[10, 200], ~200k tets (12 rings x 40 sectors + 10 x 10 core, 58 slabs),
+# +-5 % jitter; every draw from the splitmix64 stream of the member.
+FAMILY_TRAIN, FAMILY_HELD_OUT = 64, 16
+
+
+def family_member(index: int):
+    """(mesh, Re, parameters) of member `index` of the learned stage's family."""
+    u = uniform01(0xC4F40000 + int(index), 4)
+    prm = dict(radius=0.4 + 0.2 * float(u[0]), length=8.0 + 4.0 * float(u[1]), bend_deg=60.0 * float(u[2]))
+    re = 10.0 + 190.0 * float(u[3])
+    mesh = pipe_mesh(nr=12, ntheta=40, nz=58, jitter=0.05, seed=1000 + int(index), **prm)
+    return mesh, re, dict(prm, re=re)
 
 
 if __name__ == "__main__":  # pragma: no cover - convenience CLI

@@ -69,7 +69,8 @@ class Options(C.Structure):
         ("precision", C.c_int), ("threads", C.c_int), ("device", C.c_int), ("verbose", C.c_int),
         ("supg", C.c_int), ("supg_tau_scale", C.c_double), ("supg_magic", C.c_double),
         ("p_krylov", C.c_int), ("p_restart", C.c_int), ("p_inner_rtol", C.c_double), ("p_refine_max", C.c_int),
-        ("p_guess", C.c_int), ("learned", C.c_int), ("geom_from_inlet", C.c_int),
+        ("p_guess", C.c_int), ("learned", C.c_int), ("geom_from_inlet", C.c_int), ("p_guess_fresh", C.c_int),
+        ("amg_half", C.c_int),
     ]
 
     @classmethod
@@ -490,6 +491,8 @@ class Mpnn:
         return C.c_void_p(x if isinstance(x, int) else x.data_ptr())
 
     def graph(self, n, nbr, ew, dscale) -> MpnnGraph:
+        """The graph view over device arrays; it holds raw addresses, so the
+        caller keeps nbr, ew and dscale alive while the view is used."""
         return MpnnGraph(int(n), self._addr(nbr), self._addr(ew), self._addr(dscale))
 
     def set_params(self, p: np.ndarray):

@@ -24,6 +24,9 @@ VARIANTS = {
     "fgmres_short": dict(p_krylov="fgmres", p_restart=5),
     "pcg_guess2": dict(p_krylov="pcg", p_guess=2),
     "fgmres_guess1": dict(p_krylov="fgmres", p_guess=1),
+    "pcg_guess4_fresh": dict(p_krylov="pcg", p_guess=4, p_guess_fresh=1),
+    "pcg_half_guess4": dict(p_krylov="pcg", p_guess=4, amg_half=1),
+    "fgmres_half": dict(p_krylov="fgmres", amg_half=1),
 }
 
 
@@ -46,7 +49,7 @@ def test_mixed_tracks_fp64(native, meshes, variant):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("variant", ["pcg", "fgmres_guess1"])
+@pytest.mark.parametrize("variant", ["pcg", "fgmres_guess1", "pcg_half_guess4"])
 def test_mixed_is_deterministic_and_graph_equals_host_loop(native, meshes, variant):
     """Two solvers give bitwise-equal runs; the device loops (conditional
     graphs) and the launch-by-launch loops taken while the profiler is on

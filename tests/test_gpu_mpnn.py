@@ -65,10 +65,11 @@ def test_forward_matches_oracle(native, meshes, mesh, segs):
     p = M.init_params(2)
     net = native.Mpnn(n, training=True)
     net.set_params(p)
-    g = net.graph(n, _dev(torch, nbr), _dev(torch, ew), _dev(torch, dscale))
+    # the graph holds raw device addresses: keep the tensors alive
+    keep = [_dev(torch, nbr), _dev(torch, ew), _dev(torch, dscale)]
+    g = net.graph(n, *keep)
     vd = _dev(torch, v)
     z = torch.zeros(n, dtype=torch.float32, device="cuda")
-    keep = [vd, z]
     net.forward(g, vd, z, seg)
     torch.cuda.synchronize()
     zo, cache = M.forward(p, nbr, ew, dscale, v, seg)
@@ -97,7 +98,8 @@ def test_gradients_match_oracle(native, meshes, mesh):
     p = M.init_params(6)
     net = native.Mpnn(n, training=True)
     net.set_params(p)
-    g = net.graph(n, _dev(torch, nbr), _dev(torch, ew), _dev(torch, dscale))
+    keep = [_dev(torch, nbr), _dev(torch, ew), _dev(torch, dscale)]
+    g = net.graph(n, *keep)
     vd, xd = _dev(torch, v), _dev(torch, x)
     loss = net.loss_backward(g, vd, xd, seg)
     grads = net.grads()
@@ -122,7 +124,8 @@ def test_adam_steps_reduce_the_loss(native, meshes):
     x = (v + M._aggregate(nbr, ew, v[:, None])[:, 0]).astype(np.float32)
     net = native.Mpnn(n, training=True)
     net.set_params(M.init_params(3))
-    g = net.graph(n, _dev(torch, nbr), _dev(torch, ew), _dev(torch, dscale))
+    keep = [_dev(torch, nbr), _dev(torch, ew), _dev(torch, dscale)]
+    g = net.graph(n, *keep)
     vd, xd = _dev(torch, v), _dev(torch, x)
     first = net.loss_backward(g, vd, xd)
     for step in range(1, 61):
