@@ -50,7 +50,7 @@ namespace mp {
 constexpr int kH = 64;         // hidden width
 constexpr int kX = 2 * kH;     // dense-layer input width [h ; m]
 constexpr int kTile = 128;     // rows per tile (= threads per CTA)
-constexpr uint32_t kWaitTries = 1u << 22;  // bound of every mbarrier wait
+constexpr uint64_t kWaitNs = 2000000000ull;  // bound of every mbarrier wait: 2 s of wall time
 
 // parameter layout (FP32 master copy; gradients use the same layout)
 constexpr int OFF_WE = 0, OFF_BE = 128;
@@ -307,11 +307,11 @@ __global__ void __launch_bounds__(kTile) layer_fwd(FwdArgs a) {
         tc::mma_bf16(tbase, tc::sdesc(xs + 256 * s, 128, 2048), tc::sdesc(ws + 256 * s, 128, 2048), idesc, s > 0);
       tc::mma_commit(&mbar);
     }
-    const bool ok = tc::mbar_wait_bounded(&mbar, phase, kWaitTries);
+    const bool ok = tc::mbar_wait_bounded(&mbar, phase, kWaitNs);
     phase ^= 1u;
     if (__syncthreads_or(!ok)) {
       if (tid == 0) atomicOr(a.err, 1);
-      tc::mbar_wait_bounded(&mbar, phase ^ 1u, kWaitTries);  // the MMAs of this tile, if still running
+      tc::mbar_wait_bounded(&mbar, phase ^ 1u, kWaitNs);  // the MMAs of this tile, if still running
       break;
     }
     tc::fence_after_sync();
@@ -459,31 +459,26 @@ __global__ void __launch_bounds__(kTile) layer_bwd(BwdArgs a) {
       tc::mma_commit(&mbar);
     }
     first = false;
-    const bool ok = tc::mbar_wait_bounded(&mbar, phase, kWaitTries);
+    const bool ok = tc::mbar_wait_bounded(&mbar, phase, kWaitNs);
     phase ^= 1u;
     if (__syncthreads_or(!ok)) {
       if (tid == 0) atomicOr(a.err, 1);
-      tc::mbar_wait_bounded(&mbar, phase ^ 1u, kWaitTries);
+      tc::mbar_wait_bounded(&mbar, phase ^ 1u, kWaitNs);
       aborted = true;
       break;
     }
     tc::fence_after_sync();
-    if (row < a.in.n) {
-      float t[32];
-      float* ds_out = a.dself + (size_t)row * kH;
-      float* dm_out = a.dm + (size_t)row * kH;
+    // tcgen05.ld is a warp-collective (.sync.aligned): every lane of the warp
+    // executes the same loads, rows past n only skip the stores
 #pragma unroll
-      for (int part = 0; part < 4; ++part) {
-        tc::tmem_ld32(tbase + ((uint32_t)(32 * warp) << 16) + 32 * part, t);
-        float* dst = part < 2 ? ds_out + 32 * part : dm_out + 32 * (part - 2);
+    for (int part = 0; part < 4; ++part) {
+      float t[32];
+      tc::tmem_ld32(tbase + ((uint32_t)(32 * warp) << 16) + 32 * part, t);
+      if (row < a.in.n) {
+        float* dst = part < 2 ? a.dself + (size_t)row * kH + 32 * part : a.dm + (size_t)row * kH + 32 * (part - 2);
 #pragma unroll
         for (int q = 0; q < 32; q += 4) *reinterpret_cast<float4*>(dst + q) = make_float4(t[q], t[q + 1], t[q + 2], t[q + 3]);
       }
-    } else {
-      // every warp takes part in the collective TMEM loads
-      float t[32];
-#pragma unroll
-      for (int part = 0; part < 4; ++part) tc::tmem_ld32(tbase + ((uint32_t)(32 * warp) << 16) + 32 * part, t);
     }
     tc::fence_before_sync();
     __syncthreads();
