@@ -56,10 +56,11 @@ WORKLOAD = "pipe1m"
 OPTIONS = dict(re=100.0, alpha_u=0.7, alpha_p=0.3, p_rtol=1e-6, p_max=400, run_mode="converge", simple_tol=1e-6,
                max_outer=6000, amg_hierarchy="sa", amg_smoother="cheb2", pressure_solver="pcg")
 # the fast configuration of the metric
-FAST = dict(precision="mixed", p_krylov="pcg", p_guess=4)
+FAST = dict(precision="mixed", p_krylov="pcg", p_guess=4, amg_half=1)
 FAST_NOTE = ("mixed: FP64 state, momentum, continuity and outer pressure residual; FP64 defect correction around "
-             "FP32 inner PCG (FP32 operator copy, FP32 SA+cheb2 V-cycle, FP64 reductions), inner rtol 1e-3; "
-             "Galerkin initial guess over the last 4 pressure corrections; learned stage: off (see DESIGN)")
+             "FP32 inner PCG (FP32 operator copy for A p, FP64 reductions), inner rtol 1e-3; SA+cheb2 V-cycle in FP32 "
+             "with its fine-level operator in FP16 (power-of-two scaled); Galerkin initial guess over the last 4 "
+             "pressure corrections (stored products)")
 # Complete FP64 solves of OPTIONS on WORKLOAD (tests/golden/cfg_pipe1m_re100_steady.npz,
 # the reference's own run): outer and total PCG iterations, for the CPU projection.
 STEADY_STATE_FP64 = {"outer": 4193, "pcg": 75316}

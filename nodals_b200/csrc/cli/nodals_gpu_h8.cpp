@@ -45,7 +45,7 @@ bool is_hxt1(const std::string& path) {
 int run(int argc, char** argv) {
   nds_options o;
   nds_options_default(&o);
-  std::string mesh, tag = "h8", vtu;
+  std::string mesh, tag = "h8", vtu, krylov = "pcg", stageFile;
   std::string prog = argv[0];
   if (ends_with(prog, "_fp32")) o.precision = NDS_FP32;
   std::string runMode = "fixed10", momWork = "fgs1", smoother = "cheb2", hierarchy = "sa", interp = "direct",
@@ -132,8 +132,18 @@ int run(int argc, char** argv) {
       if (p == "fp64") o.precision = NDS_FP64;
       else if (p == "fp32") o.precision = NDS_FP32;
       else if (p == "amg_fp32") o.precision = NDS_AMG_FP32;
-      else throw Fail("--precision must be fp64, fp32 or amg_fp32");
+      else if (p == "mixed") o.precision = NDS_MIXED;
+      else throw Fail("--precision must be fp64, fp32, amg_fp32 or mixed");
     } else if (a == "--device") o.device = iv();
+    // controls of the mixed-precision pressure solve (no reference counterpart)
+    else if (a == "--p-krylov") krylov = sv();
+    else if (a == "--p-restart") o.p_restart = iv();
+    else if (a == "--p-inner-rtol") o.p_inner_rtol = dv();
+    else if (a == "--p-refine-max") o.p_refine_max = iv();
+    else if (a == "--p-guess") o.p_guess = iv();
+    else if (a == "--p-guess-fresh") o.p_guess_fresh = iv();
+    else if (a == "--amg-half") o.amg_half = iv();
+    else if (a == "--learned-stage") stageFile = sv();
     else throw Fail("H8 usage error");
   }
   if (mesh.empty()) throw Fail("--mesh required");
@@ -164,7 +174,12 @@ int run(int argc, char** argv) {
   o.amg_mcgs_order = pick(mcgsOrder, {"symmetric", "forward", "backward"}, "H8 amg-mcgs-order must be symmetric, forward or backward");
   if (coarsening != "pmis") throw Fail("H8 cf-coarsening currently supports pmis");
   if (strength != "classical-negative") throw Fail("H8 cf-strength currently supports classical-negative");
-  const char* prec = o.precision == NDS_FP32 ? "fp32" : o.precision == NDS_AMG_FP32 ? "amg_fp32" : "fp64";
+  o.p_krylov = pick(krylov, {"pcg", "fgmres"}, "--p-krylov must be pcg or fgmres");
+  o.learned = stageFile.empty() ? 0 : 1;
+  const char* prec = o.precision == NDS_FP32       ? "fp32"
+                     : o.precision == NDS_AMG_FP32 ? "amg_fp32"
+                     : o.precision == NDS_MIXED    ? "mixed"
+                                                   : "fp64";
 
   const auto t0 = std::chrono::steady_clock::now();
   nds_mesh* M = nullptr;
@@ -179,6 +194,15 @@ int run(int argc, char** argv) {
   const double setup_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   nds_solver* S = nullptr;
   ck(nds_solver_create(P, &S), "device setup");
+  if (!stageFile.empty()) {
+    // learned stage parameters: NDS_MPNN_NPARAM float32 values
+    std::vector<float> prm(NDS_MPNN_NPARAM);
+    FILE* f = std::fopen(stageFile.c_str(), "rb");
+    const size_t got = f ? std::fread(prm.data(), sizeof(float), prm.size(), f) : 0;
+    if (f) std::fclose(f);
+    if (got != prm.size()) throw Fail("--learned-stage: cannot read " + std::to_string(prm.size()) + " parameters");
+    ck(nds_solver_load_stage(S, prm.data(), (int)prm.size()), "learned stage");
+  }
   const double upload_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() - setup_s;
   std::printf("NODALS_GPU_H8_CONFIG tag=%s precision=%s device=B200 cells=%d runMode=%s momentumWork=%s "
               "momentumResidualPolicy=%s physicalOperator=exact_current_CSR alphaU=%.8g alphaP=%.8g simpleTol=%.3e "

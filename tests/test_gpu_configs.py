@@ -27,7 +27,7 @@ CFG1 = dict(re=20.0, alpha_u=0.7, alpha_p=0.3, p_rtol=1e-6, p_max=400, run_mode=
 CFG2 = dict(re=100.0, alpha_u=0.7, alpha_p=0.3, p_rtol=1e-6, p_max=400, run_mode="converge", simple_tol=1e-6,
             max_outer=6000, **SA)
 # the benchmark's fast path (bench.py)
-MIXED = dict(precision="mixed", p_krylov="pcg", p_guess=2)
+MIXED = dict(precision="mixed", p_krylov="pcg", p_guess=4, amg_half=1)
 
 
 def _history(S, n_max, printed):
