@@ -999,27 +999,37 @@ __global__ void __launch_bounds__(kRefreshBlock) sell_refresh(int nc, const int3
   }
   __syncthreads();  // image zeroed, rAU of every row staged
   T asum = 0;
-  for (int q0 = qb; q0 < qe; q0 += 32) {  // warp-uniform bounds
-    const int q = q0 + lane;
-    unsigned v = 0xFFFFu;
-    T p = 0;
-    if (q < qe) {
-      v = cs[q];
-      if (v != 0xFFFFu) p = sR[r][v & 7u] * G[q];
+  // the code words and factors of up to kPF chunks are loaded before any of
+  // them is summed (more loads in flight); the sums are unchanged
+  constexpr int kPF = 4;
+  for (int q1 = qb; q1 < qe; q1 += 32 * kPF) {  // warp-uniform bounds
+    unsigned vv[kPF];
+    T gg[kPF];
+#pragma unroll
+    for (int u = 0; u < kPF; ++u) {
+      const int q = q1 + 32 * u + lane;
+      vv[u] = q < qe ? (unsigned)cs[q] : 0xFFFFu;
+      gg[u] = q < qe ? G[q] : T(0);
     }
-    const bool real = v != 0xFFFFu;
-    const int pos = real ? (int)((v >> 3) & 7u) : 0;
-    const int maxpos = __reduce_max_sync(0xffffffffu, pos);
-    T acc = p;
-    for (int j = 1; j <= maxpos; ++j) {
-      const T up = __shfl_up_sync(0xffffffffu, acc, 1);
-      if (pos == j) acc = up + p;
-    }
-    if (real && (v & 64u)) {
-      const int sl = (int)(v >> 7);
-      sv[sl * 33 + r] = acc;
-      if (sl == ds) diag[c] = TA(acc);
-      asum += fabs(acc);
+#pragma unroll
+    for (int u = 0; u < kPF; ++u) {
+      if (q1 + 32 * u >= qe) break;
+      const unsigned v = vv[u];
+      const T p = v != 0xFFFFu ? sR[r][v & 7u] * gg[u] : T(0);
+      const bool real = v != 0xFFFFu;
+      const int pos = real ? (int)((v >> 3) & 7u) : 0;
+      const int maxpos = __reduce_max_sync(0xffffffffu, pos);
+      T acc = p;
+      for (int j = 1; j <= maxpos; ++j) {
+        const T up = __shfl_up_sync(0xffffffffu, acc, 1);
+        if (pos == j) acc = up + p;
+      }
+      if (real && (v & 64u)) {
+        const int sl = (int)(v >> 7);
+        sv[sl * 33 + r] = acc;
+        if (sl == ds) diag[c] = TA(acc);
+        asum += fabs(acc);
+      }
     }
   }
   if (l1 && live_row) {

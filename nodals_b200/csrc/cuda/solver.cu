@@ -1755,7 +1755,8 @@ class Solver final : public ISolver {
     PRes R;
     if constexpr (!kSame) {
       const double* rhs = rhs_t;
-      const double bn = std::sqrt(dot_fetch(rhs, rhs, nc_, S_TMP));
+      // ||b|| = ||B u + fixedDiv||: the continuity norm this iteration already read back
+      const double bn = std::sqrt(hsc_[S_CONT2]);
       if (!std::isfinite(bn)) throw SolveFailure(NDS_E_BREAKDOWN, "pressure initial norm nonfinite");
       const double target = std::max(o_.p_atol, o_.p_rtol * bn);
       start_readback();
