@@ -166,19 +166,22 @@ def _barrier_max(x: float, ws: int, device: int) -> float:
     return float(t.item())
 
 
-def fine_spmv_bytes(problem, s: int) -> float:
+def fine_spmv_bytes(problem, s: int, sx: int | None = None) -> float:
     """Compulsory bytes of one fine Schur SpMV in CSR terms: values (s B) and
-    column indices (4 B) of every entry, row offsets, x and y once."""
+    column indices (4 B) of every entry, row offsets, x and y once (sx B
+    each; default s)."""
+    sx = s if sx is None else sx
     row = problem.array("fine.row")
     n = len(row) - 1
     nnz = int(row[-1])
-    return nnz * (s + 4) + 4 * (n + 1) + 2 * s * n
+    return nnz * (s + 4) + 4 * (n + 1) + 2 * sx * n
 
 
-def sell_format_bytes(problem, s: int) -> float:
+def sell_format_bytes(problem, s: int, sx: int | None = None) -> float:
     """Bytes the SELL-32x4 fine operator actually streams per SpMV: padded
     values (s B) and 16-bit column deltas (slice width rounded up to a
-    multiple of 4), slice offsets/widths, x and y."""
+    multiple of 4), slice offsets/widths, x and y (sx B each)."""
+    sx = s if sx is None else sx
     row = problem.array("fine.row")
     n = len(row) - 1
     lens = np.diff(row)
@@ -187,7 +190,7 @@ def sell_format_bytes(problem, s: int) -> float:
     w[:n] = lens
     widths = (w.reshape(ns, 32).max(axis=1) + 3) // 4 * 4
     padded = int(widths.sum()) * 32
-    return padded * (s + 2) + 8 * ns + 2 * s * n
+    return padded * (s + 2) + 8 * ns + 2 * sx * n
 
 
 def _rel(a, b):
@@ -256,30 +259,42 @@ def run_nodals(args):
         raise RuntimeError(f"the fast solve did not converge ({rep.outer_its} iterations)")
     del S
 
-    # --- roofline: the FP32 fine-level SELL SpMV (V-cycle and inner Krylov) --
+    # --- roofline: the dominant kernel, the V-cycle's fine-level SELL SpMV --
+    # (FP16 values, FP32 vectors: 4 per inner iteration); the inner Krylov
+    # product (FP32 values) and the FP64 defect product are reported beside it
     roof = None
-    calls, tot = prof["fine_spmv_amg"]
+    half = bool(FAST.get("amg_half"))
+    cat = "fine_spmv_half" if half else "fine_spmv_amg"
+    calls, tot = prof[cat]
+    peak, peak_kind = _peaks()
+
+    def side(name, s_val, s_vec):
+        c, t = prof[name]
+        if c == 0:
+            return None
+        return {"avg_launch_ms": round(t / c, 5), "launches": c,
+                "achieved": round(fine_spmv_bytes(P, s_val, s_vec) / (t / c * 1e-3) / 1e9, 1)}
     if args.profile_steps > 0 and calls > 0:
         avg_ms = tot / calls
-        alg = fine_spmv_bytes(P, 4)
-        fmt = sell_format_bytes(P, 4)
-        peak, peak_kind = _peaks()
+        sv = 2 if half else 4
+        alg = fine_spmv_bytes(P, sv, 4)
+        fmt = sell_format_bytes(P, sv, 4)
         achieved = alg / (avg_ms * 1e-3) / 1e9
-        c64, t64 = prof["fine_spmv"]
         roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                "frac": round(achieved / peak, 4), "traffic": _traffic("bytes_per_launch_pipe1m_fp32"),
+                "frac": round(achieved / peak, 4),
+                "traffic": _traffic("bytes_per_launch_pipe1m_half" if half else "bytes_per_launch_pipe1m_fp32"),
                 "peak_kind": peak_kind,
-                "kernel": "fine Schur SELL-32x4 SpMV in FP32 (sell_spmv<float,*>): V-cycle fine-level smoothing "
-                          "and residual steps and the inner Krylov A p",
+                "kernel": ("fine Schur SELL-32x4 SpMV of the V-cycle (sell_spmv<float,*,*,__half>: FP16 values, "
+                           "16-bit column deltas, FP32 vectors): fine-level smoothing and residual steps") if half else
+                          "fine Schur SELL-32x4 SpMV in FP32 (sell_spmv<float,*>)",
                 "algorithmic_bytes_per_launch": int(alg),
-                "algorithmic_bytes_rule": "nnz*(4+4) + 4(n+1) + 2*4*n (CSR index 4 B, value 4 B, x and y once)",
+                "algorithmic_bytes_rule": f"nnz*({sv}+4) + 4(n+1) + 2*4*n (CSR index 4 B, value {sv} B, x and y once)",
                 "format_bytes_per_launch": int(fmt),
                 "format_frac": round(fmt / (avg_ms * 1e-3) / 1e9 / peak, 4),
                 "avg_launch_ms": round(avg_ms, 5), "launches": calls,
                 "timed_in": f"profiled pass of {args.profile_steps} steps after the timed steps",
-                "fp64_defect_spmv": None if c64 == 0 else {
-                    "avg_launch_ms": round(t64 / c64, 5), "launches": c64,
-                    "achieved": round(fine_spmv_bytes(P, 8) / (t64 / c64 * 1e-3) / 1e9, 1)}}
+                "inner_krylov_spmv_fp32": side("fine_spmv_amg", 4, 4),
+                "fp64_defect_spmv": side("fine_spmv", 8, 8)}
 
     # --- field error against the plain FP64 path (untimed) -------------------
     errors = None

@@ -334,9 +334,9 @@ __global__ void __launch_bounds__(kBlock) mom_assemble(MomArgs<T> g) {
 }
 
 // One multicolour Gauss-Seidel colour pass on the shared momentum matrix,
-// three right-hand sides (g5e_fp32_kernels.cuh:106-116).  rows: the colour's
-// rows; span: their (begin, end) in the CSR, in the same order, so the row's
-// entries and its own data load in parallel.
+// three right-hand sides (g5e_fp32_kernels.cuh:106-116).  8 lanes per row.
+// rows: the colour's rows; span: their (begin, end) in the CSR, in the same
+// order, so the row's entries and its own data load in parallel.
 template <class T>
 __global__ void __launch_bounds__(kBlock) mom_gs_color(int count, const int32_t* __restrict__ rows,
                                                        const int2* __restrict__ span, const int32_t* __restrict__ ci,
@@ -344,42 +344,25 @@ __global__ void __launch_bounds__(kBlock) mom_gs_color(int count, const int32_t*
                                                        const T* __restrict__ b0, const T* __restrict__ b1,
                                                        const T* __restrict__ b2, T* __restrict__ x0, T* __restrict__ x1,
                                                        T* __restrict__ x2, T omega) {
-  // one thread per row of the colour; the off-diagonal sum runs over the
-  // row in CSR order (the reference's and the oracle's order), with the
-  // loads of four entries and their gathers issued before the sums
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane8 = threadIdx.x & 7;
+  const int q = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
   if (q >= count) return;
+  const unsigned gmask = group8_mask();
   const int i = rows[q];
   const int2 sp = span[q];
+  T d = 0, c0 = 0, c1 = 0, c2 = 0, y0 = 0, y1 = 0, y2 = 0;
   const size_t vi = kVel * (size_t)i;
-  const T d = diag[i], c0 = b0[i], c1 = b1[i], c2 = b2[i];
-  const T y0 = x0[vi], y1 = x1[vi], y2 = x2[vi];
-  T s0 = 0, s1 = 0, s2 = 0;
-  int k = sp.x;
-  for (; k + 4 <= sp.y; k += 4) {
-    int j[4];
-    T a[4], u0[4], u1[4], u2[4];
-#pragma unroll
-    for (int e = 0; e < 4; ++e) {
-      j[e] = ci[k + e];
-      a[e] = av[k + e];
-    }
-#pragma unroll
-    for (int e = 0; e < 4; ++e) {
-      const size_t vj = kVel * (size_t)j[e];
-      u0[e] = x0[vj];
-      u1[e] = x1[vj];
-      u2[e] = x2[vj];
-    }
-#pragma unroll
-    for (int e = 0; e < 4; ++e)
-      if (j[e] != i) {
-        s0 += a[e] * u0[e];
-        s1 += a[e] * u1[e];
-        s2 += a[e] * u2[e];
-      }
+  if (lane8 == 0) {
+    d = diag[i];
+    c0 = b0[i];
+    c1 = b1[i];
+    c2 = b2[i];
+    y0 = x0[vi];
+    y1 = x1[vi];
+    y2 = x2[vi];
   }
-  for (; k < sp.y; ++k) {
+  T s0 = 0, s1 = 0, s2 = 0;
+  for (int k = sp.x + lane8; k < sp.y; k += 8) {
     const int j = ci[k];
     if (j == i) continue;
     const T a = av[k];
@@ -388,10 +371,15 @@ __global__ void __launch_bounds__(kBlock) mom_gs_color(int count, const int32_t*
     s1 += a * x1[vj];
     s2 += a * x2[vj];
   }
-  const T iv = T(1) / d;
-  x0[vi] = (T(1) - omega) * y0 + omega * ((c0 - s0) * iv);
-  x1[vi] = (T(1) - omega) * y1 + omega * ((c1 - s1) * iv);
-  x2[vi] = (T(1) - omega) * y2 + omega * ((c2 - s2) * iv);
+  s0 = group_sum<8>(s0, gmask);
+  s1 = group_sum<8>(s1, gmask);
+  s2 = group_sum<8>(s2, gmask);
+  if (lane8 == 0) {
+    const T iv = T(1) / d;
+    x0[vi] = (T(1) - omega) * y0 + omega * ((c0 - s0) * iv);
+    x1[vi] = (T(1) - omega) * y1 + omega * ((c1 - s1) * iv);
+    x2[vi] = (T(1) - omega) * y2 + omega * ((c2 - s2) * iv);
+  }
 }
 
 // ||b_d||^2 and ||b_d - A u_d||^2 (g5e_fp32_kernels.cuh:117-126); 6 partials per block.
@@ -999,37 +987,27 @@ __global__ void __launch_bounds__(kRefreshBlock) sell_refresh(int nc, const int3
   }
   __syncthreads();  // image zeroed, rAU of every row staged
   T asum = 0;
-  // the code words and factors of up to kPF chunks are loaded before any of
-  // them is summed (more loads in flight); the sums are unchanged
-  constexpr int kPF = 4;
-  for (int q1 = qb; q1 < qe; q1 += 32 * kPF) {  // warp-uniform bounds
-    unsigned vv[kPF];
-    T gg[kPF];
-#pragma unroll
-    for (int u = 0; u < kPF; ++u) {
-      const int q = q1 + 32 * u + lane;
-      vv[u] = q < qe ? (unsigned)cs[q] : 0xFFFFu;
-      gg[u] = q < qe ? G[q] : T(0);
+  for (int q0 = qb; q0 < qe; q0 += 32) {  // warp-uniform bounds
+    const int q = q0 + lane;
+    unsigned v = 0xFFFFu;
+    T p = 0;
+    if (q < qe) {
+      v = cs[q];
+      if (v != 0xFFFFu) p = sR[r][v & 7u] * G[q];
     }
-#pragma unroll
-    for (int u = 0; u < kPF; ++u) {
-      if (q1 + 32 * u >= qe) break;
-      const unsigned v = vv[u];
-      const T p = v != 0xFFFFu ? sR[r][v & 7u] * gg[u] : T(0);
-      const bool real = v != 0xFFFFu;
-      const int pos = real ? (int)((v >> 3) & 7u) : 0;
-      const int maxpos = __reduce_max_sync(0xffffffffu, pos);
-      T acc = p;
-      for (int j = 1; j <= maxpos; ++j) {
-        const T up = __shfl_up_sync(0xffffffffu, acc, 1);
-        if (pos == j) acc = up + p;
-      }
-      if (real && (v & 64u)) {
-        const int sl = (int)(v >> 7);
-        sv[sl * 33 + r] = acc;
-        if (sl == ds) diag[c] = TA(acc);
-        asum += fabs(acc);
-      }
+    const bool real = v != 0xFFFFu;
+    const int pos = real ? (int)((v >> 3) & 7u) : 0;
+    const int maxpos = __reduce_max_sync(0xffffffffu, pos);
+    T acc = p;
+    for (int j = 1; j <= maxpos; ++j) {
+      const T up = __shfl_up_sync(0xffffffffu, acc, 1);
+      if (pos == j) acc = up + p;
+    }
+    if (real && (v & 64u)) {
+      const int sl = (int)(v >> 7);
+      sv[sl * 33 + r] = acc;
+      if (sl == ds) diag[c] = TA(acc);
+      asum += fabs(acc);
     }
   }
   if (l1 && live_row) {

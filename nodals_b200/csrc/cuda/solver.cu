@@ -82,11 +82,12 @@ struct DBuf {
 // stream (the analogue of the reference's H0Profiler, h8_main_base.cu:58-99).
 // fine_spmv: the physical fine operator (Krylov A p, power iterations);
 // fine_spmv_amg: the fine-level operator inside the V-cycle
+// fine_spmv_half: the V-cycle's fine-level operator in FP16 (amg_half)
 enum ProfCat { P_FINE_SPMV = 0, P_COARSE_SPMV, P_REFRESH, P_ASSEMBLE, P_GS, P_CONTINUITY, P_TRANSFER, P_TERMINAL,
-               P_VECTOR, P_FINE_AMG, P_NCAT };
+               P_VECTOR, P_FINE_AMG, P_FINE_HALF, P_NCAT };
 static const char* const kProfNames[P_NCAT] = {"fine_spmv", "coarse_spmv", "fine_refresh", "mom_assemble", "mom_gs",
                                                "continuity", "transfer", "terminal_dense", "vector_reduce",
-                                               "fine_spmv_amg"};
+                                               "fine_spmv_amg", "fine_spmv_half"};
 struct Profiler {
   bool on = false;
   std::vector<cudaEvent_t> ev;
@@ -283,13 +284,6 @@ class Solver final : public ISolver {
     DBuf<int32_t> row, col, crows;
     std::vector<int> coff;
     DBuf<TA> val, diag, l1, b, x, r, tmp, corr, pong;
-    // amg_half: the level operator (a setup snapshot) also in SELL-32x4 with
-    // FP16 values scaled by 1 / hinv, read by the level's SpMVs
-    k::Sell sell{};
-    DBuf<int32_t> sbase, swidth, scol;
-    DBuf<int16_t> sdcol;
-    DBuf<__half> hval;
-    double hinv = 1.0;
   };
   struct Xfer {  // P (fine rows, ELL k-major) and R = P^T (coarse rows, CSR)
     int nf = 0, nc = 0, pw = 0;
@@ -571,9 +565,6 @@ class Solver final : public ISolver {
       }
       Lv.l1.upload(l1h);
       for (auto* b : {&Lv.b, &Lv.x, &Lv.r, &Lv.tmp, &Lv.corr, &Lv.pong}) b->alloc((size_t)A.n);
-      // explicit levels of the mixed path's V-cycle in FP16 (the terminal
-      // level is applied through its dense inverse)
-      if (o_.precision == NDS_MIXED && o_.amg_half && l + 1 < H.A.size()) level_to_half(Lv, A);
       if (o_.amg_smoother == NDS_SM_MCGS && l + 1 < H.A.size()) {
         std::vector<int32_t> rows;
         std::vector<int32_t> r32 = to_i32(A.row, "AMG level CSR");
@@ -865,72 +856,12 @@ class Solver final : public ISolver {
     if (fvalH_.p) {
       A.vh = fvalH_.p;
       A.vinv = 1.0 / hscale_;
+      A.cat = P_FINE_HALF;
     }
     return A;
   }
   OpView<TA> level_op(const Level& A) const {
-    if (A.hval.p) {
-      OpView<TA> V{A.n, true, A.sell, nullptr, nullptr, nullptr, P_COARSE_SPMV};
-      V.vh = A.hval.p;
-      V.vinv = A.hinv;
-      return V;
-    }
     return {A.n, false, k::Sell{}, A.row.p, A.col.p, A.val.p, P_COARSE_SPMV};
-  }
-  // SELL-32x4 copy of a level in FP16: entry k of row 32 s + l at
-  // base[s] + 128 (k/4) + 4 l + k%4, rows padded to a multiple of 4 with zero
-  // values pointing at their own row; values scaled by the power of two that
-  // puts the largest diagonal at 2^11; 16-bit column deltas when they fit
-  void level_to_half(Level& Lv, const CsrHost& A) {
-    const int n = A.n, ns = (n + 31) / 32;
-    std::vector<int32_t> width((size_t)ns, 0), base((size_t)ns + 1, 0);
-    for (int i = 0; i < n; ++i)
-      width[(size_t)(i >> 5)] = std::max<int32_t>(width[(size_t)(i >> 5)], (int32_t)(A.row[(size_t)i + 1] - A.row[(size_t)i]));
-    auto padded = [&](int q) { return (width[(size_t)q] + 3) & ~3; };
-    for (int q = 0; q < ns; ++q) {
-      const int64_t nb = (int64_t)base[(size_t)q] + 32LL * padded(q);
-      if (nb > INT32_MAX) throw std::runtime_error("SELL level operator exceeds int32 offsets");
-      base[(size_t)q + 1] = (int32_t)nb;
-    }
-    double dmax = 0.0;
-    for (double d : A.diag) dmax = std::max(dmax, std::abs(d));
-    if (!(dmax > 0.0) || !std::isfinite(dmax)) throw std::runtime_error("FP16 level copy: no positive diagonal");
-    const double scale = std::ldexp(1.0, (int)std::floor(std::log2(2048.0 / dmax)));
-    const size_t ne = (size_t)base[(size_t)ns];
-    std::vector<int32_t> scol(ne, 0);
-    std::vector<int16_t> dcol(ne, 0);
-    std::vector<__half> hv(ne, __float2half(0.0f));
-    bool fits = true;
-    for (int q = 0; q < ns; ++q)
-      for (int l = 0; l < 32; ++l) {
-        const int i = 32 * q + l;
-        const int64_t rb = i < n ? A.row[(size_t)i] : 0;
-        const int len = i < n ? (int)(A.row[(size_t)i + 1] - rb) : 0;
-        for (int k = 0; k < padded(q); ++k) {
-          const size_t o = (size_t)base[(size_t)q] + 128 * (size_t)(k >> 2) + 4 * (size_t)l + (size_t)(k & 3);
-          const int c = k < len ? A.col[(size_t)(rb + k)] : (i < n ? i : 0);
-          scol[o] = c;
-          const int d = i < n ? c - i : 0;
-          if (d < -32767 || d > 32767) fits = false;
-          else dcol[o] = (int16_t)d;
-          if (k < len) {
-            const double v = std::min(std::max(A.val[(size_t)(rb + k)] * scale, -65504.0), 65504.0);
-            hv[o] = __float2half((float)v);
-          }
-        }
-      }
-    Lv.swidth.upload(width);
-    Lv.sbase.upload(base);
-    if (fits) {
-      Lv.sdcol.upload(dcol);
-      Lv.sell = k::Sell{n, Lv.sbase.p, Lv.swidth.p, nullptr, Lv.sdcol.p};
-    } else {
-      Lv.scol.upload(scol);
-      Lv.sell = k::Sell{n, Lv.sbase.p, Lv.swidth.p, Lv.scol.p, nullptr};
-    }
-    Lv.hval.alloc(ne);
-    NDS_CUDA(cudaMemcpy(Lv.hval.p, hv.data(), ne * sizeof(__half), cudaMemcpyHostToDevice));
-    Lv.hinv = 1.0 / scale;
   }
   template <class V>
   void op_spmv(const OpView<V>& A, const V* x, V* y) {
@@ -1930,7 +1861,7 @@ class Solver final : public ISolver {
       const int s = color_off_[(size_t)c], n = color_off_[(size_t)c + 1] - s;
       if (!n) continue;
       ProfScope ps(prof, st_, P_GS);
-      k::mom_gs_color<T><<<grid_for(n), kBlock, 0, st_>>>(n, color_rows_.p + s, color_span_.p + s, mcol_.p, A_.p,
+      k::mom_gs_color<T><<<grid_for((long long)n * 8), kBlock, 0, st_>>>(n, color_rows_.p + s, color_span_.p + s, mcol_.p, A_.p,
                                                                        diag_.p, b_[0].p, b_[1].p, b_[2].p, uc(0),
                                                                        uc(1), uc(2), T(o_.mom_omega));
       NDS_LAUNCH();
