@@ -290,6 +290,10 @@ int nds_mpnn_forward(nds_mpnn* m, const nds_mpnn_graph* g, int nseg, const int32
  * nds_mpnn_adam_step */
 int nds_mpnn_loss_backward(nds_mpnn* m, const nds_mpnn_graph* g, int nseg, const int32_t* seg_off, const float* v,
                            const float* x, double* loss);
+/* gradients from dL/dz (device, n values) of the last nds_mpnn_forward on
+ * the same graph (training handle): for losses computed outside, e.g. on the
+ * residual b - A z with the solver's operator */
+int nds_mpnn_backward(nds_mpnn* m, const nds_mpnn_graph* g, const float* dz);
 int nds_mpnn_get_grads(nds_mpnn* m, float* host_grads, int count);
 int nds_mpnn_adam_step(nds_mpnn* m, float lr, float beta1, float beta2, float eps, int step);
 /* BF16 activations h^layer (n_max x 64, row-major) into a device buffer */
@@ -303,6 +307,9 @@ void nds_mpnn_destroy(nds_mpnn* m);
 int nds_solver_load_stage(nds_solver* s, const float* host_params, int count);
 int nds_solver_stage_graph(nds_solver* s, int32_t* nbr, float* ew, float* dscale);
 int nds_solver_pressure_pair(nds_solver* s, float* rhs, float* x);
+/* y = A x with the solver's current pressure operator in FP32 (device
+ * arrays of nc values; precision mixed) */
+int nds_solver_apply_operator(nds_solver* s, const float* x, float* y);
 /* counters of the learned stage since the solver was created: applications
  * and fallbacks to the plain V-cycle */
 int nds_solver_stage_counts(nds_solver* s, long long* applied, long long* fallbacks);

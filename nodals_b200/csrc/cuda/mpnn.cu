@@ -614,6 +614,39 @@ __global__ void __launch_bounds__(kBlock) decoder_bwd(int n, const float* __rest
   }
   write_partials<kH + 2>(acc, part);
 }
+// the same from a gradient dz with respect to z = out sigma dscale:
+// dout = dz sigma dscale
+__global__ void __launch_bounds__(kBlock) decoder_bwd_dz(int n, const float* __restrict__ dz,
+                                                         const float* __restrict__ dscale,
+                                                         const float* __restrict__ sigma,
+                                                         const int32_t* __restrict__ seg_off, int nseg,
+                                                         const __nv_bfloat16* __restrict__ h3,
+                                                         const float2* __restrict__ f, const float* __restrict__ params,
+                                                         float* __restrict__ dh3, double* __restrict__ part) {
+  double acc[kH + 2];
+#pragma unroll
+  for (int q = 0; q < kH + 2; ++q) acc[q] = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float g = dz[i] * sigma[seg_of(i, seg_off, nseg)] * dscale[i];
+    const uint4* hh = reinterpret_cast<const uint4*>(h3 + (size_t)i * kH);
+    float4* d = reinterpret_cast<float4*>(dh3 + (size_t)i * kH);
+    for (int c = 0; c < 8; ++c) {
+      float hv[8];
+      unpack8(hh[c], hv);
+      float o[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        acc[8 * c + q] += (double)g * hv[q];
+        o[q] = g * params[OFF_WD + 8 * c + q];
+      }
+      d[2 * c] = make_float4(o[0], o[1], o[2], o[3]);
+      d[2 * c + 1] = make_float4(o[4], o[5], o[6], o[7]);
+    }
+    acc[kH] += g;
+    acc[kH + 1] += (double)g * f[i].x;
+  }
+  write_partials<kH + 2>(acc, part);
+}
 // out[c] = sum_r part[r][c] (fixed order), into grad at offset (FP32)
 __global__ void reduce_rows_f(const float* __restrict__ part, int rows, int cols, float* __restrict__ out) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -853,6 +886,22 @@ struct MpnnImpl {
     mp::decoder_bwd<<<rg, kBlock, 0, st>>>(g.n, out.p, x, g.dscale, sigma.p, seg_dev.p, nseg, segd.p, h3.p, f.p,
                                            params.p, dh.p, dpart.p);
     NDS_LAUNCH();
+    layers_backward(g, rg);
+    return loss;
+  }
+  // gradients from dL/dz of the last forward (which must have been run on
+  // this graph with the training buffers)
+  void backward_dz(const nds_mpnn_graph& g, const float* dz) {
+    if (!training) throw std::runtime_error("learned stage: created without training buffers");
+    const int nseg = (int)seg_host.size() - 1;
+    const int rg = std::min(grid_for(g.n), kMaxBlocks);
+    mp::decoder_bwd_dz<<<rg, kBlock, 0, st>>>(g.n, dz, g.dscale, sigma.p, seg_dev.p, nseg, h3.p, f.p, params.p, dh.p,
+                                              dpart.p);
+    NDS_LAUNCH();
+    layers_backward(g, rg);
+  }
+  // decoder partials in dpart and dh3 in dh -> every parameter gradient
+  void layers_backward(const nds_mpnn_graph& g, int rg) {
     mp::reduce_rows_d<<<1, 128, 0, st>>>(dpart.p, rg, mp::kH + 2, grads.p + mp::OFF_WD);
     NDS_LAUNCH();
     const int bgrid = std::max(1, std::min(bwd_grid, tiles(g.n)));
@@ -892,7 +941,6 @@ struct MpnnImpl {
       NDS_CUDA(cudaMemcpyAsync(grads.p + mp::OFF_WE, wtmp.p, sizeof(float) * 3 * mp::kH, cudaMemcpyDeviceToDevice, st));
     }
     check_err();
-    return loss;
   }
   void adam_step(float lr, float b1, float b2, float eps, int step) {
     const float c1 = 1.f - std::pow(b1, (float)step), c2 = 1.f - std::pow(b2, (float)step);
@@ -1007,6 +1055,13 @@ int nds_mpnn_loss_backward(nds_mpnn* m, const nds_mpnn_graph* g, int nseg, const
   return mguard([&] {
     const double L = m->impl->loss_backward(*g, v, x, segs(g->n, nseg, seg_off));
     if (loss) *loss = L;
+  });
+}
+int nds_mpnn_backward(nds_mpnn* m, const nds_mpnn_graph* g, const float* dz) {
+  if (!m || !g || !dz) return mfail(NDS_E_INVALID, "nds_mpnn_backward: null argument");
+  return mguard([&] {
+    if (g->n != m->impl->seg_n) throw std::invalid_argument("graph differs from the last forward's");
+    m->impl->backward_dz(*g, dz);
   });
 }
 int nds_mpnn_adam_step(nds_mpnn* m, float lr, float beta1, float beta2, float eps, int step) {

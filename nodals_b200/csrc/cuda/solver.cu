@@ -157,6 +157,7 @@ struct ISolver {
   virtual void stage_graph(int32_t* nbr, float* ew, float* dscale) = 0;
   virtual void pressure_pair(float* rhs, float* x) = 0;
   virtual void stage_counts(long long* applied, long long* fallbacks) = 0;
+  virtual void apply_operator(const float* x, float* y) = 0;
   Profiler prof;
 };
 
@@ -1491,6 +1492,14 @@ class Solver final : public ISolver {
     }
     NDS_CUDA(cudaStreamSynchronize(st_));
   }
+  void apply_operator(const float* x, float* y) override {
+    if constexpr (kSame) {
+      throw SolveFailure(NDS_E_INVALID, "the FP32 operator product needs precision mixed or amg_fp32");
+    } else {
+      op_spmv(fine_opA(), x, y);
+      NDS_CUDA(cudaStreamSynchronize(st_));
+    }
+  }
   void stage_counts(long long* applied, long long* fallbacks) override {
     unsigned long long c[2] = {0, 0};
     if (st_cnt_.p) {
@@ -2302,6 +2311,10 @@ int nds_solver_stage_graph(nds_solver* s, int32_t* nbr, float* ew, float* dscale
 int nds_solver_pressure_pair(nds_solver* s, float* rhs, float* x) {
   if (!s) return fail(NDS_E_INVALID, "null solver");
   return guarded([&] { s->impl->pressure_pair(rhs, x); });
+}
+int nds_solver_apply_operator(nds_solver* s, const float* x, float* y) {
+  if (!s || !x || !y) return fail(NDS_E_INVALID, "null argument");
+  return guarded([&] { s->impl->apply_operator(x, y); });
 }
 int nds_solver_stage_counts(nds_solver* s, long long* applied, long long* fallbacks) {
   if (!s) return fail(NDS_E_INVALID, "null solver");

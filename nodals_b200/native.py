@@ -218,6 +218,8 @@ def lib():
             L.nds_mpnn_forward.argtypes = [vp, C.c_void_p, C.c_int, vp, vp, vp]
             L.nds_mpnn_loss_backward.argtypes = [vp, C.c_void_p, C.c_int, vp, vp, vp, C.POINTER(C.c_double)]
             L.nds_mpnn_adam_step.argtypes = [vp, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int]
+            L.nds_mpnn_backward.argtypes = [vp, C.c_void_p, vp]
+            L.nds_solver_apply_operator.argtypes = [vp, vp, vp]
             L.nds_mpnn_activations.argtypes = [vp, C.c_int, vp]
             L.nds_mpnn_destroy.argtypes = [vp]
             L.nds_solver_load_stage.argtypes = [vp, vp, C.c_int]
@@ -529,6 +531,10 @@ class Mpnn:
                                             self._addr(x), C.byref(loss)))
         return loss.value
 
+    def backward(self, g: MpnnGraph, dz):
+        """Gradients from dL/dz of the last forward on the same graph."""
+        _check(lib().nds_mpnn_backward(self._h, C.byref(g), self._addr(dz)))
+
     def adam_step(self, lr: float, step: int, beta1=0.9, beta2=0.999, eps=1e-8):
         _check(lib().nds_mpnn_adam_step(self._h, C.c_float(lr), C.c_float(beta1), C.c_float(beta2), C.c_float(eps),
                                         int(step)))
@@ -553,6 +559,11 @@ def solver_stage_graph(solver: "Solver", nbr, ew, dscale):
 
 def solver_pressure_pair(solver: "Solver", rhs, x):
     _check(lib().nds_solver_pressure_pair(solver._h, Mpnn._addr(rhs), Mpnn._addr(x)))
+
+
+def solver_apply_operator(solver: "Solver", x, y):
+    """y = A x with the solver's current FP32 pressure operator (device arrays)."""
+    _check(lib().nds_solver_apply_operator(solver._h, Mpnn._addr(x), Mpnn._addr(y)))
 
 
 def solver_stage_counts(solver: "Solver"):

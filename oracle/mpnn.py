@@ -136,6 +136,18 @@ def loss_grad(p, nbr, ew, dscale, v, x, segs=None, exact=False):
         tt = max(np.sum(t[a:b] ** 2), 1e-300)
         loss += np.sum(d[a:b] ** 2) / tt / nseg
         dout[a:b] = 2.0 * d[a:b] / (tt * nseg)
+    return loss, _backward(c, dout), c
+
+
+def grad_from_dz(p, nbr, ew, dscale, v, dz, segs=None, exact=False):
+    """Parameter gradient of sum_i dz_i z_i (z = N(v)), i.e. the backward
+    pass from a given dL/dz: dout = dz sigma dscale."""
+    z, c = forward(p, nbr, ew, dscale, v, segs, exact)
+    return _backward(c, np.asarray(dz, dtype=np.float64) * c["sigma"] * c["dscale"]), c
+
+
+def _backward(c, dout):
+    P, nbr, ew = c["P"], c["nbr"], c["ew"]
     g = np.zeros(NPARAM)
     h, X = c["h"], c["X"]
     g[OFF_WD:OFF_WD + H] = dout @ h[3]
@@ -151,4 +163,4 @@ def loss_grad(p, nbr, ew, dscale, v, x, segs=None, exact=False):
     delta0 = dh * (c["pre0"] > 0)
     g[OFF_WE:OFF_WE + 2 * H] = (delta0.T @ c["f"]).ravel()
     g[OFF_BE:OFF_BE + H] = delta0.sum(axis=0)
-    return loss, g, c
+    return g

@@ -50,7 +50,9 @@ def face_graph(native, meshes, name):
 
 
 def _dev(torch, a):
-    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    t = torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    torch.cuda.synchronize()  # the library runs on its own streams
+    return t
 
 
 @pytest.mark.parametrize("mesh,segs", [("pipe_tiny", None), ("pipe_small", "two")])
@@ -70,6 +72,7 @@ def test_forward_matches_oracle(native, meshes, mesh, segs):
     g = net.graph(n, *keep)
     vd = _dev(torch, v)
     z = torch.zeros(n, dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
     net.forward(g, vd, z, seg)
     torch.cuda.synchronize()
     zo, cache = M.forward(p, nbr, ew, dscale, v, seg)
@@ -132,3 +135,33 @@ def test_adam_steps_reduce_the_loss(native, meshes):
         net.adam_step(2e-3, step)
         last = net.loss_backward(g, vd, xd)
     assert last < 0.7 * first, (first, last)
+
+
+def test_backward_from_dz_matches_oracle(native, meshes):
+    """nds_mpnn_backward (gradients from a given dL/dz, for losses evaluated
+    outside the network) against the oracle's backward from the same dz."""
+    import torch
+    from oracle import mpnn as M
+    nbr, ew, dscale = face_graph(native, meshes, "pipe_small")
+    n = len(nbr)
+    seg = [0, n // 3, n]
+    rng = np.random.default_rng(11)
+    v = rng.normal(size=n).astype(np.float32)
+    dz = rng.normal(size=n).astype(np.float32)
+    p = M.init_params(8)
+    net = native.Mpnn(n, training=True)
+    net.set_params(p)
+    keep = [_dev(torch, nbr), _dev(torch, ew), _dev(torch, dscale)]
+    g = net.graph(n, *keep)
+    vd, dzd = _dev(torch, v), _dev(torch, dz)
+    z = torch.zeros(n, dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    net.forward(g, vd, z, seg)
+    net.backward(g, dzd)
+    grads = net.grads()
+    go, _ = M.grad_from_dz(p, nbr, ew, dscale, v, dz, seg)
+    for l in (1, 2, 3):
+        o = M.off_w(l)
+        assert rel_l2(grads[o:o + 8192], go[o:o + 8192]) <= 2e-2, l
+    assert rel_l2(grads[M.OFF_WD:M.OFF_WD + 66], go[M.OFF_WD:M.OFF_WD + 66]) <= 2e-2
+    assert rel_l2(grads[:192], go[:192]) <= 2e-2
