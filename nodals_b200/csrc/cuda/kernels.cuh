@@ -237,6 +237,10 @@ struct MomArgs {
   const T* __restrict__ s0;
   const T* __restrict__ s1;
   const T* __restrict__ s2;
+  // fused form (no cell pass): C rows are evaluated per incidence
+  const T* __restrict__ invJ;           // 9 per cell
+  const T* __restrict__ det;            // 1 per cell
+  const T* __restrict__ centT;          // reference tensor T[8][8][8][3]
   T alpha_u, rau_scale;
   int row_cap;                          // shared row buffer length per group
   T* __restrict__ A;
@@ -249,7 +253,42 @@ struct MomArgs {
 };
 
 // 8 lanes per velocity row; lane b adds column b of each incident block.
+// Convection entries C_c[a][lane8] of one incidence (cell c, basis a), the
+// same expression and order as mom_cell_conv: lane m maps the velocity of
+// basis m by J^-1, the group shares the eight mapped velocities, lane b sums
+// over m.  ga: this lane's DOF of cell c (ref[8 c + lane8]).
 template <class T>
+__device__ __forceinline__ T conv_entry(const MomArgs<T>& g, const T* __restrict__ sT, int c, int a, int ga,
+                                        int lane8, unsigned gmask) {
+  T q0, q1, q2;
+  if (ga >= 0) {
+    q0 = g.u0[kVel * (size_t)ga];
+    q1 = g.u1[kVel * (size_t)ga];
+    q2 = g.u2[kVel * (size_t)ga];
+  } else {
+    const T* f = g.fixed + 3 * (size_t)(-ga - 1);
+    q0 = f[0];
+    q1 = f[1];
+    q2 = f[2];
+  }
+  const T* I = g.invJ + 9 * (size_t)c;
+  const T r0 = q0 * I[0] + q1 * I[1] + q2 * I[2];
+  const T r1 = q0 * I[3] + q1 * I[4] + q2 * I[5];
+  const T r2 = q0 * I[6] + q1 * I[7] + q2 * I[8];
+  T cv = 0;
+#pragma unroll
+  for (int m = 0; m < 8; ++m) {
+    const T w0 = __shfl_sync(gmask, r0, m, 8), w1 = __shfl_sync(gmask, r1, m, 8), w2 = __shfl_sync(gmask, r2, m, 8);
+    const T* t = sT + ((a * 8 + m) * 8 + lane8) * 3;
+    cv += w0 * t[0] + w1 * t[1] + w2 * t[2];
+  }
+  return cv * g.det[c];
+}
+
+// FUSED: C rows evaluated per incidence (conv_entry) instead of read from the
+// cell pass's blocks; the reference tensor is staged in shared memory after
+// the row buffers.
+template <class T, bool FUSED = false>
 __global__ void __launch_bounds__(kBlock) mom_assemble(MomArgs<T> g) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* sRow = reinterpret_cast<T*>(smem_raw);  // groups * row_cap
@@ -258,6 +297,11 @@ __global__ void __launch_bounds__(kBlock) mom_assemble(MomArgs<T> g) {
   const int grp = tid >> 3;
   const int groups = blockDim.x >> 3;
   T* buf = sRow + (size_t)grp * g.row_cap;
+  T* sT = sRow + (size_t)groups * g.row_cap;
+  if (FUSED) {
+    for (int k = tid; k < 1536; k += blockDim.x) sT[k] = g.centT[k];
+    __syncthreads();
+  }
   const unsigned gmask = group8_mask();
   for (int i = blockIdx.x * groups + grp; i < g.nrows; i += gridDim.x * groups) {
     const int rb = g.row[i], re = g.row[i + 1], len = re - rb;
@@ -265,7 +309,32 @@ __global__ void __launch_bounds__(kBlock) mom_assemble(MomArgs<T> g) {
     __syncwarp(gmask);
     T conv0 = 0, conv1 = 0, conv2 = 0, bt0 = 0, bt1 = 0, bt2 = 0;
     const int z0 = g.inc_off[i], z1 = g.inc_off[i + 1];
-    for (int z = z0; z < z1; z += 2) {
+    if (FUSED) {
+      for (int z = z0; z < z1; ++z) {
+        const uint32_t pa = g.inc[z];
+        const int ca = (int)(pa >> 3), aa = (int)(pa & 7u);
+        const int ga = g.ref[8 * (size_t)ca + lane8];
+        const int sa = g.slot[64 * (size_t)ca + 8 * aa + lane8];
+        const T va = conv_entry<T>(g, sT, ca, aa, ga, lane8, gmask);
+        if (ga >= 0) {
+          buf[sa] += va;
+        } else {
+          const T* f = g.fixed + 3 * (size_t)(-ga - 1);
+          conv0 -= va * f[0];
+          conv1 -= va * f[1];
+          conv2 -= va * f[2];
+        }
+        if (lane8 == 0) {
+          const T pv = g.p[ca];
+          const T* B = g.bco + 24 * (size_t)ca + 3 * aa;
+          bt0 += B[0] * pv;
+          bt1 += B[1] * pv;
+          bt2 += B[2] * pv;
+        }
+        __syncwarp(gmask);
+      }
+    }
+    for (int z = z0; z < (FUSED ? z0 : z1); z += 2) {
       // two incidences in flight; applied in order
       const bool two = z + 1 < z1;
       const uint32_t pa = g.inc[z], pb = two ? g.inc[z + 1] : pa;

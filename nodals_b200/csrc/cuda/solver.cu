@@ -370,7 +370,11 @@ class Solver final : public ISolver {
     mom_smem_ = (size_t)(kBlock / 8) * row_cap_ * sizeof(T);
     if (mom_smem_ > 200 * 1024) throw std::runtime_error("momentum row too long for the shared-memory assembly buffer");
     NDS_CUDA(cudaFuncSetAttribute(k::mom_assemble<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mom_smem_));
-    cconv_.alloc(64 * (size_t)nc_);
+    NDS_CUDA(cudaFuncSetAttribute(k::mom_assemble<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(mom_smem_ + 1536 * sizeof(T))));
+    // the cell blocks of the two-pass assembly (SUPG, or NDS_TWO_PASS_ASSEMBLY=1)
+    fused_assembly_ = !o_.supg && std::getenv("NDS_TWO_PASS_ASSEMBLY") == nullptr;
+    if (!fused_assembly_) cconv_.alloc(64 * (size_t)nc_);
 
     if (o_.supg) {
       h2_.upload(S.h2);
@@ -1849,7 +1853,16 @@ class Solver final : public ISolver {
     a.b0 = b_[0].p;
     a.b1 = b_[1].p;
     a.b2 = b_[2].p;
+    a.invJ = invJ_.p;
+    a.det = det_.p;
+    a.centT = centT_.p;
     ProfScope ps(prof, st_, P_ASSEMBLE);
+    if (!o_.supg && fused_assembly_) {
+      // one pass: each incidence's convection row is evaluated in place
+      k::mom_assemble<T, true><<<grid_for(nv_, kBlock / 8), kBlock, mom_smem_ + 1536 * sizeof(T), st_>>>(a);
+      NDS_LAUNCH();
+      return;
+    }
     // cell blocks: a grid of 8 blocks per SM amortises the shared tensor load
     k::SupgArgs sa{P_.setup.pipe.nu, o_.supg_tau_scale, o_.supg_magic};
     const int gc = std::min(grid_for(nc_, kBlock / 8), 8 * 148);
@@ -2177,6 +2190,7 @@ class Solver final : public ISolver {
   size_t mom_smem_ = 0, refresh_smem_ = 0;
   double cont0_ = -1, cont_rel_ = 1, fine_lambda_ = 1, p_cheb_lambda_ = 1;
   bool finite_all_ = true;
+  bool fused_assembly_ = true;
   std::vector<double> level_lambda_;
   // momentum
   DBuf<int32_t> mrow_, mcol_, mdpos_, inc_off_, ref_, color_rows_;

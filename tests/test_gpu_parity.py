@@ -187,3 +187,22 @@ def test_sell_column_formats_agree(native, meshes, monkeypatch):
         assert a.p_its == b.p_its and a.rel_cont == b.rel_cont
     for x, y in zip(A.fields(), B.fields()):
         assert np.array_equal(x, y)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_fused_assembly_matches_two_pass(native, meshes, monkeypatch, precision):
+    """The one-pass assembly (convection rows evaluated per incidence) and the
+    two-pass one (cell blocks written, then gathered by rows) evaluate every
+    entry with the same expression in the same order: equal pressure
+    iteration counts and relCont and fields to 1e-13."""
+    P = _make(native, meshes, "pipe_small", precision=precision, **ORACLE_CASES["sa_pcg"])
+    A = native.Solver(P)
+    monkeypatch.setenv("NDS_TWO_PASS_ASSEMBLY", "1")
+    B = native.Solver(P)
+    for _ in range(6):
+        a, b = A.step(), B.step()
+        assert a.p_its == b.p_its, (a.it, a.p_its, b.p_its)
+        assert abs(a.rel_cont - b.rel_cont) <= 1e-13 * abs(b.rel_cont)
+    for x, y in zip(A.fields(), B.fields()):
+        assert rel_l2(x, y) <= 1e-13
