@@ -529,8 +529,15 @@ __global__ void __launch_bounds__(kBlock) continuity(int nc, const int32_t* __re
 // per lane: columns and values, then the x gathers) covers a row of up to
 // 256 entries, so a row costs three dependent round trips (row bounds,
 // columns and values, gathers).  Longer rows take further rounds.
-template <int G, class T>
-__device__ __forceinline__ T lane_batched_dot(int rb, int re, const int32_t* __restrict__ ci, const T* __restrict__ v,
+// MT: the stored value type (T, or __half for an FP16 copy of a level whose
+// values are scaled by a power of two; the caller multiplies the row sum back)
+template <class T, class MT>
+__device__ __forceinline__ T load_val(const MT* __restrict__ v, int k) {
+  if constexpr (std::is_same<MT, __half>::value) return (T)__half2float(v[k]);
+  else return v[k];
+}
+template <int G, class T, class MT = T>
+__device__ __forceinline__ T lane_batched_dot(int rb, int re, const int32_t* __restrict__ ci, const MT* __restrict__ v,
                                               const T* __restrict__ x, int lane) {
   T s = 0;
   for (int k0 = rb + lane; k0 < re; k0 += 8 * G) {
@@ -540,7 +547,7 @@ __device__ __forceinline__ T lane_batched_dot(int rb, int re, const int32_t* __r
     for (int u = 0; u < 8; ++u) {
       const int k = k0 + u * G;
       c[u] = k < re ? ci[k] : -1;
-      a[u] = k < re ? v[k] : T(0);
+      a[u] = k < re ? load_val<T, MT>(v, k) : T(0);
     }
     T xv[8];
 #pragma unroll
@@ -552,34 +559,37 @@ __device__ __forceinline__ T lane_batched_dot(int rb, int re, const int32_t* __r
   return s;
 }
 constexpr int kRowLanes = 32;
-template <class T>
+template <class T, class MT = T>
 __device__ __forceinline__ T group_row_dot(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
-                                           const T* __restrict__ v, const T* __restrict__ x, int i, int lane,
-                                           unsigned mask) {
-  return group_sum<kRowLanes>(lane_batched_dot<kRowLanes>(rp[i], rp[i + 1], ci, v, x, lane), mask);
+                                           const MT* __restrict__ v, const T* __restrict__ x, int i, int lane,
+                                           unsigned mask, T vinv = T(1)) {
+  T s = group_sum<kRowLanes>(lane_batched_dot<kRowLanes, T, MT>(rp[i], rp[i + 1], ci, v, x, lane), mask);
+  if constexpr (!std::is_same<MT, T>::value) s *= vinv;
+  return s;
 }
 
 // y = A x
-template <class T>
+template <class T, class MT = T>
 __global__ void __launch_bounds__(kBlock) spmv(int n, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
-                                               const T* __restrict__ v, const T* __restrict__ x, T* __restrict__ y) {
+                                               const MT* __restrict__ v, const T* __restrict__ x, T* __restrict__ y,
+                                               T vinv = T(1)) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = t / kRowLanes, lane = t % kRowLanes;
   if (i >= n) return;
-  const T s = group_row_dot(rp, ci, v, x, i, lane, group_mask<kRowLanes>());
+  const T s = group_row_dot<T, MT>(rp, ci, v, x, i, lane, group_mask<kRowLanes>(), vinv);
   if (lane == 0) y[i] = s;
 }
 
 // r = b - A x  (optionally also r2 = r)
-template <class T>
+template <class T, class MT = T>
 __global__ void __launch_bounds__(kBlock) spmv_resid(int n, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
-                                                     const T* __restrict__ v, const T* __restrict__ x,
+                                                     const MT* __restrict__ v, const T* __restrict__ x,
                                                      const T* __restrict__ b, T* __restrict__ r, T* __restrict__ r2,
-                                                     const T* __restrict__ den, T w) {
+                                                     const T* __restrict__ den, T w, T vinv = T(1)) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = t / kRowLanes, lane = t % kRowLanes;
   if (i >= n) return;
-  const T s = group_row_dot(rp, ci, v, x, i, lane, group_mask<kRowLanes>());
+  const T s = group_row_dot<T, MT>(rp, ci, v, x, i, lane, group_mask<kRowLanes>(), vinv);
   if (lane == 0) {
     // r; r2 = r (den null) or the first Jacobi step w r / den
     const T q = b[i] - s;
@@ -590,16 +600,16 @@ __global__ void __launch_bounds__(kBlock) spmv_resid(int n, const int32_t* __res
 }
 
 // Jacobi-type smoothing step: x_out = x_in + w (b - A x_in) / den
-template <class T>
+template <class T, class MT = T>
 __global__ void __launch_bounds__(kBlock) spmv_smooth(int n, const int32_t* __restrict__ rp,
-                                                      const int32_t* __restrict__ ci, const T* __restrict__ v,
+                                                      const int32_t* __restrict__ ci, const MT* __restrict__ v,
                                                       const T* __restrict__ xin, const T* __restrict__ b,
                                                       const T* __restrict__ den, T w, T* __restrict__ xout,
-                                                      T* __restrict__ add_to) {
+                                                      T* __restrict__ add_to, T vinv = T(1)) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = t / kRowLanes, lane = t % kRowLanes;
   if (i >= n) return;
-  const T s = group_row_dot(rp, ci, v, xin, i, lane, group_mask<kRowLanes>());
+  const T s = group_row_dot<T, MT>(rp, ci, v, xin, i, lane, group_mask<kRowLanes>(), vinv);
   if (lane == 0) {
     // with add_to the step is added to add_to instead of stored in xout
     const T r = b[i] - s;

@@ -285,6 +285,9 @@ class Solver final : public ISolver {
     DBuf<int32_t> row, col, crows;
     std::vector<int> coff;
     DBuf<TA> val, diag, l1, b, x, r, tmp, corr, pong;
+    // amg_half: FP16 copy of the level's CSR values, scaled by 1 / hinv
+    DBuf<__half> hval;
+    double hinv = 1.0;
   };
   struct Xfer {  // P (fine rows, ELL k-major) and R = P^T (coarse rows, CSR)
     int nf = 0, nc = 0, pw = 0;
@@ -570,6 +573,9 @@ class Solver final : public ISolver {
       }
       Lv.l1.upload(l1h);
       for (auto* b : {&Lv.b, &Lv.x, &Lv.r, &Lv.tmp, &Lv.corr, &Lv.pong}) b->alloc((size_t)A.n);
+      // the mixed path's V-cycle reads FP16 copies of the explicit levels
+      // (the terminal level goes through its dense inverse)
+      if (!kSame && o_.precision == NDS_MIXED && o_.amg_half && l + 1 < H.A.size()) level_to_half(Lv, A);
       if (o_.amg_smoother == NDS_SM_MCGS && l + 1 < H.A.size()) {
         std::vector<int32_t> rows;
         std::vector<int32_t> r32 = to_i32(A.row, "AMG level CSR");
@@ -866,12 +872,34 @@ class Solver final : public ISolver {
     return A;
   }
   OpView<TA> level_op(const Level& A) const {
-    return {A.n, false, k::Sell{}, A.row.p, A.col.p, A.val.p, P_COARSE_SPMV};
+    OpView<TA> V{A.n, false, k::Sell{}, A.row.p, A.col.p, A.val.p, P_COARSE_SPMV};
+    if (A.hval.p) {
+      V.vh = A.hval.p;
+      V.vinv = A.hinv;
+    }
+    return V;
+  }
+  // FP16 copy of an explicit level's CSR values (a setup snapshot), scaled by
+  // the power of two that puts its largest diagonal at 2^11
+  void level_to_half(Level& Lv, const CsrHost& A) {
+    double dmax = 0.0;
+    for (double d : A.diag) dmax = std::max(dmax, std::abs(d));
+    if (!(dmax > 0.0) || !std::isfinite(dmax)) throw std::runtime_error("FP16 level copy: no positive diagonal");
+    const double scale = std::ldexp(1.0, (int)std::floor(std::log2(2048.0 / dmax)));
+    std::vector<__half> hv(A.val.size());
+    for (size_t k = 0; k < hv.size(); ++k)
+      hv[k] = __float2half((float)std::min(std::max(A.val[k] * scale, -65504.0), 65504.0));
+    Lv.hval.alloc(hv.size());
+    NDS_CUDA(cudaMemcpy(Lv.hval.p, hv.data(), hv.size() * sizeof(__half), cudaMemcpyHostToDevice));
+    Lv.hinv = 1.0 / scale;
   }
   template <class V>
   void op_spmv(const OpView<V>& A, const V* x, V* y) {
     ProfScope ps(prof, st_, A.cat);
     if (A.sell) sell_launch<k::SELL_Y, V>(A, grid_for(A.n), x, nullptr, nullptr, 0.0, y, nullptr);
+    else if (A.vh && std::is_same<V, float>::value)
+      k::spmv<V, __half><<<grid_for((long long)A.n * k::kRowLanes), kBlock, 0, st_>>>(A.n, A.rp, A.ci, A.vh, x, y,
+                                                                                      V(A.vinv));
     else k::spmv<V><<<grid_for((long long)A.n * k::kRowLanes), kBlock, 0, st_>>>(A.n, A.rp, A.ci, A.v, x, y);
     NDS_LAUNCH();
   }
@@ -881,6 +909,9 @@ class Solver final : public ISolver {
                 double w = 0.0) {
     ProfScope ps(prof, st_, A.cat);
     if (A.sell) sell_launch<k::SELL_RESID, V>(A, grid_for(A.n), x, b, den, w, r, r2);
+    else if (A.vh && std::is_same<V, float>::value)
+      k::spmv_resid<V, __half><<<grid_for((long long)A.n * k::kRowLanes), kBlock, 0, st_>>>(
+          A.n, A.rp, A.ci, A.vh, x, b, r, r2, den, V(w), V(A.vinv));
     else
       k::spmv_resid<V><<<grid_for((long long)A.n * k::kRowLanes), kBlock, 0, st_>>>(A.n, A.rp, A.ci, A.v, x, b, r, r2, den, V(w));
     NDS_LAUNCH();
@@ -890,6 +921,9 @@ class Solver final : public ISolver {
   void op_smooth(const OpView<V>& A, const V* xin, const V* b, const V* den, double w, V* xout, V* add_to = nullptr) {
     ProfScope ps(prof, st_, A.cat);
     if (A.sell) sell_launch<k::SELL_SMOOTH, V>(A, grid_for(A.n), xin, b, den, w, xout, add_to);
+    else if (A.vh && std::is_same<V, float>::value)
+      k::spmv_smooth<V, __half><<<grid_for((long long)A.n * k::kRowLanes), kBlock, 0, st_>>>(
+          A.n, A.rp, A.ci, A.vh, xin, b, den, V(w), xout, add_to, V(A.vinv));
     else
       k::spmv_smooth<V><<<grid_for((long long)A.n * k::kRowLanes), kBlock, 0, st_>>>(A.n, A.rp, A.ci, A.v, xin, b, den, V(w), xout,
                                                                           add_to);
