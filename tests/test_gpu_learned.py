@@ -5,8 +5,9 @@
   run bit for bit (z = V(v) + 0).
 * The trained parameters (nodals_b200/stage/mpnn_params.bin) on a held-out
   member of the seeded pipe family: every pressure solve meets the same FP64
-  target p_rtol as the plain solve, the fields follow the plain run to 1e-6,
-  the stage is applied (not all fallbacks), and it takes fewer pressure
+  target p_rtol as the plain solve, so after 20 SIMPLE iterations the fields
+  follow the plain run to 1e-5 (each solve differs within its tolerance), the
+  stage is kept at most applications, and it takes fewer pressure
   iterations than the plain V-cycle.
 """
 from __future__ import annotations
@@ -59,9 +60,10 @@ def test_trained_stage_on_held_out_pipe(native):
                                                 dict(geom_from_inlet=1, amg_terminal=300))
     applied, fallbacks = counts
     assert applied > 0 and fallbacks < applied
+    assert fallbacks <= applied // 10
     for a, b in zip(plain, stage):
         assert a.p_rel <= 1e-6 and b.p_rel <= 1e-6
-        assert abs(a.rel_cont - b.rel_cont) <= 1e-5 * abs(a.rel_cont)
+        assert abs(a.rel_cont - b.rel_cont) <= 1e-4 * abs(a.rel_cont)
     for x, y in zip(fp, fs):
-        assert rel_l2(y, x) <= 1e-6
+        assert rel_l2(y, x) <= 1e-5
     assert sum(b.p_its for b in stage) < sum(a.p_its for a in plain)
