@@ -220,7 +220,7 @@ __global__ void __launch_bounds__(kBlock) mom_cell_conv(int nc, const int32_t* _
 template <class T>
 struct MomArgs {
   int nrows;
-  const int32_t* __restrict__ row;      // momentum CSR (int32 offsets)
+  const int2* __restrict__ span;        // row i's (begin, end) in the colour-ordered storage
   const int32_t* __restrict__ dpos;     // diagonal position (absolute)
   const T* __restrict__ K;              // persistent diffusion values
   const int32_t* __restrict__ inc_off;  // row -> incident (cell,a)
@@ -285,10 +285,17 @@ __device__ __forceinline__ T conv_entry(const MomArgs<T>& g, const T* __restrict
   return cv * g.det[c];
 }
 
-// FUSED: C rows evaluated per incidence (conv_entry) instead of read from the
-// cell pass's blocks; the reference tensor is staged in shared memory after
-// the row buffers.
-template <class T, bool FUSED = false>
+// FUSED (1 or 2): C rows evaluated per incidence (conv_entry) instead of
+// read from the cell pass's blocks; the reference tensor is staged in shared
+// memory after the row buffers.  FUSED 2 keeps the loads of the next
+// incidence in flight while the current one is evaluated: the row's
+// incidence codes are loaded up front (lane l holds those of incidences l,
+// l + 8 and l + 16, broadcast by shuffles; codes past the 24th are loaded
+// when needed), and the next incidence's DOF and slot are fetched before
+// the current convection row is computed.  Both forms add the same values in
+// the same order.
+constexpr int kIncAhead = 24;
+template <class T, int FUSED = 0>
 __global__ void __launch_bounds__(kBlock) mom_assemble(MomArgs<T> g) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* sRow = reinterpret_cast<T*>(smem_raw);  // groups * row_cap
@@ -304,12 +311,64 @@ __global__ void __launch_bounds__(kBlock) mom_assemble(MomArgs<T> g) {
   }
   const unsigned gmask = group8_mask();
   for (int i = blockIdx.x * groups + grp; i < g.nrows; i += gridDim.x * groups) {
-    const int rb = g.row[i], re = g.row[i + 1], len = re - rb;
+    const int2 sp = g.span[i];
+    const int rb = sp.x, len = sp.y - sp.x;
     for (int k = lane8; k < len; k += 8) buf[k] = g.K[rb + k];
     __syncwarp(gmask);
     T conv0 = 0, conv1 = 0, conv2 = 0, bt0 = 0, bt1 = 0, bt2 = 0;
     const int z0 = g.inc_off[i], z1 = g.inc_off[i + 1];
-    if (FUSED) {
+    if (FUSED == 2) {
+      const int ninc = z1 - z0;
+      uint32_t code[kIncAhead / 8];
+#pragma unroll
+      for (int t = 0; t < kIncAhead / 8; ++t) code[t] = lane8 + 8 * t < ninc ? g.inc[z0 + lane8 + 8 * t] : 0u;
+      auto code_of = [&](int zz) -> uint32_t {  // zz is uniform over the group
+        if (zz >= kIncAhead) return g.inc[z0 + zz];
+        const uint32_t v = zz < 8 ? code[0] : (zz < 16 ? code[1] : code[2]);
+        return __shfl_sync(gmask, v, zz & 7, 8);
+      };
+      uint32_t npa = 0;
+      int nga = 0, nsa = 0;
+      if (ninc > 0) {
+        npa = code_of(0);
+        nga = g.ref[8 * (size_t)(npa >> 3) + lane8];
+        nsa = g.slot[64 * (size_t)(npa >> 3) + 8 * (npa & 7u) + lane8];
+      }
+      for (int zz = 0; zz < ninc; ++zz) {
+        const uint32_t pa = npa;
+        const int ga = nga, sa = nsa;
+        if (zz + 1 < ninc) {
+          npa = code_of(zz + 1);
+          nga = g.ref[8 * (size_t)(npa >> 3) + lane8];
+          nsa = g.slot[64 * (size_t)(npa >> 3) + 8 * (npa & 7u) + lane8];
+        }
+        const int ca = (int)(pa >> 3), aa = (int)(pa & 7u);
+        T pv = 0, B0 = 0, B1 = 0, B2 = 0;
+        if (lane8 == 0) {
+          pv = g.p[ca];
+          const T* B = g.bco + 24 * (size_t)ca + 3 * aa;
+          B0 = B[0];
+          B1 = B[1];
+          B2 = B[2];
+        }
+        const T va = conv_entry<T>(g, sT, ca, aa, ga, lane8, gmask);
+        if (ga >= 0) {
+          buf[sa] += va;
+        } else {
+          const T* f = g.fixed + 3 * (size_t)(-ga - 1);
+          conv0 -= va * f[0];
+          conv1 -= va * f[1];
+          conv2 -= va * f[2];
+        }
+        if (lane8 == 0) {
+          bt0 += B0 * pv;
+          bt1 += B1 * pv;
+          bt2 += B2 * pv;
+        }
+        __syncwarp(gmask);
+      }
+    }
+    if (FUSED == 1) {
       for (int z = z0; z < z1; ++z) {
         const uint32_t pa = g.inc[z];
         const int ca = (int)(pa >> 3), aa = (int)(pa & 7u);
@@ -404,8 +463,17 @@ __global__ void __launch_bounds__(kBlock) mom_assemble(MomArgs<T> g) {
 
 // One multicolour Gauss-Seidel colour pass on the shared momentum matrix,
 // three right-hand sides (g5e_fp32_kernels.cuh:106-116).  8 lanes per row.
-// rows: the colour's rows; span: their (begin, end) in the CSR, in the same
-// order, so the row's entries and its own data load in parallel.
+// The matrix is stored colour by colour (the rows of one colour contiguous,
+// each colour's rows in ascending order), so one pass streams one block of
+// the matrix; span: the storage range of each of the colour's rows (pad
+// entries have the row's own column), rows: their natural indices (their
+// right-hand sides, diagonals and unknowns).
+// Each lane takes its entries kGsAhead at a time: it loads their columns and
+// values, then gathers their unknowns, so a batch's loads are in flight
+// together; the diagonal entry and the padding of a batch contribute 0.
+// Per lane the entries are summed in the order of the storage, then over
+// the 8 lanes.
+constexpr int kGsAhead = 3;
 template <class T>
 __global__ void __launch_bounds__(kBlock) mom_gs_color(int count, const int32_t* __restrict__ rows,
                                                        const int2* __restrict__ span, const int32_t* __restrict__ ci,
@@ -419,6 +487,7 @@ __global__ void __launch_bounds__(kBlock) mom_gs_color(int count, const int32_t*
   const unsigned gmask = group8_mask();
   const int i = rows[q];
   const int2 sp = span[q];
+  const int kb = sp.x, ke = sp.y;
   T d = 0, c0 = 0, c1 = 0, c2 = 0, y0 = 0, y1 = 0, y2 = 0;
   const size_t vi = kVel * (size_t)i;
   if (lane8 == 0) {
@@ -431,14 +500,23 @@ __global__ void __launch_bounds__(kBlock) mom_gs_color(int count, const int32_t*
     y2 = x2[vi];
   }
   T s0 = 0, s1 = 0, s2 = 0;
-  for (int k = sp.x + lane8; k < sp.y; k += 8) {
-    const int j = ci[k];
-    if (j == i) continue;
-    const T a = av[k];
-    const size_t vj = kVel * (size_t)j;
-    s0 += a * x0[vj];
-    s1 += a * x1[vj];
-    s2 += a * x2[vj];
+  for (int k0 = kb + lane8; k0 < ke; k0 += 8 * kGsAhead) {
+    int jj[kGsAhead];
+    T aa[kGsAhead];
+#pragma unroll
+    for (int u = 0; u < kGsAhead; ++u) {
+      const int k = k0 + 8 * u;
+      jj[u] = k < ke ? ci[k] : i;
+      aa[u] = k < ke ? av[k] : T(0);
+    }
+#pragma unroll
+    for (int u = 0; u < kGsAhead; ++u) {
+      const T a = jj[u] == i ? T(0) : aa[u];
+      const size_t vj = kVel * (size_t)jj[u];
+      s0 += a * x0[vj];
+      s1 += a * x1[vj];
+      s2 += a * x2[vj];
+    }
   }
   s0 = group_sum<8>(s0, gmask);
   s1 = group_sum<8>(s1, gmask);
@@ -453,7 +531,7 @@ __global__ void __launch_bounds__(kBlock) mom_gs_color(int count, const int32_t*
 
 // ||b_d||^2 and ||b_d - A u_d||^2 (g5e_fp32_kernels.cuh:117-126); 6 partials per block.
 template <class T>
-__global__ void __launch_bounds__(kBlock) mom_audit(int n, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+__global__ void __launch_bounds__(kBlock) mom_audit(int n, const int2* __restrict__ span, const int32_t* __restrict__ ci,
                                                     const T* __restrict__ av, const T* __restrict__ b0,
                                                     const T* __restrict__ b1, const T* __restrict__ b2,
                                                     const T* __restrict__ x0, const T* __restrict__ x1,
@@ -464,7 +542,8 @@ __global__ void __launch_bounds__(kBlock) mom_audit(int n, const int32_t* __rest
   const int groups_total = (gridDim.x * blockDim.x) >> 3;
   for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 3; i < n; i += groups_total) {
     T a0 = 0, a1 = 0, a2 = 0;
-    for (int k = rp[i] + lane8; k < rp[i + 1]; k += 8) {
+    const int2 sp = span[i];
+    for (int k = sp.x + lane8; k < sp.y; k += 8) {
       const size_t vj = kVel * (size_t)ci[k];
       const T a = av[k];
       a0 += a * x0[vj];
@@ -922,6 +1001,29 @@ __device__ __forceinline__ T sell_row(const Sell& A, const MT* __restrict__ v, c
   const int w8 = w & ~7, wp = (w + 3) & ~3;
   T s0 = 0, s1 = 0;
   int k = 0;
+  if constexpr (std::is_same<MT, __half>::value) {
+    // the FP16 copy moves 4 B per entry: 16 entries in flight per thread
+    // keep as many bytes in flight as 8 entries of the wider formats
+    const int w16 = w & ~15;
+    for (; k < w16; k += 16) {
+      int j[16];
+      T a[16];
+#pragma unroll
+      for (int g4 = 0; g4 < 4; ++g4) {
+        const int o = sell_offset(b, lane, k + 4 * g4);
+        sell_col4<D16>(A, o, i, j + 4 * g4);
+        sell_vals4<T, MT>(v, o, a + 4 * g4);
+      }
+      T xv[16];
+#pragma unroll
+      for (int u = 0; u < 16; ++u) xv[u] = x[j[u]];
+#pragma unroll
+      for (int u = 0; u < 16; u += 2) {
+        s0 += a[u] * xv[u];
+        s1 += a[u + 1] * xv[u + 1];
+      }
+    }
+  }
   for (; k < w8; k += 8) {
     int j[8];
     T a[8];
@@ -1055,6 +1157,10 @@ __global__ void __launch_bounds__(kRefreshBlock) sell_refresh(int nc, const int3
   const int c = slice * 32 + r;
   const bool live_row = c < nc;
   int qb = 0, qe = 0, ds = -1;
+  // the code word and factor of this lane's contribution in the next chunk,
+  // loaded one chunk ahead (the first chunk's loads overlap the rAU staging)
+  unsigned vn = 0xFFFFu;
+  T gn = 0;
   if (live_row) {
     if (lane < 8) {
       const int g = ref[8 * (size_t)c + lane];
@@ -1063,17 +1169,23 @@ __global__ void __launch_bounds__(kRefreshBlock) sell_refresh(int nc, const int3
     qb = coff[c];
     qe = coff[c + 1];
     ds = dslot[c];
+    if (qb + lane < qe) {
+      vn = cs[qb + lane];
+      gn = G[qb + lane];
+    }
   }
   __syncthreads();  // image zeroed, rAU of every row staged
   T asum = 0;
   for (int q0 = qb; q0 < qe; q0 += 32) {  // warp-uniform bounds
-    const int q = q0 + lane;
-    unsigned v = 0xFFFFu;
-    T p = 0;
-    if (q < qe) {
-      v = cs[q];
-      if (v != 0xFFFFu) p = sR[r][v & 7u] * G[q];
+    const unsigned v = vn;
+    const T gq = gn;
+    vn = 0xFFFFu;
+    gn = 0;
+    if (q0 + 32 + lane < qe) {
+      vn = cs[q0 + 32 + lane];
+      gn = G[q0 + 32 + lane];
     }
+    const T p = v != 0xFFFFu ? sR[r][v & 7u] * gq : T(0);
     const bool real = v != 0xFFFFu;
     const int pos = real ? (int)((v >> 3) & 7u) : 0;
     const int maxpos = __reduce_max_sync(0xffffffffu, pos);

@@ -325,11 +325,50 @@ class Solver final : public ISolver {
     StageTimer tm("device_upload");
     nc_ = S.nc;
     nv_ = S.nv;
-    mrow_.upload(to_i32(S.mom.row, "momentum CSR"));
-    mcol_.upload(S.mom.col);
-    mdpos_.upload(S.mom_diag_pos);
-    K_.upload(S.mom.val);
-    A_.alloc(S.mom.col.size());
+    {
+      // The momentum matrix is stored colour by colour: the Gauss-Seidel
+      // pass of one colour then streams one contiguous block.  Each row
+      // starts on a 32-byte boundary and is padded to a whole number of
+      // 32-byte sectors (pad entries: column = the row itself, value 0), so
+      // the assembly, which visits the rows in their natural order, writes
+      // whole sectors.  The assembly and the audit address row i through
+      // its span; the pads add zeros, so every value and sum is the one of
+      // the natural order.  NDS_MOM_NATURAL_ORDER=1 keeps the natural CSR.
+      const bool natural = std::getenv("NDS_MOM_NATURAL_ORDER") != nullptr;
+      const int64_t pad = natural ? 1 : (int64_t)(32 / sizeof(T));
+      int64_t nz = natural ? S.mom.row[(size_t)nv_] : 0;
+      std::vector<int64_t> pos(natural ? 0 : (size_t)nv_);
+      for (int q = 0; q < nv_ && !natural; ++q) {
+        const int i = S.color_rows[(size_t)q];
+        const int64_t len = S.mom.row[(size_t)i + 1] - S.mom.row[(size_t)i];
+        pos[(size_t)i] = nz;
+        nz += (len + pad - 1) / pad * pad;
+      }
+      if (nz > (int64_t)INT32_MAX) throw std::runtime_error("momentum CSR exceeds int32 offsets");
+      std::vector<int32_t> col((size_t)nz), dpos((size_t)nv_);
+      std::vector<int2> span((size_t)nv_);
+      std::vector<T> kv((size_t)nz, T(0));
+      for (int i = 0; i < nv_; ++i) {
+        const int64_t rb = S.mom.row[(size_t)i], re = S.mom.row[(size_t)i + 1];
+        const int64_t cb = natural ? rb : pos[(size_t)i];
+        const int64_t ce = natural ? re : cb + (re - rb + pad - 1) / pad * pad;
+        span[(size_t)i] = make_int2((int)cb, (int)ce);
+        dpos[(size_t)i] = (int32_t)(cb + (S.mom_diag_pos[(size_t)i] - rb));
+        for (int64_t k = rb; k < re; ++k) {
+          col[(size_t)(cb + (k - rb))] = S.mom.col[(size_t)k];
+          kv[(size_t)(cb + (k - rb))] = (T)S.mom.val[(size_t)k];
+        }
+        for (int64_t k = cb + (re - rb); k < ce; ++k) col[(size_t)k] = i;
+      }
+      std::vector<int2> gspan((size_t)nv_);
+      for (int q = 0; q < nv_; ++q) gspan[(size_t)q] = span[(size_t)S.color_rows[(size_t)q]];
+      mspan_.upload(span);
+      gspan_.upload(gspan);
+      mcol_.upload(col);
+      mdpos_.upload(dpos);
+      K_.upload(kv);
+      A_.alloc((size_t)nz);
+    }
     diag_.alloc((size_t)nv_);
     delta_.alloc((size_t)nv_);
     rau_.upload(S.init_rau);
@@ -354,14 +393,6 @@ class Solver final : public ISolver {
     color_rows_.upload(S.color_rows);
     color_off_ = S.color_off;
     {
-      std::vector<int2> span(S.color_rows.size());
-      for (size_t q = 0; q < span.size(); ++q) {
-        const int i = S.color_rows[q];
-        span[q] = make_int2((int)S.mom.row[(size_t)i], (int)S.mom.row[(size_t)i + 1]);
-      }
-      color_span_.upload(span);
-    }
-    {
       const RefTensors& RT = ref_tensors();
       std::vector<double> t(1536);
       std::memcpy(t.data(), &RT.T[0][0][0][0], sizeof(double) * 1536);
@@ -373,10 +404,13 @@ class Solver final : public ISolver {
     mom_smem_ = (size_t)(kBlock / 8) * row_cap_ * sizeof(T);
     if (mom_smem_ > 200 * 1024) throw std::runtime_error("momentum row too long for the shared-memory assembly buffer");
     NDS_CUDA(cudaFuncSetAttribute(k::mom_assemble<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mom_smem_));
-    NDS_CUDA(cudaFuncSetAttribute(k::mom_assemble<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    NDS_CUDA(cudaFuncSetAttribute(k::mom_assemble<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(mom_smem_ + 1536 * sizeof(T))));
+    NDS_CUDA(cudaFuncSetAttribute(k::mom_assemble<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)(mom_smem_ + 1536 * sizeof(T))));
     // the cell blocks of the two-pass assembly (SUPG, or NDS_TWO_PASS_ASSEMBLY=1)
     fused_assembly_ = !o_.supg && std::getenv("NDS_TWO_PASS_ASSEMBLY") == nullptr;
+    serial_assembly_ = std::getenv("NDS_SERIAL_ASSEMBLY") != nullptr;
     if (!fused_assembly_) cconv_.alloc(64 * (size_t)nc_);
 
     if (o_.supg) {
@@ -1860,7 +1894,7 @@ class Solver final : public ISolver {
   void assemble() {
     k::MomArgs<T> a;
     a.nrows = nv_;
-    a.row = mrow_.p;
+    a.span = mspan_.p;
     a.dpos = mdpos_.p;
     a.K = K_.p;
     a.inc_off = inc_off_.p;
@@ -1893,7 +1927,10 @@ class Solver final : public ISolver {
     ProfScope ps(prof, st_, P_ASSEMBLE);
     if (!o_.supg && fused_assembly_) {
       // one pass: each incidence's convection row is evaluated in place
-      k::mom_assemble<T, true><<<grid_for(nv_, kBlock / 8), kBlock, mom_smem_ + 1536 * sizeof(T), st_>>>(a);
+      if (serial_assembly_)
+        k::mom_assemble<T, 1><<<grid_for(nv_, kBlock / 8), kBlock, mom_smem_ + 1536 * sizeof(T), st_>>>(a);
+      else
+        k::mom_assemble<T, 2><<<grid_for(nv_, kBlock / 8), kBlock, mom_smem_ + 1536 * sizeof(T), st_>>>(a);
       NDS_LAUNCH();
       return;
     }
@@ -1917,7 +1954,7 @@ class Solver final : public ISolver {
       const int s = color_off_[(size_t)c], n = color_off_[(size_t)c + 1] - s;
       if (!n) continue;
       ProfScope ps(prof, st_, P_GS);
-      k::mom_gs_color<T><<<grid_for((long long)n * 8), kBlock, 0, st_>>>(n, color_rows_.p + s, color_span_.p + s, mcol_.p, A_.p,
+      k::mom_gs_color<T><<<grid_for((long long)n * 8), kBlock, 0, st_>>>(n, color_rows_.p + s, gspan_.p + s, mcol_.p, A_.p,
                                                                        diag_.p, b_[0].p, b_[1].p, b_[2].p, uc(0),
                                                                        uc(1), uc(2), T(o_.mom_omega));
       NDS_LAUNCH();
@@ -1925,7 +1962,7 @@ class Solver final : public ISolver {
   }
   std::array<double, 3> audit() {
     const int g = red_grid((long long)nv_ * 8);
-    k::mom_audit<T><<<g, kBlock, 0, st_>>>(nv_, mrow_.p, mcol_.p, A_.p, b_[0].p, b_[1].p, b_[2].p, uc(0), uc(1),
+    k::mom_audit<T><<<g, kBlock, 0, st_>>>(nv_, mspan_.p, mcol_.p, A_.p, b_[0].p, b_[1].p, b_[2].p, uc(0), uc(1),
                                            uc(2), part_.p);
     NDS_LAUNCH();
     reduce_to<6>(g, S_AUDIT);
@@ -2224,10 +2261,10 @@ class Solver final : public ISolver {
   size_t mom_smem_ = 0, refresh_smem_ = 0;
   double cont0_ = -1, cont_rel_ = 1, fine_lambda_ = 1, p_cheb_lambda_ = 1;
   bool finite_all_ = true;
-  bool fused_assembly_ = true;
+  bool fused_assembly_ = true, serial_assembly_ = false;
   std::vector<double> level_lambda_;
   // momentum
-  DBuf<int32_t> mrow_, mcol_, mdpos_, inc_off_, ref_, color_rows_;
+  DBuf<int32_t> mcol_, mdpos_, inc_off_, ref_, color_rows_;
   DBuf<uint32_t> inc_;
   DBuf<uint8_t> slot_;
   DBuf<T> K_, A_, diag_, delta_, rau_, rau_pc_, det_, invJ_, bco_, fixed_, fixed_div_, centT_, cconv_, fgeo_, p_;
@@ -2236,7 +2273,7 @@ class Solver final : public ISolver {
   static constexpr int kVelComponents = k::kVel;
   T* uc(int d) const { return u3_.p + d; }
   std::vector<int> color_off_;
-  DBuf<int2> color_span_;
+  DBuf<int2> mspan_, gspan_;  // momentum rows' storage spans, by row / by colour position
   // pressure
   DBuf<int32_t> fcoff_, fine_crows_, sbase_, swidth_, scol_, fdslot_;
   DBuf<int16_t> sdcol_;

@@ -5,7 +5,8 @@ gpu/serial_cuda/h8_main_base.cu:2046-2119, print cadence :2115-2117).
 
 * ~40k-tet pipe (47,880 cells), Re 20, alpha_u 0.7, alpha_p 0.3, SA + cheb2
   PCG rtol 1e-6, 300 outer iterations: relCont at every printed iteration to
-  1e-8 relative, equal PCG counts, P0 pressure and cell-average velocity to
+  1e-8 relative (+ 1e-16 absolute, the rounding level of relCont(1) = 1),
+  equal PCG counts, P0 pressure and cell-average velocity to
   1e-8 relative L2, the analytic-error line to 1e-8.
 * ~1M-tet pipe (1,231,200 cells), Re 100, converge at 1e-6 (relCont and the
   momentum audit): the same 4193 outer iterations, relCont at every printed
@@ -52,10 +53,14 @@ def _cell_fields(native, P, S):
     return p, uc, (u0, u1, u2)
 
 
-def _check_history(g, got, tol=1e-8):
+def _check_history(g, got, tol=1e-8, floor=1e-16):
+    """relCont is the continuity residual over the first iteration's, so
+    relCont(1) = 1 and floor is the FP64 rounding level of that residual:
+    near steady state (relCont ~ 1e-9) the two solvers' different, each
+    deterministic, reduction orders leave differences of ~5e-17 there."""
     for it, rel, pcg in zip(g["it"], g["rel_cont"], g["p_its"]):
         r, k = got[int(it)]
-        assert abs(r - rel) <= tol * abs(rel), (int(it), r, float(rel))
+        assert abs(r - rel) <= tol * abs(rel) + floor, (int(it), r, float(rel))
         assert k == int(pcg), (int(it), k, int(pcg))
 
 
