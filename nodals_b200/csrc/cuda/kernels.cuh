@@ -157,13 +157,17 @@ __device__ __forceinline__ void supg_column(const T* __restrict__ I, T h2, T dc,
 }
 
 // 8 lanes per cell; lane b computes column b of the cell's block (convection,
-// plus the SUPG terms when SUPG; supg_rule and h2 are read only then).
+// plus the SUPG terms when SUPG; supg_rule and h2 are read only then).  Row a
+// of the block is written to C[8 z + b], z the incidence (c, a) in the
+// velocity rows' incidence lists, so that a row's blocks lie contiguous; the
+// cell's pressure goes to pz[z] for the B^T p terms of the row pass.
 template <class T, bool SUPG>
-__global__ void __launch_bounds__(kBlock) mom_cell_conv(int nc, const int32_t* __restrict__ ref,
+__global__ void __launch_bounds__(kBlock, SUPG ? 2 : 4) mom_cell_conv(int nc, const int32_t* __restrict__ ref,
                                                         const T* __restrict__ fixed, const T* __restrict__ u0,
                                                         const T* __restrict__ u1, const T* __restrict__ u2,
                                                         const T* __restrict__ invJ, const T* __restrict__ det,
-                                                        const T* __restrict__ centT, T* __restrict__ C,
+                                                        const T* __restrict__ centT, const int32_t* __restrict__ zpos,
+                                                        T* __restrict__ C, const T* __restrict__ p, T* __restrict__ pz,
                                                         const T* __restrict__ supg_rule, const T* __restrict__ h2,
                                                         SupgArgs sa) {
   __shared__ T sT[1536];
@@ -201,7 +205,10 @@ __global__ void __launch_bounds__(kBlock) mom_cell_conv(int nc, const int32_t* _
       w[m][2] = __shfl_sync(gmask, r2, m, 8);
     }
     const T dc = det[c];
-    T* out = C + 64 * (size_t)c + lane8;
+    // row a of the block goes to the incidence slot zpos[8c + a] (-1: the
+    // dof of basis a is fixed and has no momentum row)
+    const int zl = zpos[8 * (size_t)c + lane8];
+    if (zl >= 0) pz[zl] = p[c];  // the cell's pressure, by the incidences of its bases
     T S[8];
     if (SUPG) supg_column<T>(I, h2[c], dc, q0, q1, q2, sQ, sa, lane8, gmask, S);
 #pragma unroll 2
@@ -212,7 +219,8 @@ __global__ void __launch_bounds__(kBlock) mom_cell_conv(int nc, const int32_t* _
         const T* t = sT + ((a * 8 + m) * 8 + lane8) * 3;
         cv += w[m][0] * t[0] + w[m][1] * t[1] + w[m][2] * t[2];
       }
-      out[8 * a] = SUPG ? cv * dc + S[a] : cv * dc;
+      const int za = __shfl_sync(gmask, zl, a, 8);
+      if (za >= 0) C[8 * (size_t)za + lane8] = SUPG ? cv * dc + S[a] : cv * dc;
     }
   }
 }
@@ -227,7 +235,11 @@ struct MomArgs {
   const uint32_t* __restrict__ inc;     // (cell << 3) | a
   const int32_t* __restrict__ ref;      // 8 per cell
   const uint8_t* __restrict__ slot;     // 64 per cell
-  const T* __restrict__ C;              // 64 per cell: convection blocks from mom_cell_conv
+  const T* __restrict__ C;              // 8 per incidence: convection rows from mom_cell_conv
+  const uint8_t* __restrict__ slotz;    // 8 per incidence: slot[c][a][b] of incidence (c, a)
+  const T* __restrict__ Bz;             // 3 per incidence: B[c][a]
+  const T* __restrict__ pz;             // per incidence: p_c (written by the cell pass)
+  const uint8_t* __restrict__ fixz;     // per incidence: bit b set when dof b of the cell is fixed
   const T* __restrict__ bco;            // 24 per cell
   const T* __restrict__ fixed;          // 3 per fixed slot
   const T* __restrict__ u0;
@@ -285,16 +297,13 @@ __device__ __forceinline__ T conv_entry(const MomArgs<T>& g, const T* __restrict
   return cv * g.det[c];
 }
 
-// FUSED (1 or 2): C rows evaluated per incidence (conv_entry) instead of
-// read from the cell pass's blocks; the reference tensor is staged in shared
-// memory after the row buffers.  FUSED 2 keeps the loads of the next
-// incidence in flight while the current one is evaluated: the row's
-// incidence codes are loaded up front (lane l holds those of incidences l,
-// l + 8 and l + 16, broadcast by shuffles; codes past the 24th are loaded
-// when needed), and the next incidence's DOF and slot are fetched before
-// the current convection row is computed.  Both forms add the same values in
+// FUSED 0: the row pass of the two-pass assembly; each velocity row reads
+// its incident cells' convection rows, which the cell pass wrote contiguous
+// in incidence order, kAsmAhead at a time.  FUSED 1: C rows evaluated per
+// incidence (conv_entry) instead, with the reference tensor staged in shared
+// memory after the row buffers (no cell pass).  Both add the same values in
 // the same order.
-constexpr int kIncAhead = 24;
+constexpr int kAsmAhead = 4;
 template <class T, int FUSED = 0>
 __global__ void __launch_bounds__(kBlock) mom_assemble(MomArgs<T> g) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -317,57 +326,6 @@ __global__ void __launch_bounds__(kBlock) mom_assemble(MomArgs<T> g) {
     __syncwarp(gmask);
     T conv0 = 0, conv1 = 0, conv2 = 0, bt0 = 0, bt1 = 0, bt2 = 0;
     const int z0 = g.inc_off[i], z1 = g.inc_off[i + 1];
-    if (FUSED == 2) {
-      const int ninc = z1 - z0;
-      uint32_t code[kIncAhead / 8];
-#pragma unroll
-      for (int t = 0; t < kIncAhead / 8; ++t) code[t] = lane8 + 8 * t < ninc ? g.inc[z0 + lane8 + 8 * t] : 0u;
-      auto code_of = [&](int zz) -> uint32_t {  // zz is uniform over the group
-        if (zz >= kIncAhead) return g.inc[z0 + zz];
-        const uint32_t v = zz < 8 ? code[0] : (zz < 16 ? code[1] : code[2]);
-        return __shfl_sync(gmask, v, zz & 7, 8);
-      };
-      uint32_t npa = 0;
-      int nga = 0, nsa = 0;
-      if (ninc > 0) {
-        npa = code_of(0);
-        nga = g.ref[8 * (size_t)(npa >> 3) + lane8];
-        nsa = g.slot[64 * (size_t)(npa >> 3) + 8 * (npa & 7u) + lane8];
-      }
-      for (int zz = 0; zz < ninc; ++zz) {
-        const uint32_t pa = npa;
-        const int ga = nga, sa = nsa;
-        if (zz + 1 < ninc) {
-          npa = code_of(zz + 1);
-          nga = g.ref[8 * (size_t)(npa >> 3) + lane8];
-          nsa = g.slot[64 * (size_t)(npa >> 3) + 8 * (npa & 7u) + lane8];
-        }
-        const int ca = (int)(pa >> 3), aa = (int)(pa & 7u);
-        T pv = 0, B0 = 0, B1 = 0, B2 = 0;
-        if (lane8 == 0) {
-          pv = g.p[ca];
-          const T* B = g.bco + 24 * (size_t)ca + 3 * aa;
-          B0 = B[0];
-          B1 = B[1];
-          B2 = B[2];
-        }
-        const T va = conv_entry<T>(g, sT, ca, aa, ga, lane8, gmask);
-        if (ga >= 0) {
-          buf[sa] += va;
-        } else {
-          const T* f = g.fixed + 3 * (size_t)(-ga - 1);
-          conv0 -= va * f[0];
-          conv1 -= va * f[1];
-          conv2 -= va * f[2];
-        }
-        if (lane8 == 0) {
-          bt0 += B0 * pv;
-          bt1 += B1 * pv;
-          bt2 += B2 * pv;
-        }
-        __syncwarp(gmask);
-      }
-    }
     if (FUSED == 1) {
       for (int z = z0; z < z1; ++z) {
         const uint32_t pa = g.inc[z];
@@ -393,48 +351,60 @@ __global__ void __launch_bounds__(kBlock) mom_assemble(MomArgs<T> g) {
         __syncwarp(gmask);
       }
     }
-    for (int z = z0; z < (FUSED ? z0 : z1); z += 2) {
-      // two incidences in flight; applied in order
-      const bool two = z + 1 < z1;
-      const uint32_t pa = g.inc[z], pb = two ? g.inc[z + 1] : pa;
-      const int ca = (int)(pa >> 3), aa = (int)(pa & 7u), cb = (int)(pb >> 3), ab = (int)(pb & 7u);
-      const int ga = g.ref[8 * (size_t)ca + lane8], gb = g.ref[8 * (size_t)cb + lane8];
-      const T va = g.C[64 * (size_t)ca + 8 * aa + lane8], vb = g.C[64 * (size_t)cb + 8 * ab + lane8];
-      const int sa = g.slot[64 * (size_t)ca + 8 * aa + lane8], sb = g.slot[64 * (size_t)cb + 8 * ab + lane8];
-      if (ga >= 0) {
-        buf[sa] += va;
-      } else {
-        const T* f = g.fixed + 3 * (size_t)(-ga - 1);
-        conv0 -= va * f[0];
-        conv1 -= va * f[1];
-        conv2 -= va * f[2];
-      }
-      if (lane8 == 0) {
-        const T pv = g.p[ca];
-        const T* B = g.bco + 24 * (size_t)ca + 3 * aa;
-        bt0 += B[0] * pv;
-        bt1 += B[1] * pv;
-        bt2 += B[2] * pv;
-      }
-      __syncwarp(gmask);
-      if (two) {
-        if (gb >= 0) {
-          buf[sb] += vb;
-        } else {
-          const T* f = g.fixed + 3 * (size_t)(-gb - 1);
-          conv0 -= vb * f[0];
-          conv1 -= vb * f[1];
-          conv2 -= vb * f[2];
+    if (FUSED == 0) {
+      // B^T p: the lanes fetch the terms of eight incidences at a time
+      // (contiguous per row), lane 0 adds them in incidence order
+      for (int zb = z0; zb < z1; zb += 8) {
+        T pv = 0, B0 = 0, B1 = 0, B2 = 0;
+        if (zb + lane8 < z1) {
+          const size_t z = (size_t)(zb + lane8);
+          pv = g.pz[z];
+          B0 = g.Bz[3 * z];
+          B1 = g.Bz[3 * z + 1];
+          B2 = g.Bz[3 * z + 2];
         }
-        if (lane8 == 0) {
-          const T pv = g.p[cb];
-          const T* B = g.bco + 24 * (size_t)cb + 3 * ab;
-          bt0 += B[0] * pv;
-          bt1 += B[1] * pv;
-          bt2 += B[2] * pv;
+        const int cnt = min(8, z1 - zb);
+        for (int u = 0; u < cnt; ++u) {
+          const T pu = __shfl_sync(gmask, pv, u, 8), b0 = __shfl_sync(gmask, B0, u, 8),
+                  b1 = __shfl_sync(gmask, B1, u, 8), b2 = __shfl_sync(gmask, B2, u, 8);
+          if (lane8 == 0) {
+            bt0 += b0 * pu;
+            bt1 += b1 * pu;
+            bt2 += b2 * pu;
+          }
         }
       }
-      __syncwarp(gmask);
+      // the row's convection rows, contiguous in incidence order, kAsmAhead
+      // at a time; added in incidence order
+      for (int zb = z0; zb < z1; zb += kAsmAhead) {
+        T cz[kAsmAhead];
+        int sz[kAsmAhead];
+        uint32_t fm[kAsmAhead];
+#pragma unroll
+        for (int u = 0; u < kAsmAhead; ++u) {
+          const int z = zb + u;
+          const bool ok = z < z1;
+          cz[u] = ok ? g.C[8 * (size_t)z + lane8] : T(0);
+          sz[u] = ok ? g.slotz[8 * (size_t)z + lane8] : 0;
+          fm[u] = ok ? g.fixz[z] : 0u;
+        }
+#pragma unroll
+        for (int u = 0; u < kAsmAhead; ++u) {
+          if (zb + u < z1) {
+            if ((fm[u] >> lane8) & 1u) {
+              const uint32_t pa = g.inc[zb + u];
+              const int ga = g.ref[8 * (size_t)(pa >> 3) + lane8];
+              const T* f = g.fixed + 3 * (size_t)(-ga - 1);
+              conv0 -= cz[u] * f[0];
+              conv1 -= cz[u] * f[1];
+              conv2 -= cz[u] * f[2];
+            } else {
+              buf[sz[u]] += cz[u];
+            }
+          }
+          __syncwarp(gmask);
+        }
+      }
     }
     conv0 = group_sum<8>(conv0, gmask);
     conv1 = group_sum<8>(conv1, gmask);
@@ -473,9 +443,8 @@ __global__ void __launch_bounds__(kBlock) mom_assemble(MomArgs<T> g) {
 // together; the diagonal entry and the padding of a batch contribute 0.
 // Per lane the entries are summed in the order of the storage, then over
 // the 8 lanes.
-constexpr int kGsAhead = 3;
-template <class T>
-__global__ void __launch_bounds__(kBlock) mom_gs_color(int count, const int32_t* __restrict__ rows,
+template <class T, int kGsAhead = 2>
+__global__ void __launch_bounds__(kBlock, kGsAhead == 2 ? 6 : 5) mom_gs_color(int count, const int32_t* __restrict__ rows,
                                                        const int2* __restrict__ span, const int32_t* __restrict__ ci,
                                                        const T* __restrict__ av, const T* __restrict__ diag,
                                                        const T* __restrict__ b0, const T* __restrict__ b1,

@@ -406,12 +406,34 @@ class Solver final : public ISolver {
     NDS_CUDA(cudaFuncSetAttribute(k::mom_assemble<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mom_smem_));
     NDS_CUDA(cudaFuncSetAttribute(k::mom_assemble<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)(mom_smem_ + 1536 * sizeof(T))));
-    NDS_CUDA(cudaFuncSetAttribute(k::mom_assemble<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)(mom_smem_ + 1536 * sizeof(T))));
-    // the cell blocks of the two-pass assembly (SUPG, or NDS_TWO_PASS_ASSEMBLY=1)
-    fused_assembly_ = !o_.supg && std::getenv("NDS_TWO_PASS_ASSEMBLY") == nullptr;
-    serial_assembly_ = std::getenv("NDS_SERIAL_ASSEMBLY") != nullptr;
-    if (!fused_assembly_) cconv_.alloc(64 * (size_t)nc_);
+    // The two-pass assembly by default: the cell pass writes each cell's
+    // convection block row by row into the incidence slots of the velocity
+    // rows (8 values per incidence, contiguous per row), the row pass
+    // streams them.  NDS_FUSED_ASSEMBLY=1 (not with SUPG) evaluates the
+    // convection rows inside the row pass instead.
+    fused_assembly_ = !o_.supg && std::getenv("NDS_FUSED_ASSEMBLY") != nullptr;
+    if (!fused_assembly_) {
+      const size_t nz = S.fine.packed.size();
+      std::vector<int32_t> zpos(8 * (size_t)nc_, -1);
+      std::vector<uint8_t> slotz(8 * nz), fixz(nz, 0);
+      std::vector<T> bz(3 * nz);
+      for (size_t z = 0; z < nz; ++z) {
+        const uint32_t pa = S.fine.packed[z];
+        const size_t c = pa >> 3, a = pa & 7u;
+        zpos[8 * c + a] = (int32_t)z;
+        for (int d = 0; d < 3; ++d) bz[3 * z + (size_t)d] = (T)S.bco[24 * c + 3 * a + (size_t)d];
+        for (int b = 0; b < 8; ++b) {
+          slotz[8 * z + (size_t)b] = S.row_slot[64 * c + 8 * a + (size_t)b];
+          if (S.ref[8 * c + (size_t)b] < 0) fixz[z] |= (uint8_t)(1u << b);
+        }
+      }
+      zpos_.upload(zpos);
+      slotz_.upload(slotz);
+      fixz_.upload(fixz);
+      bz_.upload(bz);
+      pz_.alloc(nz);
+      cconv_.alloc(8 * nz);
+    }
 
     if (o_.supg) {
       h2_.upload(S.h2);
@@ -1902,6 +1924,10 @@ class Solver final : public ISolver {
     a.ref = ref_.p;
     a.slot = slot_.p;
     a.C = cconv_.p;
+    a.slotz = slotz_.p;
+    a.Bz = bz_.p;
+    a.pz = pz_.p;
+    a.fixz = fixz_.p;
     a.bco = bco_.p;
     a.fixed = fixed_.p;
     a.u0 = uc(0);
@@ -1925,12 +1951,9 @@ class Solver final : public ISolver {
     a.det = det_.p;
     a.centT = centT_.p;
     ProfScope ps(prof, st_, P_ASSEMBLE);
-    if (!o_.supg && fused_assembly_) {
+    if (fused_assembly_) {
       // one pass: each incidence's convection row is evaluated in place
-      if (serial_assembly_)
-        k::mom_assemble<T, 1><<<grid_for(nv_, kBlock / 8), kBlock, mom_smem_ + 1536 * sizeof(T), st_>>>(a);
-      else
-        k::mom_assemble<T, 2><<<grid_for(nv_, kBlock / 8), kBlock, mom_smem_ + 1536 * sizeof(T), st_>>>(a);
+      k::mom_assemble<T, 1><<<grid_for(nv_, kBlock / 8), kBlock, mom_smem_ + 1536 * sizeof(T), st_>>>(a);
       NDS_LAUNCH();
       return;
     }
@@ -1939,10 +1962,12 @@ class Solver final : public ISolver {
     const int gc = std::min(grid_for(nc_, kBlock / 8), 8 * 148);
     if (o_.supg)
       k::mom_cell_conv<T, true><<<gc, kBlock, 0, st_>>>(nc_, ref_.p, fixed_.p, uc(0), uc(1), uc(2), invJ_.p,
-                                                       det_.p, centT_.p, cconv_.p, supg_rule_.p, h2_.p, sa);
+                                                       det_.p, centT_.p, zpos_.p, cconv_.p, p_.p, pz_.p, supg_rule_.p,
+                                                       h2_.p, sa);
     else
       k::mom_cell_conv<T, false><<<gc, kBlock, 0, st_>>>(nc_, ref_.p, fixed_.p, uc(0), uc(1), uc(2), invJ_.p,
-                                                        det_.p, centT_.p, cconv_.p, nullptr, nullptr, sa);
+                                                        det_.p, centT_.p, zpos_.p, cconv_.p, p_.p, pz_.p, nullptr,
+                                                        nullptr, sa);
     NDS_LAUNCH();
     k::mom_assemble<T><<<grid_for(nv_, kBlock / 8), kBlock, mom_smem_, st_>>>(a);
     NDS_LAUNCH();
@@ -1954,9 +1979,14 @@ class Solver final : public ISolver {
       const int s = color_off_[(size_t)c], n = color_off_[(size_t)c + 1] - s;
       if (!n) continue;
       ProfScope ps(prof, st_, P_GS);
-      k::mom_gs_color<T><<<grid_for((long long)n * 8), kBlock, 0, st_>>>(n, color_rows_.p + s, gspan_.p + s, mcol_.p, A_.p,
-                                                                       diag_.p, b_[0].p, b_[1].p, b_[2].p, uc(0),
-                                                                       uc(1), uc(2), T(o_.mom_omega));
+      if (gs_ahead3_)
+        k::mom_gs_color<T, 3><<<grid_for((long long)n * 8), kBlock, 0, st_>>>(
+            n, color_rows_.p + s, gspan_.p + s, mcol_.p, A_.p, diag_.p, b_[0].p, b_[1].p, b_[2].p, uc(0), uc(1), uc(2),
+            T(o_.mom_omega));
+      else
+        k::mom_gs_color<T, 2><<<grid_for((long long)n * 8), kBlock, 0, st_>>>(
+            n, color_rows_.p + s, gspan_.p + s, mcol_.p, A_.p, diag_.p, b_[0].p, b_[1].p, b_[2].p, uc(0), uc(1), uc(2),
+            T(o_.mom_omega));
       NDS_LAUNCH();
     }
   }
@@ -2261,13 +2291,15 @@ class Solver final : public ISolver {
   size_t mom_smem_ = 0, refresh_smem_ = 0;
   double cont0_ = -1, cont_rel_ = 1, fine_lambda_ = 1, p_cheb_lambda_ = 1;
   bool finite_all_ = true;
-  bool fused_assembly_ = true, serial_assembly_ = false;
+  bool fused_assembly_ = false;
+  bool gs_ahead3_ = std::getenv("NDS_GS_AHEAD3") != nullptr;
   std::vector<double> level_lambda_;
   // momentum
   DBuf<int32_t> mcol_, mdpos_, inc_off_, ref_, color_rows_;
   DBuf<uint32_t> inc_;
-  DBuf<uint8_t> slot_;
-  DBuf<T> K_, A_, diag_, delta_, rau_, rau_pc_, det_, invJ_, bco_, fixed_, fixed_div_, centT_, cconv_, fgeo_, p_;
+  DBuf<int32_t> zpos_;  // incidence of (cell, basis), -1 for a fixed dof
+  DBuf<uint8_t> slot_, slotz_, fixz_;  // slots per (cell, basis) and per incidence; fixed-dof masks
+  DBuf<T> K_, A_, diag_, delta_, rau_, rau_pc_, det_, invJ_, bco_, fixed_, fixed_div_, centT_, cconv_, fgeo_, p_, bz_, pz_;
   DBuf<T> h2_, supg_rule_;
   DBuf<T> u3_, b_[3], s_[3], v_[3];  // u3_: interleaved velocity; v_: staging of get/set fields
   static constexpr int kVelComponents = k::kVel;

@@ -192,13 +192,15 @@ def test_sell_column_formats_agree(native, meshes, monkeypatch):
 @pytest.mark.gpu
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_fused_assembly_matches_two_pass(native, meshes, monkeypatch, precision):
-    """The one-pass assembly (convection rows evaluated per incidence) and the
-    two-pass one (cell blocks written, then gathered by rows) evaluate every
-    entry with the same expression in the same order: equal pressure
-    iteration counts and relCont and fields to 1e-13."""
+    """The two-pass assembly (cell blocks written row by row into the
+    velocity rows' incidence slots, then streamed by the row pass; the
+    default) and the one-pass one (NDS_FUSED_ASSEMBLY=1: convection rows
+    evaluated per incidence) evaluate every entry with the same expression in
+    the same order: equal pressure iteration counts and relCont and fields to
+    1e-13."""
     P = _make(native, meshes, "pipe_small", precision=precision, **ORACLE_CASES["sa_pcg"])
     A = native.Solver(P)
-    monkeypatch.setenv("NDS_TWO_PASS_ASSEMBLY", "1")
+    monkeypatch.setenv("NDS_FUSED_ASSEMBLY", "1")
     B = native.Solver(P)
     for _ in range(6):
         a, b = A.step(), B.step()
