@@ -584,9 +584,12 @@ __device__ __forceinline__ T load_val(const MT* __restrict__ v, int k) {
   if constexpr (std::is_same<MT, __half>::value) return (T)__half2float(v[k]);
   else return v[k];
 }
-template <int G, class T, class MT = T>
-__device__ __forceinline__ T lane_batched_dot(int rb, int re, const int32_t* __restrict__ ci, const MT* __restrict__ v,
-                                              const T* __restrict__ x, int lane) {
+// column of entry k of row i: absolute (int32) or a 16-bit delta to the row
+__device__ __forceinline__ int col_at(const int32_t* __restrict__ ci, int k, int) { return ci[k]; }
+__device__ __forceinline__ int col_at(const int16_t* __restrict__ ci, int k, int i) { return i + ci[k]; }
+template <int G, class T, class MT = T, class CT = int32_t>
+__device__ __forceinline__ T lane_batched_dot(int rb, int re, const CT* __restrict__ ci, const MT* __restrict__ v,
+                                              const T* __restrict__ x, int lane, int i = 0) {
   T s = 0;
   for (int k0 = rb + lane; k0 < re; k0 += 8 * G) {
     int c[8];
@@ -594,7 +597,7 @@ __device__ __forceinline__ T lane_batched_dot(int rb, int re, const int32_t* __r
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
       const int k = k0 + u * G;
-      c[u] = k < re ? ci[k] : -1;
+      c[u] = k < re ? col_at(ci, k, i) : -1;
       a[u] = k < re ? load_val<T, MT>(v, k) : T(0);
     }
     T xv[8];
@@ -607,37 +610,37 @@ __device__ __forceinline__ T lane_batched_dot(int rb, int re, const int32_t* __r
   return s;
 }
 constexpr int kRowLanes = 32;
-template <class T, class MT = T>
-__device__ __forceinline__ T group_row_dot(const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+template <class T, class MT = T, class CT = int32_t>
+__device__ __forceinline__ T group_row_dot(const int32_t* __restrict__ rp, const CT* __restrict__ ci,
                                            const MT* __restrict__ v, const T* __restrict__ x, int i, int lane,
                                            unsigned mask, T vinv = T(1)) {
-  T s = group_sum<kRowLanes>(lane_batched_dot<kRowLanes, T, MT>(rp[i], rp[i + 1], ci, v, x, lane), mask);
+  T s = group_sum<kRowLanes>(lane_batched_dot<kRowLanes, T, MT, CT>(rp[i], rp[i + 1], ci, v, x, lane, i), mask);
   if constexpr (!std::is_same<MT, T>::value) s *= vinv;
   return s;
 }
 
 // y = A x
-template <class T, class MT = T>
-__global__ void __launch_bounds__(kBlock) spmv(int n, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+template <class T, class MT = T, class CT = int32_t>
+__global__ void __launch_bounds__(kBlock) spmv(int n, const int32_t* __restrict__ rp, const CT* __restrict__ ci,
                                                const MT* __restrict__ v, const T* __restrict__ x, T* __restrict__ y,
                                                T vinv = T(1)) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = t / kRowLanes, lane = t % kRowLanes;
   if (i >= n) return;
-  const T s = group_row_dot<T, MT>(rp, ci, v, x, i, lane, group_mask<kRowLanes>(), vinv);
+  const T s = group_row_dot<T, MT, CT>(rp, ci, v, x, i, lane, group_mask<kRowLanes>(), vinv);
   if (lane == 0) y[i] = s;
 }
 
 // r = b - A x  (optionally also r2 = r)
-template <class T, class MT = T>
-__global__ void __launch_bounds__(kBlock) spmv_resid(int n, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+template <class T, class MT = T, class CT = int32_t>
+__global__ void __launch_bounds__(kBlock) spmv_resid(int n, const int32_t* __restrict__ rp, const CT* __restrict__ ci,
                                                      const MT* __restrict__ v, const T* __restrict__ x,
                                                      const T* __restrict__ b, T* __restrict__ r, T* __restrict__ r2,
                                                      const T* __restrict__ den, T w, T vinv = T(1)) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = t / kRowLanes, lane = t % kRowLanes;
   if (i >= n) return;
-  const T s = group_row_dot<T, MT>(rp, ci, v, x, i, lane, group_mask<kRowLanes>(), vinv);
+  const T s = group_row_dot<T, MT, CT>(rp, ci, v, x, i, lane, group_mask<kRowLanes>(), vinv);
   if (lane == 0) {
     // r; r2 = r (den null) or the first Jacobi step w r / den
     const T q = b[i] - s;
@@ -648,16 +651,16 @@ __global__ void __launch_bounds__(kBlock) spmv_resid(int n, const int32_t* __res
 }
 
 // Jacobi-type smoothing step: x_out = x_in + w (b - A x_in) / den
-template <class T, class MT = T>
+template <class T, class MT = T, class CT = int32_t>
 __global__ void __launch_bounds__(kBlock) spmv_smooth(int n, const int32_t* __restrict__ rp,
-                                                      const int32_t* __restrict__ ci, const MT* __restrict__ v,
+                                                      const CT* __restrict__ ci, const MT* __restrict__ v,
                                                       const T* __restrict__ xin, const T* __restrict__ b,
                                                       const T* __restrict__ den, T w, T* __restrict__ xout,
                                                       T* __restrict__ add_to, T vinv = T(1)) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = t / kRowLanes, lane = t % kRowLanes;
   if (i >= n) return;
-  const T s = group_row_dot<T, MT>(rp, ci, v, xin, i, lane, group_mask<kRowLanes>(), vinv);
+  const T s = group_row_dot<T, MT, CT>(rp, ci, v, xin, i, lane, group_mask<kRowLanes>(), vinv);
   if (lane == 0) {
     // with add_to the step is added to add_to instead of stored in xout
     const T r = b[i] - s;
@@ -714,16 +717,22 @@ __global__ void __launch_bounds__(kBlock) dot(int n, const T* __restrict__ x, co
   write_partials<1>(acc, part);
 }
 // x += a p; r -= a q; partial r.r.  a = alpha_dev ? *alpha_dev : alpha
+// With x1: also the first (diagonal) step of the next preconditioner
+// application's fine pre-smoother on the new r, x1 = w0 r / den0 (the
+// expression of jacobi_zero).
 template <class T>
 __global__ void __launch_bounds__(kBlock) xr_update(int n, double alpha, const double* __restrict__ alpha_dev,
                                                     const T* __restrict__ p, const T* __restrict__ q,
-                                                    T* __restrict__ x, T* __restrict__ r, double* __restrict__ part) {
+                                                    T* __restrict__ x, T* __restrict__ r, double* __restrict__ part,
+                                                    const T* __restrict__ den0 = nullptr, T w0 = T(0),
+                                                    T* __restrict__ x1 = nullptr) {
   const T a = T(alpha_dev ? *alpha_dev : alpha);
   double acc[1] = {0.0};
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     x[i] += a * p[i];
     const T rr = r[i] - a * q[i];
     r[i] = rr;
+    if (x1) x1[i] = w0 * rr / den0[i];
     acc[0] += (double)rr * (double)rr;
   }
   write_partials<1>(acc, part);
@@ -738,7 +747,7 @@ __global__ void p_update(int n, const double* __restrict__ beta_dev, const T* __
 
 // PCG scalar steps on device.  flags bit 1: pAp <= 0 or non-finite; bit 2: rho <= 0 or non-finite.
 // sc layout: [0] rho  [1] pq  [2] alpha  [3] rn2  [4] rhon  [5] beta
-__global__ void pcg_alpha(double* __restrict__ sc, int* __restrict__ flags) {
+__device__ __forceinline__ void pcg_alpha_step(double* __restrict__ sc, int* __restrict__ flags) {
   const double pq = sc[1];
   if (!(pq > 0.0) || !isfinite(pq)) {
     *flags |= 1;
@@ -747,6 +756,7 @@ __global__ void pcg_alpha(double* __restrict__ sc, int* __restrict__ flags) {
   }
   sc[2] = sc[0] / pq;
 }
+__global__ void pcg_alpha(double* __restrict__ sc, int* __restrict__ flags) { pcg_alpha_step(sc, flags); }
 __global__ void pcg_beta(double* __restrict__ sc, int* __restrict__ flags) {
   const double rhon = sc[4];
   if (!(rhon > 0.0) || !isfinite(rhon)) {
@@ -764,7 +774,8 @@ __global__ void pcg_beta(double* __restrict__ sc, int* __restrict__ flags) {
 //
 // rho step of the loop body: on the first iteration rho = r.z (p = z follows),
 // afterwards beta = rho_new / rho as pcg_beta.
-__global__ void pcg_rho_dev(double* __restrict__ sc, int* __restrict__ flags, const int* __restrict__ ctl) {
+__device__ __forceinline__ void pcg_rho_step(double* __restrict__ sc, int* __restrict__ flags,
+                                             const int* __restrict__ ctl) {
   const double rhon = sc[4];
   if (ctl[2]) {
     if (!(rhon > 0.0) || !isfinite(rhon)) *flags |= 8;
@@ -780,6 +791,9 @@ __global__ void pcg_rho_dev(double* __restrict__ sc, int* __restrict__ flags, co
   sc[5] = rhon / sc[0];
   sc[0] = rhon;
 }
+__global__ void pcg_rho_dev(double* __restrict__ sc, int* __restrict__ flags, const int* __restrict__ ctl) {
+  pcg_rho_step(sc, flags, ctl);
+}
 // p = z on the first iteration, else p = z + beta p
 template <class T>
 __global__ void p_update_dev(int n, const double* __restrict__ beta_dev, const int* __restrict__ ctl,
@@ -794,9 +808,9 @@ __global__ void p_update_dev(int n, const double* __restrict__ beta_dev, const i
 // the count reaches max_its.
 // max_its < 0: the cap is ctl[3] (set per solve by the host).  in_graph = 0:
 // launched outside a graph (host-driven loop), no condition to set.
-__global__ void pcg_check(const double* __restrict__ sc, int rn2_slot, int r0_slot, int target_slot,
-                          int* __restrict__ flags, int* __restrict__ ctl, int max_its,
-                          cudaGraphConditionalHandle loop, int in_graph = 1) {
+__device__ __forceinline__ void pcg_check_step(const double* __restrict__ sc, int rn2_slot, int r0_slot,
+                                               int target_slot, int* __restrict__ flags, int* __restrict__ ctl,
+                                               int max_its, cudaGraphConditionalHandle loop, int in_graph) {
   if (max_its < 0) max_its = ctl[3];
   const int it = ++ctl[0];
   ctl[2] = 0;
@@ -806,6 +820,37 @@ __global__ void pcg_check(const double* __restrict__ sc, int rn2_slot, int r0_sl
   ctl[1] = conv;
   const bool stop = conv || *flags != 0 || it >= max_its;
   if (in_graph) cudaGraphSetConditional(loop, stop ? 0u : 1u);
+}
+__global__ void pcg_check(const double* __restrict__ sc, int rn2_slot, int r0_slot, int target_slot,
+                          int* __restrict__ flags, int* __restrict__ ctl, int max_its,
+                          cudaGraphConditionalHandle loop, int in_graph = 1) {
+  pcg_check_step(sc, rn2_slot, r0_slot, target_slot, flags, ctl, max_its, loop, in_graph);
+}
+
+// A reduction of one value's block partials (as reduce_partials<1>) whose
+// thread 0 then takes the next scalar step of the device PCG: rho and beta
+// (PCG_RHO), alpha (PCG_ALPHA) or the stopping test (PCG_CHECK).  One launch
+// instead of two; the same sums and the same scalar arithmetic.
+enum { PCG_RHO = 1, PCG_ALPHA = 2, PCG_CHECK = 3 };
+struct PcgScalars {
+  double* sc;
+  int* flags;
+  int* ctl;
+  int rn2_slot, r0_slot, target_slot, max_its;
+  cudaGraphConditionalHandle loop;
+  int in_graph;
+};
+template <int STEP>
+__global__ void reduce_pcg(const double* __restrict__ part, int nblocks, double* __restrict__ out, PcgScalars s) {
+  double v[1] = {0.0};
+  for (int b = threadIdx.x; b < nblocks; b += blockDim.x) v[0] += part[b];
+  block_sum<1>(v);
+  if (threadIdx.x == 0) {
+    out[0] = v[0];
+    if (STEP == PCG_RHO) pcg_rho_step(s.sc, s.flags, s.ctl);
+    else if (STEP == PCG_ALPHA) pcg_alpha_step(s.sc, s.flags);
+    else pcg_check_step(s.sc, s.rn2_slot, s.r0_slot, s.target_slot, s.flags, s.ctl, s.max_its, s.loop, s.in_graph);
+  }
 }
 
 // ---------------------------------------------------------------------------

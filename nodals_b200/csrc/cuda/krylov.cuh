@@ -25,9 +25,15 @@ namespace nds {
 namespace k {
 
 // y = float(s x)
-__global__ void scale_to_float(int n, const double* __restrict__ x, double s, float* __restrict__ y) {
+// y = s x in FP32; with x1 also the first (diagonal) step of the fine
+// pre-smoother on y, x1 = w0 y / den0 (the expression of jacobi_zero)
+__global__ void scale_to_float(int n, const double* __restrict__ x, double s, float* __restrict__ y,
+                               const float* __restrict__ den0 = nullptr, float w0 = 0.f, float* __restrict__ x1 = nullptr) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) y[i] = (float)(s * x[i]);
+  if (i >= n) return;
+  const float v = (float)(s * x[i]);
+  y[i] = v;
+  if (x1) x1[i] = w0 * v / den0[i];
 }
 // x += s y (y in FP32, x in FP64)
 __global__ void axpy_from_float(int n, double s, const float* __restrict__ y, double* __restrict__ x) {

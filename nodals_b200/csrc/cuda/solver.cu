@@ -285,8 +285,10 @@ class Solver final : public ISolver {
     DBuf<int32_t> row, col, crows;
     std::vector<int> coff;
     DBuf<TA> val, diag, l1, b, x, r, tmp, corr, pong;
-    // amg_half: FP16 copy of the level's CSR values, scaled by 1 / hinv
+    // amg_half: FP16 copy of the level's CSR values, scaled by 1 / hinv,
+    // and its columns as 16-bit deltas to the row when they all fit
     DBuf<__half> hval;
+    DBuf<int16_t> hcol;
     double hinv = 1.0;
   };
   struct Xfer {  // P (fine rows, ELL k-major) and R = P^T (coarse rows, CSR)
@@ -859,6 +861,13 @@ class Solver final : public ISolver {
     k::reduce_partials<NV><<<1, kBlock, 0, st_>>>(part_.p, nblocks, sc_.p + slot);
     NDS_LAUNCH();
   }
+  // reduction of one value into sc[slot], then the PCG scalar step STEP
+  template <int STEP>
+  void reduce_pcg(int nblocks, int slot, int max_its = 0, cudaGraphConditionalHandle h = {}, int in_graph = 1) {
+    const k::PcgScalars ps{sc_.p, flags_.p, ctl_.p, S_RN2, S_R0, S_TARGET, max_its, h, in_graph};
+    k::reduce_pcg<STEP><<<1, kBlock, 0, st_>>>(part_.p, nblocks, sc_.p + slot, ps);
+    NDS_LAUNCH();
+  }
   void fetch(int first, int count) {
     NDS_CUDA(cudaMemcpyAsync(hsc_ + first, sc_.p + first, sizeof(double) * count, cudaMemcpyDeviceToHost, st_));
     NDS_CUDA(cudaStreamSynchronize(st_));
@@ -890,8 +899,9 @@ class Solver final : public ISolver {
     const int32_t* ci;
     const V* v;
     int cat;                     // profiler category
-    const __half* vh = nullptr;  // FP16 copy of the values (SELL only), scaled by 1 / vinv
+    const __half* vh = nullptr;  // FP16 copy of the values, scaled by 1 / vinv
     double vinv = 1.0;
+    const int16_t* ch = nullptr;  // CSR levels with vh: columns as deltas to the row
   };
   template <int MODE, class V>
   void sell_launch(const OpView<V>& A, int grid, const V* x, const V* b, const V* den, double w, V* y, V* y2) {
@@ -932,6 +942,7 @@ class Solver final : public ISolver {
     if (A.hval.p) {
       V.vh = A.hval.p;
       V.vinv = A.hinv;
+      V.ch = A.hcol.p;
     }
     return V;
   }
@@ -948,11 +959,26 @@ class Solver final : public ISolver {
     Lv.hval.alloc(hv.size());
     NDS_CUDA(cudaMemcpy(Lv.hval.p, hv.data(), hv.size() * sizeof(__half), cudaMemcpyHostToDevice));
     Lv.hinv = 1.0 / scale;
+    std::vector<int16_t> dc(A.col.size());
+    bool fits = true;
+    for (int i = 0; i < A.n && fits; ++i)
+      for (int64_t k = A.row[(size_t)i]; k < A.row[(size_t)i + 1]; ++k) {
+        const int d = A.col[(size_t)k] - i;
+        if (d < -32767 || d > 32767) {
+          fits = false;
+          break;
+        }
+        dc[(size_t)k] = (int16_t)d;
+      }
+    if (fits && !std::getenv("NDS_SELL_COL32")) Lv.hcol.upload(dc);
   }
   template <class V>
   void op_spmv(const OpView<V>& A, const V* x, V* y) {
     ProfScope ps(prof, st_, A.cat);
     if (A.sell) sell_launch<k::SELL_Y, V>(A, grid_for(A.n), x, nullptr, nullptr, 0.0, y, nullptr);
+    else if (A.vh && A.ch && std::is_same<V, float>::value)
+      k::spmv<V, __half, int16_t><<<grid_for((long long)A.n * k::kRowLanes), kBlock, 0, st_>>>(A.n, A.rp, A.ch, A.vh,
+                                                                                               x, y, V(A.vinv));
     else if (A.vh && std::is_same<V, float>::value)
       k::spmv<V, __half><<<grid_for((long long)A.n * k::kRowLanes), kBlock, 0, st_>>>(A.n, A.rp, A.ci, A.vh, x, y,
                                                                                       V(A.vinv));
@@ -965,6 +991,9 @@ class Solver final : public ISolver {
                 double w = 0.0) {
     ProfScope ps(prof, st_, A.cat);
     if (A.sell) sell_launch<k::SELL_RESID, V>(A, grid_for(A.n), x, b, den, w, r, r2);
+    else if (A.vh && A.ch && std::is_same<V, float>::value)
+      k::spmv_resid<V, __half, int16_t><<<grid_for((long long)A.n * k::kRowLanes), kBlock, 0, st_>>>(
+          A.n, A.rp, A.ch, A.vh, x, b, r, r2, den, V(w), V(A.vinv));
     else if (A.vh && std::is_same<V, float>::value)
       k::spmv_resid<V, __half><<<grid_for((long long)A.n * k::kRowLanes), kBlock, 0, st_>>>(
           A.n, A.rp, A.ci, A.vh, x, b, r, r2, den, V(w), V(A.vinv));
@@ -977,6 +1006,9 @@ class Solver final : public ISolver {
   void op_smooth(const OpView<V>& A, const V* xin, const V* b, const V* den, double w, V* xout, V* add_to = nullptr) {
     ProfScope ps(prof, st_, A.cat);
     if (A.sell) sell_launch<k::SELL_SMOOTH, V>(A, grid_for(A.n), xin, b, den, w, xout, add_to);
+    else if (A.vh && A.ch && std::is_same<V, float>::value)
+      k::spmv_smooth<V, __half, int16_t><<<grid_for((long long)A.n * k::kRowLanes), kBlock, 0, st_>>>(
+          A.n, A.rp, A.ch, A.vh, xin, b, den, V(w), xout, add_to, V(A.vinv));
     else if (A.vh && std::is_same<V, float>::value)
       k::spmv_smooth<V, __half><<<grid_for((long long)A.n * k::kRowLanes), kBlock, 0, st_>>>(
           A.n, A.rp, A.ci, A.vh, xin, b, den, V(w), xout, add_to, V(A.vinv));
@@ -1331,22 +1363,18 @@ class Solver final : public ISolver {
   // alpha; x, r update; ||r||^2; check
   void pcg_loop_body(cudaGraphConditionalHandle h) {
     amg_T(r_.p, z_.p);
-    dot_dev(r_.p, z_.p, nc_, S_RHON);
-    k::pcg_rho_dev<<<1, 1, 0, st_>>>(sc_.p, flags_.p, ctl_.p);
+    const int g = red_grid(nc_);
+    k::dot<T><<<g, kBlock, 0, st_>>>(nc_, r_.p, z_.p, part_.p);
     NDS_LAUNCH();
+    reduce_pcg<k::PCG_RHO>(g, S_RHON);
     k::p_update_dev<T><<<grid_for(nc_), kBlock, 0, st_>>>(nc_, sc_.p + S_BETA, ctl_.p, z_.p, pp_.p);
     NDS_LAUNCH();
-    const int g = red_grid(nc_);
     sell_launch<k::SELL_DOT, T>(fine_op(), g, pp_.p, nullptr, nullptr, 0.0, q_.p, nullptr);
     NDS_LAUNCH();
-    reduce_to<1>(g, S_PQ);
-    k::pcg_alpha<<<1, 1, 0, st_>>>(sc_.p, flags_.p);
-    NDS_LAUNCH();
+    reduce_pcg<k::PCG_ALPHA>(g, S_PQ);
     k::xr_update<T><<<g, kBlock, 0, st_>>>(nc_, 0.0, sc_.p + S_ALPHA, pp_.p, q_.p, x_.p, r_.p, part_.p);
     NDS_LAUNCH();
-    reduce_to<1>(g, S_RN2);
-    k::pcg_check<<<1, 1, 0, st_>>>(sc_.p, S_RN2, S_R0, S_TARGET, flags_.p, ctl_.p, o_.p_max, h);
-    NDS_LAUNCH();
+    reduce_pcg<k::PCG_CHECK>(g, S_RN2, o_.p_max, h);
   }
   // PCG with the iteration loop on the device: two host synchronisations per
   // solve (initial norm, final state) instead of one per iteration.  Same
@@ -1488,6 +1516,9 @@ class Solver final : public ISolver {
   // learned stage: z1 = N(v), t = v - A z1; the V-cycle then solves for t and
   // z = z1 + V(t) -- or, when the stage did not reduce the residual
   // (||t|| >= ||v||), z = V(v) (the plain preconditioner as fallback).
+  // the inner PCG takes the fine pre-smoother's first step in the kernels
+  // that produce r (plain V-cycle with a polynomial smoother only)
+  bool pre_fused() const { return !stage_ && o_.amg_smoother != NDS_SM_MCGS; }
   void precond_f(const float* v, float* z) {
     if constexpr (!kSame) {
       if (!stage_) {
@@ -1606,26 +1637,31 @@ class Solver final : public ISolver {
   // one pass of the FP32 PCG loop: z = M r; rho; p; q = A p; alpha; x, r; check
   void pcgf_body(cudaGraphConditionalHandle h) {
     if constexpr (!kSame) {
-      precond_f(rf_.p, zf_.p);
-      dot_dev(rf_.p, zf_.p, nc_, S_RHON);
-      k::pcg_rho_dev<<<1, 1, 0, st_>>>(sc_.p, flags_.p, ctl_.p);
+      // the fine pre-smoother's first step on r is already in place (taken
+      // by scale_to_float before the loop and by xr_update after it)
+      if (pre_fused()) amg_apply(rf_.p, zf_.p, true);
+      else precond_f(rf_.p, zf_.p);
+      const int g = red_grid(nc_);
+      k::dot<float><<<g, kBlock, 0, st_>>>(nc_, rf_.p, zf_.p, part_.p);
       NDS_LAUNCH();
+      reduce_pcg<k::PCG_RHO>(g, S_RHON);
       k::p_update_dev<float><<<grid_for(nc_), kBlock, 0, st_>>>(nc_, sc_.p + S_BETA, ctl_.p, zf_.p, pf_.p);
       NDS_LAUNCH();
-      const int g = red_grid(nc_);
       {
         ProfScope ps(prof, st_, P_FINE_AMG);
         sell_launch<k::SELL_DOT, float>(fine_opA(), g, pf_.p, nullptr, nullptr, 0.0, qf_.p, nullptr);
         NDS_LAUNCH();
       }
-      reduce_to<1>(g, S_PQ);
-      k::pcg_alpha<<<1, 1, 0, st_>>>(sc_.p, flags_.p);
+      reduce_pcg<k::PCG_ALPHA>(g, S_PQ);
+      if (pre_fused()) {
+        const PolyPlan pl = fine_plan();
+        k::xr_update<float><<<g, kBlock, 0, st_>>>(nc_, 0.0, sc_.p + S_ALPHA, pf_.p, qf_.p, xf_.p, rf_.p, part_.p,
+                                                    pl.den0, float(pl.w0), poly_first(pl, zf_.p, fpong_.p));
+      } else {
+        k::xr_update<float><<<g, kBlock, 0, st_>>>(nc_, 0.0, sc_.p + S_ALPHA, pf_.p, qf_.p, xf_.p, rf_.p, part_.p);
+      }
       NDS_LAUNCH();
-      k::xr_update<float><<<g, kBlock, 0, st_>>>(nc_, 0.0, sc_.p + S_ALPHA, pf_.p, qf_.p, xf_.p, rf_.p, part_.p);
-      NDS_LAUNCH();
-      reduce_to<1>(g, S_RN2);
-      k::pcg_check<<<1, 1, 0, st_>>>(sc_.p, S_RN2, S_R0, S_TARGET, flags_.p, ctl_.p, -1, h, in_graph_);
-      NDS_LAUNCH();
+      reduce_pcg<k::PCG_CHECK>(g, S_RN2, -1, h, in_graph_);
     }
   }
   // one Arnoldi step of FGMRES: z_j = M v_j, w = A z_j, classical Gram-Schmidt
@@ -1893,7 +1929,13 @@ class Solver final : public ISolver {
         if (fg_m_ > 0) {
           R.its += inner_fgmres(rn, tol, std::min(cap, fg_m_));
         } else {
-          k::scale_to_float<<<grid_for(nc_), kBlock, 0, st_>>>(nc_, r_.p, 1.0 / rn, rf_.p);
+          if (pre_fused()) {
+            const PolyPlan pl = fine_plan();
+            k::scale_to_float<<<grid_for(nc_), kBlock, 0, st_>>>(nc_, r_.p, 1.0 / rn, rf_.p, pl.den0, float(pl.w0),
+                                                                 poly_first(pl, zf_.p, fpong_.p));
+          } else {
+            k::scale_to_float<<<grid_for(nc_), kBlock, 0, st_>>>(nc_, r_.p, 1.0 / rn, rf_.p);
+          }
           NDS_LAUNCH();
           R.its += inner_pcg(tol, cap);
           k::axpy_from_float<<<grid_for(nc_), kBlock, 0, st_>>>(nc_, rn, xf_.p, x_.p);

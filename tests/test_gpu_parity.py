@@ -174,11 +174,14 @@ def check_hp(got: dict, want, tol: float):
 
 
 @pytest.mark.gpu
-def test_sell_column_formats_agree(native, meshes, monkeypatch):
-    """The fine operator keeps 16-bit column deltas when the ordering allows
-    and absolute 32-bit columns otherwise (NDS_SELL_COL32 forces the latter):
+@pytest.mark.parametrize("variant", ["amg_fp32", "mixed_half"])
+def test_sell_column_formats_agree(native, meshes, monkeypatch, variant):
+    """The fine operator (and, with the FP16 V-cycle, the explicit levels'
+    FP16 copies) keep 16-bit column deltas when the ordering allows and
+    absolute 32-bit columns otherwise (NDS_SELL_COL32 forces the latter):
     both formats give bitwise-equal solves."""
-    P = _make(native, meshes, "pipe_small", precision="amg_fp32", **ORACLE_CASES["sa_pcg"])
+    kw = dict(precision="amg_fp32") if variant == "amg_fp32" else dict(precision="mixed", p_guess=4, amg_half=1)
+    P = _make(native, meshes, "pipe_small", **kw, **ORACLE_CASES["sa_pcg"])
     A = native.Solver(P)
     monkeypatch.setenv("NDS_SELL_COL32", "1")
     B = native.Solver(P)
