@@ -610,37 +610,37 @@ __device__ __forceinline__ T lane_batched_dot(int rb, int re, const CT* __restri
   return s;
 }
 constexpr int kRowLanes = 32;
-template <class T, class MT = T, class CT = int32_t>
+template <class T, class MT = T, class CT = int32_t, int GL = kRowLanes>
 __device__ __forceinline__ T group_row_dot(const int32_t* __restrict__ rp, const CT* __restrict__ ci,
                                            const MT* __restrict__ v, const T* __restrict__ x, int i, int lane,
                                            unsigned mask, T vinv = T(1)) {
-  T s = group_sum<kRowLanes>(lane_batched_dot<kRowLanes, T, MT, CT>(rp[i], rp[i + 1], ci, v, x, lane, i), mask);
+  T s = group_sum<GL>(lane_batched_dot<GL, T, MT, CT>(rp[i], rp[i + 1], ci, v, x, lane, i), mask);
   if constexpr (!std::is_same<MT, T>::value) s *= vinv;
   return s;
 }
 
-// y = A x
-template <class T, class MT = T, class CT = int32_t>
+// y = A x (GL lanes per row)
+template <class T, class MT = T, class CT = int32_t, int GL = kRowLanes>
 __global__ void __launch_bounds__(kBlock) spmv(int n, const int32_t* __restrict__ rp, const CT* __restrict__ ci,
                                                const MT* __restrict__ v, const T* __restrict__ x, T* __restrict__ y,
                                                T vinv = T(1)) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int i = t / kRowLanes, lane = t % kRowLanes;
+  const int i = t / GL, lane = t % GL;
   if (i >= n) return;
-  const T s = group_row_dot<T, MT, CT>(rp, ci, v, x, i, lane, group_mask<kRowLanes>(), vinv);
+  const T s = group_row_dot<T, MT, CT, GL>(rp, ci, v, x, i, lane, group_mask<GL>(), vinv);
   if (lane == 0) y[i] = s;
 }
 
 // r = b - A x  (optionally also r2 = r)
-template <class T, class MT = T, class CT = int32_t>
+template <class T, class MT = T, class CT = int32_t, int GL = kRowLanes>
 __global__ void __launch_bounds__(kBlock) spmv_resid(int n, const int32_t* __restrict__ rp, const CT* __restrict__ ci,
                                                      const MT* __restrict__ v, const T* __restrict__ x,
                                                      const T* __restrict__ b, T* __restrict__ r, T* __restrict__ r2,
                                                      const T* __restrict__ den, T w, T vinv = T(1)) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int i = t / kRowLanes, lane = t % kRowLanes;
+  const int i = t / GL, lane = t % GL;
   if (i >= n) return;
-  const T s = group_row_dot<T, MT, CT>(rp, ci, v, x, i, lane, group_mask<kRowLanes>(), vinv);
+  const T s = group_row_dot<T, MT, CT, GL>(rp, ci, v, x, i, lane, group_mask<GL>(), vinv);
   if (lane == 0) {
     // r; r2 = r (den null) or the first Jacobi step w r / den
     const T q = b[i] - s;
@@ -651,16 +651,16 @@ __global__ void __launch_bounds__(kBlock) spmv_resid(int n, const int32_t* __res
 }
 
 // Jacobi-type smoothing step: x_out = x_in + w (b - A x_in) / den
-template <class T, class MT = T, class CT = int32_t>
+template <class T, class MT = T, class CT = int32_t, int GL = kRowLanes>
 __global__ void __launch_bounds__(kBlock) spmv_smooth(int n, const int32_t* __restrict__ rp,
                                                       const CT* __restrict__ ci, const MT* __restrict__ v,
                                                       const T* __restrict__ xin, const T* __restrict__ b,
                                                       const T* __restrict__ den, T w, T* __restrict__ xout,
                                                       T* __restrict__ add_to, T vinv = T(1)) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int i = t / kRowLanes, lane = t % kRowLanes;
+  const int i = t / GL, lane = t % GL;
   if (i >= n) return;
-  const T s = group_row_dot<T, MT, CT>(rp, ci, v, xin, i, lane, group_mask<kRowLanes>(), vinv);
+  const T s = group_row_dot<T, MT, CT, GL>(rp, ci, v, xin, i, lane, group_mask<GL>(), vinv);
   if (lane == 0) {
     // with add_to the step is added to add_to instead of stored in xout
     const T r = b[i] - s;
@@ -1269,15 +1269,15 @@ __global__ void sell_gs_color(int count, const int32_t* __restrict__ rows, Sell 
 
 // c = P^T f, a kRowLanes group per coarse row over R = P^T (deterministic
 // tree per row)
-template <class T>
+template <class T, int GL = kRowLanes>
 __global__ void __launch_bounds__(kBlock) restrict_rows(int nc, const int32_t* __restrict__ rr,
                                                         const int32_t* __restrict__ rc, const T* __restrict__ rv,
                                                         const T* __restrict__ f, T* __restrict__ c,
                                                         const T* __restrict__ den0, T w0, T* __restrict__ x1) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int I = t / kRowLanes, lane = t % kRowLanes;
+  const int I = t / GL, lane = t % GL;
   if (I >= nc) return;
-  const T s = group_row_dot(rr, rc, rv, f, I, lane, group_mask<kRowLanes>());
+  const T s = group_row_dot<T, T, int32_t, GL>(rr, rc, rv, f, I, lane, group_mask<GL>());
   if (lane == 0) {
     c[I] = s;
     // with x1: the coarse pre-smoother's diagonal step w0 c / den0

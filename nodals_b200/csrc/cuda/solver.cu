@@ -972,13 +972,23 @@ class Solver final : public ISolver {
       }
     if (fits && !std::getenv("NDS_SELL_COL32")) Lv.hcol.upload(dc);
   }
+  // launch f with the lanes per row of the FP16 level kernels
+  template <class V, class F>
+  void level_half_launch(const OpView<V>& A, F&& f) {
+    if (level_lanes_ == 8) f(std::integral_constant<int, 8>{});
+    else if (level_lanes_ == 16) f(std::integral_constant<int, 16>{});
+    else f(std::integral_constant<int, 32>{});
+  }
   template <class V>
   void op_spmv(const OpView<V>& A, const V* x, V* y) {
     ProfScope ps(prof, st_, A.cat);
     if (A.sell) sell_launch<k::SELL_Y, V>(A, grid_for(A.n), x, nullptr, nullptr, 0.0, y, nullptr);
     else if (A.vh && A.ch && std::is_same<V, float>::value)
-      k::spmv<V, __half, int16_t><<<grid_for((long long)A.n * k::kRowLanes), kBlock, 0, st_>>>(A.n, A.rp, A.ch, A.vh,
-                                                                                               x, y, V(A.vinv));
+      level_half_launch(A, [&](auto gl) {
+        constexpr int GL = decltype(gl)::value;
+        k::spmv<V, __half, int16_t, GL><<<grid_for((long long)A.n * GL), kBlock, 0, st_>>>(A.n, A.rp, A.ch, A.vh, x,
+                                                                                             y, V(A.vinv));
+      });
     else if (A.vh && std::is_same<V, float>::value)
       k::spmv<V, __half><<<grid_for((long long)A.n * k::kRowLanes), kBlock, 0, st_>>>(A.n, A.rp, A.ci, A.vh, x, y,
                                                                                       V(A.vinv));
@@ -992,8 +1002,11 @@ class Solver final : public ISolver {
     ProfScope ps(prof, st_, A.cat);
     if (A.sell) sell_launch<k::SELL_RESID, V>(A, grid_for(A.n), x, b, den, w, r, r2);
     else if (A.vh && A.ch && std::is_same<V, float>::value)
-      k::spmv_resid<V, __half, int16_t><<<grid_for((long long)A.n * k::kRowLanes), kBlock, 0, st_>>>(
-          A.n, A.rp, A.ch, A.vh, x, b, r, r2, den, V(w), V(A.vinv));
+      level_half_launch(A, [&](auto gl) {
+        constexpr int GL = decltype(gl)::value;
+        k::spmv_resid<V, __half, int16_t, GL><<<grid_for((long long)A.n * GL), kBlock, 0, st_>>>(
+            A.n, A.rp, A.ch, A.vh, x, b, r, r2, den, V(w), V(A.vinv));
+      });
     else if (A.vh && std::is_same<V, float>::value)
       k::spmv_resid<V, __half><<<grid_for((long long)A.n * k::kRowLanes), kBlock, 0, st_>>>(
           A.n, A.rp, A.ci, A.vh, x, b, r, r2, den, V(w), V(A.vinv));
@@ -1007,8 +1020,11 @@ class Solver final : public ISolver {
     ProfScope ps(prof, st_, A.cat);
     if (A.sell) sell_launch<k::SELL_SMOOTH, V>(A, grid_for(A.n), xin, b, den, w, xout, add_to);
     else if (A.vh && A.ch && std::is_same<V, float>::value)
-      k::spmv_smooth<V, __half, int16_t><<<grid_for((long long)A.n * k::kRowLanes), kBlock, 0, st_>>>(
-          A.n, A.rp, A.ch, A.vh, xin, b, den, V(w), xout, add_to, V(A.vinv));
+      level_half_launch(A, [&](auto gl) {
+        constexpr int GL = decltype(gl)::value;
+        k::spmv_smooth<V, __half, int16_t, GL><<<grid_for((long long)A.n * GL), kBlock, 0, st_>>>(
+            A.n, A.rp, A.ch, A.vh, xin, b, den, V(w), xout, add_to, V(A.vinv));
+      });
     else if (A.vh && std::is_same<V, float>::value)
       k::spmv_smooth<V, __half><<<grid_for((long long)A.n * k::kRowLanes), kBlock, 0, st_>>>(
           A.n, A.rp, A.ci, A.vh, xin, b, den, V(w), xout, add_to, V(A.vinv));
@@ -1161,8 +1177,18 @@ class Solver final : public ISolver {
       w0 = pl.w0;
       x1 = poly_first(pl, C.x.p, C.pong.p);
     }
-    k::restrict_rows<TA><<<grid_for((long long)X.nc * k::kRowLanes), kBlock, 0, st_>>>(X.nc, X.rrow.p, X.rcol.p, X.rval.p, f, c,
-                                                                            den0, TA(w0), x1);
+    if (mixed_ && o_.amg_half && level_lanes_ != 32) {
+      auto run = [&](auto gl) {
+        constexpr int GL = decltype(gl)::value;
+        k::restrict_rows<TA, GL><<<grid_for((long long)X.nc * GL), kBlock, 0, st_>>>(X.nc, X.rrow.p, X.rcol.p,
+                                                                                    X.rval.p, f, c, den0, TA(w0), x1);
+      };
+      if (level_lanes_ == 8) run(std::integral_constant<int, 8>{});
+      else run(std::integral_constant<int, 16>{});
+    } else {
+      k::restrict_rows<TA><<<grid_for((long long)X.nc * k::kRowLanes), kBlock, 0, st_>>>(
+          X.nc, X.rrow.p, X.rcol.p, X.rval.p, f, c, den0, TA(w0), x1);
+    }
     NDS_LAUNCH();
   }
   void prolong(const Xfer& X, const TA* c, TA* f) {
@@ -2335,6 +2361,10 @@ class Solver final : public ISolver {
   bool finite_all_ = true;
   bool fused_assembly_ = false;
   bool gs_ahead3_ = std::getenv("NDS_GS_AHEAD3") != nullptr;
+  // lanes per row of the FP16 level SpMVs and of the restriction in the
+  // mixed FP16 V-cycle (16 measured best at pipe1m: 0.25 ms per SIMPLE
+  // iteration less than 32 or 8); NDS_LEVEL_LANES=8|16|32 overrides
+  int level_lanes_ = std::getenv("NDS_LEVEL_LANES") ? std::atoi(std::getenv("NDS_LEVEL_LANES")) : 16;
   std::vector<double> level_lambda_;
   // momentum
   DBuf<int32_t> mcol_, mdpos_, inc_off_, ref_, color_rows_;
