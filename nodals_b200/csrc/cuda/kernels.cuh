@@ -161,7 +161,7 @@ __device__ __forceinline__ void supg_column(const T* __restrict__ I, T h2, T dc,
 // of the block is written to C[8 z + b], z the incidence (c, a) in the
 // velocity rows' incidence lists, so that a row's blocks lie contiguous; the
 // cell's pressure goes to pz[z] for the B^T p terms of the row pass.
-template <class T, bool SUPG>
+template <class T, bool SUPG, int UNR = 2>
 __global__ void __launch_bounds__(kBlock, SUPG ? 2 : 4) mom_cell_conv(int nc, const int32_t* __restrict__ ref,
                                                         const T* __restrict__ fixed, const T* __restrict__ u0,
                                                         const T* __restrict__ u1, const T* __restrict__ u2,
@@ -211,7 +211,7 @@ __global__ void __launch_bounds__(kBlock, SUPG ? 2 : 4) mom_cell_conv(int nc, co
     if (zl >= 0) pz[zl] = p[c];  // the cell's pressure, by the incidences of its bases
     T S[8];
     if (SUPG) supg_column<T>(I, h2[c], dc, q0, q1, q2, sQ, sa, lane8, gmask, S);
-#pragma unroll 2
+#pragma unroll UNR
     for (int a = 0; a < 8; ++a) {
       T cv = 0;
 #pragma unroll
@@ -550,8 +550,28 @@ __global__ void __launch_bounds__(kBlock) continuity(int nc, const int32_t* __re
   double acc[1] = {0.0};
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
     T s = fixed_div[c];
-    const int32_t* rf = ref + 8 * (size_t)c;
-    const T* B = bco + 24 * (size_t)c;
+    // the cell's 8 dofs and 24 coefficients in 16-byte loads (the records
+    // are 32 and 24 * sizeof(T) bytes, so 16-byte aligned)
+    int rf[8];
+    T B[24];
+    {
+      const int4* r4 = reinterpret_cast<const int4*>(ref + 8 * (size_t)c);
+      const int4 q0 = r4[0], q1 = r4[1];
+      rf[0] = q0.x; rf[1] = q0.y; rf[2] = q0.z; rf[3] = q0.w;
+      rf[4] = q1.x; rf[5] = q1.y; rf[6] = q1.z; rf[7] = q1.w;
+      if constexpr (sizeof(T) == 8) {
+        const double2* b2 = reinterpret_cast<const double2*>(bco + 24 * (size_t)c);
+#pragma unroll
+        for (int k = 0; k < 12; ++k) {
+          const double2 v = b2[k];
+          B[2 * k] = v.x;
+          B[2 * k + 1] = v.y;
+        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < 24; ++k) B[k] = bco[24 * (size_t)c + k];
+      }
+    }
 #pragma unroll
     for (int a = 0; a < 8; ++a) {
       const int g = rf[a];

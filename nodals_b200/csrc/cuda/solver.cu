@@ -990,8 +990,11 @@ class Solver final : public ISolver {
                                                                                              y, V(A.vinv));
       });
     else if (A.vh && std::is_same<V, float>::value)
-      k::spmv<V, __half><<<grid_for((long long)A.n * k::kRowLanes), kBlock, 0, st_>>>(A.n, A.rp, A.ci, A.vh, x, y,
-                                                                                      V(A.vinv));
+      level_half_launch(A, [&](auto gl) {
+        constexpr int GL = decltype(gl)::value;
+        k::spmv<V, __half, int32_t, GL><<<grid_for((long long)A.n * GL), kBlock, 0, st_>>>(A.n, A.rp, A.ci, A.vh, x,
+                                                                                             y, V(A.vinv));
+      });
     else k::spmv<V><<<grid_for((long long)A.n * k::kRowLanes), kBlock, 0, st_>>>(A.n, A.rp, A.ci, A.v, x, y);
     NDS_LAUNCH();
   }
@@ -1008,8 +1011,11 @@ class Solver final : public ISolver {
             A.n, A.rp, A.ch, A.vh, x, b, r, r2, den, V(w), V(A.vinv));
       });
     else if (A.vh && std::is_same<V, float>::value)
-      k::spmv_resid<V, __half><<<grid_for((long long)A.n * k::kRowLanes), kBlock, 0, st_>>>(
-          A.n, A.rp, A.ci, A.vh, x, b, r, r2, den, V(w), V(A.vinv));
+      level_half_launch(A, [&](auto gl) {
+        constexpr int GL = decltype(gl)::value;
+        k::spmv_resid<V, __half, int32_t, GL><<<grid_for((long long)A.n * GL), kBlock, 0, st_>>>(
+            A.n, A.rp, A.ci, A.vh, x, b, r, r2, den, V(w), V(A.vinv));
+      });
     else
       k::spmv_resid<V><<<grid_for((long long)A.n * k::kRowLanes), kBlock, 0, st_>>>(A.n, A.rp, A.ci, A.v, x, b, r, r2, den, V(w));
     NDS_LAUNCH();
@@ -1026,8 +1032,11 @@ class Solver final : public ISolver {
             A.n, A.rp, A.ch, A.vh, xin, b, den, V(w), xout, add_to, V(A.vinv));
       });
     else if (A.vh && std::is_same<V, float>::value)
-      k::spmv_smooth<V, __half><<<grid_for((long long)A.n * k::kRowLanes), kBlock, 0, st_>>>(
-          A.n, A.rp, A.ci, A.vh, xin, b, den, V(w), xout, add_to, V(A.vinv));
+      level_half_launch(A, [&](auto gl) {
+        constexpr int GL = decltype(gl)::value;
+        k::spmv_smooth<V, __half, int32_t, GL><<<grid_for((long long)A.n * GL), kBlock, 0, st_>>>(
+            A.n, A.rp, A.ci, A.vh, xin, b, den, V(w), xout, add_to, V(A.vinv));
+      });
     else
       k::spmv_smooth<V><<<grid_for((long long)A.n * k::kRowLanes), kBlock, 0, st_>>>(A.n, A.rp, A.ci, A.v, xin, b, den, V(w), xout,
                                                                           add_to);
@@ -2032,6 +2041,10 @@ class Solver final : public ISolver {
       k::mom_cell_conv<T, true><<<gc, kBlock, 0, st_>>>(nc_, ref_.p, fixed_.p, uc(0), uc(1), uc(2), invJ_.p,
                                                        det_.p, centT_.p, zpos_.p, cconv_.p, p_.p, pz_.p, supg_rule_.p,
                                                        h2_.p, sa);
+    else if (cell_unroll4_)
+      k::mom_cell_conv<T, false, 4><<<gc, kBlock, 0, st_>>>(nc_, ref_.p, fixed_.p, uc(0), uc(1), uc(2), invJ_.p,
+                                                           det_.p, centT_.p, zpos_.p, cconv_.p, p_.p, pz_.p, nullptr,
+                                                           nullptr, sa);
     else
       k::mom_cell_conv<T, false><<<gc, kBlock, 0, st_>>>(nc_, ref_.p, fixed_.p, uc(0), uc(1), uc(2), invJ_.p,
                                                         det_.p, centT_.p, zpos_.p, cconv_.p, p_.p, pz_.p, nullptr,
@@ -2361,6 +2374,7 @@ class Solver final : public ISolver {
   bool finite_all_ = true;
   bool fused_assembly_ = false;
   bool gs_ahead3_ = std::getenv("NDS_GS_AHEAD3") != nullptr;
+  bool cell_unroll4_ = std::getenv("NDS_CELL_UNROLL4") != nullptr;
   // lanes per row of the FP16 level SpMVs and of the restriction in the
   // mixed FP16 V-cycle (16 measured best at pipe1m: 0.25 ms per SIMPLE
   // iteration less than 32 or 8); NDS_LEVEL_LANES=8|16|32 overrides
