@@ -161,7 +161,7 @@ __device__ __forceinline__ void supg_column(const T* __restrict__ I, T h2, T dc,
 // of the block is written to C[8 z + b], z the incidence (c, a) in the
 // velocity rows' incidence lists, so that a row's blocks lie contiguous; the
 // cell's pressure goes to pz[z] for the B^T p terms of the row pass.
-template <class T, bool SUPG, int UNR = 2>
+template <class T, bool SUPG>
 __global__ void __launch_bounds__(kBlock, SUPG ? 2 : 4) mom_cell_conv(int nc, const int32_t* __restrict__ ref,
                                                         const T* __restrict__ fixed, const T* __restrict__ u0,
                                                         const T* __restrict__ u1, const T* __restrict__ u2,
@@ -211,7 +211,7 @@ __global__ void __launch_bounds__(kBlock, SUPG ? 2 : 4) mom_cell_conv(int nc, co
     if (zl >= 0) pz[zl] = p[c];  // the cell's pressure, by the incidences of its bases
     T S[8];
     if (SUPG) supg_column<T>(I, h2[c], dc, q0, q1, q2, sQ, sa, lane8, gmask, S);
-#pragma unroll UNR
+#pragma unroll 2
     for (int a = 0; a < 8; ++a) {
       T cv = 0;
 #pragma unroll

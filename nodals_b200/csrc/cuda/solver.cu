@@ -2041,10 +2041,6 @@ class Solver final : public ISolver {
       k::mom_cell_conv<T, true><<<gc, kBlock, 0, st_>>>(nc_, ref_.p, fixed_.p, uc(0), uc(1), uc(2), invJ_.p,
                                                        det_.p, centT_.p, zpos_.p, cconv_.p, p_.p, pz_.p, supg_rule_.p,
                                                        h2_.p, sa);
-    else if (cell_unroll4_)
-      k::mom_cell_conv<T, false, 4><<<gc, kBlock, 0, st_>>>(nc_, ref_.p, fixed_.p, uc(0), uc(1), uc(2), invJ_.p,
-                                                           det_.p, centT_.p, zpos_.p, cconv_.p, p_.p, pz_.p, nullptr,
-                                                           nullptr, sa);
     else
       k::mom_cell_conv<T, false><<<gc, kBlock, 0, st_>>>(nc_, ref_.p, fixed_.p, uc(0), uc(1), uc(2), invJ_.p,
                                                         det_.p, centT_.p, zpos_.p, cconv_.p, p_.p, pz_.p, nullptr,
@@ -2374,7 +2370,6 @@ class Solver final : public ISolver {
   bool finite_all_ = true;
   bool fused_assembly_ = false;
   bool gs_ahead3_ = std::getenv("NDS_GS_AHEAD3") != nullptr;
-  bool cell_unroll4_ = std::getenv("NDS_CELL_UNROLL4") != nullptr;
   // lanes per row of the FP16 level SpMVs and of the restriction in the
   // mixed FP16 V-cycle (16 measured best at pipe1m: 0.25 ms per SIMPLE
   // iteration less than 32 or 8); NDS_LEVEL_LANES=8|16|32 overrides
