@@ -1171,6 +1171,12 @@ __global__ void refresh_geometry(int nc, const int32_t* __restrict__ coff, const
 // TA); the diagonal and L1 row sums feed the AMG smoothers.
 // Launch: blockDim 1024; dynamic shared memory 33 * padded max width * sizeof(T).
 constexpr int kRefreshBlock = 1024;
+template <class T>
+__device__ __forceinline__ T mul_rn(T a, T b);
+template <>
+__device__ __forceinline__ double mul_rn<double>(double a, double b) { return __dmul_rn(a, b); }
+template <>
+__device__ __forceinline__ float mul_rn<float>(float a, float b) { return __fmul_rn(a, b); }
 template <class T, class TA>
 __global__ void __launch_bounds__(kRefreshBlock) sell_refresh(int nc, const int32_t* __restrict__ coff,
                                                               const uint16_t* __restrict__ cs, const T* __restrict__ G,
@@ -1219,7 +1225,8 @@ __global__ void __launch_bounds__(kRefreshBlock) sell_refresh(int nc, const int3
       vn = cs[q0 + 32 + lane];
       gn = G[q0 + 32 + lane];
     }
-    const T p = v != 0xFFFFu ? sR[r][v & 7u] * gq : T(0);
+    // each product rounded on its own, then summed serially along the run
+    const T p = v != 0xFFFFu ? mul_rn<T>(sR[r][v & 7u], gq) : T(0);
     const bool real = v != 0xFFFFu;
     const int pos = real ? (int)((v >> 3) & 7u) : 0;
     const int maxpos = __reduce_max_sync(0xffffffffu, pos);

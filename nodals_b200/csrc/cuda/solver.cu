@@ -68,9 +68,14 @@ struct DBuf {
   }
   template <class U>
   void upload(const std::vector<U>& h) {
-    std::vector<T> t(h.begin(), h.end());
-    alloc(t.size());
-    if (n) NDS_CUDA(cudaMemcpy(p, t.data(), n * sizeof(T), cudaMemcpyHostToDevice));
+    if constexpr (std::is_same<U, T>::value) {
+      alloc(h.size());
+      if (n) NDS_CUDA(cudaMemcpy(p, h.data(), n * sizeof(T), cudaMemcpyHostToDevice));
+    } else {
+      std::vector<T> t(h.begin(), h.end());
+      alloc(t.size());
+      if (n) NDS_CUDA(cudaMemcpy(p, t.data(), n * sizeof(T), cudaMemcpyHostToDevice));
+    }
   }
   void zero(cudaStream_t s) {
     if (n) NDS_CUDA(cudaMemsetAsync(p, 0, n * sizeof(T), s));
@@ -350,6 +355,7 @@ class Solver final : public ISolver {
       std::vector<int32_t> col((size_t)nz), dpos((size_t)nv_);
       std::vector<int2> span((size_t)nv_);
       std::vector<T> kv((size_t)nz, T(0));
+#pragma omp parallel for schedule(static)
       for (int i = 0; i < nv_; ++i) {
         const int64_t rb = S.mom.row[(size_t)i], re = S.mom.row[(size_t)i + 1];
         const int64_t cb = natural ? rb : pos[(size_t)i];
@@ -363,6 +369,7 @@ class Solver final : public ISolver {
         for (int64_t k = cb + (re - rb); k < ce; ++k) col[(size_t)k] = i;
       }
       std::vector<int2> gspan((size_t)nv_);
+#pragma omp parallel for schedule(static)
       for (int q = 0; q < nv_; ++q) gspan[(size_t)q] = span[(size_t)S.color_rows[(size_t)q]];
       mspan_.upload(span);
       gspan_.upload(gspan);
@@ -419,6 +426,7 @@ class Solver final : public ISolver {
       std::vector<int32_t> zpos(8 * (size_t)nc_, -1);
       std::vector<uint8_t> slotz(8 * nz), fixz(nz, 0);
       std::vector<T> bz(3 * nz);
+#pragma omp parallel for schedule(static)
       for (size_t z = 0; z < nz; ++z) {
         const uint32_t pa = S.fine.packed[z];
         const size_t c = pa >> 3, a = pa & 7u;
@@ -624,6 +632,7 @@ class Solver final : public ISolver {
       Lv.val.upload(A.val);
       Lv.diag.upload(A.diag);
       std::vector<double> l1h((size_t)A.n);
+#pragma omp parallel for schedule(static)
       for (int i = 0; i < A.n; ++i) {
         double ss = 0.0;
         for (int64_t k = A.row[(size_t)i]; k < A.row[(size_t)i + 1]; ++k) ss += std::abs(A.val[(size_t)k]);
@@ -654,6 +663,7 @@ class Solver final : public ISolver {
         for (int i = 0; i < Ph.nf; ++i) pw = std::max<int>(pw, (int)(Ph.row[(size_t)i + 1] - Ph.row[(size_t)i]));
         std::vector<int32_t> ec((size_t)pw * Ph.nf, 0);
         std::vector<double> ev((size_t)pw * Ph.nf, 0.0);
+#pragma omp parallel for schedule(static)
         for (int i = 0; i < Ph.nf; ++i)
           for (int64_t q = Ph.row[(size_t)i]; q < Ph.row[(size_t)i + 1]; ++q) {
             const size_t o = (size_t)(q - Ph.row[(size_t)i]) * Ph.nf + i;
@@ -954,22 +964,22 @@ class Solver final : public ISolver {
     if (!(dmax > 0.0) || !std::isfinite(dmax)) throw std::runtime_error("FP16 level copy: no positive diagonal");
     const double scale = std::ldexp(1.0, (int)std::floor(std::log2(2048.0 / dmax)));
     std::vector<__half> hv(A.val.size());
+#pragma omp parallel for schedule(static)
     for (size_t k = 0; k < hv.size(); ++k)
       hv[k] = __float2half((float)std::min(std::max(A.val[k] * scale, -65504.0), 65504.0));
     Lv.hval.alloc(hv.size());
     NDS_CUDA(cudaMemcpy(Lv.hval.p, hv.data(), hv.size() * sizeof(__half), cudaMemcpyHostToDevice));
     Lv.hinv = 1.0 / scale;
     std::vector<int16_t> dc(A.col.size());
-    bool fits = true;
-    for (int i = 0; i < A.n && fits; ++i)
+    int too_far = 0;
+#pragma omp parallel for schedule(static) reduction(| : too_far)
+    for (int i = 0; i < A.n; ++i)
       for (int64_t k = A.row[(size_t)i]; k < A.row[(size_t)i + 1]; ++k) {
         const int d = A.col[(size_t)k] - i;
-        if (d < -32767 || d > 32767) {
-          fits = false;
-          break;
-        }
-        dc[(size_t)k] = (int16_t)d;
+        if (d < -32767 || d > 32767) too_far = 1;
+        else dc[(size_t)k] = (int16_t)d;
       }
+    const bool fits = too_far == 0;
     if (fits && !std::getenv("NDS_SELL_COL32")) Lv.hcol.upload(dc);
   }
   // launch f with the lanes per row of the FP16 level kernels
