@@ -443,8 +443,9 @@ __global__ void __launch_bounds__(kBlock) mom_assemble(MomArgs<T> g) {
 // together; the diagonal entry and the padding of a batch contribute 0.
 // Per lane the entries are summed in the order of the storage, then over
 // the 8 lanes.
-template <class T, int kGsAhead = 2>
-__global__ void __launch_bounds__(kBlock, kGsAhead == 2 ? 6 : 5) mom_gs_color(int count, const int32_t* __restrict__ rows,
+constexpr int kGsAhead = 2;
+template <class T>
+__global__ void __launch_bounds__(kBlock, 6) mom_gs_color(int count, const int32_t* __restrict__ rows,
                                                        const int2* __restrict__ span, const int32_t* __restrict__ ci,
                                                        const T* __restrict__ av, const T* __restrict__ diag,
                                                        const T* __restrict__ b0, const T* __restrict__ b1,

@@ -2066,14 +2066,9 @@ class Solver final : public ISolver {
       const int s = color_off_[(size_t)c], n = color_off_[(size_t)c + 1] - s;
       if (!n) continue;
       ProfScope ps(prof, st_, P_GS);
-      if (gs_ahead3_)
-        k::mom_gs_color<T, 3><<<grid_for((long long)n * 8), kBlock, 0, st_>>>(
-            n, color_rows_.p + s, gspan_.p + s, mcol_.p, A_.p, diag_.p, b_[0].p, b_[1].p, b_[2].p, uc(0), uc(1), uc(2),
-            T(o_.mom_omega));
-      else
-        k::mom_gs_color<T, 2><<<grid_for((long long)n * 8), kBlock, 0, st_>>>(
-            n, color_rows_.p + s, gspan_.p + s, mcol_.p, A_.p, diag_.p, b_[0].p, b_[1].p, b_[2].p, uc(0), uc(1), uc(2),
-            T(o_.mom_omega));
+      k::mom_gs_color<T><<<grid_for((long long)n * 8), kBlock, 0, st_>>>(
+          n, color_rows_.p + s, gspan_.p + s, mcol_.p, A_.p, diag_.p, b_[0].p, b_[1].p, b_[2].p, uc(0), uc(1), uc(2),
+          T(o_.mom_omega));
       NDS_LAUNCH();
     }
   }
@@ -2379,7 +2374,6 @@ class Solver final : public ISolver {
   double cont0_ = -1, cont_rel_ = 1, fine_lambda_ = 1, p_cheb_lambda_ = 1;
   bool finite_all_ = true;
   bool fused_assembly_ = false;
-  bool gs_ahead3_ = std::getenv("NDS_GS_AHEAD3") != nullptr;
   // lanes per row of the FP16 level SpMVs and of the restriction in the
   // mixed FP16 V-cycle (16 measured best at pipe1m: 0.25 ms per SIMPLE
   // iteration less than 32 or 8); NDS_LEVEL_LANES=8|16|32 overrides
