@@ -457,8 +457,8 @@ class Solver final : public ISolver {
 
     tm.mark("momentum_and_cells");
     // fine Schur refresh contributions, regrouped by destination slot in the
-    // reference's order and laid out in runs (one run per fine entry) that
-    // never straddle a 32-contribution chunk of the row: a run that would
+    // reference's order and laid out in runs (one run per fine entry, the
+    // longest first) that never straddle a 32-contribution chunk of the row: a run that would
     // cross a chunk boundary starts the next chunk, the gap is filled with
     // pad entries.  Per contribution: the code word cs (basis a bits 0-2,
     // position in its run bits 3-5, run tail bit 6, slot bits 7-15; pads are
@@ -468,27 +468,44 @@ class Solver final : public ISolver {
       std::vector<int32_t> plen((size_t)nc_ + 1, 0);
       std::vector<int32_t> poff((size_t)nc_ + 1, 0);
       OmpErr oerr;
-      // pass 1: counts per slot and padded row lengths
+      // pass 1: counts per slot and padded row lengths.  A row's runs are
+      // laid out longest first (stable in slot order), so the few long runs
+      // share a chunk and the chunks of short runs need few chain steps;
+      // the order of the contributions inside a run is unchanged.
       std::vector<uint8_t> cnt(F.col.size(), 0);
-#pragma omp parallel for schedule(dynamic, 1024)
-      for (int c = 0; c < nc_; ++c) {
-        oerr.run([&] {
-          const int rb = F.row[(size_t)c], len = F.row[(size_t)c + 1] - rb;
-          for (int q = F.contrib_off[(size_t)c]; q < F.contrib_off[(size_t)c + 1]; ++q) {
-            if (cnt[(size_t)rb + F.slot[(size_t)q]] == 32)
-              throw std::runtime_error("more than 32 contributions to one fine entry");
-            ++cnt[(size_t)rb + F.slot[(size_t)q]];
-          }
-          if (cnt[(size_t)F.diag_pos[(size_t)c]] == 0) throw std::runtime_error("fine Schur row without a diagonal contribution");
-          int L = 0;
-          for (int sl = 0; sl < len; ++sl) {
-            const int n = cnt[(size_t)rb + sl];
-            if (!n) continue;
-            if ((L & 31) + n > 32) L = (L + 31) & ~31;
-            L += n;
-          }
-          plen[(size_t)c + 1] = L;
+      auto run_order = [&](int rb, int len, std::vector<int32_t>& ord) {
+        ord.clear();
+        for (int sl = 0; sl < len; ++sl)
+          if (cnt[(size_t)rb + sl]) ord.push_back(sl);
+        std::stable_sort(ord.begin(), ord.end(), [&](int32_t x, int32_t y) {
+          return cnt[(size_t)rb + x] > cnt[(size_t)rb + y];
         });
+      };
+#pragma omp parallel
+      {
+        std::vector<int32_t> ord;
+#pragma omp for schedule(dynamic, 1024)
+        for (int c = 0; c < nc_; ++c) {
+          oerr.run([&] {
+            const int rb = F.row[(size_t)c], len = F.row[(size_t)c + 1] - rb;
+            for (int q = F.contrib_off[(size_t)c]; q < F.contrib_off[(size_t)c + 1]; ++q) {
+              // the code word holds a position in the run in three bits
+              if (cnt[(size_t)rb + F.slot[(size_t)q]] == 8)
+                throw std::runtime_error("more than 8 contributions to one fine entry");
+              ++cnt[(size_t)rb + F.slot[(size_t)q]];
+            }
+            if (cnt[(size_t)F.diag_pos[(size_t)c]] == 0)
+              throw std::runtime_error("fine Schur row without a diagonal contribution");
+            run_order(rb, len, ord);
+            int L = 0;
+            for (const int32_t sl : ord) {
+              const int n = cnt[(size_t)rb + sl];
+              if ((L & 31) + n > 32) L = (L + 31) & ~31;
+              L += n;
+            }
+            plen[(size_t)c + 1] = L;
+          });
+        }
       }
       oerr.rethrow();
       for (int c = 0; c < nc_; ++c) poff[(size_t)c + 1] = poff[(size_t)c] + plen[(size_t)c + 1];
@@ -498,16 +515,16 @@ class Solver final : public ISolver {
       // pass 2: stable placement (the order of (a, incidence)) into the runs
 #pragma omp parallel
       {
-        std::vector<int32_t> start, fill;
+        std::vector<int32_t> start, fill, ord;
 #pragma omp for schedule(dynamic, 1024)
         for (int c = 0; c < nc_; ++c) {
           const int rb = F.row[(size_t)c], len = F.row[(size_t)c + 1] - rb;
           start.assign((size_t)len, 0);
           fill.assign((size_t)len, 0);
+          run_order(rb, len, ord);
           int L = 0;
-          for (int sl = 0; sl < len; ++sl) {
+          for (const int32_t sl : ord) {
             const int n = cnt[(size_t)rb + sl];
-            if (!n) continue;
             if ((L & 31) + n > 32) L = (L + 31) & ~31;
             start[(size_t)sl] = L;
             L += n;
