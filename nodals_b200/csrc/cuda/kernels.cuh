@@ -1155,11 +1155,13 @@ __global__ void refresh_geometry(int nc, const int32_t* __restrict__ coff, const
 // Fine Schur numeric refresh A_p = B diag(rau) B^T (h8_precomputed_b.cuh:37-91)
 // into the SELL layout.  Each value is sum_q rau_{g(c,a_q)} G_q over the
 // row's contributions to that entry, in the reference's (basis, incidence)
-// order (h2b_fine_csr.cuh:480-520).  The contributions of a row are stored
-// as runs, one per fine entry, that never straddle a 32-entry chunk; the
-// code word cs gives the basis a (bits 0-2), the position in the run (bits
-// 3-5), the run's last entry (bit 6) and the entry's slot (bits 7-15); pads
-// are 0xFFFF.
+// order (h2b_fine_csr.cuh:480-520), each product rounded on its own.  The
+// contributions of a row are stored as runs, one per fine entry (the row's
+// longest runs first), that never straddle a 32-entry chunk; the code word
+// cs gives the basis a (bits 0-2), the position in the run (bits 3-5), the
+// run's last entry (bit 6) and the entry's slot (bits 7-15); pads are
+// 0xFFFF.  The next chunk's code words and factors are loaded before the
+// current chunk is summed.
 //
 // One block of 32 warps per SELL slice, a warp per row, a lane per
 // contribution: a shuffle chain sums every run sequentially (the lane at
@@ -1168,8 +1170,9 @@ __global__ void refresh_geometry(int nc, const int32_t* __restrict__ coff, const
 // puts the value into the slice's shared-memory image ([entry][row], row
 // stride 33 against bank conflicts), which the block then writes out
 // contiguously in SELL order (padding as zeros).  Values go to val
-// (operator precision T) and, in the mixed mode, also to valA (AMG precision
-// TA); the diagonal and L1 row sums feed the AMG smoothers.
+// (operator precision T) and, in the mixed modes, also to valA (AMG precision
+// TA) and valH (FP16, scaled by hscale and saturated); the diagonal and L1
+// row sums feed the AMG smoothers.
 // Launch: blockDim 1024; dynamic shared memory 33 * padded max width * sizeof(T).
 constexpr int kRefreshBlock = 1024;
 template <class T>
