@@ -593,13 +593,15 @@ __global__ void __launch_bounds__(kBlock) continuity(int nc, const int32_t* __re
 // Lane l of a G-lane group sums entries rb+l, rb+l+G, ... in that order;
 // the loads of eight entries are issued before their products are added
 // (same order, an eighth of the dependent memory round trips).
-// Coarse-level CSR rows (one to a few hundred entries) go to a warp each.
-// Lane l takes entries rb + l + 32u; one round of predicated loads (eight
-// per lane: columns and values, then the x gathers) covers a row of up to
-// 256 entries, so a row costs three dependent round trips (row bounds,
-// columns and values, gathers).  Longer rows take further rounds.
+// Coarse-level CSR rows (one to a few hundred entries) go to a warp each
+// (G = 32), or to 16 lanes on the FP16 copies of the mixed path.  Lane l
+// takes entries rb + l + G u; one round of predicated loads (eight per lane:
+// columns and values, then the x gathers) covers a row of up to 8 G entries,
+// so a row costs three dependent round trips (row bounds, columns and
+// values, gathers).  Longer rows take further rounds.
 // MT: the stored value type (T, or __half for an FP16 copy of a level whose
-// values are scaled by a power of two; the caller multiplies the row sum back)
+// values are scaled by a power of two; the caller multiplies the row sum back).
+// CT: the column type (int32 absolute, or int16 deltas to the row).
 template <class T, class MT>
 __device__ __forceinline__ T load_val(const MT* __restrict__ v, int k) {
   if constexpr (std::is_same<MT, __half>::value) return (T)__half2float(v[k]);
