@@ -919,63 +919,6 @@ __global__ void __launch_bounds__(kBlock) dense_mv(int n, const T* __restrict__ 
   if (lane == 0) x[i] = s;
 }
 
-// The coarsest step of the V-cycle in one block: c = R f (GL lanes per
-// coarse row, as restrict_rows), y = Ainv c (a warp per row, as dense_mv),
-// x += P y (a thread per row of the level above, as prolong_add), with c and
-// y in shared memory (2 nt values).  The same sums in the same order as the
-// three kernels; one launch instead of three tiny ones.
-// Launch: one block of 1024 threads, dynamic shared memory 2 * nt * sizeof(T).
-template <class T, int GL>
-__global__ void __launch_bounds__(1024) coarse_terminal(int nt, const int32_t* __restrict__ rr,
-                                                        const int32_t* __restrict__ rc, const T* __restrict__ rv,
-                                                        const T* __restrict__ f, const T* __restrict__ Ainv, int nf,
-                                                        int pw, const int32_t* __restrict__ pc,
-                                                        const T* __restrict__ pv, T* __restrict__ x) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* cs = reinterpret_cast<T*>(smem_raw);
-  T* ys = cs + nt;
-  const int t = threadIdx.x;
-  {
-    const int lane = t % GL, groups = blockDim.x / GL;
-    for (int I = t / GL; I < nt; I += groups) {
-      const T v = group_row_dot<T, T, int32_t, GL>(rr, rc, rv, f, I, lane, group_mask<GL>());
-      if (lane == 0) cs[I] = v;
-    }
-  }
-  __syncthreads();
-  {
-    const int lane = t & 31, warps = blockDim.x >> 5;
-    for (int i = t >> 5; i < nt; i += warps) {
-      const T* a = Ainv + (size_t)i * nt;
-      T v = 0;
-      for (int j = lane; j < nt; j += 32) v += a[j] * cs[j];
-      v = warp_sum(v);
-      if (lane == 0) ys[i] = v;
-    }
-  }
-  __syncthreads();
-  const size_t n = (size_t)nf;
-  for (int i = t; i < nf; i += blockDim.x) {
-    T v = 0;
-    int k = 0;
-    for (; k + 3 < pw; k += 4) {
-      const size_t o = (size_t)k * n + i;
-      const int c0 = pc[o], c1 = pc[o + n], c2 = pc[o + 2 * n], c3 = pc[o + 3 * n];
-      const T a0 = pv[o], a1 = pv[o + n], a2 = pv[o + 2 * n], a3 = pv[o + 3 * n];
-      const T x0 = ys[c0], x1 = ys[c1], x2 = ys[c2], x3 = ys[c3];
-      v += a0 * x0;
-      v += a1 * x1;
-      v += a2 * x2;
-      v += a3 * x3;
-    }
-    for (; k < pw; ++k) {
-      const size_t o = (size_t)k * n + i;
-      v += pv[o] * ys[pc[o]];
-    }
-    x[i] += v;
-  }
-}
-
 // multicolour GS colour pass on an AMG level (h8_main_base.cu:205-223)
 template <class T>
 __global__ void amg_gs_color(int count, const int32_t* __restrict__ rows, const int32_t* __restrict__ rp,

@@ -1202,13 +1202,6 @@ class Solver final : public ISolver {
   // lanes per coarse row of the restriction (the FP16 levels' count on the
   // mixed FP16 path, a warp otherwise)
   int restrict_lanes() const { return mixed_ && o_.amg_half ? level_lanes_ : 32; }
-  // the last restriction, the terminal solve and the prolongation as one
-  // block (the terminal level's two vectors fit shared memory; a
-  // polynomial smoother, so no diagonal step rides on that restriction)
-  bool terminal_fused() const {
-    return fuse_terminal_ && L_.size() >= 2 && o_.amg_smoother != NDS_SM_MCGS &&
-           2 * (size_t)L_.back().n * sizeof(TA) <= 48 * 1024 && restrict_lanes() != 8;
-  }
   // c = R f; with level >= 0 also the diagonal step of that level's
   // pre-smoother (see fuse_pre)
   void restrict_to(const Xfer& X, const TA* f, TA* c, int level = -1) {
@@ -1257,24 +1250,10 @@ class Solver final : public ISolver {
     smooth_level(A, b, x, level_lambda_[(size_t)l], pre_done);
     op_resid(level_op(A), x, b, A.r.p);
     Level& C = L_[(size_t)l + 1];
-    if (l + 2 == (int)L_.size() && terminal_fused()) {
-      // restriction, terminal solve and prolongation in one block
-      const Xfer& X = X_[(size_t)l + 1];
-      ProfScope ps(prof, st_, P_TERMINAL);
-      const size_t smem = 2 * (size_t)C.n * sizeof(TA);
-      if (restrict_lanes() == 16)
-        k::coarse_terminal<TA, 16><<<1, 1024, smem, st_>>>(C.n, X.rrow.p, X.rcol.p, X.rval.p, A.r.p, tinv_.p, X.nf,
-                                                           X.pw, X.pcol.p, X.pval.p, x);
-      else
-        k::coarse_terminal<TA, k::kRowLanes><<<1, 1024, smem, st_>>>(C.n, X.rrow.p, X.rcol.p, X.rval.p, A.r.p,
-                                                                     tinv_.p, X.nf, X.pw, X.pcol.p, X.pval.p, x);
-      NDS_LAUNCH();
-    } else {
-      const bool fuse = fuse_pre(l + 1);
-      restrict_to(X_[(size_t)l + 1], A.r.p, C.b.p, fuse ? l + 1 : -1);
-      vcycle(l + 1, C.b.p, C.x.p, fuse);
-      prolong(X_[(size_t)l + 1], C.x.p, x);
-    }
+    const bool fuse = fuse_pre(l + 1);
+    restrict_to(X_[(size_t)l + 1], A.r.p, C.b.p, fuse ? l + 1 : -1);
+    vcycle(l + 1, C.b.p, C.x.p, fuse);
+    prolong(X_[(size_t)l + 1], C.x.p, x);
     // r = b - A x into b (b is no longer needed), then the post-smoother
     // solves A corr = r and x += corr
     const double lam = level_lambda_[(size_t)l];
@@ -2415,7 +2394,6 @@ class Solver final : public ISolver {
   double cont0_ = -1, cont_rel_ = 1, fine_lambda_ = 1, p_cheb_lambda_ = 1;
   bool finite_all_ = true;
   bool fused_assembly_ = false;
-  bool fuse_terminal_ = std::getenv("NDS_SEPARATE_TERMINAL") == nullptr;
   // lanes per row of the FP16 level SpMVs and of the restriction in the
   // mixed FP16 V-cycle (16 measured best at pipe1m: 0.25 ms per SIMPLE
   // iteration less than 32 or 8); NDS_LEVEL_LANES=8|16|32 overrides

@@ -194,25 +194,6 @@ def test_sell_column_formats_agree(native, meshes, monkeypatch, variant):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_fused_terminal_step_agrees(native, meshes, monkeypatch, precision):
-    """The V-cycle's last restriction, terminal solve and prolongation in one
-    block (the default) and as three kernels (NDS_SEPARATE_TERMINAL=1) add
-    the same values in the same order: bitwise-equal runs."""
-    kw = dict(precision=precision) if precision == "fp64" else dict(precision="mixed", p_guess=4, amg_half=1)
-    P = _make(native, meshes, "pipe_small", **kw, **dict(ORACLE_CASES["sa_pcg"], amg_terminal=40))
-    assert P.counts()["levels"] >= 2
-    A = native.Solver(P)
-    monkeypatch.setenv("NDS_SEPARATE_TERMINAL", "1")
-    B = native.Solver(P)
-    for _ in range(6):
-        a, b = A.step(), B.step()
-        assert a.p_its == b.p_its and a.rel_cont == b.rel_cont and a.p_rel == b.p_rel
-    for x, y in zip(A.fields(), B.fields()):
-        assert np.array_equal(x, y)
-
-
-@pytest.mark.gpu
-@pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_momentum_storage_orders_agree(native, meshes, monkeypatch, precision):
     """The momentum matrix stored colour by colour with sector-padded rows
     (the default) and in natural CSR order (NDS_MOM_NATURAL_ORDER=1) give
