@@ -2,6 +2,9 @@
 
 #include <algorithm>
 #include <cerrno>
+#ifdef _OPENMP
+#include <parallel/algorithm>
+#endif
 #include <climits>
 #include <cmath>
 #include <cstdio>
@@ -138,7 +141,13 @@ void canonical_faces(Mesh& m, const std::vector<std::array<int32_t, 4>>& cells,
       sort3(r.a, r.b, r.c);
       f.push_back(r);
     }
+  // the keys are unique up to the two cells of an internal face, whose order
+  // the pairing below does not use: a parallel sort gives the same faces
+#ifdef _OPENMP
+  __gnu_parallel::sort(f.begin(), f.end(), tri_less);
+#else
   std::sort(f.begin(), f.end(), tri_less);
+#endif
   struct Internal { int32_t own, nei, a, b, c; };
   std::vector<Internal> in;
   std::vector<FaceRec> bd;
@@ -155,9 +164,15 @@ void canonical_faces(Mesh& m, const std::vector<std::array<int32_t, 4>>& cells,
     }
     i = j;
   }
-  std::sort(in.begin(), in.end(), [](const Internal& x, const Internal& y) {
+  // (owner, neighbour) pairs are unique
+  const auto own_nei = [](const Internal& x, const Internal& y) {
     return x.own != y.own ? x.own < y.own : x.nei < y.nei;
-  });
+  };
+#ifdef _OPENMP
+  __gnu_parallel::sort(in.begin(), in.end(), own_nei);
+#else
+  std::sort(in.begin(), in.end(), own_nei);
+#endif
   // boundary tags
   std::vector<FaceRec> tags(btri.size());
   for (size_t i = 0; i < btri.size(); ++i) {
