@@ -352,26 +352,18 @@ __global__ void __launch_bounds__(kBlock) mom_assemble(MomArgs<T> g) {
       }
     }
     if (FUSED == 0) {
-      // B^T p: the lanes fetch the terms of eight incidences at a time
-      // (contiguous per row), lane 0 adds them in incidence order
-      for (int zb = z0; zb < z1; zb += 8) {
-        T pv = 0, B0 = 0, B1 = 0, B2 = 0;
-        if (zb + lane8 < z1) {
-          const size_t z = (size_t)(zb + lane8);
-          pv = g.pz[z];
-          B0 = g.Bz[3 * z];
-          B1 = g.Bz[3 * z + 1];
-          B2 = g.Bz[3 * z + 2];
-        }
-        const int cnt = min(8, z1 - zb);
-        for (int u = 0; u < cnt; ++u) {
-          const T pu = __shfl_sync(gmask, pv, u, 8), b0 = __shfl_sync(gmask, B0, u, 8),
-                  b1 = __shfl_sync(gmask, B1, u, 8), b2 = __shfl_sync(gmask, B2, u, 8);
-          if (lane8 == 0) {
-            bt0 += b0 * pu;
-            bt1 += b1 * pu;
-            bt2 += b2 * pu;
-          }
+      // B^T p: lane d < 3 sums component d over the row's incidences in
+      // incidence order (B and p contiguous per row); lane 0 then takes the
+      // other two components
+      {
+        T btd = 0;
+        if (lane8 < 3)
+          for (int z = z0; z < z1; ++z) btd += g.Bz[3 * (size_t)z + lane8] * g.pz[z];
+        const T t1 = __shfl_sync(gmask, btd, 1, 8), t2 = __shfl_sync(gmask, btd, 2, 8);
+        if (lane8 == 0) {
+          bt0 = btd;
+          bt1 = t1;
+          bt2 = t2;
         }
       }
       // the row's convection rows, contiguous in incidence order, kAsmAhead
