@@ -1016,7 +1016,7 @@ __device__ __forceinline__ int sell_col(const Sell& A, int o, int i) {
   return A.col[o];
 }
 
-enum SellMode { SELL_Y = 0, SELL_RESID = 1, SELL_SMOOTH = 2, SELL_DOT = 3, SELL_SMOOTH_DOT = 4 };
+enum SellMode { SELL_Y = 0, SELL_RESID = 1, SELL_SMOOTH = 2, SELL_DOT = 3 };
 
 // Row dot product: entries in batches of 8 (two vector loads of values and
 // of columns, then the 8 x gathers), even entries into s0 and odd ones into
@@ -1086,29 +1086,13 @@ __device__ __forceinline__ T sell_row(const Sell& A, const MT* __restrict__ v, c
 // MODE SELL_RESID:  y = b - A x (and y2 = y when y2 != null)
 // MODE SELL_SMOOTH: y = x + w (b - A x) / den
 // MODE SELL_DOT:    y = A x, partials of x.y (grid-stride; blockDim = kBlock)
-// MODE SELL_SMOOTH_DOT: the smoothing step added to y2, then partials of
-//                   dv.y2 with the new y2 (grid-stride; the same rows per
-//                   thread and the same partials as the dot kernel)
 // MT: the operator's value type (T, or __half for the FP16 copy whose values
 // are a s, with vinv = 1 / s: a power of two, so the product is exact)
 template <class T, int MODE, bool D16, class MT = T>
 __global__ void __launch_bounds__(kBlock, 8) sell_spmv(Sell A, const MT* __restrict__ v, const T* __restrict__ x,
                                                     const T* __restrict__ b, const T* __restrict__ den, T w,
                                                     T* __restrict__ y, T* __restrict__ y2, double* __restrict__ part,
-                                                    T vinv = T(1), const T* __restrict__ dv = nullptr) {
-  if (MODE == SELL_SMOOTH_DOT) {
-    double acc[1] = {0.0};
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n; i += gridDim.x * blockDim.x) {
-      T s = sell_row<T, D16, MT>(A, v, x, i);
-      if constexpr (!std::is_same<MT, T>::value) s *= vinv;
-      const T val = x[i] + w * (b[i] - s) / den[i];
-      const T z = y2[i] + val;
-      y2[i] = z;
-      acc[0] += (double)dv[i] * (double)z;
-    }
-    write_partials<1>(acc, part);
-    return;
-  }
+                                                    T vinv = T(1)) {
   if (MODE == SELL_DOT) {
     double acc[1] = {0.0};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n; i += gridDim.x * blockDim.x) {

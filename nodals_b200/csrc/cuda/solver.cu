@@ -931,23 +931,22 @@ class Solver final : public ISolver {
     const int16_t* ch = nullptr;  // CSR levels with vh: columns as deltas to the row
   };
   template <int MODE, class V>
-  void sell_launch(const OpView<V>& A, int grid, const V* x, const V* b, const V* den, double w, V* y, V* y2,
-                   const V* dv = nullptr) {
+  void sell_launch(const OpView<V>& A, int grid, const V* x, const V* b, const V* den, double w, V* y, V* y2) {
     if constexpr (std::is_same<V, float>::value) {
       if (A.vh) {
         if (A.s.dcol)
           k::sell_spmv<V, MODE, true, __half><<<grid, kBlock, 0, st_>>>(A.s, A.vh, x, b, den, V(w), y, y2, part_.p,
-                                                                          V(A.vinv), dv);
+                                                                          V(A.vinv));
         else
           k::sell_spmv<V, MODE, false, __half><<<grid, kBlock, 0, st_>>>(A.s, A.vh, x, b, den, V(w), y, y2, part_.p,
-                                                                           V(A.vinv), dv);
+                                                                           V(A.vinv));
         return;
       }
     }
     if (A.s.dcol)
-      k::sell_spmv<V, MODE, true><<<grid, kBlock, 0, st_>>>(A.s, A.v, x, b, den, V(w), y, y2, part_.p, V(1), dv);
+      k::sell_spmv<V, MODE, true><<<grid, kBlock, 0, st_>>>(A.s, A.v, x, b, den, V(w), y, y2, part_.p);
     else
-      k::sell_spmv<V, MODE, false><<<grid, kBlock, 0, st_>>>(A.s, A.v, x, b, den, V(w), y, y2, part_.p, V(1), dv);
+      k::sell_spmv<V, MODE, false><<<grid, kBlock, 0, st_>>>(A.s, A.v, x, b, den, V(w), y, y2, part_.p);
   }
   // physical operator (precision T) and the AMG's fine operator (precision TA)
   OpView<T> fine_op() const { return {nc_, true, sell_, nullptr, nullptr, fval_.p, P_FINE_SPMV}; }
@@ -1048,16 +1047,11 @@ class Solver final : public ISolver {
       k::spmv_resid<V><<<grid_for((long long)A.n * k::kRowLanes), kBlock, 0, st_>>>(A.n, A.rp, A.ci, A.v, x, b, r, r2, den, V(w));
     NDS_LAUNCH();
   }
-  // xout = xin + w (b - A xin) / den, or (add_to given) add_to += that; with
-  // dot_with (SELL operators and add_to only) also the block partials of
-  // dot_with . add_to, as the dot kernel forms them
+  // xout = xin + w (b - A xin) / den, or (add_to given) add_to += that
   template <class V>
-  void op_smooth(const OpView<V>& A, const V* xin, const V* b, const V* den, double w, V* xout, V* add_to = nullptr,
-                 const V* dot_with = nullptr) {
+  void op_smooth(const OpView<V>& A, const V* xin, const V* b, const V* den, double w, V* xout, V* add_to = nullptr) {
     ProfScope ps(prof, st_, A.cat);
-    if (A.sell && add_to && dot_with)
-      sell_launch<k::SELL_SMOOTH_DOT, V>(A, red_grid(A.n), xin, b, den, w, xout, add_to, dot_with);
-    else if (A.sell) sell_launch<k::SELL_SMOOTH, V>(A, grid_for(A.n), xin, b, den, w, xout, add_to);
+    if (A.sell) sell_launch<k::SELL_SMOOTH, V>(A, grid_for(A.n), xin, b, den, w, xout, add_to);
     else if (A.vh && A.ch && std::is_same<V, float>::value)
       level_half_launch(A, [&](auto gl) {
         constexpr int GL = decltype(gl)::value;
@@ -1122,10 +1116,8 @@ class Solver final : public ISolver {
   // first_done: the diagonal step is already in poly_first(x, pong) (written
   // by the residual kernel); add_to: the result is added to add_to instead
   // of stored in x.
-  // dot_with: the last step also forms the partials of dot_with . add_to
   void poly_smooth(const OpView<TA>& A, const TA* diag, const TA* b, TA* x, TA* pong, double lambda, bool cheb,
-                   const TA* den_jac, int sweeps, bool first_done = false, TA* add_to = nullptr,
-                   const TA* dot_with = nullptr) {
+                   const TA* den_jac, int sweeps, bool first_done = false, TA* add_to = nullptr) {
     const int n = A.n;
     const PolyPlan pl = poly_plan(lambda, cheb, diag, den_jac, sweeps);
     TA* cur = poly_first(pl, x, pong);
@@ -1137,8 +1129,7 @@ class Solver final : public ISolver {
     const double lo = cheb ? o_.amg_lambda_low_fraction * lambda : 0.0;
     for (int kk = 1; kk <= pl.m; ++kk) {
       const double w = cheb ? 1.0 / cheb_root(lambda, lo, kk, o_.amg_cheb_degree) : o_.amg_jacobi_omega;
-      op_smooth(A, cur, b, cheb ? diag : den_jac, w, nxt, kk == pl.m ? add_to : nullptr,
-                kk == pl.m ? dot_with : nullptr);
+      op_smooth(A, cur, b, cheb ? diag : den_jac, w, nxt, kk == pl.m ? add_to : nullptr);
       std::swap(cur, nxt);
     }
     if (pl.m == 0 && add_to) vaxpy(n, 1.0, (const TA*)x, add_to);
@@ -1281,11 +1272,8 @@ class Solver final : public ISolver {
     op_resid(level_op(A), x, b, A.b.p, poly_first(pl, A.corr.p, A.pong.p), pl.den0, pl.w0);
     poly_smooth(level_op(A), A.diag.p, A.b.p, A.corr.p, A.pong.p, lam, cheb, den, o_.amg_jacobi_coarse_sweeps, true, x);
   }
-  // pre_done: the fine pre-smoother's diagonal step is already in place;
-  // dot_with: the last post-smoothing step also forms the partials of
-  // dot_with . z (only where it is a SELL step added to z: the caller checks
-  // fused_dot_ok())
-  void amg_apply(const TA* b, TA* z, bool pre_done = false, const TA* dot_with = nullptr) {
+  // pre_done: the fine pre-smoother's diagonal step is already in place
+  void amg_apply(const TA* b, TA* z, bool pre_done = false) {
     smooth_fine(b, z, pre_done);
     op_resid(fine_opV(), z, b, fr_.p);
     Level& C = L_[0];
@@ -1307,11 +1295,8 @@ class Solver final : public ISolver {
     const PolyPlan pl = poly_plan(fine_lambda_, cheb, fdiag_.p, den, o_.amg_jacobi_fine_sweeps);
     op_resid(fine_opV(), z, b, frhs_.p, poly_first(pl, fcorr_.p, fpong_.p), pl.den0, pl.w0);
     poly_smooth(fine_opV(), fdiag_.p, frhs_.p, fcorr_.p, fpong_.p, fine_lambda_, cheb, den, o_.amg_jacobi_fine_sweeps,
-                true, z, dot_with);
+                true, z);
   }
-  // the fine post-smoother ends with a SELL step added to z (so that step can
-  // form the r.z partials of PCG)
-  bool fused_dot_ok() const { return o_.amg_smoother != NDS_SM_MCGS && fine_plan().m > 0; }
 
   // ------------------------------------------------------ spectrum estimates
   double power_fine(int its, double safety) {
@@ -1717,19 +1702,13 @@ class Solver final : public ISolver {
   // one pass of the FP32 PCG loop: z = M r; rho; p; q = A p; alpha; x, r; check
   void pcgf_body(cudaGraphConditionalHandle h) {
     if constexpr (!kSame) {
-      // z = M r.  The fine pre-smoother's first step on r is already in
-      // place (taken by scale_to_float before the loop and by xr_update
-      // after it), and the last post-smoothing step forms the r.z partials
-      // (the same partials as the dot kernel).
+      // the fine pre-smoother's first step on r is already in place (taken
+      // by scale_to_float before the loop and by xr_update after it)
+      if (pre_fused()) amg_apply(rf_.p, zf_.p, true);
+      else precond_f(rf_.p, zf_.p);
       const int g = red_grid(nc_);
-      if (pre_fused() && fused_dot_ok()) {
-        amg_apply(rf_.p, zf_.p, true, rf_.p);
-      } else {
-        if (pre_fused()) amg_apply(rf_.p, zf_.p, true);
-        else precond_f(rf_.p, zf_.p);
-        k::dot<float><<<g, kBlock, 0, st_>>>(nc_, rf_.p, zf_.p, part_.p);
-        NDS_LAUNCH();
-      }
+      k::dot<float><<<g, kBlock, 0, st_>>>(nc_, rf_.p, zf_.p, part_.p);
+      NDS_LAUNCH();
       reduce_pcg<k::PCG_RHO>(g, S_RHON);
       k::p_update_dev<float><<<grid_for(nc_), kBlock, 0, st_>>>(nc_, sc_.p + S_BETA, ctl_.p, zf_.p, pf_.p);
       NDS_LAUNCH();
