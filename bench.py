@@ -177,6 +177,51 @@ def fine_spmv_bytes(problem, s: int, sx: int | None = None) -> float:
     return nnz * (s + 4) + 4 * (n + 1) + 2 * sx * n
 
 
+def outer_kernel_bytes(problem) -> dict:
+    """Compulsory bytes per SIMPLE iteration of the kernels outside the
+    pressure solve, FP64 values (s = 8) and 4-byte indices, counted once per
+    array with the actual counts: momentum assembly (reset, convection,
+    finalize, B^T p, right-hand sides), one Gauss-Seidel sweep, the
+    continuity residual, and the fine-operator refresh (FP64 values plus the
+    FP32 and FP16 copies of the mixed path)."""
+    s = 8
+    c = problem.counts()
+    nc, nv = c["nc"], c["nv"]
+    zm = int(problem.array("mom.row")[-1])
+    zp = int(problem.array("fine.row")[-1])
+    zd = int(problem.array("fine.contribOff")[-1])
+    return {
+        "mom_assemble": 5 * s * zm + (172 + 48 * s) * nc + (12 + 25 * s) * nv,
+        "mom_gs": (4 + s) * zm + (16 + 8 * s) * nv,
+        "continuity": (48 * s + 36) * nc,
+        "fine_refresh": (s + 4 + 2) * zp + 5 * zd + (24 * s + 8) * nc + s * nv,
+    }
+
+
+def outer_kernels(prof, kbytes, steps) -> dict | None:
+    """Achieved algorithmic GB/s of the kernels outside the pressure solve in
+    the profiled pass (CUDA events around their launches; the sweep runs
+    beside the refresh on another stream, so both times include the
+    contention), and their fraction of the measured copy bandwidth."""
+    if steps <= 0:
+        return None
+    peak, kind = _peaks()
+    out = {}
+    for name, b in kbytes.items():
+        calls, tot = prof.get(name, (0, 0.0))
+        if calls == 0:
+            continue
+        ms = tot / steps
+        gbs = b / (ms * 1e-3) / 1e9
+        out[name] = {"ms_per_step": round(ms, 4), "algorithmic_bytes": int(b), "achieved_gbs": round(gbs, 1),
+                     "frac": round(gbs / peak, 3)}
+    out["peak_gbs"] = peak
+    out["peak_kind"] = kind
+    out["note"] = ("mom_gs and fine_refresh run concurrently on two streams; mom_assemble covers the cell and row "
+                   "passes; bytes per the survey's per-kernel formulas with FP64 values")
+    return out
+
+
 def sell_format_bytes(problem, s: int, sx: int | None = None) -> float:
     """Bytes the SELL-32x4 fine operator actually streams per SpMV: padded
     values (s B) and 16-bit column deltas (slice width rounded up to a
@@ -237,6 +282,7 @@ def run_nodals(args):
         prof = S.profile_read()
         S.profile(False)
         counts = P.counts()
+        kbytes = outer_kernel_bytes(P)
         del S, P
 
         # --- the metric: a complete solve through the C ABI from host arrays --
@@ -344,6 +390,9 @@ def run_nodals(args):
             "gpu_launches_complete_solve": int(solve_launches),
             "clocks": clk.summary(),
             "kernel_ms_profiled_pass": {k: round(v[1], 3) for k, v in prof.items()},
+            "outer_kernels": outer_kernels(prof, kbytes, args.profile_steps),
+            "simple_its_per_s": round(rep.outer_its / max(rep.loop_ms / 1e3, 1e-9), 2),
+            "pressure_ms_per_outer_iteration": round(rep.pressure_ms / max(rep.outer_its, 1), 3),
         }
         print(json.dumps(line), flush=True)
     if ws > 1:
